@@ -1,0 +1,715 @@
+// pgb_g5.cu -- GRAPE-5 API (newton) and the newton_quad g5c_* API on the B200 engine.
+//
+// Drop-in for PG5/newton/libpg5 (gp5util.h:10-39, phantom_g5.c, pg5_fortran.c) and
+// PG5/newton_quad/quad (quad_util.h:8-15, quad_g5c.c).  Built twice:
+//   libpg5.so     plain softening   (g5_set_xmj(adr, nj, xj, mj))
+//   libpg5sym.so  -DPGB_SYMMETRIC   (g5_set_xmj(adr, nj, xj, mj, epsj2), GravityKernel0)
+//
+// Semantics kept from the reference:
+//  * set_* calls convert double -> float immediately (phantom_g5.c:100-205); j-records are
+//    addressed absolutely (xj[adr..adr+nj) is read, as phantom_g5.c:193 does).
+//  * g5_set_xi uses eps^2 = (float)(Eps*Eps) from g5_set_eps_to_all (phantom_g5.c:107);
+//    g5_set_xei takes eps^2 per particle (phantom_g5.c:126).
+//  * g5_get_force returns acc = sum m dx/r^3 and pot = +sum m/r (self pair included), the sign
+//    the reference returns after Pot_correct (phantom_g5.c:251-259).  The reference's rsqrt
+//    bias factors (1-3 bias, 1-bias) are NOT applied: they only undo the 12-bit rsqrt's mean
+//    error, and the Newton-refined MUFU rsqrt has none to undo.
+//  * g5c_* (quad_g5c.c:198-303) share the i-pipes of g5_set_xiMC and the output path of
+//    g5_get_forceMC, so the quadrupole potential comes back as -sum(phi_p + phi_q) while the
+//    monopole one comes back positive; callers reconcile this (source.cpp:854, 866).
+// Deliberate differences:
+//  * g5_calculate_force_on_x[e][MC] evaluate all ni in one launch instead of ni/4 calls.
+//  * set_xmj does not write the zero padding at [nj, nj + (4 - nj%4)%4) (phantom_g5.c:199-204):
+//    the kernels loop over exactly n j-records, and that padding can overwrite real records
+//    when adr > 0.  set_xmjMC with an odd nj does not read xj[adr+nj] (quad_g5c.c:206-259,
+//    phantom_g5.c:148-166 read one record past the end).
+//  * j-memory capacity is 1 Mi records (PGB_G5_JMEMSIZE), not 64 Ki; exceeding it is an error,
+//    not an out-of-bounds write.
+#include "pgb_g5_kernels.cuh"
+
+using namespace pgb;
+
+namespace {
+
+#ifdef PGB_SYMMETRIC
+const char* LIB = "libpg5sym";
+constexpr int PARTICLE_KIND = G5_SYMMETRIC;
+#else
+const char* LIB = "libpg5";
+constexpr int PARTICLE_KIND = G5_NEWTON;
+#endif
+
+ErrorSlot g_err;
+
+constexpr int MAXDEV = 64;
+constexpr int NT = 128, IPT = 4, ITILE = NT * IPT;
+constexpr int MAXPIPE = 4096;
+
+int env_int(const char* name, int dflt, int lo, int hi) {
+    const char* s = std::getenv(name);
+    if (!s || !*s) return dflt;
+    int v = std::atoi(s);
+    return v < lo ? lo : (v > hi ? hi : v);
+}
+
+int npipes() {
+    static int v = env_int("PGB_G5_NPIPES", 4, 1, MAXPIPE);
+    return v;
+}
+int jmemsize() {
+    static int v = env_int("PGB_G5_JMEMSIZE", 1 << 20, 1024, 1 << 26);
+    return v;
+}
+
+std::mutex g_init_mu;
+int g_device = -1;
+double g_eps = 0.0;  // phantom_g5.c:17, shared by all devids
+
+bool ensure_device() {
+    if (g_device >= 0) {
+        PGB_CUDA_OR(g_err, LIB, cudaSetDevice(g_device), return false);
+        return true;
+    }
+    std::lock_guard<std::mutex> g(g_init_mu);
+    if (g_device < 0) {
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) {
+            raise(g_err, LIB, PGB_ERR_NOGPU, "no CUDA device available");
+            return false;
+        }
+        int d = env_int("PGB_DEVICE", 0, 0, n - 1);
+        PGB_CUDA_OR(g_err, LIB, cudaSetDevice(d), return false);
+        g_device = d;
+    }
+    PGB_CUDA_OR(g_err, LIB, cudaSetDevice(g_device), return false);
+    return true;
+}
+
+template <int KIND>
+int occupancy() {
+    static int v = 0;
+    if (!v) {
+        int b = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g5_kernel<KIND, NT, IPT>, NT, 0);
+        v = b > 0 ? b : 1;
+    }
+    return v;
+}
+
+int occupancy_of(int kind) {
+    switch (kind) {
+        case G5_SYMMETRIC: return occupancy<G5_SYMMETRIC>();
+        case G5_QUAD: return occupancy<G5_QUAD>();
+        default: return occupancy<G5_NEWTON>();
+    }
+}
+
+cudaError_t launch_kind(int kind, int grid, const G5Args& a, cudaStream_t s) {
+    switch (kind) {
+        case G5_SYMMETRIC: g5_kernel<G5_SYMMETRIC, NT, IPT><<<grid, NT, 0, s>>>(a); break;
+        case G5_QUAD: g5_kernel<G5_QUAD, NT, IPT><<<grid, NT, 0, s>>>(a); break;
+        default: g5_kernel<G5_NEWTON, NT, IPT><<<grid, NT, 0, s>>>(a); break;
+    }
+    return cudaGetLastError();
+}
+
+// Chunk length for one item so that the whole call yields about 4 tasks per resident CTA.
+int choose_jchunk(long long itiles_total, int nj, int slots) {
+    if (nj <= 0) return 1;
+    long long target = 4LL * slots;
+    long long nch = (target + itiles_total - 1) / (itiles_total > 0 ? itiles_total : 1);
+    long long maxch = (nj + 127) / 128;  // at least 128 j per chunk
+    if (nch > maxch) nch = maxch;
+    if (nch < 1) nch = 1;
+    return (int)((nj + nch - 1) / nch);
+}
+
+// Staged work list + launch of one devid / plan.
+struct Launcher {
+    Stager<float4, double4> st;
+
+    bool stage(cudaStream_t s, const std::vector<Task>& tasks, const std::vector<Group>& groups, int rows,
+               const float4* i_host, int ni_host) {
+        PGB_CUDA_OR(g_err, LIB, st.stage(s, tasks, groups, rows, ITILE, i_host, ni_host), return false);
+        return true;
+    }
+
+    // Launch over the staged work list.  `reset_counter`: zero the task counter first (needed
+    // when the same staged list is launched again, e.g. from a CUDA graph).
+    bool launch(int kind, cudaStream_t s, const float4* i_dev, const float4* jpos, const float4* jaux,
+                double4* out, bool reset_counter) {
+        if (st.ntasks <= 0) return true;
+        if (reset_counter) PGB_CUDA_OR(g_err, LIB, cudaMemsetAsync(st.counter(), 0, sizeof(int), s), return false);
+        G5Args a;
+        a.ipos = i_dev ? i_dev : st.irecs();
+        a.jpos = jpos;
+        a.jaux = jaux;
+        a.tasks = st.tasks();
+        a.ntasks = st.ntasks;
+        a.task_counter = st.counter();
+        a.groups = st.groups();
+        a.group_counters = st.dgcnt.p;
+        a.partial = st.dpart.p;
+        a.out = out;
+        a.itile = ITILE;
+        int slots = sm_count(g_device) * occupancy_of(kind);
+        int grid = st.ntasks < slots ? st.ntasks : slots;
+        PGB_CUDA_OR(g_err, LIB, launch_kind(kind, grid, a, s), return false);
+        return true;
+    }
+    void release() { st.release(); }
+};
+
+struct Dev {
+    std::mutex mu;
+    bool ready = false;
+    cudaStream_t stream = nullptr;
+    // j-particles: host mirror (pinned) + device copy, dirty range uploaded lazily
+    HostBuf<float4> jh;
+    HostBuf<float4> jeh;  // symmetric: eps2_j in .x
+    DevBuf<float4> jd, jed;
+    int jdirty_lo = 1 << 30, jdirty_hi = 0, jcap = 0;
+    int nbody = 0;
+    // quadrupole cells: word 0 (x y z m) + 2 words of Q per cell
+    HostBuf<float4> ch, cqh;
+    DevBuf<float4> cd, cqd;
+    int cdirty_lo = 1 << 30, cdirty_hi = 0, ccap = 0;
+    int ncell = 0;
+    // i pipes and results of g5_run / g5c_run
+    float4 ip[MAXPIPE];
+    DevBuf<double4> outd;
+    HostBuf<double4> outh;
+    HostBuf<float4> ibuf;
+    int pending = 0;     // number of results of the last g5_run / g5c_run (0: none)
+    bool inflight = false;  // a g5_run has not been synchronised yet
+    Launcher L;
+};
+
+// Wait for an unsynchronised g5_run before the host mirrors it reads from are rewritten.
+bool quiesce(Dev& d) {
+    if (!d.inflight) return true;
+    PGB_CUDA_OR(g_err, LIB, cudaStreamSynchronize(d.stream), return false);
+    d.inflight = false;
+    return true;
+}
+
+Dev g_devs[MAXDEV];
+
+Dev* get_dev(int devid) {
+    if (devid < 0 || devid >= MAXDEV) {
+        raise(g_err, LIB, PGB_ERR_ARG, "devid %d out of range [0, %d)", devid, MAXDEV);
+        return nullptr;
+    }
+    if (!ensure_device()) return nullptr;
+    Dev& d = g_devs[devid];
+    if (!d.ready) {
+        PGB_CUDA_OR(g_err, LIB, cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking), return nullptr);
+        d.ready = true;
+    }
+    return &d;
+}
+
+bool grow_j(Dev& d, int need) {
+    if (need > jmemsize()) {
+        raise(g_err, LIB, PGB_ERR_CAPACITY, "j-memory overflow: %d records > jmemsize %d", need, jmemsize());
+        return false;
+    }
+    if (need <= d.jcap) return true;
+    int cap = d.jcap ? d.jcap : 4096;
+    while (cap < need) cap *= 2;
+    if (cap > jmemsize()) cap = jmemsize();
+    PGB_CUDA_OR(g_err, LIB, d.jh.reserve(cap, true), return false);
+    PGB_CUDA_OR(g_err, LIB, d.jeh.reserve(cap, true), return false);
+    for (int j = d.jcap; j < cap; j++) {
+        d.jh.p[j] = make_float4(0, 0, 0, 0);
+        d.jeh.p[j] = make_float4(1, 0, 0, 0);
+    }
+    d.jdirty_lo = 0;  // new device buffer: upload everything written so far
+    d.jdirty_hi = cap;
+    d.jcap = cap;
+    return true;
+}
+
+bool grow_c(Dev& d, int need) {
+    if (need > jmemsize() / 2) {
+        raise(g_err, LIB, PGB_ERR_CAPACITY, "cell-memory overflow: %d cells > %d", need, jmemsize() / 2);
+        return false;
+    }
+    if (need <= d.ccap) return true;
+    int cap = d.ccap ? d.ccap : 2048;
+    while (cap < need) cap *= 2;
+    PGB_CUDA_OR(g_err, LIB, d.ch.reserve(cap, true), return false);
+    PGB_CUDA_OR(g_err, LIB, d.cqh.reserve(2 * (size_t)cap, true), return false);
+    for (int j = d.ccap; j < cap; j++) {
+        d.ch.p[j] = make_float4(0, 0, 0, 0);
+        d.cqh.p[2 * j] = make_float4(0, 0, 0, 0);
+        d.cqh.p[2 * j + 1] = make_float4(0, 0, 0, 0);
+    }
+    d.cdirty_lo = 0;
+    d.cdirty_hi = cap;
+    d.ccap = cap;
+    return true;
+}
+
+bool flush_j(Dev& d) {
+    if (d.jdirty_hi <= d.jdirty_lo) return true;
+    PGB_CUDA_OR(g_err, LIB, d.jd.reserve(d.jcap), return false);
+    size_t lo = d.jdirty_lo, n = (size_t)(d.jdirty_hi - d.jdirty_lo);
+    PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(d.jd.p + lo, d.jh.p + lo, n * sizeof(float4),
+                                            cudaMemcpyHostToDevice, d.stream), return false);
+    if (PARTICLE_KIND == G5_SYMMETRIC) {
+        PGB_CUDA_OR(g_err, LIB, d.jed.reserve(d.jcap), return false);
+        PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(d.jed.p + lo, d.jeh.p + lo, n * sizeof(float4),
+                                                cudaMemcpyHostToDevice, d.stream), return false);
+    }
+    d.jdirty_lo = 1 << 30;
+    d.jdirty_hi = 0;
+    return true;
+}
+
+bool flush_c(Dev& d) {
+    if (d.cdirty_hi <= d.cdirty_lo) return true;
+    PGB_CUDA_OR(g_err, LIB, d.cd.reserve(d.ccap), return false);
+    PGB_CUDA_OR(g_err, LIB, d.cqd.reserve(2 * (size_t)d.ccap), return false);
+    size_t lo = d.cdirty_lo, n = (size_t)(d.cdirty_hi - d.cdirty_lo);
+    PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(d.cd.p + lo, d.ch.p + lo, n * sizeof(float4),
+                                            cudaMemcpyHostToDevice, d.stream), return false);
+    PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(d.cqd.p + 2 * lo, d.cqh.p + 2 * lo, 2 * n * sizeof(float4),
+                                            cudaMemcpyHostToDevice, d.stream), return false);
+    d.cdirty_lo = 1 << 30;
+    d.cdirty_hi = 0;
+    return true;
+}
+
+// Launch `kind` for ni i-records (host) against this devid's j-memory (nbody records) or cell
+// memory (ncell cells).  Results land in d.outh after the stream synchronises.
+bool compute(Dev& d, int kind, int ni, const float4* ih) {
+    int nj = kind == G5_QUAD ? d.ncell : d.nbody;
+    if (kind == G5_QUAD) {
+        if (!grow_c(d, nj > 0 ? nj : 1) || !flush_c(d)) return false;
+    } else {
+        if (!grow_j(d, nj > 0 ? nj : 1) || !flush_j(d)) return false;
+    }
+    PGB_CUDA_OR(g_err, LIB, d.outd.reserve(ni > 0 ? ni : 1), return false);
+    PGB_CUDA_OR(g_err, LIB, d.outh.reserve(ni > 0 ? ni : 1), return false);
+    std::vector<Task> tasks;
+    std::vector<Group> groups;
+    int slots = sm_count(g_device) * occupancy_of(kind);
+    long long itiles = (ni + ITILE - 1) / ITILE;
+    int jchunk = choose_jchunk(itiles, nj, slots);
+    int rows = plan_item(tasks, groups, 0, ni, 0, nj, ITILE, jchunk, 0);
+    const float4* jpos = kind == G5_QUAD ? d.cd.p : d.jd.p;
+    const float4* jaux = kind == G5_QUAD ? d.cqd.p : (kind == G5_SYMMETRIC ? d.jed.p : nullptr);
+    if (!d.L.stage(d.stream, tasks, groups, rows, ih, ni)) return false;
+    if (!d.L.launch(kind, d.stream, nullptr, jpos, jaux, d.outd.p, false)) return false;
+    if (ni > 0)
+        PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(d.outh.p, d.outd.p, (size_t)ni * sizeof(double4),
+                                                cudaMemcpyDeviceToHost, d.stream), return false);
+    return true;
+}
+
+bool sync_dev(Dev& d) {
+    PGB_CUDA_OR(g_err, LIB, cudaStreamSynchronize(d.stream), return false);
+    d.inflight = false;
+    return true;
+}
+
+void write_out(const double4* o, int ni, double (*a)[3], double* p) {
+    for (int i = 0; i < ni; i++) {
+        a[i][0] = o[i].x;
+        a[i][1] = o[i].y;
+        a[i][2] = o[i].z;
+        p[i] = -o[i].w;  // GRAPE-5 return sign (phantom_g5.c:251-259)
+    }
+}
+
+bool check_ni(int ni) {
+    if (ni < 0 || ni > npipes()) {
+        raise(g_err, LIB, PGB_ERR_ARG, "ni = %d outside [0, %d] pipelines", ni, npipes());
+        return false;
+    }
+    return true;
+}
+
+void set_xi_impl(int devid, int ni, const double (*xi)[3], const double* eps2, bool per_i) {
+    if (!check_ni(ni)) return;
+    Dev* d = get_dev(devid);
+    if (!d) return;
+    std::lock_guard<std::mutex> g(d->mu);
+    float e_all = (float)(g_eps * g_eps);
+    for (int i = 0; i < ni; i++)
+        d->ip[i] = make_float4((float)xi[i][0], (float)xi[i][1], (float)xi[i][2], per_i ? (float)eps2[i] : e_all);
+}
+
+void run_impl(int devid, int kind) {
+    Dev* d = get_dev(devid);
+    if (!d) return;
+    std::lock_guard<std::mutex> g(d->mu);
+    int n = npipes();
+    if (!quiesce(*d)) return;
+    if (compute(*d, kind, n, d->ip)) {
+        d->pending = n;
+        d->inflight = true;
+    }
+}
+
+void get_force_impl(int devid, int ni, double (*a)[3], double* p) {
+    if (!check_ni(ni)) return;
+    Dev* d = get_dev(devid);
+    if (!d) return;
+    std::lock_guard<std::mutex> g(d->mu);
+    if (!d->pending) {
+        raise(g_err, LIB, PGB_ERR_ARG, "g5_get_force without a preceding g5_run on devid %d", devid);
+        return;
+    }
+    if (!sync_dev(*d)) return;
+    write_out(d->outh.p, ni, a, p);
+}
+
+// All ni in one launch (the reference loops over npipes-wide calls, phantom_g5.c:276-300).
+void calc_impl(int devid, int kind, const double (*x)[3], const double* eps2, double (*a)[3], double* p, int ni) {
+    if (ni <= 0) return;
+    Dev* d = get_dev(devid);
+    if (!d) return;
+    Dev* dj = d;
+    std::lock_guard<std::mutex> g(dj->mu);
+    if (!quiesce(*dj)) return;
+    if (dj->ibuf.reserve(ni) != cudaSuccess) {
+        raise(g_err, LIB, PGB_ERR_CUDA, "pinned i-buffer allocation failed (%d)", ni);
+        return;
+    }
+    float e_all = (float)(g_eps * g_eps);
+    for (int i = 0; i < ni; i++)
+        dj->ibuf.p[i] = make_float4((float)x[i][0], (float)x[i][1], (float)x[i][2], eps2 ? (float)eps2[i] : e_all);
+    if (!compute(*dj, kind, ni, dj->ibuf.p) || !sync_dev(*dj)) return;
+    write_out(dj->outh.p, ni, a, p);
+}
+
+}  // namespace
+
+// ============================================================================================
+// GRAPE-5 API (PG5/newton/libpg5/gp5util.h:10-39)
+
+PGB_EXPORT int g5_get_number_of_pipelines(void) { return npipes(); }
+PGB_EXPORT int g5_get_jmemsize(void) { return jmemsize(); }
+
+PGB_EXPORT void g5_open(void) { ensure_device(); }
+
+PGB_EXPORT void g5_close(void) {
+    if (g_device < 0) return;
+    cudaSetDevice(g_device);
+    for (auto& d : g_devs) {
+        std::lock_guard<std::mutex> g(d.mu);
+        if (d.ready) {
+            cudaStreamSynchronize(d.stream);
+            d.jd.release();
+            d.jed.release();
+            d.cd.release();
+            d.cqd.release();
+            d.outd.release();
+            d.L.release();
+            d.jdirty_lo = 0;
+            d.jdirty_hi = d.jcap;
+            d.cdirty_lo = 0;
+            d.cdirty_hi = d.ccap;
+            d.pending = 0;
+        }
+    }
+}
+
+PGB_EXPORT void g5_set_eps_to_all(double eps) { g_eps = eps; }
+
+PGB_EXPORT void g5_set_epsMC(int devid, int ni, double* eps) {
+    if (!check_ni(ni)) return;
+    Dev* d = get_dev(devid);
+    if (!d) return;
+    std::lock_guard<std::mutex> g(d->mu);
+    for (int i = 0; i < ni; i++) d->ip[i].w = (float)(eps[i] * eps[i]);  // phantom_g5.c:72-82
+}
+PGB_EXPORT void g5_set_eps(int ni, double* eps) { g5_set_epsMC(0, ni, eps); }
+
+PGB_EXPORT void g5_set_nMC(int devid, int n) {
+    Dev* d = get_dev(devid);
+    if (!d) return;
+    if (n < 0 || n > jmemsize()) {
+        raise(g_err, LIB, PGB_ERR_CAPACITY, "g5_set_n(%d) outside [0, %d]", n, jmemsize());
+        return;
+    }
+    std::lock_guard<std::mutex> g(d->mu);
+    d->nbody = n;
+}
+PGB_EXPORT void g5_set_n(int n) { g5_set_nMC(0, n); }
+
+PGB_EXPORT void g5_set_xiMC(int devid, int ni, double (*xi)[3]) { set_xi_impl(devid, ni, xi, nullptr, false); }
+PGB_EXPORT void g5_set_xeiMC(int devid, int ni, double (*xi)[3], double* eps2) {
+    set_xi_impl(devid, ni, xi, eps2, true);
+}
+PGB_EXPORT void g5_set_xi(int ni, double (*xi)[3]) { g5_set_xiMC(0, ni, xi); }
+PGB_EXPORT void g5_set_xei(int ni, double (*xi)[3], double* eps2) { g5_set_xeiMC(0, ni, xi, eps2); }
+
+#ifdef PGB_SYMMETRIC
+PGB_EXPORT void g5_set_xmjMC(int devid, int adr, int nj, double (*xj)[3], double* mj, double* epsj2) {
+#else
+PGB_EXPORT void g5_set_xmjMC(int devid, int adr, int nj, double (*xj)[3], double* mj) {
+#endif
+    if (adr < 0 || nj < 0) {
+        raise(g_err, LIB, PGB_ERR_ARG, "g5_set_xmj: adr %d nj %d", adr, nj);
+        return;
+    }
+    Dev* d = get_dev(devid);
+    if (!d) return;
+    std::lock_guard<std::mutex> g(d->mu);
+    if (!quiesce(*d) || !grow_j(*d, adr + nj)) return;
+    for (int j = adr; j < adr + nj; j++) {
+        d->jh.p[j] = make_float4((float)xj[j][0], (float)xj[j][1], (float)xj[j][2], (float)mj[j]);
+#ifdef PGB_SYMMETRIC
+        d->jeh.p[j] = make_float4((float)epsj2[j], 0, 0, 0);
+#endif
+    }
+    if (nj > 0) {
+        if (adr < d->jdirty_lo) d->jdirty_lo = adr;
+        if (adr + nj > d->jdirty_hi) d->jdirty_hi = adr + nj;
+    }
+}
+
+#ifdef PGB_SYMMETRIC
+PGB_EXPORT void g5_set_xmj(int adr, int nj, double (*xj)[3], double* mj, double* epsj2) {
+    g5_set_xmjMC(0, adr, nj, xj, mj, epsj2);
+}
+#else
+PGB_EXPORT void g5_set_xmj(int adr, int nj, double (*xj)[3], double* mj) { g5_set_xmjMC(0, adr, nj, xj, mj); }
+#endif
+
+PGB_EXPORT void g5_runMC(int devid) { run_impl(devid, PARTICLE_KIND); }
+PGB_EXPORT void g5_run(void) { g5_runMC(0); }
+
+PGB_EXPORT void g5_get_forceMC(int devid, int ni, double (*a)[3], double* p) { get_force_impl(devid, ni, a, p); }
+PGB_EXPORT void g5_get_force(int ni, double (*a)[3], double* p) { g5_get_forceMC(0, ni, a, p); }
+
+PGB_EXPORT void g5_calculate_force_on_xMC(int devid, double (*x)[3], double (*a)[3], double* p, int ni) {
+    calc_impl(devid, PARTICLE_KIND, x, nullptr, a, p, ni);
+}
+PGB_EXPORT void g5_calculate_force_on_xeMC(int devid, double (*x)[3], double* eps2, double (*a)[3], double* p,
+                                           int ni) {
+    calc_impl(devid, PARTICLE_KIND, x, eps2, a, p, ni);
+}
+PGB_EXPORT void g5_calculate_force_on_x(double (*x)[3], double (*a)[3], double* p, int ni) {
+    g5_calculate_force_on_xMC(0, x, a, p, ni);
+}
+PGB_EXPORT void g5_calculate_force_on_xe(double (*x)[3], double* eps2, double (*a)[3], double* p, int ni) {
+    g5_calculate_force_on_xeMC(0, x, eps2, a, p, ni);
+}
+
+// ============================================================================================
+// Quadrupole j-cells (PG5/newton_quad/quad/quad_util.h:8-15)
+
+PGB_EXPORT void g5c_set_nMC(int devid, int n) {
+    Dev* d = get_dev(devid);
+    if (!d) return;
+    if (n < 0 || n > jmemsize() / 2) {
+        raise(g_err, LIB, PGB_ERR_CAPACITY, "g5c_set_n(%d) outside [0, %d]", n, jmemsize() / 2);
+        return;
+    }
+    std::lock_guard<std::mutex> g(d->mu);
+    d->ncell = n;
+}
+
+// qj = (xx, xy, xz, yy, yz, zz) of the traceless moment sum m (3 d d - d^2 I) (source.cpp:215-248)
+PGB_EXPORT void g5c_set_xmjMC(int devid, int adr, int nj, double (*xj)[3], double* mj, double (*qj)[6]) {
+    if (adr < 0 || nj < 0) {
+        raise(g_err, LIB, PGB_ERR_ARG, "g5c_set_xmj: adr %d nj %d", adr, nj);
+        return;
+    }
+    Dev* d = get_dev(devid);
+    if (!d) return;
+    std::lock_guard<std::mutex> g(d->mu);
+    if (!quiesce(*d) || !grow_c(*d, adr + nj)) return;
+    for (int j = adr; j < adr + nj; j++) {
+        d->ch.p[j] = make_float4((float)xj[j][0], (float)xj[j][1], (float)xj[j][2], (float)mj[j]);
+        d->cqh.p[2 * j] = make_float4((float)qj[j][0], (float)qj[j][1], (float)qj[j][2], (float)qj[j][3]);
+        d->cqh.p[2 * j + 1] = make_float4((float)qj[j][4], (float)qj[j][5], 0.f, 0.f);
+    }
+    if (nj > 0) {
+        if (adr < d->cdirty_lo) d->cdirty_lo = adr;
+        if (adr + nj > d->cdirty_hi) d->cdirty_hi = adr + nj;
+    }
+}
+// The reference's structure-of-arrays variant (quad_g5c.c:19-196) computes the same sums.
+PGB_EXPORT void g5c_set_xmjMC0(int devid, int adr, int nj, double (*xj)[3], double* mj, double (*qj)[6]) {
+    g5c_set_xmjMC(devid, adr, nj, xj, mj, qj);
+}
+
+PGB_EXPORT void g5c_runMC(int devid) { run_impl(devid, G5_QUAD); }
+PGB_EXPORT void g5c_runMC0(int devid) { g5c_runMC(devid); }
+
+PGB_EXPORT void g5c_calculate_force_on_xMC(int devid, double (*x)[3], double (*a)[3], double* p, int ni) {
+    calc_impl(devid, G5_QUAD, x, nullptr, a, p, ni);
+}
+PGB_EXPORT void g5c_calculate_force_on_xMC0(int devid, double (*x)[3], double (*a)[3], double* p, int ni) {
+    g5c_calculate_force_on_xMC(devid, x, a, p, ni);
+}
+
+// ============================================================================================
+// Fortran bindings (PG5/newton/libpg5/pg5_fortran.c:1-119)
+
+PGB_EXPORT int g5_get_number_of_pipelines_(void) { return g5_get_number_of_pipelines(); }
+PGB_EXPORT int g5_get_jmemsize_(void) { return g5_get_jmemsize(); }
+PGB_EXPORT void g5_open_(void) { g5_open(); }
+PGB_EXPORT void g5_close_(void) { g5_close(); }
+PGB_EXPORT void g5_set_eps_to_all_(double* eps) { g5_set_eps_to_all(*eps); }
+PGB_EXPORT void g5_set_n_(int* n) { g5_set_n(*n); }
+PGB_EXPORT void g5_set_nMC_(int* devid, int* n) { g5_set_nMC(*devid, *n); }
+PGB_EXPORT void g5_set_xi_(int* ni, double (*xi)[3]) { g5_set_xi(*ni, xi); }
+PGB_EXPORT void g5_set_xei_(int* ni, double (*xi)[3], double* eps2) { g5_set_xei(*ni, xi, eps2); }
+PGB_EXPORT void g5_set_xiMC_(int* devid, int* ni, double (*xi)[3]) { g5_set_xiMC(*devid, *ni, xi); }
+PGB_EXPORT void g5_set_xeiMC_(int* devid, int* ni, double (*xi)[3], double* eps2) {
+    g5_set_xeiMC(*devid, *ni, xi, eps2);
+}
+#ifdef PGB_SYMMETRIC
+PGB_EXPORT void g5_set_xmj_(int* adr, int* nj, double (*xj)[3], double* mj, double* eps2) {
+    g5_set_xmj(*adr, *nj, xj, mj, eps2);
+}
+PGB_EXPORT void g5_set_xmjMC_(int* devid, int* adr, int* nj, double (*xj)[3], double* mj, double* eps2) {
+    g5_set_xmjMC(*devid, *adr, *nj, xj, mj, eps2);
+}
+#else
+PGB_EXPORT void g5_set_xmj_(int* adr, int* nj, double (*xj)[3], double* mj) { g5_set_xmj(*adr, *nj, xj, mj); }
+PGB_EXPORT void g5_set_xmjMC_(int* devid, int* adr, int* nj, double (*xj)[3], double* mj) {
+    g5_set_xmjMC(*devid, *adr, *nj, xj, mj);
+}
+#endif
+PGB_EXPORT void g5_run_(void) { g5_run(); }
+PGB_EXPORT void g5_runMC_(int* devid) { g5_runMC(*devid); }
+PGB_EXPORT void g5_get_force_(int* ni, double (*a)[3], double* p) { g5_get_force(*ni, a, p); }
+PGB_EXPORT void g5_get_forceMC_(int* devid, int* ni, double (*a)[3], double* p) { g5_get_forceMC(*devid, *ni, a, p); }
+PGB_EXPORT void g5_calculate_force_on_x_(double (*x)[3], double (*a)[3], double* p, int* ni) {
+    g5_calculate_force_on_x(x, a, p, *ni);
+}
+PGB_EXPORT void g5_calculate_force_on_xe_(double (*x)[3], double* eps2, double (*a)[3], double* p, int* ni) {
+    g5_calculate_force_on_xe(x, eps2, a, p, *ni);
+}
+PGB_EXPORT void g5_calculate_force_on_xMC_(int* devid, double (*x)[3], double (*a)[3], double* p, int* ni) {
+    g5_calculate_force_on_xMC(*devid, x, a, p, *ni);
+}
+PGB_EXPORT void g5_calculate_force_on_xeMC_(int* devid, double (*x)[3], double* eps2, double (*a)[3], double* p,
+                                            int* ni) {
+    g5_calculate_force_on_xeMC(*devid, x, eps2, a, p, *ni);
+}
+
+// ============================================================================================
+// Library status and the batched path (no reference counterpart; see include/pgb_g5.h)
+
+PGB_EXPORT int pgb5_last_error(char* buf, int len) {
+    std::lock_guard<std::mutex> g(g_err.mu);
+    if (buf && len > 0) {
+        std::strncpy(buf, g_err.msg.c_str(), (size_t)len - 1);
+        buf[len - 1] = 0;
+    }
+    return g_err.code;
+}
+PGB_EXPORT void pgb5_clear_error(void) {
+    std::lock_guard<std::mutex> g(g_err.mu);
+    g_err.code = 0;
+    g_err.msg.clear();
+}
+PGB_EXPORT void pgb5_set_abort(int on) {
+    std::lock_guard<std::mutex> g(g_err.mu);
+    g_err.abort_on_error = on ? 1 : 0;
+}
+
+struct pgb5_plan {
+    int kind;
+    std::vector<Task> tasks;
+    std::vector<Group> groups;
+    int rows;
+    long long interactions;
+    Launcher L;
+};
+
+namespace {
+bool check_kind(int kind) {
+    if (kind != G5_NEWTON && kind != G5_SYMMETRIC && kind != G5_QUAD) {
+        raise(g_err, LIB, PGB_ERR_ARG, "unknown kind %d", kind);
+        return false;
+    }
+    return true;
+}
+}  // namespace
+
+// items: [nitem][4] = (i_offset, i_count, j_offset, j_count) into the i- and j-arrays.
+PGB_EXPORT int pgb5_plan_create(pgb5_plan** out, int kind, int nitem, const int* items) {
+    if (!out || nitem < 0 || (nitem && !items) || !check_kind(kind)) return PGB_ERR_ARG;
+    if (!ensure_device()) return PGB_ERR_NOGPU;
+    auto* P = new pgb5_plan();
+    P->kind = kind;
+    P->interactions = 0;
+    int slots = sm_count(g_device) * occupancy_of(kind);
+    long long itiles = 0;
+    for (int k = 0; k < nitem; k++) itiles += (items[4 * k + 1] + ITILE - 1) / ITILE;
+    // One chunk length for the whole batch: about 4 tasks per resident CTA in total.
+    long long work = 0;
+    for (int k = 0; k < nitem; k++) work += (long long)items[4 * k + 1] * items[4 * k + 3];
+    P->rows = 0;
+    long long per_task = work / (4LL * slots) + 1;
+    for (int k = 0; k < nitem; k++) {
+        int ni = items[4 * k + 1], nj = items[4 * k + 3];
+        if (ni < 0 || nj < 0 || items[4 * k] < 0 || items[4 * k + 2] < 0) {
+            delete P;
+            raise(g_err, LIB, PGB_ERR_ARG, "item %d has a negative offset or count", k);
+            return PGB_ERR_ARG;
+        }
+        long long tile_i = ni < ITILE ? ni : ITILE;
+        long long jc = tile_i > 0 ? per_task / tile_i : nj;
+        if (jc < 256) jc = 256;
+        if (jc > nj) jc = nj > 0 ? nj : 1;
+        P->rows += plan_item(P->tasks, P->groups, items[4 * k], ni, items[4 * k + 2], nj, ITILE, (int)jc, P->rows);
+        P->interactions += (long long)ni * nj;
+    }
+    // longest tasks first (persistent CTAs then finish together)
+    std::stable_sort(P->tasks.begin(), P->tasks.end(), [](const Task& a, const Task& b) {
+        return (long long)a.ni * a.nj > (long long)b.ni * b.nj;
+    });
+    cudaStream_t s = nullptr;
+    bool ok = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess;
+    ok = ok && P->L.stage(s, P->tasks, P->groups, P->rows, nullptr, 0);
+    ok = ok && cudaStreamSynchronize(s) == cudaSuccess;
+    if (s) cudaStreamDestroy(s);
+    if (!ok) {
+        P->L.release();
+        delete P;
+        raise(g_err, LIB, PGB_ERR_CUDA, "plan staging failed");
+        return PGB_ERR_CUDA;
+    }
+    *out = P;
+    return PGB_OK;
+}
+
+PGB_EXPORT long long pgb5_plan_interactions(const pgb5_plan* P) { return P ? P->interactions : 0; }
+PGB_EXPORT int pgb5_plan_tasks(const pgb5_plan* P) { return P ? (int)P->tasks.size() : 0; }
+
+// Device-resident launch: ipos float4 (x,y,z,eps2), jpos float4 (x,y,z,m), jaux (symmetric:
+// float4 eps2_j in .x; quad: two float4 of Q per cell), out double4 (ax,ay,az,pot_raw) where
+// pot_raw = -sum m/r (newton/symmetric) or +sum(phi_p+phi_q) (quad).  stream: cudaStream_t.
+PGB_EXPORT int pgb5_plan_launch(pgb5_plan* P, const void* ipos, const void* jpos, const void* jaux, void* out,
+                                void* stream) {
+    if (!P) return PGB_ERR_ARG;
+    if (!ensure_device()) return PGB_ERR_NOGPU;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!ipos || !jpos || !out || (P->kind != G5_NEWTON && !jaux)) {
+        raise(g_err, LIB, PGB_ERR_ARG, "pgb5_plan_launch: null device pointer");
+        return PGB_ERR_ARG;
+    }
+    if (!P->L.launch(P->kind, s, (const float4*)ipos, (const float4*)jpos, (const float4*)jaux, (double4*)out, true))
+        return g_err.code ? g_err.code : PGB_ERR_CUDA;
+    return PGB_OK;
+}
+
+PGB_EXPORT void pgb5_plan_destroy(pgb5_plan* P) {
+    if (!P) return;
+    if (g_device >= 0) {
+        cudaSetDevice(g_device);
+        cudaDeviceSynchronize();
+    }
+    P->L.release();
+    delete P;
+}

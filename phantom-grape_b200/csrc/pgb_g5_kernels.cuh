@@ -1,0 +1,180 @@
+// pgb_g5_kernels.cuh -- PG5 Newtonian (plain and symmetric softening) and quadrupole-cell
+// interaction kernels for sm_100a.
+//
+// Work decomposition (all kernels): a persistent grid of CTAs pulls Tasks (i-tile x j-chunk)
+// from a global counter.  A CTA of NT threads owns NT*IPT i-particles (IPT per thread, kept
+// in registers), streams its j-chunk through shared memory in tiles of NT records (one
+// coalesced 16-byte load per thread per record word), and every thread reads each j record
+// with a broadcast LDS.128.  Sums are accumulated in FP32 within a j tile and folded into FP64
+// accumulators after every tile (the cross-tile reduction runs in FP64).  Split j-ranges
+// write FP64 partial rows; the last CTA of a group reduces them in chunk order.
+//
+// Formulae (scaled so that the Newton-refined rsqrt needs no extra multiply):
+//   q = -2/r (pgb::minus2_over_r),  pot_sum += m q,  acc_sum += (m q^3) dx   (m q^3 = -8 m/r^3)
+//   acc = acc_sum * (-1/8),  pot_raw = pot_sum * (1/2) = -sum m/r
+// i.e. the reference's GravityKernel accumulators (PG5/newton/libpg5/gravity_avx2.c:95-153:
+// phi -= m/r, acc += m dx / r^3) without its 12-bit rsqrt.
+#pragma once
+
+#include "pgb_common.cuh"
+
+namespace pgb {
+
+struct G5Args {
+    const float4* ipos;     // [.] x, y, z, eps2 of each i-particle
+    const float4* jpos;     // [.] x, y, z, m of each j-particle (or cell word 0)
+    const float4* jaux;     // symmetric: [.] eps2_j in .x; quad: [2*nc] (q0 q1 q2 q3)(q4 q5 - -)
+    const Task* tasks;
+    int ntasks;
+    int* task_counter;      // zero before launch
+    const Group* groups;
+    int* group_counters;    // zero at allocation, self-cleaning
+    double4* partial;       // [rows][itile]
+    double4* out;           // [.] (ax, ay, az, pot_raw) per i, indexed by absolute i
+    int itile;              // NT*IPT
+};
+
+// kinds
+enum { G5_NEWTON = 0, G5_SYMMETRIC = 1, G5_QUAD = 2 };
+
+template <int KIND>
+struct JWords { static constexpr int n = (KIND == G5_NEWTON) ? 1 : (KIND == G5_SYMMETRIC ? 2 : 3); };
+
+template <int KIND, int NT>
+__device__ __forceinline__ void g5_interact(const float4* sj, int j, float xi, float yi, float zi,
+                                            float ei, float (&a)[4]) {
+    float4 J = sj[j];
+    float dx = J.x - xi, dy = J.y - yi, dz = J.z - zi;
+    if constexpr (KIND == G5_QUAD) {
+        // c_GravityKernel, PG5/newton_quad/quad/quad_avx2.c:35-149 (FP64 form source.cpp:1160-1184)
+        float4 Q0 = sj[NT + 2 * j];      // q00 q01 q02 q11
+        float4 Q1 = sj[NT + 2 * j + 1];  // q12 q22  -   -
+        float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmaf_rn(dx, dx, ei)));
+        float q = minus2_over_r(r2);
+        float ri = -0.5f * q;
+        float ri2 = ri * ri;
+        float phi_p = J.w * ri;
+        float qx = __fmaf_rn(Q0.z, dz, __fmaf_rn(Q0.y, dy, Q0.x * dx));
+        float qy = __fmaf_rn(Q1.x, dz, __fmaf_rn(Q0.w, dy, Q0.y * dx));
+        float qz = __fmaf_rn(Q1.y, dz, __fmaf_rn(Q1.x, dy, Q0.z * dx));
+        float drqdr = __fmaf_rn(dz, qz, __fmaf_rn(dy, qy, dx * qx));
+        float dr5i = ri2 * ri2 * ri;
+        float phi_q = 0.5f * dr5i * drqdr;
+        a[3] += phi_p + phi_q;
+        float mr3i = __fmaf_rn(5.0f, phi_q, phi_p) * ri2;
+        a[0] = __fmaf_rn(dx, mr3i, __fmaf_rn(-qx, dr5i, a[0]));
+        a[1] = __fmaf_rn(dy, mr3i, __fmaf_rn(-qy, dr5i, a[1]));
+        a[2] = __fmaf_rn(dz, mr3i, __fmaf_rn(-qz, dr5i, a[2]));
+    } else {
+        float e = ei;
+        if constexpr (KIND == G5_SYMMETRIC) e += sj[NT + j].x;  // GravityKernel0
+        float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmaf_rn(dx, dx, e)));
+        float q = minus2_over_r(r2);
+        float mq = J.w * q;
+        float q2 = q * q;
+        float mq3 = mq * q2;
+        a[3] += mq;
+        a[0] = __fmaf_rn(mq3, dx, a[0]);
+        a[1] = __fmaf_rn(mq3, dy, a[1]);
+        a[2] = __fmaf_rn(mq3, dz, a[2]);
+    }
+}
+
+// Final scaling of the FP64 sums into (acc, pot_raw).
+template <int KIND>
+__device__ __forceinline__ double4 g5_finish(double4 s) {
+    if constexpr (KIND == G5_QUAD) return s;  // quad sums are already (acc, +sum(phi_p+phi_q))
+    return make_double4(-0.125 * s.x, -0.125 * s.y, -0.125 * s.z, 0.5 * s.w);
+}
+
+__device__ __forceinline__ double4 add4(double4 a, double4 b) {
+    return make_double4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
+}
+
+template <int KIND, int NT, int IPT>
+__global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
+    constexpr int W = JWords<KIND>::n;   // 16-byte words per j record
+    __shared__ float4 sj[NT * W];
+    __shared__ int s_task, s_flag;
+
+    for (;;) {
+        int t = next_task(A.task_counter, &s_task);
+        if (t >= A.ntasks) break;
+        const Task T = A.tasks[t];
+
+        float xi[IPT], yi[IPT], zi[IPT], ei[IPT];
+        double S[IPT][4];
+#pragma unroll
+        for (int k = 0; k < IPT; k++) {
+            int li = threadIdx.x + k * NT;
+            int ii = T.i0 + (li < T.ni ? li : 0);
+            float4 p = A.ipos[ii];
+            xi[k] = p.x; yi[k] = p.y; zi[k] = p.z; ei[k] = p.w;
+            S[k][0] = S[k][1] = S[k][2] = S[k][3] = 0.0;
+        }
+
+        for (int jt = 0; jt < T.nj; jt += NT) {
+            const int nt = min(NT, T.nj - jt);
+            __syncthreads();
+            if (threadIdx.x < nt) {
+                const int jj = T.j0 + jt + threadIdx.x;
+                sj[threadIdx.x] = A.jpos[jj];
+                if constexpr (W == 2) sj[NT + threadIdx.x] = A.jaux[jj];
+                if constexpr (W == 3) {
+                    sj[NT + 2 * threadIdx.x] = A.jaux[2 * jj];
+                    sj[NT + 2 * threadIdx.x + 1] = A.jaux[2 * jj + 1];
+                }
+            }
+            __syncthreads();
+            float a[IPT][4];
+#pragma unroll
+            for (int k = 0; k < IPT; k++) a[k][0] = a[k][1] = a[k][2] = a[k][3] = 0.f;
+#pragma unroll 4
+            for (int j = 0; j < nt; j++) {
+#pragma unroll
+                for (int k = 0; k < IPT; k++) g5_interact<KIND, NT>(sj, j, xi[k], yi[k], zi[k], ei[k], a[k]);
+            }
+#pragma unroll
+            for (int k = 0; k < IPT; k++) {
+                S[k][0] += (double)a[k][0];
+                S[k][1] += (double)a[k][1];
+                S[k][2] += (double)a[k][2];
+                S[k][3] += (double)a[k][3];
+            }
+        }
+
+        if (T.group < 0) {
+#pragma unroll
+            for (int k = 0; k < IPT; k++) {
+                int li = threadIdx.x + k * NT;
+                if (li < T.ni)
+                    A.out[T.i0 + li] = g5_finish<KIND>(make_double4(S[k][0], S[k][1], S[k][2], S[k][3]));
+            }
+            continue;
+        }
+        double4* row = A.partial + (size_t)T.slot * A.itile;
+#pragma unroll
+        for (int k = 0; k < IPT; k++) {
+            int li = threadIdx.x + k * NT;
+            if (li < T.ni) row[li] = make_double4(S[k][0], S[k][1], S[k][2], S[k][3]);
+        }
+        const Group G = A.groups[T.group];
+        if (group_arrive(A.group_counters, T.group, G.nchunk, &s_flag)) {
+#pragma unroll
+            for (int k = 0; k < IPT; k++) {
+                int li = threadIdx.x + k * NT;
+                if (li >= G.ni) continue;
+                double4 s = make_double4(0, 0, 0, 0);
+                for (int c = 0; c < G.nchunk; c++) {
+                    const double4* r = A.partial + (size_t)(G.slot0 + c) * A.itile + li;
+                    double4 v;
+                    v.x = __ldcg(&r->x); v.y = __ldcg(&r->y); v.z = __ldcg(&r->z); v.w = __ldcg(&r->w);
+                    s = add4(s, v);
+                }
+                A.out[G.i0 + li] = g5_finish<KIND>(s);
+            }
+        }
+    }
+}
+
+}  // namespace pgb

@@ -1,0 +1,551 @@
+// pgb_g6.cu -- GRAPE-6 API of libpg6 on the B200 engine, plus the batched pgb6_* path.
+//
+// Drop-in for PG6/libpg6 (gp6util.h:1-101, phantom_g6.c, gravity.c).  Semantics kept:
+//  * g6_set_j_particle stores (pos, vel, acc/2, jerk/6, mass, t, id) at address padr
+//    (phantom_g6.c:118-125, gravity.c:95-115); the caller supplies acc/2 and jerk/6
+//    (banana01.c:206-212).
+//  * g6_set_ti sets the prediction time and a flag; the first g6calc_firsthalf after it
+//    predicts all nj j-particles to t_i in FP64 (phantom_g6.c:138-164, gravity.c:149-193).
+//  * g6calc_lasthalf* evaluate ni <= g6_npipes() i-particles against the nj predicted
+//    j-particles, excluding the pair whose id equals the i id, and return
+//    acc = sum m dx/r^3, jerk = sum m (dv/r^3 - 3 (dx.dv) dx/r^5), pot = -sum m/r
+//    (the reference's -1/8 and 1/2 rescaling, phantom_g6.c:13-14, 200-208), nnb = id of the
+//    nearest neighbour, rnnb = its softened distance (-2/key, gravity.c:651-657).
+//  * lasthalfn / 2n / 2np also build neighbour lists (softened r <= h_i, gravity.c:788-793),
+//    read back with g6_read_neighbour_list / g6_get_neighbour_list (phantom_g6.c:482-504),
+//    lists in j-address order as the reference produces them.
+//  * g6_set_tunit/xunit/reset/reset_fofpga/setup_njdata are no-ops, as in the reference.
+// Deliberate differences:
+//  * the self pair is excluded by an exact int id compare (the reference compares ids
+//    converted to float, gravity.c:347-351: identical below 2^24 ids);
+//  * pot is returned with FP64 precision (the reference stores it as float, avx_type.h:19);
+//  * nearest-neighbour ties go to the smallest j address (the reference: lane j%4 first);
+//  * a neighbour list longer than the capacity (1024, PGB_G6_NBMAX) is counted, flagged by
+//    g6_read_neighbour_list and refused by g6_get_neighbour_list, never written out of bounds
+//    (gravity.c:896-906 writes before it checks).
+#include "pgb_g6_kernels.cuh"
+
+using namespace pgb;
+
+namespace {
+
+const char* LIB = "libpg6";
+ErrorSlot g_err;
+
+int env_int(const char* name, int dflt, int lo, int hi) {
+    const char* s = std::getenv(name);
+    if (!s || !*s) return dflt;
+    int v = std::atoi(s);
+    return v < lo ? lo : (v > hi ? hi : v);
+}
+
+int npipes() {
+    static int v = env_int("PGB_G6_NPIPES", 48, 1, 1 << 20);
+    return v;
+}
+int jmemsize() {
+    static int v = env_int("PGB_G6_JMEMSIZE", 1 << 22, 1024, 1 << 26);
+    return v;
+}
+int nbmax() {
+    static int v = env_int("PGB_G6_NBMAX", 1024, 1, 1 << 16);
+    return v;
+}
+
+std::mutex g_init_mu;
+int g_device = -1;
+
+bool ensure_device() {
+    if (g_device >= 0) {
+        PGB_CUDA_OR(g_err, LIB, cudaSetDevice(g_device), return false);
+        return true;
+    }
+    std::lock_guard<std::mutex> g(g_init_mu);
+    if (g_device < 0) {
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) {
+            raise(g_err, LIB, PGB_ERR_NOGPU, "no CUDA device available");
+            return false;
+        }
+        int d = env_int("PGB_DEVICE", 0, 0, n - 1);
+        PGB_CUDA_OR(g_err, LIB, cudaSetDevice(d), return false);
+        g_device = d;
+    }
+    PGB_CUDA_OR(g_err, LIB, cudaSetDevice(g_device), return false);
+    return true;
+}
+
+// ------------------------------------------------------------------------------------------
+// kernel configurations: (threads per CTA, i per thread)
+
+enum Cfg { CFG_64x1 = 0, CFG_128x1 = 1, CFG_128x2 = 2, NCFG = 3 };
+constexpr int CFG_NT[NCFG] = {64, 128, 128};
+constexpr int CFG_IPT[NCFG] = {1, 1, 2};
+inline int cfg_itile(int c) { return CFG_NT[c] * CFG_IPT[c]; }
+constexpr int ITILE_MAX = 256;
+
+template <int NT, int IPT, bool NN, bool NBL>
+void launch_one(int grid, const G6Args& a, cudaStream_t s) {
+    g6_kernel<NT, IPT, NN, NBL><<<grid, NT, 0, s>>>(a);
+}
+
+template <int NT, int IPT>
+int occ_of(bool nn, bool nbl) {
+    static int v[4] = {0, 0, 0, 0};
+    int k = (nn ? 1 : 0) + (nbl ? 2 : 0);
+    if (!v[k]) {
+        int b = 0;
+        if (k == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, false, false>, NT, 0);
+        if (k == 1) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, true, false>, NT, 0);
+        if (k == 2) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, false, true>, NT, 0);
+        if (k == 3) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, true, true>, NT, 0);
+        v[k] = b > 0 ? b : 1;
+    }
+    return v[k];
+}
+
+int occupancy(int cfg, bool nn, bool nbl) {
+    switch (cfg) {
+        case CFG_64x1: return occ_of<64, 1>(nn, nbl);
+        case CFG_128x1: return occ_of<128, 1>(nn, nbl);
+        default: return occ_of<128, 2>(nn, nbl);
+    }
+}
+
+template <int NT, int IPT>
+void launch_cfg(bool nn, bool nbl, int grid, const G6Args& a, cudaStream_t s) {
+    if (nn && nbl) launch_one<NT, IPT, true, true>(grid, a, s);
+    else if (nn) launch_one<NT, IPT, true, false>(grid, a, s);
+    else if (nbl) launch_one<NT, IPT, false, true>(grid, a, s);
+    else launch_one<NT, IPT, false, false>(grid, a, s);
+}
+
+cudaError_t launch_kernel(int cfg, bool nn, bool nbl, int grid, const G6Args& a, cudaStream_t s) {
+    switch (cfg) {
+        case CFG_64x1: launch_cfg<64, 1>(nn, nbl, grid, a, s); break;
+        case CFG_128x1: launch_cfg<128, 1>(nn, nbl, grid, a, s); break;
+        default: launch_cfg<128, 2>(nn, nbl, grid, a, s); break;
+    }
+    return cudaGetLastError();
+}
+
+// Forced configuration for tuning sweeps (PGB_G6_CFG = 0/1/2), else by i count.
+int pick_cfg(long long ni_max) {
+    static int forced = env_int("PGB_G6_CFG", -1, -1, NCFG - 1);
+    if (forced >= 0) return forced;
+    if (ni_max <= 64) return CFG_64x1;
+    if (ni_max <= 4096) return CFG_128x1;
+    return CFG_128x2;
+}
+
+// Plan one batch of items ([k][4] = i_off, i_cnt, j_off, j_cnt) for a configuration:
+// about 4 tasks per resident CTA, chunks of at least 128 j.
+long long plan_items(std::vector<Task>& tasks, std::vector<Group>& groups, int& rows, int nitem, const int* items,
+                     int cfg, bool nn, bool nbl) {
+    int slots = sm_count(g_device) * occupancy(cfg, nn, nbl);
+    int itile = cfg_itile(cfg);
+    long long work = 0;
+    for (int k = 0; k < nitem; k++) {
+        long long ni = items[4 * k + 1];
+        long long tiles = (ni + itile - 1) / itile;
+        work += tiles * itile * (long long)items[4 * k + 3];
+    }
+    long long per_task = work / (4LL * slots) + 1;
+    long long inter = 0;
+    rows = 0;
+    for (int k = 0; k < nitem; k++) {
+        int ni = items[4 * k + 1], nj = items[4 * k + 3];
+        long long jc = per_task / itile;
+        if (jc < 128) jc = 128;
+        if (jc > nj) jc = nj > 0 ? nj : 1;
+        rows += plan_item(tasks, groups, items[4 * k], ni, items[4 * k + 2], nj, itile, (int)jc, rows);
+        inter += (long long)ni * nj;
+    }
+    std::stable_sort(tasks.begin(), tasks.end(), [](const Task& a, const Task& b) {
+        return (long long)a.ni * a.nj > (long long)b.ni * b.nj;
+    });
+    return inter;
+}
+
+// ------------------------------------------------------------------------------------------
+// library state (the reference keeps one global j-memory, gravity.c:31-47)
+
+struct State {
+    std::mutex mu;
+    bool ready = false;
+    cudaStream_t stream = nullptr;
+    HostBuf<G6Ptcl> jh;
+    DevBuf<G6Ptcl> jd;
+    DevBuf<G6PredJ> pred;
+    int jcap = 0, jdirty_lo = 1 << 30, jdirty_hi = 0;
+    double ti = 0.0;
+    int predict_flag = 0;
+    HostBuf<G6I> ibuf;
+    DevBuf<G6Out> outd;
+    HostBuf<G6Out> outh;
+    Stager<G6I, G6Out> st;
+    // neighbour lists of the last lasthalf*n call
+    DevBuf<int> nbc_d, nbl_d;
+    HostBuf<int> nbc_h, nbl_h;
+    std::vector<std::vector<int>> nblists;
+    std::vector<int> nbcounts;
+    int nb_ni = 0, nb_error = 0;
+};
+State S;
+
+bool init_state() {
+    if (!ensure_device()) return false;
+    if (!S.ready) {
+        PGB_CUDA_OR(g_err, LIB, cudaStreamCreateWithFlags(&S.stream, cudaStreamNonBlocking), return false);
+        S.ready = true;
+    }
+    return true;
+}
+
+bool grow_j(int need) {
+    if (need > jmemsize()) {
+        raise(g_err, LIB, PGB_ERR_CAPACITY, "j-memory overflow: address %d >= jmemsize %d", need - 1, jmemsize());
+        return false;
+    }
+    if (need <= S.jcap) return true;
+    int cap = S.jcap ? S.jcap : 8192;
+    while (cap < need) cap *= 2;
+    if (cap > jmemsize()) cap = jmemsize();
+    PGB_CUDA_OR(g_err, LIB, S.jh.reserve(cap, true), return false);
+    std::memset((void*)(S.jh.p + S.jcap), 0, (size_t)(cap - S.jcap) * sizeof(G6Ptcl));
+    S.jdirty_lo = 0;
+    S.jdirty_hi = cap;
+    S.jcap = cap;
+    return true;
+}
+
+bool flush_and_predict(int nj) {
+    if (nj <= 0) return true;
+    if (!grow_j(nj)) return false;
+    if (S.jdirty_hi > S.jdirty_lo) {
+        PGB_CUDA_OR(g_err, LIB, S.jd.reserve(S.jcap), return false);
+        size_t lo = S.jdirty_lo, n = (size_t)(S.jdirty_hi - S.jdirty_lo);
+        PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(S.jd.p + lo, S.jh.p + lo, n * sizeof(G6Ptcl),
+                                                cudaMemcpyHostToDevice, S.stream), return false);
+        S.jdirty_lo = 1 << 30;
+        S.jdirty_hi = 0;
+    }
+    PGB_CUDA_OR(g_err, LIB, S.pred.reserve(S.jcap), return false);
+    g6_predict_kernel<<<(nj + 255) / 256, 256, 0, S.stream>>>(S.jd.p, nj, S.ti, S.pred.p);
+    PGB_CUDA_OR(g_err, LIB, cudaGetLastError(), return false);
+    // j-memory is read asynchronously from the pinned mirror: later set_j calls wait for it
+    PGB_CUDA_OR(g_err, LIB, cudaStreamSynchronize(S.stream), return false);
+    return true;
+}
+
+bool run_force(int nj, int ni, float eps2, bool nn, bool nbl) {
+    std::vector<Task> tasks;
+    std::vector<Group> groups;
+    int rows = 0;
+    int cfg = pick_cfg(ni);
+    int item[4] = {0, ni, 0, nj};
+    plan_items(tasks, groups, rows, 1, item, cfg, nn, nbl);
+    PGB_CUDA_OR(g_err, LIB, S.st.stage(S.stream, tasks, groups, rows, ITILE_MAX, S.ibuf.p, ni), return false);
+    PGB_CUDA_OR(g_err, LIB, S.outd.reserve(ni), return false);
+    PGB_CUDA_OR(g_err, LIB, S.outh.reserve(ni), return false);
+    G6Args a;
+    a.ipart = S.st.irecs();
+    a.jpred = S.pred.p;
+    a.eps2 = eps2;
+    a.tasks = S.st.tasks();
+    a.ntasks = S.st.ntasks;
+    a.task_counter = S.st.counter();
+    a.groups = S.st.groups();
+    a.group_counters = S.st.dgcnt.p;
+    a.partial = S.st.dpart.p;
+    a.out = S.outd.p;
+    a.itile = cfg_itile(cfg);
+    a.nb_count = nullptr;
+    a.nb_list = nullptr;
+    a.nb_maxlen = nbmax();
+    if (nbl) {
+        PGB_CUDA_OR(g_err, LIB, S.nbc_d.reserve(ni), return false);
+        PGB_CUDA_OR(g_err, LIB, S.nbl_d.reserve((size_t)ni * nbmax()), return false);
+        PGB_CUDA_OR(g_err, LIB, cudaMemsetAsync(S.nbc_d.p, 0, (size_t)ni * sizeof(int), S.stream), return false);
+        a.nb_count = S.nbc_d.p;
+        a.nb_list = S.nbl_d.p;
+    }
+    if (a.ntasks == 0) return true;
+    int slots = sm_count(g_device) * occupancy(cfg, nn, nbl);
+    int grid = a.ntasks < slots ? a.ntasks : slots;
+    PGB_CUDA_OR(g_err, LIB, launch_kernel(cfg, nn, nbl, grid, a, S.stream), return false);
+    return true;
+}
+
+// Counts + lists back to the host; each list is sorted by j address (the reference's order,
+// gravity.c:888-900) and mapped to particle ids.  Lists longer than the capacity keep only
+// their count and set the overflow flag.
+void nblist_collect(int ni) {
+    S.nb_ni = ni;
+    S.nb_error = 0;
+    S.nbcounts.assign(ni, 0);
+    S.nblists.assign(ni, {});
+    if (S.nbc_h.reserve(ni) != cudaSuccess || S.nbl_h.reserve((size_t)ni * nbmax()) != cudaSuccess) {
+        raise(g_err, LIB, PGB_ERR_CUDA, "pinned neighbour-list buffer allocation failed");
+        return;
+    }
+    PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(S.nbc_h.p, S.nbc_d.p, (size_t)ni * sizeof(int), cudaMemcpyDeviceToHost,
+                                            S.stream), return);
+    PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(S.nbl_h.p, S.nbl_d.p, (size_t)ni * nbmax() * sizeof(int),
+                                            cudaMemcpyDeviceToHost, S.stream), return);
+    PGB_CUDA_OR(g_err, LIB, cudaStreamSynchronize(S.stream), return);
+    for (int i = 0; i < ni; i++) {
+        int c = S.nbc_h.p[i];
+        S.nbcounts[i] = c;
+        if (c > nbmax()) {
+            S.nb_error = 1;
+            continue;
+        }
+        std::vector<int> v(S.nbl_h.p + (size_t)i * nbmax(), S.nbl_h.p + (size_t)i * nbmax() + c);
+        std::sort(v.begin(), v.end());
+        for (auto& x : v) x = S.jh.p[x].idx;
+        S.nblists[i] = std::move(v);
+    }
+}
+
+// The common body of every g6calc_lasthalf* variant.
+int lasthalf_impl(int nj, int ni, const int* pidx, const double (*pos)[3], const double (*vel)[3], double eps2,
+                  const double* h2, double (*acc)[3], double (*jrk)[3], double* pot, int* nnb, float* rnnb,
+                  bool nbl) {
+    if (ni < 0 || ni > npipes()) {
+        raise(g_err, LIB, PGB_ERR_ARG, "ni = %d outside [0, %d] pipes", ni, npipes());
+        return 0;
+    }
+    if (nj < 0 || nj > S.jcap) {
+        raise(g_err, LIB, PGB_ERR_ARG, "nj = %d but only %d j-particles were set", nj, S.jcap);
+        return 0;
+    }
+    if (ni == 0) return 0;
+    std::lock_guard<std::mutex> g(S.mu);
+    if (!init_state()) return 0;
+    if (S.ibuf.reserve(ni) != cudaSuccess) {
+        raise(g_err, LIB, PGB_ERR_CUDA, "pinned i-buffer allocation failed");
+        return 0;
+    }
+    for (int i = 0; i < ni; i++) {
+        G6I& r = S.ibuf.p[i];
+        r.x = pos[i][0];
+        r.y = pos[i][1];
+        r.z = pos[i][2];
+        r.vx = (float)vel[i][0];
+        r.vy = (float)vel[i][1];
+        r.vz = (float)vel[i][2];
+        r.id = pidx[i];
+        r.h2 = (nbl && h2) ? (float)h2[i] : 0.f;
+        r.pad = 0.f;
+    }
+    bool nn = (nnb != nullptr);
+    // eps2 is a per-call scalar, used as float (phantom_g6.c:191)
+    if (!run_force(nj, ni, (float)eps2, nn, nbl)) return 0;
+    PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(S.outh.p, S.outd.p, (size_t)ni * sizeof(G6Out),
+                                            cudaMemcpyDeviceToHost, S.stream), return 0);
+    PGB_CUDA_OR(g_err, LIB, cudaStreamSynchronize(S.stream), return 0);
+    for (int i = 0; i < ni; i++) {
+        const G6Out& o = S.outh.p[i];
+        acc[i][0] = o.ax;
+        acc[i][1] = o.ay;
+        acc[i][2] = o.az;
+        jrk[i][0] = o.jx;
+        jrk[i][1] = o.jy;
+        jrk[i][2] = o.jz;
+        pot[i] = o.pot;
+        if (nnb) nnb[i] = (o.jadr >= 0 && o.jadr < S.jcap) ? S.jh.p[o.jadr].idx : -1;
+        if (rnnb) rnnb[i] = -2.0f / o.key;
+    }
+    if (nbl) nblist_collect(ni);
+    return 0;
+}
+
+}  // namespace
+
+// ============================================================================================
+// GRAPE-6 API (PG6/libpg6/gp6util.h:1-101)
+
+PGB_EXPORT void g6_open(int gpid) {
+    (void)gpid;
+    std::lock_guard<std::mutex> g(S.mu);
+    init_state();
+}
+PGB_EXPORT void g6_close(int gpid) {
+    (void)gpid;
+    std::lock_guard<std::mutex> g(S.mu);
+    if (!S.ready) return;
+    cudaSetDevice(g_device);
+    cudaStreamSynchronize(S.stream);
+    S.jd.release();
+    S.pred.release();
+    S.outd.release();
+    S.st.release();
+    S.nbc_d.release();
+    S.nbl_d.release();
+    S.jdirty_lo = 0;
+    S.jdirty_hi = S.jcap;
+}
+PGB_EXPORT void g6_set_tunit(int) {}
+PGB_EXPORT void g6_set_xunit(int) {}
+PGB_EXPORT void g6_reset(int) {}
+PGB_EXPORT void g6_reset_fofpga(int) {}
+PGB_EXPORT int g6_npipes(void) { return npipes(); }
+PGB_EXPORT void g6_setup_njdata(int, int) {}
+
+PGB_EXPORT void g6_set_j_particle(int gpid, int padr, int pidx, double t, double dt, double mss, double* snp,
+                                  double* jrk, double* acc, double* vel, double* pos) {
+    (void)gpid;
+    (void)dt;
+    (void)snp;
+    if (padr < 0) {
+        raise(g_err, LIB, PGB_ERR_ARG, "g6_set_j_particle: negative address %d", padr);
+        return;
+    }
+    std::lock_guard<std::mutex> g(S.mu);
+    if (!grow_j(padr + 1)) return;
+    G6Ptcl& p = S.jh.p[padr];
+    for (int d = 0; d < 3; d++) {
+        p.pos[d] = pos[d];
+        p.vel[d] = vel[d];
+        p.acc2[d] = acc[d];
+        p.jrk6[d] = jrk[d];
+    }
+    p.mass = mss;
+    p.tim = t;
+    p.idx = pidx;
+    if (padr < S.jdirty_lo) S.jdirty_lo = padr;
+    if (padr + 1 > S.jdirty_hi) S.jdirty_hi = padr + 1;
+}
+
+PGB_EXPORT void g6_set_ti(int gpid, double time) {
+    (void)gpid;
+    std::lock_guard<std::mutex> g(S.mu);
+    S.ti = time;
+    S.predict_flag = 1;
+}
+
+PGB_EXPORT void g6calc_firsthalf(int gpid, int nj, int ni, int* pidx, double (*pos)[3], double (*vel)[3],
+                                 double (*acc)[3], double (*jrk)[3], double* pot, double eps2, double* h2) {
+    (void)gpid; (void)ni; (void)pidx; (void)pos; (void)vel; (void)acc; (void)jrk; (void)pot; (void)eps2; (void)h2;
+    std::lock_guard<std::mutex> g(S.mu);
+    if (!init_state()) return;
+    if (S.predict_flag == 1) {
+        if (!flush_and_predict(nj)) return;
+        S.predict_flag = 0;
+    }
+    S.nb_error = 0;  // avx_initialize_neighbourlist (gravity.c:123-128)
+}
+
+#define LASTHALF_ARGS int gpid, int nj, int ni, int *pidx, double(*pos)[3], double(*vel)[3], double eps2, double *h2, \
+                      double(*acc)[3], double(*jrk)[3], double *pot
+
+PGB_EXPORT int g6calc_lasthalf(LASTHALF_ARGS) {
+    (void)gpid;
+    return lasthalf_impl(nj, ni, pidx, pos, vel, eps2, h2, acc, jrk, pot, nullptr, nullptr, false);
+}
+PGB_EXPORT int g6calc_lasthalf2(LASTHALF_ARGS, int* nnb) {
+    (void)gpid;
+    return lasthalf_impl(nj, ni, pidx, pos, vel, eps2, h2, acc, jrk, pot, nnb, nullptr, false);
+}
+PGB_EXPORT int g6calc_lasthalf2p(LASTHALF_ARGS, int* nnb, float* rnnb) {
+    (void)gpid;
+    return lasthalf_impl(nj, ni, pidx, pos, vel, eps2, h2, acc, jrk, pot, nnb, rnnb, false);
+}
+PGB_EXPORT int g6calc_lasthalfn(LASTHALF_ARGS) {
+    (void)gpid;
+    return lasthalf_impl(nj, ni, pidx, pos, vel, eps2, h2, acc, jrk, pot, nullptr, nullptr, true);
+}
+PGB_EXPORT int g6calc_lasthalf2n(LASTHALF_ARGS, int* nnb) {
+    (void)gpid;
+    return lasthalf_impl(nj, ni, pidx, pos, vel, eps2, h2, acc, jrk, pot, nnb, nullptr, true);
+}
+PGB_EXPORT int g6calc_lasthalf2np(LASTHALF_ARGS, int* nnb, float* rnnb) {
+    (void)gpid;
+    return lasthalf_impl(nj, ni, pidx, pos, vel, eps2, h2, acc, jrk, pot, nnb, rnnb, true);
+}
+
+// 0: success, 1: a list of the last lasthalf*n call overflowed (phantom_g6.c:482-486)
+PGB_EXPORT int g6_read_neighbour_list(int gpid) {
+    (void)gpid;
+    return S.nb_error;
+}
+
+// 0: success, 1: nb > maxlen (phantom_g6.c:495-499, gravity.c:135-147)
+PGB_EXPORT int g6_get_neighbour_list(int gpid, int ipipe, int maxlen, int* nblen, int* nbl) {
+    (void)gpid;
+    if (ipipe < 0 || ipipe >= S.nb_ni) {
+        raise(g_err, LIB, PGB_ERR_ARG, "g6_get_neighbour_list: ipipe %d outside [0, %d)", ipipe, S.nb_ni);
+        return 1;
+    }
+    if (S.nbcounts[ipipe] > maxlen || S.nbcounts[ipipe] > nbmax()) return 1;
+    const std::vector<int>& v = S.nblists[ipipe];
+    *nblen = (int)v.size();
+    for (size_t k = 0; k < v.size(); k++) nbl[k] = v[k];
+    return 0;
+}
+
+PGB_EXPORT void g6_debugfunc(int tmp) {
+    FILE* fp = std::fopen("dump.dat", "a");
+    if (!fp) return;
+    std::fprintf(fp, "%d\n", tmp);
+    std::fclose(fp);
+}
+PGB_EXPORT void g6_debugfunc_double(double tmp) {
+    FILE* fp = std::fopen("dump.dat", "a");
+    if (!fp) return;
+    std::fprintf(fp, "%+e\n", tmp);
+    std::fclose(fp);
+}
+PGB_EXPORT void g6_dump(double tim, int n, double* m, double (*x)[3], double (*v)[3]) {
+    char out[64];
+    std::snprintf(out, sizeof out, "dump.dat.%05d", (int)tim);
+    FILE* fp = std::fopen(out, "w");
+    if (!fp) return;
+    for (int i = 0; i < n; i++) {
+        std::fprintf(fp, "%+.16e", m[i]);
+        std::fprintf(fp, " %+.16e %+.16e %+.16e", x[i][0], x[i][1], x[i][2]);
+        std::fprintf(fp, " %+.16e %+.16e %+.16e", v[i][0], v[i][1], v[i][2]);
+        std::fprintf(fp, "\n");
+    }
+    std::fclose(fp);
+}
+
+// Fortran twins (phantom_g6.c: every entry point has a `_` variant taking pointers)
+PGB_EXPORT void g6_open_(int* gpid) { g6_open(*gpid); }
+PGB_EXPORT void g6_close_(int* gpid) { g6_close(*gpid); }
+PGB_EXPORT void g6_set_tunit_(int* v) { g6_set_tunit(*v); }
+PGB_EXPORT void g6_set_xunit_(int* v) { g6_set_xunit(*v); }
+PGB_EXPORT void g6_reset_(int* v) { g6_reset(*v); }
+PGB_EXPORT void g6_reset_fofpga_(int* v) { g6_reset_fofpga(*v); }
+PGB_EXPORT int g6_npipes_(void) { return g6_npipes(); }
+PGB_EXPORT void g6_setup_njdata_(int* gpid, int* nj) { g6_setup_njdata(*gpid, *nj); }
+PGB_EXPORT void g6_set_j_particle_(int* gpid, int* padr, int* pidx, double* t, double* dt, double* mss, double* snp,
+                                   double* jrk, double* acc, double* vel, double* pos) {
+    g6_set_j_particle(*gpid, *padr, *pidx, *t, *dt, *mss, snp, jrk, acc, vel, pos);
+}
+PGB_EXPORT void g6_set_ti_(int* gpid, double* t) { g6_set_ti(*gpid, *t); }
+PGB_EXPORT void g6calc_firsthalf_(int* gpid, int* nj, int* ni, int* pidx, double (*pos)[3], double (*vel)[3],
+                                  double (*acc)[3], double (*jrk)[3], double* pot, double* eps2, double* h2) {
+    g6calc_firsthalf(*gpid, *nj, *ni, pidx, pos, vel, acc, jrk, pot, *eps2, h2);
+}
+#define LASTHALF_FARGS int *gpid, int *nj, int *ni, int *pidx, double(*pos)[3], double(*vel)[3], double *eps2, \
+                       double *h2, double(*acc)[3], double(*jrk)[3], double *pot
+#define LASTHALF_FCALL *gpid, *nj, *ni, pidx, pos, vel, *eps2, h2, acc, jrk, pot
+PGB_EXPORT int g6calc_lasthalf_(LASTHALF_FARGS) { return g6calc_lasthalf(LASTHALF_FCALL); }
+PGB_EXPORT int g6calc_lasthalf2_(LASTHALF_FARGS, int* nnb) { return g6calc_lasthalf2(LASTHALF_FCALL, nnb); }
+PGB_EXPORT int g6calc_lasthalf2p_(LASTHALF_FARGS, int* nnb, float* rnnb) {
+    return g6calc_lasthalf2p(LASTHALF_FCALL, nnb, rnnb);
+}
+PGB_EXPORT int g6calc_lasthalfn_(LASTHALF_FARGS) { return g6calc_lasthalfn(LASTHALF_FCALL); }
+PGB_EXPORT int g6calc_lasthalf2n_(LASTHALF_FARGS, int* nnb) { return g6calc_lasthalf2n(LASTHALF_FCALL, nnb); }
+PGB_EXPORT int g6calc_lasthalf2np_(LASTHALF_FARGS, int* nnb, float* rnnb) {
+    return g6calc_lasthalf2np(LASTHALF_FCALL, nnb, rnnb);
+}
+PGB_EXPORT int g6_read_neighbour_list_(int* gpid) { return g6_read_neighbour_list(*gpid); }
+PGB_EXPORT int g6_get_neighbour_list_(int* gpid, int* ipipe, int* maxlen, int* nblen, int* nbl) {
+    return g6_get_neighbour_list(*gpid, *ipipe, *maxlen, nblen, nbl);
+}
+PGB_EXPORT void g6_debugfunc_(int* v) { g6_debugfunc(*v); }
+PGB_EXPORT void g6_debugfunc_double_(double* v) { g6_debugfunc_double(*v); }
+PGB_EXPORT void g6_dump_(double* tim, int* n, double* m, double (*x)[3], double (*v)[3]) { g6_dump(*tim, *n, m, x, v); }

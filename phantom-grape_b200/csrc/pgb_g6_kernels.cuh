@@ -1,0 +1,269 @@
+// pgb_g6_kernels.cuh -- PG6 (GRAPE-6) j-predictor and 4th-order Hermite force / jerk /
+// potential / nearest-neighbour / neighbour-list kernels for sm_100a.
+//
+// Precision layout (the reference's, PG6/libpg6/gravity.c:311-420): the predictor and the
+// relative position x_j - x_i are FP64; the difference is rounded to FP32 and everything after
+// it (r^2, rsqrt, velocity difference, products) is FP32.  Sums are FP32 within one j tile and
+// folded into FP64 after every tile; split j-ranges are reduced in FP64 in chunk order.
+//
+// Per pair (q = -2/r with one Newton step, pgb::minus2_over_r; self pair masked by index):
+//   pot_sum += m q, acc_sum += (m q^3) dx, jrk_sum += (m q^3) (dv - (3/4) q^2 (dx.dv) dx)
+// and finally acc = -acc_sum/8, jerk = -jrk_sum/8, pot = pot_sum/2 (phantom_g6.c:200-208), i.e.
+//   acc = sum m dx/r^3, jerk = sum m (dv/r^3 - 3 (dx.dv) dx/r^5), pot = -sum m/r.
+// Nearest neighbour: the smallest key q (= -2/r_soft) over j != i; ties -> smallest j address.
+// Neighbour list: j with q <= -2/h_i (softened r <= h_i), appended with an atomic counter.
+#pragma once
+
+#include "pgb_common.cuh"
+
+namespace pgb {
+
+// j-memory record as stored by g6_set_j_particle (gravity.c:31-40): a2 = acc/2, j6 = jerk/6.
+struct G6Ptcl {
+    double pos[3], vel[3], acc2[3], jrk6[3];
+    double mass, tim;
+    int idx, pad[3];
+};
+
+// Predicted j record in HBM and shared memory: 48 bytes, three 16-byte words.
+struct __align__(16) G6PredJ {
+    double x, y;          // word 0
+    double z;             // word 1
+    float m;
+    int id;
+    float vx, vy, vz;     // word 2
+    float pad;
+};
+
+// i-particle record: 48 bytes.
+struct __align__(16) G6I {
+    double x, y;
+    double z;
+    float vx, vy;
+    float vz;
+    int id;
+    float h2;             // neighbour radius^2 (0: no neighbours)
+    float pad;
+};
+
+// Per-i result (final or partial).  key/jadr: nearest-neighbour key and j address.
+struct __align__(16) G6Out {
+    double ax, ay, az;
+    double jx, jy, jz;
+    double pot;
+    float key;
+    int jadr;
+};
+
+struct G6Args {
+    const G6I* ipart;
+    const G6PredJ* jpred;
+    float eps2;
+    const Task* tasks;
+    int ntasks;
+    int* task_counter;
+    const Group* groups;
+    int* group_counters;
+    G6Out* partial;        // [rows][itile]
+    G6Out* out;            // [.] indexed by absolute i
+    int itile;
+    // neighbour lists (NBL variant): per absolute i, count and up to maxlen j addresses
+    int* nb_count;
+    int* nb_list;
+    int nb_maxlen;
+};
+
+// FP64 predictor: one thread per j (gravity.c:149-193; velocity stored as float, :168-173).
+__global__ void g6_predict_kernel(const G6Ptcl* __restrict__ p, int nj, double ti, G6PredJ* __restrict__ out) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nj) return;
+    const G6Ptcl& P = p[j];
+    double dt = ti - P.tim;
+    double dt2 = dt * dt, dt3 = dt2 * dt;
+    G6PredJ o;
+    o.x = P.pos[0] + P.vel[0] * dt + P.acc2[0] * dt2 + P.jrk6[0] * dt3;
+    o.y = P.pos[1] + P.vel[1] * dt + P.acc2[1] * dt2 + P.jrk6[1] * dt3;
+    o.z = P.pos[2] + P.vel[2] * dt + P.acc2[2] * dt2 + P.jrk6[2] * dt3;
+    o.vx = (float)(P.vel[0] + 2.0 * P.acc2[0] * dt + 3.0 * P.jrk6[0] * dt2);
+    o.vy = (float)(P.vel[1] + 2.0 * P.acc2[1] * dt + 3.0 * P.jrk6[1] * dt2);
+    o.vz = (float)(P.vel[2] + 2.0 * P.acc2[2] * dt + 3.0 * P.jrk6[2] * dt2);
+    o.m = (float)P.mass;
+    o.id = P.idx;
+    o.pad = 0.f;
+    out[j] = o;
+}
+
+struct G6Acc {
+    float ax, ay, az, jx, jy, jz, pot;
+};
+
+template <bool NN, bool NBL>
+__device__ __forceinline__ void g6_pair(const G6PredJ& J, int jadr, double xi, double yi, double zi, float vxi,
+                                        float vyi, float vzi, int idi, float eps2, float hinv, G6Acc& a,
+                                        float& kmin, int& kadr, int* nbc, int* nbl, int nbmax) {
+    float dx = __double2float_rn(J.x - xi);
+    float dy = __double2float_rn(J.y - yi);
+    float dz = __double2float_rn(J.z - zi);
+    float dvx = J.vx - vxi, dvy = J.vy - vyi, dvz = J.vz - vzi;
+    float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmaf_rn(dx, dx, eps2)));
+    float q = minus2_over_r(r2);
+    q = (J.id == idi) ? 0.0f : q;
+    if constexpr (NN) {
+        bool lt = q < kmin;
+        kmin = lt ? q : kmin;
+        kadr = lt ? jadr : kadr;
+    }
+    if constexpr (NBL) {
+        if (q <= hinv) {
+            int slot = atomicAdd(nbc, 1);
+            if (slot < nbmax) nbl[slot] = jadr;
+        }
+    }
+    a.pot = __fmaf_rn(J.m, q, a.pot);
+    float rv = __fmaf_rn(dz, dvz, __fmaf_rn(dy, dvy, dx * dvx));
+    float mq = J.m * q;
+    float q2 = q * q;
+    float mq3 = mq * q2;
+    float c = -0.75f * q2 * rv;
+    a.ax = __fmaf_rn(mq3, dx, a.ax);
+    a.ay = __fmaf_rn(mq3, dy, a.ay);
+    a.az = __fmaf_rn(mq3, dz, a.az);
+    a.jx = __fmaf_rn(mq3, __fmaf_rn(c, dx, dvx), a.jx);
+    a.jy = __fmaf_rn(mq3, __fmaf_rn(c, dy, dvy), a.jy);
+    a.jz = __fmaf_rn(mq3, __fmaf_rn(c, dz, dvz), a.jz);
+}
+
+__device__ __forceinline__ G6Out g6_finish(const G6Out& s) {
+    G6Out o;
+    o.ax = -0.125 * s.ax;
+    o.ay = -0.125 * s.ay;
+    o.az = -0.125 * s.az;
+    o.jx = -0.125 * s.jx;
+    o.jy = -0.125 * s.jy;
+    o.jz = -0.125 * s.jz;
+    o.pot = 0.5 * s.pot;
+    o.key = s.key;
+    o.jadr = s.jadr;
+    return o;
+}
+
+__device__ __forceinline__ G6Out ldcg_out(const G6Out* p) {
+    G6Out v;
+    const double* d = reinterpret_cast<const double*>(p);
+    v.ax = __ldcg(d + 0);
+    v.ay = __ldcg(d + 1);
+    v.az = __ldcg(d + 2);
+    v.jx = __ldcg(d + 3);
+    v.jy = __ldcg(d + 4);
+    v.jz = __ldcg(d + 5);
+    v.pot = __ldcg(d + 6);
+    const float* f = reinterpret_cast<const float*>(d + 7);
+    v.key = __ldcg(f);
+    v.jadr = __ldcg(reinterpret_cast<const int*>(f + 1));
+    return v;
+}
+
+template <int NT, int IPT, bool NN, bool NBL>
+__global__ void __launch_bounds__(NT) g6_kernel(G6Args A) {
+    __shared__ G6PredJ sj[NT];
+    __shared__ int s_task, s_flag;
+
+    for (;;) {
+        int t = next_task(A.task_counter, &s_task);
+        if (t >= A.ntasks) break;
+        const Task T = A.tasks[t];
+
+        double xi[IPT], yi[IPT], zi[IPT];
+        float vxi[IPT], vyi[IPT], vzi[IPT], hinv[IPT];
+        int idi[IPT];
+        double S[IPT][7];
+        float kmin[IPT];
+        int kadr[IPT];
+#pragma unroll
+        for (int k = 0; k < IPT; k++) {
+            int li = threadIdx.x + k * NT;
+            int ii = T.i0 + (li < T.ni ? li : 0);
+            const G6I P = A.ipart[ii];
+            xi[k] = P.x; yi[k] = P.y; zi[k] = P.z;
+            vxi[k] = P.vx; vyi[k] = P.vy; vzi[k] = P.vz;
+            idi[k] = P.id;
+            // gravity.c:688-695: -2/h, or -1e10 when h2 == 0 (no neighbours); padding lanes none
+            hinv[k] = (li >= T.ni) ? -INFINITY : ((P.h2 == 0.0f) ? -1e10f : -2.0f / sqrtf(P.h2));
+#pragma unroll
+            for (int c = 0; c < 7; c++) S[k][c] = 0.0;
+            kmin[k] = 10.0f;   // gravity_kernel2 starts its key at 10 and index at -1 (:495-496)
+            kadr[k] = -1;
+        }
+
+        for (int jt = 0; jt < T.nj; jt += NT) {
+            const int nt = min(NT, T.nj - jt);
+            __syncthreads();
+            if (threadIdx.x < nt) sj[threadIdx.x] = A.jpred[T.j0 + jt + threadIdx.x];
+            __syncthreads();
+            G6Acc a[IPT];
+#pragma unroll
+            for (int k = 0; k < IPT; k++) a[k] = G6Acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll 2
+            for (int j = 0; j < nt; j++) {
+                const G6PredJ J = sj[j];
+                const int jadr = T.j0 + jt + j;
+#pragma unroll
+                for (int k = 0; k < IPT; k++) {
+                    int li = threadIdx.x + k * NT;
+                    int gi = T.i0 + (li < T.ni ? li : 0);
+                    g6_pair<NN, NBL>(J, jadr, xi[k], yi[k], zi[k], vxi[k], vyi[k], vzi[k], idi[k], A.eps2, hinv[k],
+                                     a[k], kmin[k], kadr[k], NBL ? A.nb_count + gi : nullptr,
+                                     NBL ? A.nb_list + (size_t)gi * A.nb_maxlen : nullptr, A.nb_maxlen);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < IPT; k++) {
+                S[k][0] += (double)a[k].ax;
+                S[k][1] += (double)a[k].ay;
+                S[k][2] += (double)a[k].az;
+                S[k][3] += (double)a[k].jx;
+                S[k][4] += (double)a[k].jy;
+                S[k][5] += (double)a[k].jz;
+                S[k][6] += (double)a[k].pot;
+            }
+        }
+
+        G6Out* dst_row = (T.group < 0) ? nullptr : A.partial + (size_t)T.slot * A.itile;
+#pragma unroll
+        for (int k = 0; k < IPT; k++) {
+            int li = threadIdx.x + k * NT;
+            if (li >= T.ni) continue;
+            G6Out o;
+            o.ax = S[k][0]; o.ay = S[k][1]; o.az = S[k][2];
+            o.jx = S[k][3]; o.jy = S[k][4]; o.jz = S[k][5];
+            o.pot = S[k][6];
+            o.key = kmin[k];
+            o.jadr = kadr[k];
+            if (dst_row) dst_row[li] = o;
+            else A.out[T.i0 + li] = g6_finish(o);
+        }
+        if (!dst_row) continue;
+        const Group G = A.groups[T.group];
+        if (group_arrive(A.group_counters, T.group, G.nchunk, &s_flag)) {
+#pragma unroll
+            for (int k = 0; k < IPT; k++) {
+                int li = threadIdx.x + k * NT;
+                if (li >= G.ni) continue;
+                G6Out s = ldcg_out(A.partial + (size_t)G.slot0 * A.itile + li);
+                for (int c = 1; c < G.nchunk; c++) {
+                    G6Out v = ldcg_out(A.partial + (size_t)(G.slot0 + c) * A.itile + li);
+                    s.ax += v.ax; s.ay += v.ay; s.az += v.az;
+                    s.jx += v.jx; s.jy += v.jy; s.jz += v.jz;
+                    s.pot += v.pot;
+                    if (v.key < s.key) {  // strict: the earlier chunk (smaller j) wins ties
+                        s.key = v.key;
+                        s.jadr = v.jadr;
+                    }
+                }
+                A.out[G.i0 + li] = g6_finish(s);
+            }
+        }
+    }
+}
+
+}  // namespace pgb

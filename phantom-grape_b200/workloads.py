@@ -1,0 +1,199 @@
+"""Seeded synthetic particle sets for the force-engine workloads.
+
+All randomness comes from a counter-based splitmix64 stream (``Rng``), so every harness
+(tests, benchmark, fixture scripts) gets identical bits on any machine.  Seeds are
+``20261203 + config index`` by default.  The sets stand in for the reference's sample
+inputs (Plummer spheres, uniform boxes, cluster sets) with the same shapes, sizes and
+distributions; no data file is read.
+
+Workloads
+---------
+* ``plummer_g5``      PG5 newton direct sum: N=16384 equal-mass Plummer sphere, G=1, a=1,
+                      radii truncated at 22.8 a, float32-rounded positions, eps = 0.01.
+* ``hermite_state``   PG6 Hermite: Plummer sphere with distribution-function velocities,
+                      FP64, eps = 1e-4, block time-step state (levels 3..12, t_j lagging
+                      t_now by 0, 1/2 or 1 of the particle's step).
+* ``hermite_schedule``64 force calls with active sets of 2^k particles, k uniform in 4..16.
+* ``cluster_set``     1024 independent Plummer clusters, N log-uniform in [256, 16384].
+* ``uniform_box_groups`` PG5 table (TreePM PP): N=2^20 uniform periodic box, i-groups from a
+                      128^3 cell mesh, j-lists within r_cut with explicit periodic shifts.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+SEED0 = 20261203
+_GOLD = np.uint64(0x9E3779B97F4A7C15)
+_M1 = np.uint64(0xBF58476D1CE4E5B9)
+_M2 = np.uint64(0x94D049BB133111EB)
+
+
+class Rng:
+    """Counter-based splitmix64: value k of stream s is mix(s + (k+1) * golden)."""
+
+    def __init__(self, seed: int):
+        self.state = np.uint64(seed & 0xFFFFFFFFFFFFFFFF)
+        self.k = 0
+
+    def u64(self, n: int) -> np.ndarray:
+        with np.errstate(over="ignore"):
+            ks = np.arange(self.k + 1, self.k + 1 + n, dtype=np.uint64)
+            z = self.state + ks * _GOLD
+            z = (z ^ (z >> np.uint64(30))) * _M1
+            z = (z ^ (z >> np.uint64(27))) * _M2
+            z = z ^ (z >> np.uint64(31))
+        self.k += n
+        return z
+
+    def uniform(self, n: int) -> np.ndarray:
+        """Uniform doubles in [0, 1) with 53 random bits."""
+        return (self.u64(n) >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+
+    def integers(self, lo: int, hi: int, n: int) -> np.ndarray:
+        """Integers in [lo, hi) (hi - lo small; bias < 2^-40)."""
+        return lo + (self.u64(n) % np.uint64(hi - lo)).astype(np.int64)
+
+    def permutation(self, n: int) -> np.ndarray:
+        return np.argsort(self.u64(n), kind="stable")
+
+
+def _isotropic(rng: Rng, r: np.ndarray) -> np.ndarray:
+    n = len(r)
+    cth = 2.0 * rng.uniform(n) - 1.0
+    phi = 2.0 * math.pi * rng.uniform(n)
+    sth = np.sqrt(np.maximum(0.0, 1.0 - cth * cth))
+    return np.stack([r * sth * np.cos(phi), r * sth * np.sin(phi), r * cth], axis=1)
+
+
+def plummer_radii(rng: Rng, n: int, rmax: float = 22.8) -> np.ndarray:
+    out = np.empty(0)
+    while len(out) < n:
+        u = rng.uniform(2 * (n - len(out)) + 16)
+        u = u[u > 0]
+        r = 1.0 / np.sqrt(u ** (-2.0 / 3.0) - 1.0)
+        out = np.concatenate([out, r[r <= rmax]])
+    return out[:n]
+
+
+def plummer_speeds(rng: Rng, r: np.ndarray) -> np.ndarray:
+    """Aarseth-Henon-Wielen rejection: q on g(q) = q^2 (1-q^2)^(7/2), v = q sqrt(2) (1+r^2)^(-1/4)."""
+    n = len(r)
+    q = np.empty(0)
+    while len(q) < n:
+        m = 4 * (n - len(q)) + 16
+        x = rng.uniform(m)
+        y = 0.1 * rng.uniform(m)
+        ok = y < x * x * (1.0 - x * x) ** 3.5
+        q = np.concatenate([q, x[ok]])
+    q = q[:n]
+    return q * math.sqrt(2.0) * (1.0 + r * r) ** -0.25
+
+
+@dataclass
+class G5Set:
+    x: np.ndarray        # [n,3] float64 (float32-representable)
+    m: np.ndarray        # [n]   float64 (float32-representable)
+    eps: float
+
+
+def plummer_g5(n: int = 16384, seed: int = SEED0 + 0, eps: float = 0.01) -> G5Set:
+    rng = Rng(seed)
+    x = _isotropic(rng, plummer_radii(rng, n))
+    x = x.astype(np.float32).astype(np.float64)
+    m = np.full(n, np.float64(np.float32(1.0 / n)))
+    return G5Set(x=x, m=m, eps=eps)
+
+
+@dataclass
+class HermiteState:
+    pos: np.ndarray      # [n,3] FP64 at t_j
+    vel: np.ndarray      # [n,3]
+    acc2: np.ndarray     # [n,3] acc / 2   (the library's predictor convention)
+    jrk6: np.ndarray     # [n,3] jerk / 6
+    mass: np.ndarray     # [n]
+    tj: np.ndarray       # [n]  particle times
+    idx: np.ndarray      # [n]  int32 ids
+    eps2: float
+    t_now: float
+
+
+def plummer_hermite(n: int, seed: int, rmax: float = 22.8):
+    rng = Rng(seed)
+    r = plummer_radii(rng, n, rmax)
+    x = _isotropic(rng, r)
+    v = _isotropic(rng, plummer_speeds(rng, r))
+    # centre of mass / momentum at rest
+    x -= x.mean(axis=0)
+    v -= v.mean(axis=0)
+    return x, v, np.full(n, 1.0 / n), rng
+
+
+def hermite_state(n: int = 65536, seed: int = SEED0 + 1, eps: float = 1e-4,
+                  force_fn=None, t_now: float = 1.0) -> HermiteState:
+    """Block time-step state.  ``force_fn(x, v, m, eps2) -> (acc, jrk)`` supplies the
+    instantaneous acceleration and jerk (an FP64 direct sum in tests, the GPU engine in the
+    benchmark); with ``None`` they are zero (pure drift prediction)."""
+    x, v, m, rng = plummer_hermite(n, seed)
+    eps2 = eps * eps
+    if force_fn is not None:
+        a, j = force_fn(x, v, m, eps2)
+    else:
+        a = np.zeros_like(x)
+        j = np.zeros_like(x)
+    lev = rng.integers(3, 13, n)
+    dt = np.ldexp(1.0, -lev)
+    u = rng.integers(0, 3, n) * 0.5
+    tj = t_now - dt * u
+    # positions at t_j consistent with the Taylor expansion about t_now (back-extrapolated)
+    h = (tj - t_now)[:, None]
+    pos = x + v * h + 0.5 * a * h * h + j * h ** 3 / 6.0
+    vel = v + a * h + 0.5 * j * h * h
+    acc = a + j * h
+    return HermiteState(pos=pos, vel=vel, acc2=0.5 * acc, jrk6=j / 6.0, mass=m, tj=tj,
+                        idx=np.arange(n, dtype=np.int32), eps2=eps2, t_now=t_now)
+
+
+def hermite_schedule(n: int = 65536, ncalls: int = 64, kmin: int = 4, kmax: int = 16,
+                     seed: int = SEED0 + 101):
+    """List of active sets (int32 index arrays) of size 2^k, k uniform in [kmin, kmax]."""
+    rng = Rng(seed)
+    ks = rng.integers(kmin, kmax + 1, ncalls)
+    sets = []
+    for k in ks:
+        size = min(1 << int(k), n)
+        perm = rng.permutation(n)
+        sets.append(np.sort(perm[:size]).astype(np.int32))
+    return sets
+
+
+@dataclass
+class ClusterSet:
+    offsets: np.ndarray  # [ncl+1] particle offsets
+    pos: np.ndarray      # [N,3] FP64
+    vel: np.ndarray
+    mass: np.ndarray
+    eps2: float
+    sizes: np.ndarray = field(default=None)
+
+
+def cluster_set(ncl: int = 1024, nmin: int = 256, nmax: int = 16384,
+                seed: int = SEED0 + 4, eps: float = 1e-4, spacing: float = 64.0) -> ClusterSet:
+    rng = Rng(seed)
+    u = rng.uniform(ncl)
+    sizes = np.rint(np.exp(math.log(nmin) + u * (math.log(nmax) - math.log(nmin)))).astype(np.int64)
+    sizes = np.clip(sizes, nmin, nmax)
+    offs = np.concatenate([[0], np.cumsum(sizes)])
+    pos = np.empty((offs[-1], 3))
+    vel = np.empty((offs[-1], 3))
+    mass = np.empty(offs[-1])
+    for c in range(ncl):
+        x, v, m, _ = plummer_hermite(int(sizes[c]), seed * 7919 + c)
+        centre = np.array([spacing * (c % 32), spacing * ((c // 32) % 32), spacing * (c // 1024)])
+        s = slice(offs[c], offs[c + 1])
+        pos[s] = x + centre
+        vel[s] = v
+        mass[s] = m
+    return ClusterSet(offsets=offs, pos=pos, vel=vel, mass=mass, eps2=eps * eps, sizes=sizes)

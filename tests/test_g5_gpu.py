@@ -1,0 +1,235 @@
+"""GPU parity of the GRAPE-5 newton / symmetric / quadrupole path (lib/libpg5*.so).
+
+Every case is checked against the FP64 oracle (oracle/pg_oracle.c) and, where the reference
+library was compiled here (oracle/_ref), against the reference's own AVX2 result on the same
+inputs.  Tolerances:
+  * vs FP64: rms relative |da|/|a| <= 1e-6, rms relative pot error <= 1e-6
+  * vs reference AVX2: max relative |da|/|a| <= 2e-3 and pot <= 2e-5 (newton), and
+    rms 1e-3 / max 1e-2 / pot 3e-4 (quadrupole cells), the reference's own error against
+    FP64 (raw 12-bit rsqrt) being the floor.
+"""
+import threading
+
+import numpy as np
+import pytest
+
+from conftest import pgb, gpu_available
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+W = pgb.workloads
+
+
+def rel_err(a, b):
+    return np.linalg.norm(a - b, axis=1) / np.linalg.norm(b, axis=1)
+
+
+def rms(x):
+    return float(np.sqrt(np.mean(np.square(x))))
+
+
+@pytest.fixture(scope="module")
+def g5():
+    if not gpu_available():
+        pytest.skip("no GPU")
+    lib = pgb.ffi.G5()
+    lib.L.g5_open()
+    return lib
+
+
+@pytest.fixture(scope="module")
+def plummer():
+    return W.plummer_g5(16384)
+
+
+def test_newton_full_size_vs_fp64(g5, plummer):
+    s = plummer
+    a, p = g5.force(s.x, s.m, s.eps, s.x)
+    ao, po = O.g5_newton(s.x, s.eps ** 2, s.x, s.m)
+    ea = rel_err(a, ao)
+    ep = np.abs(p - po) / np.abs(po)
+    assert rms(ea) <= 1e-6, (rms(ea), ea.max())
+    assert ea.max() <= 1e-4
+    assert rms(ep) <= 1e-6 and ep.max() <= 1e-5
+
+
+@pytest.mark.skipif(not O.ref_available("libpg5_ref.so"), reason="reference not built")
+def test_newton_vs_reference_avx2(g5):
+    from oracle import refapi
+    s = W.plummer_g5(4096, seed=77)
+    a, p = g5.force(s.x, s.m, s.eps, s.x)
+    ar, pr = refapi.RefG5().force(s.x, s.m, s.eps, s.x)
+    assert rel_err(a, ar).max() <= 2e-3
+    assert (np.abs(p - pr) / np.abs(pr)).max() <= 2e-5
+
+
+@pytest.mark.parametrize("ni,nj", [(1, 1), (1, 7), (3, 129), (513, 1), (4, 0), (1000, 3001), (517, 5000)])
+def test_newton_ragged_sizes(g5, ni, nj):
+    rng = W.Rng(1000 + ni * 7 + nj)
+    xj = (rng.uniform(3 * nj).reshape(-1, 3) - 0.5).astype(np.float32).astype(np.float64)
+    mj = rng.uniform(nj).astype(np.float32).astype(np.float64) + 0.1
+    xi = (rng.uniform(3 * ni).reshape(-1, 3) - 0.5).astype(np.float32).astype(np.float64)
+    eps = 0.05
+    g5.set_xmj(0, xj, mj)
+    g5.L.g5_set_eps_to_all(eps)
+    g5.L.g5_set_n(nj)
+    a, p = g5.calculate_force_on_x(xi)
+    if nj == 0:
+        assert np.all(a == 0) and np.all(p == 0)
+        return
+    ao, po = O.g5_newton(xi, np.float32(eps * eps), xj, mj)
+    np.testing.assert_allclose(a, ao, rtol=2e-6, atol=2e-6 * np.abs(ao).max())
+    np.testing.assert_allclose(p, po, rtol=2e-6)
+
+
+def test_pipeline_path_run_get_force(g5):
+    """g5_set_xi / g5_run / g5_get_force in chunks of g5_get_number_of_pipelines()."""
+    s = W.plummer_g5(2000, seed=5)
+    g5.set_xmj(0, s.x, s.m)
+    g5.L.g5_set_eps_to_all(s.eps)
+    g5.L.g5_set_n(len(s.m))
+    npipe = g5.L.g5_get_number_of_pipelines()
+    xi = np.ascontiguousarray(s.x[:37])
+    a = np.zeros((37, 3))
+    p = np.zeros(37)
+    for off in range(0, 37, npipe):
+        n = min(npipe, 37 - off)
+        g5.L.g5_set_xi(n, pgb.ffi.ptr(xi[off:off + n]))
+        g5.L.g5_run()
+        aa = np.zeros((n, 3))
+        pp = np.zeros(n)
+        g5.L.g5_get_force(n, pgb.ffi.ptr(aa), pgb.ffi.ptr(pp))
+        a[off:off + n] = aa
+        p[off:off + n] = pp
+    ao, po = O.g5_newton(xi, np.float32(s.eps ** 2), s.x, s.m)
+    assert rms(rel_err(a, ao)) <= 1e-6
+    np.testing.assert_allclose(p, po, rtol=1e-5)
+
+
+def test_set_xei_per_particle_eps_and_partial_upload(g5):
+    s = W.plummer_g5(3000, seed=9)
+    # upload j in two absolute-address pieces: xj is indexed absolutely (phantom_g5.c:193)
+    xj = np.ascontiguousarray(s.x)
+    mj = np.ascontiguousarray(s.m)
+    g5.L.g5_set_xmj(0, 1001, pgb.ffi.ptr(xj), pgb.ffi.ptr(mj))
+    g5.L.g5_set_xmj(1001, 1999, pgb.ffi.ptr(xj), pgb.ffi.ptr(mj))
+    g5.L.g5_set_n(3000)
+    xi = s.x[::7].copy()
+    e2 = (np.linspace(0.001, 0.05, len(xi)) ** 2).astype(np.float32).astype(np.float64)
+    a, p = g5.calculate_force_on_x(xi, eps2=e2)
+    ao, po = O.g5_newton(xi, e2, s.x, s.m)
+    assert rms(rel_err(a, ao)) <= 1e-6
+    np.testing.assert_allclose(p, po, rtol=1e-5)
+
+
+def test_mc_devids_from_threads(g5):
+    """*MC entry points are independent per devid (phantom_g5.c:19-28); run 4 host threads."""
+    sets = [W.plummer_g5(1500 + 100 * k, seed=40 + k) for k in range(4)]
+    g5.L.g5_set_eps_to_all(0.01)
+    res = [None] * 4
+
+    def work(k):
+        s = sets[k]
+        g5.set_xmj(0, s.x, s.m, devid=k)
+        g5.L.g5_set_nMC(k, len(s.m))
+        res[k] = g5.calculate_force_on_x(s.x, devid=k)
+
+    th = [threading.Thread(target=work, args=(k,)) for k in range(4)]
+    [t.start() for t in th]
+    [t.join() for t in th]
+    for k, s in enumerate(sets):
+        ao, po = O.g5_newton(s.x, np.float32(0.01 ** 2), s.x, s.m)
+        assert rms(rel_err(res[k][0], ao)) <= 1e-6
+
+
+def test_symmetric_softening_vs_fp64():
+    if not gpu_available():
+        pytest.skip("no GPU")
+    g = pgb.ffi.G5Sym()
+    g.L.g5_open()
+    s = W.plummer_g5(4096, seed=11)
+    rng = W.Rng(12)
+    epsj2 = ((0.005 + 0.02 * rng.uniform(len(s.m))) ** 2).astype(np.float32).astype(np.float64)
+    g.set_xmj(0, s.x, s.m, epsj2)
+    g.L.g5_set_eps_to_all(0.0)
+    g.L.g5_set_n(len(s.m))
+    xi = s.x[:1000]
+    e2i = epsj2[:1000]
+    a, p = g.calculate_force_on_x(xi, eps2=e2i)
+    ao, po = O.g5_newton(xi, e2i, s.x, s.m, eps2j=epsj2)
+    assert rms(rel_err(a, ao)) <= 1e-6
+    np.testing.assert_allclose(p, po, rtol=1e-5)
+    if O.ref_available("libpg5sym_ref.so"):
+        from oracle import refapi
+        ar, pr = refapi.RefG5(symmetric=True).force(s.x, s.m, 0.0, xi, eps2j=epsj2, eps2i=e2i)
+        assert rel_err(a, ar).max() <= 2e-3
+
+
+def _cells(nc, seed):
+    rng = W.Rng(seed)
+    xc = (4.0 * (rng.uniform(3 * nc).reshape(-1, 3) - 0.5)).astype(np.float32).astype(np.float64)
+    mc = (0.5 + rng.uniform(nc)).astype(np.float32).astype(np.float64)
+    q = 0.01 * (rng.uniform(6 * nc).reshape(-1, 6) - 0.5)
+    q[:, 5] = -(q[:, 0] + q[:, 3])  # traceless, as source.cpp:247
+    return xc, mc, q.astype(np.float32).astype(np.float64)
+
+
+def test_quad_cells_vs_fp64(g5):
+    xc, mc, qc = _cells(3001, 21)
+    rng = W.Rng(22)
+    xi = (0.3 * (rng.uniform(3 * 700).reshape(-1, 3) - 0.5)).astype(np.float32).astype(np.float64)
+    eps = 1e-3
+    a, p = g5.quad_force(eps, xi, xc, mc, qc)
+    ao, po = O.g5_quad(xi, np.float32(eps * eps), xc, mc, qc)
+    assert rms(rel_err(a, ao)) <= 1e-6
+    # GRAPE-5 output path: the quadrupole potential comes back negated (quad_g5c.c:292)
+    np.testing.assert_allclose(-p, po, rtol=1e-5)
+    if O.ref_available("libquad_ref.so"):
+        from oracle import refapi
+        _, _, ar, pr = refapi.RefQuad().force(eps, xi, xc[:2], mc[:2], xc, mc, qc)
+        # the reference's raw 12-bit rsqrt enters as r^-5 here: its own error against FP64 on
+        # this case is rms 5.6e-4, max 5.7e-3 (acc) and 1.0e-4 (pot)
+        assert rms(rel_err(a, ar)) <= 1e-3 and rel_err(a, ar).max() <= 1e-2
+        np.testing.assert_allclose(p, pr, rtol=3e-4)
+
+
+def test_batched_plan_matches_per_group_oracle(g5):
+    import torch
+    rng = W.Rng(31)
+    # 40 groups of uneven size, each with its own j-list segment
+    ni = rng.integers(1, 700, 40)
+    nj = rng.integers(0, 5000, 40)
+    ioff = np.concatenate([[0], np.cumsum(ni)])
+    joff = np.concatenate([[0], np.cumsum(nj)])
+    xi = (rng.uniform(3 * ioff[-1]).reshape(-1, 3) - 0.5).astype(np.float32)
+    xj = (rng.uniform(3 * joff[-1]).reshape(-1, 3) - 0.5).astype(np.float32)
+    mj = (rng.uniform(joff[-1]) + 0.5).astype(np.float32) / joff[-1]
+    eps2 = np.float32(1e-4)
+    ipos = np.concatenate([xi, np.full((len(xi), 1), eps2, np.float32)], 1)
+    jpos = np.concatenate([xj, mj[:, None]], 1)
+    items = np.stack([ioff[:-1], ni, joff[:-1], nj], 1)
+    dev = torch.device("cuda")
+    d_i = torch.from_numpy(ipos).to(dev)
+    d_j = torch.from_numpy(jpos).to(dev)
+    d_o = torch.zeros((len(xi), 4), dtype=torch.float64, device=dev)
+    plan = g5.plan_create(g5.NEWTON, items)
+    try:
+        for _ in range(2):  # launching the same plan twice gives the same answer
+            d_o.zero_()
+            g5.plan_launch(plan, d_i.data_ptr(), d_j.data_ptr(), None, d_o.data_ptr(),
+                           torch.cuda.current_stream().cuda_stream)
+            torch.cuda.synchronize()
+            out = d_o.cpu().numpy()
+            for k in range(40):
+                si = slice(ioff[k], ioff[k + 1])
+                sj = slice(joff[k], joff[k + 1])
+                if nj[k] == 0:
+                    assert np.all(out[si] == 0)
+                    continue
+                ao, po = O.g5_newton(xi[si].astype(np.float64), eps2, xj[sj].astype(np.float64),
+                                     mj[sj].astype(np.float64))
+                np.testing.assert_allclose(out[si, :3], ao, rtol=2e-6, atol=2e-6 * np.abs(ao).max())
+                np.testing.assert_allclose(-out[si, 3], po, rtol=2e-6)
+    finally:
+        g5.plan_destroy(plan)
