@@ -1,0 +1,119 @@
+/*
+ * pgb_g6.h -- C ABI of lib/libpg6.so: the GRAPE-6 4th-order Hermite API on the B200 engine.
+ *
+ * Drop-in replacement for the reference library built from PG6/libpg6 (gp6util.h:1-101):
+ * same symbols (each with its Fortran `_` twin), same conventions: g6_set_j_particle takes
+ * acc/2 and jerk/6, g6calc_lasthalf* return acc = sum m dx/r^3, jerk, pot = -sum m/r with the
+ * self pair excluded by id, nnb = nearest-neighbour id, rnnb = its softened distance.
+ * Differences are listed in the library source (csrc/pgb_g6.cu header comment).
+ */
+#ifndef PGB_G6_H
+#define PGB_G6_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- GRAPE-6 API: PG6/libpg6/gp6util.h:1-101 (phantom_g6.c line numbers) ---------------- */
+void g6_open(int gpid);                   /* :18-26 */
+void g6_open_(int *gpid);
+void g6_set_tunit(int tunit);             /* :36-40 (no-op) */
+void g6_set_tunit_(int *tunit);
+void g6_set_xunit(int xunit);             /* :50-54 (no-op) */
+void g6_set_xunit_(int *xunit);
+void g6_reset(int gpid);                  /* :64-68 (no-op) */
+void g6_reset_(int *gpid);
+void g6_reset_fofpga(int gpid);           /* :78-82 (no-op) */
+void g6_reset_fofpga_(int *gpid);
+void g6_close(int gpid);                  /* :92-96 */
+void g6_close_(int *gpid);
+int  g6_npipes(void);                     /* :106-109 (48; PGB_G6_NPIPES) */
+int  g6_npipes_(void);
+void g6_set_j_particle(int gpid, int padr, int pidx, double t, double dt, double mss,
+                       double *snp, double *jrk, double *acc, double *vel, double *pos);   /* :118-125 */
+void g6_set_j_particle_(int *gpid, int *padr, int *pidx, double *t, double *dt, double *mss,
+                        double *snp, double *jrk, double *acc, double *vel, double *pos);
+void g6_set_ti(int gpid, double time);    /* :138-143 */
+void g6_set_ti_(int *gpid, double *time);
+void g6calc_firsthalf(int gpid, int nj, int ni, int *pidx, double (*pos)[3], double (*vel)[3],
+                      double (*acc)[3], double (*jrk)[3], double *pot, double eps2, double *h2);  /* :153-164 */
+void g6calc_firsthalf_(int *gpid, int *nj, int *ni, int *pidx, double (*pos)[3], double (*vel)[3],
+                       double (*acc)[3], double (*jrk)[3], double *pot, double *eps2, double *h2);
+int  g6calc_lasthalf(int gpid, int nj, int ni, int *pidx, double (*pos)[3], double (*vel)[3], double eps2,
+                     double *h2, double (*acc)[3], double (*jrk)[3], double *pot);                 /* :177-211 */
+int  g6calc_lasthalf_(int *gpid, int *nj, int *ni, int *pidx, double (*pos)[3], double (*vel)[3], double *eps2,
+                      double *h2, double (*acc)[3], double (*jrk)[3], double *pot);
+int  g6calc_lasthalf2(int gpid, int nj, int ni, int *pidx, double (*pos)[3], double (*vel)[3], double eps2,
+                      double *h2, double (*acc)[3], double (*jrk)[3], double *pot, int *nnb);      /* :223-258 */
+int  g6calc_lasthalf2_(int *gpid, int *nj, int *ni, int *pidx, double (*pos)[3], double (*vel)[3],
+                       double *eps2, double *h2, double (*acc)[3], double (*jrk)[3], double *pot, int *nnb);
+int  g6calc_lasthalf2p(int gpid, int nj, int ni, int *pidx, double (*pos)[3], double (*vel)[3], double eps2,
+                       double *h2, double (*acc)[3], double (*jrk)[3], double *pot, int *nnb,
+                       float *rnnb);                                                            /* :270-306 */
+int  g6calc_lasthalf2p_(int *gpid, int *nj, int *ni, int *pidx, double (*pos)[3], double (*vel)[3],
+                        double *eps2, double *h2, double (*acc)[3], double (*jrk)[3], double *pot, int *nnb,
+                        float *rnnb);
+int  g6calc_lasthalfn(int gpid, int nj, int ni, int *pidx, double (*pos)[3], double (*vel)[3], double eps2,
+                      double *h2, double (*acc)[3], double (*jrk)[3], double *pot);                /* :318-355 */
+int  g6calc_lasthalfn_(int *gpid, int *nj, int *ni, int *pidx, double (*pos)[3], double (*vel)[3],
+                       double *eps2, double *h2, double (*acc)[3], double (*jrk)[3], double *pot);
+int  g6calc_lasthalf2n(int gpid, int nj, int ni, int *pidx, double (*pos)[3], double (*vel)[3], double eps2,
+                       double *h2, double (*acc)[3], double (*jrk)[3], double *pot, int *nnb);     /* :367-405 */
+int  g6calc_lasthalf2n_(int *gpid, int *nj, int *ni, int *pidx, double (*pos)[3], double (*vel)[3],
+                        double *eps2, double *h2, double (*acc)[3], double (*jrk)[3], double *pot, int *nnb);
+int  g6calc_lasthalf2np(int gpid, int nj, int ni, int *pidx, double (*pos)[3], double (*vel)[3], double eps2,
+                        double *h2, double (*acc)[3], double (*jrk)[3], double *pot, int *nnb,
+                        float *rnnb);                                                           /* :417-456 */
+int  g6calc_lasthalf2np_(int *gpid, int *nj, int *ni, int *pidx, double (*pos)[3], double (*vel)[3],
+                         double *eps2, double *h2, double (*acc)[3], double (*jrk)[3], double *pot, int *nnb,
+                         float *rnnb);
+void g6_setup_njdata(int gpid, int nj);   /* :468-472 (no-op) */
+void g6_setup_njdata_(int *gpid, int *nj);
+int  g6_read_neighbour_list(int gpid);    /* :482-486: 0 ok, 1 overflow */
+int  g6_read_neighbour_list_(int *gpid);
+int  g6_get_neighbour_list(int gpid, int ipipe, int maxlen, int *nblen, int *nbl);   /* :495-499 */
+int  g6_get_neighbour_list_(int *gpid, int *ipipe, int *maxlen, int *nblen, int *nbl);
+void g6_debugfunc(int tmp);               /* :508-517 */
+void g6_debugfunc_(int *tmp);
+void g6_debugfunc_double(double tmp);     /* :527-535 */
+void g6_debugfunc_double_(double *tmp);
+void g6_dump(double tim, int n, double *m, double (*x)[3], double (*v)[3]);   /* :545-561 */
+void g6_dump_(double *tim, int *n, double *m, double (*x)[3], double (*v)[3]);
+
+/* ---- library status (no reference counterpart: the reference has no error reporting) ---- */
+int  pgb6_last_error(char *buf, int len);
+void pgb6_clear_error(void);
+void pgb6_set_abort(int on);
+
+/* ---- batched path (no reference counterpart) ----------------------------------------------
+ * Replaces loops of g6calc_firsthalf/lasthalf over npipes-sized i chunks (PG6/banana/
+ * hermite.c:214-252), or over independent clusters, by one persistent launch.
+ * items[k] = {i_offset, i_count, j_offset, j_count}.  Device records (sizes from
+ * pgb6_record_sizes): j-memory G6Ptcl {double pos[3], vel[3], acc2[3], jrk6[3], mass, tim;
+ * int idx, pad[3]} (128 B), predicted j G6PredJ {double x, y, z; float m; int id; float vx, vy,
+ * vz, pad} (48 B), i G6I {double x, y, z; float vx, vy, vz; int id; float h2, pad} (48 B),
+ * result G6Out {double ax, ay, az, jx, jy, jz, pot; float key; int jadr} (64 B) with
+ * key = -2/r_soft of the nearest neighbour and jadr its j address (flags & PGB6_NN).     */
+enum { PGB6_NN = 1 };
+typedef struct pgb6_plan pgb6_plan;
+void pgb6_record_sizes(int *ptcl, int *predj, int *irec, int *out);
+int  pgb6_plan_create(pgb6_plan **plan, int nitem, const int *items, int flags);
+int  pgb6_plan_launch(pgb6_plan *plan, const void *ipart, const void *jpred, double eps2, void *out,
+                      void *stream);
+void pgb6_plan_destroy(pgb6_plan *plan);
+long long pgb6_plan_interactions(const pgb6_plan *plan);
+int  pgb6_plan_tasks(const pgb6_plan *plan);
+int  pgb6_plan_config(const pgb6_plan *plan);
+/* FP64 j predictor on device records (gravity.c:149-193): pred[j] = predict(ptcl[j], ti) */
+int  pgb6_predict(const void *ptcl, int nj, double ti, void *pred, void *stream);
+/* host-buffer batch: inputs and outputs in host memory, copies included; nnb/rnnb optional */
+int  pgb6_batch_host(int nitem, const int *items, int ni, const double (*xi)[3], const double (*vi)[3],
+                     const int *idi, int nj, const double (*xj)[3], const double (*vj)[3], const double *mj,
+                     const int *idj, double eps2, double (*acc)[3], double (*jrk)[3], double *pot, int *nnb,
+                     float *rnnb);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PGB_G6_H */

@@ -31,7 +31,10 @@ using namespace pgb;
 
 namespace {
 
-#ifdef PGB_SYMMETRIC
+#if defined(PGB_TABLE)
+const char* LIB = "libpg5table";
+constexpr int PARTICLE_KIND = G5_TABLE;
+#elif defined(PGB_SYMMETRIC)
 const char* LIB = "libpg5sym";
 constexpr int PARTICLE_KIND = G5_SYMMETRIC;
 #else
@@ -100,6 +103,7 @@ int occupancy_of(int kind) {
     switch (kind) {
         case G5_SYMMETRIC: return occupancy<G5_SYMMETRIC>();
         case G5_QUAD: return occupancy<G5_QUAD>();
+        case G5_TABLE: return occupancy<G5_TABLE>();
         default: return occupancy<G5_NEWTON>();
     }
 }
@@ -108,6 +112,7 @@ cudaError_t launch_kind(int kind, int grid, const G5Args& a, cudaStream_t s) {
     switch (kind) {
         case G5_SYMMETRIC: g5_kernel<G5_SYMMETRIC, NT, IPT><<<grid, NT, 0, s>>>(a); break;
         case G5_QUAD: g5_kernel<G5_QUAD, NT, IPT><<<grid, NT, 0, s>>>(a); break;
+        case G5_TABLE: g5_kernel<G5_TABLE, NT, IPT><<<grid, NT, 0, s>>>(a); break;
         default: g5_kernel<G5_NEWTON, NT, IPT><<<grid, NT, 0, s>>>(a); break;
     }
     return cudaGetLastError();
@@ -122,6 +127,123 @@ int choose_jchunk(long long itiles_total, int nj, int slots) {
     if (nch > maxch) nch = maxch;
     if (nch < 1) nch = 1;
     return (int)((nj + nch - 1) / nch);
+}
+
+// ------------------------------------------------------------------------------------------
+// Force-shape table of the cutoff (TreePM PP) force: PG5/table/libpg5/pg5_table.c:43-113.
+// One table per library, as the reference's global Force_table; uploaded when it changes.
+struct TableState {
+    std::mutex mu;
+    int exp_bit = 4;           // pg5_table.h:7-8 (EXP_BIT 4, FRC_BIT 5 -> 512 entries)
+    int frc_bit = -1;          // -1: PGB_G5T_FRC_BIT or 5
+    std::vector<float> tab;    // [size][2] (f, df/ds)
+    double xscale = 0.0;       // pg5_set_xscale (phantom_g5.c:43-50)
+    bool built = false;
+    int version = 0;
+    DevBuf<float2> dev;
+    int dev_version = -1;
+};
+TableState g_tab;
+
+inline int tab_frc() {
+    if (g_tab.frc_bit < 0) g_tab.frc_bit = env_int("PGB_G5T_FRC_BIT", 5, 1, 8);
+    return g_tab.frc_bit;
+}
+inline int tab_size() { return 1 << (g_tab.exp_bit + tab_frc()); }
+
+inline float bits_float(uint32_t u) {
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+inline uint32_t float_bits(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    return u;
+}
+
+// Table generation in the reference's float arithmetic (bit-identical tables).
+void gen_table_locked(double (*force_func)(double), double rcut) {
+    const int frc = tab_frc(), tbl = tab_size();
+    const uint32_t tick = 1u << (23 - frc);
+    const float r2max = (float)(rcut * rcut);
+    const float fmax = (float)((double)(1 << (1 << g_tab.exp_bit)) * (2.0 - 1.0 / (1 << frc)));
+    const float r2scale = (fmax - 2.0f) / r2max;
+    g_tab.tab.assign((size_t)tbl * 2, 0.f);
+    uint32_t u = float_bits(2.0f);
+    for (int i = 0; i < tbl; i++, u += tick) {
+        float f = bits_float(u);
+        float r2 = (float)(((double)f - 2.0) / (double)r2scale);
+        float r = sqrtf(r2);
+        g_tab.tab[2 * i] = (float)force_func((double)r);
+    }
+    u = float_bits(2.0f);
+    int i;
+    for (i = 0; i < tbl - 1; i++) {
+        float x0 = bits_float(u);
+        u += tick;
+        float x1 = bits_float(u);
+        float y0 = g_tab.tab[2 * i], y1 = g_tab.tab[2 * (i + 1)];
+        g_tab.tab[2 * i + 1] = (y1 - y0) / (x1 - x0);
+    }
+    g_tab.tab[2 * i + 1] = 0.0f;
+    g_tab.xscale = (double)sqrtf(r2scale);
+    g_tab.built = true;
+    g_tab.version++;
+}
+
+// S2 softening-difference shape, the table g5_open builds (pg5_table.c:8-35).
+double reff(double sft, double r) {
+    double eta = 2.0 * r / sft;
+    if (eta < 1.0)
+        return (224. + eta * eta * (-224. + eta * (70. + eta * (48. - eta * 21.)))) * 2.0 / (35.0 * std::pow(sft, 3));
+    if (eta < 2.0)
+        return (12. / (eta * eta) - 224. +
+                eta * (896. + eta * (-840. + eta * (224. + eta * (70. + eta * (-48. + eta * 7.)))))) *
+               2.0 / (35.0 * eta * std::pow(sft, 3));
+    return 1.0 / std::pow(r, 3);
+}
+double g_sft_pp = 0.1 / 64, g_sft_pm = 3.0 / 64;  // pppm.h:4-6
+double s2_force(double r) { return reff(g_sft_pp, r) - reff(g_sft_pm, r); }
+
+void ensure_table_locked() {
+    if (!g_tab.built) {
+        g_sft_pp = 0.1 / 64;
+        g_sft_pm = 3.0 / 64;
+        gen_table_locked(s2_force, g_sft_pm);
+    }
+}
+
+bool table_args(G5Args& a) {
+    std::lock_guard<std::mutex> g(g_tab.mu);
+    ensure_table_locked();
+    const int tbl = tab_size(), frc = tab_frc();
+    if (tbl > G5_TBL_MAX) {
+        raise(g_err, LIB, PGB_ERR_CAPACITY, "table of %d entries > %d", tbl, G5_TBL_MAX);
+        return false;
+    }
+    if (g_tab.dev_version != g_tab.version) {
+        PGB_CUDA_OR(g_err, LIB, g_tab.dev.reserve(tbl), return false);
+        PGB_CUDA_OR(g_err, LIB, cudaMemcpy(g_tab.dev.p, g_tab.tab.data(), (size_t)tbl * sizeof(float2),
+                                           cudaMemcpyHostToDevice), return false);
+        g_tab.dev_version = g_tab.version;
+    }
+    a.table = g_tab.dev.p;
+    a.tbl_size = tbl;
+    a.tbl_shift = 23 - frc;
+    a.r2cut = bits_float((1u << 30) | ((uint32_t)(tbl - 1) << (23 - frc)));
+    a.ascale = 1.0 / g_tab.xscale;
+    return true;
+}
+
+// i and j coordinates of the table kind are pre-scaled by xscale: j in float arithmetic
+// (phantom_g5.c:112-128: cvtpd2ps then * (float)xscale), i through double
+// (phantom_g5.c:96-104: (float)x * Xscale rounded to float).
+inline float scale_j(double x) {
+    return (float)x * (float)g_tab.xscale;
+}
+inline float scale_i(double x) {
+    return (float)((double)(float)x * g_tab.xscale);
 }
 
 // Staged work list + launch of one devid / plan.
@@ -152,6 +274,12 @@ struct Launcher {
         a.partial = st.dpart.p;
         a.out = out;
         a.itile = ITILE;
+        a.table = nullptr;
+        a.tbl_size = 0;
+        a.tbl_shift = 0;
+        a.r2cut = 0.f;
+        a.ascale = 1.0;
+        if (kind == G5_TABLE && !table_args(a)) return false;
         int slots = sm_count(g_device) * occupancy_of(kind);
         int grid = st.ntasks < slots ? st.ntasks : slots;
         PGB_CUDA_OR(g_err, LIB, launch_kind(kind, grid, a, s), return false);
@@ -319,8 +447,33 @@ void write_out(const double4* o, int ni, double (*a)[3], double* p) {
         a[i][0] = o[i].x;
         a[i][1] = o[i].y;
         a[i][2] = o[i].z;
+#ifdef PGB_TABLE
+        p[i] = 0.0;      // the table kernel computes no potential (PG5/table phantom_g5.c:145-154)
+#else
         p[i] = -o[i].w;  // GRAPE-5 return sign (phantom_g5.c:251-259)
+#endif
     }
+}
+
+// The current xscale of the table library (building the default table on first use, as
+// g5_open does); 0 for the other builds, which do not scale.
+double current_xscale() {
+#ifdef PGB_TABLE
+    std::lock_guard<std::mutex> g(g_tab.mu);
+    ensure_table_locked();
+    return g_tab.xscale;
+#else
+    return 0.0;
+#endif
+}
+
+inline float4 make_i(const double* x, float e2) {
+#ifdef PGB_TABLE
+    (void)e2;
+    return make_float4(scale_i(x[0]), scale_i(x[1]), scale_i(x[2]), 0.f);
+#else
+    return make_float4((float)x[0], (float)x[1], (float)x[2], e2);
+#endif
 }
 
 bool check_ni(int ni) {
@@ -335,10 +488,10 @@ void set_xi_impl(int devid, int ni, const double (*xi)[3], const double* eps2, b
     if (!check_ni(ni)) return;
     Dev* d = get_dev(devid);
     if (!d) return;
+    current_xscale();
     std::lock_guard<std::mutex> g(d->mu);
     float e_all = (float)(g_eps * g_eps);
-    for (int i = 0; i < ni; i++)
-        d->ip[i] = make_float4((float)xi[i][0], (float)xi[i][1], (float)xi[i][2], per_i ? (float)eps2[i] : e_all);
+    for (int i = 0; i < ni; i++) d->ip[i] = make_i(xi[i], per_i ? (float)eps2[i] : e_all);
 }
 
 void run_impl(int devid, int kind) {
@@ -369,6 +522,7 @@ void get_force_impl(int devid, int ni, double (*a)[3], double* p) {
 // All ni in one launch (the reference loops over npipes-wide calls, phantom_g5.c:276-300).
 void calc_impl(int devid, int kind, const double (*x)[3], const double* eps2, double (*a)[3], double* p, int ni) {
     if (ni <= 0) return;
+    current_xscale();
     Dev* d = get_dev(devid);
     if (!d) return;
     Dev* dj = d;
@@ -379,8 +533,7 @@ void calc_impl(int devid, int kind, const double (*x)[3], const double* eps2, do
         return;
     }
     float e_all = (float)(g_eps * g_eps);
-    for (int i = 0; i < ni; i++)
-        dj->ibuf.p[i] = make_float4((float)x[i][0], (float)x[i][1], (float)x[i][2], eps2 ? (float)eps2[i] : e_all);
+    for (int i = 0; i < ni; i++) dj->ibuf.p[i] = make_i(x[i], eps2 ? (float)eps2[i] : e_all);
     if (!compute(*dj, kind, ni, dj->ibuf.p) || !sync_dev(*dj)) return;
     write_out(dj->outh.p, ni, a, p);
 }
@@ -393,7 +546,16 @@ void calc_impl(int devid, int kind, const double (*x)[3], const double* eps2, do
 PGB_EXPORT int g5_get_number_of_pipelines(void) { return npipes(); }
 PGB_EXPORT int g5_get_jmemsize(void) { return jmemsize(); }
 
-PGB_EXPORT void g5_open(void) { ensure_device(); }
+#ifdef PGB_TABLE
+extern "C" void pg5_gen_s2_force_table(double sft_for_PP, double sft_for_PM);
+#endif
+
+PGB_EXPORT void g5_open(void) {
+    ensure_device();
+#ifdef PGB_TABLE
+    pg5_gen_s2_force_table(0.1 / 64, 3.0 / 64);  // g5_open builds the S2 table (phantom_g5.c:56-61)
+#endif
+}
 
 PGB_EXPORT void g5_close(void) {
     if (g_device < 0) return;
@@ -456,12 +618,17 @@ PGB_EXPORT void g5_set_xmjMC(int devid, int adr, int nj, double (*xj)[3], double
         raise(g_err, LIB, PGB_ERR_ARG, "g5_set_xmj: adr %d nj %d", adr, nj);
         return;
     }
+    current_xscale();
     Dev* d = get_dev(devid);
     if (!d) return;
     std::lock_guard<std::mutex> g(d->mu);
     if (!quiesce(*d) || !grow_j(*d, adr + nj)) return;
     for (int j = adr; j < adr + nj; j++) {
+#ifdef PGB_TABLE
+        d->jh.p[j] = make_float4(scale_j(xj[j][0]), scale_j(xj[j][1]), scale_j(xj[j][2]), (float)mj[j]);
+#else
         d->jh.p[j] = make_float4((float)xj[j][0], (float)xj[j][1], (float)xj[j][2], (float)mj[j]);
+#endif
 #ifdef PGB_SYMMETRIC
         d->jeh.p[j] = make_float4((float)epsj2[j], 0, 0, 0);
 #endif
@@ -500,6 +667,85 @@ PGB_EXPORT void g5_calculate_force_on_xe(double (*x)[3], double* eps2, double (*
     g5_calculate_force_on_xeMC(0, x, eps2, a, p, ni);
 }
 
+#ifdef PGB_TABLE
+// ============================================================================================
+// Table (cutoff-force) API (PG5/table/libpg5/gp5util.h:9-35, pg5_table.h:38-40)
+
+extern "C" {
+// The reference exports its table as a global (pg5_table.h:31); this copy mirrors the current
+// table (first 2^(EXP_BIT+FRC_BIT) rows) after every table generation.
+__attribute__((visibility("default"))) float Force_table[G5_TBL_MAX][2];
+}
+
+namespace {
+void mirror_table_locked() {
+    int n = tab_size() < G5_TBL_MAX ? tab_size() : G5_TBL_MAX;
+    std::memcpy(Force_table, g_tab.tab.data(), (size_t)n * 2 * sizeof(float));
+}
+}  // namespace
+
+PGB_EXPORT void pg5_set_xscale(double xscale) {
+    std::lock_guard<std::mutex> g(g_tab.mu);
+    g_tab.xscale = xscale;  // phantom_g5.c:43-50
+}
+
+// f(r) is the force shape divided by r (an r^-3-like function); rcut the cutoff radius.
+PGB_EXPORT void pg5_gen_force_table(double (*force_func)(double), double rcut) {
+    if (!force_func || !(rcut > 0)) {
+        raise(g_err, LIB, PGB_ERR_ARG, "pg5_gen_force_table: null function or rcut <= 0");
+        return;
+    }
+    std::lock_guard<std::mutex> g(g_tab.mu);
+    gen_table_locked(force_func, rcut);
+    mirror_table_locked();
+}
+
+PGB_EXPORT void pg5_gen_s2_force_table(double sft_for_PP, double sft_for_PM) {
+    std::lock_guard<std::mutex> g(g_tab.mu);
+    g_sft_pp = sft_for_PP;
+    g_sft_pm = sft_for_PM;
+    gen_table_locked(s2_force, sft_for_PM);
+    mirror_table_locked();
+}
+
+// Table resolution: 2^(exp_bit + frc_bit) entries (the reference fixes EXP_BIT 4, FRC_BIT 5 at
+// compile time, pg5_table.h:7-17).  Takes effect at the next table generation.
+PGB_EXPORT int pg5_set_table_bits(int exp_bit, int frc_bit) {
+    if (exp_bit != 4 || frc_bit < 1 || frc_bit > 8) {
+        raise(g_err, LIB, PGB_ERR_ARG, "pg5_set_table_bits(%d, %d): EXP_BIT must be 4, FRC_BIT 1..8", exp_bit, frc_bit);
+        return PGB_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> g(g_tab.mu);
+    g_tab.exp_bit = exp_bit;
+    g_tab.frc_bit = frc_bit;
+    g_tab.built = false;
+    return PGB_OK;
+}
+
+// Copy of the current table: returns the number of entries, writes min(n, max_entries) rows.
+PGB_EXPORT int pg5_get_table(float* out, int max_entries, double* xscale) {
+    std::lock_guard<std::mutex> g(g_tab.mu);
+    ensure_table_locked();
+    int n = tab_size();
+    if (out) std::memcpy(out, g_tab.tab.data(), (size_t)(n < max_entries ? n : max_entries) * 2 * sizeof(float));
+    if (xscale) *xscale = g_tab.xscale;
+    return n;
+}
+
+PGB_EXPORT void g5_set_range(double xmin, double xmax, double mmin) {
+    (void)xmin; (void)xmax; (void)mmin;  // no-op, as phantom_g5.c:77-78
+}
+PGB_EXPORT void g5_set_eta(double eta) { (void)eta; }
+
+// The reference leaves this a stub (phantom_g5.c:80-84, "please implement"): here it installs
+// ffunc as the force shape with cutoff fcut (the table kernel has no potential, so pfunc,
+// pcut and the corrections are ignored).
+PGB_EXPORT void g5_set_cutoff_table(double (*ffunc)(double), double fcut, double fcor, double (*pfunc)(double),
+                                    double pcut, double pcor) {
+    (void)fcor; (void)pfunc; (void)pcut; (void)pcor;
+    if (ffunc) pg5_gen_force_table(ffunc, fcut);
+}
+#else
 // ============================================================================================
 // Quadrupole j-cells (PG5/newton_quad/quad/quad_util.h:8-15)
 
@@ -596,6 +842,8 @@ PGB_EXPORT void g5_calculate_force_on_xeMC_(int* devid, double (*x)[3], double* 
     g5_calculate_force_on_xeMC(*devid, x, eps2, a, p, *ni);
 }
 
+#endif  // PGB_TABLE
+
 // ============================================================================================
 // Library status and the batched path (no reference counterpart; see include/pgb_g5.h)
 
@@ -628,7 +876,11 @@ struct pgb5_plan {
 
 namespace {
 bool check_kind(int kind) {
+#ifdef PGB_TABLE
+    if (kind != G5_TABLE) {
+#else
     if (kind != G5_NEWTON && kind != G5_SYMMETRIC && kind != G5_QUAD) {
+#endif
         raise(g_err, LIB, PGB_ERR_ARG, "unknown kind %d", kind);
         return false;
     }
@@ -695,7 +947,7 @@ PGB_EXPORT int pgb5_plan_launch(pgb5_plan* P, const void* ipos, const void* jpos
     if (!P) return PGB_ERR_ARG;
     if (!ensure_device()) return PGB_ERR_NOGPU;
     cudaStream_t s = (cudaStream_t)stream;
-    if (!ipos || !jpos || !out || (P->kind != G5_NEWTON && !jaux)) {
+    if (!ipos || !jpos || !out || ((P->kind == G5_SYMMETRIC || P->kind == G5_QUAD) && !jaux)) {
         raise(g_err, LIB, PGB_ERR_ARG, "pgb5_plan_launch: null device pointer");
         return PGB_ERR_ARG;
     }

@@ -32,13 +32,41 @@ struct G5Args {
     double4* partial;       // [rows][itile]
     double4* out;           // [.] (ax, ay, az, pot_raw) per i, indexed by absolute i
     int itile;              // NT*IPT
+    // table kind only: force-shape table (f, df/ds) in s = 2 + |dx'|^2, 2^(EXP+FRC) entries
+    const float2* table;
+    int tbl_size;
+    int tbl_shift;          // 23 - FRC_BIT
+    float r2cut;            // float with bits (1<<30) | ((tbl_size-1) << tbl_shift)
+    double ascale;          // 1 / xscale
 };
 
 // kinds
-enum { G5_NEWTON = 0, G5_SYMMETRIC = 1, G5_QUAD = 2 };
+enum { G5_NEWTON = 0, G5_SYMMETRIC = 1, G5_QUAD = 2, G5_TABLE = 3 };
+constexpr int G5_TBL_MAX = 4096;   // largest table held in shared memory (32 KB)
 
 template <int KIND>
-struct JWords { static constexpr int n = (KIND == G5_NEWTON) ? 1 : (KIND == G5_SYMMETRIC ? 2 : 3); };
+struct JWords { static constexpr int n = (KIND == G5_SYMMETRIC) ? 2 : (KIND == G5_QUAD ? 3 : 1); };
+
+// Table lookup of the cutoff force (PG5/table/libpg5/gravity_kernel_avx2.c:70-124):
+// s = min(2 + |dx'|^2, r2cut); the table bin is the float bit pattern of s shifted right by
+// 23-FRC_BIT (the exponent and FRC_BIT leading mantissa bits); the bin's node is s with its
+// low bits cleared; f = T[bin].x + (s - node) T[bin].y.  `tab` is pre-offset by the bin of 2.0
+// so that it can be indexed by the shifted bits directly.  s >= 2 and the clamp (fminf returns
+// r2cut for a NaN s) keep every index inside the table.
+__device__ __forceinline__ void g5_table_pair(float4 J, float xi, float yi, float zi, const float2* tab,
+                                              int shift, float r2cut, float (&a)[4]) {
+    float dx = J.x - xi, dy = J.y - yi, dz = J.z - zi;
+    float s = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmaf_rn(dx, dx, 2.0f)));
+    s = fminf(s, r2cut);
+    unsigned u = __float_as_uint(s);
+    float node = __uint_as_float((u >> shift) << shift);
+    float2 T = tab[u >> shift];
+    float f = __fmaf_rn(s - node, T.y, T.x);
+    float mf = J.w * f;
+    a[0] = __fmaf_rn(mf, dx, a[0]);
+    a[1] = __fmaf_rn(mf, dy, a[1]);
+    a[2] = __fmaf_rn(mf, dz, a[2]);
+}
 
 template <int KIND, int NT>
 __device__ __forceinline__ void g5_interact(const float4* sj, int j, float xi, float yi, float zi,
@@ -82,8 +110,10 @@ __device__ __forceinline__ void g5_interact(const float4* sj, int j, float xi, f
 
 // Final scaling of the FP64 sums into (acc, pot_raw).
 template <int KIND>
-__device__ __forceinline__ double4 g5_finish(double4 s) {
+__device__ __forceinline__ double4 g5_finish(double4 s, double ascale) {
     if constexpr (KIND == G5_QUAD) return s;  // quad sums are already (acc, +sum(phi_p+phi_q))
+    if constexpr (KIND == G5_TABLE)           // acc *= 1/xscale (gravity_kernel_avx2.c:127-129)
+        return make_double4(ascale * s.x, ascale * s.y, ascale * s.z, 0.0);
     return make_double4(-0.125 * s.x, -0.125 * s.y, -0.125 * s.z, 0.5 * s.w);
 }
 
@@ -96,6 +126,16 @@ __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
     constexpr int W = JWords<KIND>::n;   // 16-byte words per j record
     __shared__ float4 sj[NT * W];
     __shared__ int s_task, s_flag;
+    // table kind: the whole force table in shared memory for the lifetime of the CTA
+    __shared__ float2 stab[KIND == G5_TABLE ? G5_TBL_MAX : 1];
+    const float2* tab = stab;
+    int shift = 0;
+    if constexpr (KIND == G5_TABLE) {
+        for (int k = threadIdx.x; k < A.tbl_size; k += NT) stab[k] = A.table[k];
+        shift = A.tbl_shift;
+        tab = stab - (0x40000000u >> shift);  // index by (bits of s) >> shift directly
+        // (visibility of stab is ensured by the __syncthreads in next_task)
+    }
 
     for (;;) {
         int t = next_task(A.task_counter, &s_task);
@@ -131,8 +171,14 @@ __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
             for (int k = 0; k < IPT; k++) a[k][0] = a[k][1] = a[k][2] = a[k][3] = 0.f;
 #pragma unroll 4
             for (int j = 0; j < nt; j++) {
+                if constexpr (KIND == G5_TABLE) {
+                    const float4 J = sj[j];
 #pragma unroll
-                for (int k = 0; k < IPT; k++) g5_interact<KIND, NT>(sj, j, xi[k], yi[k], zi[k], ei[k], a[k]);
+                    for (int k = 0; k < IPT; k++) g5_table_pair(J, xi[k], yi[k], zi[k], tab, shift, A.r2cut, a[k]);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < IPT; k++) g5_interact<KIND, NT>(sj, j, xi[k], yi[k], zi[k], ei[k], a[k]);
+                }
             }
 #pragma unroll
             for (int k = 0; k < IPT; k++) {
@@ -148,7 +194,7 @@ __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
             for (int k = 0; k < IPT; k++) {
                 int li = threadIdx.x + k * NT;
                 if (li < T.ni)
-                    A.out[T.i0 + li] = g5_finish<KIND>(make_double4(S[k][0], S[k][1], S[k][2], S[k][3]));
+                    A.out[T.i0 + li] = g5_finish<KIND>(make_double4(S[k][0], S[k][1], S[k][2], S[k][3]), A.ascale);
             }
             continue;
         }
@@ -171,7 +217,7 @@ __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
                     v.x = __ldcg(&r->x); v.y = __ldcg(&r->y); v.z = __ldcg(&r->z); v.w = __ldcg(&r->w);
                     s = add4(s, v);
                 }
-                A.out[G.i0 + li] = g5_finish<KIND>(s);
+                A.out[G.i0 + li] = g5_finish<KIND>(s, A.ascale);
             }
         }
     }

@@ -549,3 +549,225 @@ PGB_EXPORT int g6_get_neighbour_list_(int* gpid, int* ipipe, int* maxlen, int* n
 PGB_EXPORT void g6_debugfunc_(int* v) { g6_debugfunc(*v); }
 PGB_EXPORT void g6_debugfunc_double_(double* v) { g6_debugfunc_double(*v); }
 PGB_EXPORT void g6_dump_(double* tim, int* n, double* m, double (*x)[3], double (*v)[3]) { g6_dump(*tim, *n, m, x, v); }
+
+// ============================================================================================
+// Library status and the batched path (no reference counterpart; declared in include/pgb_g6.h)
+
+PGB_EXPORT int pgb6_last_error(char* buf, int len) {
+    std::lock_guard<std::mutex> g(g_err.mu);
+    if (buf && len > 0) {
+        std::strncpy(buf, g_err.msg.c_str(), (size_t)len - 1);
+        buf[len - 1] = 0;
+    }
+    return g_err.code;
+}
+PGB_EXPORT void pgb6_clear_error(void) {
+    std::lock_guard<std::mutex> g(g_err.mu);
+    g_err.code = 0;
+    g_err.msg.clear();
+}
+PGB_EXPORT void pgb6_set_abort(int on) {
+    std::lock_guard<std::mutex> g(g_err.mu);
+    g_err.abort_on_error = on ? 1 : 0;
+}
+
+// Sizes of the device record types, so callers can lay out device buffers:
+// G6Ptcl (j-memory), G6PredJ (predicted j), G6I (i-particle), G6Out (result).
+PGB_EXPORT void pgb6_record_sizes(int* ptcl, int* predj, int* irec, int* out) {
+    if (ptcl) *ptcl = (int)sizeof(G6Ptcl);
+    if (predj) *predj = (int)sizeof(G6PredJ);
+    if (irec) *irec = (int)sizeof(G6I);
+    if (out) *out = (int)sizeof(G6Out);
+}
+
+struct pgb6_plan {
+    int cfg;
+    bool nn;
+    std::vector<Task> tasks;
+    std::vector<Group> groups;
+    int rows = 0;
+    long long interactions = 0;
+    Stager<G6I, G6Out> st;
+};
+
+enum { PGB6_NN = 1 };
+
+// items: [nitem][4] = (i_offset, i_count, j_offset, j_count) into the i- and j-arrays.
+// flags: PGB6_NN (1) also computes the nearest neighbour (key, j address).
+PGB_EXPORT int pgb6_plan_create(pgb6_plan** out, int nitem, const int* items, int flags) {
+    if (!out || nitem < 0 || (nitem && !items)) {
+        raise(g_err, LIB, PGB_ERR_ARG, "pgb6_plan_create: bad arguments");
+        return PGB_ERR_ARG;
+    }
+    for (int k = 0; k < nitem; k++)
+        if (items[4 * k] < 0 || items[4 * k + 1] < 0 || items[4 * k + 2] < 0 || items[4 * k + 3] < 0) {
+            raise(g_err, LIB, PGB_ERR_ARG, "pgb6_plan_create: item %d has a negative offset or count", k);
+            return PGB_ERR_ARG;
+        }
+    if (!ensure_device()) return PGB_ERR_NOGPU;
+    auto* P = new pgb6_plan();
+    P->nn = (flags & PGB6_NN) != 0;
+    long long nimax = 0;
+    for (int k = 0; k < nitem; k++) nimax = std::max<long long>(nimax, items[4 * k + 1]);
+    // many small items fill the GPU with short tiles; large ones prefer 2 i per thread
+    long long total_i = 0;
+    for (int k = 0; k < nitem; k++) total_i += items[4 * k + 1];
+    P->cfg = pick_cfg(nitem > 1 ? std::max<long long>(nimax, total_i / 4) : nimax);
+    P->interactions = plan_items(P->tasks, P->groups, P->rows, nitem, items, P->cfg, P->nn, false);
+    cudaStream_t s = nullptr;
+    bool ok = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess;
+    ok = ok && P->st.stage(s, P->tasks, P->groups, P->rows, ITILE_MAX, (const G6I*)nullptr, 0) == cudaSuccess;
+    ok = ok && cudaStreamSynchronize(s) == cudaSuccess;
+    if (s) cudaStreamDestroy(s);
+    if (!ok) {
+        P->st.release();
+        delete P;
+        raise(g_err, LIB, PGB_ERR_CUDA, "pgb6_plan_create: staging failed");
+        return PGB_ERR_CUDA;
+    }
+    *out = P;
+    return PGB_OK;
+}
+
+PGB_EXPORT long long pgb6_plan_interactions(const pgb6_plan* P) { return P ? P->interactions : 0; }
+PGB_EXPORT int pgb6_plan_tasks(const pgb6_plan* P) { return P ? (int)P->tasks.size() : 0; }
+PGB_EXPORT int pgb6_plan_config(const pgb6_plan* P) { return P ? P->cfg : -1; }
+
+// Device-resident launch (capturable in a CUDA graph): ipart = G6I[], jpred = G6PredJ[],
+// out = G6Out[] indexed by absolute i (acc, jerk, pot final; key = -2/r_soft of the nearest
+// neighbour, jadr = its j address, when the plan has PGB6_NN).
+PGB_EXPORT int pgb6_plan_launch(pgb6_plan* P, const void* ipart, const void* jpred, double eps2, void* out,
+                                void* stream) {
+    if (!P || !ipart || !jpred || !out) {
+        raise(g_err, LIB, PGB_ERR_ARG, "pgb6_plan_launch: null argument");
+        return PGB_ERR_ARG;
+    }
+    if (!ensure_device()) return PGB_ERR_NOGPU;
+    if (P->st.ntasks == 0) return PGB_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    PGB_CUDA_OR(g_err, LIB, cudaMemsetAsync(P->st.counter(), 0, sizeof(int), s), return PGB_ERR_CUDA);
+    G6Args a;
+    a.ipart = (const G6I*)ipart;
+    a.jpred = (const G6PredJ*)jpred;
+    a.eps2 = (float)eps2;
+    a.tasks = P->st.tasks();
+    a.ntasks = P->st.ntasks;
+    a.task_counter = P->st.counter();
+    a.groups = P->st.groups();
+    a.group_counters = P->st.dgcnt.p;
+    a.partial = P->st.dpart.p;
+    a.out = (G6Out*)out;
+    a.itile = cfg_itile(P->cfg);
+    a.nb_count = nullptr;
+    a.nb_list = nullptr;
+    a.nb_maxlen = 0;
+    int slots = sm_count(g_device) * occupancy(P->cfg, P->nn, false);
+    int grid = a.ntasks < slots ? a.ntasks : slots;
+    PGB_CUDA_OR(g_err, LIB, launch_kernel(P->cfg, P->nn, false, grid, a, s), return PGB_ERR_CUDA);
+    return PGB_OK;
+}
+
+PGB_EXPORT void pgb6_plan_destroy(pgb6_plan* P) {
+    if (!P) return;
+    if (g_device >= 0) cudaSetDevice(g_device);
+    P->st.release();
+    delete P;
+}
+
+// FP64 predictor on device records: pred[j] = predict(ptcl[j], ti) for j < nj.
+PGB_EXPORT int pgb6_predict(const void* ptcl, int nj, double ti, void* pred, void* stream) {
+    if (nj < 0 || (nj > 0 && (!ptcl || !pred))) {
+        raise(g_err, LIB, PGB_ERR_ARG, "pgb6_predict: bad arguments");
+        return PGB_ERR_ARG;
+    }
+    if (!ensure_device()) return PGB_ERR_NOGPU;
+    if (nj == 0) return PGB_OK;
+    g6_predict_kernel<<<(nj + 255) / 256, 256, 0, (cudaStream_t)stream>>>((const G6Ptcl*)ptcl, nj, ti, (G6PredJ*)pred);
+    PGB_CUDA_OR(g_err, LIB, cudaGetLastError(), return PGB_ERR_CUDA);
+    return PGB_OK;
+}
+
+namespace {
+struct HostBatch {
+    std::mutex mu;
+    cudaStream_t s = nullptr;
+    HostBuf<G6I> ih;
+    HostBuf<G6PredJ> jh;
+    HostBuf<G6Out> oh;
+    DevBuf<G6I> id;
+    DevBuf<G6PredJ> jd;
+    DevBuf<G6Out> od;
+};
+HostBatch HB;
+}  // namespace
+
+// Host-buffer batch: the whole list of items in one launch, inputs and outputs in host memory
+// (copies included).  Positions FP64; velocities, masses rounded to float as the GRAPE-6 path
+// does.  nnb / rnnb may be NULL.
+PGB_EXPORT int pgb6_batch_host(int nitem, const int* items, int ni, const double (*xi)[3], const double (*vi)[3],
+                               const int* idi, int nj, const double (*xj)[3], const double (*vj)[3], const double* mj,
+                               const int* idj, double eps2, double (*acc)[3], double (*jrk)[3], double* pot, int* nnb,
+                               float* rnnb) {
+    if (ni < 0 || nj < 0) {
+        raise(g_err, LIB, PGB_ERR_ARG, "pgb6_batch_host: negative sizes");
+        return PGB_ERR_ARG;
+    }
+    for (int k = 0; k < nitem; k++) {
+        const int* it = items + 4 * k;
+        if (it[0] < 0 || it[1] < 0 || it[2] < 0 || it[3] < 0 || it[0] + it[1] > ni || it[2] + it[3] > nj) {
+            raise(g_err, LIB, PGB_ERR_ARG, "pgb6_batch_host: item %d outside the arrays", k);
+            return PGB_ERR_ARG;
+        }
+    }
+    if (!ensure_device()) return PGB_ERR_NOGPU;
+    std::lock_guard<std::mutex> g(HB.mu);
+    if (!HB.s) PGB_CUDA_OR(g_err, LIB, cudaStreamCreateWithFlags(&HB.s, cudaStreamNonBlocking), return PGB_ERR_CUDA);
+    PGB_CUDA_OR(g_err, LIB, HB.ih.reserve(ni + 1), return PGB_ERR_CUDA);
+    PGB_CUDA_OR(g_err, LIB, HB.jh.reserve(nj + 1), return PGB_ERR_CUDA);
+    PGB_CUDA_OR(g_err, LIB, HB.oh.reserve(ni + 1), return PGB_ERR_CUDA);
+    PGB_CUDA_OR(g_err, LIB, HB.id.reserve(ni + 1), return PGB_ERR_CUDA);
+    PGB_CUDA_OR(g_err, LIB, HB.jd.reserve(nj + 1), return PGB_ERR_CUDA);
+    PGB_CUDA_OR(g_err, LIB, HB.od.reserve(ni + 1), return PGB_ERR_CUDA);
+    for (int i = 0; i < ni; i++) {
+        G6I& r = HB.ih.p[i];
+        r.x = xi[i][0]; r.y = xi[i][1]; r.z = xi[i][2];
+        r.vx = (float)vi[i][0]; r.vy = (float)vi[i][1]; r.vz = (float)vi[i][2];
+        r.id = idi[i];
+        r.h2 = 0.f;
+        r.pad = 0.f;
+    }
+    for (int j = 0; j < nj; j++) {
+        G6PredJ& r = HB.jh.p[j];
+        r.x = xj[j][0]; r.y = xj[j][1]; r.z = xj[j][2];
+        r.vx = (float)vj[j][0]; r.vy = (float)vj[j][1]; r.vz = (float)vj[j][2];
+        r.m = (float)mj[j];
+        r.id = idj[j];
+        r.pad = 0.f;
+    }
+    PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(HB.id.p, HB.ih.p, (size_t)ni * sizeof(G6I), cudaMemcpyHostToDevice, HB.s),
+                return PGB_ERR_CUDA);
+    PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(HB.jd.p, HB.jh.p, (size_t)nj * sizeof(G6PredJ), cudaMemcpyHostToDevice, HB.s),
+                return PGB_ERR_CUDA);
+    pgb6_plan* P = nullptr;
+    int rc = pgb6_plan_create(&P, nitem, items, (nnb || rnnb) ? PGB6_NN : 0);
+    if (rc) return rc;
+    rc = pgb6_plan_launch(P, HB.id.p, HB.jd.p, eps2, HB.od.p, HB.s);
+    if (!rc && ni > 0)
+        PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(HB.oh.p, HB.od.p, (size_t)ni * sizeof(G6Out), cudaMemcpyDeviceToHost, HB.s),
+                    rc = PGB_ERR_CUDA);
+    if (!rc) PGB_CUDA_OR(g_err, LIB, cudaStreamSynchronize(HB.s), rc = PGB_ERR_CUDA);
+    pgb6_plan_destroy(P);
+    if (rc) return rc;
+    // outputs only for i covered by an item
+    for (int k = 0; k < nitem; k++) {
+        for (int i = items[4 * k]; i < items[4 * k] + items[4 * k + 1]; i++) {
+            const G6Out& o = HB.oh.p[i];
+            acc[i][0] = o.ax; acc[i][1] = o.ay; acc[i][2] = o.az;
+            jrk[i][0] = o.jx; jrk[i][1] = o.jy; jrk[i][2] = o.jz;
+            pot[i] = o.pot;
+            if (nnb) nnb[i] = (o.jadr >= 0 && o.jadr < nj) ? idj[o.jadr] : -1;
+            if (rnnb) rnnb[i] = -2.0f / o.key;
+        }
+    }
+    return PGB_OK;
+}

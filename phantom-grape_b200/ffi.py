@@ -193,3 +193,229 @@ class G5(_ErrMixin):
 class G5Sym(G5):
     LIBNAME = "libpg5sym.so"
     SYMMETRIC = True
+
+
+class G6(_ErrMixin):
+    """GRAPE-6 API (libpg6.so): g6_open ... g6calc_lasthalf2np, plus the batched pgb6_* path."""
+
+    prefix = "pgb6"
+    NN = 1
+
+    def __init__(self):
+        L = self.L = _load("libpg6.so")
+        for n in ("g6_open", "g6_close", "g6_set_tunit", "g6_set_xunit", "g6_reset", "g6_reset_fofpga"):
+            _sig(L, n, [C.c_int])
+        _sig(L, "g6_npipes", [], C.c_int)
+        _sig(L, "g6_setup_njdata", [C.c_int, C.c_int])
+        _sig(L, "g6_set_j_particle", [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                      dp, dp, dp, dp, dp])
+        _sig(L, "g6_set_ti", [C.c_int, C.c_double])
+        _sig(L, "g6calc_firsthalf", [C.c_int, C.c_int, C.c_int, ip, dp, dp, dp, dp, dp, C.c_double, dp])
+        base = [C.c_int, C.c_int, C.c_int, ip, dp, dp, C.c_double, dp, dp, dp, dp]
+        _sig(L, "g6calc_lasthalf", base, C.c_int)
+        _sig(L, "g6calc_lasthalf2", base + [ip], C.c_int)
+        _sig(L, "g6calc_lasthalf2p", base + [ip, fp], C.c_int)
+        _sig(L, "g6calc_lasthalfn", base, C.c_int)
+        _sig(L, "g6calc_lasthalf2n", base + [ip], C.c_int)
+        _sig(L, "g6calc_lasthalf2np", base + [ip, fp], C.c_int)
+        _sig(L, "g6_read_neighbour_list", [C.c_int], C.c_int)
+        _sig(L, "g6_get_neighbour_list", [C.c_int, C.c_int, C.c_int, ip, ip], C.c_int)
+        _sig(L, "pgb6_last_error", [C.c_char_p, C.c_int], C.c_int)
+        _sig(L, "pgb6_clear_error", [])
+        _sig(L, "pgb6_set_abort", [C.c_int])
+        _sig(L, "pgb6_record_sizes", [ip, ip, ip, ip])
+        _sig(L, "pgb6_plan_create", [C.POINTER(vp), C.c_int, ip, C.c_int], C.c_int)
+        _sig(L, "pgb6_plan_launch", [vp, vp, vp, C.c_double, vp, vp], C.c_int)
+        _sig(L, "pgb6_plan_destroy", [vp])
+        _sig(L, "pgb6_plan_interactions", [vp], C.c_longlong)
+        _sig(L, "pgb6_plan_tasks", [vp], C.c_int)
+        _sig(L, "pgb6_plan_config", [vp], C.c_int)
+        _sig(L, "pgb6_predict", [vp, C.c_int, C.c_double, vp, vp], C.c_int)
+        _sig(L, "pgb6_batch_host", [C.c_int, ip, C.c_int, dp, dp, ip, C.c_int, dp, dp, dp, ip, C.c_double,
+                                    dp, dp, dp, ip, fp], C.c_int)
+        sz = [C.c_int() for _ in range(4)]
+        L.pgb6_record_sizes(*[C.byref(s) for s in sz])
+        self.sizes = dict(ptcl=sz[0].value, predj=sz[1].value, irec=sz[2].value, out=sz[3].value)
+
+    # numpy helpers --------------------------------------------------------------------------
+    def set_j(self, pos, vel, acc2, jrk6, mass, tj, idx=None, addr=None):
+        """g6_set_j_particle for every particle (acc2 = acc/2, jrk6 = jerk/6)."""
+        pos, vel, acc2, jrk6 = (f64(a, (-1, 3)) for a in (pos, vel, acc2, jrk6))
+        snp = np.zeros(3)
+        n = len(pos)
+        for j in range(n):
+            a = int(addr[j]) if addr is not None else j
+            self.L.g6_set_j_particle(0, a, int(idx[j]) if idx is not None else j, float(tj[j]), 0.0,
+                                     float(mass[j]), ptr(snp), ptr(jrk6[j]), ptr(acc2[j]), ptr(vel[j]),
+                                     ptr(pos[j]))
+
+    def calc(self, ti, nj, xi, vi, idi, eps2, h2=None, variant="2p", set_ti=True, maxlen=1024):
+        """g6_set_ti + chunked g6calc_firsthalf / g6calc_lasthalf<variant> over all i."""
+        xi, vi = f64(xi, (-1, 3)), f64(vi, (-1, 3))
+        idi = np.ascontiguousarray(idi, np.int32)
+        ni = len(xi)
+        h2 = f64(np.zeros(ni) if h2 is None else np.broadcast_to(h2, (ni,)))
+        acc = np.zeros((ni, 3))
+        jrk = np.zeros((ni, 3))
+        pot = np.zeros(ni)
+        nnb = np.zeros(ni, np.int32)
+        rnnb = np.zeros(ni, np.float32)
+        nbl = {}
+        if set_ti:
+            self.L.g6_set_ti(0, ti)
+        npipe = self.L.g6_npipes()
+        fn = getattr(self.L, "g6calc_lasthalf" + ("" if variant == "plain" else variant))
+        for i0 in range(0, ni, npipe):
+            n = min(npipe, ni - i0)
+            sl = slice(i0, i0 + n)
+            args = [0, nj, n, ptr(idi[sl], C.c_int), ptr(xi[sl]), ptr(vi[sl])]
+            self.L.g6calc_firsthalf(*args, ptr(acc[sl]), ptr(jrk[sl]), ptr(pot[sl]), eps2, ptr(h2[sl]))
+            rest = [eps2, ptr(h2[sl]), ptr(acc[sl]), ptr(jrk[sl]), ptr(pot[sl])]
+            if variant in ("2", "2n"):
+                rest.append(ptr(nnb[sl], C.c_int))
+            if variant in ("2p", "2np"):
+                rest += [ptr(nnb[sl], C.c_int), ptr(rnnb[sl], C.c_float)]
+            fn(*args, *rest)
+            if variant in ("n", "2n", "2np"):
+                err = self.L.g6_read_neighbour_list(0)
+                for ii in range(n):
+                    cnt = C.c_int()
+                    buf = np.zeros(maxlen, np.int32)
+                    rc = self.L.g6_get_neighbour_list(0, ii, maxlen, C.byref(cnt), ptr(buf, C.c_int))
+                    nbl[i0 + ii] = (rc, err, buf[:cnt.value].copy() if rc == 0 else None)
+        return dict(acc=acc, jrk=jrk, pot=pot, nnb=nnb, rnnb=rnnb, nbl=nbl)
+
+    def batch_host(self, items, xi, vi, idi, xj, vj, mj, idj, eps2, nn=True):
+        items = np.ascontiguousarray(items, np.int32).reshape(-1, 4)
+        xi, vi, xj, vj, mj = f64(xi, (-1, 3)), f64(vi, (-1, 3)), f64(xj, (-1, 3)), f64(vj, (-1, 3)), f64(mj)
+        idi = np.ascontiguousarray(idi, np.int32)
+        idj = np.ascontiguousarray(idj, np.int32)
+        ni = len(xi)
+        acc = np.zeros((ni, 3))
+        jrk = np.zeros((ni, 3))
+        pot = np.zeros(ni)
+        nnb = np.zeros(ni, np.int32) if nn else None
+        rnnb = np.zeros(ni, np.float32) if nn else None
+        rc = self.L.pgb6_batch_host(len(items), ptr(items, C.c_int), ni, ptr(xi), ptr(vi), ptr(idi, C.c_int),
+                                    len(xj), ptr(xj), ptr(vj), ptr(mj), ptr(idj, C.c_int), eps2, ptr(acc),
+                                    ptr(jrk), ptr(pot), ptr(nnb, C.c_int), ptr(rnnb, C.c_float))
+        if rc:
+            raise RuntimeError(f"pgb6_batch_host failed: {self.last_error()}")
+        return dict(acc=acc, jrk=jrk, pot=pot, nnb=nnb, rnnb=rnnb)
+
+    def plan_create(self, items, nn=True):
+        items = np.ascontiguousarray(items, dtype=np.int32).reshape(-1, 4)
+        h = vp()
+        rc = self.L.pgb6_plan_create(C.byref(h), len(items), ptr(items, C.c_int), self.NN if nn else 0)
+        if rc:
+            raise RuntimeError(f"pgb6_plan_create failed: {self.last_error()}")
+        return h
+
+    def plan_launch(self, plan, ipart, jpred, eps2, out, stream=0):
+        rc = self.L.pgb6_plan_launch(plan, ipart, jpred, eps2, out, stream)
+        if rc:
+            raise RuntimeError(f"pgb6_plan_launch failed: {self.last_error()}")
+
+    def plan_destroy(self, plan):
+        self.L.pgb6_plan_destroy(plan)
+
+
+# Device record layouts (must match csrc/pgb_g6_kernels.cuh), as numpy structured dtypes.
+G6PTCL = np.dtype([("pos", "<f8", 3), ("vel", "<f8", 3), ("acc2", "<f8", 3), ("jrk6", "<f8", 3),
+                   ("mass", "<f8"), ("tim", "<f8"), ("idx", "<i4"), ("pad", "<i4", 3)])
+G6PREDJ = np.dtype([("x", "<f8"), ("y", "<f8"), ("z", "<f8"), ("m", "<f4"), ("id", "<i4"),
+                    ("vx", "<f4"), ("vy", "<f4"), ("vz", "<f4"), ("pad", "<f4")])
+G6IREC = np.dtype([("x", "<f8"), ("y", "<f8"), ("z", "<f8"), ("vx", "<f4"), ("vy", "<f4"),
+                   ("vz", "<f4"), ("id", "<i4"), ("h2", "<f4"), ("pad", "<f4")])
+G6OUT = np.dtype([("ax", "<f8"), ("ay", "<f8"), ("az", "<f8"), ("jx", "<f8"), ("jy", "<f8"),
+                  ("jz", "<f8"), ("pot", "<f8"), ("key", "<f4"), ("jadr", "<i4")])
+
+
+FORCE_FN = C.CFUNCTYPE(C.c_double, C.c_double)
+
+
+class G5Table(_ErrMixin):
+    """GRAPE-5 table (cutoff force) API, libpg5table.so."""
+
+    TABLE = 3   # kind of the batched path
+
+    def __init__(self):
+        L = self.L = _load("libpg5table.so")
+        _sig(L, "g5_open", [])
+        _sig(L, "g5_close", [])
+        _sig(L, "g5_get_number_of_pipelines", [], C.c_int)
+        _sig(L, "g5_set_range", [C.c_double, C.c_double, C.c_double])
+        _sig(L, "g5_set_eta", [C.c_double])
+        _sig(L, "g5_set_eps_to_all", [C.c_double])
+        _sig(L, "g5_set_n", [C.c_int])
+        _sig(L, "g5_set_nMC", [C.c_int, C.c_int])
+        _sig(L, "g5_set_xmj", [C.c_int, C.c_int, dp, dp])
+        _sig(L, "g5_set_xmjMC", [C.c_int, C.c_int, C.c_int, dp, dp])
+        _sig(L, "g5_set_xi", [C.c_int, dp])
+        _sig(L, "g5_set_xiMC", [C.c_int, C.c_int, dp])
+        _sig(L, "g5_run", [])
+        _sig(L, "g5_runMC", [C.c_int])
+        _sig(L, "g5_get_force", [C.c_int, dp, dp])
+        _sig(L, "g5_get_forceMC", [C.c_int, C.c_int, dp, dp])
+        _sig(L, "g5_calculate_force_on_x", [dp, dp, dp, C.c_int])
+        _sig(L, "g5_calculate_force_on_xMC", [C.c_int, dp, dp, dp, C.c_int])
+        _sig(L, "g5_set_cutoff_table", [C.c_void_p, C.c_double, C.c_double, C.c_void_p, C.c_double, C.c_double])
+        _sig(L, "pg5_gen_force_table", [C.c_void_p, C.c_double])
+        _sig(L, "pg5_gen_s2_force_table", [C.c_double, C.c_double])
+        _sig(L, "pg5_set_xscale", [C.c_double])
+        _sig(L, "pg5_set_table_bits", [C.c_int, C.c_int], C.c_int)
+        _sig(L, "pg5_get_table", [fp, C.c_int, dp], C.c_int)
+        _sig(L, "pgb5_last_error", [C.c_char_p, C.c_int], C.c_int)
+        _sig(L, "pgb5_clear_error", [])
+        _sig(L, "pgb5_set_abort", [C.c_int])
+        _sig(L, "pgb5_plan_create", [C.POINTER(vp), C.c_int, C.c_int, ip], C.c_int)
+        _sig(L, "pgb5_plan_launch", [vp, vp, vp, vp, vp, vp], C.c_int)
+        _sig(L, "pgb5_plan_destroy", [vp])
+        _sig(L, "pgb5_plan_interactions", [vp], C.c_longlong)
+        _sig(L, "pgb5_plan_tasks", [vp], C.c_int)
+        self._cb = None
+
+    def set_table(self, func, rcut, frc_bit=None):
+        if frc_bit is not None:
+            self.L.pg5_set_table_bits(4, frc_bit)
+        self._cb = FORCE_FN(func)  # keep the callback alive
+        self.L.pg5_gen_force_table(C.cast(self._cb, C.c_void_p), rcut)
+
+    def table(self):
+        xs = C.c_double()
+        n = self.L.pg5_get_table(None, 0, C.byref(xs))
+        t = np.zeros((n, 2), np.float32)
+        self.L.pg5_get_table(ptr(t, C.c_float), n, C.byref(xs))
+        return t, xs.value
+
+    def force(self, xj, mj, xi, devid=None):
+        xj, mj, xi = f64(xj, (-1, 3)), f64(mj), f64(xi, (-1, 3))
+        if devid is None:
+            self.L.g5_set_xmj(0, len(xj), ptr(xj), ptr(mj))
+            self.L.g5_set_n(len(xj))
+        else:
+            self.L.g5_set_xmjMC(devid, 0, len(xj), ptr(xj), ptr(mj))
+            self.L.g5_set_nMC(devid, len(xj))
+        a = np.zeros((len(xi), 3))
+        p = np.zeros(len(xi))
+        if devid is None:
+            self.L.g5_calculate_force_on_x(ptr(xi), ptr(a), ptr(p), len(xi))
+        else:
+            self.L.g5_calculate_force_on_xMC(devid, ptr(xi), ptr(a), ptr(p), len(xi))
+        return a, p
+
+    def plan_create(self, items):
+        items = np.ascontiguousarray(items, dtype=np.int32).reshape(-1, 4)
+        h = vp()
+        rc = self.L.pgb5_plan_create(C.byref(h), self.TABLE, len(items), ptr(items, C.c_int))
+        if rc:
+            raise RuntimeError(f"pgb5_plan_create failed: {self.last_error()}")
+        return h
+
+    def plan_launch(self, plan, ipos, jpos, out, stream=0):
+        rc = self.L.pgb5_plan_launch(plan, ipos, jpos, None, out, stream)
+        if rc:
+            raise RuntimeError(f"pgb5_plan_launch failed: {self.last_error()}")
+
+    def plan_destroy(self, plan):
+        self.L.pgb5_plan_destroy(plan)

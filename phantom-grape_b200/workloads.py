@@ -15,8 +15,9 @@ Workloads
                       t_now by 0, 1/2 or 1 of the particle's step).
 * ``hermite_schedule``64 force calls with active sets of 2^k particles, k uniform in 4..16.
 * ``cluster_set``     1024 independent Plummer clusters, N log-uniform in [256, 16384].
-* ``uniform_box_groups`` PG5 table (TreePM PP): N=2^20 uniform periodic box, i-groups from a
-                      128^3 cell mesh, j-lists within r_cut with explicit periodic shifts.
+* ``treepm_groups``  PG5 table (TreePM PP): N=2^20 uniform periodic box, i-groups from a
+                      128^3 cell mesh, j-lists within r_cut with explicit periodic shifts;
+                      ``gaussian_split_force`` is the matching force shape for the table.
 """
 from __future__ import annotations
 
@@ -197,3 +198,112 @@ def cluster_set(ncl: int = 1024, nmin: int = 256, nmax: int = 16384,
         vel[s] = v
         mass[s] = m
     return ClusterSet(offsets=offs, pos=pos, vel=vel, mass=mass, eps2=eps * eps, sizes=sizes)
+
+
+# ------------------------------------------------------------------------------------------
+# PG5 table (TreePM particle-particle part)
+
+def gaussian_split_force(rs: float, rcut: float, eps: float):
+    """Force shape over r of the TreePM short-range part, for pg5_gen_force_table:
+    f(r) = g(r) / (r^2 + eps^2)^(3/2) with g(r) = erfc(r / 2 rs) + r / (sqrt(pi) rs) exp(-r^2 / 4 rs^2),
+    and f = 0 at r >= rcut so that the table's last entry (the clamp value) is zero; the
+    table's last node sits at rcut up to float rounding, hence the 1e-6 relative margin.
+    The Plummer-softened denominator keeps entry 0 (r = 0) finite."""
+    inv_sqrt_pi = 1.0 / math.sqrt(math.pi)
+    rzero = rcut * (1.0 - 1e-6)
+
+    def f(r):
+        if r >= rzero:
+            return 0.0
+        g = math.erfc(r / (2.0 * rs)) + r * inv_sqrt_pi / rs * math.exp(-r * r / (4.0 * rs * rs))
+        return g / (r * r + eps * eps) ** 1.5
+
+    return f
+
+
+@dataclass
+class TreePMSet:
+    x: np.ndarray        # [n,3] particle positions in the unit box (float32-representable)
+    m: np.ndarray        # [n]
+    xi: np.ndarray       # [n,3] i-particles ordered by group
+    order: np.ndarray    # xi = x[order]
+    items: np.ndarray    # [ngroups,4] int32: i_offset, i_count, j_offset, j_count
+    xj: np.ndarray       # [nj_total,3] j-lists, periodic images already shifted
+    mj: np.ndarray       # [nj_total]
+    rs: float
+    rcut: float
+    eps: float
+
+    @property
+    def interactions(self) -> int:
+        return int((self.items[:, 1].astype(np.int64) * self.items[:, 3]).sum())
+
+
+def treepm_groups(n: int = 1 << 20, seed: int = SEED0 + 2, mesh: int = 128, block: int = 8,
+                  nmax: int = 512) -> TreePMSet:
+    """Uniform periodic unit box; i-groups are blocks of block^3 cells of a mesh^3 cell mesh,
+    split into octants while they hold more than nmax particles; each group's j-list holds every
+    particle (or periodic image) within rcut of the group's box.  Candidates come from the 27
+    blocks around the group's block (a block is at least rcut wide)."""
+    rng = Rng(seed)
+    x = rng.uniform(3 * n).reshape(n, 3).astype(np.float32).astype(np.float64)
+    m = np.full(n, 1.0 / n)
+    rs = 1.25 / n ** (1.0 / 3.0)
+    rcut = 4.5 * rs
+    eps = 0.1 / n ** (1.0 / 3.0)
+    nb = mesh // block
+    assert block / mesh >= rcut, "blocks must be at least rcut wide"
+    cell = np.minimum((x * mesh).astype(np.int64), mesh - 1)
+    blk = cell // block
+    bid = (blk[:, 0] * nb + blk[:, 1]) * nb + blk[:, 2]
+    border = np.argsort(bid, kind="stable")
+    bstart = np.searchsorted(bid[border], np.arange(nb ** 3 + 1))
+
+    order, items, xjs, mjs = [], [], [], []
+    ioff = joff = 0
+    for bx in range(nb):
+        for by in range(nb):
+            for bz in range(nb):
+                b = (bx * nb + by) * nb + bz
+                members = border[bstart[b]:bstart[b + 1]]
+                # neighbour candidates with periodic shifts
+                cand, shifts = [], []
+                for ox in (-1, 0, 1):
+                    for oy in (-1, 0, 1):
+                        for oz in (-1, 0, 1):
+                            wx, wy, wz = bx + ox, by + oy, bz + oz
+                            nbid = ((wx % nb) * nb + (wy % nb)) * nb + (wz % nb)
+                            sl = border[bstart[nbid]:bstart[nbid + 1]]
+                            cand.append(sl)
+                            shifts.append(np.broadcast_to(
+                                np.array([wx // nb, wy // nb, wz // nb], np.float64), (len(sl), 3)))
+                cand = np.concatenate(cand)
+                pc = x[cand] + np.concatenate(shifts)
+                # split the block into octants while a group is too large
+                todo = [(np.array([bx, by, bz]) * block, block, members)]
+                while todo:
+                    lo, size, mem = todo.pop(0)
+                    if len(mem) > nmax and size > 1:
+                        h = size // 2
+                        cm = cell[mem]
+                        for ox in (0, h):
+                            for oy in (0, h):
+                                for oz in (0, h):
+                                    o = lo + np.array([ox, oy, oz])
+                                    sel = np.all((cm >= o) & (cm < o + h), axis=1)
+                                    todo.append((o, h, mem[sel]))
+                        continue
+                    if len(mem) == 0:
+                        continue
+                    blo, bhi = lo / mesh, (lo + size) / mesh
+                    d = np.maximum(0.0, np.maximum(blo - pc, pc - bhi))
+                    keep = (d * d).sum(axis=1) <= rcut * rcut
+                    order.append(mem)
+                    xjs.append(pc[keep])
+                    mjs.append(m[cand[keep]])
+                    items.append((ioff, len(mem), joff, int(keep.sum())))
+                    ioff += len(mem)
+                    joff += int(keep.sum())
+    order = np.concatenate(order)
+    return TreePMSet(x=x, m=m, xi=x[order], order=order, items=np.array(items, np.int32),
+                     xj=np.concatenate(xjs), mj=np.concatenate(mjs), rs=rs, rcut=rcut, eps=eps)

@@ -204,10 +204,11 @@ def test_batched_plan_matches_per_group_oracle(g5):
     joff = np.concatenate([[0], np.cumsum(nj)])
     xi = (rng.uniform(3 * ioff[-1]).reshape(-1, 3) - 0.5).astype(np.float32)
     xj = (rng.uniform(3 * joff[-1]).reshape(-1, 3) - 0.5).astype(np.float32)
-    mj = (rng.uniform(joff[-1]) + 0.5).astype(np.float32) / joff[-1]
+    mj = ((rng.uniform(joff[-1]) + 0.5) / joff[-1]).astype(np.float32)
     eps2 = np.float32(1e-4)
-    ipos = np.concatenate([xi, np.full((len(xi), 1), eps2, np.float32)], 1)
-    jpos = np.concatenate([xj, mj[:, None]], 1)
+    ipos = np.concatenate([xi, np.full((len(xi), 1), eps2, np.float32)], 1).astype(np.float32)
+    jpos = np.concatenate([xj, mj[:, None]], 1).astype(np.float32)
+    assert ipos.dtype == np.float32 and jpos.dtype == np.float32  # device layout: float4 records
     items = np.stack([ioff[:-1], ni, joff[:-1], nj], 1)
     dev = torch.device("cuda")
     d_i = torch.from_numpy(ipos).to(dev)
