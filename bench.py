@@ -1,0 +1,525 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 pairwise-force engine (one JSON line on stdout from rank 0).
+
+Workload (default, ``--workload hermite``): the PG6 4th-order Hermite force path on a
+N = 65536 Plummer sphere (distribution-function velocities, FP64 state, eps = 1e-4) in a
+block-time-step state; one step = 64 force calls with active sets of 2^k particles
+(k uniform in 4..16), each call = j-prediction of all 65536 particles to the call's time +
+force / jerk / potential / nearest neighbour of the active set against all j.
+About 4.1e10 pair interactions per step (60-flop convention, PG6/banana/banana01.h:9).
+
+Numbers:
+* ``value``   Gint/s of the batched device path (pgb6 plans: one persistent launch per call,
+              the 64 calls captured in one CUDA graph; inputs resident in HBM), device time
+              from CUDA events, L2 flushed (256 MiB write) between steps.
+* ``e2e``     the same schedule through the drop-in GRAPE-6 API (g6_set_ti,
+              g6calc_firsthalf / g6calc_lasthalf2p per npipes chunk, g6_set_j_particle of the
+              active set) with host buffers, timed on the host clock; the same driver replays
+              the reference library's identical call sequence for ``--impl reference``.
+* ``roofline`` the Hermite force kernel against the FP32 pipe: achieved = 60 flop x pairs / the
+              kernel's CUDA-event time; peak = 148 SMs x 128 lanes x 2 x SM clock.
+* ``cpu_baseline`` the reference's own AVX2 + OpenMP library (oracle/_ref) on the host cores,
+              on a bounded sample of the same schedule.
+
+Other workloads (``--workload``): ``direct`` (PG5 newton, N = 16384 Plummer, all i vs all j),
+``clusters`` (1024 independent Plummer clusters, N log-uniform in [256, 16384], one Hermite
+force evaluation each; batched vs 1024 sequences of plain calls), ``treepm`` (PG5 table, N=2^20
+uniform periodic box, 1024-entry table, 4096 i-groups with their j-lists in one launch).
+
+Multi-GPU (torchrun): every rank runs the full per-GPU workload on its own replica (the work
+items are independent: no data-path collective), ``scaling`` is "weak", ``value`` is the sum
+over ranks divided by the slowest rank's time (max over ranks via an NCCL all-reduce).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SM_COUNT = 148
+FP32_LANES = 128
+
+
+def load_pkg():
+    name = "phantom_grape_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    d = os.path.join(ROOT, "phantom-grape_b200")
+    spec = importlib.util.spec_from_file_location(name, os.path.join(d, "__init__.py"),
+                                                  submodule_search_locations=[d])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return {"sm_max_mhz": 1965.0, "hbm_gbs": 6650.0}
+
+
+# ----------------------------------------------------------------------------------------
+# clocks sampled during the timed region
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                rows.append(f)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows),
+                "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())}
+
+
+# ----------------------------------------------------------------------------------------
+# distributed plumbing
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def dist_init(ws, local, backend="nccl"):
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    if ws > 1:
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=timedelta(seconds=120))
+    return dist
+
+
+def reduce_max(value: float, ws: int, device) -> float:
+    """Max over ranks (NCCL all-reduce on a one-element tensor); identity on one rank."""
+    if ws <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def reduce_sum(value: float, ws: int, device) -> float:
+    if ws <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ----------------------------------------------------------------------------------------
+# Hermite workload (PG6 API)
+
+def predict_np(t, st):
+    """FP64 j-prediction (the library's own predictor formula, used here only to prepare the
+    i-particles of each call as a host integrator's predictor would, hermite.c:39-60)."""
+    dt = (t - st.tj)[:, None]
+    x = st.pos + st.vel * dt + st.acc2 * dt * dt + st.jrk6 * dt ** 3
+    v = st.vel + 2.0 * st.acc2 * dt + 3.0 * st.jrk6 * dt * dt
+    return x, v
+
+
+def hermite_workload(pgb, g6, n=65536, ncalls=64, seed_offset=0):
+    W = pgb.workloads
+
+    def gpu_force(x, v, m, eps2):
+        idx = np.arange(len(x), dtype=np.int32)
+        r = g6.batch_host([[0, len(x), 0, len(x)]], x, v, idx, x, v, m, idx, eps2, nn=False)
+        return r["acc"], r["jrk"]
+
+    st = W.hermite_state(n, seed=W.SEED0 + 1 + seed_offset, force_fn=gpu_force)
+    sets = W.hermite_schedule(n, ncalls, seed=W.SEED0 + 101 + seed_offset)
+    t_calls = st.t_now + np.arange(ncalls) * 2.0 ** -20
+    set_off = np.concatenate([[0], np.cumsum([len(s) for s in sets])]).astype(np.int32)
+    set_idx = np.concatenate(sets).astype(np.int32)
+    xi = np.empty((len(set_idx), 3))
+    vi = np.empty((len(set_idx), 3))
+    for c, s in enumerate(sets):
+        x, v = predict_np(t_calls[c], st)
+        xi[set_off[c]:set_off[c + 1]] = x[s]
+        vi[set_off[c]:set_off[c + 1]] = v[s]
+    return dict(st=st, sets=sets, t_calls=t_calls, set_off=set_off, set_idx=set_idx, xi=xi, vi=vi, n=n,
+                pairs=int(len(set_idx)) * n)
+
+
+class Driver:
+    """ctypes view of lib/libpgbdrv.so (drivers/pgb_drivers.c)."""
+
+    def __init__(self, pgb):
+        L = self.L = C.CDLL(pgb.ffi.lib_path("libpgbdrv.so"), mode=os.RTLD_LOCAL | os.RTLD_NOW)
+        dp, ip, vp = C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_void_p
+        L.g6drv_open.argtypes = [C.c_char_p]
+        L.g6drv_open.restype = vp
+        L.g6drv_npipes.argtypes = [vp]
+        L.g6drv_npipes.restype = C.c_int
+        L.g6drv_set_j.argtypes = [vp, C.c_int, dp, dp, dp, dp, dp, dp, ip, ip]
+        L.g6drv_set_j.restype = C.c_double
+        L.g6drv_schedule.argtypes = [vp, C.c_int, C.c_int, ip, ip, dp, dp, dp, C.c_double, C.c_int, C.c_int,
+                                     dp, dp, dp, dp, dp, dp, ip, dp, dp, dp, ip, C.POINTER(C.c_float)]
+        L.g6drv_schedule.restype = C.c_double
+        L.g5drv_open.argtypes = [C.c_char_p]
+        L.g5drv_open.restype = vp
+        L.g5drv_direct.argtypes = [vp, C.c_int, dp, dp, C.c_double, dp, dp]
+        L.g5drv_direct.restype = C.c_double
+        L.g5drv_groups.argtypes = [vp, C.c_int, ip, dp, dp, dp, C.c_double, dp, dp, C.c_int]
+        L.g5drv_groups.restype = C.c_double
+
+    @staticmethod
+    def p(a, t=C.c_double):
+        return None if a is None else a.ctypes.data_as(C.POINTER(t))
+
+    def g6_open(self, path):
+        h = self.L.g6drv_open(path.encode())
+        if not h:
+            raise RuntimeError(f"cannot open {path}")
+        return h
+
+    def g6_set_j(self, h, st):
+        p = self.p
+        return self.L.g6drv_set_j(h, len(st.mass), p(st.pos), p(st.vel), p(st.acc2), p(st.jrk6), p(st.mass),
+                                  p(st.tj), p(st.idx, C.c_int), None)
+
+    def g6_schedule(self, h, wl, calls=None, resend=True, outputs=False):
+        """Run calls [0, calls) of the schedule; returns (seconds, pairs, outputs or None)."""
+        st, p = wl["st"], self.p
+        ncalls = len(wl["sets"]) if calls is None else calls
+        off = wl["set_off"]
+        nact = int(off[ncalls])
+        out = None
+        if outputs:
+            out = dict(acc=np.zeros((nact, 3)), jrk=np.zeros((nact, 3)), pot=np.zeros(nact),
+                       nnb=np.zeros(nact, np.int32), rnnb=np.zeros(nact, np.float32))
+        o = out or {}
+        sec = self.L.g6drv_schedule(h, wl["n"], ncalls, p(off, C.c_int), p(wl["set_idx"], C.c_int), p(wl["t_calls"]),
+                                    p(wl["xi"]), p(wl["vi"]), st.eps2, 1, 1 if resend else 0, p(st.pos), p(st.vel),
+                                    p(st.acc2), p(st.jrk6), p(st.mass), p(st.tj), p(st.idx, C.c_int),
+                                    p(o.get("acc")), p(o.get("jrk")), p(o.get("pot")), p(o.get("nnb"), C.c_int),
+                                    p(o.get("rnnb"), C.c_float))
+        return sec, nact * wl["n"], out
+
+
+def ref_lib(name):
+    """The reference's own build (oracle/_ref), compiled here when the reference is present."""
+    path = os.path.join(ROOT, "oracle", "_ref", name)
+    if not os.path.exists(path) and os.path.isdir("/root/reference"):
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=False)
+    return path if os.path.exists(path) else None
+
+
+def cpu_sample_calls(wl, target_pairs):
+    """Smallest prefix of the schedule with at least target_pairs interactions."""
+    cum = np.cumsum([len(s) * wl["n"] for s in wl["sets"]])
+    return int(min(len(cum), np.searchsorted(cum, target_pairs) + 1))
+
+
+def cpu_baseline_hermite(pgb, wl, target_pairs=1.2e10):
+    path = ref_lib("libpg6_ref.so")
+    if path is None:
+        return {"value": None, "unit": "Gint/s", "cores": os.cpu_count(), "kind": "reference",
+                "sample": "unavailable: reference library not built"}
+    drv = Driver(pgb)
+    h = drv.g6_open(path)
+    drv.g6_set_j(h, wl["st"])
+    calls = cpu_sample_calls(wl, target_pairs)
+    drv.g6_schedule(h, wl, calls=1)                 # warm-up (OpenMP pool, page faults)
+    sec, pairs, _ = drv.g6_schedule(h, wl, calls=calls)
+    return {"value": pairs / sec / 1e9, "unit": "Gint/s", "cores": os.cpu_count(), "kind": "reference",
+            "sample": f"first {calls} of 64 block-step calls ({pairs:.3e} pairs, {sec:.1f} s), "
+                      f"libpg6 AVX2 + OpenMP (PG6/libpg6 built from its sources), npipes 48"}
+
+
+def run_hermite(args, pgb, ws, rank, local):
+    import torch
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    ffi = pgb.ffi
+    g6 = ffi.G6()
+    g6.L.g6_open(0)
+    wl = hermite_workload(pgb, g6, seed_offset=rank)
+    st, n, sets = wl["st"], wl["n"], wl["sets"]
+
+    # device-resident inputs: j-memory records, the i-records of every call, outputs
+    ptcl = np.zeros(n, ffi.G6PTCL)
+    ptcl["pos"], ptcl["vel"], ptcl["acc2"], ptcl["jrk6"] = st.pos, st.vel, st.acc2, st.jrk6
+    ptcl["mass"], ptcl["tim"], ptcl["idx"] = st.mass, st.tj, st.idx
+    nact = len(wl["set_idx"])
+    irec = np.zeros(nact, ffi.G6IREC)
+    for k, name in enumerate("xyz"):
+        irec[name] = wl["xi"][:, k]
+        irec["v" + name] = wl["vi"][:, k]
+    irec["id"] = st.idx[wl["set_idx"]]
+    d_ptcl = torch.from_numpy(ptcl.view(np.uint8)).to(dev)
+    d_irec = torch.from_numpy(irec.view(np.uint8)).to(dev)
+    d_pred = torch.zeros(n * ffi.G6PREDJ.itemsize, dtype=torch.uint8, device=dev)
+    d_out = torch.zeros(nact * ffi.G6OUT.itemsize, dtype=torch.uint8, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    off = wl["set_off"]
+    plans = [g6.plan_create([[int(off[c]), len(sets[c]), 0, n]], nn=True) for c in range(len(sets))]
+    s = torch.cuda.Stream(device=dev)
+
+    def step_launches():
+        for c in range(len(sets)):
+            rc = g6.L.pgb6_predict(d_ptcl.data_ptr(), n, float(wl["t_calls"][c]), d_pred.data_ptr(), s.cuda_stream)
+            assert rc == 0
+            g6.plan_launch(plans[c], d_irec.data_ptr(), d_pred.data_ptr(), st.eps2, d_out.data_ptr(), s.cuda_stream)
+
+    with torch.cuda.stream(s):
+        step_launches()
+    s.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=s):
+        step_launches()
+
+    for _ in range(args.warmup):
+        graph.replay()
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    clocks.start()
+    barrier(ws)
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        with torch.cuda.stream(s):
+            ev[k][0].record(s)
+            graph.replay()
+            ev[k][1].record(s)
+            flush.fill_(k & 0xFF)   # 256 MiB write between steps: L2 (126 MB) flushed
+    torch.cuda.synchronize()
+    barrier(ws)
+    clk = clocks.stop()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    t_local = sum(step_ms) / 1e3
+    t_max = reduce_max(t_local, ws, dev)
+    pairs_total = reduce_sum(float(wl["pairs"]) * args.steps, ws, dev)
+    value = pairs_total / t_max / 1e9
+
+    # roofline pass (after the timed region): each force launch timed alone with CUDA events
+    fev = []
+    with torch.cuda.stream(s):
+        for c in range(len(sets)):
+            g6.L.pgb6_predict(d_ptcl.data_ptr(), n, float(wl["t_calls"][c]), d_pred.data_ptr(), s.cuda_stream)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(s)
+            g6.plan_launch(plans[c], d_irec.data_ptr(), d_pred.data_ptr(), st.eps2, d_out.data_ptr(), s.cuda_stream)
+            b.record(s)
+            fev.append((a, b, len(sets[c]) * n))
+    torch.cuda.synchronize()
+    kern_s = sum(a.elapsed_time(b) for a, b, _ in fev) / 1e3
+    kern_pairs = sum(p for _, _, p in fev)
+    big = max(fev, key=lambda e: e[2])
+    big_ms = big[0].elapsed_time(big[1])
+
+    # end to end through the GRAPE-6 API with host buffers (same driver as the reference arm)
+    drv = Driver(pgb)
+    h = drv.g6_open(pgb.ffi.lib_path("libpg6.so"))
+    drv.g6_set_j(h, st)
+    drv.g6_schedule(h, wl, calls=4)   # warm-up
+    e2e_steps = max(1, min(args.steps, args.e2e_steps))
+    torch.cuda.synchronize()
+    barrier(ws)
+    e2e_t = 0.0
+    for _ in range(e2e_steps):
+        sec, _, _ = drv.g6_schedule(h, wl)
+        e2e_t += sec
+    e2e_max = reduce_max(e2e_t, ws, dev)
+    e2e_val = reduce_sum(float(wl["pairs"]) * e2e_steps, ws, dev) / e2e_max / 1e9
+    npipe = g6.L.g6_npipes()
+    nchunks = sum((len(x) + npipe - 1) // npipe for x in sets)
+    h2d = nact * (ffi.G6IREC.itemsize + ffi.G6PTCL.itemsize + 4) + nchunks * 16 + len(sets) * 0
+    d2h = nact * ffi.G6OUT.itemsize
+
+    pk = peaks()
+    sm_mhz = clk.get("sm_mhz") or pk.get("sm_max_mhz", 1965.0)
+    fp32_peak_tf = SM_COUNT * FP32_LANES * 2 * sm_mhz * 1e6 / 1e12
+    fp32_peak_max = SM_COUNT * FP32_LANES * 2 * pk.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
+    achieved_tf = kern_pairs * 60 / kern_s / 1e12
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_hermite(pgb, wl)
+    for p_ in plans:
+        g6.plan_destroy(p_)
+    del graph
+    line = {
+        "metric": "Gint/s (PG6 Hermite force+jerk+pot+NN, batched)",
+        "value": round(value, 2),
+        "unit": "Gint/s",
+        "n_gpus": ws,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(t_max / args.steps * 1e3, 3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 (f64 predictor + x_j-x_i, f64 cross-tile sums)",
+        "data": "synthetic (seeded Plummer, DF velocities; no dataset)",
+        "config": {"workload": "PG6 Hermite N=65536 Plummer eps=1e-4, 64 block-step calls of 2^k active "
+                               "(k=4..16), force+jerk+pot+nearest neighbour",
+                   "pairs_per_step": wl["pairs"], "flop_per_pair": 60, "l2": "flushed between steps (256 MiB write)",
+                   "parallelism": f"replicas x{ws} (independent schedules, no data-path collective)",
+                   "graph": "64 x (predict + persistent force launch) in one CUDA graph"},
+        "frac_fp32": round(value * 1e9 * 60 / 1e12 / fp32_peak_tf, 4),
+        "roofline": {"bound": "fp32", "achieved": round(achieved_tf, 2), "peak": round(fp32_peak_tf, 2),
+                     "unit": "TFLOP/s", "frac": round(achieved_tf / fp32_peak_tf, 4), "traffic": None,
+                     "kernel": "pgb::g6_kernel<128,2,NN> (and <128,1>/<64,1> for small active sets)",
+                     "peak_source": f"148 SM x 128 FP32 lanes x 2 x median SM clock {sm_mhz:.0f} MHz sampled "
+                                    f"in the timed region ({fp32_peak_max:.1f} TFLOP/s at sm_max_mhz)",
+                     "largest_launch_ms": round(big_ms, 3), "largest_launch_pairs": big[2]},
+        "e2e": {"value": round(e2e_val, 2), "unit": "Gint/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "api": "GRAPE-6 drop-in (g6_set_ti, g6calc_firsthalf, "
+                "g6calc_lasthalf2p per npipes chunk, g6_set_j_particle of the active set), host buffers",
+                "npipes": npipe, "steps": e2e_steps},
+        "gpu_launches": args.steps * 2 * len(sets),
+        "clocks": clk,
+        "cpu_baseline": cpu,
+    }
+    return line
+
+
+# ----------------------------------------------------------------------------------------
+# reference arm
+
+def run_reference(args, pgb, ws, rank):
+    if rank != 0:
+        return None
+    path = ref_lib("libpg6_ref.so")
+    if path is None:
+        return {"impl": "reference", "unavailable": "reference library (oracle/_ref/libpg6_ref.so) not built"}
+    W = pgb.workloads
+    drv = Driver(pgb)
+    h = drv.g6_open(path)
+    # same workload; a = j from an FP64-free source is not needed for timing: use the engine's
+    # own force only if a GPU is present, else zero acc/jerk (prediction cost is the same)
+    st = W.hermite_state(65536, seed=W.SEED0 + 1)
+    sets = W.hermite_schedule(65536, 64, seed=W.SEED0 + 101)
+    t_calls = st.t_now + np.arange(64) * 2.0 ** -20
+    set_off = np.concatenate([[0], np.cumsum([len(s) for s in sets])]).astype(np.int32)
+    set_idx = np.concatenate(sets).astype(np.int32)
+    xi = np.empty((len(set_idx), 3))
+    vi = np.empty((len(set_idx), 3))
+    for c, s in enumerate(sets):
+        x, v = predict_np(t_calls[c], st)
+        xi[set_off[c]:set_off[c + 1]] = x[s]
+        vi[set_off[c]:set_off[c + 1]] = v[s]
+    wl = dict(st=st, sets=sets, t_calls=t_calls, set_off=set_off, set_idx=set_idx, xi=xi, vi=vi, n=65536)
+    drv.g6_set_j(h, st)
+    calls = cpu_sample_calls(wl, args.ref_pairs)
+    for _ in range(args.warmup):
+        drv.g6_schedule(h, wl, calls=calls)
+    tot, pairs = 0.0, 0
+    for _ in range(args.steps):
+        sec, p_, _ = drv.g6_schedule(h, wl, calls=calls)
+        tot += sec
+        pairs += p_
+    val = pairs / tot / 1e9
+    sample = (f"first {calls} of the 64 block-step calls per step ({pairs // args.steps:.3e} pairs), "
+              f"PG6/libpg6 AVX2 + OpenMP built from its own sources, npipes 48")
+    return {
+        "metric": "Gint/s (PG6 Hermite force+jerk+pot+NN, batched)",
+        "value": round(val, 3), "unit": "Gint/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(tot / args.steps * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (f64 predictor + x_j-x_i)", "data": "synthetic",
+        "config": {"workload": "PG6 Hermite N=65536 Plummer eps=1e-4, 64 block-step calls of 2^k active "
+                               "(k=4..16), force+jerk+pot+nearest neighbour (sampled prefix)",
+                   "flop_per_pair": 60},
+        "impl": "reference",
+        "cpu_baseline": {"value": round(val, 3), "unit": "Gint/s", "cores": os.cpu_count(), "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": round(val, 3), "unit": "Gint/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+# ----------------------------------------------------------------------------------------
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["hermite"], default="hermite")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--ref-pairs", type=float, default=4e9, help="pairs per reference-arm step")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    ws, rank, local = dist_setup()
+    pgb = load_pkg()
+    if args.impl == "reference":
+        line = run_reference(args, pgb, ws, rank)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return
+    dist = dist_init(ws, local)
+    line = run_hermite(args, pgb, ws, rank, local)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -178,6 +178,14 @@ struct State {
     DevBuf<G6Ptcl> jd;
     DevBuf<G6PredJ> pred;
     int jcap = 0, jdirty_lo = 1 << 30, jdirty_hi = 0;
+    // sparse updates (a block step re-sends only its active particles): dirty addresses
+    std::vector<int> dirty;
+    std::vector<unsigned char> dirty_flag;
+    bool all_dirty = true;
+    HostBuf<G6Ptcl> sbuf;   // packed dirty records
+    HostBuf<int> sidx;      // their addresses
+    DevBuf<G6Ptcl> sbuf_d;
+    DevBuf<int> sidx_d;
     double ti = 0.0;
     int predict_flag = 0;
     HostBuf<G6I> ibuf;
@@ -213,23 +221,60 @@ bool grow_j(int need) {
     if (cap > jmemsize()) cap = jmemsize();
     PGB_CUDA_OR(g_err, LIB, S.jh.reserve(cap, true), return false);
     std::memset((void*)(S.jh.p + S.jcap), 0, (size_t)(cap - S.jcap) * sizeof(G6Ptcl));
+    S.dirty_flag.resize(cap, 0);
+    S.all_dirty = true;  // new device buffer: upload everything
     S.jdirty_lo = 0;
     S.jdirty_hi = cap;
     S.jcap = cap;
     return true;
 }
 
+void mark_dirty(int padr) {
+    if (padr < S.jdirty_lo) S.jdirty_lo = padr;
+    if (padr + 1 > S.jdirty_hi) S.jdirty_hi = padr + 1;
+    if (!S.all_dirty && !S.dirty_flag[padr]) {
+        S.dirty_flag[padr] = 1;
+        S.dirty.push_back(padr);
+    }
+}
+
+// Upload the j-memory changes: the contiguous dirty range, or, when the changed records are
+// sparse in it (a block step's active set), only those records plus a scatter on the device.
+bool flush_j() {
+    if (S.jdirty_hi <= S.jdirty_lo) return true;
+    PGB_CUDA_OR(g_err, LIB, S.jd.reserve(S.jcap), return false);
+    size_t lo = S.jdirty_lo, range = (size_t)(S.jdirty_hi - S.jdirty_lo), n = S.dirty.size();
+    if (!S.all_dirty && n * 4 < range) {
+        PGB_CUDA_OR(g_err, LIB, S.sbuf.reserve(n), return false);
+        PGB_CUDA_OR(g_err, LIB, S.sidx.reserve(n), return false);
+        PGB_CUDA_OR(g_err, LIB, S.sbuf_d.reserve(n), return false);
+        PGB_CUDA_OR(g_err, LIB, S.sidx_d.reserve(n), return false);
+        for (size_t k = 0; k < n; k++) {
+            S.sbuf.p[k] = S.jh.p[S.dirty[k]];
+            S.sidx.p[k] = S.dirty[k];
+        }
+        PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(S.sbuf_d.p, S.sbuf.p, n * sizeof(G6Ptcl), cudaMemcpyHostToDevice,
+                                                S.stream), return false);
+        PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(S.sidx_d.p, S.sidx.p, n * sizeof(int), cudaMemcpyHostToDevice,
+                                                S.stream), return false);
+        g6_scatter_kernel<<<(int)((n + 255) / 256), 256, 0, S.stream>>>(S.sbuf_d.p, S.sidx_d.p, (int)n, S.jcap,
+                                                                         S.jd.p);
+        PGB_CUDA_OR(g_err, LIB, cudaGetLastError(), return false);
+    } else {
+        PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(S.jd.p + lo, S.jh.p + lo, range * sizeof(G6Ptcl),
+                                                cudaMemcpyHostToDevice, S.stream), return false);
+    }
+    for (int a : S.dirty) S.dirty_flag[a] = 0;
+    S.dirty.clear();
+    S.all_dirty = false;
+    S.jdirty_lo = 1 << 30;
+    S.jdirty_hi = 0;
+    return true;
+}
+
 bool flush_and_predict(int nj) {
     if (nj <= 0) return true;
-    if (!grow_j(nj)) return false;
-    if (S.jdirty_hi > S.jdirty_lo) {
-        PGB_CUDA_OR(g_err, LIB, S.jd.reserve(S.jcap), return false);
-        size_t lo = S.jdirty_lo, n = (size_t)(S.jdirty_hi - S.jdirty_lo);
-        PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(S.jd.p + lo, S.jh.p + lo, n * sizeof(G6Ptcl),
-                                                cudaMemcpyHostToDevice, S.stream), return false);
-        S.jdirty_lo = 1 << 30;
-        S.jdirty_hi = 0;
-    }
+    if (!grow_j(nj) || !flush_j()) return false;
     PGB_CUDA_OR(g_err, LIB, S.pred.reserve(S.jcap), return false);
     g6_predict_kernel<<<(nj + 255) / 256, 256, 0, S.stream>>>(S.jd.p, nj, S.ti, S.pred.p);
     PGB_CUDA_OR(g_err, LIB, cudaGetLastError(), return false);
@@ -383,6 +428,11 @@ PGB_EXPORT void g6_close(int gpid) {
     S.st.release();
     S.nbc_d.release();
     S.nbl_d.release();
+    S.sbuf_d.release();
+    S.sidx_d.release();
+    for (int a : S.dirty) S.dirty_flag[a] = 0;
+    S.dirty.clear();
+    S.all_dirty = true;
     S.jdirty_lo = 0;
     S.jdirty_hi = S.jcap;
 }
@@ -414,8 +464,7 @@ PGB_EXPORT void g6_set_j_particle(int gpid, int padr, int pidx, double t, double
     p.mass = mss;
     p.tim = t;
     p.idx = pidx;
-    if (padr < S.jdirty_lo) S.jdirty_lo = padr;
-    if (padr + 1 > S.jdirty_hi) S.jdirty_hi = padr + 1;
+    mark_dirty(padr);
 }
 
 PGB_EXPORT void g6_set_ti(int gpid, double time) {

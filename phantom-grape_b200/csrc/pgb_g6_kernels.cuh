@@ -93,6 +93,15 @@ __global__ void g6_predict_kernel(const G6Ptcl* __restrict__ p, int nj, double t
     out[j] = o;
 }
 
+// Sparse j-memory update: jd[idx[k]] = rec[k] (addresses checked against the capacity).
+__global__ void g6_scatter_kernel(const G6Ptcl* __restrict__ rec, const int* __restrict__ idx, int n, int cap,
+                                  G6Ptcl* __restrict__ jd) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int a = idx[k];
+    if (a >= 0 && a < cap) jd[a] = rec[k];
+}
+
 struct G6Acc {
     float ax, ay, az, jx, jy, jz, pot;
 };

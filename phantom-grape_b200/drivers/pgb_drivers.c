@@ -1,0 +1,218 @@
+/*
+ * pgb_drivers.c -- call-sequence drivers for the GRAPE-5 / GRAPE-6 C APIs.
+ *
+ * Each driver dlopen()s a library that exports the GRAPE API -- this project's lib/libpg*.so
+ * or the reference's own build -- and replays the call sequence of the reference's sample
+ * programs, timing it with CLOCK_MONOTONIC.  The benchmark uses the same driver for both
+ * implementations, so the two arms make identical API calls:
+ *
+ *  g6drv_schedule  block time-step force calls as PG6/banana/hermite.c:214-275 makes them:
+ *                  g6_set_ti, then per npipes-sized chunk g6calc_firsthalf + g6calc_lasthalf2p,
+ *                  then g6_set_j_particle for the corrected active particles.
+ *  g5drv_direct    PG5/newton/direct/direct.c:133-176: g5_set_xmj, g5_set_eps_to_all,
+ *                  g5_set_n, g5_calculate_force_on_x.
+ *  g5drv_groups    PG5/newton_quad/source.cpp:813-860 style: OpenMP over i-groups, each thread
+ *                  with its own devid: g5_set_xmjMC, g5_set_nMC, g5_calculate_force_on_xMC.
+ *
+ * Libraries are opened with RTLD_LOCAL so several GRAPE libraries can coexist in one process.
+ */
+#define _GNU_SOURCE
+#include <dlfcn.h>
+#include <omp.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+
+static double now(void) {
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
+
+#define LOAD(h, var, name)                                                       \
+    do {                                                                         \
+        *(void **)(&(var)) = dlsym((h), (name));                                 \
+        if (!(var)) {                                                            \
+            fprintf(stderr, "pgb_drivers: %s has no symbol %s\n", path, (name)); \
+            return NULL;                                                         \
+        }                                                                        \
+    } while (0)
+
+/* ---------------------------------------------------------------------------------------- */
+/* GRAPE-6 (PG6/libpg6/gp6util.h) */
+
+typedef struct {
+    void *h;
+    void (*open)(int);
+    int (*npipes)(void);
+    void (*set_j)(int, int, int, double, double, double, double *, double *, double *, double *, double *);
+    void (*set_ti)(int, double);
+    void (*firsthalf)(int, int, int, int *, double (*)[3], double (*)[3], double (*)[3], double (*)[3], double *,
+                      double, double *);
+    int (*lasthalf2p)(int, int, int, int *, double (*)[3], double (*)[3], double, double *, double (*)[3],
+                      double (*)[3], double *, int *, float *);
+    int (*lasthalf)(int, int, int, int *, double (*)[3], double (*)[3], double, double *, double (*)[3],
+                    double (*)[3], double *);
+} g6api;
+
+void *g6drv_open(const char *path) {
+    void *h = dlopen(path, RTLD_LOCAL | RTLD_NOW);
+    if (!h) {
+        fprintf(stderr, "pgb_drivers: dlopen(%s): %s\n", path, dlerror());
+        return NULL;
+    }
+    g6api *a = (g6api *)calloc(1, sizeof(g6api));
+    a->h = h;
+    LOAD(h, a->open, "g6_open");
+    LOAD(h, a->npipes, "g6_npipes");
+    LOAD(h, a->set_j, "g6_set_j_particle");
+    LOAD(h, a->set_ti, "g6_set_ti");
+    LOAD(h, a->firsthalf, "g6calc_firsthalf");
+    LOAD(h, a->lasthalf2p, "g6calc_lasthalf2p");
+    LOAD(h, a->lasthalf, "g6calc_lasthalf");
+    a->open(0);
+    return a;
+}
+
+int g6drv_npipes(void *handle) { return ((g6api *)handle)->npipes(); }
+
+/* g6_set_j_particle for n particles (addr NULL: address = index). */
+double g6drv_set_j(void *handle, int n, const double *pos, const double *vel, const double *acc2, const double *jrk6,
+                   const double *mass, const double *tj, const int *idx, const int *addr) {
+    g6api *a = (g6api *)handle;
+    double snp[3] = {0, 0, 0};
+    double t0 = now();
+    for (int k = 0; k < n; k++) {
+        int j = addr ? addr[k] : k;
+        a->set_j(0, j, idx[j], tj[j], 0.0, mass[j], snp, (double *)jrk6 + 3 * j, (double *)acc2 + 3 * j,
+                 (double *)vel + 3 * j, (double *)pos + 3 * j);
+    }
+    return now() - t0;
+}
+
+/* One pass over `ncalls` block steps.  Call c uses time t_calls[c] and the active particles
+ * set_idx[set_off[c] .. set_off[c+1]) whose predicted positions / velocities are
+ * xi/vi[set_off[c] ..].  With `resend`, the active particles' j-records (from pos..tj) are
+ * re-sent after each call, as the corrector does (hermite.c:255-275).  Outputs (optional) are
+ * written per active particle in the same concatenated order.  Returns the elapsed seconds. */
+double g6drv_schedule(void *handle, int nj, int ncalls, const int *set_off, const int *set_idx,
+                      const double *t_calls, const double *xi, const double *vi, double eps2, int with_nnb,
+                      int resend, const double *pos, const double *vel, const double *acc2, const double *jrk6,
+                      const double *mass, const double *tj, const int *idx, double *acc_out, double *jrk_out,
+                      double *pot_out, int *nnb_out, float *rnnb_out) {
+    g6api *a = (g6api *)handle;
+    int npipe = a->npipes();
+    int *pidx = (int *)malloc(sizeof(int) * npipe);
+    double(*acc)[3] = malloc(sizeof(double) * 3 * npipe);
+    double(*jrk)[3] = malloc(sizeof(double) * 3 * npipe);
+    double *pot = (double *)malloc(sizeof(double) * npipe);
+    double *h2 = (double *)calloc(npipe, sizeof(double));
+    int *nnb = (int *)malloc(sizeof(int) * npipe);
+    float *rnnb = (float *)malloc(sizeof(float) * npipe);
+    double snp[3] = {0, 0, 0};
+    double t0 = now();
+    for (int c = 0; c < ncalls; c++) {
+        int off = set_off[c], ni = set_off[c + 1] - set_off[c];
+        a->set_ti(0, t_calls[c]);
+        for (int i = 0; i < ni; i += npipe) {
+            int nii = ni - i < npipe ? ni - i : npipe;
+            for (int k = 0; k < nii; k++) pidx[k] = idx[set_idx[off + i + k]];
+            double(*px)[3] = (double(*)[3])(xi + 3 * (size_t)(off + i));
+            double(*pv)[3] = (double(*)[3])(vi + 3 * (size_t)(off + i));
+            a->firsthalf(0, nj, nii, pidx, px, pv, acc, jrk, pot, eps2, h2);
+            if (with_nnb)
+                a->lasthalf2p(0, nj, nii, pidx, px, pv, eps2, h2, acc, jrk, pot, nnb, rnnb);
+            else
+                a->lasthalf(0, nj, nii, pidx, px, pv, eps2, h2, acc, jrk, pot);
+            size_t o = (size_t)(off + i);
+            if (acc_out) memcpy(acc_out + 3 * o, acc, sizeof(double) * 3 * nii);
+            if (jrk_out) memcpy(jrk_out + 3 * o, jrk, sizeof(double) * 3 * nii);
+            if (pot_out) memcpy(pot_out + o, pot, sizeof(double) * nii);
+            if (nnb_out && with_nnb) memcpy(nnb_out + o, nnb, sizeof(int) * nii);
+            if (rnnb_out && with_nnb) memcpy(rnnb_out + o, rnnb, sizeof(float) * nii);
+        }
+        if (resend) {
+            for (int k = 0; k < ni; k++) {
+                int j = set_idx[off + k];
+                a->set_j(0, j, idx[j], tj[j], 0.0, mass[j], snp, (double *)jrk6 + 3 * j, (double *)acc2 + 3 * j,
+                         (double *)vel + 3 * j, (double *)pos + 3 * j);
+            }
+        }
+    }
+    double el = now() - t0;
+    free(pidx);
+    free(acc);
+    free(jrk);
+    free(pot);
+    free(h2);
+    free(nnb);
+    free(rnnb);
+    return el;
+}
+
+/* ---------------------------------------------------------------------------------------- */
+/* GRAPE-5 (PG5/newton/libpg5/gp5util.h, PG5/table/libpg5/gp5util.h) */
+
+typedef struct {
+    void *h;
+    void (*open)(void);
+    void (*set_eps_to_all)(double);
+    void (*set_xmj)(int, int, double (*)[3], double *);
+    void (*set_n)(int);
+    void (*calc)(double (*)[3], double (*)[3], double *, int);
+    void (*set_xmjMC)(int, int, int, double (*)[3], double *);
+    void (*set_nMC)(int, int);
+    void (*calcMC)(int, double (*)[3], double (*)[3], double *, int);
+} g5api;
+
+void *g5drv_open(const char *path) {
+    void *h = dlopen(path, RTLD_LOCAL | RTLD_NOW);
+    if (!h) {
+        fprintf(stderr, "pgb_drivers: dlopen(%s): %s\n", path, dlerror());
+        return NULL;
+    }
+    g5api *a = (g5api *)calloc(1, sizeof(g5api));
+    a->h = h;
+    LOAD(h, a->open, "g5_open");
+    LOAD(h, a->set_eps_to_all, "g5_set_eps_to_all");
+    LOAD(h, a->set_xmj, "g5_set_xmj");
+    LOAD(h, a->set_n, "g5_set_n");
+    LOAD(h, a->calc, "g5_calculate_force_on_x");
+    LOAD(h, a->set_xmjMC, "g5_set_xmjMC");
+    LOAD(h, a->set_nMC, "g5_set_nMC");
+    LOAD(h, a->calcMC, "g5_calculate_force_on_xMC");
+    a->open();
+    return a;
+}
+
+/* Direct summation, all i against all j (direct.c:133-176). */
+double g5drv_direct(void *handle, int n, const double *x, const double *m, double eps, double *acc, double *pot) {
+    g5api *a = (g5api *)handle;
+    double t0 = now();
+    a->set_xmj(0, n, (double(*)[3])x, (double *)m);
+    a->set_eps_to_all(eps);
+    a->set_n(n);
+    a->calc((double(*)[3])x, (double(*)[3])acc, pot, n);
+    return now() - t0;
+}
+
+/* Interaction-list groups: items[k] = {i_off, i_cnt, j_off, j_cnt}; OpenMP over groups with
+ * devid = thread id (source.cpp:813-860).  nthreads <= 0: OpenMP default. */
+double g5drv_groups(void *handle, int ngroups, const int *items, const double *xi, const double *xj,
+                    const double *mj, double eps, double *acc, double *pot, int nthreads) {
+    g5api *a = (g5api *)handle;
+    a->set_eps_to_all(eps);
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+    double t0 = now();
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int g = 0; g < ngroups; g++) {
+        int dev = omp_get_thread_num();
+        const int *it = items + 4 * g;
+        a->set_xmjMC(dev, 0, it[3], (double(*)[3])(xj + 3 * (size_t)it[2]), (double *)mj + it[2]);
+        a->set_nMC(dev, it[3]);
+        a->calcMC(dev, (double(*)[3])(xi + 3 * (size_t)it[0]), (double(*)[3])(acc + 3 * (size_t)it[0]),
+                  pot + it[0], it[1]);
+    }
+    return now() - t0;
+}
