@@ -123,7 +123,8 @@ int choose_jchunk(long long itiles_total, int nj, int slots) {
     if (nj <= 0) return 1;
     long long target = 4LL * slots;
     long long nch = (target + itiles_total - 1) / (itiles_total > 0 ? itiles_total : 1);
-    long long maxch = (nj + 127) / 128;  // at least 128 j per chunk
+    long long maxch = (nj + 127) / 128;  // at least 128 j per chunk, at most 512 chunks
+    if (maxch > 512) maxch = 512;
     if (nch > maxch) nch = maxch;
     if (nch < 1) nch = 1;
     return (int)((nj + nch - 1) / nch);
@@ -913,6 +914,7 @@ PGB_EXPORT int pgb5_plan_create(pgb5_plan** out, int kind, int nitem, const int*
         long long tile_i = ni < ITILE ? ni : ITILE;
         long long jc = tile_i > 0 ? per_task / tile_i : nj;
         if (jc < 256) jc = 256;
+        if (jc * 512 < nj) jc = (nj + 511) / 512;
         if (jc > nj) jc = nj > 0 ? nj : 1;
         P->rows += plan_item(P->tasks, P->groups, items[4 * k], ni, items[4 * k + 2], nj, ITILE, (int)jc, P->rows);
         P->interactions += (long long)ni * nj;

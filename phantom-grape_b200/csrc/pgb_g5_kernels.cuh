@@ -124,7 +124,7 @@ __device__ __forceinline__ double4 add4(double4 a, double4 b) {
 template <int KIND, int NT, int IPT>
 __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
     constexpr int W = JWords<KIND>::n;   // 16-byte words per j record
-    __shared__ float4 sj[NT * W];
+    __shared__ float4 sj[NT * (W > 2 ? W : 2)];  // also the reduction buffer (double4 x NT)
     __shared__ int s_task, s_flag;
     // table kind: the whole force table in shared memory for the lifetime of the CTA
     __shared__ float2 stab[KIND == G5_TABLE ? G5_TBL_MAX : 1];
@@ -206,18 +206,32 @@ __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
         }
         const Group G = A.groups[T.group];
         if (group_arrive(A.group_counters, T.group, G.nchunk, &s_flag)) {
-#pragma unroll
-            for (int k = 0; k < IPT; k++) {
-                int li = threadIdx.x + k * NT;
-                if (li >= G.ni) continue;
+            // Cooperative reduction of the group's partial rows: P threads per i, each summing a
+            // fixed strided subset of the rows, then the P sums in thread order (deterministic
+            // for a given group shape).  `red` reuses the j-tile buffer.
+            double4* red = reinterpret_cast<double4*>(sj);
+            static_assert(sizeof(float4) * NT * (W > 2 ? W : 2) >= sizeof(double4) * NT, "reduction buffer");
+            int P = 1;
+            while (P * 2 * G.ni <= NT) P *= 2;
+            const int per = NT / P;
+            for (int base = 0; base < G.ni; base += per) {
+                const int li = base + threadIdx.x / P, p = threadIdx.x % P;
                 double4 s = make_double4(0, 0, 0, 0);
-                for (int c = 0; c < G.nchunk; c++) {
-                    const double4* r = A.partial + (size_t)(G.slot0 + c) * A.itile + li;
-                    double4 v;
-                    v.x = __ldcg(&r->x); v.y = __ldcg(&r->y); v.z = __ldcg(&r->z); v.w = __ldcg(&r->w);
-                    s = add4(s, v);
+                if (li < G.ni) {
+                    for (int c = p; c < G.nchunk; c += P) {
+                        const double4* r = A.partial + (size_t)(G.slot0 + c) * A.itile + li;
+                        double4 v;
+                        v.x = __ldcg(&r->x); v.y = __ldcg(&r->y); v.z = __ldcg(&r->z); v.w = __ldcg(&r->w);
+                        s = add4(s, v);
+                    }
                 }
-                A.out[G.i0 + li] = g5_finish<KIND>(s, A.ascale);
+                __syncthreads();
+                red[threadIdx.x] = s;
+                __syncthreads();
+                if (p == 0 && li < G.ni) {
+                    for (int q = 1; q < P; q++) s = add4(s, red[threadIdx.x + q]);
+                    A.out[G.i0 + li] = g5_finish<KIND>(s, A.ascale);
+                }
             }
         }
     }

@@ -76,73 +76,94 @@ bool ensure_device() {
 }
 
 // ------------------------------------------------------------------------------------------
-// kernel configurations: (threads per CTA, i per thread)
+// kernel configurations: (threads per CTA, i per thread, j-lanes); i-tile = NT/JL*IPT
 
-enum Cfg { CFG_64x1 = 0, CFG_128x1 = 1, CFG_128x2 = 2, NCFG = 3 };
-constexpr int CFG_NT[NCFG] = {64, 128, 128};
-constexpr int CFG_IPT[NCFG] = {1, 1, 2};
-inline int cfg_itile(int c) { return CFG_NT[c] * CFG_IPT[c]; }
+enum Cfg { CFG_SMALL = 0, CFG_MED = 1, CFG_LARGE = 2, CFG_128x1 = 3, NCFG = 4 };
+constexpr int CFG_NT[NCFG] = {512, 256, 128, 128};
+constexpr int CFG_IPT[NCFG] = {1, 1, 2, 1};
+constexpr int CFG_JL[NCFG] = {8, 2, 1, 1};
+inline int cfg_itile(int c) { return CFG_NT[c] / CFG_JL[c] * CFG_IPT[c]; }
 constexpr int ITILE_MAX = 256;
 
-template <int NT, int IPT, bool NN, bool NBL>
-void launch_one(int grid, const G6Args& a, cudaStream_t s) {
-    g6_kernel<NT, IPT, NN, NBL><<<grid, NT, 0, s>>>(a);
-}
-
-template <int NT, int IPT>
+template <int NT, int IPT, int JL, bool FF>
 int occ_of(bool nn, bool nbl) {
     static int v[4] = {0, 0, 0, 0};
     int k = (nn ? 1 : 0) + (nbl ? 2 : 0);
     if (!v[k]) {
         int b = 0;
-        if (k == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, false, false>, NT, 0);
-        if (k == 1) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, true, false>, NT, 0);
-        if (k == 2) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, false, true>, NT, 0);
-        if (k == 3) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, true, true>, NT, 0);
+        if (k == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, JL, FF, false, false>, NT, 0);
+        if (k == 1) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, JL, FF, true, false>, NT, 0);
+        if (k == 2) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, JL, FF, false, true>, NT, 0);
+        if (k == 3) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, JL, FF, true, true>, NT, 0);
         v[k] = b > 0 ? b : 1;
     }
     return v[k];
 }
 
-int occupancy(int cfg, bool nn, bool nbl) {
+template <bool FF>
+int occupancy_ff(int cfg, bool nn, bool nbl) {
     switch (cfg) {
-        case CFG_64x1: return occ_of<64, 1>(nn, nbl);
-        case CFG_128x1: return occ_of<128, 1>(nn, nbl);
-        default: return occ_of<128, 2>(nn, nbl);
+        case CFG_SMALL: return occ_of<512, 1, 8, FF>(nn, nbl);
+        case CFG_MED: return occ_of<256, 1, 2, FF>(nn, nbl);
+        case CFG_128x1: return occ_of<128, 1, 1, FF>(nn, nbl);
+        default: return occ_of<128, 2, 1, FF>(nn, nbl);
     }
 }
 
-template <int NT, int IPT>
+int occupancy(int cfg, bool ff, bool nn, bool nbl) {
+    return ff ? occupancy_ff<true>(cfg, nn, nbl) : occupancy_ff<false>(cfg, nn, nbl);
+}
+
+template <int NT, int IPT, int JL, bool FF>
 void launch_cfg(bool nn, bool nbl, int grid, const G6Args& a, cudaStream_t s) {
-    if (nn && nbl) launch_one<NT, IPT, true, true>(grid, a, s);
-    else if (nn) launch_one<NT, IPT, true, false>(grid, a, s);
-    else if (nbl) launch_one<NT, IPT, false, true>(grid, a, s);
-    else launch_one<NT, IPT, false, false>(grid, a, s);
+    if (nn && nbl) g6_kernel<NT, IPT, JL, FF, true, true><<<grid, NT, 0, s>>>(a);
+    else if (nn) g6_kernel<NT, IPT, JL, FF, true, false><<<grid, NT, 0, s>>>(a);
+    else if (nbl) g6_kernel<NT, IPT, JL, FF, false, true><<<grid, NT, 0, s>>>(a);
+    else g6_kernel<NT, IPT, JL, FF, false, false><<<grid, NT, 0, s>>>(a);
 }
 
-cudaError_t launch_kernel(int cfg, bool nn, bool nbl, int grid, const G6Args& a, cudaStream_t s) {
+template <bool FF>
+void launch_ff(int cfg, bool nn, bool nbl, int grid, const G6Args& a, cudaStream_t s) {
     switch (cfg) {
-        case CFG_64x1: launch_cfg<64, 1>(nn, nbl, grid, a, s); break;
-        case CFG_128x1: launch_cfg<128, 1>(nn, nbl, grid, a, s); break;
-        default: launch_cfg<128, 2>(nn, nbl, grid, a, s); break;
+        case CFG_SMALL: launch_cfg<512, 1, 8, FF>(nn, nbl, grid, a, s); break;
+        case CFG_MED: launch_cfg<256, 1, 2, FF>(nn, nbl, grid, a, s); break;
+        case CFG_128x1: launch_cfg<128, 1, 1, FF>(nn, nbl, grid, a, s); break;
+        default: launch_cfg<128, 2, 1, FF>(nn, nbl, grid, a, s); break;
     }
+}
+
+cudaError_t launch_kernel(int cfg, bool ff, bool nn, bool nbl, int grid, const G6Args& a, cudaStream_t s) {
+    if (ff) launch_ff<true>(cfg, nn, nbl, grid, a, s);
+    else launch_ff<false>(cfg, nn, nbl, grid, a, s);
     return cudaGetLastError();
 }
 
-// Forced configuration for tuning sweeps (PGB_G6_CFG = 0/1/2), else by i count.
+// Relative-coordinate arithmetic of the library's own calls: double-float (default) or FP64
+// subtraction + conversion (PGB_G6_DX=f64), see rel1() in pgb_g6_kernels.cuh.
+bool dx_ff() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = std::getenv("PGB_G6_DX");
+        v = (e && std::strcmp(e, "f64") == 0) ? 0 : 1;
+    }
+    return v == 1;
+}
+
+// Forced configuration for tuning sweeps (PGB_G6_CFG = 0..3), else by i count.
 int pick_cfg(long long ni_max) {
     static int forced = env_int("PGB_G6_CFG", -1, -1, NCFG - 1);
     if (forced >= 0) return forced;
-    if (ni_max <= 64) return CFG_64x1;
-    if (ni_max <= 4096) return CFG_128x1;
-    return CFG_128x2;
+    if (ni_max <= 64) return CFG_SMALL;
+    if (ni_max <= 4096) return CFG_MED;
+    return CFG_LARGE;
 }
 
 // Plan one batch of items ([k][4] = i_off, i_cnt, j_off, j_cnt) for a configuration:
-// about 4 tasks per resident CTA, chunks of at least 128 j.
+// about 4 tasks per resident CTA, chunks of at least 128 j, at most 512 chunks per i-tile
+// (their partial rows are summed by the cooperative reduction of the group's last CTA).
 long long plan_items(std::vector<Task>& tasks, std::vector<Group>& groups, int& rows, int nitem, const int* items,
-                     int cfg, bool nn, bool nbl) {
-    int slots = sm_count(g_device) * occupancy(cfg, nn, nbl);
+                     int cfg, bool ff, bool nn, bool nbl) {
+    int slots = sm_count(g_device) * occupancy(cfg, ff, nn, nbl);
     int itile = cfg_itile(cfg);
     long long work = 0;
     for (int k = 0; k < nitem; k++) {
@@ -150,13 +171,17 @@ long long plan_items(std::vector<Task>& tasks, std::vector<Group>& groups, int& 
         long long tiles = (ni + itile - 1) / itile;
         work += tiles * itile * (long long)items[4 * k + 3];
     }
-    long long per_task = work / (4LL * slots) + 1;
+    // about 4 tasks per resident CTA for load balance; a small call (one i-tile, the drop-in
+    // API's npipes-sized calls) instead gets one wave of one fat task per resident CTA, which
+    // keeps the number of partial rows (the reduction depth) low
+    long long per_task = (cfg == CFG_SMALL) ? work / slots + 1 : work / (4LL * slots) + 1;
     long long inter = 0;
     rows = 0;
     for (int k = 0; k < nitem; k++) {
         int ni = items[4 * k + 1], nj = items[4 * k + 3];
         long long jc = per_task / itile;
         if (jc < 128) jc = 128;
+        if (jc * 512 < nj) jc = (nj + 511) / 512;
         if (jc > nj) jc = nj > 0 ? nj : 1;
         rows += plan_item(tasks, groups, items[4 * k], ni, items[4 * k + 2], nj, itile, (int)jc, rows);
         inter += (long long)ni * nj;
@@ -276,7 +301,7 @@ bool flush_and_predict(int nj) {
     if (nj <= 0) return true;
     if (!grow_j(nj) || !flush_j()) return false;
     PGB_CUDA_OR(g_err, LIB, S.pred.reserve(S.jcap), return false);
-    g6_predict_kernel<<<(nj + 255) / 256, 256, 0, S.stream>>>(S.jd.p, nj, S.ti, S.pred.p);
+    g6_predict_kernel<<<(nj + 255) / 256, 256, 0, S.stream>>>(S.jd.p, nj, S.ti, S.pred.p, dx_ff());
     PGB_CUDA_OR(g_err, LIB, cudaGetLastError(), return false);
     // j-memory is read asynchronously from the pinned mirror: later set_j calls wait for it
     PGB_CUDA_OR(g_err, LIB, cudaStreamSynchronize(S.stream), return false);
@@ -289,7 +314,8 @@ bool run_force(int nj, int ni, float eps2, bool nn, bool nbl) {
     int rows = 0;
     int cfg = pick_cfg(ni);
     int item[4] = {0, ni, 0, nj};
-    plan_items(tasks, groups, rows, 1, item, cfg, nn, nbl);
+    const bool ff = dx_ff();
+    plan_items(tasks, groups, rows, 1, item, cfg, ff, nn, nbl);
     PGB_CUDA_OR(g_err, LIB, S.st.stage(S.stream, tasks, groups, rows, ITILE_MAX, S.ibuf.p, ni), return false);
     PGB_CUDA_OR(g_err, LIB, S.outd.reserve(ni), return false);
     PGB_CUDA_OR(g_err, LIB, S.outh.reserve(ni), return false);
@@ -316,9 +342,9 @@ bool run_force(int nj, int ni, float eps2, bool nn, bool nbl) {
         a.nb_list = S.nbl_d.p;
     }
     if (a.ntasks == 0) return true;
-    int slots = sm_count(g_device) * occupancy(cfg, nn, nbl);
+    int slots = sm_count(g_device) * occupancy(cfg, ff, nn, nbl);
     int grid = a.ntasks < slots ? a.ntasks : slots;
-    PGB_CUDA_OR(g_err, LIB, launch_kernel(cfg, nn, nbl, grid, a, S.stream), return false);
+    PGB_CUDA_OR(g_err, LIB, launch_kernel(cfg, ff, nn, nbl, grid, a, S.stream), return false);
     return true;
 }
 
@@ -374,9 +400,7 @@ int lasthalf_impl(int nj, int ni, const int* pidx, const double (*pos)[3], const
     }
     for (int i = 0; i < ni; i++) {
         G6I& r = S.ibuf.p[i];
-        r.x = pos[i][0];
-        r.y = pos[i][1];
-        r.z = pos[i][2];
+        store_pos(r.p, pos[i][0], pos[i][1], pos[i][2], dx_ff());
         r.vx = (float)vel[i][0];
         r.vy = (float)vel[i][1];
         r.vz = (float)vel[i][2];
@@ -632,6 +656,7 @@ PGB_EXPORT void pgb6_record_sizes(int* ptcl, int* predj, int* irec, int* out) {
 struct pgb6_plan {
     int cfg;
     bool nn;
+    bool ff;
     std::vector<Task> tasks;
     std::vector<Group> groups;
     int rows = 0;
@@ -639,10 +664,11 @@ struct pgb6_plan {
     Stager<G6I, G6Out> st;
 };
 
-enum { PGB6_NN = 1 };
+enum { PGB6_NN = 1, PGB6_POS_F64 = 2 };
 
 // items: [nitem][4] = (i_offset, i_count, j_offset, j_count) into the i- and j-arrays.
-// flags: PGB6_NN (1) also computes the nearest neighbour (key, j address).
+// flags: PGB6_NN (1) also computes the nearest neighbour (key, j address); PGB6_POS_F64 (2):
+// the i/j records hold FP64 positions (default: double-float positions, see Pos3).
 PGB_EXPORT int pgb6_plan_create(pgb6_plan** out, int nitem, const int* items, int flags) {
     if (!out || nitem < 0 || (nitem && !items)) {
         raise(g_err, LIB, PGB_ERR_ARG, "pgb6_plan_create: bad arguments");
@@ -656,13 +682,14 @@ PGB_EXPORT int pgb6_plan_create(pgb6_plan** out, int nitem, const int* items, in
     if (!ensure_device()) return PGB_ERR_NOGPU;
     auto* P = new pgb6_plan();
     P->nn = (flags & PGB6_NN) != 0;
+    P->ff = (flags & PGB6_POS_F64) == 0;
     long long nimax = 0;
     for (int k = 0; k < nitem; k++) nimax = std::max<long long>(nimax, items[4 * k + 1]);
     // many small items fill the GPU with short tiles; large ones prefer 2 i per thread
     long long total_i = 0;
     for (int k = 0; k < nitem; k++) total_i += items[4 * k + 1];
     P->cfg = pick_cfg(nitem > 1 ? std::max<long long>(nimax, total_i / 4) : nimax);
-    P->interactions = plan_items(P->tasks, P->groups, P->rows, nitem, items, P->cfg, P->nn, false);
+    P->interactions = plan_items(P->tasks, P->groups, P->rows, nitem, items, P->cfg, P->ff, P->nn, false);
     cudaStream_t s = nullptr;
     bool ok = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess;
     ok = ok && P->st.stage(s, P->tasks, P->groups, P->rows, ITILE_MAX, (const G6I*)nullptr, 0) == cudaSuccess;
@@ -710,9 +737,9 @@ PGB_EXPORT int pgb6_plan_launch(pgb6_plan* P, const void* ipart, const void* jpr
     a.nb_count = nullptr;
     a.nb_list = nullptr;
     a.nb_maxlen = 0;
-    int slots = sm_count(g_device) * occupancy(P->cfg, P->nn, false);
+    int slots = sm_count(g_device) * occupancy(P->cfg, P->ff, P->nn, false);
     int grid = a.ntasks < slots ? a.ntasks : slots;
-    PGB_CUDA_OR(g_err, LIB, launch_kernel(P->cfg, P->nn, false, grid, a, s), return PGB_ERR_CUDA);
+    PGB_CUDA_OR(g_err, LIB, launch_kernel(P->cfg, P->ff, P->nn, false, grid, a, s), return PGB_ERR_CUDA);
     return PGB_OK;
 }
 
@@ -724,14 +751,16 @@ PGB_EXPORT void pgb6_plan_destroy(pgb6_plan* P) {
 }
 
 // FP64 predictor on device records: pred[j] = predict(ptcl[j], ti) for j < nj.
-PGB_EXPORT int pgb6_predict(const void* ptcl, int nj, double ti, void* pred, void* stream) {
+// flags: PGB6_POS_F64 (2) writes FP64 positions, else the double-float layout.
+PGB_EXPORT int pgb6_predict(const void* ptcl, int nj, double ti, void* pred, int flags, void* stream) {
     if (nj < 0 || (nj > 0 && (!ptcl || !pred))) {
         raise(g_err, LIB, PGB_ERR_ARG, "pgb6_predict: bad arguments");
         return PGB_ERR_ARG;
     }
     if (!ensure_device()) return PGB_ERR_NOGPU;
     if (nj == 0) return PGB_OK;
-    g6_predict_kernel<<<(nj + 255) / 256, 256, 0, (cudaStream_t)stream>>>((const G6Ptcl*)ptcl, nj, ti, (G6PredJ*)pred);
+    g6_predict_kernel<<<(nj + 255) / 256, 256, 0, (cudaStream_t)stream>>>((const G6Ptcl*)ptcl, nj, ti, (G6PredJ*)pred,
+                                                                           (flags & PGB6_POS_F64) == 0);
     PGB_CUDA_OR(g_err, LIB, cudaGetLastError(), return PGB_ERR_CUDA);
     return PGB_OK;
 }
@@ -779,7 +808,7 @@ PGB_EXPORT int pgb6_batch_host(int nitem, const int* items, int ni, const double
     PGB_CUDA_OR(g_err, LIB, HB.od.reserve(ni + 1), return PGB_ERR_CUDA);
     for (int i = 0; i < ni; i++) {
         G6I& r = HB.ih.p[i];
-        r.x = xi[i][0]; r.y = xi[i][1]; r.z = xi[i][2];
+        store_pos(r.p, xi[i][0], xi[i][1], xi[i][2], dx_ff());
         r.vx = (float)vi[i][0]; r.vy = (float)vi[i][1]; r.vz = (float)vi[i][2];
         r.id = idi[i];
         r.h2 = 0.f;
@@ -787,7 +816,7 @@ PGB_EXPORT int pgb6_batch_host(int nitem, const int* items, int ni, const double
     }
     for (int j = 0; j < nj; j++) {
         G6PredJ& r = HB.jh.p[j];
-        r.x = xj[j][0]; r.y = xj[j][1]; r.z = xj[j][2];
+        store_pos(r.p, xj[j][0], xj[j][1], xj[j][2], dx_ff());
         r.vx = (float)vj[j][0]; r.vy = (float)vj[j][1]; r.vz = (float)vj[j][2];
         r.m = (float)mj[j];
         r.id = idj[j];
@@ -798,7 +827,7 @@ PGB_EXPORT int pgb6_batch_host(int nitem, const int* items, int ni, const double
     PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(HB.jd.p, HB.jh.p, (size_t)nj * sizeof(G6PredJ), cudaMemcpyHostToDevice, HB.s),
                 return PGB_ERR_CUDA);
     pgb6_plan* P = nullptr;
-    int rc = pgb6_plan_create(&P, nitem, items, (nnb || rnnb) ? PGB6_NN : 0);
+    int rc = pgb6_plan_create(&P, nitem, items, ((nnb || rnnb) ? PGB6_NN : 0) | (dx_ff() ? 0 : PGB6_POS_F64));
     if (rc) return rc;
     rc = pgb6_plan_launch(P, HB.id.p, HB.jd.p, eps2, HB.od.p, HB.s);
     if (!rc && ni > 0)

@@ -25,10 +25,17 @@ struct G6Ptcl {
     int idx, pad[3];
 };
 
+// A position as stored for the force kernel: FP64 (x, y, z), or -- the layout of the kernel's
+// double-float variant -- a pair of floats per coordinate, hi = fl32(x), lo = fl32(x - hi),
+// which represents x to ~2^-48 relative.
+union __align__(8) Pos3 {
+    struct { double x, y, z; } d;
+    struct { float xh, yh, zh, xl, yl, zl; } f;
+};
+
 // Predicted j record in HBM and shared memory: 48 bytes, three 16-byte words.
 struct __align__(16) G6PredJ {
-    double x, y;          // word 0
-    double z;             // word 1
+    Pos3 p;               // words 0-1
     float m;
     int id;
     float vx, vy, vz;     // word 2
@@ -37,14 +44,29 @@ struct __align__(16) G6PredJ {
 
 // i-particle record: 48 bytes.
 struct __align__(16) G6I {
-    double x, y;
-    double z;
-    float vx, vy;
-    float vz;
+    Pos3 p;
+    float vx, vy, vz;
     int id;
     float h2;             // neighbour radius^2 (0: no neighbours)
     float pad;
 };
+
+__host__ __device__ inline void split_ff(double x, float& hi, float& lo) {
+    hi = (float)x;
+    lo = (float)(x - (double)hi);
+}
+
+__host__ __device__ inline void store_pos(Pos3& p, double x, double y, double z, bool ff) {
+    if (ff) {
+        split_ff(x, p.f.xh, p.f.xl);
+        split_ff(y, p.f.yh, p.f.yl);
+        split_ff(z, p.f.zh, p.f.zl);
+    } else {
+        p.d.x = x;
+        p.d.y = y;
+        p.d.z = z;
+    }
+}
 
 // Per-i result (final or partial).  key/jadr: nearest-neighbour key and j address.
 struct __align__(16) G6Out {
@@ -74,16 +96,18 @@ struct G6Args {
 };
 
 // FP64 predictor: one thread per j (gravity.c:149-193; velocity stored as float, :168-173).
-__global__ void g6_predict_kernel(const G6Ptcl* __restrict__ p, int nj, double ti, G6PredJ* __restrict__ out) {
+// ff: store the predicted position in the double-float layout.
+__global__ void g6_predict_kernel(const G6Ptcl* __restrict__ p, int nj, double ti, G6PredJ* __restrict__ out,
+                                  bool ff) {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= nj) return;
     const G6Ptcl& P = p[j];
     double dt = ti - P.tim;
     double dt2 = dt * dt, dt3 = dt2 * dt;
     G6PredJ o;
-    o.x = P.pos[0] + P.vel[0] * dt + P.acc2[0] * dt2 + P.jrk6[0] * dt3;
-    o.y = P.pos[1] + P.vel[1] * dt + P.acc2[1] * dt2 + P.jrk6[1] * dt3;
-    o.z = P.pos[2] + P.vel[2] * dt + P.acc2[2] * dt2 + P.jrk6[2] * dt3;
+    store_pos(o.p, P.pos[0] + P.vel[0] * dt + P.acc2[0] * dt2 + P.jrk6[0] * dt3,
+              P.pos[1] + P.vel[1] * dt + P.acc2[1] * dt2 + P.jrk6[1] * dt3,
+              P.pos[2] + P.vel[2] * dt + P.acc2[2] * dt2 + P.jrk6[2] * dt3, ff);
     o.vx = (float)(P.vel[0] + 2.0 * P.acc2[0] * dt + 3.0 * P.jrk6[0] * dt2);
     o.vy = (float)(P.vel[1] + 2.0 * P.acc2[1] * dt + 3.0 * P.jrk6[1] * dt2);
     o.vz = (float)(P.vel[2] + 2.0 * P.acc2[2] * dt + 3.0 * P.jrk6[2] * dt2);
@@ -106,13 +130,31 @@ struct G6Acc {
     float ax, ay, az, jx, jy, jz, pot;
 };
 
-template <bool NN, bool NBL>
-__device__ __forceinline__ void g6_pair(const G6PredJ& J, int jadr, double xi, double yi, double zi, float vxi,
+// x_j - x_i rounded to FP32.  FP64 layout: an FP64 subtraction and a conversion (DADD + F2F,
+// the reference's own split, gravity.c:316-333).  Double-float layout: (xjh - xih) + (xjl - xil)
+// in FP32 -- the hi difference is exact whenever the two positions are within a factor 2
+// (Sterbenz), i.e. for every close pair, so the result is fl32(x_j - x_i) to within 1 ulp,
+// with three FP32 adds instead of an FP64 add and an F2F on the XU pipe shared with MUFU.
+template <bool FF>
+__device__ __forceinline__ float rel1(const Pos3& j, const Pos3& i, int c) {
+    if constexpr (FF) {
+        const float* jf = &j.f.xh;
+        const float* iff = &i.f.xh;
+        return __fadd_rn(__fsub_rn(jf[c], iff[c]), __fsub_rn(jf[c + 3], iff[c + 3]));
+    } else {
+        const double* jd = &j.d.x;
+        const double* id = &i.d.x;
+        return __double2float_rn(jd[c] - id[c]);
+    }
+}
+
+template <bool FF, bool NN, bool NBL>
+__device__ __forceinline__ void g6_pair(const G6PredJ& J, int jadr, const Pos3& I, float vxi,
                                         float vyi, float vzi, int idi, float eps2, float hinv, G6Acc& a,
                                         float& kmin, int& kadr, int* nbc, int* nbl, int nbmax) {
-    float dx = __double2float_rn(J.x - xi);
-    float dy = __double2float_rn(J.y - yi);
-    float dz = __double2float_rn(J.z - zi);
+    float dx = rel1<FF>(J.p, I, 0);
+    float dy = rel1<FF>(J.p, I, 1);
+    float dz = rel1<FF>(J.p, I, 2);
     float dvx = J.vx - vxi, dvy = J.vy - vyi, dvz = J.vz - vzi;
     float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmaf_rn(dx, dx, eps2)));
     float q = minus2_over_r(r2);
@@ -172,17 +214,44 @@ __device__ __forceinline__ G6Out ldcg_out(const G6Out* p) {
     return v;
 }
 
-template <int NT, int IPT, bool NN, bool NBL>
+// (key, j address) order of the nearest-neighbour search: smaller key, ties to the smaller
+// address -- independent of the order in which partial results are combined.
+__device__ __forceinline__ bool nn_better(float k1, int a1, float k0, int a0) {
+    return k1 < k0 || (k1 == k0 && (unsigned)a1 < (unsigned)a0);
+}
+
+__device__ __forceinline__ void out_add(G6Out& s, const G6Out& v) {
+    s.ax += v.ax; s.ay += v.ay; s.az += v.az;
+    s.jx += v.jx; s.jy += v.jy; s.jz += v.jz;
+    s.pot += v.pot;
+    if (nn_better(v.key, v.jadr, s.key, s.jadr)) {
+        s.key = v.key;
+        s.jadr = v.jadr;
+    }
+}
+
+// Thread layout of a CTA: NT threads = JL j-lanes x ISL i-slots (ISL = NT/JL, whole warps per
+// lane so that the shared-memory j reads stay warp-broadcasts).  A thread owns IPT i-particles
+// li = slot + k*ISL of the task's i-tile (ITILE = ISL*IPT) and every JL-th j of each j-tile.
+// The j-lanes are summed in lane order through shared memory at the end of the task.
+template <int NT, int IPT, int JL, bool FF, bool NN, bool NBL>
 __global__ void __launch_bounds__(NT) g6_kernel(G6Args A) {
-    __shared__ G6PredJ sj[NT];
+    static_assert(JL == 1 || IPT == 1, "j-lanes are used with one i per thread");
+    constexpr int ISL = NT / JL;
+    // j tile during the loop, per-thread results (G6Out) after it
+    __shared__ __align__(16) unsigned char smem[NT * sizeof(G6Out)];
+    G6PredJ* sj = reinterpret_cast<G6PredJ*>(smem);
+    G6Out* red = reinterpret_cast<G6Out*>(smem);
     __shared__ int s_task, s_flag;
+    const int slot = threadIdx.x % ISL;
+    const int jl = threadIdx.x / ISL;
 
     for (;;) {
         int t = next_task(A.task_counter, &s_task);
         if (t >= A.ntasks) break;
         const Task T = A.tasks[t];
 
-        double xi[IPT], yi[IPT], zi[IPT];
+        Pos3 pi[IPT];
         float vxi[IPT], vyi[IPT], vzi[IPT], hinv[IPT];
         int idi[IPT];
         double S[IPT][7];
@@ -190,10 +259,10 @@ __global__ void __launch_bounds__(NT) g6_kernel(G6Args A) {
         int kadr[IPT];
 #pragma unroll
         for (int k = 0; k < IPT; k++) {
-            int li = threadIdx.x + k * NT;
+            int li = slot + k * ISL;
             int ii = T.i0 + (li < T.ni ? li : 0);
             const G6I P = A.ipart[ii];
-            xi[k] = P.x; yi[k] = P.y; zi[k] = P.z;
+            pi[k] = P.p;
             vxi[k] = P.vx; vyi[k] = P.vy; vzi[k] = P.vz;
             idi[k] = P.id;
             // gravity.c:688-695: -2/h, or -1e10 when h2 == 0 (no neighbours); padding lanes none
@@ -213,14 +282,14 @@ __global__ void __launch_bounds__(NT) g6_kernel(G6Args A) {
 #pragma unroll
             for (int k = 0; k < IPT; k++) a[k] = G6Acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll 2
-            for (int j = 0; j < nt; j++) {
+            for (int j = jl; j < nt; j += JL) {
                 const G6PredJ J = sj[j];
                 const int jadr = T.j0 + jt + j;
 #pragma unroll
                 for (int k = 0; k < IPT; k++) {
-                    int li = threadIdx.x + k * NT;
+                    int li = slot + k * ISL;
                     int gi = T.i0 + (li < T.ni ? li : 0);
-                    g6_pair<NN, NBL>(J, jadr, xi[k], yi[k], zi[k], vxi[k], vyi[k], vzi[k], idi[k], A.eps2, hinv[k],
+                    g6_pair<FF, NN, NBL>(J, jadr, pi[k], vxi[k], vyi[k], vzi[k], idi[k], A.eps2, hinv[k],
                                      a[k], kmin[k], kadr[k], NBL ? A.nb_count + gi : nullptr,
                                      NBL ? A.nb_list + (size_t)gi * A.nb_maxlen : nullptr, A.nb_maxlen);
                 }
@@ -240,36 +309,51 @@ __global__ void __launch_bounds__(NT) g6_kernel(G6Args A) {
         G6Out* dst_row = (T.group < 0) ? nullptr : A.partial + (size_t)T.slot * A.itile;
 #pragma unroll
         for (int k = 0; k < IPT; k++) {
-            int li = threadIdx.x + k * NT;
-            if (li >= T.ni) continue;
             G6Out o;
             o.ax = S[k][0]; o.ay = S[k][1]; o.az = S[k][2];
             o.jx = S[k][3]; o.jy = S[k][4]; o.jz = S[k][5];
             o.pot = S[k][6];
             o.key = kmin[k];
             o.jadr = kadr[k];
+            if constexpr (JL > 1) {
+                // sum the j-lanes in lane order (lane 0 holds the CTA's result afterwards)
+                __syncthreads();
+                red[threadIdx.x] = o;
+                __syncthreads();
+                if (jl != 0) continue;
+                for (int l = 1; l < JL; l++) out_add(o, red[slot + l * ISL]);
+            }
+            int li = slot + k * ISL;
+            if (li >= T.ni) continue;
             if (dst_row) dst_row[li] = o;
             else A.out[T.i0 + li] = g6_finish(o);
         }
         if (!dst_row) continue;
         const Group G = A.groups[T.group];
         if (group_arrive(A.group_counters, T.group, G.nchunk, &s_flag)) {
-#pragma unroll
-            for (int k = 0; k < IPT; k++) {
-                int li = threadIdx.x + k * NT;
-                if (li >= G.ni) continue;
-                G6Out s = ldcg_out(A.partial + (size_t)G.slot0 * A.itile + li);
-                for (int c = 1; c < G.nchunk; c++) {
-                    G6Out v = ldcg_out(A.partial + (size_t)(G.slot0 + c) * A.itile + li);
-                    s.ax += v.ax; s.ay += v.ay; s.az += v.az;
-                    s.jx += v.jx; s.jy += v.jy; s.jz += v.jz;
-                    s.pot += v.pot;
-                    if (v.key < s.key) {  // strict: the earlier chunk (smaller j) wins ties
-                        s.key = v.key;
-                        s.jadr = v.jadr;
-                    }
+            // Cooperative reduction of the group's partial rows: P threads per i, each summing a
+            // fixed strided subset of rows, then the P partial sums in thread order
+            // (deterministic for a given group shape).
+            int P = 1;
+            while (P * 2 * G.ni <= NT) P *= 2;
+            const int per = NT / P;
+            for (int base = 0; base < G.ni; base += per) {
+                const int li = base + threadIdx.x / P, p = threadIdx.x % P;
+                G6Out s;
+                s.ax = s.ay = s.az = s.jx = s.jy = s.jz = s.pot = 0.0;
+                s.key = INFINITY;
+                s.jadr = -1;
+                if (li < G.ni) {
+                    const G6Out* col = A.partial + (size_t)G.slot0 * A.itile + li;
+                    for (int c = p; c < G.nchunk; c += P) out_add(s, ldcg_out(col + (size_t)c * A.itile));
                 }
-                A.out[G.i0 + li] = g6_finish(s);
+                __syncthreads();
+                red[threadIdx.x] = s;
+                __syncthreads();
+                if (p == 0 && li < G.ni) {
+                    for (int q = 1; q < P; q++) out_add(s, red[threadIdx.x + q]);
+                    A.out[G.i0 + li] = g6_finish(s);
+                }
             }
         }
     }

@@ -200,6 +200,7 @@ class G6(_ErrMixin):
 
     prefix = "pgb6"
     NN = 1
+    POS_F64 = 2
 
     def __init__(self):
         L = self.L = _load("libpg6.so")
@@ -230,7 +231,7 @@ class G6(_ErrMixin):
         _sig(L, "pgb6_plan_interactions", [vp], C.c_longlong)
         _sig(L, "pgb6_plan_tasks", [vp], C.c_int)
         _sig(L, "pgb6_plan_config", [vp], C.c_int)
-        _sig(L, "pgb6_predict", [vp, C.c_int, C.c_double, vp, vp], C.c_int)
+        _sig(L, "pgb6_predict", [vp, C.c_int, C.c_double, vp, C.c_int, vp], C.c_int)
         _sig(L, "pgb6_batch_host", [C.c_int, ip, C.c_int, dp, dp, ip, C.c_int, dp, dp, dp, ip, C.c_double,
                                     dp, dp, dp, ip, fp], C.c_int)
         sz = [C.c_int() for _ in range(4)]
@@ -303,10 +304,12 @@ class G6(_ErrMixin):
             raise RuntimeError(f"pgb6_batch_host failed: {self.last_error()}")
         return dict(acc=acc, jrk=jrk, pot=pot, nnb=nnb, rnnb=rnnb)
 
-    def plan_create(self, items, nn=True):
+    def plan_create(self, items, nn=True, f64=False):
+        """f64: the device records hold FP64 positions (else the double-float layout)."""
         items = np.ascontiguousarray(items, dtype=np.int32).reshape(-1, 4)
         h = vp()
-        rc = self.L.pgb6_plan_create(C.byref(h), len(items), ptr(items, C.c_int), self.NN if nn else 0)
+        flags = (self.NN if nn else 0) | (self.POS_F64 if f64 else 0)
+        rc = self.L.pgb6_plan_create(C.byref(h), len(items), ptr(items, C.c_int), flags)
         if rc:
             raise RuntimeError(f"pgb6_plan_create failed: {self.last_error()}")
         return h
@@ -323,10 +326,51 @@ class G6(_ErrMixin):
 # Device record layouts (must match csrc/pgb_g6_kernels.cuh), as numpy structured dtypes.
 G6PTCL = np.dtype([("pos", "<f8", 3), ("vel", "<f8", 3), ("acc2", "<f8", 3), ("jrk6", "<f8", 3),
                    ("mass", "<f8"), ("tim", "<f8"), ("idx", "<i4"), ("pad", "<i4", 3)])
+# Positions: FP64 layout (x, y, z doubles) or the double-float layout (xh, yh, zh, xl, yl, zl
+# floats, x = xh + xl) selected by the plan's PGB6_POS_F64 flag.
 G6PREDJ = np.dtype([("x", "<f8"), ("y", "<f8"), ("z", "<f8"), ("m", "<f4"), ("id", "<i4"),
                     ("vx", "<f4"), ("vy", "<f4"), ("vz", "<f4"), ("pad", "<f4")])
 G6IREC = np.dtype([("x", "<f8"), ("y", "<f8"), ("z", "<f8"), ("vx", "<f4"), ("vy", "<f4"),
                    ("vz", "<f4"), ("id", "<i4"), ("h2", "<f4"), ("pad", "<f4")])
+_FF = [("xh", "<f4"), ("yh", "<f4"), ("zh", "<f4"), ("xl", "<f4"), ("yl", "<f4"), ("zl", "<f4")]
+G6PREDJ_FF = np.dtype(_FF + [("m", "<f4"), ("id", "<i4"), ("vx", "<f4"), ("vy", "<f4"), ("vz", "<f4"),
+                             ("pad", "<f4")])
+G6IREC_FF = np.dtype(_FF + [("vx", "<f4"), ("vy", "<f4"), ("vz", "<f4"), ("id", "<i4"), ("h2", "<f4"),
+                            ("pad", "<f4")])
+
+
+def _set_pos(rec, pos, ff):
+    pos = np.asarray(pos, np.float64)
+    for k, c in enumerate("xyz"):
+        if ff:
+            hi = pos[:, k].astype(np.float32)
+            rec[c + "h"] = hi
+            rec[c + "l"] = (pos[:, k] - hi.astype(np.float64)).astype(np.float32)
+        else:
+            rec[c] = pos[:, k]
+
+
+def g6_irecords(pos, vel, ids, h2=None, ff=True):
+    """i-particle records (G6I) as a numpy structured array."""
+    rec = np.zeros(len(pos), G6IREC_FF if ff else G6IREC)
+    _set_pos(rec, pos, ff)
+    for k, c in enumerate("xyz"):
+        rec["v" + c] = np.asarray(vel)[:, k]
+    rec["id"] = ids
+    if h2 is not None:
+        rec["h2"] = h2
+    return rec
+
+
+def g6_jrecords(pos, vel, mass, ids, ff=True):
+    """predicted j records (G6PredJ) as a numpy structured array."""
+    rec = np.zeros(len(pos), G6PREDJ_FF if ff else G6PREDJ)
+    _set_pos(rec, pos, ff)
+    for k, c in enumerate("xyz"):
+        rec["v" + c] = np.asarray(vel)[:, k]
+    rec["m"] = mass
+    rec["id"] = ids
+    return rec
 G6OUT = np.dtype([("ax", "<f8"), ("ay", "<f8"), ("az", "<f8"), ("jx", "<f8"), ("jy", "<f8"),
                   ("jz", "<f8"), ("pot", "<f8"), ("key", "<f4"), ("jadr", "<i4")])
 

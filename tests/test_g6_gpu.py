@@ -194,28 +194,22 @@ def test_batched_clusters_vs_fp64(g6):
         check_nn({"nnb": res["nnb"][s], "rnnb": res["rnnb"][s]}, ref)
 
 
-def test_device_plan_graph_capture(g6):
-    """The batched plan launches from a captured CUDA graph and replays with identical bits."""
+@pytest.mark.parametrize("ff", [True, False])
+def test_device_plan_graph_capture(g6, ff):
+    """The batched plan launches from a captured CUDA graph and replays with identical bits, for
+    both position layouts; both layouts agree with the FP64 oracle."""
     import torch
     cs = W.cluster_set(ncl=6, nmin=100, nmax=2000, seed=123)
     n = len(cs.mass)
     idx = np.arange(n, dtype=np.int32)
-    irec = np.zeros(n, pgb.ffi.G6IREC)
-    jrec = np.zeros(n, pgb.ffi.G6PREDJ)
-    for k, name in enumerate("xyz"):
-        irec[name] = cs.pos[:, k]
-        jrec[name] = cs.pos[:, k]
-        irec["v" + name] = cs.vel[:, k]
-        jrec["v" + name] = cs.vel[:, k]
-    irec["id"] = idx
-    jrec["id"] = idx
-    jrec["m"] = cs.mass
+    irec = pgb.ffi.g6_irecords(cs.pos, cs.vel, idx, ff=ff)
+    jrec = pgb.ffi.g6_jrecords(cs.pos, cs.vel, cs.mass, idx, ff=ff)
     dev = torch.device("cuda")
     d_i = torch.from_numpy(irec.view(np.uint8)).to(dev)
     d_j = torch.from_numpy(jrec.view(np.uint8)).to(dev)
     d_o = torch.zeros(n * pgb.ffi.G6OUT.itemsize, dtype=torch.uint8, device=dev)
     items = np.stack([cs.offsets[:-1], cs.sizes, cs.offsets[:-1], cs.sizes], 1)
-    plan = g6.plan_create(items, nn=True)
+    plan = g6.plan_create(items, nn=True, f64=not ff)
     try:
         s = torch.cuda.Stream()
         with torch.cuda.stream(s):
@@ -232,5 +226,12 @@ def test_device_plan_graph_capture(g6):
         again = d_o.cpu().numpy().view(pgb.ffi.G6OUT)
         assert first.tobytes() == again.tobytes()
         del graph
+        vf = cs.vel.astype(np.float32).astype(np.float64)
+        mf = cs.mass.astype(np.float32).astype(np.float64)
+        for c in range(len(cs.sizes)):
+            sl = slice(cs.offsets[c], cs.offsets[c + 1])
+            ref = O.g6_force(cs.pos[sl], vf[sl], idx[sl], np.float32(cs.eps2), cs.pos[sl], vf[sl], mf[sl], idx[sl])
+            acc = np.stack([first["ax"][sl], first["ay"][sl], first["az"][sl]], 1)
+            assert rms(rel(acc, ref["acc"])) <= 1e-6
     finally:
         g6.plan_destroy(plan)
