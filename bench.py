@@ -326,6 +326,23 @@ def run_hermite(args, pgb, ws, rank, local):
     with torch.cuda.stream(s):
         step_launches()
     s.synchronize()
+    tuned = {}
+    if not args.no_tune and not args.profile_largest:
+        # autotune the kernel configuration once per active-set size, on the real data
+        for c in range(len(sets)):
+            if len(sets[c]) in tuned:
+                continue
+            g6.L.pgb6_predict(d_ptcl.data_ptr(), n, float(wl["t_calls"][c]), d_pred.data_ptr(), pflags,
+                              s.cuda_stream)
+            cfg, ms = g6.plan_tune(plans[c], d_irec.data_ptr(), d_pred.data_ptr(), st.eps2, d_out.data_ptr(),
+                                   s.cuda_stream)
+            tuned[len(sets[c])] = cfg
+        for c in range(len(sets)):   # re-create the plans so that every plan picks up its tuned shape
+            g6.plan_destroy(plans[c])
+            plans[c] = g6.plan_create([[int(off[c]), len(sets[c]), 0, n]], nn=True, f64=not ff)
+        with torch.cuda.stream(s):
+            step_launches()
+        s.synchronize()
     if args.profile_largest:
         # profiling target: after the warm pass above (1 + 64 force launches), the largest call's
         # force launch three times; nothing else allocated, no timing
@@ -448,10 +465,267 @@ def run_hermite(args, pgb, ws, rank, local):
                 "g6calc_lasthalf2p per npipes chunk, g6_set_j_particle of the active set), host buffers",
                 "npipes": npipe, "steps": e2e_steps},
         "gpu_launches": args.steps * 2 * len(sets),
+        "autotune": {str(k): int(v) for k, v in sorted(tuned.items())},
         "clocks": clk,
         "cpu_baseline": cpu,
     }
     return line
+
+
+# ----------------------------------------------------------------------------------------
+# other workloads (PG5 direct, PG5 table / TreePM, independent Hermite clusters)
+
+def _timed_launches(torch, s, launch, steps, warmup, flush):
+    for _ in range(warmup):
+        with torch.cuda.stream(s):
+            launch()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for k in range(steps):
+        with torch.cuda.stream(s):
+            ev[k][0].record(s)
+            launch()
+            ev[k][1].record(s)
+            flush.fill_(k & 0xFF)
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) / 1e3 for a, b in ev]
+
+
+def _line(args, ws, metric, value, t_step, pairs, flop, workload, dtype, achieved_tf, clk, e2e, cpu, launches,
+          extra=None, kernel=""):
+    pk = peaks()
+    sm_mhz = clk.get("sm_mhz") or pk.get("sm_max_mhz", 1965.0)
+    peak_tf = SM_COUNT * FP32_LANES * 2 * sm_mhz * 1e6 / 1e12
+    line = {
+        "metric": metric, "value": round(value, 2), "unit": "Gint/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(t_step * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": dtype, "data": "synthetic (seeded; no dataset)",
+        "config": {"workload": workload, "pairs_per_step": pairs, "flop_per_pair": flop,
+                   "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{ws}"},
+        "frac_fp32": round(value * 1e9 * flop / 1e12 / peak_tf, 4),
+        "roofline": {"bound": "fp32", "achieved": round(achieved_tf, 2), "peak": round(peak_tf, 2), "unit": "TFLOP/s",
+                     "frac": round(achieved_tf / peak_tf, 4), "traffic": None, "kernel": kernel,
+                     "peak_source": f"148 SM x 128 FP32 lanes x 2 x median SM clock {sm_mhz:.0f} MHz"},
+        "e2e": e2e, "gpu_launches": launches, "clocks": clk, "cpu_baseline": cpu,
+    }
+    if extra:
+        line.update(extra)
+    return line
+
+
+def run_direct(args, pgb, ws, rank, local):
+    """PG5 newton direct sum, N=16384 Plummer (eps=0.01), all i against all j (38 flop/pair)."""
+    import torch
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    W = pgb.workloads
+    g5 = pgb.ffi.G5()
+    g5.L.g5_open()
+    st = W.plummer_g5(16384, seed=W.SEED0 + rank)
+    n = len(st.m)
+    ipos = np.concatenate([st.x, np.full((n, 1), st.eps ** 2)], 1).astype(np.float32)
+    jpos = np.concatenate([st.x, st.m[:, None]], 1).astype(np.float32)
+    d_i = torch.from_numpy(ipos).to(dev)
+    d_j = torch.from_numpy(jpos).to(dev)
+    d_o = torch.zeros((n, 4), dtype=torch.float64, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    plan = g5.plan_create(g5.NEWTON, [[0, n, 0, n]])
+    s = torch.cuda.Stream(device=dev)
+    launch = lambda: g5.plan_launch(plan, d_i.data_ptr(), d_j.data_ptr(), None, d_o.data_ptr(), s.cuda_stream)  # noqa
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(ws)
+    ts = _timed_launches(torch, s, launch, max(args.steps, 50), args.warmup, flush)
+    barrier(ws)
+    clk = clocks.stop()
+    t_local = sum(ts)
+    t_max = reduce_max(t_local, ws, dev)
+    pairs = n * n
+    value = reduce_sum(float(pairs) * len(ts), ws, dev) / t_max / 1e9
+    achieved = pairs * len(ts) * 38 / t_local / 1e12
+    drv = Driver(pgb)
+    h = drv.L.g5drv_open(pgb.ffi.lib_path("libpg5.so").encode())
+    acc = np.zeros((n, 3))
+    pot = np.zeros(n)
+    x = np.ascontiguousarray(st.x)
+    m = np.ascontiguousarray(st.m)
+    drv.L.g5drv_direct(h, n, Driver.p(x), Driver.p(m), st.eps, Driver.p(acc), Driver.p(pot))
+    e2e_t = sum(drv.L.g5drv_direct(h, n, Driver.p(x), Driver.p(m), st.eps, Driver.p(acc), Driver.p(pot))
+                for _ in range(args.e2e_steps * 5))
+    e2e_val = reduce_sum(float(pairs) * args.e2e_steps * 5, ws, dev) / reduce_max(e2e_t, ws, dev) / 1e9
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        path = ref_lib("libpg5_ref.so")
+        if path:
+            hr = drv.L.g5drv_open(path.encode())
+            drv.L.g5drv_direct(hr, n, Driver.p(x), Driver.p(m), st.eps, Driver.p(acc), Driver.p(pot))
+            reps = 3
+            tr = sum(drv.L.g5drv_direct(hr, n, Driver.p(x), Driver.p(m), st.eps, Driver.p(acc), Driver.p(pot))
+                     for _ in range(reps))
+            cpu = {"value": pairs * reps / tr / 1e9, "unit": "Gint/s", "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"{reps} full evaluations, PG5/newton/libpg5 AVX2 + OpenMP (g5_calculate_force_on_x)"}
+    g5.plan_destroy(plan)
+    return _line(args, ws, "Gint/s (PG5 newton direct sum, batched)", value, t_max / len(ts), pairs, 38,
+                 "PG5 newton N=16384 Plummer eps=0.01, all i vs all j (acc + pot)", "f32 (f64 cross-tile sums)",
+                 achieved, clk,
+                 {"value": round(e2e_val, 2), "unit": "Gint/s", "h2d_bytes_per_step": n * 16 * 2,
+                  "d2h_bytes_per_step": n * 32, "api": "g5_set_xmj + g5_set_eps_to_all + g5_set_n + "
+                  "g5_calculate_force_on_x (direct.c:133-176), host buffers"},
+                 cpu, len(ts), kernel="pgb::g5_kernel<NEWTON,128,4>")
+
+
+def run_clusters(args, pgb, ws, rank, local):
+    """1024 independent Plummer clusters, N log-uniform in [256, 16384], one Hermite force+jerk+pot+NN
+    evaluation each: one batched launch vs 1024 sequences of plain g6 calls."""
+    import torch
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    W = pgb.workloads
+    ffi = pgb.ffi
+    g6 = ffi.G6()
+    g6.L.g6_open(0)
+    cs = W.cluster_set(seed=W.SEED0 + 4 + rank)
+    n = len(cs.mass)
+    idx = np.arange(n, dtype=np.int32)
+    irec = ffi.g6_irecords(cs.pos, cs.vel, idx)
+    jrec = ffi.g6_jrecords(cs.pos, cs.vel, cs.mass, idx)
+    d_i = torch.from_numpy(irec.view(np.uint8)).to(dev)
+    d_j = torch.from_numpy(jrec.view(np.uint8)).to(dev)
+    d_o = torch.zeros(n * ffi.G6OUT.itemsize, dtype=torch.uint8, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    items = np.stack([cs.offsets[:-1], cs.sizes, cs.offsets[:-1], cs.sizes], 1)
+    plan = g6.plan_create(items, nn=True)
+    s = torch.cuda.Stream(device=dev)
+    launch = lambda: g6.plan_launch(plan, d_i.data_ptr(), d_j.data_ptr(), cs.eps2, d_o.data_ptr(), s.cuda_stream)  # noqa
+    cfg = None
+    if not args.no_tune:
+        cfg, _ = g6.plan_tune(plan, d_i.data_ptr(), d_j.data_ptr(), cs.eps2, d_o.data_ptr(), s.cuda_stream)
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(ws)
+    ts = _timed_launches(torch, s, launch, args.steps, args.warmup, flush)
+    barrier(ws)
+    clk = clocks.stop()
+    t_local = sum(ts)
+    t_max = reduce_max(t_local, ws, dev)
+    pairs = int((cs.sizes.astype(np.int64) ** 2).sum())
+    value = reduce_sum(float(pairs) * len(ts), ws, dev) / t_max / 1e9
+    achieved = pairs * len(ts) * 60 / t_local / 1e12
+    # plain: 1024 x (g6_set_j_particle x N_k, g6_set_ti, npipes chunks of firsthalf/lasthalf2p)
+    drv = Driver(pgb)
+    p = Driver.p
+    drv.L.g6drv_clusters.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double),
+                                     C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_double] + \
+        [C.POINTER(C.c_double)] * 3 + [C.POINTER(C.c_int), C.POINTER(C.c_float)]
+    drv.L.g6drv_clusters.restype = C.c_double
+    offs = cs.offsets.astype(np.int32)
+    pos, vel, mass = (np.ascontiguousarray(a) for a in (cs.pos, cs.vel, cs.mass))
+    h = drv.g6_open(pgb.ffi.lib_path("libpg6.so"))
+    drv.L.g6drv_clusters(h, 0, 8, p(offs, C.c_int), p(pos), p(vel), p(mass), cs.eps2, None, None, None, None, None)
+    e2e_t = drv.L.g6drv_clusters(h, 0, len(cs.sizes), p(offs, C.c_int), p(pos), p(vel), p(mass), cs.eps2,
+                                 None, None, None, None, None)
+    e2e_val = reduce_sum(float(pairs), ws, dev) / reduce_max(e2e_t, ws, dev) / 1e9
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        path = ref_lib("libpg6_ref.so")
+        if path:
+            hr = drv.g6_open(path)
+            # bounded sample: the first clusters up to ~4e9 pairs
+            cum = np.cumsum(cs.sizes.astype(np.int64) ** 2)
+            ncl = int(np.searchsorted(cum, 4e9) + 1)
+            drv.L.g6drv_clusters(hr, 0, 2, p(offs, C.c_int), p(pos), p(vel), p(mass), cs.eps2, None, None, None,
+                                 None, None)
+            tr = drv.L.g6drv_clusters(hr, 0, ncl, p(offs, C.c_int), p(pos), p(vel), p(mass), cs.eps2, None, None,
+                                      None, None, None)
+            cpu = {"value": float(cum[ncl - 1]) / tr / 1e9, "unit": "Gint/s", "cores": os.cpu_count(),
+                   "kind": "reference", "sample": f"first {ncl} of 1024 clusters ({cum[ncl - 1]:.3e} pairs), "
+                   "PG6/libpg6 AVX2 + OpenMP through the same plain call sequence"}
+    g6.plan_destroy(plan)
+    return _line(args, ws, "Gint/s (independent Hermite clusters, batched)", value, t_max / len(ts), pairs, 60,
+                 "1024 Plummer clusters, N log-uniform [256,16384], eps=1e-4, one force+jerk+pot+NN each",
+                 "f32 (double-float x_j-x_i, f64 cross-tile sums)", achieved, clk,
+                 {"value": round(e2e_val, 3), "unit": "Gint/s", "h2d_bytes_per_step": n * (128 + 48),
+                  "d2h_bytes_per_step": n * 64, "api": "plain GRAPE-6 calls per cluster (g6_set_j_particle x N_k, "
+                  "g6_set_ti, g6calc_firsthalf/lasthalf2p per npipes), host buffers"},
+                 cpu, len(ts), extra={"autotune": cfg, "batched_vs_plain": round(value / e2e_val, 1)},
+                 kernel="pgb::g6_kernel (autotuned configuration)")
+
+
+def run_treepm(args, pgb, ws, rank, local):
+    """PG5 table cutoff force (TreePM PP part): N=2^20 uniform periodic box, 1024-entry table,
+    4096 i-groups of 203-325 particles with their j-lists (4.0-4.5k entries) in one launch."""
+    import torch
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    W = pgb.workloads
+    tab = pgb.ffi.G5Table()
+    ts_ = W.treepm_groups(seed=W.SEED0 + 2 + rank)
+    f = W.gaussian_split_force(ts_.rs, ts_.rcut, ts_.eps)
+    tab.set_table(f, ts_.rcut, frc_bit=6)
+    _, xs = tab.table()
+    # table units: j in float arithmetic as g5_set_xmj does, i through double as g5_set_xi does
+    ip = np.zeros((len(ts_.xi), 4), np.float32)
+    ip[:, :3] = (ts_.xi.astype(np.float32).astype(np.float64) * xs).astype(np.float32)
+    jp = np.zeros((len(ts_.xj), 4), np.float32)
+    jp[:, :3] = ts_.xj.astype(np.float32) * np.float32(xs)
+    jp[:, 3] = ts_.mj
+    d_i = torch.from_numpy(ip).to(dev)
+    d_j = torch.from_numpy(jp).to(dev)
+    d_o = torch.zeros((len(ip), 4), dtype=torch.float64, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    plan = tab.plan_create(ts_.items)
+    s = torch.cuda.Stream(device=dev)
+    launch = lambda: tab.plan_launch(plan, d_i.data_ptr(), d_j.data_ptr(), d_o.data_ptr(), s.cuda_stream)  # noqa
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(ws)
+    tms = _timed_launches(torch, s, launch, args.steps, args.warmup, flush)
+    barrier(ws)
+    clk = clocks.stop()
+    t_local = sum(tms)
+    t_max = reduce_max(t_local, ws, dev)
+    pairs = ts_.interactions
+    value = reduce_sum(float(pairs) * len(tms), ws, dev) / t_max / 1e9
+    achieved = pairs * len(tms) * 38 / t_local / 1e12
+    drv = Driver(pgb)
+    p = Driver.p
+    items = np.ascontiguousarray(ts_.items, np.int32)
+    xi, xj, mj = (np.ascontiguousarray(a) for a in (ts_.xi, ts_.xj, ts_.mj))
+    acc = np.zeros((len(xi), 3))
+    pot = np.zeros(len(xi))
+    h = drv.L.g5drv_open(pgb.ffi.lib_path("libpg5table.so").encode())
+    tab.set_table(f, ts_.rcut, frc_bit=6)    # this process's library instance is the same .so
+    nthr = min(os.cpu_count() or 1, 16)
+    drv.L.g5drv_groups(h, 16, p(items, C.c_int), p(xi), p(xj), p(mj), 0.0, p(acc), p(pot), nthr)
+    e2e_t = drv.L.g5drv_groups(h, len(items), p(items, C.c_int), p(xi), p(xj), p(mj), 0.0, p(acc), p(pot), nthr)
+    e2e_val = reduce_sum(float(pairs), ws, dev) / reduce_max(e2e_t, ws, dev) / 1e9
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        path = ref_lib("libpg5table_ref.so")
+        if path:
+            hr = drv.L.g5drv_open(path.encode())
+            # the same force shape in the reference's table (dlopen of the same file: same instance)
+            Lr = C.CDLL(path, mode=os.RTLD_LOCAL | os.RTLD_NOW)
+            Lr.pg5_gen_force_table.argtypes = [C.c_void_p, C.c_double]
+            cb = pgb.ffi.FORCE_FN(f)
+            Lr.pg5_gen_force_table(C.cast(cb, C.c_void_p), ts_.rcut)
+            ng = 1024
+            tr = drv.L.g5drv_groups(hr, ng, p(items, C.c_int), p(xi), p(xj), p(mj), 0.0, p(acc), p(pot),
+                                    min(os.cpu_count() or 1, 24))
+            sp = int((items[:ng, 1].astype(np.int64) * items[:ng, 3]).sum())
+            cpu = {"value": sp / tr / 1e9, "unit": "Gint/s", "cores": min(os.cpu_count() or 1, 24),
+                   "kind": "reference", "sample": f"first {ng} of {len(items)} groups ({sp:.3e} pairs), "
+                   "PG5/table/libpg5 (512-entry table: the table size is fixed at compile time there), "
+                   "OpenMP over groups with g5_*MC(devid) as source.cpp does"}
+    tab.plan_destroy(plan)
+    return _line(args, ws, "Gint/s (PG5 table cutoff force, TreePM PP, batched)", value, t_max / len(tms), pairs, 38,
+                 "PG5 table N=2^20 uniform periodic box, 1024-entry Gaussian-split table, 4096 i-groups",
+                 "f32 (f64 cross-tile sums)", achieved, clk,
+                 {"value": round(e2e_val, 2), "unit": "Gint/s",
+                  "h2d_bytes_per_step": int(len(xj) * 16 + len(xi) * 16), "d2h_bytes_per_step": int(len(xi) * 32),
+                  "api": f"per group g5_set_xmjMC + g5_set_nMC + g5_calculate_force_on_xMC, {nthr} host threads "
+                         "(one devid each), host buffers"},
+                 cpu, len(tms), kernel="pgb::g5_kernel<TABLE,128,4>")
 
 
 # ----------------------------------------------------------------------------------------
@@ -515,10 +789,11 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["hermite"], default="hermite")
+    ap.add_argument("--workload", choices=["hermite", "direct", "clusters", "treepm"], default="hermite")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--ref-pairs", type=float, default=4e9, help="pairs per reference-arm step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="skip the kernel-configuration autotuner")
     ap.add_argument("--f64-positions", action="store_true",
                     help="FP64 x_j - x_i (DADD + F2F) instead of the double-float subtraction")
     ap.add_argument("--profile-largest", action="store_true",
@@ -534,7 +809,8 @@ def main():
             print(json.dumps(line), flush=True)
         return
     dist = dist_init(ws, local)
-    line = run_hermite(args, pgb, ws, rank, local)
+    runner = {"hermite": run_hermite, "direct": run_direct, "clusters": run_clusters, "treepm": run_treepm}
+    line = runner[args.workload](args, pgb, ws, rank, local)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if ws > 1:

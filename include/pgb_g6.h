@@ -90,11 +90,13 @@ void pgb6_set_abort(int on);
  * hermite.c:214-252), or over independent clusters, by one persistent launch.
  * items[k] = {i_offset, i_count, j_offset, j_count}.  Device records (sizes from
  * pgb6_record_sizes): j-memory G6Ptcl {double pos[3], vel[3], acc2[3], jrk6[3], mass, tim;
- * int idx, pad[3]} (128 B), predicted j G6PredJ {double x, y, z; float m; int id; float vx, vy,
- * vz, pad} (48 B), i G6I {double x, y, z; float vx, vy, vz; int id; float h2, pad} (48 B),
- * result G6Out {double ax, ay, az, jx, jy, jz, pot; float key; int jadr} (64 B) with
- * key = -2/r_soft of the nearest neighbour and jadr its j address (flags & PGB6_NN).     */
-enum { PGB6_NN = 1 };
+ * int idx, pad[3]} (128 B), predicted j G6PredJ {POS p; float m; int id; float vx, vy, vz,
+ * pad} (48 B), i G6I {POS p; float vx, vy, vz; int id; float h2, pad} (48 B), where POS is
+ * 24 bytes: by default the double-float layout {float xh, yh, zh, xl, yl, zl} (x = xh + xl,
+ * xh = (float)x), with flag PGB6_POS_F64 {double x, y, z}; result G6Out {double ax, ay, az,
+ * jx, jy, jz, pot; float key; int jadr} (64 B) with key = -2/r_soft of the nearest neighbour
+ * and jadr its j address (flags & PGB6_NN).                                                 */
+enum { PGB6_NN = 1, PGB6_POS_F64 = 2 };
 typedef struct pgb6_plan pgb6_plan;
 void pgb6_record_sizes(int *ptcl, int *predj, int *irec, int *out);
 int  pgb6_plan_create(pgb6_plan **plan, int nitem, const int *items, int flags);
@@ -104,8 +106,13 @@ void pgb6_plan_destroy(pgb6_plan *plan);
 long long pgb6_plan_interactions(const pgb6_plan *plan);
 int  pgb6_plan_tasks(const pgb6_plan *plan);
 int  pgb6_plan_config(const pgb6_plan *plan);
-/* FP64 j predictor on device records (gravity.c:149-193): pred[j] = predict(ptcl[j], ti) */
-int  pgb6_predict(const void *ptcl, int nj, double ti, void *pred, void *stream);
+/* autotuner: times every kernel configuration on the caller's data, keeps the fastest for this
+ * plan and for later plans of the same shape; returns the configuration, *best_ms its time */
+int  pgb6_plan_tune(pgb6_plan *plan, const void *ipart, const void *jpred, double eps2, void *out,
+                    void *stream, float *best_ms);
+/* FP64 j predictor on device records (gravity.c:149-193): pred[j] = predict(ptcl[j], ti);
+ * flags & PGB6_POS_F64 writes FP64 positions, else the double-float layout */
+int  pgb6_predict(const void *ptcl, int nj, double ti, void *pred, int flags, void *stream);
 /* host-buffer batch: inputs and outputs in host memory, copies included; nnb/rnnb optional */
 int  pgb6_batch_host(int nitem, const int *items, int ni, const double (*xi)[3], const double (*vi)[3],
                      const int *idi, int nj, const double (*xj)[3], const double (*vj)[3], const double *mj,

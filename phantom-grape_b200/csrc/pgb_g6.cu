@@ -78,12 +78,12 @@ bool ensure_device() {
 // ------------------------------------------------------------------------------------------
 // kernel configurations: (threads per CTA, i per thread, j-lanes); i-tile = NT/JL*IPT
 
-enum Cfg { CFG_SMALL = 0, CFG_MED = 1, CFG_LARGE = 2, CFG_128x1 = 3, NCFG = 4 };
-constexpr int CFG_NT[NCFG] = {512, 256, 128, 128};
-constexpr int CFG_IPT[NCFG] = {1, 1, 2, 1};
-constexpr int CFG_JL[NCFG] = {8, 2, 1, 1};
+enum Cfg { CFG_SMALL = 0, CFG_MED = 1, CFG_LARGE = 2, CFG_128x1 = 3, CFG_128x4 = 4, CFG_256x2 = 5, NCFG = 6 };
+constexpr int CFG_NT[NCFG] = {512, 256, 128, 128, 128, 256};
+constexpr int CFG_IPT[NCFG] = {1, 1, 2, 1, 4, 2};
+constexpr int CFG_JL[NCFG] = {8, 2, 1, 1, 1, 1};
 inline int cfg_itile(int c) { return CFG_NT[c] / CFG_JL[c] * CFG_IPT[c]; }
-constexpr int ITILE_MAX = 256;
+constexpr int ITILE_MAX = 512;
 
 template <int NT, int IPT, int JL, bool FF>
 int occ_of(bool nn, bool nbl) {
@@ -106,6 +106,8 @@ int occupancy_ff(int cfg, bool nn, bool nbl) {
         case CFG_SMALL: return occ_of<512, 1, 8, FF>(nn, nbl);
         case CFG_MED: return occ_of<256, 1, 2, FF>(nn, nbl);
         case CFG_128x1: return occ_of<128, 1, 1, FF>(nn, nbl);
+        case CFG_128x4: return occ_of<128, 4, 1, FF>(nn, nbl);
+        case CFG_256x2: return occ_of<256, 2, 1, FF>(nn, nbl);
         default: return occ_of<128, 2, 1, FF>(nn, nbl);
     }
 }
@@ -128,6 +130,8 @@ void launch_ff(int cfg, bool nn, bool nbl, int grid, const G6Args& a, cudaStream
         case CFG_SMALL: launch_cfg<512, 1, 8, FF>(nn, nbl, grid, a, s); break;
         case CFG_MED: launch_cfg<256, 1, 2, FF>(nn, nbl, grid, a, s); break;
         case CFG_128x1: launch_cfg<128, 1, 1, FF>(nn, nbl, grid, a, s); break;
+        case CFG_128x4: launch_cfg<128, 4, 1, FF>(nn, nbl, grid, a, s); break;
+        case CFG_256x2: launch_cfg<256, 2, 1, FF>(nn, nbl, grid, a, s); break;
         default: launch_cfg<128, 2, 1, FF>(nn, nbl, grid, a, s); break;
     }
 }
@@ -653,10 +657,53 @@ PGB_EXPORT void pgb6_record_sizes(int* ptcl, int* predj, int* irec, int* out) {
     if (out) *out = (int)sizeof(G6Out);
 }
 
+namespace {
+// Autotune cache: work-item-table shape -> best kernel configuration measured by
+// pgb6_plan_tune.  The shape key buckets the item count, the largest i and j counts (powers of
+// two) and the variant flags, so plans of the same shape reuse a measured choice.
+std::mutex g_tune_mu;
+std::vector<std::pair<long long, int>> g_tune;
+
+int ilog2up(long long v) {
+    int k = 0;
+    while ((1LL << k) < v && k < 62) k++;
+    return k;
+}
+
+long long shape_key(int nitem, const int* items, bool ff, bool nn) {
+    long long nimax = 0, njmax = 0;
+    for (int k = 0; k < nitem; k++) {
+        nimax = std::max<long long>(nimax, items[4 * k + 1]);
+        njmax = std::max<long long>(njmax, items[4 * k + 3]);
+    }
+    return ((long long)ilog2up(nitem + 1) << 24) | ((long long)ilog2up(nimax + 1) << 16) |
+           ((long long)ilog2up(njmax + 1) << 8) | (ff ? 2 : 0) | (nn ? 1 : 0);
+}
+
+int tuned_cfg(long long key) {
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    for (auto& e : g_tune)
+        if (e.first == key) return e.second;
+    return -1;
+}
+
+void set_tuned(long long key, int cfg) {
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    for (auto& e : g_tune)
+        if (e.first == key) {
+            e.second = cfg;
+            return;
+        }
+    g_tune.emplace_back(key, cfg);
+}
+}  // namespace
+
 struct pgb6_plan {
     int cfg;
     bool nn;
     bool ff;
+    std::vector<int> items;    // the work-item table, kept for re-planning (autotuning)
+    long long shape_key = 0;   // autotune cache key of this work-item table
     std::vector<Task> tasks;
     std::vector<Group> groups;
     int rows = 0;
@@ -688,7 +735,10 @@ PGB_EXPORT int pgb6_plan_create(pgb6_plan** out, int nitem, const int* items, in
     // many small items fill the GPU with short tiles; large ones prefer 2 i per thread
     long long total_i = 0;
     for (int k = 0; k < nitem; k++) total_i += items[4 * k + 1];
-    P->cfg = pick_cfg(nitem > 1 ? std::max<long long>(nimax, total_i / 4) : nimax);
+    P->items.assign(items, items + 4 * (size_t)nitem);
+    P->shape_key = shape_key(nitem, items, P->ff, P->nn);
+    int tuned = tuned_cfg(P->shape_key);
+    P->cfg = tuned >= 0 ? tuned : pick_cfg(nitem > 1 ? std::max<long long>(nimax, total_i / 4) : nimax);
     P->interactions = plan_items(P->tasks, P->groups, P->rows, nitem, items, P->cfg, P->ff, P->nn, false);
     cudaStream_t s = nullptr;
     bool ok = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess;
@@ -741,6 +791,60 @@ PGB_EXPORT int pgb6_plan_launch(pgb6_plan* P, const void* ipart, const void* jpr
     int grid = a.ntasks < slots ? a.ntasks : slots;
     PGB_CUDA_OR(g_err, LIB, launch_kernel(P->cfg, P->ff, P->nn, false, grid, a, s), return PGB_ERR_CUDA);
     return PGB_OK;
+}
+
+// Autotuner: launches the plan with every kernel configuration (threads per CTA x i per
+// thread x j-lanes) on the caller's data, keeps the fastest (CUDA-event time, best of 2 after a
+// warm-up launch), re-stages the plan with it and records it for plans of the same shape.
+// Returns the chosen configuration index; *best_ms (optional) receives its launch time.
+// Overwrites `out`.  Not capturable (it synchronises the stream).
+PGB_EXPORT int pgb6_plan_tune(pgb6_plan* P, const void* ipart, const void* jpred, double eps2, void* out,
+                              void* stream, float* best_ms) {
+    if (!P || !ipart || !jpred || !out) {
+        raise(g_err, LIB, PGB_ERR_ARG, "pgb6_plan_tune: null argument");
+        return -1;
+    }
+    if (!ensure_device()) return -1;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaEvent_t e0, e1;
+    PGB_CUDA_OR(g_err, LIB, cudaEventCreate(&e0), return -1);
+    PGB_CUDA_OR(g_err, LIB, cudaEventCreate(&e1), return -1);
+    int nitem = (int)(P->items.size() / 4);
+    int best = P->cfg;
+    float best_t = 1e30f;
+    for (int cfg = 0; cfg < NCFG; cfg++) {
+        P->tasks.clear();
+        P->groups.clear();
+        P->cfg = cfg;
+        plan_items(P->tasks, P->groups, P->rows, nitem, P->items.data(), cfg, P->ff, P->nn, false);
+        if (P->st.stage(s, P->tasks, P->groups, P->rows, ITILE_MAX, (const G6I*)nullptr, 0) != cudaSuccess) break;
+        float t = 1e30f;
+        for (int rep = 0; rep < 3; rep++) {
+            cudaEventRecord(e0, s);
+            if (pgb6_plan_launch(P, ipart, jpred, eps2, out, stream) != PGB_OK) break;
+            cudaEventRecord(e1, s);
+            cudaEventSynchronize(e1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (rep > 0 && ms < t) t = ms;
+        }
+        if (t < best_t) {
+            best_t = t;
+            best = cfg;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    P->tasks.clear();
+    P->groups.clear();
+    P->cfg = best;
+    plan_items(P->tasks, P->groups, P->rows, nitem, P->items.data(), best, P->ff, P->nn, false);
+    PGB_CUDA_OR(g_err, LIB, P->st.stage(s, P->tasks, P->groups, P->rows, ITILE_MAX, (const G6I*)nullptr, 0),
+                return -1);
+    PGB_CUDA_OR(g_err, LIB, cudaStreamSynchronize(s), return -1);
+    set_tuned(P->shape_key, best);
+    if (best_ms) *best_ms = best_t;
+    return best;
 }
 
 PGB_EXPORT void pgb6_plan_destroy(pgb6_plan* P) {

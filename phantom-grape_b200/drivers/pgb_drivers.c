@@ -216,3 +216,54 @@ double g5drv_groups(void *handle, int ngroups, const int *items, const double *x
     }
     return now() - t0;
 }
+
+/* Independent clusters through the plain GRAPE-6 calls: for cluster c (particles
+ * [off[c], off[c+1]) of the arrays), its particles are written to j-addresses 0..n_c-1 with
+ * g6_set_j_particle (zero acc/2, jerk/6, time 0), then g6_set_ti(0) and npipes-sized
+ * g6calc_firsthalf / g6calc_lasthalf2p over all of them.  Outputs per particle (optional).
+ * Clusters [c0, c1) only.  Returns the elapsed seconds. */
+double g6drv_clusters(void *handle, int c0, int c1, const int *off, const double *pos, const double *vel,
+                      const double *mass, double eps2, double *acc_out, double *jrk_out, double *pot_out,
+                      int *nnb_out, float *rnnb_out) {
+    g6api *a = (g6api *)handle;
+    int npipe = a->npipes();
+    int *pidx = (int *)malloc(sizeof(int) * npipe);
+    double(*acc)[3] = malloc(sizeof(double) * 3 * npipe);
+    double(*jrk)[3] = malloc(sizeof(double) * 3 * npipe);
+    double *pot = (double *)malloc(sizeof(double) * npipe);
+    double *h2 = (double *)calloc(npipe, sizeof(double));
+    int *nnb = (int *)malloc(sizeof(int) * npipe);
+    float *rnnb = (float *)malloc(sizeof(float) * npipe);
+    double zero3[3] = {0, 0, 0};
+    double t0 = now();
+    for (int c = c0; c < c1; c++) {
+        int o = off[c], n = off[c + 1] - off[c];
+        for (int k = 0; k < n; k++)
+            a->set_j(0, k, k, 0.0, 0.0, mass[o + k], zero3, zero3, zero3, (double *)vel + 3 * (size_t)(o + k),
+                     (double *)pos + 3 * (size_t)(o + k));
+        a->set_ti(0, 0.0);
+        for (int i = 0; i < n; i += npipe) {
+            int nii = n - i < npipe ? n - i : npipe;
+            for (int k = 0; k < nii; k++) pidx[k] = i + k;
+            double(*px)[3] = (double(*)[3])(pos + 3 * (size_t)(o + i));
+            double(*pv)[3] = (double(*)[3])(vel + 3 * (size_t)(o + i));
+            a->firsthalf(0, n, nii, pidx, px, pv, acc, jrk, pot, eps2, h2);
+            a->lasthalf2p(0, n, nii, pidx, px, pv, eps2, h2, acc, jrk, pot, nnb, rnnb);
+            size_t q = (size_t)(o + i);
+            if (acc_out) memcpy(acc_out + 3 * q, acc, sizeof(double) * 3 * nii);
+            if (jrk_out) memcpy(jrk_out + 3 * q, jrk, sizeof(double) * 3 * nii);
+            if (pot_out) memcpy(pot_out + q, pot, sizeof(double) * nii);
+            if (nnb_out) memcpy(nnb_out + q, nnb, sizeof(int) * nii);
+            if (rnnb_out) memcpy(rnnb_out + q, rnnb, sizeof(float) * nii);
+        }
+    }
+    double el = now() - t0;
+    free(pidx);
+    free(acc);
+    free(jrk);
+    free(pot);
+    free(h2);
+    free(nnb);
+    free(rnnb);
+    return el;
+}

@@ -231,6 +231,7 @@ class G6(_ErrMixin):
         _sig(L, "pgb6_plan_interactions", [vp], C.c_longlong)
         _sig(L, "pgb6_plan_tasks", [vp], C.c_int)
         _sig(L, "pgb6_plan_config", [vp], C.c_int)
+        _sig(L, "pgb6_plan_tune", [vp, vp, vp, C.c_double, vp, vp, C.POINTER(C.c_float)], C.c_int)
         _sig(L, "pgb6_predict", [vp, C.c_int, C.c_double, vp, C.c_int, vp], C.c_int)
         _sig(L, "pgb6_batch_host", [C.c_int, ip, C.c_int, dp, dp, ip, C.c_int, dp, dp, dp, ip, C.c_double,
                                     dp, dp, dp, ip, fp], C.c_int)
@@ -318,6 +319,13 @@ class G6(_ErrMixin):
         rc = self.L.pgb6_plan_launch(plan, ipart, jpred, eps2, out, stream)
         if rc:
             raise RuntimeError(f"pgb6_plan_launch failed: {self.last_error()}")
+
+    def plan_tune(self, plan, ipart, jpred, eps2, out, stream=0):
+        ms = C.c_float()
+        cfg = self.L.pgb6_plan_tune(plan, ipart, jpred, eps2, out, stream, C.byref(ms))
+        if cfg < 0:
+            raise RuntimeError(f"pgb6_plan_tune failed: {self.last_error()}")
+        return cfg, ms.value
 
     def plan_destroy(self, plan):
         self.L.pgb6_plan_destroy(plan)
