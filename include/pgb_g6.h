@@ -119,6 +119,21 @@ int  pgb6_batch_host(int nitem, const int *items, int ni, const double (*xi)[3],
                      const int *idj, double eps2, double (*acc)[3], double (*jrk)[3], double *pot, int *nnb,
                      float *rnnb);
 
+/* ---- allocation-free force call (no counterpart in the reference) ------------------------
+ * For callers that cannot let a library allocate GPU memory: codes whose device memory is
+ * owned by their own pool allocator, and step loops that cannot afford the device-wide
+ * synchronisation of cudaMalloc / cudaFree.  Same kernel and results as a one-item plan
+ * (ni G6I records against nj G6PredJ records, G6Out results, flags PGB6_NN / PGB6_POS_F64),
+ * but its work list and partial sums live in a fixed 16 MiB array of the library's static
+ * device memory (held on every GPU the library is loaded on until exit); it never calls
+ * cudaMalloc or cudaFree.  Limit: at most 4096 i-tiles (ni <= 1,048,576 with the 256-particle
+ * tile that large calls use); larger ni returns
+ * PGB_ERR_CAPACITY.  The first call on a device looks up the array's address there and
+ * should come before any stream capture.  All calls share the array: calls that overlap on
+ * the GPU race and must be serialised by the caller. */
+int  pgb6_force_noalloc(const void *ipart, int ni, const void *jpred, int nj, double eps2, void *out, int flags,
+                        void *stream);
+
 #ifdef __cplusplus
 }
 #endif

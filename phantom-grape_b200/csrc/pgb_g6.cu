@@ -953,3 +953,129 @@ PGB_EXPORT int pgb6_batch_host(int nitem, const int* items, int ni, const double
     }
     return PGB_OK;
 }
+
+// ============================================================================================
+// Allocation-free Hermite force call (no counterpart in the reference).
+//
+// For callers that must not allocate GPU memory: codes whose device memory is owned by their
+// own pool allocator (a simulation that reserves most of HBM at start-up and hands libraries
+// fixed buffers), and time-step loops that cannot afford the device-wide synchronisation a
+// cudaMalloc / cudaFree may cause.  pgb6_force_noalloc runs the same force kernel as the
+// plans, but its work list, group counters and partial sums live in one fixed array in the
+// library's own static device memory (g6_noalloc_scratch below, 16 MiB, held on every GPU the
+// library is loaded on until the process exits).  It never calls cudaMalloc or cudaFree.
+//
+// Set-up: the first call on a device looks up the array's device address there (this first
+// call should come before any stream capture).  Every call shares the array and leaves its
+// contents behind; each call clears the counters it needs first.  Calls whose launches overlap
+// on the GPU (different streams, or different host threads) race on the array and corrupt
+// each other's results: serialise them.
+
+namespace {
+constexpr size_t NOALLOC_BYTES = size_t(16) << 20;     // the whole scratch array
+constexpr int NOALLOC_MAX_ITILES = 4096;                // i-tiles (one group counter each)
+constexpr int NOALLOC_MAX_TASKS = 16384;
+constexpr size_t NA_OFF_GCNT = 256;                                        // task counter first
+constexpr size_t NA_OFF_TASKS = NA_OFF_GCNT + sizeof(int) * NOALLOC_MAX_ITILES;
+constexpr size_t NA_OFF_GROUPS = NA_OFF_TASKS + sizeof(Task) * NOALLOC_MAX_TASKS;
+constexpr size_t NA_OFF_PART = (NA_OFF_GROUPS + sizeof(Group) * NOALLOC_MAX_ITILES + 255) & ~size_t(255);
+constexpr size_t NOALLOC_MAX_PART = (NOALLOC_BYTES - NA_OFF_PART) / sizeof(G6Out);
+}  // namespace
+
+static __device__ __align__(256) unsigned char g6_noalloc_scratch[NOALLOC_BYTES];
+
+namespace {
+std::mutex g_na_mu;
+void* g_na_addr[64];  // device address of g6_noalloc_scratch per device (set-up once)
+
+// Regular decomposition of one (ni x nj) item into itiles x nch tasks, written to the scratch
+// work list (the layout the force kernel reads from a staged plan).
+__global__ void g6_regular_tasks(Task* tasks, Group* groups, int ni, int nj, int itile, int itiles, int nch) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= itiles * nch) return;
+    int it = t / nch, c = t % nch;
+    int i0 = it * itile;
+    int nii = min(itile, ni - i0);
+    int j0 = (int)((long long)c * nj / nch), j1 = (int)((long long)(c + 1) * nj / nch);
+    if (nch == 1) {
+        tasks[t] = Task{i0, nii, 0, nj, -1, 0, -1, 0};
+        return;
+    }
+    tasks[t] = Task{i0, nii, j0, j1 - j0, it, c, it * nch + c, 0};
+    if (c == 0) groups[it] = Group{i0, nii, nch, it * nch};
+}
+}  // namespace
+
+// One item: ni i-records (G6I) against nj predicted j-records (G6PredJ), results G6Out per i
+// in out (device pointers, caller-owned).  flags: PGB6_NN, PGB6_POS_F64 as for plans.
+// Limits: ni <= 4096 i-tiles (1,048,576 particles with the 256-particle tile that large calls
+// use); larger ni is refused
+// with PGB_ERR_CAPACITY.  Returns PGB_OK or an error code (message in pgb6_last_error).
+PGB_EXPORT int pgb6_force_noalloc(const void* ipart, int ni, const void* jpred, int nj, double eps2, void* out,
+                                  int flags, void* stream) {
+    if (ni < 0 || nj < 0 || (ni > 0 && (!ipart || !out)) || (nj > 0 && !jpred)) {
+        raise(g_err, LIB, PGB_ERR_ARG, "pgb6_force_noalloc: bad arguments (ni %d, nj %d)", ni, nj);
+        return PGB_ERR_ARG;
+    }
+    if (ni == 0) return PGB_OK;
+    if (!ensure_device()) return PGB_ERR_NOGPU;
+    const bool nn = (flags & PGB6_NN) != 0, ff = (flags & PGB6_POS_F64) == 0;
+    const int cfg = pick_cfg(ni);
+    const int itile = cfg_itile(cfg);
+    const long long itiles = (ni + (long long)itile - 1) / itile;
+    if (itiles > NOALLOC_MAX_ITILES) {
+        raise(g_err, LIB, PGB_ERR_CAPACITY, "pgb6_force_noalloc: ni = %d exceeds the fixed scratch (%d i-tiles of %d)",
+              ni, NOALLOC_MAX_ITILES, itile);
+        return PGB_ERR_CAPACITY;
+    }
+    void* base = nullptr;
+    {
+        std::lock_guard<std::mutex> g(g_na_mu);
+        if (g_device < 0 || g_device >= 64) return PGB_ERR_NOGPU;
+        if (!g_na_addr[g_device]) {
+            cudaError_t e = cudaGetSymbolAddress(&g_na_addr[g_device], g6_noalloc_scratch);
+            if (e != cudaSuccess) {
+                g_na_addr[g_device] = nullptr;
+                raise(g_err, LIB, PGB_ERR_CUDA, "pgb6_force_noalloc: cudaGetSymbolAddress failed: %s",
+                      cudaGetErrorString(e));
+                return PGB_ERR_CUDA;
+            }
+        }
+        base = g_na_addr[g_device];
+    }
+    // j-chunks per i-tile: about 4 tasks per resident CTA, at least 128 j per chunk, within
+    // the scratch's task and partial-row capacity
+    const int slots = sm_count(g_device) * occupancy(cfg, ff, nn, false);
+    long long nch = (4LL * slots + itiles - 1) / itiles;
+    nch = std::min<long long>(nch, std::max<long long>(1, nj / 128));
+    nch = std::min<long long>(nch, 512);
+    nch = std::min<long long>(nch, NOALLOC_MAX_TASKS / itiles);
+    nch = std::min<long long>(nch, (long long)(NOALLOC_MAX_PART / ((size_t)itiles * itile)));
+    if (nch < 1) nch = 1;
+    const int ntasks = (int)(itiles * nch);
+    unsigned char* b = (unsigned char*)base;
+    cudaStream_t s = (cudaStream_t)stream;
+    // the task counter and the group counters must start at zero
+    PGB_CUDA_OR(g_err, LIB, cudaMemsetAsync(b, 0, NA_OFF_TASKS, s), return PGB_ERR_CUDA);
+    g6_regular_tasks<<<(ntasks + 255) / 256, 256, 0, s>>>((Task*)(b + NA_OFF_TASKS), (Group*)(b + NA_OFF_GROUPS), ni,
+                                                          nj, itile, (int)itiles, (int)nch);
+    PGB_CUDA_OR(g_err, LIB, cudaGetLastError(), return PGB_ERR_CUDA);
+    G6Args a;
+    a.ipart = (const G6I*)ipart;
+    a.jpred = (const G6PredJ*)jpred;
+    a.eps2 = (float)eps2;
+    a.tasks = (const Task*)(b + NA_OFF_TASKS);
+    a.ntasks = ntasks;
+    a.task_counter = (int*)b;
+    a.groups = (const Group*)(b + NA_OFF_GROUPS);
+    a.group_counters = (int*)(b + NA_OFF_GCNT);
+    a.partial = (G6Out*)(b + NA_OFF_PART);
+    a.out = (G6Out*)out;
+    a.itile = itile;
+    a.nb_count = nullptr;
+    a.nb_list = nullptr;
+    a.nb_maxlen = 0;
+    int grid = ntasks < slots ? ntasks : slots;
+    PGB_CUDA_OR(g_err, LIB, launch_kernel(cfg, ff, nn, false, grid, a, s), return PGB_ERR_CUDA);
+    return PGB_OK;
+}

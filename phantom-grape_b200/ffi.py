@@ -471,3 +471,9 @@ class G5Table(_ErrMixin):
 
     def plan_destroy(self, plan):
         self.L.pgb5_plan_destroy(plan)
+
+
+def bind_noalloc(g6: "G6"):
+    """Bind pgb6_force_noalloc (the allocation-free force call) on a G6 instance's library."""
+    _sig(g6.L, "pgb6_force_noalloc", [vp, C.c_int, vp, C.c_int, C.c_double, vp, C.c_int, vp], C.c_int)
+    return g6.L.pgb6_force_noalloc

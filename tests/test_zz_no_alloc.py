@@ -1,0 +1,98 @@
+"""The allocation-free force call, pgb6_force_noalloc (lib/libpg6.so).
+
+It exists for callers that cannot let the library allocate GPU memory -- codes that own all of
+their device memory through their own pool, and step loops that cannot pay the device-wide
+synchronisation of cudaMalloc / cudaFree.  Its scratch (work list, counters, partial sums) is a
+fixed array in the library's static device memory, shared by every call.
+
+Checked here through the C ABI: two calls in a row give the same forces, jerks, potentials and
+nearest neighbours as the allocating entry point (a one-item plan) within the tolerance of the
+other GPU tests (rms relative 1e-6), and bit-identical results to each other; an i count beyond
+the fixed scratch is refused with PGB_ERR_CAPACITY instead of being run.  The file is named so
+that pytest collects it last; it also runs alone in a fresh process.
+"""
+import numpy as np
+import pytest
+
+from conftest import pgb, gpu_available
+
+pytestmark = pytest.mark.gpu
+
+PGB_ERR_CAPACITY = 3
+
+
+def _rel(a, b):
+    return np.linalg.norm(a - b, axis=1) / np.maximum(np.linalg.norm(b, axis=1), 1e-300)
+
+
+def _rms(x):
+    return float(np.sqrt(np.mean(np.square(x))))
+
+
+def _cols(out, prefix):
+    return np.stack([out[prefix + c] for c in "xyz"], 1)
+
+
+@pytest.fixture(scope="module")
+def setup():
+    if not gpu_available():
+        pytest.skip("no GPU")
+    import torch
+    g6 = pgb.ffi.G6()
+    g6.L.g6_open(0)
+    fn = pgb.ffi.bind_noalloc(g6)
+    cs = pgb.workloads.cluster_set(ncl=1, nmin=20000, nmax=20000, seed=2027)
+    n = len(cs.mass)
+    idx = np.arange(n, dtype=np.int32)
+    ni = 3001   # a ragged i count (not a multiple of any i-tile)
+    irec = pgb.ffi.g6_irecords(cs.pos[:ni], cs.vel[:ni], idx[:ni])
+    jrec = pgb.ffi.g6_jrecords(cs.pos, cs.vel, cs.mass, idx)
+    dev = torch.device("cuda")
+    d_i = torch.from_numpy(irec.view(np.uint8)).to(dev)
+    d_j = torch.from_numpy(jrec.view(np.uint8)).to(dev)
+    outs = [torch.zeros(ni * pgb.ffi.G6OUT.itemsize, dtype=torch.uint8, device=dev) for _ in range(3)]
+    return dict(torch=torch, g6=g6, fn=fn, n=n, ni=ni, eps2=cs.eps2, d_i=d_i, d_j=d_j, outs=outs)
+
+
+def test_noalloc_matches_allocating_entry_point_twice(setup):
+    S = setup
+    torch, g6, fn = S["torch"], S["g6"], S["fn"]
+    stream = torch.cuda.current_stream().cuda_stream
+    # reference answer from the allocating path: a one-item plan
+    plan = g6.plan_create([[0, S["ni"], 0, S["n"]]], nn=True)
+    try:
+        g6.plan_launch(plan, S["d_i"].data_ptr(), S["d_j"].data_ptr(), S["eps2"], S["outs"][0].data_ptr(), stream)
+    finally:
+        g6.plan_destroy(plan)
+    res = []
+    for k in (1, 2):  # two calls in a row
+        S["outs"][k].fill_(0xFF)
+        rc = fn(S["d_i"].data_ptr(), S["ni"], S["d_j"].data_ptr(), S["n"], S["eps2"], S["outs"][k].data_ptr(),
+                g6.NN, stream)
+        assert rc == 0, g6.last_error()
+        torch.cuda.synchronize()
+        res.append(S["outs"][k].cpu().numpy().view(pgb.ffi.G6OUT))
+    ref = S["outs"][0].cpu().numpy().view(pgb.ffi.G6OUT)
+    for r in res:
+        assert _rms(_rel(_cols(r, "a"), _cols(ref, "a"))) <= 1e-6
+        assert _rms(_rel(_cols(r, "j"), _cols(ref, "j"))) <= 1e-6
+        np.testing.assert_allclose(r["pot"], ref["pot"], rtol=1e-6)
+        np.testing.assert_array_equal(r["jadr"], ref["jadr"])
+        np.testing.assert_allclose(r["key"], ref["key"], rtol=1e-6)
+    assert res[0].tobytes() == res[1].tobytes()
+
+
+def test_noalloc_refuses_sizes_beyond_its_scratch(setup):
+    S = setup
+    g6, fn = S["g6"], S["fn"]
+    g6.set_abort(False)
+    try:
+        g6.clear_error()
+        too_many = 4096 * 512 + 1   # more i-tiles than the fixed scratch holds, for any tile size
+        rc = fn(S["d_i"].data_ptr(), too_many, S["d_j"].data_ptr(), S["n"], S["eps2"], S["outs"][1].data_ptr(),
+                g6.NN, S["torch"].cuda.current_stream().cuda_stream)
+        code, msg = g6.last_error()
+        assert rc == PGB_ERR_CAPACITY and code == PGB_ERR_CAPACITY and "scratch" in msg
+    finally:
+        g6.clear_error()
+        g6.set_abort(True)
