@@ -133,12 +133,13 @@ template <class T>
 struct HostBuf {
     T* p = nullptr;
     size_t n = 0;
-    cudaError_t reserve(size_t want, bool keep = false) {
+    // flags: cudaHostAllocMapped for a buffer that kernels write through its device address
+    cudaError_t reserve(size_t want, bool keep = false, unsigned flags = cudaHostAllocPortable) {
         if (want <= n) return cudaSuccess;
         size_t m = n ? n : 256;
         while (m < want) m *= 2;
         T* q = nullptr;
-        cudaError_t e = cudaHostAlloc(&q, m * sizeof(T), cudaHostAllocPortable);
+        cudaError_t e = cudaHostAlloc(&q, m * sizeof(T), flags);
         if (e != cudaSuccess) return e;
         if (keep && p) std::memcpy(q, p, n * sizeof(T));
         if (p) cudaFreeHost(p);
@@ -170,6 +171,27 @@ struct Group {
     int nchunk;      // number of tasks (partial rows) in the group
     int slot0;       // first partial row; rows slot0 .. slot0+nchunk-1 in chunk order
 };
+
+// Number of j-chunks for one item of `itiles` equal i-tiles on `slots` resident CTAs: the
+// persistent CTAs run ceil(itiles*nch/slots) waves of tasks of nj/nch pairs per i, so the time
+// is proportional to waves/nch; a small penalty per chunk accounts for the partial-row
+// reduction.  Chunks hold at least `minj` j and there are at most `maxch` of them.
+inline int best_nch(long long itiles, long long nj, long long slots, int maxch, int minj = 128) {
+    long long hi = nj / minj;
+    if (hi > maxch) hi = maxch;
+    if (hi < 1) return 1;
+    double best = 1e300;
+    int arg = 1;
+    for (long long n = 1; n <= hi; n++) {
+        long long waves = (itiles * n + slots - 1) / slots;
+        double cost = (double)waves / (double)n * (1.0 + 0.002 * (double)n);
+        if (cost < best) {
+            best = cost;
+            arg = (int)n;
+        }
+    }
+    return arg;
+}
 
 // Split [0,ni) x [0,nj) into tasks of at most `itile` i and about `jchunk` j, appending to
 // `tasks`/`groups`.  Offsets are added to i0/j0.  Returns the partial rows used.
@@ -214,11 +236,11 @@ struct Stager {
     DevBuf<ORec> dpart;            // partial rows, [rows][itile]
     HostBuf<unsigned char> hcall;  // pinned staging of the call block
     cudaEvent_t copied = nullptr;  // last H2D copy out of hcall
-    size_t off_g = 0, off_i = 0;
+    size_t off_g = 0, off_i = 0, off_bc = 0;
     int ntasks = 0;
 
     cudaError_t stage(cudaStream_t s, const std::vector<Task>& tasks, const std::vector<Group>& groups, int rows,
-                      int itile, const IRec* i_host, int ni_host) {
+                      int itile, const IRec* i_host, int ni_host, size_t min_groups = 0) {
         cudaError_t e;
         if (!copied && (e = cudaEventCreateWithFlags(&copied, cudaEventDisableTiming)) != cudaSuccess) return e;
         // the previous copy out of hcall must have left before hcall is rewritten
@@ -233,19 +255,29 @@ struct Stager {
         if (!tasks.empty()) std::memcpy(hcall.p + off_t, tasks.data(), tasks.size() * sizeof(Task));
         if (!groups.empty()) std::memcpy(hcall.p + off_g, groups.data(), groups.size() * sizeof(Group));
         if (ni_host) std::memcpy(hcall.p + off_i, i_host, (size_t)ni_host * sizeof(IRec));
-        size_t old_g = dgcnt.n;
-        if ((e = dgcnt.reserve(groups.size() + 1)) != cudaSuccess) return e;
-        if (dgcnt.n != old_g && (e = dgcnt.zero_fill(s)) != cudaSuccess) return e;
-        if (rows > 0 && (e = dpart.reserve((size_t)rows * itile)) != cudaSuccess) return e;
+        if ((e = reserve_scratch(s, rows, itile, std::max(groups.size(), min_groups))) != cudaSuccess) return e;
         if ((e = cudaMemcpyAsync(dcall.p, hcall.p, total, cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
         if ((e = cudaEventRecord(copied, s)) != cudaSuccess) return e;
         ntasks = (int)tasks.size();
+        return cudaSuccess;
+    }
+    // Partial rows and zeroed counters: one per group (`ngroups` includes groups that the
+    // kernel derives itself, regular mode), then one per partial row for the two-level
+    // reduction of long groups.  Enough for a launch that uploads nothing.
+    cudaError_t reserve_scratch(cudaStream_t s, int rows, int itile, size_t ngroups) {
+        cudaError_t e;
+        off_bc = ngroups;
+        const size_t old = dgcnt.n;
+        if ((e = dgcnt.reserve(off_bc + (size_t)rows + 1)) != cudaSuccess) return e;
+        if (dgcnt.n != old && (e = dgcnt.zero_fill(s)) != cudaSuccess) return e;
+        if (rows > 0 && (e = dpart.reserve((size_t)rows * itile)) != cudaSuccess) return e;
         return cudaSuccess;
     }
     int* counter() const { return (int*)dcall.p; }
     const Task* tasks() const { return (const Task*)(dcall.p + 16); }
     const Group* groups() const { return (const Group*)(dcall.p + off_g); }
     const IRec* irecs() const { return (const IRec*)(dcall.p + off_i); }
+    int* bundle_counters() const { return dgcnt.p + off_bc; }
     void release() {
         if (copied) cudaEventSynchronize(copied);
         dcall.release();
@@ -275,10 +307,20 @@ __device__ __forceinline__ float minus2_over_r(float r2) {
     return u * y;
 }
 
-// The persistent scheduler: CTAs pull task indices from a global counter.
-__device__ __forceinline__ int next_task(int* counter, int* s_slot) {
+// The persistent scheduler.  A CTA's first task is its block index; later ones are drawn from
+// a global counter as gridDim.x + k.  Every CTA draws until it gets a task >= ntasks, so a
+// launch draws exactly ntasks times (the ntasks - min(grid, ntasks) extra tasks plus one failed
+// draw per working CTA) and the CTA that draws k = ntasks - 1 is the last to touch the counter:
+// it resets it to zero, so the counter is ready for the next launch without a memset.
+// `first` skips the barrier too: callers that stage shared memory before the loop sync first.
+__device__ __forceinline__ int next_task(int* counter, int* s_slot, int ntasks, bool first) {
+    if (first) return (int)blockIdx.x;
     __syncthreads();
-    if (threadIdx.x == 0) *s_slot = atomicAdd(counter, 1);
+    if (threadIdx.x == 0) {
+        const int k = atomicAdd(counter, 1);
+        if (k == ntasks - 1) atomicExch(counter, 0);
+        *s_slot = (int)gridDim.x + k;
+    }
     __syncthreads();
     return *s_slot;
 }

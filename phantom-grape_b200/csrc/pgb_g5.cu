@@ -118,16 +118,12 @@ cudaError_t launch_kind(int kind, int grid, const G5Args& a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-// Chunk length for one item so that the whole call yields about 4 tasks per resident CTA.
+// Chunk length for one item: its tasks are all the same size, so one wave of tasks (one per
+// resident CTA) balances, and fewer chunks keep the partial-row reduction short.
 int choose_jchunk(long long itiles_total, int nj, int slots) {
     if (nj <= 0) return 1;
-    long long target = 4LL * slots;
-    long long nch = (target + itiles_total - 1) / (itiles_total > 0 ? itiles_total : 1);
-    long long maxch = (nj + 127) / 128;  // at least 128 j per chunk, at most 512 chunks
-    if (maxch > 512) maxch = 512;
-    if (nch > maxch) nch = maxch;
-    if (nch < 1) nch = 1;
-    return (int)((nj + nch - 1) / nch);
+    int nch = best_nch(itiles_total > 0 ? itiles_total : 1, nj, slots, 512);
+    return (nj + nch - 1) / nch;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -257,12 +253,11 @@ struct Launcher {
         return true;
     }
 
-    // Launch over the staged work list.  `reset_counter`: zero the task counter first (needed
-    // when the same staged list is launched again, e.g. from a CUDA graph).
+    // Launch over the staged work list.  The kernel leaves its task counter at zero, so the same
+    // staged list can be launched again (e.g. from a CUDA graph) without a reset.
     bool launch(int kind, cudaStream_t s, const float4* i_dev, const float4* jpos, const float4* jaux,
-                double4* out, bool reset_counter) {
+                double4* out) {
         if (st.ntasks <= 0) return true;
-        if (reset_counter) PGB_CUDA_OR(g_err, LIB, cudaMemsetAsync(st.counter(), 0, sizeof(int), s), return false);
         G5Args a;
         a.ipos = i_dev ? i_dev : st.irecs();
         a.jpos = jpos;
@@ -430,7 +425,7 @@ bool compute(Dev& d, int kind, int ni, const float4* ih) {
     const float4* jpos = kind == G5_QUAD ? d.cd.p : d.jd.p;
     const float4* jaux = kind == G5_QUAD ? d.cqd.p : (kind == G5_SYMMETRIC ? d.jed.p : nullptr);
     if (!d.L.stage(d.stream, tasks, groups, rows, ih, ni)) return false;
-    if (!d.L.launch(kind, d.stream, nullptr, jpos, jaux, d.outd.p, false)) return false;
+    if (!d.L.launch(kind, d.stream, nullptr, jpos, jaux, d.outd.p)) return false;
     if (ni > 0)
         PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(d.outh.p, d.outd.p, (size_t)ni * sizeof(double4),
                                                 cudaMemcpyDeviceToHost, d.stream), return false);
@@ -903,7 +898,8 @@ PGB_EXPORT int pgb5_plan_create(pgb5_plan** out, int kind, int nitem, const int*
     long long work = 0;
     for (int k = 0; k < nitem; k++) work += (long long)items[4 * k + 1] * items[4 * k + 3];
     P->rows = 0;
-    long long per_task = work / (4LL * slots) + 1;
+    // a single item: one wave of equal tasks; many uneven items: about 4 tasks per resident CTA
+    long long per_task = work / ((nitem == 1 ? 1LL : 4LL) * slots) + 1;
     for (int k = 0; k < nitem; k++) {
         int ni = items[4 * k + 1], nj = items[4 * k + 3];
         if (ni < 0 || nj < 0 || items[4 * k] < 0 || items[4 * k + 2] < 0) {
@@ -912,9 +908,15 @@ PGB_EXPORT int pgb5_plan_create(pgb5_plan** out, int kind, int nitem, const int*
             return PGB_ERR_ARG;
         }
         long long tile_i = ni < ITILE ? ni : ITILE;
-        long long jc = tile_i > 0 ? per_task / tile_i : nj;
-        if (jc < 256) jc = 256;
-        if (jc * 512 < nj) jc = (nj + 511) / 512;
+        long long jc;
+        if (nitem == 1) {
+            // one item of equal tasks: the chunk count that minimises the wave quantisation
+            jc = choose_jchunk((ni + ITILE - 1) / ITILE, nj, slots);
+        } else {
+            jc = tile_i > 0 ? per_task / tile_i : nj;
+            if (jc < 256) jc = 256;
+            if (jc * 512 < nj) jc = (nj + 511) / 512;
+        }
         if (jc > nj) jc = nj > 0 ? nj : 1;
         P->rows += plan_item(P->tasks, P->groups, items[4 * k], ni, items[4 * k + 2], nj, ITILE, (int)jc, P->rows);
         P->interactions += (long long)ni * nj;
@@ -953,7 +955,7 @@ PGB_EXPORT int pgb5_plan_launch(pgb5_plan* P, const void* ipos, const void* jpos
         raise(g_err, LIB, PGB_ERR_ARG, "pgb5_plan_launch: null device pointer");
         return PGB_ERR_ARG;
     }
-    if (!P->L.launch(P->kind, s, (const float4*)ipos, (const float4*)jpos, (const float4*)jaux, (double4*)out, true))
+    if (!P->L.launch(P->kind, s, (const float4*)ipos, (const float4*)jpos, (const float4*)jaux, (double4*)out))
         return g_err.code ? g_err.code : PGB_ERR_CUDA;
     return PGB_OK;
 }

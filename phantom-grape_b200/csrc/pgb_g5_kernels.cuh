@@ -134,11 +134,11 @@ __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
         for (int k = threadIdx.x; k < A.tbl_size; k += NT) stab[k] = A.table[k];
         shift = A.tbl_shift;
         tab = stab - (0x40000000u >> shift);  // index by (bits of s) >> shift directly
-        // (visibility of stab is ensured by the __syncthreads in next_task)
+        __syncthreads();
     }
 
-    for (;;) {
-        int t = next_task(A.task_counter, &s_task);
+    for (bool first = true;; first = false) {
+        int t = next_task(A.task_counter, &s_task, A.ntasks, first);
         if (t >= A.ntasks) break;
         const Task T = A.tasks[t];
 
@@ -218,12 +218,24 @@ __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
                 const int li = base + threadIdx.x / P, p = threadIdx.x % P;
                 double4 s = make_double4(0, 0, 0, 0);
                 if (li < G.ni) {
-                    for (int c = p; c < G.nchunk; c += P) {
-                        const double4* r = A.partial + (size_t)(G.slot0 + c) * A.itile + li;
-                        double4 v;
-                        v.x = __ldcg(&r->x); v.y = __ldcg(&r->y); v.z = __ldcg(&r->z); v.w = __ldcg(&r->w);
-                        s = add4(s, v);
+                    // four independent partial sums keep four rows' loads in flight; combined in
+                    // a fixed order (deterministic)
+                    const double4* col = A.partial + (size_t)G.slot0 * A.itile + li;
+                    auto ld = [&](int c) {
+                        const double4* r = col + (size_t)c * A.itile;
+                        return make_double4(__ldcg(&r->x), __ldcg(&r->y), __ldcg(&r->z), __ldcg(&r->w));
+                    };
+                    double4 s1 = s, s2 = s, s3 = s;
+                    int c = p;
+                    for (; c + 3 * P < G.nchunk; c += 4 * P) {
+                        double4 v0 = ld(c), v1 = ld(c + P), v2 = ld(c + 2 * P), v3 = ld(c + 3 * P);
+                        s = add4(s, v0);
+                        s1 = add4(s1, v1);
+                        s2 = add4(s2, v2);
+                        s3 = add4(s3, v3);
                     }
+                    for (; c < G.nchunk; c += P) s = add4(s, ld(c));
+                    s = add4(add4(s, s1), add4(s2, s3));
                 }
                 __syncthreads();
                 red[threadIdx.x] = s;

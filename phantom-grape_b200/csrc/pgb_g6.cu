@@ -85,16 +85,16 @@ constexpr int CFG_JL[NCFG] = {8, 2, 1, 1, 1, 1};
 inline int cfg_itile(int c) { return CFG_NT[c] / CFG_JL[c] * CFG_IPT[c]; }
 constexpr int ITILE_MAX = 512;
 
-template <int NT, int IPT, int JL, bool FF>
+template <int NT, int IPT, int JL, bool FF, int NIP = 0>
 int occ_of(bool nn, bool nbl) {
     static int v[4] = {0, 0, 0, 0};
     int k = (nn ? 1 : 0) + (nbl ? 2 : 0);
     if (!v[k]) {
         int b = 0;
-        if (k == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, JL, FF, false, false>, NT, 0);
-        if (k == 1) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, JL, FF, true, false>, NT, 0);
-        if (k == 2) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, JL, FF, false, true>, NT, 0);
-        if (k == 3) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, JL, FF, true, true>, NT, 0);
+        if (k == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, JL, FF, false, false, NIP>, NT, 0);
+        if (k == 1) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, JL, FF, true, false, NIP>, NT, 0);
+        if (k == 2) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, JL, FF, false, true, NIP>, NT, 0);
+        if (k == 3) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, JL, FF, true, true, NIP>, NT, 0);
         v[k] = b > 0 ? b : 1;
     }
     return v[k];
@@ -116,12 +116,12 @@ int occupancy(int cfg, bool ff, bool nn, bool nbl) {
     return ff ? occupancy_ff<true>(cfg, nn, nbl) : occupancy_ff<false>(cfg, nn, nbl);
 }
 
-template <int NT, int IPT, int JL, bool FF>
-void launch_cfg(bool nn, bool nbl, int grid, const G6Args& a, cudaStream_t s) {
-    if (nn && nbl) g6_kernel<NT, IPT, JL, FF, true, true><<<grid, NT, 0, s>>>(a);
-    else if (nn) g6_kernel<NT, IPT, JL, FF, true, false><<<grid, NT, 0, s>>>(a);
-    else if (nbl) g6_kernel<NT, IPT, JL, FF, false, true><<<grid, NT, 0, s>>>(a);
-    else g6_kernel<NT, IPT, JL, FF, false, false><<<grid, NT, 0, s>>>(a);
+template <int NT, int IPT, int JL, bool FF, int NIP = 0>
+void launch_cfg(bool nn, bool nbl, int grid, const G6Args& a, cudaStream_t s, const G6IBlock<NIP>& ib = {}) {
+    if (nn && nbl) g6_kernel<NT, IPT, JL, FF, true, true, NIP><<<grid, NT, 0, s>>>(a, ib);
+    else if (nn) g6_kernel<NT, IPT, JL, FF, true, false, NIP><<<grid, NT, 0, s>>>(a, ib);
+    else if (nbl) g6_kernel<NT, IPT, JL, FF, false, true, NIP><<<grid, NT, 0, s>>>(a, ib);
+    else g6_kernel<NT, IPT, JL, FF, false, false, NIP><<<grid, NT, 0, s>>>(a, ib);
 }
 
 template <bool FF>
@@ -139,6 +139,22 @@ void launch_ff(int cfg, bool nn, bool nbl, int grid, const G6Args& a, cudaStream
 cudaError_t launch_kernel(int cfg, bool ff, bool nn, bool nbl, int grid, const G6Args& a, cudaStream_t s) {
     if (ff) launch_ff<true>(cfg, nn, nbl, grid, a, s);
     else launch_ff<false>(cfg, nn, nbl, grid, a, s);
+    return cudaGetLastError();
+}
+
+// Small calls of the drop-in API (one i-tile of the 512-thread configuration): the i-records
+// travel in the kernel's parameter block.
+constexpr int IBLOCK = 64;
+static_assert(IBLOCK == CFG_NT[CFG_SMALL] / CFG_JL[CFG_SMALL] * CFG_IPT[CFG_SMALL], "i-block = small i-tile");
+
+int occupancy_iblock(bool ff, bool nn, bool nbl) {
+    return ff ? occ_of<512, 1, 8, true, IBLOCK>(nn, nbl) : occ_of<512, 1, 8, false, IBLOCK>(nn, nbl);
+}
+
+cudaError_t launch_iblock(bool ff, bool nn, bool nbl, int grid, const G6Args& a, const G6IBlock<IBLOCK>& ib,
+                          cudaStream_t s) {
+    if (ff) launch_cfg<512, 1, 8, true, IBLOCK>(nn, nbl, grid, a, s, ib);
+    else launch_cfg<512, 1, 8, false, IBLOCK>(nn, nbl, grid, a, s, ib);
     return cudaGetLastError();
 }
 
@@ -175,17 +191,26 @@ long long plan_items(std::vector<Task>& tasks, std::vector<Group>& groups, int& 
         long long tiles = (ni + itile - 1) / itile;
         work += tiles * itile * (long long)items[4 * k + 3];
     }
-    // about 4 tasks per resident CTA for load balance; a small call (one i-tile, the drop-in
-    // API's npipes-sized calls) instead gets one wave of one fat task per resident CTA, which
-    // keeps the number of partial rows (the reduction depth) low
-    long long per_task = (cfg == CFG_SMALL) ? work / slots + 1 : work / (4LL * slots) + 1;
+    // about 4 tasks per resident CTA for load balance of uneven items; a single item (equal
+    // tasks) or a small call (the drop-in API's npipes-sized calls) instead gets one wave of one
+    // fat task per resident CTA, which keeps the number of partial rows (the reduction depth) low
+    long long per_task = (cfg == CFG_SMALL || nitem == 1) ? work / slots + 1 : work / (4LL * slots) + 1;
     long long inter = 0;
     rows = 0;
+    static const long long maxch = env_int("PGB_G6_MAXCHUNKS", 512, 1, 4096);
     for (int k = 0; k < nitem; k++) {
         int ni = items[4 * k + 1], nj = items[4 * k + 3];
-        long long jc = per_task / itile;
-        if (jc < 128) jc = 128;
-        if (jc * 512 < nj) jc = (nj + 511) / 512;
+        long long jc;
+        if (nitem == 1) {
+            // one item of equal tasks: the chunk count that minimises the wave quantisation
+            long long itiles = (ni + itile - 1) / itile;
+            int nch = best_nch(itiles, nj, slots, (int)maxch);
+            jc = (nj + nch - 1) / nch;
+        } else {
+            jc = per_task / itile;
+            if (jc < 128) jc = 128;
+            if (jc * maxch < nj) jc = (nj + maxch - 1) / maxch;
+        }
         if (jc > nj) jc = nj > 0 ? nj : 1;
         rows += plan_item(tasks, groups, items[4 * k], ni, items[4 * k + 2], nj, itile, (int)jc, rows);
         inter += (long long)ni * nj;
@@ -218,8 +243,9 @@ struct State {
     double ti = 0.0;
     int predict_flag = 0;
     HostBuf<G6I> ibuf;
-    DevBuf<G6Out> outd;
-    HostBuf<G6Out> outh;
+    HostBuf<G6Out> outh;    // mapped: the kernel writes the final results into it
+    DevBuf<int> pcnt;       // task counter of the parameter-block launches (self-resetting)
+    G6IBlock<IBLOCK> iblk;  // their i-records
     Stager<G6I, G6Out> st;
     // neighbour lists of the last lasthalf*n call
     DevBuf<int> nbc_d, nbl_d;
@@ -312,32 +338,58 @@ bool flush_and_predict(int nj) {
     return true;
 }
 
+// One drop-in API call: ni i-particles (in S.ibuf) against j-records [0, nj).  The kernel runs in
+// regular mode (it derives its i-tile x j-chunk tasks from the shape, so no task list is
+// uploaded; its task counter resets itself) and writes the final results straight into the
+// mapped pinned buffer S.outh, so no device-to-host copy follows.  A call of at most one small
+// i-tile (the reference's 48 pipes) passes its i-records in the kernel's parameter block: the
+// whole call is then one kernel launch and one stream synchronisation.
 bool run_force(int nj, int ni, float eps2, bool nn, bool nbl) {
-    std::vector<Task> tasks;
-    std::vector<Group> groups;
-    int rows = 0;
-    int cfg = pick_cfg(ni);
-    int item[4] = {0, ni, 0, nj};
+    const int cfg = pick_cfg(ni);
     const bool ff = dx_ff();
-    plan_items(tasks, groups, rows, 1, item, cfg, ff, nn, nbl);
-    PGB_CUDA_OR(g_err, LIB, S.st.stage(S.stream, tasks, groups, rows, ITILE_MAX, S.ibuf.p, ni), return false);
-    PGB_CUDA_OR(g_err, LIB, S.outd.reserve(ni), return false);
-    PGB_CUDA_OR(g_err, LIB, S.outh.reserve(ni), return false);
+    const int itile = cfg_itile(cfg);
+    const bool iblock = (cfg == CFG_SMALL && ni <= IBLOCK);
+    const int slots = sm_count(g_device) * (iblock ? occupancy_iblock(ff, nn, nbl) : occupancy(cfg, ff, nn, nbl));
+    static const int maxch = env_int("PGB_G6_MAXCHUNKS", 512, 1, 4096);
+    const int itiles = (ni + itile - 1) / itile;
+    int nch = best_nch(itiles, nj, slots, maxch);
+    if (nch > nj) nch = nj > 0 ? nj : 1;
+    const int rows = nch > 1 ? itiles * nch : 0;
+    if (iblock) {
+        PGB_CUDA_OR(g_err, LIB, S.st.reserve_scratch(S.stream, rows, ITILE_MAX, (size_t)itiles), return false);
+        if (!S.pcnt.p) {
+            PGB_CUDA_OR(g_err, LIB, S.pcnt.reserve(1), return false);
+            PGB_CUDA_OR(g_err, LIB, S.pcnt.zero_fill(S.stream), return false);
+        }
+    } else {
+        static const std::vector<Task> no_tasks;
+        static const std::vector<Group> no_groups;
+        PGB_CUDA_OR(g_err, LIB,
+                    S.st.stage(S.stream, no_tasks, no_groups, rows, ITILE_MAX, S.ibuf.p, ni, (size_t)itiles),
+                    return false);
+    }
+    PGB_CUDA_OR(g_err, LIB, S.outh.reserve(ni, false, cudaHostAllocPortable | cudaHostAllocMapped), return false);
+    G6Out* out_dev = nullptr;
+    PGB_CUDA_OR(g_err, LIB, cudaHostGetDevicePointer((void**)&out_dev, S.outh.p, 0), return false);
     G6Args a;
-    a.ipart = S.st.irecs();
+    a.ipart = iblock ? nullptr : S.st.irecs();
     a.jpred = S.pred.p;
     a.eps2 = eps2;
-    a.tasks = S.st.tasks();
-    a.ntasks = S.st.ntasks;
-    a.task_counter = S.st.counter();
-    a.groups = S.st.groups();
+    a.tasks = nullptr;
+    a.ntasks = itiles * nch;
+    a.task_counter = iblock ? S.pcnt.p : S.st.counter();
+    a.groups = nullptr;
     a.group_counters = S.st.dgcnt.p;
     a.partial = S.st.dpart.p;
-    a.out = S.outd.p;
-    a.itile = cfg_itile(cfg);
+    a.out = out_dev;
+    a.itile = itile;
+    a.bundle_counters = S.st.bundle_counters();
     a.nb_count = nullptr;
     a.nb_list = nullptr;
     a.nb_maxlen = nbmax();
+    a.reg_ni = ni;
+    a.reg_nj = nj;
+    a.reg_nch = nch;
     if (nbl) {
         PGB_CUDA_OR(g_err, LIB, S.nbc_d.reserve(ni), return false);
         PGB_CUDA_OR(g_err, LIB, S.nbl_d.reserve((size_t)ni * nbmax()), return false);
@@ -346,9 +398,13 @@ bool run_force(int nj, int ni, float eps2, bool nn, bool nbl) {
         a.nb_list = S.nbl_d.p;
     }
     if (a.ntasks == 0) return true;
-    int slots = sm_count(g_device) * occupancy(cfg, ff, nn, nbl);
-    int grid = a.ntasks < slots ? a.ntasks : slots;
-    PGB_CUDA_OR(g_err, LIB, launch_kernel(cfg, ff, nn, nbl, grid, a, S.stream), return false);
+    const int grid = a.ntasks < slots ? a.ntasks : slots;
+    if (iblock) {
+        std::memcpy(S.iblk.rec, S.ibuf.p, (size_t)ni * sizeof(G6I));
+        PGB_CUDA_OR(g_err, LIB, launch_iblock(ff, nn, nbl, grid, a, S.iblk, S.stream), return false);
+    } else {
+        PGB_CUDA_OR(g_err, LIB, launch_kernel(cfg, ff, nn, nbl, grid, a, S.stream), return false);
+    }
     return true;
 }
 
@@ -415,8 +471,6 @@ int lasthalf_impl(int nj, int ni, const int* pidx, const double (*pos)[3], const
     bool nn = (nnb != nullptr);
     // eps2 is a per-call scalar, used as float (phantom_g6.c:191)
     if (!run_force(nj, ni, (float)eps2, nn, nbl)) return 0;
-    PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(S.outh.p, S.outd.p, (size_t)ni * sizeof(G6Out),
-                                            cudaMemcpyDeviceToHost, S.stream), return 0);
     PGB_CUDA_OR(g_err, LIB, cudaStreamSynchronize(S.stream), return 0);
     for (int i = 0; i < ni; i++) {
         const G6Out& o = S.outh.p[i];
@@ -452,8 +506,8 @@ PGB_EXPORT void g6_close(int gpid) {
     cudaStreamSynchronize(S.stream);
     S.jd.release();
     S.pred.release();
-    S.outd.release();
     S.st.release();
+    S.pcnt.release();
     S.nbc_d.release();
     S.nbl_d.release();
     S.sbuf_d.release();
@@ -771,7 +825,6 @@ PGB_EXPORT int pgb6_plan_launch(pgb6_plan* P, const void* ipart, const void* jpr
     if (!ensure_device()) return PGB_ERR_NOGPU;
     if (P->st.ntasks == 0) return PGB_OK;
     cudaStream_t s = (cudaStream_t)stream;
-    PGB_CUDA_OR(g_err, LIB, cudaMemsetAsync(P->st.counter(), 0, sizeof(int), s), return PGB_ERR_CUDA);
     G6Args a;
     a.ipart = (const G6I*)ipart;
     a.jpred = (const G6PredJ*)jpred;
@@ -784,6 +837,7 @@ PGB_EXPORT int pgb6_plan_launch(pgb6_plan* P, const void* ipart, const void* jpr
     a.partial = P->st.dpart.p;
     a.out = (G6Out*)out;
     a.itile = cfg_itile(P->cfg);
+    a.bundle_counters = P->st.bundle_counters();
     a.nb_count = nullptr;
     a.nb_list = nullptr;
     a.nb_maxlen = 0;

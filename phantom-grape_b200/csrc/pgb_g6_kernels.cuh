@@ -93,7 +93,30 @@ struct G6Args {
     int* nb_count;
     int* nb_list;
     int nb_maxlen;
+    // regular mode (tasks == nullptr): one item of reg_ni i against reg_nj j, split into
+    // ceil(reg_ni/itile) i-tiles x reg_nch j-chunks, task t = (i-tile t / nch, chunk t % nch)
+    int reg_ni = 0, reg_nj = 0, reg_nch = 1;
+    // per partial row (zero, self-cleaning): arrival counters of the two-level reduction of
+    // groups with many chunks; nullptr: every group is reduced in one level
+    int* bundle_counters = nullptr;
 };
+
+// The task and group of regular mode (the same decomposition plan_item() writes out).
+__device__ __forceinline__ Task regular_task(const G6Args& A, int t) {
+    const int nch = A.reg_nch;
+    const int it = t / nch, c = t % nch;
+    const int i0 = it * A.itile;
+    const int nii = min(A.itile, A.reg_ni - i0);
+    if (nch == 1) return Task{i0, nii, 0, A.reg_nj, -1, 0, -1, 0};
+    const int j0 = (int)((long long)c * A.reg_nj / nch);
+    const int j1 = (int)((long long)(c + 1) * A.reg_nj / nch);
+    return Task{i0, nii, j0, j1 - j0, it, c, it * nch + c, 0};
+}
+
+__device__ __forceinline__ Group regular_group(const G6Args& A, int g) {
+    const int i0 = g * A.itile;
+    return Group{i0, min(A.itile, A.reg_ni - i0), A.reg_nch, g * A.reg_nch};
+}
 
 // FP64 predictor: one thread per j (gravity.c:149-193; velocity stored as float, :168-173).
 // ff: store the predicted position in the double-float layout.
@@ -198,22 +221,6 @@ __device__ __forceinline__ G6Out g6_finish(const G6Out& s) {
     return o;
 }
 
-__device__ __forceinline__ G6Out ldcg_out(const G6Out* p) {
-    G6Out v;
-    const double* d = reinterpret_cast<const double*>(p);
-    v.ax = __ldcg(d + 0);
-    v.ay = __ldcg(d + 1);
-    v.az = __ldcg(d + 2);
-    v.jx = __ldcg(d + 3);
-    v.jy = __ldcg(d + 4);
-    v.jz = __ldcg(d + 5);
-    v.pot = __ldcg(d + 6);
-    const float* f = reinterpret_cast<const float*>(d + 7);
-    v.key = __ldcg(f);
-    v.jadr = __ldcg(reinterpret_cast<const int*>(f + 1));
-    return v;
-}
-
 // (key, j address) order of the nearest-neighbour search: smaller key, ties to the smaller
 // address -- independent of the order in which partial results are combined.
 __device__ __forceinline__ bool nn_better(float k1, int a1, float k0, int a0) {
@@ -230,12 +237,108 @@ __device__ __forceinline__ void out_add(G6Out& s, const G6Out& v) {
     }
 }
 
+// Chunks per bundle of the two-level group reduction: ceil(sqrt(nchunk)) for groups of more
+// than 16 chunks (when bundle counters exist), else the whole group in one level.
+__device__ __forceinline__ int bundle_size(int nchunk, bool two_level) {
+    if (!two_level || nchunk <= 16) return nchunk;
+    int b = (int)sqrtf((float)nchunk);
+    while (b * b < nchunk) b++;
+    return b;
+}
+
+// A G6Out is four 16-byte words: (ax, ay) (az, jx) (jy, jz) (pot, key|jadr).  Word 3's second
+// half packs the nearest-neighbour key (low 32 bits) and j address (high 32 bits).
+__device__ __forceinline__ double2 word_add(double2 s, double2 v, bool w3) {
+    s.x += v.x;
+    if (!w3) {
+        s.y += v.y;
+    } else {
+        const long long a = __double_as_longlong(s.y), b = __double_as_longlong(v.y);
+        if (nn_better(__int_as_float((int)(b & 0xffffffffLL)), (int)(b >> 32),
+                      __int_as_float((int)(a & 0xffffffffLL)), (int)(a >> 32)))
+            s.y = v.y;
+    }
+    return s;
+}
+
+__device__ __forceinline__ double2 word_zero(bool w3) {
+    // word 3: key +inf, address -1 (every real candidate is better)
+    return make_double2(0.0, w3 ? __longlong_as_double((long long)0xffffffff7f800000ULL) : 0.0);
+}
+
+// Sum `nrows` partial rows of `ni` G6Out (row r at base + r*stride) word by word: thread
+// (g, f) of R = NT/(4 ni) row groups sums word f of rows g, g+R, ... (coalesced 16-byte loads
+// through L2, four rows in flight), then the R group sums are added in group order through
+// shared memory W (NT words).  The order is fixed for a given (NT, ni, nrows): deterministic.
+// finish: write the final scaled result (acc, jerk x -1/8, pot x 1/2) instead of the raw sum.
+// dst may be row 0 itself (every word is read before it is written).
+template <int NT>
+__device__ __forceinline__ void reduce_rows(const G6Out* base, size_t stride, int nrows, int ni, G6Out* dst,
+                                            bool finish, double2* W) {
+    const int nw = 4 * ni;
+    const int R = (2 * nw <= NT) ? NT / nw : 1;
+    const double2* src = reinterpret_cast<const double2*>(base);
+    double2* out = reinterpret_cast<double2*>(dst);
+    const size_t wstride = 4 * stride;
+    for (int f0 = 0; f0 < nw; f0 += (R > 1 ? nw : NT)) {
+        const int g = (R > 1) ? threadIdx.x / nw : 0;
+        const int f = (R > 1) ? threadIdx.x % nw : f0 + threadIdx.x;
+        const bool w3 = (f & 3) == 3;
+        double2 s0 = word_zero(w3);
+        if (g < R && f < nw) {
+            double2 s1 = s0, s2 = s0, s3 = s0;
+            const double2* col = src + f;
+            int r = g;
+            for (; r + 3 * R < nrows; r += 4 * R) {
+                const double2 v0 = __ldcg(col + (size_t)r * wstride);
+                const double2 v1 = __ldcg(col + (size_t)(r + R) * wstride);
+                const double2 v2 = __ldcg(col + (size_t)(r + 2 * R) * wstride);
+                const double2 v3 = __ldcg(col + (size_t)(r + 3 * R) * wstride);
+                s0 = word_add(s0, v0, w3);
+                s1 = word_add(s1, v1, w3);
+                s2 = word_add(s2, v2, w3);
+                s3 = word_add(s3, v3, w3);
+            }
+            for (; r < nrows; r += R) s0 = word_add(s0, __ldcg(col + (size_t)r * wstride), w3);
+            s0 = word_add(s0, s1, w3);
+            s0 = word_add(s0, s2, w3);
+            s0 = word_add(s0, s3, w3);
+        }
+        if (R > 1) {
+            __syncthreads();
+            W[threadIdx.x] = s0;
+            __syncthreads();
+            if (threadIdx.x >= nw) continue;
+            for (int q = 1; q < R; q++) s0 = word_add(s0, W[q * nw + threadIdx.x], w3);
+        } else if (f >= nw) {
+            continue;
+        }
+        if (finish) {
+            s0.x *= w3 ? 0.5 : -0.125;
+            if (!w3) s0.y *= -0.125;
+        }
+        out[f] = s0;
+    }
+}
+
 // Thread layout of a CTA: NT threads = JL j-lanes x ISL i-slots (ISL = NT/JL, whole warps per
 // lane so that the shared-memory j reads stay warp-broadcasts).  A thread owns IPT i-particles
 // li = slot + k*ISL of the task's i-tile (ITILE = ISL*IPT) and every JL-th j of each j-tile.
 // The j-lanes are summed in lane order through shared memory at the end of the task.
-template <int NT, int IPT, int JL, bool FF, bool NN, bool NBL>
-__global__ void __launch_bounds__(NT) g6_kernel(G6Args A) {
+// The i-records of a small call passed by value in the kernel's parameter block (read from
+// the constant bank), which saves the host-to-device copy of a separate upload.
+template <int N>
+struct G6IBlock {
+    G6I rec[N];
+};
+template <>
+struct G6IBlock<0> {
+    int unused;
+};
+
+template <int NT, int IPT, int JL, bool FF, bool NN, bool NBL, int NIP = 0>
+__global__ void __launch_bounds__(NT) g6_kernel(const G6Args A, const __grid_constant__ G6IBlock<NIP> ib) {
+    static_assert(NIP == 0 || NIP >= NT / JL * IPT, "an i-block holds the whole i-tile");
     static_assert(JL == 1 || IPT == 1, "j-lanes are used with one i per thread");
     constexpr int ISL = NT / JL;
     // j tile during the loop, per-thread results (G6Out) after it
@@ -246,10 +349,10 @@ __global__ void __launch_bounds__(NT) g6_kernel(G6Args A) {
     const int slot = threadIdx.x % ISL;
     const int jl = threadIdx.x / ISL;
 
-    for (;;) {
-        int t = next_task(A.task_counter, &s_task);
+    for (bool first = true;; first = false) {
+        int t = next_task(A.task_counter, &s_task, A.ntasks, first);
         if (t >= A.ntasks) break;
-        const Task T = A.tasks[t];
+        const Task T = A.tasks ? A.tasks[t] : regular_task(A, t);
 
         Pos3 pi[IPT];
         float vxi[IPT], vyi[IPT], vzi[IPT], hinv[IPT];
@@ -261,7 +364,9 @@ __global__ void __launch_bounds__(NT) g6_kernel(G6Args A) {
         for (int k = 0; k < IPT; k++) {
             int li = slot + k * ISL;
             int ii = T.i0 + (li < T.ni ? li : 0);
-            const G6I P = A.ipart[ii];
+            G6I P;
+            if constexpr (NIP > 0) P = ib.rec[ii];
+            else P = A.ipart[ii];
             pi[k] = P.p;
             vxi[k] = P.vx; vyi[k] = P.vy; vzi[k] = P.vz;
             idi[k] = P.id;
@@ -329,32 +434,26 @@ __global__ void __launch_bounds__(NT) g6_kernel(G6Args A) {
             else A.out[T.i0 + li] = g6_finish(o);
         }
         if (!dst_row) continue;
-        const Group G = A.groups[T.group];
-        if (group_arrive(A.group_counters, T.group, G.nchunk, &s_flag)) {
-            // Cooperative reduction of the group's partial rows: P threads per i, each summing a
-            // fixed strided subset of rows, then the P partial sums in thread order
-            // (deterministic for a given group shape).
-            int P = 1;
-            while (P * 2 * G.ni <= NT) P *= 2;
-            const int per = NT / P;
-            for (int base = 0; base < G.ni; base += per) {
-                const int li = base + threadIdx.x / P, p = threadIdx.x % P;
-                G6Out s;
-                s.ax = s.ay = s.az = s.jx = s.jy = s.jz = s.pot = 0.0;
-                s.key = INFINITY;
-                s.jadr = -1;
-                if (li < G.ni) {
-                    const G6Out* col = A.partial + (size_t)G.slot0 * A.itile + li;
-                    for (int c = p; c < G.nchunk; c += P) out_add(s, ldcg_out(col + (size_t)c * A.itile));
-                }
-                __syncthreads();
-                red[threadIdx.x] = s;
-                __syncthreads();
-                if (p == 0 && li < G.ni) {
-                    for (int q = 1; q < P; q++) out_add(s, red[threadIdx.x + q]);
-                    A.out[G.i0 + li] = g6_finish(s);
-                }
-            }
+        const Group G = A.groups ? A.groups[T.group] : regular_group(A, T.group);
+        double2* W = reinterpret_cast<double2*>(smem);
+        const int B = bundle_size(G.nchunk, A.bundle_counters != nullptr);
+        if (B < G.nchunk) {
+            // two levels: the last CTA of each bundle of B consecutive chunks sums the bundle's
+            // rows into the bundle's first row, the last bundle of the group sums those
+            const int b = T.chunk / B;
+            const int r0 = G.slot0 + b * B;
+            const int nbk = min(B, G.nchunk - b * B);
+            if (!group_arrive(A.bundle_counters, r0, nbk, &s_flag)) continue;
+            G6Out* row0 = A.partial + (size_t)r0 * A.itile;
+            reduce_rows<NT>(row0, (size_t)A.itile, nbk, G.ni, row0, false, W);
+            const int nb = (G.nchunk + B - 1) / B;
+            if (!group_arrive(A.group_counters, T.group, nb, &s_flag)) continue;
+            reduce_rows<NT>(A.partial + (size_t)G.slot0 * A.itile, (size_t)B * A.itile, nb, G.ni, A.out + G.i0, true,
+                            W);
+        } else {
+            if (!group_arrive(A.group_counters, T.group, G.nchunk, &s_flag)) continue;
+            reduce_rows<NT>(A.partial + (size_t)G.slot0 * A.itile, (size_t)A.itile, G.nchunk, G.ni, A.out + G.i0,
+                            true, W);
         }
     }
 }
