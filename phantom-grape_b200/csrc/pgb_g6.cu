@@ -24,6 +24,7 @@
 //    g6_read_neighbour_list and refused by g6_get_neighbour_list, never written out of bounds
 //    (gravity.c:896-906 writes before it checks).
 #include "pgb_g6_kernels.cuh"
+#include "pgb_g6_small.cuh"
 
 using namespace pgb;
 
@@ -85,16 +86,16 @@ constexpr int CFG_JL[NCFG] = {8, 2, 1, 1, 1, 1};
 inline int cfg_itile(int c) { return CFG_NT[c] / CFG_JL[c] * CFG_IPT[c]; }
 constexpr int ITILE_MAX = 512;
 
-template <int NT, int IPT, int JL, bool FF, int NIP = 0>
+template <int NT, int IPT, int JL, bool FF>
 int occ_of(bool nn, bool nbl) {
     static int v[4] = {0, 0, 0, 0};
     int k = (nn ? 1 : 0) + (nbl ? 2 : 0);
     if (!v[k]) {
         int b = 0;
-        if (k == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, JL, FF, false, false, NIP>, NT, 0);
-        if (k == 1) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, JL, FF, true, false, NIP>, NT, 0);
-        if (k == 2) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, JL, FF, false, true, NIP>, NT, 0);
-        if (k == 3) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, JL, FF, true, true, NIP>, NT, 0);
+        if (k == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, JL, FF, false, false>, NT, 0);
+        if (k == 1) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, JL, FF, true, false>, NT, 0);
+        if (k == 2) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, JL, FF, false, true>, NT, 0);
+        if (k == 3) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, JL, FF, true, true>, NT, 0);
         v[k] = b > 0 ? b : 1;
     }
     return v[k];
@@ -116,12 +117,12 @@ int occupancy(int cfg, bool ff, bool nn, bool nbl) {
     return ff ? occupancy_ff<true>(cfg, nn, nbl) : occupancy_ff<false>(cfg, nn, nbl);
 }
 
-template <int NT, int IPT, int JL, bool FF, int NIP = 0>
-void launch_cfg(bool nn, bool nbl, int grid, const G6Args& a, cudaStream_t s, const G6IBlock<NIP>& ib = {}) {
-    if (nn && nbl) g6_kernel<NT, IPT, JL, FF, true, true, NIP><<<grid, NT, 0, s>>>(a, ib);
-    else if (nn) g6_kernel<NT, IPT, JL, FF, true, false, NIP><<<grid, NT, 0, s>>>(a, ib);
-    else if (nbl) g6_kernel<NT, IPT, JL, FF, false, true, NIP><<<grid, NT, 0, s>>>(a, ib);
-    else g6_kernel<NT, IPT, JL, FF, false, false, NIP><<<grid, NT, 0, s>>>(a, ib);
+template <int NT, int IPT, int JL, bool FF>
+void launch_cfg(bool nn, bool nbl, int grid, const G6Args& a, cudaStream_t s) {
+    if (nn && nbl) g6_kernel<NT, IPT, JL, FF, true, true><<<grid, NT, 0, s>>>(a);
+    else if (nn) g6_kernel<NT, IPT, JL, FF, true, false><<<grid, NT, 0, s>>>(a);
+    else if (nbl) g6_kernel<NT, IPT, JL, FF, false, true><<<grid, NT, 0, s>>>(a);
+    else g6_kernel<NT, IPT, JL, FF, false, false><<<grid, NT, 0, s>>>(a);
 }
 
 template <bool FF>
@@ -142,20 +143,88 @@ cudaError_t launch_kernel(int cfg, bool ff, bool nn, bool nbl, int grid, const G
     return cudaGetLastError();
 }
 
-// Small calls of the drop-in API (one i-tile of the 512-thread configuration): the i-records
-// travel in the kernel's parameter block.
-constexpr int IBLOCK = 64;
-static_assert(IBLOCK == CFG_NT[CFG_SMALL] / CFG_JL[CFG_SMALL] * CFG_IPT[CFG_SMALL], "i-block = small i-tile");
+// The small-call cluster kernel (pgb_g6_small.cuh): i-slots x j-lanes by the call's i count.
+struct SmallShape {
+    int isl, jl;
+};
+inline SmallShape small_shape(int ni) {
+    if (ni <= 16) return {16, 32};
+    if (ni <= 32) return {32, 16};
+    if (ni <= 48) return {48, 10};
+    return {64, 8};
+}
+constexpr int SMALL_CL = 8;  // CTAs per cluster (portable maximum)
 
-int occupancy_iblock(bool ff, bool nn, bool nbl) {
-    return ff ? occ_of<512, 1, 8, true, IBLOCK>(nn, nbl) : occ_of<512, 1, 8, false, IBLOCK>(nn, nbl);
+template <int ISL, int JL, bool FF, bool NN, bool NBL>
+cudaError_t small_launch(int grid, int cl, const G6SmallArgs& a, const G6IBlock& ib, cudaStream_t s,
+                         int* max_clusters) {
+    auto kern = g6_small_kernel<ISL, JL, FF, NN, NBL>;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = cl;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(ISL * JL);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    if (max_clusters) return cudaOccupancyMaxActiveClusters(max_clusters, (void*)kern, &cfg);
+    return cudaLaunchKernelEx(&cfg, kern, a, ib);
 }
 
-cudaError_t launch_iblock(bool ff, bool nn, bool nbl, int grid, const G6Args& a, const G6IBlock<IBLOCK>& ib,
-                          cudaStream_t s) {
-    if (ff) launch_cfg<512, 1, 8, true, IBLOCK>(nn, nbl, grid, a, s, ib);
-    else launch_cfg<512, 1, 8, false, IBLOCK>(nn, nbl, grid, a, s, ib);
-    return cudaGetLastError();
+template <int ISL, int JL, bool FF>
+cudaError_t small_launch_nn(bool nn, bool nbl, int grid, int cl, const G6SmallArgs& a,
+                            const G6IBlock& ib, cudaStream_t s, int* mc) {
+    if (nn && nbl) return small_launch<ISL, JL, FF, true, true>(grid, cl, a, ib, s, mc);
+    if (nn) return small_launch<ISL, JL, FF, true, false>(grid, cl, a, ib, s, mc);
+    if (nbl) return small_launch<ISL, JL, FF, false, true>(grid, cl, a, ib, s, mc);
+    return small_launch<ISL, JL, FF, false, false>(grid, cl, a, ib, s, mc);
+}
+
+template <bool FF>
+cudaError_t small_launch_ff(SmallShape sh, bool nn, bool nbl, int grid, int cl, const G6SmallArgs& a,
+                            const G6IBlock& ib, cudaStream_t s, int* mc) {
+    if (sh.isl == 16) return small_launch_nn<16, 32, FF>(nn, nbl, grid, cl, a, ib, s, mc);
+    if (sh.isl == 32) return small_launch_nn<32, 16, FF>(nn, nbl, grid, cl, a, ib, s, mc);
+    if (sh.isl == 48) return small_launch_nn<48, 10, FF>(nn, nbl, grid, cl, a, ib, s, mc);
+    return small_launch_nn<64, 8, FF>(nn, nbl, grid, cl, a, ib, s, mc);
+}
+
+// Launch (mc == nullptr) or query the co-resident clusters of cl CTAs (into *mc).
+cudaError_t small_kernel(SmallShape sh, bool ff, bool nn, bool nbl, int grid, int cl, const G6SmallArgs& a,
+                         const G6IBlock& ib, cudaStream_t s, int* mc) {
+    return ff ? small_launch_ff<true>(sh, nn, nbl, grid, cl, a, ib, s, mc)
+              : small_launch_ff<false>(sh, nn, nbl, grid, cl, a, ib, s, mc);
+}
+
+// Chunks (= CTAs, all co-resident) and cluster size of a small call over nj j-records: at least
+// 128 j per chunk, at most the co-resident clusters' CTAs (queried once per kernel variant).
+void small_grid(SmallShape sh, bool ff, bool nn, bool nbl, int nj, int& grid, int& cl) {
+    static int cache[4][2][2][2] = {};
+    const int v = sh.isl / 16 - 1;
+    int& mc = cache[v][ff][nn][nbl];
+    if (!mc) {
+        G6SmallArgs a{};
+        G6IBlock ib{};
+        int n = 0;
+        if (small_kernel(sh, ff, nn, nbl, SMALL_CL, SMALL_CL, a, ib, nullptr, &n) != cudaSuccess || n < 1) {
+            cudaGetLastError();
+            n = sm_count(g_device) / SMALL_CL;
+        }
+        mc = n;
+    }
+    static const int forced = env_int("PGB_G6_SMALL_CTAS", 0, 0, 1 << 16);
+    int by_j = nj / 128;
+    int want = mc * SMALL_CL;
+    if (forced) want = std::min(want, forced);
+    want = std::min(want, by_j);
+    if (want < 1) want = 1;
+    cl = 1;
+    while (cl < SMALL_CL && cl * 2 <= want) cl *= 2;
+    grid = want / cl * cl;
 }
 
 // Relative-coordinate arithmetic of the library's own calls: double-float (default) or FP64
@@ -244,8 +313,9 @@ struct State {
     int predict_flag = 0;
     HostBuf<G6I> ibuf;
     HostBuf<G6Out> outh;    // mapped: the kernel writes the final results into it
-    DevBuf<int> pcnt;       // task counter of the parameter-block launches (self-resetting)
-    G6IBlock<IBLOCK> iblk;  // their i-records
+    DevBuf<int> pcnt;       // self-resetting counters of the parameter-block launches
+    G6IBlock iblk;  // their i-records
+    DevBuf<G6Out> spart;    // cluster rows of the small-call kernel
     Stager<G6I, G6Out> st;
     // neighbour lists of the last lasthalf*n call
     DevBuf<int> nbc_d, nbl_d;
@@ -338,46 +408,72 @@ bool flush_and_predict(int nj) {
     return true;
 }
 
-// One drop-in API call: ni i-particles (in S.ibuf) against j-records [0, nj).  The kernel runs in
-// regular mode (it derives its i-tile x j-chunk tasks from the shape, so no task list is
-// uploaded; its task counter resets itself) and writes the final results straight into the
-// mapped pinned buffer S.outh, so no device-to-host copy follows.  A call of at most one small
-// i-tile (the reference's 48 pipes) passes its i-records in the kernel's parameter block: the
-// whole call is then one kernel launch and one stream synchronisation.
+// The small-call path: one launch of the cluster kernel (i-records in its parameter block),
+// results into the mapped buffer; the call is one launch and one stream synchronisation.
+bool run_small(int nj, int ni, float eps2, bool nn, bool nbl, G6Out* out_dev) {
+    const bool ff = dx_ff();
+    const SmallShape sh = small_shape(ni);
+    int grid = 1, cl = 1;
+    small_grid(sh, ff, nn, nbl, nj, grid, cl);
+    PGB_CUDA_OR(g_err, LIB, S.spart.reserve((size_t)(grid / cl) * sh.isl), return false);
+    if (!S.pcnt.p) {
+        PGB_CUDA_OR(g_err, LIB, S.pcnt.reserve(SMALL_CL), return false);
+        PGB_CUDA_OR(g_err, LIB, S.pcnt.zero_fill(S.stream), return false);
+    }
+    G6SmallArgs a;
+    a.jpred = S.pred.p;
+    a.eps2 = eps2;
+    a.ni = ni;
+    a.nj = nj;
+    a.partial = S.spart.p;
+    a.counter = S.pcnt.p;
+    a.out = out_dev;
+    a.nb_count = nullptr;
+    a.nb_list = nullptr;
+    a.nb_maxlen = nbmax();
+    if (nbl) {
+        PGB_CUDA_OR(g_err, LIB, S.nbc_d.reserve(ni), return false);
+        PGB_CUDA_OR(g_err, LIB, S.nbl_d.reserve((size_t)ni * nbmax()), return false);
+        PGB_CUDA_OR(g_err, LIB, cudaMemsetAsync(S.nbc_d.p, 0, (size_t)ni * sizeof(int), S.stream), return false);
+        a.nb_count = S.nbc_d.p;
+        a.nb_list = S.nbl_d.p;
+    }
+    std::memcpy(S.iblk.rec, S.ibuf.p, (size_t)ni * sizeof(G6I));
+    PGB_CUDA_OR(g_err, LIB, small_kernel(sh, ff, nn, nbl, grid, cl, a, S.iblk, S.stream, nullptr), return false);
+    return true;
+}
+
+// One drop-in API call: ni i-particles (in S.ibuf) against j-records [0, nj), results into
+// the mapped pinned buffer S.outh (the kernel writes them there: no device-to-host copy).
+// Up to G6_SMALL_MAXI i-particles (the reference's 48 pipes): the small-call cluster kernel, one
+// launch.  More (PGB_G6_NPIPES > 64): the general kernel in regular mode -- it derives its i-tile
+// x j-chunk tasks from the shape, so only the i-records are uploaded, and its task counter
+// resets itself.
 bool run_force(int nj, int ni, float eps2, bool nn, bool nbl) {
+    PGB_CUDA_OR(g_err, LIB, S.outh.reserve(ni, false, cudaHostAllocPortable | cudaHostAllocMapped), return false);
+    G6Out* out_dev = nullptr;
+    PGB_CUDA_OR(g_err, LIB, cudaHostGetDevicePointer((void**)&out_dev, S.outh.p, 0), return false);
+    if (ni <= G6_SMALL_MAXI && nj > 0) return run_small(nj, ni, eps2, nn, nbl, out_dev);
     const int cfg = pick_cfg(ni);
     const bool ff = dx_ff();
     const int itile = cfg_itile(cfg);
-    const bool iblock = (cfg == CFG_SMALL && ni <= IBLOCK);
-    const int slots = sm_count(g_device) * (iblock ? occupancy_iblock(ff, nn, nbl) : occupancy(cfg, ff, nn, nbl));
+    const int slots = sm_count(g_device) * occupancy(cfg, ff, nn, nbl);
     static const int maxch = env_int("PGB_G6_MAXCHUNKS", 512, 1, 4096);
     const int itiles = (ni + itile - 1) / itile;
     int nch = best_nch(itiles, nj, slots, maxch);
     if (nch > nj) nch = nj > 0 ? nj : 1;
     const int rows = nch > 1 ? itiles * nch : 0;
-    if (iblock) {
-        PGB_CUDA_OR(g_err, LIB, S.st.reserve_scratch(S.stream, rows, ITILE_MAX, (size_t)itiles), return false);
-        if (!S.pcnt.p) {
-            PGB_CUDA_OR(g_err, LIB, S.pcnt.reserve(1), return false);
-            PGB_CUDA_OR(g_err, LIB, S.pcnt.zero_fill(S.stream), return false);
-        }
-    } else {
-        static const std::vector<Task> no_tasks;
-        static const std::vector<Group> no_groups;
-        PGB_CUDA_OR(g_err, LIB,
-                    S.st.stage(S.stream, no_tasks, no_groups, rows, ITILE_MAX, S.ibuf.p, ni, (size_t)itiles),
-                    return false);
-    }
-    PGB_CUDA_OR(g_err, LIB, S.outh.reserve(ni, false, cudaHostAllocPortable | cudaHostAllocMapped), return false);
-    G6Out* out_dev = nullptr;
-    PGB_CUDA_OR(g_err, LIB, cudaHostGetDevicePointer((void**)&out_dev, S.outh.p, 0), return false);
+    static const std::vector<Task> no_tasks;
+    static const std::vector<Group> no_groups;
+    PGB_CUDA_OR(g_err, LIB, S.st.stage(S.stream, no_tasks, no_groups, rows, ITILE_MAX, S.ibuf.p, ni, (size_t)itiles),
+                return false);
     G6Args a;
-    a.ipart = iblock ? nullptr : S.st.irecs();
+    a.ipart = S.st.irecs();
     a.jpred = S.pred.p;
     a.eps2 = eps2;
     a.tasks = nullptr;
     a.ntasks = itiles * nch;
-    a.task_counter = iblock ? S.pcnt.p : S.st.counter();
+    a.task_counter = S.st.counter();
     a.groups = nullptr;
     a.group_counters = S.st.dgcnt.p;
     a.partial = S.st.dpart.p;
@@ -399,12 +495,7 @@ bool run_force(int nj, int ni, float eps2, bool nn, bool nbl) {
     }
     if (a.ntasks == 0) return true;
     const int grid = a.ntasks < slots ? a.ntasks : slots;
-    if (iblock) {
-        std::memcpy(S.iblk.rec, S.ibuf.p, (size_t)ni * sizeof(G6I));
-        PGB_CUDA_OR(g_err, LIB, launch_iblock(ff, nn, nbl, grid, a, S.iblk, S.stream), return false);
-    } else {
-        PGB_CUDA_OR(g_err, LIB, launch_kernel(cfg, ff, nn, nbl, grid, a, S.stream), return false);
-    }
+    PGB_CUDA_OR(g_err, LIB, launch_kernel(cfg, ff, nn, nbl, grid, a, S.stream), return false);
     return true;
 }
 
@@ -508,6 +599,7 @@ PGB_EXPORT void g6_close(int gpid) {
     S.pred.release();
     S.st.release();
     S.pcnt.release();
+    S.spart.release();
     S.nbc_d.release();
     S.nbl_d.release();
     S.sbuf_d.release();

@@ -266,29 +266,42 @@ __device__ __forceinline__ double2 word_zero(bool w3) {
     return make_double2(0.0, w3 ? __longlong_as_double((long long)0xffffffff7f800000ULL) : 0.0);
 }
 
-// Sum `nrows` partial rows of `ni` G6Out (row r at base + r*stride) word by word: thread
-// (g, f) of R = NT/(4 ni) row groups sums word f of rows g, g+R, ... (coalesced 16-byte loads
-// through L2, four rows in flight), then the R group sums are added in group order through
-// shared memory W (NT words).  The order is fixed for a given (NT, ni, nrows): deterministic.
-// finish: write the final scaled result (acc, jerk x -1/8, pot x 1/2) instead of the raw sum.
-// dst may be row 0 itself (every word is read before it is written).
+// Sum `nrows` partial rows (row r at base + r*stride G6Out) word by word over the words
+// [wbeg, wbeg + nw) of a row (4 words per G6Out): thread (g, f) of R <= NT/nw row groups sums word
+// f of rows g, g+R, ... (coalesced 16-byte loads through L2, up to eight rows in flight), then
+// the R group sums are added in group order through shared memory W (NT words).  The order is
+// fixed for a given (NT, nw, nrows): deterministic.  finish: write the final scaled result (acc,
+// jerk x -1/8, pot x 1/2) instead of the raw sum.  dst (same word indexing) may be row 0 itself:
+// every word is read before it is written.
 template <int NT>
-__device__ __forceinline__ void reduce_rows(const G6Out* base, size_t stride, int nrows, int ni, G6Out* dst,
-                                            bool finish, double2* W) {
-    const int nw = 4 * ni;
-    const int R = (2 * nw <= NT) ? NT / nw : 1;
+__device__ __forceinline__ void reduce_rows(const G6Out* base, size_t stride, int nrows, int wbeg, int nw,
+                                            G6Out* dst, bool finish, double2* W) {
+    // row groups: as many as the threads allow, but no more than the rows and at most 8 (their
+    // sums are combined serially)
+    const int R = (2 * nw <= NT) ? min(min(NT / nw, nrows), 8) : 1;
     const double2* src = reinterpret_cast<const double2*>(base);
     double2* out = reinterpret_cast<double2*>(dst);
     const size_t wstride = 4 * stride;
-    for (int f0 = 0; f0 < nw; f0 += (R > 1 ? nw : NT)) {
+    for (int k0 = 0; k0 < nw; k0 += (R > 1 ? nw : NT)) {
         const int g = (R > 1) ? threadIdx.x / nw : 0;
-        const int f = (R > 1) ? threadIdx.x % nw : f0 + threadIdx.x;
+        const int k = (R > 1) ? threadIdx.x % nw : k0 + threadIdx.x;
+        const int f = wbeg + k;
         const bool w3 = (f & 3) == 3;
         double2 s0 = word_zero(w3);
-        if (g < R && f < nw) {
+        if (g < R && k < nw) {
             double2 s1 = s0, s2 = s0, s3 = s0;
             const double2* col = src + f;
             int r = g;
+            // eight rows' loads in flight (L2 latency bound), four running sums
+            for (; r + 7 * R < nrows; r += 8 * R) {
+                double2 v[8];
+#pragma unroll
+                for (int u = 0; u < 8; u++) v[u] = __ldcg(col + (size_t)(r + u * R) * wstride);
+                s0 = word_add(word_add(s0, v[0], w3), v[4], w3);
+                s1 = word_add(word_add(s1, v[1], w3), v[5], w3);
+                s2 = word_add(word_add(s2, v[2], w3), v[6], w3);
+                s3 = word_add(word_add(s3, v[3], w3), v[7], w3);
+            }
             for (; r + 3 * R < nrows; r += 4 * R) {
                 const double2 v0 = __ldcg(col + (size_t)r * wstride);
                 const double2 v1 = __ldcg(col + (size_t)(r + R) * wstride);
@@ -310,7 +323,7 @@ __device__ __forceinline__ void reduce_rows(const G6Out* base, size_t stride, in
             __syncthreads();
             if (threadIdx.x >= nw) continue;
             for (int q = 1; q < R; q++) s0 = word_add(s0, W[q * nw + threadIdx.x], w3);
-        } else if (f >= nw) {
+        } else if (k >= nw) {
             continue;
         }
         if (finish) {
@@ -325,20 +338,8 @@ __device__ __forceinline__ void reduce_rows(const G6Out* base, size_t stride, in
 // lane so that the shared-memory j reads stay warp-broadcasts).  A thread owns IPT i-particles
 // li = slot + k*ISL of the task's i-tile (ITILE = ISL*IPT) and every JL-th j of each j-tile.
 // The j-lanes are summed in lane order through shared memory at the end of the task.
-// The i-records of a small call passed by value in the kernel's parameter block (read from
-// the constant bank), which saves the host-to-device copy of a separate upload.
-template <int N>
-struct G6IBlock {
-    G6I rec[N];
-};
-template <>
-struct G6IBlock<0> {
-    int unused;
-};
-
-template <int NT, int IPT, int JL, bool FF, bool NN, bool NBL, int NIP = 0>
-__global__ void __launch_bounds__(NT) g6_kernel(const G6Args A, const __grid_constant__ G6IBlock<NIP> ib) {
-    static_assert(NIP == 0 || NIP >= NT / JL * IPT, "an i-block holds the whole i-tile");
+template <int NT, int IPT, int JL, bool FF, bool NN, bool NBL>
+__global__ void __launch_bounds__(NT) g6_kernel(const G6Args A) {
     static_assert(JL == 1 || IPT == 1, "j-lanes are used with one i per thread");
     constexpr int ISL = NT / JL;
     // j tile during the loop, per-thread results (G6Out) after it
@@ -364,9 +365,7 @@ __global__ void __launch_bounds__(NT) g6_kernel(const G6Args A, const __grid_con
         for (int k = 0; k < IPT; k++) {
             int li = slot + k * ISL;
             int ii = T.i0 + (li < T.ni ? li : 0);
-            G6I P;
-            if constexpr (NIP > 0) P = ib.rec[ii];
-            else P = A.ipart[ii];
+            const G6I P = A.ipart[ii];
             pi[k] = P.p;
             vxi[k] = P.vx; vyi[k] = P.vy; vzi[k] = P.vz;
             idi[k] = P.id;
@@ -445,14 +444,14 @@ __global__ void __launch_bounds__(NT) g6_kernel(const G6Args A, const __grid_con
             const int nbk = min(B, G.nchunk - b * B);
             if (!group_arrive(A.bundle_counters, r0, nbk, &s_flag)) continue;
             G6Out* row0 = A.partial + (size_t)r0 * A.itile;
-            reduce_rows<NT>(row0, (size_t)A.itile, nbk, G.ni, row0, false, W);
+            reduce_rows<NT>(row0, (size_t)A.itile, nbk, 0, 4 * G.ni, row0, false, W);
             const int nb = (G.nchunk + B - 1) / B;
             if (!group_arrive(A.group_counters, T.group, nb, &s_flag)) continue;
-            reduce_rows<NT>(A.partial + (size_t)G.slot0 * A.itile, (size_t)B * A.itile, nb, G.ni, A.out + G.i0, true,
+            reduce_rows<NT>(A.partial + (size_t)G.slot0 * A.itile, (size_t)B * A.itile, nb, 0, 4 * G.ni, A.out + G.i0, true,
                             W);
         } else {
             if (!group_arrive(A.group_counters, T.group, G.nchunk, &s_flag)) continue;
-            reduce_rows<NT>(A.partial + (size_t)G.slot0 * A.itile, (size_t)A.itile, G.nchunk, G.ni, A.out + G.i0,
+            reduce_rows<NT>(A.partial + (size_t)G.slot0 * A.itile, (size_t)A.itile, G.nchunk, 0, 4 * G.ni, A.out + G.i0,
                             true, W);
         }
     }

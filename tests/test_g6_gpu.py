@@ -112,6 +112,32 @@ def test_hermite_vs_reference_avx2(g6):
     np.testing.assert_allclose(res["rnnb"], ref["rnnb"], rtol=1e-6)
 
 
+@pytest.mark.parametrize("ni,nj", [(1, 1), (5, 100), (16, 300), (17, 700), (31, 1500), (32, 8192), (33, 999),
+                                   (47, 4097), (48, 8192), (48, 129)])
+def test_small_call_shapes_vs_fp64(g6, state, ni, nj):
+    """One g6calc_lasthalf2p call of ni <= 48 i-particles against the first nj j-particles: the
+    small-call kernel's i-slot variants (16/32/48), single-CTA calls (nj < 256) and clusters of
+    2, 4 and 8 CTAs (j-chunks of >= 128 j), each against the FP64 oracle."""
+    st = state
+    g6.set_j(st.pos, st.vel, st.acc2, st.jrk6, st.mass, st.tj, st.idx)
+    active = np.sort(W.Rng(100 + ni).permutation(nj)[:ni]).astype(np.int32)
+    xp, vp = O.g6_predict(st.t_now, st.pos, st.vel, st.acc2, st.jrk6, st.tj)
+    vpf = vp.astype(np.float32).astype(np.float64)
+    mf = st.mass.astype(np.float32).astype(np.float64)
+    ref = O.g6_force(xp[active], vpf[active], st.idx[active], np.float32(st.eps2), xp[:nj], vpf[:nj], mf[:nj],
+                     st.idx[:nj])
+    res = g6.calc(st.t_now, nj, xp[active], vp[active], st.idx[active], st.eps2, variant="2p")
+    if nj == 1:
+        assert np.all(res["acc"] == 0) and np.all(res["pot"] == 0)
+        return
+    ea, ej = rel(res["acc"], ref["acc"]), rel(res["jrk"], ref["jrk"])
+    ep = np.abs(res["pot"] - ref["pot"]) / np.abs(ref["pot"])
+    # rms as for the full calls; the max bounds catch a lost or doubled j-chunk (an O(1e-2) error)
+    assert ea.max() <= 1e-4 and ej.max() <= 1e-2 and ep.max() <= 1e-4, (ea.max(), ej.max(), ep.max())
+    assert rms(ea) <= 1e-6 and rms(ej) <= 1e-5 and rms(ep) <= 1e-6
+    check_nn(res, ref)
+
+
 def test_neighbour_lists_vs_fp64(g6, state):
     st = state
     g6.set_j(st.pos, st.vel, st.acc2, st.jrk6, st.mass, st.tj, st.idx)
