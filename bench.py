@@ -51,6 +51,7 @@ sys.path.insert(0, ROOT)
 SM_COUNT = 148
 # DRAM bytes (read + write) of one launch of the roofline kernel, from the committed ncu captures
 # (dram__bytes_read.sum + dram__bytes_write.sum); the bench cannot run ncu itself.
+G5_CFG_NAMES = ["128x4", "256x2", "512x2", "1024x1", "384x2", "128x2"]   # pgb5 configurations (threads x i/thread)
 PROFILED_TRAFFIC = {
     "hermite": {"bytes": 25_623_040, "source": "profiles/g6_kernel_hermite_65536x65536.md (256x2 configuration)"},
 }
@@ -100,6 +101,11 @@ class ClockSampler:
                  "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
+            return
+        # the sampler is running (its first line written) before the timed region starts
+        t0 = time.time()
+        while time.time() - t0 < 5.0 and os.path.getsize(self.path) == 0 and self.proc.poll() is None:
+            time.sleep(0.02)
 
     def stop(self):
         if self.proc is None:
@@ -551,11 +557,23 @@ def run_direct(args, pgb, ws, rank, local):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     plan = g5.plan_create(g5.NEWTON, [[0, n, 0, n]])
     s = torch.cuda.Stream(device=dev)
+    if not args.no_tune and not args.profile_largest:
+        g5.plan_tune(plan, d_i.data_ptr(), d_j.data_ptr(), None, d_o.data_ptr(), s.cuda_stream)
+    dcfg = g5.L.pgb5_plan_config(plan)
     launch = lambda: g5.plan_launch(plan, d_i.data_ptr(), d_j.data_ptr(), None, d_o.data_ptr(), s.cuda_stream)  # noqa
+    if args.profile_largest:
+        # profiling target: the evaluation's force launch four times; no timing
+        for _ in range(4):
+            launch()
+        s.synchronize()
+        g5.plan_destroy(plan)
+        return {"profile": "PG5 direct evaluation", "n": n, "launches": 4}
     clocks = ClockSampler(local)
     clocks.start()
     barrier(ws)
-    ts = _timed_launches(torch, s, launch, max(args.steps, 50), args.warmup, flush)
+    # one evaluation takes ~0.2 ms: at least 2000 of them, so that the clock sampler (every
+    # 200 ms) sees the timed region
+    ts = _timed_launches(torch, s, launch, max(args.steps, 2000), args.warmup, flush)
     barrier(ws)
     clk = clocks.stop()
     t_local = sum(ts)
@@ -591,7 +609,8 @@ def run_direct(args, pgb, ws, rank, local):
                  {"value": round(e2e_val, 2), "unit": "Gint/s", "h2d_bytes_per_step": n * 16 * 2,
                   "d2h_bytes_per_step": n * 32, "api": "g5_set_xmj + g5_set_eps_to_all + g5_set_n + "
                   "g5_calculate_force_on_x (direct.c:133-176), host buffers"},
-                 cpu, len(ts), kernel="pgb::g5_kernel<NEWTON,128,4>")
+                 cpu, len(ts), extra={"steps": len(ts)},
+                 kernel=f"pgb::g5_kernel<NEWTON,{G5_CFG_NAMES[dcfg]}> (autotuned)")
 
 
 def run_clusters(args, pgb, ws, rank, local):
@@ -695,6 +714,10 @@ def run_treepm(args, pgb, ws, rank, local):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     plan = tab.plan_create(ts_.items)
     s = torch.cuda.Stream(device=dev)
+    tcfg = None
+    if not args.no_tune:
+        tcfg, _ = tab.plan_tune(plan, d_i.data_ptr(), d_j.data_ptr(), d_o.data_ptr(), s.cuda_stream)
+    tcfg = tab.L.pgb5_plan_config(plan)
     launch = lambda: tab.plan_launch(plan, d_i.data_ptr(), d_j.data_ptr(), d_o.data_ptr(), s.cuda_stream)  # noqa
     clocks = ClockSampler(local)
     clocks.start()
@@ -745,7 +768,7 @@ def run_treepm(args, pgb, ws, rank, local):
                   "h2d_bytes_per_step": int(len(xj) * 16 + len(xi) * 16), "d2h_bytes_per_step": int(len(xi) * 32),
                   "api": f"per group g5_set_xmjMC + g5_set_nMC + g5_calculate_force_on_xMC, {nthr} host threads "
                          "(one devid each), host buffers"},
-                 cpu, len(tms), kernel="pgb::g5_kernel<TABLE,128,4>")
+                 cpu, len(tms), kernel=f"pgb::g5_kernel<TABLE,{G5_CFG_NAMES[tcfg]}> (autotuned)")
 
 
 # ----------------------------------------------------------------------------------------
@@ -817,7 +840,8 @@ def main():
     ap.add_argument("--f64-positions", action="store_true",
                     help="FP64 x_j - x_i (DADD + F2F) instead of the double-float subtraction")
     ap.add_argument("--profile-largest", action="store_true",
-                    help="profiling target: set up, warm, then run the largest call's force launch 3 times")
+                    help="profiling target: set up, warm, then run the largest call's force launch 3 times "
+                         "(direct: the evaluation's launch 4 times)")
     ap.add_argument("--profile-api", action="store_true",
                     help="profiling target: four full-size drop-in API calls (48 i x N j) and exit")
     args = ap.parse_args()

@@ -101,8 +101,14 @@ void pgb5_set_abort(int on);                /* 1 (default): abort on error, as a
  * Device layouts: ipos float4 (x, y, z, eps2); jpos float4 (x, y, z, m); jaux: symmetric
  * float4 (eps2_j, 0, 0, 0) per j, quad two float4 (q0 q1 q2 q3)(q4 q5 0 0) per cell;
  * out double4 (ax, ay, az, pot_raw) with pot_raw = -sum m/r (newton) or +sum(phi_p + phi_q)
- * (quad), indexed by absolute i.  pgb5_plan_launch only resets a counter and launches one
- * kernel on `stream` (a cudaStream_t), so it can be captured in a CUDA graph.            */
+ * (quad), indexed by absolute i.  pgb5_plan_launch launches one kernel on `stream` (a
+ * cudaStream_t) and uploads nothing, so it can be captured in a CUDA graph.
+ * pgb5_plan_tune times the plan once per kernel configuration (threads x i per thread) on
+ * the caller's data (out is overwritten), keeps the fastest for this plan and for later
+ * plans of the same shape, and returns its index (-1 on error; *best_ms its launch time).
+ * pgb5_plan_config returns the plan's configuration index; pgb5_plan_set_config pins one
+ * (an error for a configuration the kind cannot use: the table kind takes CTAs of <= 256
+ * threads, the quadrupole kind <= 512).                                                  */
 enum { PGB5_NEWTON = 0, PGB5_SYMMETRIC = 1, PGB5_QUAD = 2, PGB5_TABLE = 3 };
 typedef struct pgb5_plan pgb5_plan;
 int  pgb5_plan_create(pgb5_plan **plan, int kind, int nitem, const int *items);
@@ -111,6 +117,11 @@ int  pgb5_plan_launch(pgb5_plan *plan, const void *ipos, const void *jpos, const
 void pgb5_plan_destroy(pgb5_plan *plan);
 long long pgb5_plan_interactions(const pgb5_plan *plan);
 int  pgb5_plan_tasks(const pgb5_plan *plan);
+int  pgb5_plan_tune(pgb5_plan *plan, const void *ipos, const void *jpos, const void *jaux, void *out,
+                    void *stream, float *best_ms);
+int  pgb5_plan_config(const pgb5_plan *plan);
+int  pgb5_plan_set_config(pgb5_plan *plan, int cfg);   /* pin one (PGB5_NCFG configurations) */
+enum { PGB5_NCFG = 6 };
 
 #ifdef __cplusplus
 }

@@ -45,7 +45,22 @@ constexpr int PARTICLE_KIND = G5_NEWTON;
 ErrorSlot g_err;
 
 constexpr int MAXDEV = 64;
-constexpr int NT = 128, IPT = 4, ITILE = NT * IPT;
+// Kernel configurations: threads per CTA x i-particles per thread.  Large CTAs win on large
+// single items (fewer, longer tasks), small i-tiles on batches of small groups; the table
+// kind keeps its force table in static shared memory (CTAs of <= 256 threads) and the quad
+// kind stages three words per cell (<= 512 threads).  Plans pick one with pgb5_plan_tune.
+enum G5Cfg { G5C_128x4 = 0, G5C_256x2 = 1, G5C_512x2 = 2, G5C_1024x1 = 3, G5C_384x2 = 4, G5C_128x2 = 5, G5_NCFG = 6 };
+constexpr int G5C_NT[G5_NCFG] = {128, 256, 512, 1024, 384, 128};
+constexpr int G5C_IPT[G5_NCFG] = {4, 2, 2, 1, 2, 2};
+constexpr int ITILE_MAX = 1024;
+inline int cfg_itile(int c) { return G5C_NT[c] * G5C_IPT[c]; }
+template <int KIND, int NT>
+constexpr bool kind_fits() {
+    return KIND == G5_TABLE ? NT <= 256 : (KIND == G5_QUAD ? NT <= 512 : true);
+}
+inline bool cfg_valid(int kind, int c) {
+    return kind == G5_TABLE ? G5C_NT[c] <= 256 : (kind == G5_QUAD ? G5C_NT[c] <= 512 : true);
+}
 constexpr int MAXPIPE = 4096;
 
 int env_int(const char* name, int dflt, int lo, int hi) {
@@ -88,34 +103,66 @@ bool ensure_device() {
     return true;
 }
 
+// Launch (occ == nullptr) or query the resident CTAs per SM (into *occ) of one kernel.
+template <int KIND, int NT, int IPT>
+cudaError_t launch_k(int grid, const G5Args& a, cudaStream_t s, int* occ) {
+    if constexpr (!kind_fits<KIND, NT>()) {
+        return cudaErrorInvalidConfiguration;
+    } else {
+        if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, g5_kernel<KIND, NT, IPT>, NT, 0);
+        g5_kernel<KIND, NT, IPT><<<grid, NT, 0, s>>>(a);
+        return cudaGetLastError();
+    }
+}
+
 template <int KIND>
-int occupancy() {
-    static int v = 0;
+cudaError_t launch_cfg(int cfg, int grid, const G5Args& a, cudaStream_t s, int* occ) {
+    switch (cfg) {
+        case G5C_256x2: return launch_k<KIND, 256, 2>(grid, a, s, occ);
+        case G5C_512x2: return launch_k<KIND, 512, 2>(grid, a, s, occ);
+        case G5C_1024x1: return launch_k<KIND, 1024, 1>(grid, a, s, occ);
+        case G5C_384x2: return launch_k<KIND, 384, 2>(grid, a, s, occ);
+        case G5C_128x2: return launch_k<KIND, 128, 2>(grid, a, s, occ);
+        default: return launch_k<KIND, 128, 4>(grid, a, s, occ);
+    }
+}
+
+// The kinds each library serves: the table library the table kind, the others the particle
+// kind of their build plus the quadrupole cells.
+cudaError_t launch_kind(int kind, int cfg, int grid, const G5Args& a, cudaStream_t s, int* occ = nullptr) {
+#ifdef PGB_TABLE
+    (void)kind;
+    return launch_cfg<G5_TABLE>(cfg, grid, a, s, occ);
+#else
+    if (kind == G5_QUAD) return launch_cfg<G5_QUAD>(cfg, grid, a, s, occ);
+    return launch_cfg<PARTICLE_KIND>(cfg, grid, a, s, occ);
+#endif
+}
+
+int occupancy_of(int kind, int cfg) {
+    static int cache[4][G5_NCFG] = {};
+    int& v = cache[kind & 3][cfg];
     if (!v) {
         int b = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g5_kernel<KIND, NT, IPT>, NT, 0);
-        v = b > 0 ? b : 1;
+        G5Args a{};
+        if (launch_kind(kind, cfg, 0, a, nullptr, &b) != cudaSuccess || b < 1) {
+            cudaGetLastError();
+            b = 1;
+        }
+        v = b;
     }
     return v;
 }
 
-int occupancy_of(int kind) {
-    switch (kind) {
-        case G5_SYMMETRIC: return occupancy<G5_SYMMETRIC>();
-        case G5_QUAD: return occupancy<G5_QUAD>();
-        case G5_TABLE: return occupancy<G5_TABLE>();
-        default: return occupancy<G5_NEWTON>();
-    }
-}
-
-cudaError_t launch_kind(int kind, int grid, const G5Args& a, cudaStream_t s) {
-    switch (kind) {
-        case G5_SYMMETRIC: g5_kernel<G5_SYMMETRIC, NT, IPT><<<grid, NT, 0, s>>>(a); break;
-        case G5_QUAD: g5_kernel<G5_QUAD, NT, IPT><<<grid, NT, 0, s>>>(a); break;
-        case G5_TABLE: g5_kernel<G5_TABLE, NT, IPT><<<grid, NT, 0, s>>>(a); break;
-        default: g5_kernel<G5_NEWTON, NT, IPT><<<grid, NT, 0, s>>>(a); break;
-    }
-    return cudaGetLastError();
+// Default configuration of a call or plan whose largest item has ni i-particles (and
+// PGB_G5_CFG forces one for sweeps): big CTAs for big items, 256-particle tiles for groups.
+int pick_cfg(int kind, long long ni_max) {
+    static int forced = env_int("PGB_G5_CFG", -1, -1, G5_NCFG - 1);
+    if (forced >= 0 && cfg_valid(kind, forced)) return forced;
+    if (kind == G5_TABLE || kind == G5_QUAD) return ni_max <= 256 ? G5C_128x2 : G5C_256x2;
+    if (ni_max <= 256) return G5C_128x2;
+    if (ni_max <= 2048) return G5C_256x2;
+    return G5C_1024x1;
 }
 
 // Chunk length for one item: its tasks are all the same size, so one wave of tasks (one per
@@ -249,13 +296,13 @@ struct Launcher {
 
     bool stage(cudaStream_t s, const std::vector<Task>& tasks, const std::vector<Group>& groups, int rows,
                const float4* i_host, int ni_host) {
-        PGB_CUDA_OR(g_err, LIB, st.stage(s, tasks, groups, rows, ITILE, i_host, ni_host), return false);
+        PGB_CUDA_OR(g_err, LIB, st.stage(s, tasks, groups, rows, ITILE_MAX, i_host, ni_host), return false);
         return true;
     }
 
     // Launch over the staged work list.  The kernel leaves its task counter at zero, so the same
     // staged list can be launched again (e.g. from a CUDA graph) without a reset.
-    bool launch(int kind, cudaStream_t s, const float4* i_dev, const float4* jpos, const float4* jaux,
+    bool launch(int kind, int cfg, cudaStream_t s, const float4* i_dev, const float4* jpos, const float4* jaux,
                 double4* out) {
         if (st.ntasks <= 0) return true;
         G5Args a;
@@ -269,16 +316,16 @@ struct Launcher {
         a.group_counters = st.dgcnt.p;
         a.partial = st.dpart.p;
         a.out = out;
-        a.itile = ITILE;
+        a.itile = cfg_itile(cfg);
         a.table = nullptr;
         a.tbl_size = 0;
         a.tbl_shift = 0;
         a.r2cut = 0.f;
         a.ascale = 1.0;
         if (kind == G5_TABLE && !table_args(a)) return false;
-        int slots = sm_count(g_device) * occupancy_of(kind);
+        int slots = sm_count(g_device) * occupancy_of(kind, cfg);
         int grid = st.ntasks < slots ? st.ntasks : slots;
-        PGB_CUDA_OR(g_err, LIB, launch_kind(kind, grid, a, s), return false);
+        PGB_CUDA_OR(g_err, LIB, launch_kind(kind, cfg, grid, a, s), return false);
         return true;
     }
     void release() { st.release(); }
@@ -418,14 +465,16 @@ bool compute(Dev& d, int kind, int ni, const float4* ih) {
     PGB_CUDA_OR(g_err, LIB, d.outh.reserve(ni > 0 ? ni : 1), return false);
     std::vector<Task> tasks;
     std::vector<Group> groups;
-    int slots = sm_count(g_device) * occupancy_of(kind);
-    long long itiles = (ni + ITILE - 1) / ITILE;
+    const int cfg = pick_cfg(kind, ni);
+    const int itile = cfg_itile(cfg);
+    int slots = sm_count(g_device) * occupancy_of(kind, cfg);
+    long long itiles = (ni + itile - 1) / itile;
     int jchunk = choose_jchunk(itiles, nj, slots);
-    int rows = plan_item(tasks, groups, 0, ni, 0, nj, ITILE, jchunk, 0);
+    int rows = plan_item(tasks, groups, 0, ni, 0, nj, itile, jchunk, 0);
     const float4* jpos = kind == G5_QUAD ? d.cd.p : d.jd.p;
     const float4* jaux = kind == G5_QUAD ? d.cqd.p : (kind == G5_SYMMETRIC ? d.jed.p : nullptr);
     if (!d.L.stage(d.stream, tasks, groups, rows, ih, ni)) return false;
-    if (!d.L.launch(kind, d.stream, nullptr, jpos, jaux, d.outd.p)) return false;
+    if (!d.L.launch(kind, cfg, d.stream, nullptr, jpos, jaux, d.outd.p)) return false;
     if (ni > 0)
         PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(d.outh.p, d.outd.p, (size_t)ni * sizeof(double4),
                                                 cudaMemcpyDeviceToHost, d.stream), return false);
@@ -863,6 +912,9 @@ PGB_EXPORT void pgb5_set_abort(int on) {
 
 struct pgb5_plan {
     int kind;
+    int cfg;
+    std::vector<int> items;        // [nitem][4], kept for re-planning by the autotuner
+    long long shape_key = 0;
     std::vector<Task> tasks;
     std::vector<Group> groups;
     int rows;
@@ -882,52 +934,106 @@ bool check_kind(int kind) {
     }
     return true;
 }
-}  // namespace
 
-// items: [nitem][4] = (i_offset, i_count, j_offset, j_count) into the i- and j-arrays.
-PGB_EXPORT int pgb5_plan_create(pgb5_plan** out, int kind, int nitem, const int* items) {
-    if (!out || nitem < 0 || (nitem && !items) || !check_kind(kind)) return PGB_ERR_ARG;
-    if (!ensure_device()) return PGB_ERR_NOGPU;
-    auto* P = new pgb5_plan();
-    P->kind = kind;
-    P->interactions = 0;
-    int slots = sm_count(g_device) * occupancy_of(kind);
-    long long itiles = 0;
-    for (int k = 0; k < nitem; k++) itiles += (items[4 * k + 1] + ITILE - 1) / ITILE;
-    // One chunk length for the whole batch: about 4 tasks per resident CTA in total.
+// Work list of a batch for one configuration.  A single item: one wave of equal tasks; many
+// uneven items: about 4 tasks per resident CTA (j-chunks of >= 256 j, <= 512 chunks per item).
+void plan_items(pgb5_plan* P) {
+    const int nitem = (int)(P->items.size() / 4);
+    const int* items = P->items.data();
+    const int itile = cfg_itile(P->cfg);
+    const int slots = sm_count(g_device) * occupancy_of(P->kind, P->cfg);
     long long work = 0;
     for (int k = 0; k < nitem; k++) work += (long long)items[4 * k + 1] * items[4 * k + 3];
+    const long long per_task = work / ((nitem == 1 ? 1LL : 4LL) * slots) + 1;
+    P->tasks.clear();
+    P->groups.clear();
     P->rows = 0;
-    // a single item: one wave of equal tasks; many uneven items: about 4 tasks per resident CTA
-    long long per_task = work / ((nitem == 1 ? 1LL : 4LL) * slots) + 1;
+    P->interactions = 0;
     for (int k = 0; k < nitem; k++) {
         int ni = items[4 * k + 1], nj = items[4 * k + 3];
-        if (ni < 0 || nj < 0 || items[4 * k] < 0 || items[4 * k + 2] < 0) {
-            delete P;
-            raise(g_err, LIB, PGB_ERR_ARG, "item %d has a negative offset or count", k);
-            return PGB_ERR_ARG;
-        }
-        long long tile_i = ni < ITILE ? ni : ITILE;
+        long long tile_i = ni < itile ? ni : itile;
         long long jc;
         if (nitem == 1) {
             // one item of equal tasks: the chunk count that minimises the wave quantisation
-            jc = choose_jchunk((ni + ITILE - 1) / ITILE, nj, slots);
+            jc = choose_jchunk((ni + itile - 1) / itile, nj, slots);
         } else {
             jc = tile_i > 0 ? per_task / tile_i : nj;
             if (jc < 256) jc = 256;
             if (jc * 512 < nj) jc = (nj + 511) / 512;
         }
         if (jc > nj) jc = nj > 0 ? nj : 1;
-        P->rows += plan_item(P->tasks, P->groups, items[4 * k], ni, items[4 * k + 2], nj, ITILE, (int)jc, P->rows);
+        P->rows += plan_item(P->tasks, P->groups, items[4 * k], ni, items[4 * k + 2], nj, itile, (int)jc, P->rows);
         P->interactions += (long long)ni * nj;
     }
     // longest tasks first (persistent CTAs then finish together)
     std::stable_sort(P->tasks.begin(), P->tasks.end(), [](const Task& a, const Task& b) {
         return (long long)a.ni * a.nj > (long long)b.ni * b.nj;
     });
+}
+
+// Autotune results by batch shape (kind, item count, largest item), shared by later plans.
+std::mutex g_tune_mu;
+std::vector<std::pair<long long, int>> g_tune;
+
+int ilog2up(long long v) {
+    int b = 0;
+    while ((1LL << b) < v) b++;
+    return b;
+}
+
+long long shape_key(int kind, int nitem, const int* items) {
+    long long nimax = 0, njmax = 0;
+    for (int k = 0; k < nitem; k++) {
+        nimax = std::max<long long>(nimax, items[4 * k + 1]);
+        njmax = std::max<long long>(njmax, items[4 * k + 3]);
+    }
+    return ((long long)ilog2up(nitem + 1) << 24) | ((long long)ilog2up(nimax + 1) << 16) |
+           ((long long)ilog2up(njmax + 1) << 8) | kind;
+}
+
+int tuned_cfg(long long key) {
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    for (auto& e : g_tune)
+        if (e.first == key) return e.second;
+    return -1;
+}
+
+void set_tuned(long long key, int cfg) {
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    for (auto& e : g_tune)
+        if (e.first == key) {
+            e.second = cfg;
+            return;
+        }
+    g_tune.emplace_back(key, cfg);
+}
+
+bool stage_plan(pgb5_plan* P, cudaStream_t s) {
+    return P->L.stage(s, P->tasks, P->groups, P->rows, nullptr, 0);
+}
+}  // namespace
+
+// items: [nitem][4] = (i_offset, i_count, j_offset, j_count) into the i- and j-arrays.
+PGB_EXPORT int pgb5_plan_create(pgb5_plan** out, int kind, int nitem, const int* items) {
+    if (!out || nitem < 0 || (nitem && !items) || !check_kind(kind)) return PGB_ERR_ARG;
+    for (int k = 0; k < nitem; k++)
+        if (items[4 * k + 1] < 0 || items[4 * k + 3] < 0 || items[4 * k] < 0 || items[4 * k + 2] < 0) {
+            raise(g_err, LIB, PGB_ERR_ARG, "item %d has a negative offset or count", k);
+            return PGB_ERR_ARG;
+        }
+    if (!ensure_device()) return PGB_ERR_NOGPU;
+    auto* P = new pgb5_plan();
+    P->kind = kind;
+    P->items.assign(items, items + 4 * (size_t)nitem);
+    P->shape_key = shape_key(kind, nitem, items);
+    long long nimax = 0;
+    for (int k = 0; k < nitem; k++) nimax = std::max<long long>(nimax, items[4 * k + 1]);
+    const int tuned = tuned_cfg(P->shape_key);
+    P->cfg = tuned >= 0 ? tuned : pick_cfg(kind, nimax);
+    plan_items(P);
     cudaStream_t s = nullptr;
     bool ok = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess;
-    ok = ok && P->L.stage(s, P->tasks, P->groups, P->rows, nullptr, 0);
+    ok = ok && stage_plan(P, s);
     ok = ok && cudaStreamSynchronize(s) == cudaSuccess;
     if (s) cudaStreamDestroy(s);
     if (!ok) {
@@ -955,8 +1061,83 @@ PGB_EXPORT int pgb5_plan_launch(pgb5_plan* P, const void* ipos, const void* jpos
         raise(g_err, LIB, PGB_ERR_ARG, "pgb5_plan_launch: null device pointer");
         return PGB_ERR_ARG;
     }
-    if (!P->L.launch(P->kind, s, (const float4*)ipos, (const float4*)jpos, (const float4*)jaux, (double4*)out))
+    if (!P->L.launch(P->kind, P->cfg, s, (const float4*)ipos, (const float4*)jpos, (const float4*)jaux,
+                     (double4*)out))
         return g_err.code ? g_err.code : PGB_ERR_CUDA;
+    return PGB_OK;
+}
+
+// Autotuner: launches the plan with every kernel configuration valid for its kind on the
+// caller's data, keeps the fastest (CUDA-event time, best of 2 after a warm-up launch),
+// re-stages the plan with it and records it for later plans of the same shape.  Returns the
+// chosen configuration index (-1 on error); *best_ms (optional) receives its launch time.
+// Overwrites `out`.  Not capturable (it synchronises the stream).
+PGB_EXPORT int pgb5_plan_tune(pgb5_plan* P, const void* ipos, const void* jpos, const void* jaux, void* out,
+                              void* stream, float* best_ms) {
+    if (!P || !ipos || !jpos || !out) {
+        raise(g_err, LIB, PGB_ERR_ARG, "pgb5_plan_tune: null argument");
+        return -1;
+    }
+    if (!ensure_device()) return -1;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaEvent_t e0, e1;
+    PGB_CUDA_OR(g_err, LIB, cudaEventCreate(&e0), return -1);
+    PGB_CUDA_OR(g_err, LIB, cudaEventCreate(&e1), return -1);
+    int best = P->cfg;
+    float best_t = 1e30f;
+    for (int cfg = 0; cfg < G5_NCFG; cfg++) {
+        if (!cfg_valid(P->kind, cfg)) continue;
+        P->cfg = cfg;
+        plan_items(P);
+        if (!stage_plan(P, s)) break;
+        float t = 1e30f;
+        for (int rep = 0; rep < 3; rep++) {
+            cudaEventRecord(e0, s);
+            if (pgb5_plan_launch(P, ipos, jpos, jaux, out, stream) != PGB_OK) break;
+            cudaEventRecord(e1, s);
+            cudaEventSynchronize(e1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (rep > 0 && ms < t) t = ms;
+        }
+        if (t < best_t) {
+            best_t = t;
+            best = cfg;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    P->cfg = best;
+    plan_items(P);
+    if (!stage_plan(P, s)) return -1;
+    PGB_CUDA_OR(g_err, LIB, cudaStreamSynchronize(s), return -1);
+    set_tuned(P->shape_key, best);
+    if (best_ms) *best_ms = best_t;
+    return best;
+}
+
+PGB_EXPORT int pgb5_plan_config(const pgb5_plan* P) { return P ? P->cfg : -1; }
+
+// Pin the plan's kernel configuration (0 .. PGB5_NCFG-1; not every one serves every kind) and
+// re-stage its work list.
+PGB_EXPORT int pgb5_plan_set_config(pgb5_plan* P, int cfg) {
+    if (!P || cfg < 0 || cfg >= G5_NCFG || !cfg_valid(P->kind, cfg)) {
+        raise(g_err, LIB, PGB_ERR_ARG, "pgb5_plan_set_config: configuration %d not valid for kind %d", cfg,
+              P ? P->kind : -1);
+        return PGB_ERR_ARG;
+    }
+    if (!ensure_device()) return PGB_ERR_NOGPU;
+    P->cfg = cfg;
+    plan_items(P);
+    cudaStream_t s = nullptr;
+    bool ok = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess;
+    ok = ok && stage_plan(P, s);
+    ok = ok && cudaStreamSynchronize(s) == cudaSuccess;
+    if (s) cudaStreamDestroy(s);
+    if (!ok) {
+        raise(g_err, LIB, PGB_ERR_CUDA, "pgb5_plan_set_config: staging failed");
+        return PGB_ERR_CUDA;
+    }
     return PGB_OK;
 }
 

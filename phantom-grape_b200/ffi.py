@@ -121,6 +121,9 @@ class G5(_ErrMixin):
         _sig(L, "pgb5_plan_destroy", [vp])
         _sig(L, "pgb5_plan_interactions", [vp], C.c_longlong)
         _sig(L, "pgb5_plan_tasks", [vp], C.c_int)
+        _sig(L, "pgb5_plan_tune", [vp, vp, vp, vp, vp, vp, C.POINTER(C.c_float)], C.c_int)
+        _sig(L, "pgb5_plan_config", [vp], C.c_int)
+        _sig(L, "pgb5_plan_set_config", [vp, C.c_int], C.c_int)
 
     # convenience wrappers with numpy arrays -------------------------------------------------
     def set_xmj(self, adr, xj, mj, epsj2=None, devid=None):
@@ -185,6 +188,14 @@ class G5(_ErrMixin):
         rc = self.L.pgb5_plan_launch(plan, ipos, jpos, jaux, out, stream)
         if rc:
             raise RuntimeError(f"pgb5_plan_launch failed: {self.last_error()}")
+
+    def plan_tune(self, plan, ipos, jpos, jaux, out, stream=0):
+        """Autotune the plan's kernel configuration on these device arrays; (cfg, ms)."""
+        ms = C.c_float(0)
+        cfg = self.L.pgb5_plan_tune(plan, ipos, jpos, jaux, out, stream, C.byref(ms))
+        if cfg < 0:
+            raise RuntimeError(f"pgb5_plan_tune failed: {self.last_error()}")
+        return cfg, ms.value
 
     def plan_destroy(self, plan):
         self.L.pgb5_plan_destroy(plan)
@@ -425,6 +436,9 @@ class G5Table(_ErrMixin):
         _sig(L, "pgb5_plan_destroy", [vp])
         _sig(L, "pgb5_plan_interactions", [vp], C.c_longlong)
         _sig(L, "pgb5_plan_tasks", [vp], C.c_int)
+        _sig(L, "pgb5_plan_tune", [vp, vp, vp, vp, vp, vp, C.POINTER(C.c_float)], C.c_int)
+        _sig(L, "pgb5_plan_config", [vp], C.c_int)
+        _sig(L, "pgb5_plan_set_config", [vp, C.c_int], C.c_int)
         self._cb = None
 
     def set_table(self, func, rcut, frc_bit=None):
@@ -468,6 +482,14 @@ class G5Table(_ErrMixin):
         rc = self.L.pgb5_plan_launch(plan, ipos, jpos, None, out, stream)
         if rc:
             raise RuntimeError(f"pgb5_plan_launch failed: {self.last_error()}")
+
+    def plan_tune(self, plan, ipos, jpos, out, stream=0):
+        """Autotune the plan's kernel configuration on these device arrays; (cfg, ms)."""
+        ms = C.c_float(0)
+        cfg = self.L.pgb5_plan_tune(plan, ipos, jpos, None, out, stream, C.byref(ms))
+        if cfg < 0:
+            raise RuntimeError(f"pgb5_plan_tune failed: {self.last_error()}")
+        return cfg, ms.value
 
     def plan_destroy(self, plan):
         self.L.pgb5_plan_destroy(plan)

@@ -119,12 +119,29 @@ def test_treepm_groups_batched_vs_fp64(tab):
     d_j = torch.from_numpy(jp).to(dev)
     d_o = torch.zeros((len(ts.xi), 4), dtype=torch.float64, device=dev)
     plan = tab.plan_create(ts.items)
+    outs = []
     try:
-        tab.plan_launch(plan, d_i.data_ptr(), d_j.data_ptr(), d_o.data_ptr(), torch.cuda.current_stream().cuda_stream)
-        torch.cuda.synchronize()
-        out = d_o.cpu().numpy()
+        # the kernel configurations the table kind can use (CTAs of <= 256 threads); the others
+        # are refused
+        for cfg in range(6):
+            if cfg in (2, 3, 4):
+                tab.set_abort(False)
+                try:
+                    assert tab.L.pgb5_plan_set_config(plan, cfg) != 0
+                finally:
+                    tab.set_abort(True)
+                continue
+            rc = tab.L.pgb5_plan_set_config(plan, cfg)
+            assert rc == 0
+            tab.plan_launch(plan, d_i.data_ptr(), d_j.data_ptr(), d_o.data_ptr(),
+                            torch.cuda.current_stream().cuda_stream)
+            torch.cuda.synchronize()
+            outs.append(d_o.cpu().numpy().copy())
     finally:
         tab.plan_destroy(plan)
+    out = outs[0]
+    for o in outs[1:]:
+        assert rms(rel(o[:, :3], out[:, :3])) <= 1e-6
     errs = []
     for k in range(0, len(ts.items), 7):
         i0, ni, j0, nj = ts.items[k]
