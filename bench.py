@@ -51,7 +51,7 @@ sys.path.insert(0, ROOT)
 SM_COUNT = 148
 # DRAM bytes (read + write) of one launch of the roofline kernel, from the committed ncu captures
 # (dram__bytes_read.sum + dram__bytes_write.sum); the bench cannot run ncu itself.
-G5_CFG_NAMES = ["128x4", "256x2", "512x2", "1024x1", "384x2", "128x2"]   # pgb5 configurations (threads x i/thread)
+G5_CFG_NAMES = ["128x4", "256x2", "512x2", "1024x1", "384x2", "128x2", "128x1", "64x1"]   # pgb5 configurations (threads x i/thread)
 PROFILED_TRAFFIC = {
     "hermite": {"bytes": 25_623_040, "source": "profiles/g6_kernel_hermite_65536x65536.md (256x2 configuration)"},
 }
@@ -236,6 +236,10 @@ class Driver:
         L.g5drv_direct.restype = C.c_double
         L.g5drv_groups.argtypes = [vp, C.c_int, ip, dp, dp, dp, C.c_double, dp, dp, C.c_int]
         L.g5drv_groups.restype = C.c_double
+        lp = C.POINTER(C.c_longlong)
+        L.g5drv_bh.argtypes = [vp, C.c_int, C.c_int, ip, ip, dp, dp, dp, lp, ip, dp, dp, dp, lp, ip, C.c_double, dp, dp,
+                               C.c_int]
+        L.g5drv_bh.restype = C.c_double
 
     @staticmethod
     def p(a, t=C.c_double):
@@ -528,7 +532,7 @@ def _line(args, ws, metric, value, t_step, pairs, flop, workload, dtype, achieve
         "vs_baseline": None, "dtype": dtype, "data": "synthetic (seeded; no dataset)",
         "config": {"workload": workload, "pairs_per_step": pairs, "flop_per_pair": flop,
                    "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{ws}"},
-        "frac_fp32": round(value * 1e9 * flop / 1e12 / peak_tf, 4),
+        "frac_fp32": round((value * 1e9 * flop / 1e12 if isinstance(flop, (int, float)) else achieved_tf) / peak_tf, 4),
         "roofline": {"bound": "fp32", "achieved": round(achieved_tf, 2), "peak": round(peak_tf, 2), "unit": "TFLOP/s",
                      "frac": round(achieved_tf / peak_tf, 4), "traffic": None, "kernel": kernel,
                      "peak_source": f"148 SM x 128 FP32 lanes x 2 x median SM clock {sm_mhz:.0f} MHz"},
@@ -771,6 +775,172 @@ def run_treepm(args, pgb, ws, rank, local):
                  cpu, len(tms), kernel=f"pgb::g5_kernel<TABLE,{G5_CFG_NAMES[tcfg]}> (autotuned)")
 
 
+def run_bh(args, pgb, ws, rank, local):
+    """Barnes-Hut with quadrupole cells (newton_quad): N = 2^22 Hernquist sphere, theta = 0.5,
+    groups of <= 256, leaves of <= 16 particles; per evaluation one index-list launch over every
+    group's point-mass list (PG5 newton, 38 flop/pair) and one over every group's cell list
+    (quadrupole kernel, 60 flop/pair)."""
+    import torch
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    W = pgb.workloads
+    g5 = pgb.ffi.G5()
+    g5.L.g5_open()
+    t0 = time.time()
+    bh = W.bh_hernquist(args.bh_n, seed=W.SEED0 + 3 + rank)
+    t_tree = time.time() - t0
+    ip, pp, cp, cq = bh.records()
+    d_i, d_p = torch.from_numpy(ip).to(dev), torch.from_numpy(pp).to(dev)
+    d_c, d_q = torch.from_numpy(cp).to(dev), torch.from_numpy(cq).to(dev)
+    d_pi, d_ci = torch.from_numpy(bh.pidx).to(dev), torch.from_numpy(bh.cidx).to(dev)
+    o_p = torch.zeros((len(ip), 4), dtype=torch.float64, device=dev)
+    o_c = torch.zeros((len(ip), 4), dtype=torch.float64, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    s = torch.cuda.Stream(device=dev)
+    pl_p = g5.plan_create(g5.NEWTON, bh.items("p"))
+    pl_c = g5.plan_create(g5.QUAD, bh.items("c"))
+    args_p = (d_i.data_ptr(), d_p.data_ptr(), None, d_pi.data_ptr(), o_p.data_ptr(), s.cuda_stream)
+    args_c = (d_i.data_ptr(), d_c.data_ptr(), d_q.data_ptr(), d_ci.data_ptr(), o_c.data_ptr(), s.cuda_stream)
+    if not args.no_tune:
+        g5.plan_tune_indexed(pl_p, *args_p)
+        g5.plan_tune_indexed(pl_c, *args_c)
+    cfg_p, cfg_c = g5.L.pgb5_plan_config(pl_p), g5.L.pgb5_plan_config(pl_c)
+
+    def launch():
+        g5.plan_launch_indexed(pl_p, *args_p)
+        g5.plan_launch_indexed(pl_c, *args_c)
+
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        launch()   # outside capture once (lazy module loading)
+    torch.cuda.synchronize()
+    with torch.cuda.graph(graph, stream=s):
+        launch()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(ws)
+    tms = _timed_launches(torch, s, graph.replay, args.steps, args.warmup, flush)
+    barrier(ws)
+    clk = clocks.stop()
+    t_local = sum(tms)
+    t_max = reduce_max(t_local, ws, dev)
+    pairs = bh.p_pairs + bh.c_pairs
+    value = reduce_sum(float(pairs) * len(tms), ws, dev) / t_max / 1e9
+    flops = bh.p_pairs * 38 + bh.c_pairs * 60
+    achieved = flops * len(tms) / t_local / 1e12
+    # each kind's launch alone (CUDA events on its stream)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    with torch.cuda.stream(s):
+        ev[0].record(s)
+        g5.plan_launch_indexed(pl_p, *args_p)
+        ev[1].record(s)
+        g5.plan_launch_indexed(pl_c, *args_c)
+        ev[2].record(s)
+    torch.cuda.synchronize()
+    ms_p, ms_c = ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
+    acc_b = (o_p[:, :3] + o_c[:, :3]).cpu().numpy()
+    phi_b = (o_p[:, 3] - o_c[:, 3]).cpu().numpy()
+    del graph
+
+    # end to end through the batched API with host buffers: every step copies the records and
+    # both index lists from pinned host memory, launches both plans and reads both results back
+    h_in = [torch.from_numpy(a).pin_memory() for a in (ip, pp, cp, cq, bh.pidx, bh.cidx)]
+    d_in = [d_i, d_p, d_c, d_q, d_pi, d_ci]
+    h_out = [torch.empty_like(o_p, device="cpu").pin_memory() for _ in range(2)]
+    e2e_ms = []
+    for k in range(args.warmup + args.e2e_steps):
+        a_, b_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(s):
+            a_.record(s)
+            for d_, h_ in zip(d_in, h_in):
+                d_.copy_(h_, non_blocking=True)
+            launch()
+            h_out[0].copy_(o_p, non_blocking=True)
+            h_out[1].copy_(o_c, non_blocking=True)
+            b_.record(s)
+        s.synchronize()
+        if k >= args.warmup:
+            e2e_ms.append(a_.elapsed_time(b_))
+    e2e_val = reduce_sum(float(pairs) * len(e2e_ms), ws, dev) / reduce_max(sum(e2e_ms) / 1e3, ws, dev) / 1e9
+    h2d = sum(t.numel() * t.element_size() for t in h_in)
+    d2h = sum(t.numel() * t.element_size() for t in h_out)
+
+    # the per-group drop-in calls with host buffers (source.cpp:813-866 call sequence)
+    drv = Driver(pgb)
+    p = Driver.p
+    lp = C.POINTER(C.c_longlong)
+    f64 = lambda a: np.ascontiguousarray(a, np.float64)  # noqa: E731
+    xi, xp, mp = f64(ip[:, :3]), f64(pp[:, :3]), f64(pp[:, 3])
+    cpos, cm, cqq = f64(cp[:, :3]), f64(cp[:, 3]), f64(cq[:, :6])
+    acc = np.zeros((len(mp), 3))
+    phi = np.zeros(len(mp))
+    nthr = min(os.cpu_count() or 1, 32)
+
+    def dropin(h, g0, g1, threads):
+        return drv.L.g5drv_bh(h, g0, g1, p(bh.gfirst, C.c_int), p(bh.gcount, C.c_int), p(xi), p(xp), p(mp),
+                              p(bh.poff, C.c_longlong), p(bh.pidx, C.c_int), p(cpos), p(cm), p(cqq),
+                              p(bh.coff, C.c_longlong), p(bh.cidx, C.c_int), bh.eps, p(acc), p(phi), threads)
+
+    h = drv.L.g5drv_open(pgb.ffi.lib_path("libpg5.so").encode())
+    dropin(h, 0, min(64, bh.ngroups), nthr)   # warm-up
+    dropin_t = dropin(h, 0, bh.ngroups, nthr)
+    dropin_val = reduce_sum(float(pairs), ws, dev) / reduce_max(dropin_t, ws, dev) / 1e9
+    dropin_rms = float(np.sqrt(np.mean(np.sum((acc - acc_b) ** 2, 1) / np.sum(acc_b ** 2, 1))))
+    errors = {"dropin_vs_batched_rms": dropin_rms}
+    if rank == 0 and not args.no_errors:
+        from oracle import oracle as O
+        # FP64 on the same lists and inputs (every 97th group), and the full FP64 direct sum
+        # (multipole truncation) on 4096 sampled particles
+        e1 = []
+        for g in range(0, bh.ngroups, 97):
+            sl = slice(bh.gfirst[g], bh.gfirst[g] + bh.gcount[g])
+            pl = bh.pidx[bh.poff[g]:bh.poff[g + 1]]
+            cl = bh.cidx[bh.coff[g]:bh.coff[g + 1]]
+            a1, _ = O.g5_newton(xi[sl], float(ip[0, 3]), xp[pl], mp[pl])
+            a2, _ = O.g5_quad(xi[sl], float(ip[0, 3]), cpos[cl], cm[cl], cqq[cl])
+            ref = a1 + a2
+            e1.append(np.linalg.norm(acc_b[sl] - ref, axis=1) / np.linalg.norm(ref, axis=1))
+        e1 = np.concatenate(e1)
+        smp = np.sort(W.Rng(4096).permutation(len(mp))[:4096])
+        ad, _ = O.g5_newton(xi[smp], float(ip[0, 3]), xp, mp)
+        e2 = np.linalg.norm(acc_b[smp] - ad, axis=1) / np.linalg.norm(ad, axis=1)
+        errors.update({"same_lists_fp64": {"rms": float(np.sqrt(np.mean(e1 ** 2))), "max": float(e1.max()),
+                                           "particles": int(len(e1))},
+                       "direct_sum_fp64": {"rms": float(np.sqrt(np.mean(e2 ** 2))), "max": float(e2.max()),
+                                           "particles": 4096}})
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        path = ref_lib("libquad_ref.so")
+        if path:
+            hr = drv.L.g5drv_open(path.encode())
+            ng = min(bh.ngroups, 4000)
+            cores = min(os.cpu_count() or 1, 128)
+            tr = dropin(hr, 0, ng, cores)
+            sp = int((bh.gcount[:ng].astype(np.int64) * (np.diff(bh.poff)[:ng] + np.diff(bh.coff)[:ng])).sum())
+            cpu = {"value": sp / tr / 1e9, "unit": "Gint/s", "cores": cores, "kind": "reference",
+                   "sample": f"first {ng} of {bh.ngroups} groups ({sp:.3e} pairs), PG5/newton_quad libraries "
+                   "(libpg5 + quad, AVX2) built from their sources, OpenMP over groups with g5_*MC / g5c_*MC"}
+    g5.plan_destroy(pl_p)
+    g5.plan_destroy(pl_c)
+    return _line(args, ws, "Gint/s (Barnes-Hut point masses + quadrupole cells, batched)", value, t_max / len(tms),
+                 pairs, "38 (point mass) / 60 (quadrupole cell)", f"Barnes-Hut N={args.bh_n} Hernquist (a=1, r<=100) eps=1e-3, theta=0.5, ncrit=256, "
+                 f"nleaf=16: {bh.ngroups} groups, {bh.p_pairs:.3e} point-mass + {bh.c_pairs:.3e} cell pairs",
+                 "f32 (f64 cross-tile sums)", achieved, clk,
+                 {"value": round(e2e_val, 2), "unit": "Gint/s", "h2d_bytes_per_step": int(h2d),
+                  "d2h_bytes_per_step": int(d2h), "steps": len(e2e_ms),
+                  "api": "pgb5_plan_launch_indexed x 2 (point-mass and cell lists) with the records and index "
+                         "lists copied from pinned host memory and both results read back every step"},
+                 cpu, 2 * len(tms),
+                 extra={"dropin": {"value": round(dropin_val, 2), "unit": "Gint/s", "threads": nthr,
+                                   "api": "per group g5_set_xmjMC + g5_set_nMC + g5_calculate_force_on_xMC and "
+                                          "g5c_set_xmjMC + g5c_set_nMC + g5c_calculate_force_on_xMC, one devid per "
+                                          "host thread, host buffers; list gathers inside the timed loop"},
+                        "launch_ms": {"point_masses": round(ms_p, 3), "cells": round(ms_c, 3)},
+                        "autotune": {"point_masses": G5_CFG_NAMES[cfg_p], "cells": G5_CFG_NAMES[cfg_c]},
+                        "tree_build_s": round(t_tree, 2), "errors": errors},
+                 kernel=f"pgb::g5_kernel<NEWTON,{G5_CFG_NAMES[cfg_p]}> + <QUAD,{G5_CFG_NAMES[cfg_c]}> (index lists)")
+
+
 # ----------------------------------------------------------------------------------------
 # reference arm
 
@@ -832,7 +1002,9 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["hermite", "direct", "clusters", "treepm"], default="hermite")
+    ap.add_argument("--workload", choices=["hermite", "direct", "clusters", "treepm", "bh"], default="hermite")
+    ap.add_argument("--bh-n", type=int, default=1 << 22, help="particles of the Barnes-Hut workload")
+    ap.add_argument("--no-errors", action="store_true", help="bh: skip the FP64 error report")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--ref-pairs", type=float, default=4e9, help="pairs per reference-arm step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -855,7 +1027,8 @@ def main():
             print(json.dumps(line), flush=True)
         return
     dist = dist_init(ws, local)
-    runner = {"hermite": run_hermite, "direct": run_direct, "clusters": run_clusters, "treepm": run_treepm}
+    runner = {"hermite": run_hermite, "direct": run_direct, "clusters": run_clusters, "treepm": run_treepm,
+              "bh": run_bh}
     line = runner[args.workload](args, pgb, ws, rank, local)
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -121,7 +121,15 @@ int  pgb5_plan_tune(pgb5_plan *plan, const void *ipos, const void *jpos, const v
                     void *stream, float *best_ms);
 int  pgb5_plan_config(const pgb5_plan *plan);
 int  pgb5_plan_set_config(pgb5_plan *plan, int cfg);   /* pin one (PGB5_NCFG configurations) */
-enum { PGB5_NCFG = 6 };
+/* Tree-code interaction lists without copies: the items' j-ranges address the device index
+ * list jidx (int32), record k of an item being jpos[jidx[j_offset + k]] (and its jaux words):
+ * one plan for the point-mass lists (PGB5_NEWTON over the particle array) and one for the
+ * cell lists (PGB5_QUAD over the cell array) of every group.  Tune with the same list.       */
+int  pgb5_plan_launch_indexed(pgb5_plan *plan, const void *ipos, const void *jpos, const void *jaux,
+                              const int *jidx, void *out, void *stream);
+int  pgb5_plan_tune_indexed(pgb5_plan *plan, const void *ipos, const void *jpos, const void *jaux,
+                            const int *jidx, void *out, void *stream, float *best_ms);
+enum { PGB5_NCFG = 8 };
 
 #ifdef __cplusplus
 }

@@ -65,12 +65,17 @@ void pgb5_plan_destroy(pgb5_plan *plan);
 long long pgb5_plan_interactions(const pgb5_plan *plan);
 int  pgb5_plan_tasks(const pgb5_plan *plan);
 /* autotuner and configuration pinning, as in pgb_g5.h (the table kind uses configurations
- * 0, 1 and 5: CTAs of at most 256 threads) */
+ * 0, 1, 5, 6 and 7: CTAs of at most 256 threads) */
 int  pgb5_plan_tune(pgb5_plan *plan, const void *ipos, const void *jpos, const void *jaux, void *out,
                     void *stream, float *best_ms);
 int  pgb5_plan_config(const pgb5_plan *plan);
 int  pgb5_plan_set_config(pgb5_plan *plan, int cfg);   /* pin one (PGB5_NCFG configurations) */
-enum { PGB5_NCFG = 6 };
+/* index-list launch and tuning, as in pgb_g5.h */
+int  pgb5_plan_launch_indexed(pgb5_plan *plan, const void *ipos, const void *jpos, const void *jaux,
+                              const int *jidx, void *out, void *stream);
+int  pgb5_plan_tune_indexed(pgb5_plan *plan, const void *ipos, const void *jpos, const void *jaux,
+                            const int *jidx, void *out, void *stream, float *best_ms);
+enum { PGB5_NCFG = 8 };
 
 #ifdef __cplusplus
 }

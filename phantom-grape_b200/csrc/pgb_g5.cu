@@ -46,12 +46,17 @@ ErrorSlot g_err;
 
 constexpr int MAXDEV = 64;
 // Kernel configurations: threads per CTA x i-particles per thread.  Large CTAs win on large
-// single items (fewer, longer tasks), small i-tiles on batches of small groups; the table
+// single items (fewer, longer tasks), small i-tiles on batches of small groups (tree-code
+// groups average well below their size limit: an i-tile much larger than the group idles
+// most of its threads); the table
 // kind keeps its force table in static shared memory (CTAs of <= 256 threads) and the quad
 // kind stages three words per cell (<= 512 threads).  Plans pick one with pgb5_plan_tune.
-enum G5Cfg { G5C_128x4 = 0, G5C_256x2 = 1, G5C_512x2 = 2, G5C_1024x1 = 3, G5C_384x2 = 4, G5C_128x2 = 5, G5_NCFG = 6 };
-constexpr int G5C_NT[G5_NCFG] = {128, 256, 512, 1024, 384, 128};
-constexpr int G5C_IPT[G5_NCFG] = {4, 2, 2, 1, 2, 2};
+enum G5Cfg {
+    G5C_128x4 = 0, G5C_256x2 = 1, G5C_512x2 = 2, G5C_1024x1 = 3, G5C_384x2 = 4, G5C_128x2 = 5, G5C_128x1 = 6,
+    G5C_64x1 = 7, G5_NCFG = 8
+};
+constexpr int G5C_NT[G5_NCFG] = {128, 256, 512, 1024, 384, 128, 128, 64};
+constexpr int G5C_IPT[G5_NCFG] = {4, 2, 2, 1, 2, 2, 1, 1};
 constexpr int ITILE_MAX = 1024;
 inline int cfg_itile(int c) { return G5C_NT[c] * G5C_IPT[c]; }
 template <int KIND, int NT>
@@ -123,6 +128,8 @@ cudaError_t launch_cfg(int cfg, int grid, const G5Args& a, cudaStream_t s, int* 
         case G5C_1024x1: return launch_k<KIND, 1024, 1>(grid, a, s, occ);
         case G5C_384x2: return launch_k<KIND, 384, 2>(grid, a, s, occ);
         case G5C_128x2: return launch_k<KIND, 128, 2>(grid, a, s, occ);
+        case G5C_128x1: return launch_k<KIND, 128, 1>(grid, a, s, occ);
+        case G5C_64x1: return launch_k<KIND, 64, 1>(grid, a, s, occ);
         default: return launch_k<KIND, 128, 4>(grid, a, s, occ);
     }
 }
@@ -303,12 +310,13 @@ struct Launcher {
     // Launch over the staged work list.  The kernel leaves its task counter at zero, so the same
     // staged list can be launched again (e.g. from a CUDA graph) without a reset.
     bool launch(int kind, int cfg, cudaStream_t s, const float4* i_dev, const float4* jpos, const float4* jaux,
-                double4* out) {
+                double4* out, const int* jidx = nullptr) {
         if (st.ntasks <= 0) return true;
         G5Args a;
         a.ipos = i_dev ? i_dev : st.irecs();
         a.jpos = jpos;
         a.jaux = jaux;
+        a.jidx = jidx;
         a.tasks = st.tasks();
         a.ntasks = st.ntasks;
         a.task_counter = st.counter();
@@ -1067,13 +1075,28 @@ PGB_EXPORT int pgb5_plan_launch(pgb5_plan* P, const void* ipos, const void* jpos
     return PGB_OK;
 }
 
-// Autotuner: launches the plan with every kernel configuration valid for its kind on the
-// caller's data, keeps the fastest (CUDA-event time, best of 2 after a warm-up launch),
-// re-stages the plan with it and records it for later plans of the same shape.  Returns the
-// chosen configuration index (-1 on error); *best_ms (optional) receives its launch time.
-// Overwrites `out`.  Not capturable (it synchronises the stream).
-PGB_EXPORT int pgb5_plan_tune(pgb5_plan* P, const void* ipos, const void* jpos, const void* jaux, void* out,
-                              void* stream, float* best_ms) {
+// As pgb5_plan_launch, with the items' j-ranges addressing the index list jidx (int32, device):
+// record k of an item is jpos[jidx[j_offset + k]] (and its jaux words).  This runs the
+// interaction lists of a tree code without copying records per group.
+PGB_EXPORT int pgb5_plan_launch_indexed(pgb5_plan* P, const void* ipos, const void* jpos, const void* jaux,
+                                        const int* jidx, void* out, void* stream) {
+    if (!P) return PGB_ERR_ARG;
+    if (!ensure_device()) return PGB_ERR_NOGPU;
+    if (!ipos || !jpos || !out || !jidx || ((P->kind == G5_SYMMETRIC || P->kind == G5_QUAD) && !jaux)) {
+        raise(g_err, LIB, PGB_ERR_ARG, "pgb5_plan_launch_indexed: null device pointer");
+        return PGB_ERR_ARG;
+    }
+    if (!P->L.launch(P->kind, P->cfg, (cudaStream_t)stream, (const float4*)ipos, (const float4*)jpos,
+                     (const float4*)jaux, (double4*)out, jidx))
+        return g_err.code ? g_err.code : PGB_ERR_CUDA;
+    return PGB_OK;
+}
+
+namespace {
+// The autotuner shared by pgb5_plan_tune and pgb5_plan_tune_indexed (jidx: nullptr or the
+// index list the plan is launched with).
+int tune_impl(pgb5_plan* P, const void* ipos, const void* jpos, const void* jaux, const int* jidx, void* out,
+              void* stream, float* best_ms) {
     if (!P || !ipos || !jpos || !out) {
         raise(g_err, LIB, PGB_ERR_ARG, "pgb5_plan_tune: null argument");
         return -1;
@@ -1093,7 +1116,9 @@ PGB_EXPORT int pgb5_plan_tune(pgb5_plan* P, const void* ipos, const void* jpos, 
         float t = 1e30f;
         for (int rep = 0; rep < 3; rep++) {
             cudaEventRecord(e0, s);
-            if (pgb5_plan_launch(P, ipos, jpos, jaux, out, stream) != PGB_OK) break;
+            const int rc = jidx ? pgb5_plan_launch_indexed(P, ipos, jpos, jaux, jidx, out, stream)
+                                : pgb5_plan_launch(P, ipos, jpos, jaux, out, stream);
+            if (rc != PGB_OK) break;
             cudaEventRecord(e1, s);
             cudaEventSynchronize(e1);
             float ms = 0.f;
@@ -1114,6 +1139,27 @@ PGB_EXPORT int pgb5_plan_tune(pgb5_plan* P, const void* ipos, const void* jpos, 
     set_tuned(P->shape_key, best);
     if (best_ms) *best_ms = best_t;
     return best;
+}
+}  // namespace
+
+// Autotuner: launches the plan with every kernel configuration valid for its kind on the
+// caller's data, keeps the fastest (CUDA-event time, best of 2 after a warm-up launch),
+// re-stages the plan with it and records it for later plans of the same shape.  Returns the
+// chosen configuration index (-1 on error); *best_ms (optional) receives its launch time.
+// Overwrites `out`.  Not capturable (it synchronises the stream).
+PGB_EXPORT int pgb5_plan_tune(pgb5_plan* P, const void* ipos, const void* jpos, const void* jaux, void* out,
+                              void* stream, float* best_ms) {
+    return tune_impl(P, ipos, jpos, jaux, nullptr, out, stream, best_ms);
+}
+
+// The autotuner of a plan launched with pgb5_plan_launch_indexed (same index list).
+PGB_EXPORT int pgb5_plan_tune_indexed(pgb5_plan* P, const void* ipos, const void* jpos, const void* jaux,
+                                      const int* jidx, void* out, void* stream, float* best_ms) {
+    if (!jidx) {
+        raise(g_err, LIB, PGB_ERR_ARG, "pgb5_plan_tune_indexed: null index list");
+        return -1;
+    }
+    return tune_impl(P, ipos, jpos, jaux, jidx, out, stream, best_ms);
 }
 
 PGB_EXPORT int pgb5_plan_config(const pgb5_plan* P) { return P ? P->cfg : -1; }

@@ -24,6 +24,8 @@ struct G5Args {
     const float4* ipos;     // [.] x, y, z, eps2 of each i-particle
     const float4* jpos;     // [.] x, y, z, m of each j-particle (or cell word 0)
     const float4* jaux;     // symmetric: [.] eps2_j in .x; quad: [2*nc] (q0 q1 q2 q3)(q4 q5 - -)
+    const int* jidx;        // nullptr: task j-ranges address jpos/jaux directly; else they address
+                            // this index list (interaction lists of a tree: j = jidx[k])
     const Task* tasks;
     int ntasks;
     int* task_counter;      // zero before launch
@@ -157,7 +159,8 @@ __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
             const int nt = min(NT, T.nj - jt);
             __syncthreads();
             if (threadIdx.x < nt) {
-                const int jj = T.j0 + jt + threadIdx.x;
+                const int jk = T.j0 + jt + threadIdx.x;
+                const int jj = A.jidx ? __ldg(A.jidx + jk) : jk;
                 sj[threadIdx.x] = A.jpos[jj];
                 if constexpr (W == 2) sj[NT + threadIdx.x] = A.jaux[jj];
                 if constexpr (W == 3) {

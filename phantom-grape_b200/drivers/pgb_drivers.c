@@ -13,6 +13,7 @@
  *                  g5_set_n, g5_calculate_force_on_x.
  *  g5drv_groups    PG5/newton_quad/source.cpp:813-860 style: OpenMP over i-groups, each thread
  *                  with its own devid: g5_set_xmjMC, g5_set_nMC, g5_calculate_force_on_xMC.
+ *  g5drv_bh        the same with the quadrupole-cell lists through g5c_* (source.cpp:813-866).
  *
  * Libraries are opened with RTLD_LOCAL so several GRAPE libraries can coexist in one process.
  */
@@ -164,6 +165,10 @@ typedef struct {
     void (*set_xmjMC)(int, int, int, double (*)[3], double *);
     void (*set_nMC)(int, int);
     void (*calcMC)(int, double (*)[3], double (*)[3], double *, int);
+    /* quadrupole cells (PG5/newton_quad/quad/quad_util.h:8-15); NULL in libraries without them */
+    void (*c_set_xmjMC)(int, int, int, double (*)[3], double *, double (*)[6]);
+    void (*c_set_nMC)(int, int);
+    void (*c_calcMC)(int, double (*)[3], double (*)[3], double *, int);
 } g5api;
 
 void *g5drv_open(const char *path) {
@@ -182,6 +187,9 @@ void *g5drv_open(const char *path) {
     LOAD(h, a->set_xmjMC, "g5_set_xmjMC");
     LOAD(h, a->set_nMC, "g5_set_nMC");
     LOAD(h, a->calcMC, "g5_calculate_force_on_xMC");
+    *(void **)(&a->c_set_xmjMC) = dlsym(h, "g5c_set_xmjMC");
+    *(void **)(&a->c_set_nMC) = dlsym(h, "g5c_set_nMC");
+    *(void **)(&a->c_calcMC) = dlsym(h, "g5c_calculate_force_on_xMC");
     a->open();
     return a;
 }
@@ -213,6 +221,86 @@ double g5drv_groups(void *handle, int ngroups, const int *items, const double *x
         a->set_nMC(dev, it[3]);
         a->calcMC(dev, (double(*)[3])(xi + 3 * (size_t)it[0]), (double(*)[3])(acc + 3 * (size_t)it[0]),
                   pot + it[0], it[1]);
+    }
+    return now() - t0;
+}
+
+/* Barnes-Hut groups with point-mass and quadrupole-cell lists, the way
+ * PG5/newton_quad/source.cpp:813-866 drives the libraries: OpenMP over groups, devid = thread
+ * id; per group the point-mass list through g5_set_xmjMC + g5_set_nMC +
+ * g5_calculate_force_on_xMC and the cell list through g5c_set_xmjMC + g5c_set_nMC +
+ * g5c_calculate_force_on_xMC, then acc = a_mono + a_quad and phi = -p_mono + p_quad (the sign
+ * reconciliation of source.cpp:854, 866; its self-term correction epsinv*m is left out).
+ * Lists are index lists into tree-order particle (xp, mp) and cell (cpos, cmass, cquad) arrays,
+ * gathered per group into thread-local buffers inside the timed loop (the reference writes
+ * them in its tree walk just before the calls).  Groups [g0, g1); returns elapsed seconds,
+ * or -1 when the library has no g5c_* entry points. */
+double g5drv_bh(void *handle, int g0, int g1, const int *gfirst, const int *gcount, const double *xi,
+                const double *xp, const double *mp, const long long *poff, const int *pidx, const double *cpos,
+                const double *cmass, const double *cquad, const long long *coff, const int *cidx, double eps,
+                double *acc, double *phi, int nthreads) {
+    g5api *a = (g5api *)handle;
+    if (!a->c_set_xmjMC || !a->c_set_nMC || !a->c_calcMC) return -1.0;
+    long long maxp = 1, maxc = 1;
+    int maxi = 1;
+    for (int g = g0; g < g1; g++) {
+        if (poff[g + 1] - poff[g] > maxp) maxp = poff[g + 1] - poff[g];
+        if (coff[g + 1] - coff[g] > maxc) maxc = coff[g + 1] - coff[g];
+        if (gcount[g] > maxi) maxi = gcount[g];
+    }
+    a->set_eps_to_all(eps);
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+    double t0 = now();
+#pragma omp parallel
+    {
+        double(*xj)[3] = malloc(sizeof(double) * 3 * maxp);
+        double *mj = malloc(sizeof(double) * maxp);
+        double(*xc)[3] = malloc(sizeof(double) * 3 * maxc);
+        double *mc = malloc(sizeof(double) * maxc);
+        double(*qc)[6] = malloc(sizeof(double) * 6 * maxc);
+        double(*a2)[3] = malloc(sizeof(double) * 3 * maxi);
+        double *p1 = malloc(sizeof(double) * maxi), *p2 = malloc(sizeof(double) * maxi);
+        int dev = omp_get_thread_num();
+#pragma omp for schedule(dynamic, 1)
+        for (int g = g0; g < g1; g++) {
+            const int f = gfirst[g], ni = gcount[g];
+            const int np = (int)(poff[g + 1] - poff[g]), nc = (int)(coff[g + 1] - coff[g]);
+            for (int k = 0; k < np; k++) {
+                const int p = pidx[poff[g] + k];
+                xj[k][0] = xp[3 * (size_t)p];
+                xj[k][1] = xp[3 * (size_t)p + 1];
+                xj[k][2] = xp[3 * (size_t)p + 2];
+                mj[k] = mp[p];
+            }
+            for (int k = 0; k < nc; k++) {
+                const int c = cidx[coff[g] + k];
+                for (int d = 0; d < 3; d++) xc[k][d] = cpos[3 * (size_t)c + d];
+                mc[k] = cmass[c];
+                for (int d = 0; d < 6; d++) qc[k][d] = cquad[6 * (size_t)c + d];
+            }
+            double(*xg)[3] = (double(*)[3])(xi + 3 * (size_t)f);
+            double(*ag)[3] = (double(*)[3])(acc + 3 * (size_t)f);
+            a->set_xmjMC(dev, 0, np, xj, mj);
+            a->set_nMC(dev, np);
+            a->calcMC(dev, xg, ag, p1, ni);
+            a->c_set_xmjMC(dev, 0, nc, xc, mc, qc);
+            a->c_set_nMC(dev, nc);
+            a->c_calcMC(dev, xg, a2, p2, ni);
+            for (int i = 0; i < ni; i++) {
+                ag[i][0] += a2[i][0];
+                ag[i][1] += a2[i][1];
+                ag[i][2] += a2[i][2];
+                phi[f + i] = -p1[i] + p2[i];
+            }
+        }
+        free(xj);
+        free(mj);
+        free(xc);
+        free(mc);
+        free(qc);
+        free(a2);
+        free(p1);
+        free(p2);
     }
     return now() - t0;
 }

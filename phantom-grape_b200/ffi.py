@@ -124,6 +124,8 @@ class G5(_ErrMixin):
         _sig(L, "pgb5_plan_tune", [vp, vp, vp, vp, vp, vp, C.POINTER(C.c_float)], C.c_int)
         _sig(L, "pgb5_plan_config", [vp], C.c_int)
         _sig(L, "pgb5_plan_set_config", [vp, C.c_int], C.c_int)
+        _sig(L, "pgb5_plan_launch_indexed", [vp, vp, vp, vp, vp, vp, vp], C.c_int)
+        _sig(L, "pgb5_plan_tune_indexed", [vp, vp, vp, vp, vp, vp, vp, C.POINTER(C.c_float)], C.c_int)
 
     # convenience wrappers with numpy arrays -------------------------------------------------
     def set_xmj(self, adr, xj, mj, epsj2=None, devid=None):
@@ -188,6 +190,19 @@ class G5(_ErrMixin):
         rc = self.L.pgb5_plan_launch(plan, ipos, jpos, jaux, out, stream)
         if rc:
             raise RuntimeError(f"pgb5_plan_launch failed: {self.last_error()}")
+
+    def plan_launch_indexed(self, plan, ipos, jpos, jaux, jidx, out, stream=0):
+        rc = self.L.pgb5_plan_launch_indexed(plan, ipos, jpos, jaux, jidx, out, stream)
+        if rc:
+            raise RuntimeError(f"pgb5_plan_launch_indexed failed: {self.last_error()}")
+
+    def plan_tune_indexed(self, plan, ipos, jpos, jaux, jidx, out, stream=0):
+        """Autotune a plan launched with an index list; (cfg, ms)."""
+        ms = C.c_float(0)
+        cfg = self.L.pgb5_plan_tune_indexed(plan, ipos, jpos, jaux, jidx, out, stream, C.byref(ms))
+        if cfg < 0:
+            raise RuntimeError(f"pgb5_plan_tune_indexed failed: {self.last_error()}")
+        return cfg, ms.value
 
     def plan_tune(self, plan, ipos, jpos, jaux, out, stream=0):
         """Autotune the plan's kernel configuration on these device arrays; (cfg, ms)."""
@@ -439,6 +454,8 @@ class G5Table(_ErrMixin):
         _sig(L, "pgb5_plan_tune", [vp, vp, vp, vp, vp, vp, C.POINTER(C.c_float)], C.c_int)
         _sig(L, "pgb5_plan_config", [vp], C.c_int)
         _sig(L, "pgb5_plan_set_config", [vp, C.c_int], C.c_int)
+        _sig(L, "pgb5_plan_launch_indexed", [vp, vp, vp, vp, vp, vp, vp], C.c_int)
+        _sig(L, "pgb5_plan_tune_indexed", [vp, vp, vp, vp, vp, vp, vp, C.POINTER(C.c_float)], C.c_int)
         self._cb = None
 
     def set_table(self, func, rcut, frc_bit=None):

@@ -307,3 +307,145 @@ def treepm_groups(n: int = 1 << 20, seed: int = SEED0 + 2, mesh: int = 128, bloc
     order = np.concatenate(order)
     return TreePMSet(x=x, m=m, xi=x[order], order=order, items=np.array(items, np.int32),
                      xj=np.concatenate(xjs), mj=np.concatenate(mjs), rs=rs, rcut=rcut, eps=eps)
+
+
+# ------------------------------------------------------------------------------------------
+# Barnes-Hut with quadrupole cells (newton_quad)
+
+def hernquist_radii(rng: Rng, n: int, rmax: float = 100.0) -> np.ndarray:
+    """Hernquist (a = 1) radii by inverting M(<r)/M = r^2/(1+r)^2: r = sqrt(U)/(1 - sqrt(U)),
+    rejecting r > rmax."""
+    out = np.empty(0)
+    while len(out) < n:
+        s = np.sqrt(rng.uniform(2 * (n - len(out)) + 16))
+        s = s[s < 1.0]
+        r = s / (1.0 - s)
+        out = np.concatenate([out, r[r <= rmax]])
+    return out[:n]
+
+
+@dataclass
+class BHSet:
+    """A Barnes-Hut force evaluation: particles in tree order, the tree's cells and every
+    group's interaction list (point masses: indices into the particles; cells: indices into
+    the cell arrays).  Built by drivers/pgb_bhtree.c."""
+    x: np.ndarray        # [n,3] tree-order positions (float32-representable)
+    m: np.ndarray        # [n]
+    perm: np.ndarray     # [n] tree order -> sampling order
+    gfirst: np.ndarray   # [ng] int32 first particle of each group (tree order)
+    gcount: np.ndarray   # [ng] int32
+    gcentre: np.ndarray  # [ng,3] group cell centre
+    ghalf: np.ndarray    # [ng] group cell half side
+    poff: np.ndarray     # [ng+1] int64 point-mass list offsets
+    pidx: np.ndarray     # [np] int32
+    coff: np.ndarray     # [ng+1] int64 cell list offsets
+    cidx: np.ndarray     # [nc] int32
+    ccom: np.ndarray     # [ncell,3] cell centre of mass
+    cmass: np.ndarray    # [ncell]
+    cquad: np.ndarray    # [ncell,6] (xx, xy, xz, yy, yz, zz), traceless
+    nfirst: np.ndarray   # [ncell] the tree's nodes (= the cells): particle range, half side,
+    ncount: np.ndarray   #   geometric centre and children (-1: empty octant)
+    nhalf: np.ndarray
+    ncentre: np.ndarray
+    nchild: np.ndarray   # [ncell,8]
+    eps: float
+    theta: float
+    nleaf: int
+    ncrit: int
+
+    @property
+    def ngroups(self) -> int:
+        return len(self.gfirst)
+
+    @property
+    def p_pairs(self) -> int:
+        return int((self.gcount.astype(np.int64) * np.diff(self.poff)).sum())
+
+    @property
+    def c_pairs(self) -> int:
+        return int((self.gcount.astype(np.int64) * np.diff(self.coff)).sum())
+
+    def records(self):
+        """float32 records of the batched path: i (x, y, z, eps^2), particles (x, y, z, m), cells
+        (centre of mass, mass) and their quadrupole words (xx xy xz yy)(yz zz 0 0)."""
+        n, nc = len(self.m), len(self.cmass)
+        ip = np.empty((n, 4), np.float32)
+        ip[:, :3] = self.x
+        ip[:, 3] = np.float32(self.eps * self.eps)
+        pp = np.empty((n, 4), np.float32)
+        pp[:, :3] = self.x
+        pp[:, 3] = self.m
+        cp = np.empty((nc, 4), np.float32)
+        cp[:, :3] = self.ccom
+        cp[:, 3] = self.cmass
+        cq = np.zeros((nc, 8), np.float32)
+        cq[:, :6] = self.cquad
+        return ip, pp, cp, cq
+
+    def items(self, kind: str) -> np.ndarray:
+        """Work items (i_offset, i_count, j_offset, j_count) of the point-mass ('p') or cell
+        ('c') lists, j offsets into the index list."""
+        off = self.poff if kind == "p" else self.coff
+        return np.stack([self.gfirst, self.gcount, off[:-1], np.diff(off)], 1).astype(np.int32)
+
+
+def bh_tree(x: np.ndarray, m: np.ndarray, theta: float = 0.5, nleaf: int = 16, ncrit: int = 256,
+            eps: float = 1e-3) -> BHSet:
+    """Octree, moments and interaction lists of particles x (n x 3), m (n) with the reference's
+    rules (drivers/pgb_bhtree.c)."""
+    import ctypes as C
+    from . import ffi
+    L = C.CDLL(ffi.lib_path("libpgbdrv.so"), mode=C.RTLD_LOCAL)
+    vp, dp, ip, lp = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int), C.POINTER(C.c_longlong)
+    L.bh_build.argtypes = [C.c_int, dp, dp, C.c_double, C.c_int, C.c_int]
+    L.bh_build.restype = vp
+    for f, r in (("bh_n", C.c_int), ("bh_ngroups", C.c_int), ("bh_nnodes", C.c_int), ("bh_np", C.c_longlong),
+                 ("bh_nc", C.c_longlong)):
+        getattr(L, f).argtypes = [vp]
+        getattr(L, f).restype = r
+    L.bh_perm.argtypes = [vp, ip]
+    L.bh_groups.argtypes = [vp, ip, ip, dp, dp]
+    L.bh_cells.argtypes = [vp, dp, dp, dp]
+    L.bh_lists.argtypes = [vp, lp, ip, lp, ip]
+    L.bh_nodes.argtypes = [vp, ip, ip, dp, dp, ip]
+    L.bh_free.argtypes = [vp]
+    x = np.ascontiguousarray(x, np.float64)
+    m = np.ascontiguousarray(m, np.float64)
+    n = len(m)
+    h = L.bh_build(n, x.ctypes.data_as(dp), m.ctypes.data_as(dp), theta, nleaf, ncrit)
+    if not h:
+        raise MemoryError("bh_build failed")
+    try:
+        ng, nn, npl, ncl = L.bh_ngroups(h), L.bh_nnodes(h), L.bh_np(h), L.bh_nc(h)
+        perm = np.empty(n, np.int32)
+        L.bh_perm(h, perm.ctypes.data_as(ip))
+        gfirst, gcount = np.empty(ng, np.int32), np.empty(ng, np.int32)
+        gcentre, ghalf = np.empty((ng, 3)), np.empty(ng)
+        L.bh_groups(h, gfirst.ctypes.data_as(ip), gcount.ctypes.data_as(ip), gcentre.ctypes.data_as(dp),
+                    ghalf.ctypes.data_as(dp))
+        ccom, cmass, cquad = np.empty((nn, 3)), np.empty(nn), np.empty((nn, 6))
+        L.bh_cells(h, ccom.ctypes.data_as(dp), cmass.ctypes.data_as(dp), cquad.ctypes.data_as(dp))
+        poff, coff = np.empty(ng + 1, np.int64), np.empty(ng + 1, np.int64)
+        pidx, cidx = np.empty(max(npl, 1), np.int32), np.empty(max(ncl, 1), np.int32)
+        L.bh_lists(h, poff.ctypes.data_as(lp), pidx.ctypes.data_as(ip), coff.ctypes.data_as(lp),
+                   cidx.ctypes.data_as(ip))
+        nfirst, ncount, nhalf = np.empty(nn, np.int32), np.empty(nn, np.int32), np.empty(nn)
+        ncentre, nchild = np.empty((nn, 3)), np.empty((nn, 8), np.int32)
+        L.bh_nodes(h, nfirst.ctypes.data_as(ip), ncount.ctypes.data_as(ip), nhalf.ctypes.data_as(dp),
+                   ncentre.ctypes.data_as(dp), nchild.ctypes.data_as(ip))
+    finally:
+        L.bh_free(h)
+    return BHSet(x=x[perm], m=m[perm], perm=perm, gfirst=gfirst, gcount=gcount, gcentre=gcentre, ghalf=ghalf,
+                 poff=poff, pidx=pidx[:npl], coff=coff, cidx=cidx[:ncl], ccom=ccom, cmass=cmass, cquad=cquad,
+                 nfirst=nfirst, ncount=ncount, nhalf=nhalf, ncentre=ncentre, nchild=nchild, eps=eps, theta=theta, nleaf=nleaf, ncrit=ncrit)
+
+
+def bh_hernquist(n: int = 1 << 22, seed: int = SEED0 + 3, theta: float = 0.5, nleaf: int = 16, ncrit: int = 256,
+                 eps: float = 1e-3, rmax: float = 100.0) -> BHSet:
+    """Hernquist sphere (a = 1, M = 1, truncated at rmax), equal masses, float32-rounded
+    positions; octree with theta = 0.5, groups of <= ncrit = 256 and leaves of <= nleaf = 16
+    particles (the reference leaves nleaf to the user, source.cpp:1287-1289)."""
+    rng = Rng(seed)
+    x = _isotropic(rng, hernquist_radii(rng, n, rmax)).astype(np.float32).astype(np.float64)
+    m = np.full(n, np.float32(1.0 / n), np.float64)
+    return bh_tree(x, m, theta, nleaf, ncrit, eps)

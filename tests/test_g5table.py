@@ -123,7 +123,7 @@ def test_treepm_groups_batched_vs_fp64(tab):
     try:
         # the kernel configurations the table kind can use (CTAs of <= 256 threads); the others
         # are refused
-        for cfg in range(6):
+        for cfg in range(8):
             if cfg in (2, 3, 4):
                 tab.set_abort(False)
                 try:
