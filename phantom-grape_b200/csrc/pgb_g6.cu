@@ -23,6 +23,8 @@
 //  * a neighbour list longer than the capacity (1024, PGB_G6_NBMAX) is counted, flagged by
 //    g6_read_neighbour_list and refused by g6_get_neighbour_list, never written out of bounds
 //    (gravity.c:896-906 writes before it checks).
+#include <chrono>
+
 #include "pgb_g6_kernels.cuh"
 #include "pgb_g6_small.cuh"
 
@@ -316,6 +318,9 @@ struct State {
     DevBuf<int> pcnt;       // self-resetting counters of the parameter-block launches
     G6IBlock iblk;  // their i-records
     DevBuf<G6Out> spart;    // cluster rows of the small-call kernel
+    HostBuf<unsigned> flags;  // mapped completion flags of the small-call kernel
+    unsigned seq = 0;         // sequence number of the last flagged call
+    int wait_flags = 0;       // flags the next wait_results() polls (0: synchronise the stream)
     Stager<G6I, G6Out> st;
     // neighbour lists of the last lasthalf*n call
     DevBuf<int> nbc_d, nbl_d;
@@ -438,8 +443,44 @@ bool run_small(int nj, int ni, float eps2, bool nn, bool nbl, G6Out* out_dev) {
         a.nb_count = S.nbc_d.p;
         a.nb_list = S.nbl_d.p;
     }
+    // completion flags (mapped host memory, one per word slice of the final stage)
+    a.done = nullptr;
+    a.seq = 0;
+    if (!nbl) {
+        if (!S.flags.p) {
+            PGB_CUDA_OR(g_err, LIB, S.flags.reserve(SMALL_CL, false, cudaHostAllocPortable | cudaHostAllocMapped),
+                        return false);
+            std::memset((void*)S.flags.p, 0, SMALL_CL * sizeof(unsigned));
+        }
+        unsigned* dflags = nullptr;
+        PGB_CUDA_OR(g_err, LIB, cudaHostGetDevicePointer((void**)&dflags, S.flags.p, 0), return false);
+        a.done = dflags;
+        a.seq = ++S.seq;
+        if (a.seq == 0) a.seq = ++S.seq;   // 0 is the flags' initial value
+        S.wait_flags = cl;
+    }
     std::memcpy(S.iblk.rec, S.ibuf.p, (size_t)ni * sizeof(G6I));
     PGB_CUDA_OR(g_err, LIB, small_kernel(sh, ff, nn, nbl, grid, cl, a, S.iblk, S.stream, nullptr), return false);
+    return true;
+}
+
+// Wait for the results of the last call: by its completion flags when it has them (a bounded
+// spin, then the stream synchronisation that reports a failed launch), else the stream.
+bool wait_results() {
+    if (S.wait_flags > 0) {
+        const int n = S.wait_flags;
+        S.wait_flags = 0;
+        const unsigned seq = S.seq;
+        volatile unsigned* f = S.flags.p;
+        auto t0 = std::chrono::steady_clock::now();
+        for (long it = 0;; it++) {
+            bool all = true;
+            for (int k = 0; k < n; k++) all = all && f[k] == seq;
+            if (all) return true;
+            if ((it & 1023) == 1023 && std::chrono::steady_clock::now() - t0 > std::chrono::seconds(5)) break;
+        }
+    }
+    PGB_CUDA_OR(g_err, LIB, cudaStreamSynchronize(S.stream), return false);
     return true;
 }
 
@@ -561,8 +602,9 @@ int lasthalf_impl(int nj, int ni, const int* pidx, const double (*pos)[3], const
     }
     bool nn = (nnb != nullptr);
     // eps2 is a per-call scalar, used as float (phantom_g6.c:191)
+    S.wait_flags = 0;
     if (!run_force(nj, ni, (float)eps2, nn, nbl)) return 0;
-    PGB_CUDA_OR(g_err, LIB, cudaStreamSynchronize(S.stream), return 0);
+    if (!wait_results()) return 0;
     for (int i = 0; i < ni; i++) {
         const G6Out& o = S.outh.p[i];
         acc[i][0] = o.ax;
@@ -600,6 +642,7 @@ PGB_EXPORT void g6_close(int gpid) {
     S.st.release();
     S.pcnt.release();
     S.spart.release();
+    S.wait_flags = 0;
     S.nbc_d.release();
     S.nbl_d.release();
     S.sbuf_d.release();

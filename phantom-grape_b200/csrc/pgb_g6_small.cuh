@@ -35,7 +35,21 @@ struct G6SmallArgs {
     int* nb_count;     // neighbour lists (NBL), indexed by i
     int* nb_list;
     int nb_maxlen;
+    // completion flags in mapped host memory (nullptr: none): the CTA that writes word slice r
+    // of the results sets done[r] = seq after them, so the host can wait for the results by
+    // polling instead of synchronising the stream
+    volatile unsigned* done;
+    unsigned seq;
 };
+
+// Publish a final slice: every thread's result writes are made visible to the host before
+// thread 0 sets the slice's completion flag.
+__device__ __forceinline__ void publish_done(const G6SmallArgs& A, int slice) {
+    if (!A.done) return;
+    __threadfence_system();
+    __syncthreads();
+    if (threadIdx.x == 0) A.done[slice] = A.seq;
+}
 
 constexpr int G6_SMALL_MAXI = 64;
 
@@ -138,7 +152,10 @@ __global__ void __launch_bounds__(ISL * JL, 2)
         }
         cta_w[threadIdx.x] = v;
     }
-    if (nch == 1) return;
+    if (nch == 1) {
+        publish_done(A, 0);
+        return;
+    }
 
     // 2. the cluster: CTA `rank` reduces words [f0, f1) over the cluster's CTAs, in rank order,
     //    into the cluster's row
@@ -169,6 +186,7 @@ __global__ void __launch_bounds__(ISL * JL, 2)
     if (s_flag) {
         __threadfence();
         reduce_rows<NT>(A.partial, (size_t)ISL, nclus, f0, f1 - f0, A.out, true, reinterpret_cast<double2*>(smem));
+        publish_done(A, rank);
     }
     cl.sync();  // no CTA leaves while a peer may still read its cta_w
 }
