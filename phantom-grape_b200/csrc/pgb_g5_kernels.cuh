@@ -126,6 +126,7 @@ __device__ __forceinline__ double4 add4(double4 a, double4 b) {
 template <int KIND, int NT, int IPT>
 __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
     constexpr int W = JWords<KIND>::n;   // 16-byte words per j record
+    constexpr bool LANES = (IPT == 1 && NT <= 64);
     __shared__ float4 sj[NT * (W > 2 ? W : 2)];  // also the reduction buffer (double4 x NT)
     __shared__ int s_task, s_flag;
     // table kind: the whole force table in shared memory for the lifetime of the CTA
@@ -143,12 +144,23 @@ __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
         int t = next_task(A.task_counter, &s_task, A.ntasks, first);
         if (t >= A.ntasks) break;
         const Task T = A.tasks[t];
+        // j-lanes (the 64-thread one-i-per-thread CTAs): a task of few i takes whole warps of i-slots
+        // (isl = ni rounded up to 32) and splits each j-tile over the nl = NT / isl lanes of
+        // slots; the lanes' sums are added in lane order at the end.  Large tasks: nl = 1.
+        int nl = 1, isl = NT;
+        if constexpr (LANES) {
+            const int need = (T.ni + 31) & ~31;
+            nl = NT / (need > 0 ? need : 32);
+            isl = NT / nl;
+        }
+        const int slot = LANES ? (int)threadIdx.x % isl : (int)threadIdx.x;
+        const int lane = LANES ? (int)threadIdx.x / isl : 0;
 
         float xi[IPT], yi[IPT], zi[IPT], ei[IPT];
         double S[IPT][4];
 #pragma unroll
         for (int k = 0; k < IPT; k++) {
-            int li = threadIdx.x + k * NT;
+            int li = slot + k * NT;
             int ii = T.i0 + (li < T.ni ? li : 0);
             float4 p = A.ipos[ii];
             xi[k] = p.x; yi[k] = p.y; zi[k] = p.z; ei[k] = p.w;
@@ -173,7 +185,7 @@ __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
 #pragma unroll
             for (int k = 0; k < IPT; k++) a[k][0] = a[k][1] = a[k][2] = a[k][3] = 0.f;
 #pragma unroll 4
-            for (int j = 0; j < nt; j++) {
+            for (int j = lane; j < nt; j += (LANES ? nl : 1)) {
                 if constexpr (KIND == G5_TABLE) {
                     const float4 J = sj[j];
 #pragma unroll
@@ -192,11 +204,31 @@ __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
             }
         }
 
+        bool lane0 = true;
+        if constexpr (LANES) {
+            if (nl > 1) {
+                // lane sums in lane order through the j-tile buffer (IPT == 1)
+                double4* red = reinterpret_cast<double4*>(sj);
+                __syncthreads();
+                red[threadIdx.x] = make_double4(S[0][0], S[0][1], S[0][2], S[0][3]);
+                __syncthreads();
+                lane0 = lane == 0;
+                if (lane0) {
+                    for (int l = 1; l < nl; l++) {
+                        const double4 v = red[slot + l * isl];
+                        S[0][0] += v.x;
+                        S[0][1] += v.y;
+                        S[0][2] += v.z;
+                        S[0][3] += v.w;
+                    }
+                }
+            }
+        }
         if (T.group < 0) {
 #pragma unroll
             for (int k = 0; k < IPT; k++) {
-                int li = threadIdx.x + k * NT;
-                if (li < T.ni)
+                int li = slot + k * NT;
+                if (lane0 && li < T.ni)
                     A.out[T.i0 + li] = g5_finish<KIND>(make_double4(S[k][0], S[k][1], S[k][2], S[k][3]), A.ascale);
             }
             continue;
@@ -204,8 +236,8 @@ __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
         double4* row = A.partial + (size_t)T.slot * A.itile;
 #pragma unroll
         for (int k = 0; k < IPT; k++) {
-            int li = threadIdx.x + k * NT;
-            if (li < T.ni) row[li] = make_double4(S[k][0], S[k][1], S[k][2], S[k][3]);
+            int li = slot + k * NT;
+            if (lane0 && li < T.ni) row[li] = make_double4(S[k][0], S[k][1], S[k][2], S[k][3]);
         }
         const Group G = A.groups[T.group];
         if (group_arrive(A.group_counters, T.group, G.nchunk, &s_flag)) {
