@@ -54,7 +54,24 @@ SM_COUNT = 148
 G5_CFG_NAMES = ["128x4", "256x2", "512x2", "1024x1", "384x2", "128x2", "128x1", "64x1"]   # pgb5 configurations (threads x i/thread)
 PROFILED_TRAFFIC = {
     "hermite": {"bytes": 25_623_040, "source": "profiles/g6_kernel_hermite_65536x65536.md (256x2 configuration)"},
+    "direct": {"bytes": 542_464, "pairs": 268_435_456, "source": "profiles/g5_kernels_direct_treepm_bh.md (1024x1)"},
+    "treepm": {"bytes": 587_407_104, "pairs": 4_463_983_086,
+               "source": "profiles/g5_kernels_direct_treepm_bh.md (128x1)"},
+    # captured at N = 2^20 (both launches of a step); scaled to the run's pairs
+    "bh": {"bytes": 133_551_616 + 27_101_952 + 228_377_600 + 30_923_520, "pairs": 4_462_862_693,
+           "source": "profiles/g5_kernels_direct_treepm_bh.md (64x1, N=2^20 capture scaled by pairs)"},
 }
+
+
+def profiled_traffic(workload, pairs):
+    """DRAM bytes of one step's roofline kernel launches from the committed capture, scaled to
+    `pairs` when the run's size differs from the capture's (traffic grows with the lists)."""
+    e = PROFILED_TRAFFIC.get(workload)
+    if not e:
+        return None, None
+    if "pairs" in e and pairs != e["pairs"]:
+        return int(e["bytes"] * pairs / e["pairs"]), e["source"]
+    return e["bytes"], e["source"]
 FP32_LANES = 128
 
 
@@ -523,6 +540,7 @@ def _timed_launches(torch, s, launch, steps, warmup, flush):
 
 def _line(args, ws, metric, value, t_step, pairs, flop, workload, dtype, achieved_tf, clk, e2e, cpu, launches,
           extra=None, kernel=""):
+    traffic, tsrc = profiled_traffic(args.workload, pairs)
     pk = peaks()
     sm_mhz = clk.get("sm_mhz") or pk.get("sm_max_mhz", 1965.0)
     peak_tf = SM_COUNT * FP32_LANES * 2 * sm_mhz * 1e6 / 1e12
@@ -534,7 +552,8 @@ def _line(args, ws, metric, value, t_step, pairs, flop, workload, dtype, achieve
                    "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{ws}"},
         "frac_fp32": round((value * 1e9 * flop / 1e12 if isinstance(flop, (int, float)) else achieved_tf) / peak_tf, 4),
         "roofline": {"bound": "fp32", "achieved": round(achieved_tf, 2), "peak": round(peak_tf, 2), "unit": "TFLOP/s",
-                     "frac": round(achieved_tf / peak_tf, 4), "traffic": None, "kernel": kernel,
+                     "frac": round(achieved_tf / peak_tf, 4), "traffic": traffic, "traffic_source": tsrc,
+                     "kernel": kernel,
                      "peak_source": f"148 SM x 128 FP32 lanes x 2 x median SM clock {sm_mhz:.0f} MHz"},
         "e2e": e2e, "gpu_launches": launches, "clocks": clk, "cpu_baseline": cpu,
     }
@@ -719,10 +738,17 @@ def run_treepm(args, pgb, ws, rank, local):
     plan = tab.plan_create(ts_.items)
     s = torch.cuda.Stream(device=dev)
     tcfg = None
-    if not args.no_tune:
+    if not args.no_tune and not args.profile_largest:
         tcfg, _ = tab.plan_tune(plan, d_i.data_ptr(), d_j.data_ptr(), d_o.data_ptr(), s.cuda_stream)
     tcfg = tab.L.pgb5_plan_config(plan)
     launch = lambda: tab.plan_launch(plan, d_i.data_ptr(), d_j.data_ptr(), d_o.data_ptr(), s.cuda_stream)  # noqa
+    if args.profile_largest:
+        # profiling target: the batch's launch four times (configuration: PGB_G5_CFG or the default)
+        for _ in range(4):
+            launch()
+        s.synchronize()
+        tab.plan_destroy(plan)
+        return {"profile": "PG5 table TreePM batch", "config": G5_CFG_NAMES[tcfg], "launches": 4}
     clocks = ClockSampler(local)
     clocks.start()
     barrier(ws)
@@ -801,10 +827,20 @@ def run_bh(args, pgb, ws, rank, local):
     pl_c = g5.plan_create(g5.QUAD, bh.items("c"))
     args_p = (d_i.data_ptr(), d_p.data_ptr(), None, d_pi.data_ptr(), o_p.data_ptr(), s.cuda_stream)
     args_c = (d_i.data_ptr(), d_c.data_ptr(), d_q.data_ptr(), d_ci.data_ptr(), o_c.data_ptr(), s.cuda_stream)
-    if not args.no_tune:
+    if not args.no_tune and not args.profile_largest:
         g5.plan_tune_indexed(pl_p, *args_p)
         g5.plan_tune_indexed(pl_c, *args_c)
     cfg_p, cfg_c = g5.L.pgb5_plan_config(pl_p), g5.L.pgb5_plan_config(pl_c)
+    if args.profile_largest:
+        # profiling target: (point-mass launch, cell launch) twice (configuration: PGB_G5_CFG or
+        # the default)
+        for _ in range(2):
+            g5.plan_launch_indexed(pl_p, *args_p)
+            g5.plan_launch_indexed(pl_c, *args_c)
+        s.synchronize()
+        g5.plan_destroy(pl_p)
+        g5.plan_destroy(pl_c)
+        return {"profile": "Barnes-Hut batch", "config": [G5_CFG_NAMES[cfg_p], G5_CFG_NAMES[cfg_c]], "launches": 4}
 
     def launch():
         g5.plan_launch_indexed(pl_p, *args_p)
@@ -1013,7 +1049,7 @@ def main():
                     help="FP64 x_j - x_i (DADD + F2F) instead of the double-float subtraction")
     ap.add_argument("--profile-largest", action="store_true",
                     help="profiling target: set up, warm, then run the largest call's force launch 3 times "
-                         "(direct: the evaluation's launch 4 times)")
+                         "(direct, treepm: the batch's launch 4 times; bh: both launches twice)")
     ap.add_argument("--profile-api", action="store_true",
                     help="profiling target: four full-size drop-in API calls (48 i x N j) and exit")
     args = ap.parse_args()
