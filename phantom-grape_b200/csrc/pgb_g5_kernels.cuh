@@ -144,12 +144,14 @@ __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
         int t = next_task(A.task_counter, &s_task, A.ntasks, first);
         if (t >= A.ntasks) break;
         const Task T = A.tasks[t];
-        // j-lanes (the 64-thread one-i-per-thread CTAs): a task of few i takes whole warps of i-slots
-        // (isl = ni rounded up to 32) and splits each j-tile over the nl = NT / isl lanes of
-        // slots; the lanes' sums are added in lane order at the end.  Large tasks: nl = 1.
+        // j-lanes (the 64-thread one-i-per-thread CTAs): a task of few i takes half-warps of
+        // i-slots (isl = ni rounded up to 16; the two half-warps of a warp then read two j records,
+        // which a 16-byte shared load serves in the same two wavefronts as a broadcast) and
+        // splits each j-tile over the nl = NT / isl lanes of slots; the lanes' sums are added in
+        // lane order at the end.  Large tasks: nl = 1.
         int nl = 1, isl = NT;
         if constexpr (LANES) {
-            const int need = (T.ni + 31) & ~31;
+            const int need = (T.ni + 15) & ~15;
             nl = NT / (need > 0 ? need : 32);
             isl = NT / nl;
         }
