@@ -475,6 +475,14 @@ def run_hermite(args, pgb, ws, rank, local):
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_hermite(pgb, wl)
+        # the FP64 check of the batched results of the call closest to 1024 active particles
+        rows = d_out.cpu().numpy().view(ffi.G6OUT)
+        c = int(np.argmin([abs(len(x) - 1024) for x in sets]))
+        a0, a1 = int(off[c]), int(off[c + 1])
+        xp_c, vp_c = predict_np(wl["t_calls"][c], st)
+        cpu["fp64_check"] = fp64_check_g6(rows[a0:a1], wl["xi"][a0:a1], wl["vi"][a0:a1],
+                                          st.idx[wl["set_idx"][a0:a1]], st.eps2, xp_c, vp_c, st.mass, st.idx)
+        cpu["fp64_check"]["call"] = f"call {c} ({a1 - a0} active x {n} j)"
     for p_ in plans:
         g6.plan_destroy(p_)
     del graph
@@ -521,6 +529,34 @@ def run_hermite(args, pgb, ws, rank, local):
 
 # ----------------------------------------------------------------------------------------
 # other workloads (PG5 direct, PG5 table / TreePM, independent Hermite clusters)
+
+def _err_stats(got, ref, vec=True):
+    """rms and max relative error of got against ref (per row for vectors)."""
+    if vec:
+        e = np.linalg.norm(got - ref, axis=1) / np.linalg.norm(ref, axis=1)
+    else:
+        e = np.abs(got - ref) / np.abs(ref)
+    return {"rms": float(np.sqrt(np.mean(e * e))), "max": float(e.max())}
+
+
+def fp64_check_g6(out_rows, xi, vi, idi, eps2, xj, vj, mj, idj, jadr_base=0):
+    """Hermite results (G6OUT rows) against the FP64 oracle on the same inputs: acc, jerk and pot
+    errors, and NN index mismatches where the FP64 first and second neighbours differ by
+    > 1e-5 (relative, in r^2).  The GRAPE-6 path carries velocities and masses as float.
+    jadr_base: j address of xj[0] in the launch (the NN result is an absolute j address)."""
+    from oracle import oracle as O
+    f = lambda a: np.asarray(a, np.float32).astype(np.float64)  # noqa: E731
+    ref = O.g6_force(xi, f(vi), idi, np.float32(eps2), xj, f(vj), f(mj), idj)
+    acc = np.stack([out_rows["ax"], out_rows["ay"], out_rows["az"]], 1)
+    jrk = np.stack([out_rows["jx"], out_rows["jy"], out_rows["jz"]], 1)
+    clear = ref["r2nn2"] / ref["r2nn"] - 1.0 > 1e-5
+    nn = out_rows["jadr"].astype(np.int64) - jadr_base
+    nn_id = np.where((nn >= 0) & (nn < len(idj)), idj[np.clip(nn, 0, len(idj) - 1)], -1)
+    return {"acc": _err_stats(acc, ref["acc"]), "jerk": _err_stats(jrk, ref["jrk"]),
+            "pot": _err_stats(out_rows["pot"], ref["pot"], vec=False),
+            "nn_mismatch": int(np.sum(nn_id[clear] != ref["nnb"][clear])), "particles": int(len(xi)),
+            "oracle": "FP64 direct sum on the same inputs (oracle/pg_oracle.c)"}
+
 
 def _timed_launches(torch, s, launch, steps, warmup, flush):
     for _ in range(warmup):
@@ -625,6 +661,15 @@ def run_direct(args, pgb, ws, rank, local):
                      for _ in range(reps))
             cpu = {"value": pairs * reps / tr / 1e9, "unit": "Gint/s", "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"{reps} full evaluations, PG5/newton/libpg5 AVX2 + OpenMP (g5_calculate_force_on_x)"}
+        from oracle import oracle as O
+        smp = np.sort(W.Rng(1024).permutation(n)[:1024])
+        f64 = lambda a: np.asarray(a, np.float32).astype(np.float64)  # noqa: E731
+        ao, po = O.g5_newton(f64(ipos[smp, :3]), f64(ipos[smp, 3]), f64(jpos[:, :3]), f64(jpos[:, 3]))
+        og = d_o.cpu().numpy()[smp]
+        if cpu is None:
+            cpu = {}
+        cpu["fp64_check"] = {"acc": _err_stats(og[:, :3], ao), "pot": _err_stats(-og[:, 3], po, vec=False),
+                             "particles": 1024, "oracle": "FP64 direct sum on the same float32 inputs"}
     g5.plan_destroy(plan)
     return _line(args, ws, "Gint/s (PG5 newton direct sum, batched)", value, t_max / len(ts), pairs, 38,
                  "PG5 newton N=16384 Plummer eps=0.01, all i vs all j (acc + pot)", "f32 (f64 cross-tile sums)",
@@ -702,6 +747,27 @@ def run_clusters(args, pgb, ws, rank, local):
             cpu = {"value": float(cum[ncl - 1]) / tr / 1e9, "unit": "Gint/s", "cores": os.cpu_count(),
                    "kind": "reference", "sample": f"first {ncl} of 1024 clusters ({cum[ncl - 1]:.3e} pairs), "
                    "PG6/libpg6 AVX2 + OpenMP through the same plain call sequence"}
+        # FP64 check of the batched results of every 64th cluster
+        rows = d_o.cpu().numpy().view(ffi.G6OUT)
+        ck = {"acc": [], "jerk": [], "pot": [], "nn": 0, "n": 0}
+        nsel = 0
+        for k in range(0, len(cs.sizes), 64):
+            o, m_ = int(cs.offsets[k]), int(cs.sizes[k])
+            sl = slice(o, o + m_)
+            r = fp64_check_g6(rows[sl], cs.pos[sl], cs.vel[sl], idx[sl], cs.eps2, cs.pos[sl], cs.vel[sl],
+                              cs.mass[sl], idx[sl], jadr_base=o)
+            for key in ("acc", "jerk", "pot"):
+                ck[key].append((r[key]["rms"] ** 2 * r["particles"], r[key]["max"]))
+            ck["nn"] += r["nn_mismatch"]
+            ck["n"] += r["particles"]
+            nsel += 1
+        if cpu is None:
+            cpu = {}
+        cpu["fp64_check"] = {key: {"rms": float(np.sqrt(sum(a for a, _ in ck[key]) / ck["n"])),
+                                   "max": float(max(b for _, b in ck[key]))} for key in ("acc", "jerk", "pot")}
+        cpu["fp64_check"].update({"nn_mismatch": ck["nn"], "particles": ck["n"],
+                                  "clusters": f"every 64th of 1024 ({nsel})",
+                                  "oracle": "FP64 direct sum on the same inputs (oracle/pg_oracle.c)"})
     g6.plan_destroy(plan)
     return _line(args, ws, "Gint/s (independent Hermite clusters, batched)", value, t_max / len(ts), pairs, 60,
                  "1024 Plummer clusters, N log-uniform [256,16384], eps=1e-4, one force+jerk+pot+NN each",
@@ -711,6 +777,14 @@ def run_clusters(args, pgb, ws, rank, local):
                   "g6_set_ti, g6calc_firsthalf/lasthalf2p per npipes), host buffers"},
                  cpu, len(ts), extra={"autotune": cfg, "batched_vs_plain": round(value / e2e_val, 1)},
                  kernel="pgb::g6_kernel (autotuned configuration)")
+
+
+def split_force_np(r, ts_):
+    """The analytic TreePM force shape (workloads.gaussian_split_force) on an array of r."""
+    from scipy.special import erfc
+    rs, eps = ts_.rs, ts_.eps
+    g = erfc(r / (2.0 * rs)) + r / (np.sqrt(np.pi) * rs) * np.exp(-r * r / (4.0 * rs * rs))
+    return np.where(r >= ts_.rcut * (1.0 - 1e-6), 0.0, g / (r * r + eps * eps) ** 1.5)
 
 
 def run_treepm(args, pgb, ws, rank, local):
@@ -790,6 +864,28 @@ def run_treepm(args, pgb, ws, rank, local):
                    "kind": "reference", "sample": f"first {ng} of {len(items)} groups ({sp:.3e} pairs), "
                    "PG5/table/libpg5 (512-entry table: the table size is fixed at compile time there), "
                    "OpenMP over groups with g5_*MC(devid) as source.cpp does"}
+        # FP64 check: the same table and lerp evaluated in FP64 on every 64th group's inputs, and
+        # the table's own error against the analytic force shape on the same pairs
+        from oracle import oracle as O
+        tab.set_table(f, ts_.rcut, frc_bit=6)
+        t_, _ = tab.table()
+        og = d_o.cpu().numpy()
+        got, ref, ana = [], [], []
+        for k in range(0, len(ts_.items), 64):
+            i0, ni_, j0, nj_ = (int(v) for v in ts_.items[k])
+            xi_ = ip[i0:i0 + ni_, :3].astype(np.float64) / xs
+            xj_ = jp[j0:j0 + nj_, :3].astype(np.float64) / xs
+            ref.append(O.g5_table(xi_, xj_, ts_.mj[j0:j0 + nj_], t_, 4, 6, xs))
+            got.append(og[i0:i0 + ni_, :3])
+            d = xj_[None, :, :] - xi_[:, None, :]
+            r = np.sqrt((d * d).sum(2))
+            ana.append((ts_.mj[j0:j0 + nj_][None, :, None] * d * split_force_np(r, ts_)[:, :, None]).sum(1))
+        got, ref, ana = np.concatenate(got), np.concatenate(ref), np.concatenate(ana)
+        if cpu is None:
+            cpu = {}
+        cpu["fp64_check"] = {"acc": _err_stats(got, ref), "table_vs_analytic_acc": _err_stats(ref, ana),
+                             "particles": int(len(got)),
+                             "oracle": "FP64 evaluation of the same 1024-entry table and lerp on the same inputs"}
     tab.plan_destroy(plan)
     return _line(args, ws, "Gint/s (PG5 table cutoff force, TreePM PP, batched)", value, t_max / len(tms), pairs, 38,
                  "PG5 table N=2^20 uniform periodic box, 1024-entry Gaussian-split table, 4096 i-groups",
@@ -923,7 +1019,7 @@ def run_bh(args, pgb, ws, rank, local):
     dropin_val = reduce_sum(float(pairs), ws, dev) / reduce_max(dropin_t, ws, dev) / 1e9
     dropin_rms = float(np.sqrt(np.mean(np.sum((acc - acc_b) ** 2, 1) / np.sum(acc_b ** 2, 1))))
     errors = {"dropin_vs_batched_rms": dropin_rms}
-    if rank == 0 and not args.no_errors:
+    if rank == 0 and ws == 1 and not args.no_errors and not args.no_cpu_baseline:
         from oracle import oracle as O
         # FP64 on the same lists and inputs (every 97th group), and the full FP64 direct sum
         # (multipole truncation) on 4096 sampled particles
