@@ -66,6 +66,15 @@ def lib() -> C.CDLL:
             L.orc_g6_force.argtypes = [C.c_int, dp, dp, ip, C.c_double, dp, C.c_int, dp, dp, dp, ip,
                                        dp, dp, dp, ip, dp, dp, dp, ip, ip, C.c_int]
             L.orc_g6_force.restype = C.c_int
+            L.orc_hermite_select.argtypes = [C.c_int, dp, dp, dp, ip]
+            L.orc_hermite_select.restype = C.c_int
+            L.orc_hermite_predict.argtypes = [C.c_int, ip, C.c_double, dp, dp, dp, dp, dp, dp, dp]
+            L.orc_hermite_predict.restype = None
+            L.orc_hermite_correct.argtypes = [C.c_int, ip, C.c_double, dp, dp, dp, dp, dp, C.c_double, C.c_double,
+                                              dp, dp, dp, dp, dp, dp, dp]
+            L.orc_hermite_correct.restype = None
+            L.orc_hermite_startup.argtypes = [C.c_int, ip, dp, dp, dp, C.c_double, C.c_double, dp, dp, dp, dp, dp]
+            L.orc_hermite_startup.restype = C.c_int
             L.orc_potential_energy.argtypes = [C.c_int, dp, dp, C.c_double]
             L.orc_potential_energy.restype = C.c_double
             _lib = L
@@ -179,3 +188,116 @@ def ref_available(name: str = "libpg5_ref.so") -> bool:
 def load_ref(name: str) -> C.CDLL:
     """Load one reference library privately (RTLD_LOCAL), a fresh handle per call site."""
     return C.CDLL(ref_path(name), mode=os.RTLD_LOCAL | os.RTLD_NOW)
+
+
+# ------------------------------------------------------------------------------------------
+# Hermite block-time-step integrator (PG6/banana): see pg_oracle.c orc_hermite_*.
+
+class HermiteState:
+    """The integrator's particle state in the reference's storage precision (struct Particle,
+    PG6/banana/particle.h): t, dt, pos, vel, acc in FP64; jrk, mass, pot as floats (held in
+    float64 arrays with float values)."""
+
+    def __init__(self, pos, vel, mass, dtmax):
+        n = len(mass)
+        self.n = n
+        self.t = np.zeros(n)
+        self.dt = np.full(n, float(dtmax))
+        self.pos = np.ascontiguousarray(pos, D).copy()
+        self.vel = np.ascontiguousarray(vel, D).copy()
+        self.acc = np.zeros((n, 3))
+        self.jrk = np.zeros((n, 3))
+        self.mass = np.asarray(mass, F).astype(D)
+        self.pot = np.zeros(n)
+
+    def copy(self):
+        o = HermiteState.__new__(HermiteState)
+        o.n = self.n
+        for k in ("t", "dt", "pos", "vel", "acc", "jrk", "mass", "pot"):
+            setattr(o, k, getattr(self, k).copy())
+        return o
+
+    def jmem(self):
+        """The j-memory records the integrator writes (g6_set_j_particle arguments,
+        hermite.c:240-265): acc/2 and jrk*(1/6)."""
+        return self.pos, self.vel, self.acc * 0.5, self.jrk * (1.0 / 6.0), self.mass, self.t
+
+    def energy(self):
+        """calc_energy.c:9-33: kinetic sum m v^2 / 2 and potential sum m pot / 2."""
+        ek = 0.5 * float(np.sum(self.mass * np.sum(self.vel * self.vel, axis=1)))
+        ew = 0.5 * float(np.sum(self.mass * self.pot))
+        return ek + ew, ek, ew
+
+
+def hermite_select(st: HermiteState):
+    t_gl = C.c_double()
+    act = np.empty(st.n, I32)
+    ni = lib().orc_hermite_select(st.n, _p(st.t), _p(st.dt), C.byref(t_gl), _p(act, C.c_int))
+    return t_gl.value, act[:ni].copy()
+
+
+def hermite_predict(st: HermiteState, act, t_gl):
+    act = np.ascontiguousarray(act, I32)
+    xp = np.empty((len(act), 3))
+    vp = np.empty((len(act), 3))
+    lib().orc_hermite_predict(len(act), _p(act, C.c_int), t_gl, _p(st.t), _p(st.pos), _p(st.vel), _p(st.acc),
+                              _p(st.jrk), _p(xp), _p(vp))
+    return xp, vp
+
+
+def hermite_correct(st: HermiteState, act, t_gl, xp, vp, acc1, jrk1, pot1, eta, dtmax):
+    act = np.ascontiguousarray(act, I32)
+    lib().orc_hermite_correct(len(act), _p(act, C.c_int), t_gl, _p(_c(xp, D)), _p(_c(vp, D)), _p(_c(acc1, D)),
+                              _p(_c(jrk1, D)), _p(_c(pot1, D)), eta, dtmax, _p(st.t), _p(st.dt), _p(st.pos),
+                              _p(st.vel), _p(st.acc), _p(st.jrk), _p(st.pot))
+
+
+def hermite_startup(st: HermiteState, act, acc1, jrk1, pot1, eta_s, dtmax):
+    act = np.ascontiguousarray(act, I32)
+    return lib().orc_hermite_startup(len(act), _p(act, C.c_int), _p(_c(acc1, D)), _p(_c(jrk1, D)),
+                                     _p(_c(pot1, D)), eta_s, dtmax, _p(st.t), _p(st.dt), _p(st.acc),
+                                     _p(st.jrk), _p(st.pot))
+
+
+def hermite_run(st: HermiteState, force, eta, eta_s, dtmax, tend, outputs=None, on_step=None):
+    """The sample integrator's main loop (PG6/banana/banana01.c:96-183) restated over the
+    functions above: the start-up step at t = 0 with every particle active, then block steps
+    while the global time t_mod*dtmax + t_gl < tend.  After a step whose t_gl is a multiple of
+    dtmax the output is taken (outputs.append((time, e, ek, ew, particle_steps, block_steps)))
+    and the times are reset (reset_time, timestep.c:127-135).
+    force(act, t_gl, xp, vp, changed) -> (acc, jrk, pot) evaluates the active i-particles
+    (predicted xp, vp) against the j-memory; `changed` lists the particles whose j-memory record
+    (HermiteState.jmem) changed since the previous call.  on_step(t_gl, act) is called after
+    every block step."""
+    n = st.n
+    act = np.arange(n, dtype=I32)
+    xp, vp = hermite_predict(st, act, 0.0)
+    a, j, p = force(act, 0.0, xp, vp, act)
+    bad = hermite_startup(st, act, a, j, p, eta_s, dtmax)
+    if bad:
+        raise RuntimeError("start-up step below dtmin")
+    steps, blocks = n, 1
+    if outputs is not None:
+        outputs.append((0.0, *st.energy(), steps, blocks))
+        steps = blocks = 0
+    changed = act
+    t_mod, t_gl = 0, 0.0
+    while t_mod * dtmax + t_gl < tend:
+        t_gl, act = hermite_select(st)
+        xp, vp = hermite_predict(st, act, t_gl)
+        a, j, p = force(act, t_gl, xp, vp, changed)
+        hermite_correct(st, act, t_gl, xp, vp, a, j, p, eta, dtmax)
+        changed = act
+        steps += len(act)
+        blocks += 1
+        if on_step is not None:
+            on_step(t_gl, act)
+        if t_gl - int(t_gl * (1.0 / dtmax)) * dtmax == 0.0:
+            if outputs is not None:
+                outputs.append((t_mod * dtmax + t_gl, *st.energy(), steps, blocks))
+                steps = blocks = 0
+            t_mod += 1
+            t_gl = 0.0
+            st.t[:] = 0.0
+            changed = np.arange(n, dtype=I32)
+    return t_mod * dtmax + t_gl

@@ -287,3 +287,138 @@ double orc_potential_energy(int n, const double *x, const double *m, double eps2
     }
     return w;
 }
+
+/* ------------------------------------------------------------------------------------ */
+/* PG6 4th-order Hermite block-time-step integrator (the reference's sample integrator,
+ * PG6/banana, built with -DNORMAL as its setting.mk does).  State per particle i, as
+ * struct Particle (PG6/banana/particle.h) stores it: t, dt, pos[3], vel[3], acc[3] (double),
+ * jrk[3], mass, pot (float, held here as the double of a float).
+ *
+ * orc_hermite_select -- the block step: t_gl = min_i (t_i + dt_i) and the active set
+ *   {i : t_i + dt_i == t_gl} in index order (timestep.c:87-98 global_time, whose sorted
+ *   index list yields that set under the block-step invariant).  Returns ni.
+ * orc_hermite_predict -- the i-particle predictor (hermite.c:39-63 predict_exmotion):
+ *   x + v dt + a dt^2 (1/2) + j dt^3 (1/6), v + a dt + j dt^2 (1/2), with the reference's
+ *   decimal constants 5e-1 and 1.666666666666667e-1.
+ * orc_hermite_correct -- the corrector and the new step (hermite.c:67-108 correct,
+ *   143-205 correct_sgmotion, timestep.c:53-85 dt_criterion) for the active set, given the
+ *   new force (acc1 double; jrk1 and pot1 rounded to float as NewAccJerk stores them).
+ * orc_hermite_startup -- the first step (hermite.c:110-141 startup_sgmotion,
+ *   timestep.c:24-51 dt_startup).
+ * calc_modulus (timestep.c:137-150) decides whether t is a multiple of a block step. */
+static double orc_calc_modulus(double num, double mod, double modmax)
+{
+    double tmpmod = modmax;
+    while (num > 0.0) {
+        while (tmpmod > num) tmpmod *= 0.5;
+        if (tmpmod < mod) break;
+        num -= tmpmod;
+    }
+    return num;
+}
+
+int orc_hermite_select(int n, const double *t, const double *dt, double *t_gl, int *active)
+{
+    double tm = 1e300;
+    for (int i = 0; i < n; i++)
+        if (t[i] + dt[i] < tm) tm = t[i] + dt[i];
+    int ni = 0;
+    for (int i = 0; i < n; i++)
+        if (t[i] + dt[i] == tm) active[ni++] = i;
+    *t_gl = tm;
+    return ni;
+}
+
+void orc_hermite_predict(int ni, const int *active, double t_gl, const double *t, const double *pos,
+                         const double *vel, const double *acc, const double *jrk, double *xp, double *vp)
+{
+    const double second = 5e-1, third = 1.666666666666667e-1;
+    for (int k = 0; k < ni; k++) {
+        const int i = active[k];
+        const double d = t_gl - t[i], d2 = d * d, d3 = d * d2;
+        for (int c = 0; c < 3; c++) {
+            xp[3*k+c] = pos[3*i+c] + vel[3*i+c] * d + acc[3*i+c] * d2 * second + jrk[3*i+c] * d3 * third;
+            vp[3*k+c] = vel[3*i+c] + acc[3*i+c] * d + jrk[3*i+c] * d2 * second;
+        }
+    }
+}
+
+/* In place on the state arrays; t_gl is the step's time (= t_i + dt_i of every active i). */
+void orc_hermite_correct(int ni, const int *active, double t_gl, const double *xp, const double *vp,
+                         const double *acc1, const double *jrk1, const double *pot1, double eta,
+                         double dtmax, double *t, double *dt, double *pos, double *vel, double *acc,
+                         double *jrk, double *pot)
+{
+    const double third = 1.666666666666667e-1, fourth = 4.166666666666667e-2, fifth = 8.333333333333333e-3;
+    const double dtmin = dtmax / pow(2.0, 51.0);
+    for (int k = 0; k < ni; k++) {
+        const int i = active[k];
+        const double dts = dt[i], dtsinv = 1.0 / dts;
+        double s0[3], c0[3], x1[3], v1[3], a1[3], j1[3];
+        for (int c = 0; c < 3; c++) {
+            a1[c] = acc1[3*k+c];
+            j1[c] = (double)(float)jrk1[3*k+c];
+            x1[c] = xp[3*k+c];
+            v1[c] = vp[3*k+c];
+            const double a0 = acc[3*i+c], j0 = jrk[3*i+c];
+            s0[c] = 2.0 * (-3.0 * (a0 - a1[c]) - (2.0 * j0 + j1[c]) * dts) * dtsinv * dtsinv;
+            c0[c] = 6.0 * (2.0 * (a0 - a1[c]) + (j0 + j1[c]) * dts) * dtsinv * dtsinv * dtsinv;
+            x1[c] += s0[c] * dts * dts * dts * dts * fourth + c0[c] * dts * dts * dts * dts * dts * fifth;
+            v1[c] += s0[c] * dts * dts * dts * third + c0[c] * dts * dts * dts * dts * fourth;
+        }
+        /* dt_criterion at the new time t_gl with the old step */
+        double s1[3], a = 0, jj = 0, sn = 0, cr = 0, dnew = dts;
+        for (int c = 0; c < 3; c++) {
+            s1[c] = s0[c] + c0[c] * dts;
+            a += a1[c] * a1[c];
+            jj += j1[c] * j1[c];
+            sn += s1[c] * s1[c];
+            cr += c0[c] * c0[c];
+        }
+        a = sqrt(a); jj = sqrt(jj); sn = sqrt(sn); cr = sqrt(cr);
+        const double dti = eta * sqrt((a * sn + jj * jj) / (jj * cr + sn * sn));
+        if (dti < dnew) {
+            while (dnew > dti && dnew > dtmin) dnew *= 0.5;
+        } else if (dti > 2.0 * dnew) {
+            if (orc_calc_modulus(t_gl, 2.0 * dnew, dtmax) == 0.0) dnew = 2.0 * dnew;
+        }
+        t[i] = t_gl;
+        dt[i] = dnew;
+        for (int c = 0; c < 3; c++) {
+            pos[3*i+c] = x1[c];
+            vel[3*i+c] = v1[c];
+            acc[3*i+c] = a1[c];
+            jrk[3*i+c] = j1[c];
+        }
+        pot[i] = (double)(float)pot1[k];
+    }
+}
+
+/* Returns the number of particles whose step fell below dtmin (the reference exits there). */
+int orc_hermite_startup(int ni, const int *active, const double *acc1, const double *jrk1, const double *pot1,
+                        double eta_s, double dtmax, const double *t, double *dt, double *acc, double *jrk,
+                        double *pot)
+{
+    const double dtmin = dtmax / pow(2.0, 51.0);
+    int bad = 0;
+    for (int k = 0; k < ni; k++) {
+        const int i = active[k];
+        double a = 0, jj = 0;
+        for (int c = 0; c < 3; c++) {
+            acc[3*i+c] = acc1[3*k+c];
+            jrk[3*i+c] = (double)(float)jrk1[3*k+c];
+            a += acc[3*i+c] * acc[3*i+c];
+            jj += jrk[3*i+c] * jrk[3*i+c];
+        }
+        pot[i] = (double)(float)pot1[k];
+        const double dtcrit = eta_s * sqrt(a / jj);
+        double d = dtmax;
+        while (d > dtcrit && d > dtmin) d *= 0.5;
+        while (orc_calc_modulus(t[i], d, dtmax) != 0.0) {
+            d *= 0.5;
+            if (d < dtmin) { bad++; break; }
+        }
+        dt[i] = d;
+    }
+    return bad;
+}

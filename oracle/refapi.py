@@ -181,6 +181,15 @@ class RefG6:
                                      float(mass[j]), _p(snp), _p(jrk6[j]), _p(acc2[j]), _p(vel[j]),
                                      _p(pos[j]))
 
+    def set_j_at(self, adr, pos, vel, acc2, jrk6, mass, tj):
+        """g6_set_j_particle for the j addresses adr (records taken from the full arrays)."""
+        pos, vel, acc2, jrk6 = (np.ascontiguousarray(a, D) for a in (pos, vel, acc2, jrk6))
+        snp = np.zeros(3, D)
+        for j in adr:
+            j = int(j)
+            self.L.g6_set_j_particle(0, j, j, float(tj[j]), 0.0, float(mass[j]), _p(snp), _p(jrk6[j]),
+                                     _p(acc2[j]), _p(vel[j]), _p(pos[j]))
+
     def calc(self, ti, nj, xi, vi, idi, eps2, h2=None, variant="2p"):
         """One g6_set_ti + chunked firsthalf/lasthalf<variant> over all i (chunks of npipes)."""
         xi = np.ascontiguousarray(xi, D)
