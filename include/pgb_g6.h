@@ -134,6 +134,37 @@ int  pgb6_batch_host(int nitem, const int *items, int ni, const double (*xi)[3],
 int  pgb6_force_noalloc(const void *ipart, int ni, const void *jpred, int nj, double eps2, void *out, int flags,
                         void *stream);
 
+/* ---- Hermite block-time-step integrator on the device (no counterpart in the reference's
+ * libraries).  Replaces the steps of the reference's sample integrator around the force call
+ * (PG6/banana, -DNORMAL): global_time (timestep.c:87-98), predict_exmotion (hermite.c:39-63),
+ * the g6_set_j_particle re-send of the active particles (hermite.c:240-265), correct /
+ * correct_sgmotion (hermite.c:67-108, 143-205), dt_criterion (timestep.c:53-85), the start-up
+ * step startup_sgmotion / dt_startup (hermite.c:110-141, timestep.c:24-51) and reset_time every
+ * dtmax (timestep.c:127-135, banana01.c:161-179).  The state stays in device memory between
+ * steps; given the same forces a step's new state equals the reference's formulas evaluated in
+ * plain FP64 bit for bit.  The force is the GRAPE-6 kernel of this library (eps2, id-excluded
+ * self pair).                                                                                  */
+typedef struct pgb6_hermite pgb6_hermite;
+/* n >= 2 particles; takes the start-up step (forces at t = 0, first steps); PGB_ERR_ARG when a
+ * start-up step falls below dtmax / 2^51 */
+int  pgb6_hermite_create(pgb6_hermite **h, int n, const double *mass, const double (*pos)[3],
+                         const double (*vel)[3], double eps2, double eta, double eta_s, double dtmax);
+/* one block step; *time = global time after it, *ni = particles advanced (both optional) */
+int  pgb6_hermite_step(pgb6_hermite *h, double *time, int *ni);
+/* block steps while the global time is below tend; steps taken by this call (optional) */
+int  pgb6_hermite_advance(pgb6_hermite *h, double tend, long long *psteps, long long *bsteps);
+double pgb6_hermite_time(pgb6_hermite *h);
+/* state as struct Particle holds it (any pointer may be NULL; jrk, pot with float values) */
+int  pgb6_hermite_get(pgb6_hermite *h, double *t, double *dt, double (*pos)[3], double (*vel)[3],
+                      double (*acc)[3], double (*jrk)[3], double *pot);
+/* the last step's active particles and their force-kernel results; returns their count */
+int  pgb6_hermite_last_step(pgb6_hermite *h, int *active, double (*acc)[3], double (*jrk)[3], double *pot);
+/* kinetic and potential energy, calc_energy.c:9-33 */
+int  pgb6_hermite_energy(pgb6_hermite *h, double *ek, double *ew);
+/* particle and block steps since creation (the start-up step counts n and 1) */
+void pgb6_hermite_counts(pgb6_hermite *h, long long *psteps, long long *bsteps);
+void pgb6_hermite_destroy(pgb6_hermite *h);
+
 #ifdef __cplusplus
 }
 #endif

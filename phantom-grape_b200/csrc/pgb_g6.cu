@@ -23,10 +23,12 @@
 //  * a neighbour list longer than the capacity (1024, PGB_G6_NBMAX) is counted, flagged by
 //    g6_read_neighbour_list and refused by g6_get_neighbour_list, never written out of bounds
 //    (gravity.c:896-906 writes before it checks).
+#include <atomic>
 #include <chrono>
 
 #include "pgb_g6_kernels.cuh"
 #include "pgb_g6_small.cuh"
+#include "pgb_hermite.cuh"
 
 using namespace pgb;
 
@@ -436,6 +438,7 @@ bool run_small(int nj, int ni, float eps2, bool nn, bool nbl, G6Out* out_dev) {
     a.nb_count = nullptr;
     a.nb_list = nullptr;
     a.nb_maxlen = nbmax();
+    a.irec = nullptr;
     if (nbl) {
         PGB_CUDA_OR(g_err, LIB, S.nbc_d.reserve(ni), return false);
         PGB_CUDA_OR(g_err, LIB, S.nbl_d.reserve((size_t)ni * nbmax()), return false);
@@ -1267,4 +1270,440 @@ PGB_EXPORT int pgb6_force_noalloc(const void* ipart, int ni, const void* jpred, 
     int grid = ntasks < slots ? ntasks : slots;
     PGB_CUDA_OR(g_err, LIB, launch_kernel(cfg, ff, nn, false, grid, a, s), return PGB_ERR_CUDA);
     return PGB_OK;
+}
+
+// ------------------------------------------------------------------------------------------
+// Hermite block-time-step integrator on the device (pgb_hermite.cuh): the reference's sample
+// integrator PG6/banana (hermite.c, timestep.c; banana01.c:96-183 main loop) with the particle
+// state, the j-memory and the per-step bookkeeping resident in HBM.  The host only learns each
+// step's active count (to size the force launch) through mapped memory.
+
+namespace {
+
+// Force of ni device-resident i-records against nj predicted j-records into out[0, ni): the
+// small-call cluster kernel up to G6_SMALL_MAXI i-particles, else the general kernel in regular
+// mode (tasks derived in the kernel, self-resetting counters: nothing uploaded).
+struct ForceScratch {
+    DevBuf<int> tcount;     // task counter of the regular launches
+    DevBuf<int> pcnt;       // slice counters of the small launches
+    DevBuf<G6Out> spart;    // cluster rows of the small launches
+    Stager<G6I, G6Out> st;  // partial rows and group counters of the regular launches
+    void release() {
+        tcount.release();
+        pcnt.release();
+        spart.release();
+        st.release();
+    }
+};
+
+bool force_device(ForceScratch& F, cudaStream_t s, const G6I* irec, int ni, const G6PredJ* jpred, int nj, float eps2,
+                  G6Out* out) {
+    if (ni <= 0 || nj <= 0) return true;
+    const bool ff = dx_ff();
+    if (ni <= G6_SMALL_MAXI) {
+        const SmallShape sh = small_shape(ni);
+        int grid = 1, cl = 1;
+        small_grid(sh, ff, false, false, nj, grid, cl);
+        PGB_CUDA_OR(g_err, LIB, F.spart.reserve((size_t)(grid / cl) * sh.isl), return false);
+        if (!F.pcnt.p) {
+            PGB_CUDA_OR(g_err, LIB, F.pcnt.reserve(SMALL_CL), return false);
+            PGB_CUDA_OR(g_err, LIB, F.pcnt.zero_fill(s), return false);
+        }
+        G6SmallArgs a{};
+        a.jpred = jpred;
+        a.eps2 = eps2;
+        a.ni = ni;
+        a.nj = nj;
+        a.partial = F.spart.p;
+        a.counter = F.pcnt.p;
+        a.out = out;
+        a.nb_maxlen = nbmax();
+        a.done = nullptr;
+        a.irec = irec;
+        static const G6IBlock unused{};
+        PGB_CUDA_OR(g_err, LIB, small_kernel(sh, ff, false, false, grid, cl, a, unused, s, nullptr), return false);
+        return true;
+    }
+    const int cfg = pick_cfg(ni);
+    const int itile = cfg_itile(cfg);
+    const int slots = sm_count(g_device) * occupancy(cfg, ff, false, false);
+    static const int maxch = env_int("PGB_G6_MAXCHUNKS", 512, 1, 4096);
+    const int itiles = (ni + itile - 1) / itile;
+    int nch = best_nch(itiles, nj, slots, maxch);
+    if (nch > nj) nch = nj;
+    const int rows = nch > 1 ? itiles * nch : 0;
+    PGB_CUDA_OR(g_err, LIB, F.st.reserve_scratch(s, rows, ITILE_MAX, (size_t)itiles), return false);
+    if (!F.tcount.p) {
+        PGB_CUDA_OR(g_err, LIB, F.tcount.reserve(1), return false);
+        PGB_CUDA_OR(g_err, LIB, F.tcount.zero_fill(s), return false);
+    }
+    G6Args a;
+    a.ipart = irec;
+    a.jpred = jpred;
+    a.eps2 = eps2;
+    a.tasks = nullptr;
+    a.ntasks = itiles * nch;
+    a.task_counter = F.tcount.p;
+    a.groups = nullptr;
+    a.group_counters = F.st.dgcnt.p;
+    a.partial = F.st.dpart.p;
+    a.out = out;
+    a.itile = itile;
+    a.bundle_counters = F.st.bundle_counters();
+    a.nb_count = nullptr;
+    a.nb_list = nullptr;
+    a.nb_maxlen = 0;
+    a.reg_ni = ni;
+    a.reg_nj = nj;
+    a.reg_nch = nch;
+    const int grid = a.ntasks < slots ? a.ntasks : slots;
+    PGB_CUDA_OR(g_err, LIB, launch_kernel(cfg, ff, false, false, grid, a, s), return false);
+    return true;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+}  // namespace
+
+struct pgb6_hermite {
+    std::mutex mu;
+    int n = 0, nseg = 0;
+    double eps2 = 0.0, eta = 0.0, eta_s = 0.0, dtmax = 0.0;
+    bool ff = true;
+    cudaStream_t s = nullptr;
+    DevBuf<double> state;          // t, dt, pot, mass [n]; pos, vel, acc, jrk [n][3]
+    DevBuf<unsigned char> work;    // HmWork's arrays
+    HostBuf<HmHostCtl> ctl;        // mapped: (seq, ni, t_gl) of the step in flight
+    HmState P{};
+    HmWork W{};
+    double* energy = nullptr;      // [2] device
+    ForceScratch F;
+    unsigned seq = 0;
+    int t_mod = 0;                 // completed dtmax intervals
+    double t_gl = 0.0;             // block time within the current interval
+    bool reset_pending = false;    // reset_time due before the next step
+    long long psteps = 0, bsteps = 0;
+    int last_ni = 0;
+};
+
+namespace {
+
+bool hm_alloc(pgb6_hermite* H) {
+    const size_t n = (size_t)H->n;
+    PGB_CUDA_OR(g_err, LIB, H->state.reserve(16 * n), return false);
+    double* b = H->state.p;
+    H->P.n = H->n;
+    H->P.t = b;
+    H->P.dt = b + n;
+    H->P.pot = b + 2 * n;
+    H->P.mass = b + 3 * n;
+    H->P.pos = b + 4 * n;
+    H->P.vel = b + 7 * n;
+    H->P.acc = b + 10 * n;
+    H->P.jrk = b + 13 * n;
+    H->nseg = (int)((n + HM_SEG - 1) / HM_SEG);
+    size_t off = 0;
+    const size_t o_hdr = off;
+    off = align256(off + 64);
+    const size_t o_bcnt = off;
+    off = align256(off + sizeof(int) * H->nseg);
+    const size_t o_boff = off;
+    off = align256(off + sizeof(int) * H->nseg);
+    const size_t o_act = off;
+    off = align256(off + sizeof(int) * n);
+    const size_t o_irec = off;
+    off = align256(off + sizeof(G6I) * n);
+    const size_t o_jpred = off;
+    off = align256(off + sizeof(G6PredJ) * n);
+    const size_t o_out = off;
+    off = align256(off + sizeof(G6Out) * n);
+    const size_t o_en = off;
+    off = align256(off + 2 * sizeof(double));
+    PGB_CUDA_OR(g_err, LIB, H->work.reserve(off), return false);
+    unsigned char* w = H->work.p;
+    H->W.tmin = (unsigned long long*)(w + o_hdr);
+    H->W.t_gl = (double*)(w + o_hdr + 8);
+    H->W.ticket = (int*)(w + o_hdr + 16);
+    H->W.ni = (int*)(w + o_hdr + 20);
+    H->W.bad = (int*)(w + o_hdr + 24);
+    H->W.bcnt = (int*)(w + o_bcnt);
+    H->W.boff = (int*)(w + o_boff);
+    H->W.active = (int*)(w + o_act);
+    H->W.irec = (G6I*)(w + o_irec);
+    H->W.jpred = (G6PredJ*)(w + o_jpred);
+    H->W.out = (G6Out*)(w + o_out);
+    H->energy = (double*)(w + o_en);
+    PGB_CUDA_OR(g_err, LIB, H->ctl.reserve(1, false, cudaHostAllocPortable | cudaHostAllocMapped), return false);
+    std::memset((void*)H->ctl.p, 0, sizeof(HmHostCtl));
+    PGB_CUDA_OR(g_err, LIB, cudaHostGetDevicePointer((void**)&H->W.host, H->ctl.p, 0), return false);
+    // header: tmin all ones, ticket / ni / bad zero
+    PGB_CUDA_OR(g_err, LIB, cudaMemsetAsync(w + o_hdr, 0, 64, H->s), return false);
+    PGB_CUDA_OR(g_err, LIB, cudaMemsetAsync(w + o_hdr, 0xff, 8, H->s), return false);
+    return true;
+}
+
+// The step's selection kernels; hm_count_kernel publishes (ni, t_gl) with sequence number seq.
+bool hm_select(pgb6_hermite* H) {
+    const int reset = H->reset_pending ? 1 : 0;
+    H->reset_pending = false;
+    hm_tmin_kernel<<<H->nseg, HM_NT, 0, H->s>>>(H->P, H->W, reset);
+    if (++H->seq == 0) H->seq = 1;
+    hm_count_kernel<<<H->nseg, HM_NT, 0, H->s>>>(H->P, H->W, H->seq);
+    hm_build_kernel<<<H->nseg, HM_NT, 0, H->s>>>(H->P, H->W, H->ff);
+    PGB_CUDA_OR(g_err, LIB, cudaGetLastError(), return false);
+    return true;
+}
+
+// Wait for the published (ni, t_gl): a bounded spin on the mapped sequence number, then the
+// stream synchronisation that reports a failed launch.
+bool hm_wait(pgb6_hermite* H, int* ni, double* tg) {
+    volatile HmHostCtl* c = H->ctl.p;
+    auto t0 = std::chrono::steady_clock::now();
+    for (long it = 0;; it++) {
+        if (c->seq == H->seq) break;
+        if ((it & 1023) == 1023 && std::chrono::steady_clock::now() - t0 > std::chrono::seconds(5)) {
+            PGB_CUDA_OR(g_err, LIB, cudaStreamSynchronize(H->s), return false);
+            if (c->seq != H->seq) {
+                raise(g_err, LIB, PGB_ERR_DEVICE, "hermite: block selection did not publish its result");
+                return false;
+            }
+            break;
+        }
+    }
+    std::atomic_thread_fence(std::memory_order_acquire);
+    *ni = c->ni;
+    *tg = c->t_gl;
+    return true;
+}
+
+// One block step (startup: the first, every particle active at t = 0).
+bool hm_step(pgb6_hermite* H, bool startup) {
+    if (!hm_select(H)) return false;
+    int ni = 0;
+    double tg = 0.0;
+    if (!hm_wait(H, &ni, &tg)) return false;
+    if (ni <= 0 || ni > H->n) {
+        raise(g_err, LIB, PGB_ERR_DEVICE, "hermite: block selection returned %d active particles", ni);
+        return false;
+    }
+    if (!force_device(H->F, H->s, H->W.irec, ni, H->W.jpred, H->n, (float)H->eps2, H->W.out)) return false;
+    const int nb = (ni + 127) / 128;
+    if (startup) hm_startup_kernel<<<nb, 128, 0, H->s>>>(H->P, H->W, ni, H->eta_s, H->dtmax);
+    else hm_correct_kernel<<<nb, 128, 0, H->s>>>(H->P, H->W, ni, H->eta, H->dtmax);
+    PGB_CUDA_OR(g_err, LIB, cudaGetLastError(), return false);
+    H->psteps += ni;
+    H->bsteps += 1;
+    H->last_ni = ni;
+    if (!startup) {
+        // banana01.c:161-179: after a step that ends on a multiple of dtmax the times restart
+        H->t_gl = tg;
+        if (tg - (double)(int)(tg * (1.0 / H->dtmax)) * H->dtmax == 0.0) {
+            H->t_mod += 1;
+            H->t_gl = 0.0;
+            H->reset_pending = true;
+        }
+    }
+    return true;
+}
+
+bool hm_apply_reset(pgb6_hermite* H) {
+    if (!H->reset_pending) return true;
+    H->reset_pending = false;
+    hm_reset_kernel<<<(H->n + 255) / 256, 256, 0, H->s>>>(H->P);
+    PGB_CUDA_OR(g_err, LIB, cudaGetLastError(), return false);
+    return true;
+}
+
+void hm_free(pgb6_hermite* H) {
+    if (H->s) cudaStreamSynchronize(H->s);
+    H->F.release();
+    H->state.release();
+    H->work.release();
+    H->ctl.release();
+    if (H->s) cudaStreamDestroy(H->s);
+    H->s = nullptr;
+}
+}  // namespace
+
+// Create an integrator for n particles (n >= 2) and take its start-up step: every particle's
+// force, jerk and potential at t = 0 and its first step (startup_sgmotion).  eps2: softening^2;
+// eta / eta_s: accuracy parameters of dt_criterion / dt_startup; dtmax: the largest step and the
+// interval after which the times restart from 0 (the reference's dtstar).
+PGB_EXPORT int pgb6_hermite_create(pgb6_hermite** out, int n, const double* mass, const double (*pos)[3],
+                                   const double (*vel)[3], double eps2, double eta, double eta_s, double dtmax) {
+    if (!out || n < 2 || n > (1 << 26) || !mass || !pos || !vel || !(eps2 >= 0.0) || !(eta > 0.0) ||
+        !(eta_s > 0.0) || !(dtmax > 0.0)) {
+        raise(g_err, LIB, PGB_ERR_ARG, "pgb6_hermite_create: bad arguments (n %d, eps2 %g, eta %g, eta_s %g, dtmax %g)",
+              n, eps2, eta, eta_s, dtmax);
+        return PGB_ERR_ARG;
+    }
+    *out = nullptr;
+    if (!ensure_device()) return PGB_ERR_NOGPU;
+    auto* H = new pgb6_hermite();
+    H->n = n;
+    H->eps2 = eps2;
+    H->eta = eta;
+    H->eta_s = eta_s;
+    H->dtmax = dtmax;
+    H->ff = dx_ff();
+    bool ok = cudaStreamCreateWithFlags(&H->s, cudaStreamNonBlocking) == cudaSuccess;
+    if (!ok) raise(g_err, LIB, PGB_ERR_CUDA, "pgb6_hermite_create: stream creation failed");
+    ok = ok && hm_alloc(H);
+    if (ok) {
+        const size_t nn = (size_t)n;
+        // t, dt, pot zero; acc, jrk zero; mass, pos, vel from the caller
+        ok = cudaMemsetAsync(H->state.p, 0, 16 * nn * sizeof(double), H->s) == cudaSuccess &&
+             cudaMemcpyAsync(H->P.mass, mass, nn * sizeof(double), cudaMemcpyHostToDevice, H->s) == cudaSuccess &&
+             cudaMemcpyAsync(H->P.pos, pos, 3 * nn * sizeof(double), cudaMemcpyHostToDevice, H->s) == cudaSuccess &&
+             cudaMemcpyAsync(H->P.vel, vel, 3 * nn * sizeof(double), cudaMemcpyHostToDevice, H->s) == cudaSuccess;
+        if (!ok) raise(g_err, LIB, PGB_ERR_CUDA, "pgb6_hermite_create: upload failed");
+    }
+    ok = ok && hm_step(H, true);
+    int bad = 0;
+    if (ok) {
+        ok = cudaMemcpyAsync(&bad, H->W.bad, sizeof(int), cudaMemcpyDeviceToHost, H->s) == cudaSuccess &&
+             cudaStreamSynchronize(H->s) == cudaSuccess;
+        if (!ok) raise(g_err, LIB, PGB_ERR_CUDA, "pgb6_hermite_create: start-up step failed");
+    }
+    if (ok && bad) {
+        raise(g_err, LIB, PGB_ERR_ARG, "pgb6_hermite_create: the start-up step of %d particles is below dtmax/2^51",
+              bad);
+        ok = false;
+        hm_free(H);
+        delete H;
+        return PGB_ERR_ARG;
+    }
+    if (!ok) {
+        hm_free(H);
+        delete H;
+        return PGB_ERR_CUDA;
+    }
+    *out = H;
+    return PGB_OK;
+}
+
+// One block step: the particles with the smallest t + dt advance to it.  *time (optional): the
+// global time after the step; *ni (optional): the number of particles advanced.
+PGB_EXPORT int pgb6_hermite_step(pgb6_hermite* H, double* time, int* ni) {
+    if (!H) {
+        raise(g_err, LIB, PGB_ERR_ARG, "pgb6_hermite_step: null integrator");
+        return PGB_ERR_ARG;
+    }
+    if (!ensure_device()) return PGB_ERR_NOGPU;
+    std::lock_guard<std::mutex> g(H->mu);
+    if (!hm_step(H, false)) return PGB_ERR_CUDA;
+    if (time) *time = H->t_mod * H->dtmax + H->t_gl;
+    if (ni) *ni = H->last_ni;
+    return PGB_OK;
+}
+
+// Block steps while the global time is below tend (banana01.c:146 loop condition).  *psteps /
+// *bsteps (optional): the particle steps and block steps this call took.
+PGB_EXPORT int pgb6_hermite_advance(pgb6_hermite* H, double tend, long long* psteps, long long* bsteps) {
+    if (!H) {
+        raise(g_err, LIB, PGB_ERR_ARG, "pgb6_hermite_advance: null integrator");
+        return PGB_ERR_ARG;
+    }
+    if (!ensure_device()) return PGB_ERR_NOGPU;
+    std::lock_guard<std::mutex> g(H->mu);
+    const long long p0 = H->psteps, b0 = H->bsteps;
+    while (H->t_mod * H->dtmax + H->t_gl < tend)
+        if (!hm_step(H, false)) return PGB_ERR_CUDA;
+    PGB_CUDA_OR(g_err, LIB, cudaStreamSynchronize(H->s), return PGB_ERR_CUDA);
+    if (psteps) *psteps = H->psteps - p0;
+    if (bsteps) *bsteps = H->bsteps - b0;
+    return PGB_OK;
+}
+
+PGB_EXPORT double pgb6_hermite_time(pgb6_hermite* H) { return H ? H->t_mod * H->dtmax + H->t_gl : 0.0; }
+
+// The particle state (any pointer may be NULL): t, dt, pos, vel, acc, jerk, pot as the
+// reference's struct Particle holds them (jerk and pot with float values).
+PGB_EXPORT int pgb6_hermite_get(pgb6_hermite* H, double* t, double* dt, double (*pos)[3], double (*vel)[3],
+                                double (*acc)[3], double (*jrk)[3], double* pot) {
+    if (!H) {
+        raise(g_err, LIB, PGB_ERR_ARG, "pgb6_hermite_get: null integrator");
+        return PGB_ERR_ARG;
+    }
+    if (!ensure_device()) return PGB_ERR_NOGPU;
+    std::lock_guard<std::mutex> g(H->mu);
+    if (!hm_apply_reset(H)) return PGB_ERR_CUDA;
+    const size_t n = (size_t)H->n;
+    struct {
+        void* dst;
+        const double* src;
+        size_t cnt;
+    } cp[7] = {{t, H->P.t, n},           {dt, H->P.dt, n},          {pos, H->P.pos, 3 * n}, {vel, H->P.vel, 3 * n},
+               {acc, H->P.acc, 3 * n},   {jrk, H->P.jrk, 3 * n},    {pot, H->P.pot, n}};
+    for (auto& c : cp)
+        if (c.dst)
+            PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(c.dst, c.src, c.cnt * sizeof(double), cudaMemcpyDeviceToHost, H->s),
+                        return PGB_ERR_CUDA);
+    PGB_CUDA_OR(g_err, LIB, cudaStreamSynchronize(H->s), return PGB_ERR_CUDA);
+    return PGB_OK;
+}
+
+// The last block step's active particles (index order) and the force, jerk and potential the
+// force kernel returned for them (before the corrector's rounding of jerk and pot to float).
+// Returns the number of active particles, or a negative error code.
+PGB_EXPORT int pgb6_hermite_last_step(pgb6_hermite* H, int* active, double (*acc)[3], double (*jrk)[3],
+                                      double* pot) {
+    if (!H) {
+        raise(g_err, LIB, PGB_ERR_ARG, "pgb6_hermite_last_step: null integrator");
+        return -PGB_ERR_ARG;
+    }
+    if (!ensure_device()) return -PGB_ERR_NOGPU;
+    std::lock_guard<std::mutex> g(H->mu);
+    const int ni = H->last_ni;
+    std::vector<G6Out> o((size_t)ni);
+    if (active)
+        PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(active, H->W.active, ni * sizeof(int), cudaMemcpyDeviceToHost, H->s),
+                    return -PGB_ERR_CUDA);
+    PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(o.data(), H->W.out, ni * sizeof(G6Out), cudaMemcpyDeviceToHost, H->s),
+                return -PGB_ERR_CUDA);
+    PGB_CUDA_OR(g_err, LIB, cudaStreamSynchronize(H->s), return -PGB_ERR_CUDA);
+    for (int k = 0; k < ni; k++) {
+        if (acc) {
+            acc[k][0] = o[k].ax;
+            acc[k][1] = o[k].ay;
+            acc[k][2] = o[k].az;
+        }
+        if (jrk) {
+            jrk[k][0] = o[k].jx;
+            jrk[k][1] = o[k].jy;
+            jrk[k][2] = o[k].jz;
+        }
+        if (pot) pot[k] = o[k].pot;
+    }
+    return ni;
+}
+
+// Kinetic and potential energy of the current state (calc_energy.c:9-33), FP64, fixed order.
+PGB_EXPORT int pgb6_hermite_energy(pgb6_hermite* H, double* ek, double* ew) {
+    if (!H) {
+        raise(g_err, LIB, PGB_ERR_ARG, "pgb6_hermite_energy: null integrator");
+        return PGB_ERR_ARG;
+    }
+    if (!ensure_device()) return PGB_ERR_NOGPU;
+    std::lock_guard<std::mutex> g(H->mu);
+    double e[2] = {0.0, 0.0};
+    hm_energy_kernel<<<1, 1024, 0, H->s>>>(H->P, H->energy);
+    PGB_CUDA_OR(g_err, LIB, cudaGetLastError(), return PGB_ERR_CUDA);
+    PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(e, H->energy, sizeof e, cudaMemcpyDeviceToHost, H->s), return PGB_ERR_CUDA);
+    PGB_CUDA_OR(g_err, LIB, cudaStreamSynchronize(H->s), return PGB_ERR_CUDA);
+    if (ek) *ek = e[0];
+    if (ew) *ew = e[1];
+    return PGB_OK;
+}
+
+// Particle and block steps since creation (the start-up step counts n and 1).
+PGB_EXPORT void pgb6_hermite_counts(pgb6_hermite* H, long long* psteps, long long* bsteps) {
+    if (psteps) *psteps = H ? H->psteps : 0;
+    if (bsteps) *bsteps = H ? H->bsteps : 0;
+}
+
+PGB_EXPORT void pgb6_hermite_destroy(pgb6_hermite* H) {
+    if (!H) return;
+    if (g_device >= 0) cudaSetDevice(g_device);
+    hm_free(H);
+    delete H;
 }

@@ -261,6 +261,16 @@ class G6(_ErrMixin):
         _sig(L, "pgb6_predict", [vp, C.c_int, C.c_double, vp, C.c_int, vp], C.c_int)
         _sig(L, "pgb6_batch_host", [C.c_int, ip, C.c_int, dp, dp, ip, C.c_int, dp, dp, dp, ip, C.c_double,
                                     dp, dp, dp, ip, fp], C.c_int)
+        _sig(L, "pgb6_hermite_create", [C.POINTER(vp), C.c_int, dp, dp, dp, C.c_double, C.c_double, C.c_double,
+                                        C.c_double], C.c_int)
+        _sig(L, "pgb6_hermite_step", [vp, dp, ip], C.c_int)
+        _sig(L, "pgb6_hermite_advance", [vp, C.c_double, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)], C.c_int)
+        _sig(L, "pgb6_hermite_time", [vp], C.c_double)
+        _sig(L, "pgb6_hermite_get", [vp, dp, dp, dp, dp, dp, dp, dp], C.c_int)
+        _sig(L, "pgb6_hermite_last_step", [vp, ip, dp, dp, dp], C.c_int)
+        _sig(L, "pgb6_hermite_energy", [vp, dp, dp], C.c_int)
+        _sig(L, "pgb6_hermite_counts", [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)])
+        _sig(L, "pgb6_hermite_destroy", [vp])
         sz = [C.c_int() for _ in range(4)]
         L.pgb6_record_sizes(*[C.byref(s) for s in sz])
         self.sizes = dict(ptcl=sz[0].value, predj=sz[1].value, irec=sz[2].value, out=sz[3].value)
@@ -510,6 +520,78 @@ class G5Table(_ErrMixin):
 
     def plan_destroy(self, plan):
         self.L.pgb5_plan_destroy(plan)
+
+
+class Hermite:
+    """The device Hermite block-time-step integrator (pgb6_hermite_*) over numpy arrays."""
+
+    def __init__(self, g6: "G6", mass, pos, vel, eps2, eta, eta_s, dtmax):
+        self.g6, self.L = g6, g6.L
+        mass, pos, vel = f64(mass), f64(pos, (-1, 3)), f64(vel, (-1, 3))
+        self.n = len(mass)
+        h = vp()
+        rc = self.L.pgb6_hermite_create(C.byref(h), self.n, ptr(mass), ptr(pos), ptr(vel), eps2, eta, eta_s, dtmax)
+        if rc:
+            raise RuntimeError(f"pgb6_hermite_create failed ({rc}): {g6.last_error()}")
+        self.h = h
+
+    def _check(self, rc, what):
+        if rc:
+            raise RuntimeError(f"pgb6_hermite_{what} failed ({rc}): {self.g6.last_error()}")
+
+    def step(self):
+        """One block step; (global time after it, particles advanced)."""
+        t, ni = C.c_double(), C.c_int()
+        self._check(self.L.pgb6_hermite_step(self.h, C.byref(t), C.byref(ni)), "step")
+        return t.value, ni.value
+
+    def advance(self, tend):
+        """Block steps while the time is below tend; (particle steps, block steps) taken."""
+        p, b = C.c_longlong(), C.c_longlong()
+        self._check(self.L.pgb6_hermite_advance(self.h, tend, C.byref(p), C.byref(b)), "advance")
+        return p.value, b.value
+
+    @property
+    def time(self):
+        return self.L.pgb6_hermite_time(self.h)
+
+    def get(self):
+        n = self.n
+        st = dict(t=np.zeros(n), dt=np.zeros(n), pos=np.zeros((n, 3)), vel=np.zeros((n, 3)),
+                  acc=np.zeros((n, 3)), jrk=np.zeros((n, 3)), pot=np.zeros(n))
+        self._check(self.L.pgb6_hermite_get(self.h, *(ptr(st[k]) for k in ("t", "dt", "pos", "vel", "acc", "jrk",
+                                                                             "pot"))), "get")
+        return st
+
+    def last_step(self):
+        n = self.n
+        act = np.zeros(n, np.int32)
+        acc, jrk, pot = np.zeros((n, 3)), np.zeros((n, 3)), np.zeros(n)
+        ni = self.L.pgb6_hermite_last_step(self.h, ptr(act, C.c_int), ptr(acc), ptr(jrk), ptr(pot))
+        if ni < 0:
+            raise RuntimeError(f"pgb6_hermite_last_step failed ({ni}): {self.g6.last_error()}")
+        return act[:ni], acc[:ni], jrk[:ni], pot[:ni]
+
+    def energy(self):
+        ek, ew = C.c_double(), C.c_double()
+        self._check(self.L.pgb6_hermite_energy(self.h, C.byref(ek), C.byref(ew)), "energy")
+        return ek.value, ew.value
+
+    def counts(self):
+        p, b = C.c_longlong(), C.c_longlong()
+        self.L.pgb6_hermite_counts(self.h, C.byref(p), C.byref(b))
+        return p.value, b.value
+
+    def close(self):
+        if self.h:
+            self.L.pgb6_hermite_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def bind_noalloc(g6: "G6"):
