@@ -1076,9 +1076,216 @@ def run_bh(args, pgb, ws, rank, local):
 # ----------------------------------------------------------------------------------------
 # reference arm
 
+INT_PARAMS = dict(epsinv=0.0, eta=0.2, eta_s=0.01, dtstarinv=8.0)   # PG6/banana/input.list defaults
+
+
+def integrator_ics(pgb, n, rank=0):
+    """Initial conditions of the integrator workload: a seeded Plummer sphere in Henon units (the
+    units and shape of the reference's own PG6/banana/init/pl016k.init), equal masses 1/n."""
+    W = pgb.workloads
+    return W.plummer_henon(n, W.SEED0 + 31 + rank)
+
+
+def write_banana_init(path, m, x, v):
+    """The reference integrator's input format (PG6/banana/io.c:18-26): time, n, then per
+    particle: index, mass, position, velocity."""
+    with open(path, "w") as f:
+        f.write(f"0.0\n{len(m)}\n")
+        for i in range(len(m)):
+            f.write(f"{i + 1}\n{m[i]:.17g}\n{x[i, 0]:.17g} {x[i, 1]:.17g} {x[i, 2]:.17g}\n"
+                    f"{v[i, 0]:.17g} {v[i, 1]:.17g} {v[i, 2]:.17g}\n")
+
+
+def run_banana(path, m, x, v, intervals, threads=None):
+    """Run the reference's own Hermite integrator (oracle/_ref/banana01, PG6/banana built from its
+    sources with -DNORMAL) from t = 0 for `intervals` output intervals of 1/8.  Returns the wall
+    time of each interval (host clock at the arrival of its output line; line-buffered stdout),
+    the particle steps and block steps of each, the energies, and the start-up time."""
+    import re
+    dts = 1.0 / INT_PARAMS["dtstarinv"]
+    with tempfile.TemporaryDirectory() as d:
+        init = os.path.join(d, "ics.init")
+        write_banana_init(init, m, x, v)
+        with open(os.path.join(d, "input.list"), "w") as f:
+            f.write(f"0 {intervals * dts} 1000000\n{INT_PARAMS['epsinv']}\n"
+                    f"{INT_PARAMS['eta']} {INT_PARAMS['eta_s']} {INT_PARAMS['dtstarinv']}\n{init}\nsnap\n")
+        env = dict(os.environ)
+        if threads:
+            env["OMP_NUM_THREADS"] = str(threads)
+        cmd = ([ "stdbuf", "-oL"] if subprocess.run(["which", "stdbuf"], capture_output=True).returncode == 0
+               else []) + [path]
+        t0 = time.perf_counter()
+        proc = subprocess.Popen(cmd, cwd=d, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True, env=env)
+        stamps, lines = [], []
+        for line in proc.stdout:
+            lines.append(line)
+            if line.startswith("Time:"):
+                stamps.append(time.perf_counter() - t0)
+        proc.wait()
+        if proc.returncode != 0:
+            raise RuntimeError(f"banana01 exited {proc.returncode}: {proc.stderr.read()[-500:]}")
+    out = "".join(lines)
+    st = re.findall(r"niave: ([0-9.e+-]+) ([0-9.e+-]+)", out)
+    steps = [float(b) for _, b in st]
+    blocks = [round(float(b) / float(a)) if float(a) > 0 else 0 for a, b in st]
+    en = [float(e) for e in re.findall(r"^tot: ([-+0-9.]+)", out, re.M)]
+    times = np.diff(stamps).tolist()
+    return dict(times=times, steps=steps[1:], blocks=blocks[1:], energies=en, startup=stamps[0] if stamps else None,
+                threads=threads or os.cpu_count())
+
+
+def run_integrator(args, pgb, ws, rank, local):
+    """PG6 Hermite block-time-step integration on the device (pgb6_hermite_*): the reference
+    sample integrator's run (PG6/banana with its input.list: eps = 0, eta = 0.2, eta_s = 0.01,
+    dtstar = 1/8) of an N = 16384 Plummer sphere; one step = one output interval of 1/8."""
+    import torch
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    ffi = pgb.ffi
+    g6 = ffi.G6()
+    g6.L.g6_open(0)
+    n = args.int_n
+    x, v, m = integrator_ics(pgb, n, rank)
+    eps2 = 0.0 if INT_PARAMS["epsinv"] == 0 else 1.0 / INT_PARAMS["epsinv"] ** 2
+    dts = 1.0 / INT_PARAMS["dtstarinv"]
+    H = ffi.Hermite(g6, m, x, v, eps2, INT_PARAMS["eta"], INT_PARAMS["eta_s"], dts)
+    if args.profile_largest:
+        # profiling target: the start-up step and two intervals of 1/8 (one launch each); no timing
+        H.advance(dts)
+        H.advance(2 * dts)
+        torch.cuda.synchronize()
+        H.close()
+        return {"profile": "integrator launches", "n": n, "launches": 3}
+    ek0, ew0 = H.energy()
+    s = torch.cuda.ExternalStream(H.stream, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    for k in range(args.warmup):
+        H.advance((k + 1) * dts)
+    torch.cuda.synchronize()
+    fp0, tiles0 = H.stats()
+    clocks = ClockSampler(local)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    clocks.start()
+    barrier(ws)
+    torch.cuda.synchronize()
+    psteps = blocks = 0
+    for k in range(args.steps):
+        ev[k][0].record(s)
+        p_, b_ = H.advance((args.warmup + k + 1) * dts)
+        ev[k][1].record(s)
+        with torch.cuda.stream(s):
+            flush.fill_(k & 0xFF)   # 256 MiB write between steps: L2 (126 MB) flushed
+        psteps += p_
+        blocks += b_
+    torch.cuda.synchronize()
+    barrier(ws)
+    clk = clocks.stop()
+    t_local = sum(a.elapsed_time(b) for a, b in ev) / 1e3
+    t_max = reduce_max(t_local, ws, dev)
+    value = reduce_sum(float(psteps) * n, ws, dev) / t_max / 1e9
+    fp1, tiles1 = H.stats()
+    force_pairs = fp1 - fp0
+    tiles = [b - a for a, b in zip(tiles0, tiles1)]
+    ek, ew = H.energy()
+    de = ((ek + ew) - (ek0 + ew0)) / abs(ek0 + ew0)
+    H.close()
+
+    # end to end through the C ABI with host buffers: create (upload + start-up step), the same
+    # number of intervals from t = 0, the final state back to the host
+    e2e_int = max(1, min(args.steps, args.e2e_steps))
+    torch.cuda.synchronize()
+    barrier(ws)
+    t0 = time.perf_counter()
+    H2 = ffi.Hermite(g6, m, x, v, eps2, INT_PARAMS["eta"], INT_PARAMS["eta_s"], dts)
+    H2.advance(e2e_int * dts)
+    st2 = H2.get()
+    e2e_t = time.perf_counter() - t0
+    p2, b2 = H2.counts()
+    H2.close()
+    e2e_val = reduce_sum(float(p2) * n, ws, dev) / reduce_max(e2e_t, ws, dev) / 1e9
+
+    pk = peaks()
+    sm_mhz = clk.get("sm_mhz") or pk.get("sm_max_mhz", 1965.0)
+    fp32_peak_tf = SM_COUNT * FP32_LANES * 2 * sm_mhz * 1e6 / 1e12
+    # the whole step runs in one persistent kernel: its roofline is the pair arithmetic over the
+    # kernel's CUDA-event time (selection, prediction and corrector included)
+    achieved_tf = force_pairs * 60 / t_local / 1e12
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        path = ref_lib("banana01")
+        if path is None:
+            cpu = {"value": None, "unit": "Gint/s", "cores": os.cpu_count(), "kind": "reference",
+                   "sample": "unavailable: oracle/_ref/banana01 not built"}
+        else:
+            r = run_banana(path, m, x, v, 2)
+            cpu = {"value": round(sum(r["steps"]) * n / sum(r["times"]) / 1e9, 3), "unit": "Gint/s",
+                   "cores": r["threads"], "kind": "reference",
+                   "sample": f"the first 2 intervals (t = 0 to 1/4: {int(sum(r['steps']))} particle steps, "
+                             f"{sum(r['blocks'])} block steps, {sum(r['times']):.2f} s), PG6/banana with libpg6 "
+                             "AVX2 + OpenMP built from the reference's sources",
+                   "energies": r["energies"]}
+    line = {
+        "metric": "Gint/s (PG6 Hermite block-time-step integration: particle steps x N per second)",
+        "value": round(value, 2), "unit": "Gint/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(t_max / args.steps * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 integrator, f32 force (double-float x_j-x_i, f64 sums)",
+        "data": "synthetic (seeded Plummer in Henon units; no dataset)",
+        "config": {"workload": f"PG6 Hermite integration N={n} Plummer, eps=0, eta=0.2, eta_s=0.01, dtstar=1/8 "
+                               "(PG6/banana input.list); one step = one interval of 1/8",
+                   "particle_steps": psteps, "block_steps": blocks, "interactions": psteps * n,
+                   "l2": "flushed between steps (256 MiB write)",
+                   "parallelism": f"replicas x{ws} (independent systems, no data-path collective)",
+                   "energy_error": de, "time": (args.warmup + args.steps) * dts},
+        "roofline": {"bound": "fp32", "achieved": round(achieved_tf, 2), "peak": round(fp32_peak_tf, 2),
+                     "unit": "TFLOP/s", "frac": round(achieved_tf / fp32_peak_tf, 4), "traffic": None,
+                     "kernel": f"pgb::hm_run_kernel (one cooperative launch per interval: selection, prediction, "
+                               f"force, corrector), {force_pairs:.3e} pairs in {t_local * 1e3:.2f} ms, 60 flop per "
+                               "pair; block steps by force i-tile 16/32/64/128/512: " + "/".join(map(str, tiles)),
+                     "peak_source": f"148 SM x 128 FP32 lanes x 2 x median SM clock {sm_mhz:.0f} MHz"},
+        "e2e": {"value": round(e2e_val, 2), "unit": "Gint/s",
+                "h2d_bytes_per_step": int(n * 56 / e2e_int), "d2h_bytes_per_step": int(n * 136 / e2e_int),
+                "api": "pgb6_hermite_create (upload + start-up step) + pgb6_hermite_advance + "
+                       "pgb6_hermite_get, host buffers, host clock", "steps": e2e_int,
+                "particle_steps": p2, "block_steps": b2},
+        "gpu_launches": args.steps,   # one cooperative launch of pgb::hm_run_kernel per interval
+        "clocks": clk,
+        "cpu_baseline": cpu,
+    }
+    return line
+
+
+def run_reference_integrator(args, pgb, ws, rank):
+    path = ref_lib("banana01")
+    if path is None:
+        return {"impl": "reference", "unavailable": "oracle/_ref/banana01 (the reference integrator) not built"}
+    n = args.int_n
+    x, v, m = integrator_ics(pgb, n)
+    r = run_banana(path, m, x, v, args.warmup + args.steps)
+    times = r["times"][args.warmup:]
+    steps = r["steps"][args.warmup:]
+    val = sum(steps) * n / sum(times) / 1e9
+    return {
+        "metric": "Gint/s (PG6 Hermite block-time-step integration: particle steps x N per second)",
+        "value": round(val, 3), "unit": "Gint/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(sum(times) / len(times) * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 integrator, f32 force", "data": "synthetic",
+        "config": {"workload": f"PG6 Hermite integration N={n} Plummer, eps=0, eta=0.2, eta_s=0.01, dtstar=1/8 "
+                               "(PG6/banana input.list); one step = one interval of 1/8",
+                   "particle_steps": int(sum(steps)), "block_steps": int(sum(r["blocks"][args.warmup:]))},
+        "impl": "reference",
+        "cpu_baseline": {"value": round(val, 3), "unit": "Gint/s", "cores": r["threads"], "kind": "reference",
+                         "sample": f"intervals {args.warmup + 1}-{args.warmup + args.steps} of the run "
+                                   "(PG6/banana banana01 + libpg6 AVX2 + OpenMP, built from the reference's "
+                                   "sources; per-interval host time at its output lines)"},
+        "e2e": {"value": round(val, 3), "unit": "Gint/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
 def run_reference(args, pgb, ws, rank):
     if rank != 0:
         return None
+    if args.workload == "integrator":
+        return run_reference_integrator(args, pgb, ws, rank)
     path = ref_lib("libpg6_ref.so")
     if path is None:
         return {"impl": "reference", "unavailable": "reference library (oracle/_ref/libpg6_ref.so) not built"}
@@ -1134,7 +1341,9 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["hermite", "direct", "clusters", "treepm", "bh"], default="hermite")
+    ap.add_argument("--workload", choices=["hermite", "direct", "clusters", "treepm", "bh", "integrator"],
+                    default="hermite")
+    ap.add_argument("--int-n", type=int, default=16384, help="particles of the integrator workload")
     ap.add_argument("--bh-n", type=int, default=1 << 22, help="particles of the Barnes-Hut workload")
     ap.add_argument("--no-errors", action="store_true", help="bh: skip the FP64 error report")
     ap.add_argument("--e2e-steps", type=int, default=3)
@@ -1160,7 +1369,7 @@ def main():
         return
     dist = dist_init(ws, local)
     runner = {"hermite": run_hermite, "direct": run_direct, "clusters": run_clusters, "treepm": run_treepm,
-              "bh": run_bh}
+              "bh": run_bh, "integrator": run_integrator}
     line = runner[args.workload](args, pgb, ws, rank, local)
     if rank == 0:
         print(json.dumps(line), flush=True)

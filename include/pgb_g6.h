@@ -145,8 +145,8 @@ int  pgb6_force_noalloc(const void *ipart, int ni, const void *jpred, int nj, do
  * plain FP64 bit for bit.  The force is the GRAPE-6 kernel of this library (eps2, id-excluded
  * self pair).                                                                                  */
 typedef struct pgb6_hermite pgb6_hermite;
-/* n >= 2 particles; takes the start-up step (forces at t = 0, first steps); PGB_ERR_ARG when a
- * start-up step falls below dtmax / 2^51 */
+/* 2 <= n <= 2^20 particles; takes the start-up step (forces at t = 0, first steps); PGB_ERR_ARG
+ * when a start-up step falls below dtmax / 2^51 */
 int  pgb6_hermite_create(pgb6_hermite **h, int n, const double *mass, const double (*pos)[3],
                          const double (*vel)[3], double eps2, double eta, double eta_s, double dtmax);
 /* one block step; *time = global time after it, *ni = particles advanced (both optional) */
@@ -163,6 +163,11 @@ int  pgb6_hermite_last_step(pgb6_hermite *h, int *active, double (*acc)[3], doub
 int  pgb6_hermite_energy(pgb6_hermite *h, double *ek, double *ew);
 /* particle and block steps since creation (the start-up step counts n and 1) */
 void pgb6_hermite_counts(pgb6_hermite *h, long long *psteps, long long *bsteps);
+/* the integrator's CUDA stream (cudaStream_t) */
+void *pgb6_hermite_stream(pgb6_hermite *h);
+/* pair interactions so far (active x n) and steps by force decomposition (i-tile 16, 32, 64,
+ * 128, 512); any pointer may be NULL */
+void pgb6_hermite_stats(pgb6_hermite *h, long long *pairs, long long *steps_by_tile);
 void pgb6_hermite_destroy(pgb6_hermite *h);
 
 #ifdef __cplusplus

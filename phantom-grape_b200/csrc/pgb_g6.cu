@@ -1275,117 +1275,41 @@ PGB_EXPORT int pgb6_force_noalloc(const void* ipart, int ni, const void* jpred, 
 // ------------------------------------------------------------------------------------------
 // Hermite block-time-step integrator on the device (pgb_hermite.cuh): the reference's sample
 // integrator PG6/banana (hermite.c, timestep.c; banana01.c:96-183 main loop) with the particle
-// state, the j-memory and the per-step bookkeeping resident in HBM.  The host only learns each
-// step's active count (to size the force launch) through mapped memory.
-
-namespace {
-
-// Force of ni device-resident i-records against nj predicted j-records into out[0, ni): the
-// small-call cluster kernel up to G6_SMALL_MAXI i-particles, else the general kernel in regular
-// mode (tasks derived in the kernel, self-resetting counters: nothing uploaded).
-struct ForceScratch {
-    DevBuf<int> tcount;     // task counter of the regular launches
-    DevBuf<int> pcnt;       // slice counters of the small launches
-    DevBuf<G6Out> spart;    // cluster rows of the small launches
-    Stager<G6I, G6Out> st;  // partial rows and group counters of the regular launches
-    void release() {
-        tcount.release();
-        pcnt.release();
-        spart.release();
-        st.release();
-    }
-};
-
-bool force_device(ForceScratch& F, cudaStream_t s, const G6I* irec, int ni, const G6PredJ* jpred, int nj, float eps2,
-                  G6Out* out) {
-    if (ni <= 0 || nj <= 0) return true;
-    const bool ff = dx_ff();
-    if (ni <= G6_SMALL_MAXI) {
-        const SmallShape sh = small_shape(ni);
-        int grid = 1, cl = 1;
-        small_grid(sh, ff, false, false, nj, grid, cl);
-        PGB_CUDA_OR(g_err, LIB, F.spart.reserve((size_t)(grid / cl) * sh.isl), return false);
-        if (!F.pcnt.p) {
-            PGB_CUDA_OR(g_err, LIB, F.pcnt.reserve(SMALL_CL), return false);
-            PGB_CUDA_OR(g_err, LIB, F.pcnt.zero_fill(s), return false);
-        }
-        G6SmallArgs a{};
-        a.jpred = jpred;
-        a.eps2 = eps2;
-        a.ni = ni;
-        a.nj = nj;
-        a.partial = F.spart.p;
-        a.counter = F.pcnt.p;
-        a.out = out;
-        a.nb_maxlen = nbmax();
-        a.done = nullptr;
-        a.irec = irec;
-        static const G6IBlock unused{};
-        PGB_CUDA_OR(g_err, LIB, small_kernel(sh, ff, false, false, grid, cl, a, unused, s, nullptr), return false);
-        return true;
-    }
-    const int cfg = pick_cfg(ni);
-    const int itile = cfg_itile(cfg);
-    const int slots = sm_count(g_device) * occupancy(cfg, ff, false, false);
-    static const int maxch = env_int("PGB_G6_MAXCHUNKS", 512, 1, 4096);
-    const int itiles = (ni + itile - 1) / itile;
-    int nch = best_nch(itiles, nj, slots, maxch);
-    if (nch > nj) nch = nj;
-    const int rows = nch > 1 ? itiles * nch : 0;
-    PGB_CUDA_OR(g_err, LIB, F.st.reserve_scratch(s, rows, ITILE_MAX, (size_t)itiles), return false);
-    if (!F.tcount.p) {
-        PGB_CUDA_OR(g_err, LIB, F.tcount.reserve(1), return false);
-        PGB_CUDA_OR(g_err, LIB, F.tcount.zero_fill(s), return false);
-    }
-    G6Args a;
-    a.ipart = irec;
-    a.jpred = jpred;
-    a.eps2 = eps2;
-    a.tasks = nullptr;
-    a.ntasks = itiles * nch;
-    a.task_counter = F.tcount.p;
-    a.groups = nullptr;
-    a.group_counters = F.st.dgcnt.p;
-    a.partial = F.st.dpart.p;
-    a.out = out;
-    a.itile = itile;
-    a.bundle_counters = F.st.bundle_counters();
-    a.nb_count = nullptr;
-    a.nb_list = nullptr;
-    a.nb_maxlen = 0;
-    a.reg_ni = ni;
-    a.reg_nj = nj;
-    a.reg_nch = nch;
-    const int grid = a.ntasks < slots ? a.ntasks : slots;
-    PGB_CUDA_OR(g_err, LIB, launch_kernel(cfg, ff, false, false, grid, a, s), return false);
-    return true;
-}
-
-size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
-}  // namespace
+// state, the j-memory and the per-step bookkeeping resident in HBM.  One cooperative launch
+// runs block steps until the global time reaches the caller's tend: the host launches once per
+// call and reads the clock back.
 
 struct pgb6_hermite {
     std::mutex mu;
-    int n = 0, nseg = 0;
+    int n = 0, nseg = 0, grid = 0;
     double eps2 = 0.0, eta = 0.0, eta_s = 0.0, dtmax = 0.0;
     bool ff = true;
     cudaStream_t s = nullptr;
     DevBuf<double> state;          // t, dt, pot, mass [n]; pos, vel, acc, jrk [n][3]
     DevBuf<unsigned char> work;    // HmWork's arrays
-    HostBuf<HmHostCtl> ctl;        // mapped: (seq, ni, t_gl) of the step in flight
     HmState P{};
     HmWork W{};
     double* energy = nullptr;      // [2] device
-    ForceScratch F;
-    unsigned seq = 0;
-    int t_mod = 0;                 // completed dtmax intervals
-    double t_gl = 0.0;             // block time within the current interval
-    bool reset_pending = false;    // reset_time due before the next step
-    long long psteps = 0, bsteps = 0;
-    int last_ni = 0;
+    HmClock clk{};                 // the device clock as of the last synchronisation
 };
 
 namespace {
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// Co-resident CTAs of the persistent kernel (its cooperative grid).
+int hm_grid(bool ff) {
+    static int cache[2] = {0, 0};
+    int& g = cache[ff ? 1 : 0];
+    if (!g) {
+        int per = 0;
+        cudaError_t e = ff ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, hm_run_kernel<true>, HM_NT, 0)
+                           : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, hm_run_kernel<false>, HM_NT, 0);
+        if (e != cudaSuccess || per < 1) per = 1;
+        g = per * sm_count(g_device);
+    }
+    return g;
+}
 
 bool hm_alloc(pgb6_hermite* H) {
     const size_t n = (size_t)H->n;
@@ -1401,13 +1325,26 @@ bool hm_alloc(pgb6_hermite* H) {
     H->P.acc = b + 10 * n;
     H->P.jrk = b + 13 * n;
     H->nseg = (int)((n + HM_SEG - 1) / HM_SEG);
+    H->grid = hm_grid(H->ff);
+    // partial rows: at most (grid + i-tiles) rows of at most 512 entries; force tasks: at most
+    // grid + i-tiles of at least 16
+    const long long part_cap = (long long)H->grid * 512 + (long long)n + 512;
+    const int task_cap = H->grid + (int)(n / 16) + 2;
     size_t off = 0;
     const size_t o_hdr = off;
-    off = align256(off + 64);
+    off = align256(off + sizeof(HmClock));
+    const size_t o_sync = off;
+    off = align256(off + sizeof(HmSync) + sizeof(unsigned) * (size_t)H->grid * HM_ARRIVE_STRIDE);
+    const size_t o_gmin = off;
+    off = align256(off + 3 * sizeof(unsigned long long));
+    const size_t o_bmin = off;
+    off = align256(off + sizeof(unsigned long long) * 2 * H->nseg);
     const size_t o_bcnt = off;
-    off = align256(off + sizeof(int) * H->nseg);
-    const size_t o_boff = off;
-    off = align256(off + sizeof(int) * H->nseg);
+    off = align256(off + sizeof(int) * 2 * H->nseg);
+    const size_t o_sflag = off;
+    off = align256(off + sizeof(unsigned) * H->nseg);
+    const size_t o_tflag = off;
+    off = align256(off + sizeof(unsigned) * (size_t)task_cap);
     const size_t o_act = off;
     off = align256(off + sizeof(int) * n);
     const size_t o_irec = off;
@@ -1416,112 +1353,88 @@ bool hm_alloc(pgb6_hermite* H) {
     off = align256(off + sizeof(G6PredJ) * n);
     const size_t o_out = off;
     off = align256(off + sizeof(G6Out) * n);
+    const size_t o_part = off;
+    off = align256(off + sizeof(G6Out) * (size_t)part_cap);
     const size_t o_en = off;
     off = align256(off + 2 * sizeof(double));
     PGB_CUDA_OR(g_err, LIB, H->work.reserve(off), return false);
     unsigned char* w = H->work.p;
-    H->W.tmin = (unsigned long long*)(w + o_hdr);
-    H->W.t_gl = (double*)(w + o_hdr + 8);
-    H->W.ticket = (int*)(w + o_hdr + 16);
-    H->W.ni = (int*)(w + o_hdr + 20);
-    H->W.bad = (int*)(w + o_hdr + 24);
+    H->W.clk = (HmClock*)(w + o_hdr);
+    H->W.sync = (HmSync*)(w + o_sync);
+    H->W.gmin = (unsigned long long*)(w + o_gmin);
+    H->W.bmin = (unsigned long long*)(w + o_bmin);
     H->W.bcnt = (int*)(w + o_bcnt);
-    H->W.boff = (int*)(w + o_boff);
+    H->W.seg_flag = (unsigned*)(w + o_sflag);
+    H->W.task_flag = (unsigned*)(w + o_tflag);
+    H->W.task_cap = task_cap;
     H->W.active = (int*)(w + o_act);
     H->W.irec = (G6I*)(w + o_irec);
     H->W.jpred = (G6PredJ*)(w + o_jpred);
     H->W.out = (G6Out*)(w + o_out);
+    H->W.partial = (G6Out*)(w + o_part);
+    H->W.part_cap = part_cap;
     H->energy = (double*)(w + o_en);
-    PGB_CUDA_OR(g_err, LIB, H->ctl.reserve(1, false, cudaHostAllocPortable | cudaHostAllocMapped), return false);
-    std::memset((void*)H->ctl.p, 0, sizeof(HmHostCtl));
-    PGB_CUDA_OR(g_err, LIB, cudaHostGetDevicePointer((void**)&H->W.host, H->ctl.p, 0), return false);
-    // header: tmin all ones, ticket / ni / bad zero
-    PGB_CUDA_OR(g_err, LIB, cudaMemsetAsync(w + o_hdr, 0, 64, H->s), return false);
-    PGB_CUDA_OR(g_err, LIB, cudaMemsetAsync(w + o_hdr, 0xff, 8, H->s), return false);
+    // clock, barrier and flags zero; the step numbers that tag the flags start at 1
+    PGB_CUDA_OR(g_err, LIB, cudaMemsetAsync(w, 0, o_act, H->s), return false);
+    const unsigned first_step = 1;
+    PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(&H->W.sync->step, &first_step, sizeof first_step, cudaMemcpyHostToDevice,
+                                            H->s), return false);
+    PGB_CUDA_OR(g_err, LIB, cudaStreamSynchronize(H->s), return false);
     return true;
 }
 
-// The step's selection kernels; hm_count_kernel publishes (ni, t_gl) with sequence number seq.
-bool hm_select(pgb6_hermite* H) {
-    const int reset = H->reset_pending ? 1 : 0;
-    H->reset_pending = false;
-    hm_tmin_kernel<<<H->nseg, HM_NT, 0, H->s>>>(H->P, H->W, reset);
-    if (++H->seq == 0) H->seq = 1;
-    hm_count_kernel<<<H->nseg, HM_NT, 0, H->s>>>(H->P, H->W, H->seq);
-    hm_build_kernel<<<H->nseg, HM_NT, 0, H->s>>>(H->P, H->W, H->ff);
-    PGB_CUDA_OR(g_err, LIB, cudaGetLastError(), return false);
-    return true;
-}
-
-// Wait for the published (ni, t_gl): a bounded spin on the mapped sequence number, then the
-// stream synchronisation that reports a failed launch.
-bool hm_wait(pgb6_hermite* H, int* ni, double* tg) {
-    volatile HmHostCtl* c = H->ctl.p;
-    auto t0 = std::chrono::steady_clock::now();
-    for (long it = 0;; it++) {
-        if (c->seq == H->seq) break;
-        if ((it & 1023) == 1023 && std::chrono::steady_clock::now() - t0 > std::chrono::seconds(5)) {
-            PGB_CUDA_OR(g_err, LIB, cudaStreamSynchronize(H->s), return false);
-            if (c->seq != H->seq) {
-                raise(g_err, LIB, PGB_ERR_DEVICE, "hermite: block selection did not publish its result");
-                return false;
-            }
-            break;
-        }
-    }
-    std::atomic_thread_fence(std::memory_order_acquire);
-    *ni = c->ni;
-    *tg = c->t_gl;
-    return true;
-}
-
-// One block step (startup: the first, every particle active at t = 0).
-bool hm_step(pgb6_hermite* H, bool startup) {
-    if (!hm_select(H)) return false;
-    int ni = 0;
-    double tg = 0.0;
-    if (!hm_wait(H, &ni, &tg)) return false;
-    if (ni <= 0 || ni > H->n) {
-        raise(g_err, LIB, PGB_ERR_DEVICE, "hermite: block selection returned %d active particles", ni);
+// Wait for the stream and read the device clock; a barrier that gave up is an error.
+bool hm_sync_clock(pgb6_hermite* H) {
+    PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(&H->clk, H->W.clk, sizeof(HmClock), cudaMemcpyDeviceToHost, H->s),
+                return false);
+    PGB_CUDA_OR(g_err, LIB, cudaStreamSynchronize(H->s), return false);
+    if (H->clk.err) {
+        raise(g_err, LIB, PGB_ERR_DEVICE, "hermite: a grid barrier of the step kernel timed out");
         return false;
     }
-    if (!force_device(H->F, H->s, H->W.irec, ni, H->W.jpred, H->n, (float)H->eps2, H->W.out)) return false;
-    const int nb = (ni + 127) / 128;
-    if (startup) hm_startup_kernel<<<nb, 128, 0, H->s>>>(H->P, H->W, ni, H->eta_s, H->dtmax);
-    else hm_correct_kernel<<<nb, 128, 0, H->s>>>(H->P, H->W, ni, H->eta, H->dtmax);
-    PGB_CUDA_OR(g_err, LIB, cudaGetLastError(), return false);
-    H->psteps += ni;
-    H->bsteps += 1;
-    H->last_ni = ni;
-    if (!startup) {
-        // banana01.c:161-179: after a step that ends on a multiple of dtmax the times restart
-        H->t_gl = tg;
-        if (tg - (double)(int)(tg * (1.0 / H->dtmax)) * H->dtmax == 0.0) {
-            H->t_mod += 1;
-            H->t_gl = 0.0;
-            H->reset_pending = true;
-        }
-    }
+    return true;
+}
+
+// One cooperative launch: the start-up step, or block steps while the time is below tend (at
+// most max_steps).
+bool hm_launch(pgb6_hermite* H, bool startup, double tend, int max_steps) {
+    HmRun R;
+    R.P = H->P;
+    R.W = H->W;
+    R.eps2 = (float)H->eps2;
+    R.eta = H->eta;
+    R.eta_s = H->eta_s;
+    R.dtmax = H->dtmax;
+    R.tend = tend;
+    R.startup = startup ? 1 : 0;
+    R.max_steps = max_steps;
+    R.nseg = H->nseg;
+    static const int minj = env_int("PGB_HM_MINJ", 128, 16, 1 << 20);
+    R.minj = minj;
+    void* args[] = {&R};
+    const void* fn = H->ff ? (const void*)hm_run_kernel<true> : (const void*)hm_run_kernel<false>;
+    PGB_CUDA_OR(g_err, LIB, cudaLaunchCooperativeKernel(fn, dim3(H->grid), dim3(HM_NT), args, 0, H->s),
+                return false);
     return true;
 }
 
 bool hm_apply_reset(pgb6_hermite* H) {
-    if (!H->reset_pending) return true;
-    H->reset_pending = false;
-    hm_reset_kernel<<<(H->n + 255) / 256, 256, 0, H->s>>>(H->P);
+    if (!H->clk.reset) return true;
+    hm_reset_kernel<<<(H->n + 255) / 256, 256, 0, H->s>>>(H->P, H->W.clk);
     PGB_CUDA_OR(g_err, LIB, cudaGetLastError(), return false);
+    H->clk.reset = 0;
     return true;
 }
 
 void hm_free(pgb6_hermite* H) {
     if (H->s) cudaStreamSynchronize(H->s);
-    H->F.release();
     H->state.release();
     H->work.release();
-    H->ctl.release();
     if (H->s) cudaStreamDestroy(H->s);
     H->s = nullptr;
 }
+
+constexpr int HM_STEPS_PER_LAUNCH = 1 << 16;
 }  // namespace
 
 // Create an integrator for n particles (n >= 2) and take its start-up step: every particle's
@@ -1530,7 +1443,7 @@ void hm_free(pgb6_hermite* H) {
 // interval after which the times restart from 0 (the reference's dtstar).
 PGB_EXPORT int pgb6_hermite_create(pgb6_hermite** out, int n, const double* mass, const double (*pos)[3],
                                    const double (*vel)[3], double eps2, double eta, double eta_s, double dtmax) {
-    if (!out || n < 2 || n > (1 << 26) || !mass || !pos || !vel || !(eps2 >= 0.0) || !(eta > 0.0) ||
+    if (!out || n < 2 || n > HM_MAXSEG * HM_SEG || !mass || !pos || !vel || !(eps2 >= 0.0) || !(eta > 0.0) ||
         !(eta_s > 0.0) || !(dtmax > 0.0)) {
         raise(g_err, LIB, PGB_ERR_ARG, "pgb6_hermite_create: bad arguments (n %d, eps2 %g, eta %g, eta_s %g, dtmax %g)",
               n, eps2, eta, eta_s, dtmax);
@@ -1557,17 +1470,11 @@ PGB_EXPORT int pgb6_hermite_create(pgb6_hermite** out, int n, const double* mass
              cudaMemcpyAsync(H->P.vel, vel, 3 * nn * sizeof(double), cudaMemcpyHostToDevice, H->s) == cudaSuccess;
         if (!ok) raise(g_err, LIB, PGB_ERR_CUDA, "pgb6_hermite_create: upload failed");
     }
-    ok = ok && hm_step(H, true);
-    int bad = 0;
-    if (ok) {
-        ok = cudaMemcpyAsync(&bad, H->W.bad, sizeof(int), cudaMemcpyDeviceToHost, H->s) == cudaSuccess &&
-             cudaStreamSynchronize(H->s) == cudaSuccess;
-        if (!ok) raise(g_err, LIB, PGB_ERR_CUDA, "pgb6_hermite_create: start-up step failed");
-    }
+    ok = ok && hm_launch(H, true, 0.0, 1) && hm_sync_clock(H);
+    const int bad = ok ? H->clk.bad : 0;
     if (ok && bad) {
         raise(g_err, LIB, PGB_ERR_ARG, "pgb6_hermite_create: the start-up step of %d particles is below dtmax/2^51",
               bad);
-        ok = false;
         hm_free(H);
         delete H;
         return PGB_ERR_ARG;
@@ -1590,14 +1497,15 @@ PGB_EXPORT int pgb6_hermite_step(pgb6_hermite* H, double* time, int* ni) {
     }
     if (!ensure_device()) return PGB_ERR_NOGPU;
     std::lock_guard<std::mutex> g(H->mu);
-    if (!hm_step(H, false)) return PGB_ERR_CUDA;
-    if (time) *time = H->t_mod * H->dtmax + H->t_gl;
-    if (ni) *ni = H->last_ni;
+    if (!hm_launch(H, false, INFINITY, 1) || !hm_sync_clock(H)) return PGB_ERR_CUDA;
+    if (time) *time = H->clk.time;
+    if (ni) *ni = H->clk.ni;
     return PGB_OK;
 }
 
-// Block steps while the global time is below tend (banana01.c:146 loop condition).  *psteps /
-// *bsteps (optional): the particle steps and block steps this call took.
+// Block steps while the global time is below tend (banana01.c:146 loop condition, evaluated on
+// the device before every step).  *psteps / *bsteps (optional): the particle steps and block
+// steps this call took.
 PGB_EXPORT int pgb6_hermite_advance(pgb6_hermite* H, double tend, long long* psteps, long long* bsteps) {
     if (!H) {
         raise(g_err, LIB, PGB_ERR_ARG, "pgb6_hermite_advance: null integrator");
@@ -1605,16 +1513,15 @@ PGB_EXPORT int pgb6_hermite_advance(pgb6_hermite* H, double tend, long long* pst
     }
     if (!ensure_device()) return PGB_ERR_NOGPU;
     std::lock_guard<std::mutex> g(H->mu);
-    const long long p0 = H->psteps, b0 = H->bsteps;
-    while (H->t_mod * H->dtmax + H->t_gl < tend)
-        if (!hm_step(H, false)) return PGB_ERR_CUDA;
-    PGB_CUDA_OR(g_err, LIB, cudaStreamSynchronize(H->s), return PGB_ERR_CUDA);
-    if (psteps) *psteps = H->psteps - p0;
-    if (bsteps) *bsteps = H->bsteps - b0;
+    const long long p0 = H->clk.psteps, b0 = H->clk.bsteps;
+    while (H->clk.time < tend)
+        if (!hm_launch(H, false, tend, HM_STEPS_PER_LAUNCH) || !hm_sync_clock(H)) return PGB_ERR_CUDA;
+    if (psteps) *psteps = H->clk.psteps - p0;
+    if (bsteps) *bsteps = H->clk.bsteps - b0;
     return PGB_OK;
 }
 
-PGB_EXPORT double pgb6_hermite_time(pgb6_hermite* H) { return H ? H->t_mod * H->dtmax + H->t_gl : 0.0; }
+PGB_EXPORT double pgb6_hermite_time(pgb6_hermite* H) { return H ? H->clk.time : 0.0; }
 
 // The particle state (any pointer may be NULL): t, dt, pos, vel, acc, jerk, pot as the
 // reference's struct Particle holds them (jerk and pot with float values).
@@ -1643,7 +1550,7 @@ PGB_EXPORT int pgb6_hermite_get(pgb6_hermite* H, double* t, double* dt, double (
 }
 
 // The last block step's active particles (index order) and the force, jerk and potential the
-// force kernel returned for them (before the corrector's rounding of jerk and pot to float).
+// force phase returned for them (before the corrector's rounding of jerk and pot to float).
 // Returns the number of active particles, or a negative error code.
 PGB_EXPORT int pgb6_hermite_last_step(pgb6_hermite* H, int* active, double (*acc)[3], double (*jrk)[3],
                                       double* pot) {
@@ -1653,7 +1560,7 @@ PGB_EXPORT int pgb6_hermite_last_step(pgb6_hermite* H, int* active, double (*acc
     }
     if (!ensure_device()) return -PGB_ERR_NOGPU;
     std::lock_guard<std::mutex> g(H->mu);
-    const int ni = H->last_ni;
+    const int ni = H->clk.ni;
     std::vector<G6Out> o((size_t)ni);
     if (active)
         PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(active, H->W.active, ni * sizeof(int), cudaMemcpyDeviceToHost, H->s),
@@ -1697,8 +1604,20 @@ PGB_EXPORT int pgb6_hermite_energy(pgb6_hermite* H, double* ek, double* ew) {
 
 // Particle and block steps since creation (the start-up step counts n and 1).
 PGB_EXPORT void pgb6_hermite_counts(pgb6_hermite* H, long long* psteps, long long* bsteps) {
-    if (psteps) *psteps = H ? H->psteps : 0;
-    if (bsteps) *bsteps = H ? H->bsteps : 0;
+    if (psteps) *psteps = H ? H->clk.psteps : 0;
+    if (bsteps) *bsteps = H ? H->clk.bsteps : 0;
+}
+
+// The integrator's CUDA stream (for callers that time it with CUDA events or order their own
+// work after it).
+PGB_EXPORT void* pgb6_hermite_stream(pgb6_hermite* H) { return H ? (void*)H->s : nullptr; }
+
+// Pair interactions of the force phases so far (active particles x n) and the steps taken with
+// each force decomposition (i-tile 16, 32, 64, 128, 512); any pointer may be NULL.
+PGB_EXPORT void pgb6_hermite_stats(pgb6_hermite* H, long long* pairs, long long* steps_by_tile) {
+    if (pairs) *pairs = H ? H->clk.force_pairs : 0;
+    for (int k = 0; k < 5; k++)
+        if (steps_by_tile) steps_by_tile[k] = H ? H->clk.variant_steps[k] : 0;
 }
 
 PGB_EXPORT void pgb6_hermite_destroy(pgb6_hermite* H) {

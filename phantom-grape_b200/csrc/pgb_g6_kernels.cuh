@@ -99,6 +99,9 @@ struct G6Args {
     // per partial row (zero, self-cleaning): arrival counters of the two-level reduction of
     // groups with many chunks; nullptr: every group is reduced in one level
     int* bundle_counters = nullptr;
+    // leave the partial rows of split j-ranges unreduced (the caller's next kernel sums them in
+    // chunk order): no arrival counters, fences or last-CTA reduction in this launch
+    bool partial_only = false;
 };
 
 // The task and group of regular mode (the same decomposition plan_item() writes out).
@@ -338,101 +341,110 @@ __device__ __forceinline__ void reduce_rows(const G6Out* base, size_t stride, in
 // lane so that the shared-memory j reads stay warp-broadcasts).  A thread owns IPT i-particles
 // li = slot + k*ISL of the task's i-tile (ITILE = ISL*IPT) and every JL-th j of each j-tile.
 // The j-lanes are summed in lane order through shared memory at the end of the task.
+//
+// g6_task: one task (an i-tile against a j-range) by the whole CTA; smem holds NT G6Out.  A task
+// of a split j-range (T.group >= 0) writes its partial sums to partial row T.slot; otherwise the
+// final result to A.out.  Returns with the CTA's shared memory free for reuse after a barrier.
 template <int NT, int IPT, int JL, bool FF, bool NN, bool NBL>
-__global__ void __launch_bounds__(NT) g6_kernel(const G6Args A) {
+__device__ __forceinline__ void g6_task(const G6Args& A, const Task& T, unsigned char* smem) {
     static_assert(JL == 1 || IPT == 1, "j-lanes are used with one i per thread");
     constexpr int ISL = NT / JL;
-    // j tile during the loop, per-thread results (G6Out) after it
-    __shared__ __align__(16) unsigned char smem[NT * sizeof(G6Out)];
     G6PredJ* sj = reinterpret_cast<G6PredJ*>(smem);
     G6Out* red = reinterpret_cast<G6Out*>(smem);
-    __shared__ int s_task, s_flag;
     const int slot = threadIdx.x % ISL;
     const int jl = threadIdx.x / ISL;
+
+    Pos3 pi[IPT];
+    float vxi[IPT], vyi[IPT], vzi[IPT], hinv[IPT];
+    int idi[IPT];
+    double S[IPT][7];
+    float kmin[IPT];
+    int kadr[IPT];
+#pragma unroll
+    for (int k = 0; k < IPT; k++) {
+        int li = slot + k * ISL;
+        int ii = T.i0 + (li < T.ni ? li : 0);
+        const G6I P = A.ipart[ii];
+        pi[k] = P.p;
+        vxi[k] = P.vx; vyi[k] = P.vy; vzi[k] = P.vz;
+        idi[k] = P.id;
+        // gravity.c:688-695: -2/h, or -1e10 when h2 == 0 (no neighbours); padding lanes none
+        hinv[k] = (li >= T.ni) ? -INFINITY : ((P.h2 == 0.0f) ? -1e10f : -2.0f / sqrtf(P.h2));
+#pragma unroll
+        for (int c = 0; c < 7; c++) S[k][c] = 0.0;
+        kmin[k] = 10.0f;   // gravity_kernel2 starts its key at 10 and index at -1 (:495-496)
+        kadr[k] = -1;
+    }
+
+    for (int jt = 0; jt < T.nj; jt += NT) {
+        const int nt = min(NT, T.nj - jt);
+        __syncthreads();
+        if (threadIdx.x < nt) sj[threadIdx.x] = A.jpred[T.j0 + jt + threadIdx.x];
+        __syncthreads();
+        G6Acc a[IPT];
+#pragma unroll
+        for (int k = 0; k < IPT; k++) a[k] = G6Acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll 2
+        for (int j = jl; j < nt; j += JL) {
+            const G6PredJ J = sj[j];
+            const int jadr = T.j0 + jt + j;
+#pragma unroll
+            for (int k = 0; k < IPT; k++) {
+                int li = slot + k * ISL;
+                int gi = T.i0 + (li < T.ni ? li : 0);
+                g6_pair<FF, NN, NBL>(J, jadr, pi[k], vxi[k], vyi[k], vzi[k], idi[k], A.eps2, hinv[k],
+                                 a[k], kmin[k], kadr[k], NBL ? A.nb_count + gi : nullptr,
+                                 NBL ? A.nb_list + (size_t)gi * A.nb_maxlen : nullptr, A.nb_maxlen);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < IPT; k++) {
+            S[k][0] += (double)a[k].ax;
+            S[k][1] += (double)a[k].ay;
+            S[k][2] += (double)a[k].az;
+            S[k][3] += (double)a[k].jx;
+            S[k][4] += (double)a[k].jy;
+            S[k][5] += (double)a[k].jz;
+            S[k][6] += (double)a[k].pot;
+        }
+    }
+
+    G6Out* dst_row = (T.group < 0) ? nullptr : A.partial + (size_t)T.slot * A.itile;
+#pragma unroll
+    for (int k = 0; k < IPT; k++) {
+        G6Out o;
+        o.ax = S[k][0]; o.ay = S[k][1]; o.az = S[k][2];
+        o.jx = S[k][3]; o.jy = S[k][4]; o.jz = S[k][5];
+        o.pot = S[k][6];
+        o.key = kmin[k];
+        o.jadr = kadr[k];
+        if constexpr (JL > 1) {
+            // sum the j-lanes in lane order (lane 0 holds the CTA's result afterwards)
+            __syncthreads();
+            red[threadIdx.x] = o;
+            __syncthreads();
+            if (jl != 0) continue;
+            for (int l = 1; l < JL; l++) out_add(o, red[slot + l * ISL]);
+        }
+        int li = slot + k * ISL;
+        if (li >= T.ni) continue;
+        if (dst_row) dst_row[li] = o;
+        else A.out[T.i0 + li] = g6_finish(o);
+    }
+}
+
+template <int NT, int IPT, int JL, bool FF, bool NN, bool NBL>
+__global__ void __launch_bounds__(NT) g6_kernel(const G6Args A) {
+    // j tile during the loop, per-thread results (G6Out) after it
+    __shared__ __align__(16) unsigned char smem[NT * sizeof(G6Out)];
+    __shared__ int s_task, s_flag;
 
     for (bool first = true;; first = false) {
         int t = next_task(A.task_counter, &s_task, A.ntasks, first);
         if (t >= A.ntasks) break;
         const Task T = A.tasks ? A.tasks[t] : regular_task(A, t);
-
-        Pos3 pi[IPT];
-        float vxi[IPT], vyi[IPT], vzi[IPT], hinv[IPT];
-        int idi[IPT];
-        double S[IPT][7];
-        float kmin[IPT];
-        int kadr[IPT];
-#pragma unroll
-        for (int k = 0; k < IPT; k++) {
-            int li = slot + k * ISL;
-            int ii = T.i0 + (li < T.ni ? li : 0);
-            const G6I P = A.ipart[ii];
-            pi[k] = P.p;
-            vxi[k] = P.vx; vyi[k] = P.vy; vzi[k] = P.vz;
-            idi[k] = P.id;
-            // gravity.c:688-695: -2/h, or -1e10 when h2 == 0 (no neighbours); padding lanes none
-            hinv[k] = (li >= T.ni) ? -INFINITY : ((P.h2 == 0.0f) ? -1e10f : -2.0f / sqrtf(P.h2));
-#pragma unroll
-            for (int c = 0; c < 7; c++) S[k][c] = 0.0;
-            kmin[k] = 10.0f;   // gravity_kernel2 starts its key at 10 and index at -1 (:495-496)
-            kadr[k] = -1;
-        }
-
-        for (int jt = 0; jt < T.nj; jt += NT) {
-            const int nt = min(NT, T.nj - jt);
-            __syncthreads();
-            if (threadIdx.x < nt) sj[threadIdx.x] = A.jpred[T.j0 + jt + threadIdx.x];
-            __syncthreads();
-            G6Acc a[IPT];
-#pragma unroll
-            for (int k = 0; k < IPT; k++) a[k] = G6Acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-#pragma unroll 2
-            for (int j = jl; j < nt; j += JL) {
-                const G6PredJ J = sj[j];
-                const int jadr = T.j0 + jt + j;
-#pragma unroll
-                for (int k = 0; k < IPT; k++) {
-                    int li = slot + k * ISL;
-                    int gi = T.i0 + (li < T.ni ? li : 0);
-                    g6_pair<FF, NN, NBL>(J, jadr, pi[k], vxi[k], vyi[k], vzi[k], idi[k], A.eps2, hinv[k],
-                                     a[k], kmin[k], kadr[k], NBL ? A.nb_count + gi : nullptr,
-                                     NBL ? A.nb_list + (size_t)gi * A.nb_maxlen : nullptr, A.nb_maxlen);
-                }
-            }
-#pragma unroll
-            for (int k = 0; k < IPT; k++) {
-                S[k][0] += (double)a[k].ax;
-                S[k][1] += (double)a[k].ay;
-                S[k][2] += (double)a[k].az;
-                S[k][3] += (double)a[k].jx;
-                S[k][4] += (double)a[k].jy;
-                S[k][5] += (double)a[k].jz;
-                S[k][6] += (double)a[k].pot;
-            }
-        }
-
-        G6Out* dst_row = (T.group < 0) ? nullptr : A.partial + (size_t)T.slot * A.itile;
-#pragma unroll
-        for (int k = 0; k < IPT; k++) {
-            G6Out o;
-            o.ax = S[k][0]; o.ay = S[k][1]; o.az = S[k][2];
-            o.jx = S[k][3]; o.jy = S[k][4]; o.jz = S[k][5];
-            o.pot = S[k][6];
-            o.key = kmin[k];
-            o.jadr = kadr[k];
-            if constexpr (JL > 1) {
-                // sum the j-lanes in lane order (lane 0 holds the CTA's result afterwards)
-                __syncthreads();
-                red[threadIdx.x] = o;
-                __syncthreads();
-                if (jl != 0) continue;
-                for (int l = 1; l < JL; l++) out_add(o, red[slot + l * ISL]);
-            }
-            int li = slot + k * ISL;
-            if (li >= T.ni) continue;
-            if (dst_row) dst_row[li] = o;
-            else A.out[T.i0 + li] = g6_finish(o);
-        }
-        if (!dst_row) continue;
+        g6_task<NT, IPT, JL, FF, NN, NBL>(A, T, smem);
+        if (T.group < 0 || A.partial_only) continue;
         const Group G = A.groups ? A.groups[T.group] : regular_group(A, T.group);
         double2* W = reinterpret_cast<double2*>(smem);
         const int B = bundle_size(G.nchunk, A.bundle_counters != nullptr);

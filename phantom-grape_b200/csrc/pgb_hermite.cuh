@@ -1,30 +1,44 @@
 // pgb_hermite.cuh -- the PG6 sample integrator's 4th-order Hermite block-time-step scheme on
-// the device: block selection, i- and j-prediction, corrector and new step, start-up step.
+// the device: block selection, i- and j-prediction, force, corrector and new step, start-up
+// step, time reset -- one persistent kernel runs whole block steps back to back.
 //
 // Reference: PG6/banana (built with -DNORMAL, its setting): timestep.c:87-98 global_time
 // (block time and active set), hermite.c:39-63 predict_exmotion (i predictor), hermite.c:67-108
 // correct + 143-205 correct_sgmotion (corrector, new state), timestep.c:53-85 dt_criterion
 // (Aarseth criterion, step halved or doubled on the power-of-two grid), hermite.c:110-141
 // startup_sgmotion + timestep.c:24-51 dt_startup, timestep.c:127-135 reset_time,
-// timestep.c:137-150 calc_modulus.  The j-memory that the reference re-sends with
-// g6_set_j_particle after every step (hermite.c:240-265: pos, vel, acc/2, jerk/6, mass, t) is the
-// particle state itself here: the j predictor reads the state arrays, so nothing is re-sent.
+// timestep.c:137-150 calc_modulus, banana01.c:119-179 the main loop.  The j-memory that the
+// reference re-sends with g6_set_j_particle after every step (hermite.c:240-265: pos, vel,
+// acc/2, jerk/6, mass, t) is the particle state itself here: the j predictor reads the state
+// arrays, so nothing is re-sent.
 //
 // State in HBM, one array per field of struct Particle (PG6/banana/particle.h): t, dt, pot,
 // mass [n] and pos, vel, acc, jrk [n][3], all FP64 (jrk and pot hold float values: the
-// reference stores them as float).  One block step is five launches:
-//   hm_tmin_kernel   min over i of t_i + dt_i (the block time t_gl), atomicMin on the bits
-//                    (t + dt >= 0, so the bit patterns order like the values); with `reset`,
-//                    first sets every t_i = 0 (reset_time after a step that ended on a
-//                    multiple of dtmax);
-//   hm_count_kernel  active particles (t_i + dt_i == t_gl) per segment of SEG particles; the
-//                    last segment to arrive scans the counts in order and publishes (ni, t_gl)
-//                    to the host through mapped memory, so the host can size the force launch;
-//   hm_build_kernel  j-prediction of every particle to t_gl (the library's FP64 predictor,
-//                    gravity.c:149-193) and, for the active ones in index order, the active
-//                    list and the predicted i-records;
-//   the force kernel (pgb_g6_kernels.cuh / pgb_g6_small.cuh) on the ni i-records;
-//   hm_correct_kernel (or hm_startup_kernel for the first step) per active particle.
+// reference stores them as float).
+//
+// hm_run_kernel is a cooperative launch (every CTA resident) that loops over block steps until
+// the global time reaches tend.  Segments of HM_SEG particles belong to CTAs (segment s to CTA
+// s mod grid) in every phase.  Once per launch, then after every step:
+//   A  per segment: the minimum of t_i + dt_i and how many particles sit at it; the global
+//      minimum by atomicMin.
+// Each step is then three phases; one grid barrier closes the step, and within it CTAs wait
+// only for the data they read (per-segment and per-task flags tagged with the step number):
+//   B  every CTA reads the block time t_gl (the global minimum) and computes every segment's
+//      offset of active particles; it predicts its own segments' particles to t_gl (the
+//      library's FP64 j predictor, gravity.c:149-193) and writes their active ones, in index
+//      order, to the active list with predicted i-records; CTA 0 advances the clock;
+//   C  the force: the GRAPE-6 pair kernel's tasks (pgb_g6_kernels.cuh g6_task) over an
+//      i-tile x j-chunk decomposition of the ni x n pairs, each task once the segments of its
+//      i- and j-ranges are built; split j-ranges left as partial rows;
+//   D  per own segment, once the tasks of its active particles' i-tiles are done, one warp per
+//      active particle: its partial rows summed in chunk order, the corrector (or the start-up
+//      step); then reset_time if the step ended on a multiple of dtmax, and A for the segment.
+// Data read across CTAs within a step is double-buffered by step parity where the next step
+// could overwrite it before a slow CTA has read it (segment minima); everything else is
+// rewritten only after the closing barrier.
+// Every CTA derives the step's decisions (block time, ni, decomposition, end of the run) from
+// the same data, so they agree without further communication.  The barriers are bounded: a
+// barrier that waits longer than about a second sets an error word and the kernel returns.
 // The i-predictor and the corrector use the reference's formulas and constants in the order
 // its C source evaluates them, with every FP64 multiply and add rounded separately (no fused
 // multiply-add): given the same forces the new state equals a plain C evaluation bit for bit.
@@ -34,35 +48,72 @@
 
 namespace pgb {
 
-constexpr int HM_NT = 256;            // threads per CTA of the step kernels
-constexpr int HM_PER = 8;             // particles per thread
-constexpr int HM_SEG = HM_NT * HM_PER;  // particles per segment (one CTA)
+constexpr int HM_NT = 256;       // threads per CTA
+constexpr int HM_SEG = 256;      // particles per segment of the selection (one per thread)
+constexpr int HM_MAXSEG = 4096;  // segments at most: n <= 2^20
 
 struct HmState {
     double *t, *dt, *pos, *vel, *acc, *jrk, *pot, *mass;
     int n;
 };
 
-// Published by hm_count_kernel into mapped host memory: the step's block time and active count.
-struct HmHostCtl {
-    unsigned seq;
-    int ni;
+// The integrator's clock and counters in device memory (banana01.c:119-179 bookkeeping): the
+// last step's block time and active count, the global time after it (t_mod * dtmax + t_gl, or
+// t_mod * dtmax after a reset), the completed dtmax intervals, the pending reset_time, the
+// particle / block steps and the device time of the force phases.
+struct HmClock {
     double t_gl;
+    double time;
+    long long psteps, bsteps;
+    long long force_pairs;
+    long long variant_steps[5];   // steps by force decomposition (i-tile 16, 32, 64, 128, 512)
+    int t_mod;
+    int reset;
+    int ni;       // the last step's active count
+    int nch;      // its force decomposition: j-chunks and i-tile
+    int itile;
+    int bad;      // start-up steps below dtmin
+    int err;      // a wait gave up
+    int pad;
+};
+
+// Grid barrier state: the generation CTA 0 last released, the step number (the tag of the
+// flags below) at the end of the last launch, and per CTA the generation it last arrived at
+// (32-bit words 128 bytes apart so that arrivals do not share a line).
+constexpr int HM_ARRIVE_STRIDE = 32;
+struct HmSync {
+    unsigned gen;
+    unsigned step;
+    unsigned pad[HM_ARRIVE_STRIDE - 2];
+    unsigned arrive[1];   // [grid * HM_ARRIVE_STRIDE]
 };
 
 struct HmWork {
-    unsigned long long* tmin;  // atomic min of the bits of t + dt; all ones between steps
-    int* ticket;               // arrivals on hm_count_kernel (self-resetting)
-    int* bcnt;                 // active count per segment
-    int* boff;                 // exclusive prefix of bcnt
-    int* ni;                   // the step's active count
-    double* t_gl;              // the step's block time
-    int* bad;                  // start-up steps below dtmin
+    unsigned long long* bmin;  // [2][nseg] per segment: the minimum of t + dt (bits), by step parity
+    int* bcnt;                 // [2][nseg] per segment: particles at that minimum
+    unsigned long long* gmin;  // [3] the global minimum, by step number mod 3 (atomicMin)
+    unsigned* seg_flag;        // [nseg] step number of the segment's last build (phase B)
+    unsigned* task_flag;       // [task_cap] step number of the force task's last completion
+    int task_cap;
+    HmClock* clk;
+    HmSync* sync;
     int* active;               // [n] active particles in index order
     G6I* irec;                 // [n] their predicted i-records
     G6PredJ* jpred;            // [n] every particle predicted to t_gl
-    G6Out* out;                // [n] force, jerk, potential of the active particles
-    HmHostCtl* host;           // device address of the mapped control block
+    G6Out* out;                // [n] force, jerk, potential of the active particles (final)
+    G6Out* partial;            // partial rows of split j-ranges, part_cap entries
+    long long part_cap;
+};
+
+struct HmRun {
+    HmState P;
+    HmWork W;
+    float eps2;
+    double eta, eta_s, dtmax, tend;
+    int startup;     // take the start-up step only
+    int max_steps;   // block steps of this launch at most
+    int nseg;
+    int minj;        // j per chunk at least
 };
 
 __device__ __forceinline__ double hm_mul(double a, double b) { return __dmul_rn(a, b); }
@@ -116,26 +167,6 @@ __device__ __forceinline__ unsigned long long block_min_u64(unsigned long long v
     return v;
 }
 
-__global__ void __launch_bounds__(HM_NT) hm_tmin_kernel(HmState P, HmWork W, int reset) {
-    __shared__ unsigned long long sm[HM_NT / 32];
-    const int seg0 = blockIdx.x * HM_SEG;
-    unsigned long long m = ~0ull;
-#pragma unroll 4
-    for (int r = 0; r < HM_PER; r++) {
-        const int i = seg0 + r * HM_NT + (int)threadIdx.x;
-        if (i >= P.n) break;
-        double t = P.t[i];
-        if (reset) {
-            t = 0.0;
-            P.t[i] = 0.0;
-        }
-        const unsigned long long b = (unsigned long long)__double_as_longlong(hm_add(t, P.dt[i]));
-        m = b < m ? b : m;
-    }
-    m = block_min_u64<HM_NT>(m, sm);
-    if (threadIdx.x == 0) atomicMin(W.tmin, m);
-}
-
 // Inclusive scan of v over the CTA (warp shuffles, then the warp totals); *total = the sum.
 template <int NT>
 __device__ __forceinline__ int block_scan(int v, int* sw, int* total) {
@@ -158,113 +189,46 @@ __device__ __forceinline__ int block_scan(int v, int* sw, int* total) {
     return v + base;
 }
 
-__global__ void __launch_bounds__(HM_NT) hm_count_kernel(HmState P, HmWork W, unsigned seq) {
-    __shared__ int sw[HM_NT / 32];
-    __shared__ int s_last;
-    const double tg = __longlong_as_double((long long)*W.tmin);
-    const int seg0 = blockIdx.x * HM_SEG;
-    int c = 0;
-#pragma unroll 4
-    for (int r = 0; r < HM_PER; r++) {
-        const int i = seg0 + r * HM_NT + (int)threadIdx.x;
-        if (i >= P.n) break;
-        c += hm_add(P.t[i], P.dt[i]) == tg;
+// The force of active particle k, by the whole warp: with nch > 1 the sum of its nch j-chunk
+// partial rows in a fixed order (lane l takes chunks l, l+32, ..., then a butterfly; lane 0's
+// sum is the result) scaled as the force kernel's final stage does, written to out[k]; with
+// nch == 1 the force kernel's final result out[k].
+__device__ __forceinline__ G6Out hm_force_of(const HmWork& W, int k, int nch, int itile) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    if (nch == 1) return W.out[k];
+    const int it = k / itile, li = k - it * itile;
+    const double2* row = reinterpret_cast<const double2*>(W.partial + (size_t)it * nch * itile + li);
+    const size_t stride = (size_t)itile * 4;   // double2 words per partial row
+    double s[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int c = lane; c < nch; c += 32) {
+        const double2* r = row + (size_t)c * stride;
+        const double2 w0 = __ldcg(r), w1 = __ldcg(r + 1), w2 = __ldcg(r + 2), w3 = __ldcg(r + 3);
+        s[0] += w0.x; s[1] += w0.y; s[2] += w1.x; s[3] += w1.y; s[4] += w2.x; s[5] += w2.y; s[6] += w3.x;
     }
-    int tot;
-    block_scan<HM_NT>(c, sw, &tot);
-    if (threadIdx.x == 0) W.bcnt[blockIdx.x] = tot;
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) s_last = atomicAdd(W.ticket, 1) == (int)gridDim.x - 1;
-    __syncthreads();
-    if (!s_last) return;
-    // the last segment: every count is written; scan them in segment order
-    __threadfence();
-    int run = 0;
-    for (int b0 = 0; b0 < (int)gridDim.x; b0 += HM_NT) {
-        const int b = b0 + (int)threadIdx.x;
-        const int v = b < (int)gridDim.x ? __ldcg(W.bcnt + b) : 0;
-        int sum;
-        const int inc = block_scan<HM_NT>(v, sw, &sum);
-        if (b < (int)gridDim.x) W.boff[b] = run + inc - v;
-        run += sum;
-    }
-    if (threadIdx.x == 0) {
-        *W.ni = run;
-        *W.t_gl = tg;
-        *W.tmin = ~0ull;   // every segment has read it
-        *W.ticket = 0;
-        W.host->ni = run;
-        W.host->t_gl = tg;
-        __threadfence_system();
-        *(volatile unsigned*)&W.host->seq = seq;
-    }
-}
-
-__global__ void __launch_bounds__(HM_NT) hm_build_kernel(HmState P, HmWork W, bool ff) {
-    __shared__ int sw[HM_NT / 32];
-    const double tg = *W.t_gl;
-    const int seg0 = blockIdx.x * HM_SEG;
-    int base = W.boff[blockIdx.x];
-    for (int r = 0; r < HM_PER; r++) {
-        const int i = seg0 + r * HM_NT + (int)threadIdx.x;
-        const bool in = i < P.n;
-        bool act = false;
-        if (in) {
-            // j predictor of the library (gravity.c:149-193) on (pos, vel, acc/2, jerk/6, t)
-            const double d = tg - P.t[i], d2 = d * d, d3 = d2 * d;
-            double x[3];
-            float v[3];
 #pragma unroll
-            for (int c = 0; c < 3; c++) {
-                const double a2 = P.acc[3 * i + c] * 0.5, j6 = P.jrk[3 * i + c] * (1.0 / 6.0);
-                x[c] = P.pos[3 * i + c] + P.vel[3 * i + c] * d + a2 * d2 + j6 * d3;
-                v[c] = (float)(P.vel[3 * i + c] + 2.0 * a2 * d + 3.0 * j6 * d2);
-            }
-            G6PredJ o;
-            store_pos(o.p, x[0], x[1], x[2], ff);
-            o.m = (float)P.mass[i];
-            o.id = i;
-            o.vx = v[0];
-            o.vy = v[1];
-            o.vz = v[2];
-            o.pad = 0.f;
-            W.jpred[i] = o;
-            act = hm_add(P.t[i], P.dt[i]) == tg;
-        }
-        int tot;
-        const int inc = block_scan<HM_NT>(act ? 1 : 0, sw, &tot);
-        if (act) {
-            const int k = base + inc - 1;
-            W.active[k] = i;
-            double xp[3], vp[3];
-            hm_predict_i(P, i, tg, xp, vp);
-            G6I rec;
-            store_pos(rec.p, xp[0], xp[1], xp[2], ff);
-            rec.vx = (float)vp[0];
-            rec.vy = (float)vp[1];
-            rec.vz = (float)vp[2];
-            rec.id = i;
-            rec.h2 = 0.f;
-            rec.pad = 0.f;
-            W.irec[k] = rec;
-        }
-        base += tot;
-    }
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int q = 0; q < 7; q++) s[q] += __shfl_xor_sync(full, s[q], o);
+#pragma unroll
+    for (int q = 0; q < 7; q++) s[q] = __shfl_sync(full, s[q], 0);
+    G6Out F;
+    F.ax = -0.125 * s[0]; F.ay = -0.125 * s[1]; F.az = -0.125 * s[2];
+    F.jx = -0.125 * s[3]; F.jy = -0.125 * s[4]; F.jz = -0.125 * s[5];
+    F.pot = 0.5 * s[6];
+    F.key = 0.f;
+    F.jadr = -1;
+    if (lane == 0) W.out[k] = F;
+    return F;
 }
 
 // Corrector and new step of active particle k (hermite.c:67-108, 143-205; timestep.c:53-85),
 // given its new acceleration (FP64), jerk and potential (rounded to float as the reference's
 // struct NewAccJerk stores them).
-__global__ void hm_correct_kernel(HmState P, HmWork W, int ni, double eta, double dtmax) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= ni) return;
-    const int i = W.active[k];
-    const double tg = *W.t_gl;
+__device__ __forceinline__ void hm_correct(const HmState& P, int i, double tg, const G6Out& F, double eta, double dtmax) {
     const double dtmin = dtmax / 2251799813685248.0;  // dtmax / 2^51
     double x1[3], v1[3];
     hm_predict_i(P, i, tg, x1, v1);
-    const G6Out F = W.out[k];
     const double a1[3] = {F.ax, F.ay, F.az};
     const double j1[3] = {hm_float(F.jx), hm_float(F.jy), hm_float(F.jz)};
     const double dts = P.dt[i], dtsinv = 1.0 / dts;
@@ -321,13 +285,10 @@ __global__ void hm_correct_kernel(HmState P, HmWork W, int ni, double eta, doubl
 
 // Start-up step (hermite.c:110-141, timestep.c:24-51): every particle active at t = 0; the new
 // force becomes the state and the first step is the largest power-of-two fraction of dtmax
-// below eta_s |a|/|j| that divides t.  Counts the steps that fell below dtmin into *W.bad.
-__global__ void hm_startup_kernel(HmState P, HmWork W, int ni, double eta_s, double dtmax) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= ni) return;
-    const int i = W.active[k];
+// below eta_s |a|/|j| that divides t.  Counts the steps that fell below dtmin into W.clk->bad.
+__device__ __forceinline__ void hm_startup(const HmState& P, const HmWork& W, int i, const G6Out& F, double eta_s,
+                                           double dtmax) {
     const double dtmin = dtmax / 2251799813685248.0;
-    const G6Out F = W.out[k];
     const double a1[3] = {F.ax, F.ay, F.az};
     const double j1[3] = {hm_float(F.jx), hm_float(F.jy), hm_float(F.jz)};
     double a = 0.0, jj = 0.0;
@@ -345,17 +306,327 @@ __global__ void hm_startup_kernel(HmState P, HmWork W, int ni, double eta_s, dou
     for (int it = 0; hm_modulus(P.t[i], d, dtmax) != 0.0 && it < 64; it++) {
         d *= 0.5;
         if (d < dtmin) {
-            atomicAdd(W.bad, 1);
+            atomicAdd(&W.clk->bad, 1);
             break;
         }
     }
     P.dt[i] = d;
 }
 
-// reset_time (timestep.c:127-135) on its own, for reads of the state between steps.
-__global__ void hm_reset_kernel(HmState P) {
+// Grid barrier for a cooperative launch.  Each CTA publishes the barrier's generation number
+// in its own arrival word; CTA 0's threads watch the arrival words, and once every CTA is in
+// they release the generation, for which the other CTAs wait.  No atomics, no shared counter.
+// Release/acquire through the fences around the flag stores and loads.  A wait gives up after
+// about a second of SM clock (error word set); returns false on error (the caller returns).
+__device__ __forceinline__ bool hm_spin_until(volatile unsigned* w, unsigned target, HmClock* C) {
+    const long long t0 = clock64();
+    while (*w != target) {
+        if (clock64() - t0 > 2000000000LL) {
+            atomicExch(&C->err, 1);
+            return false;
+        }
+    }
+    return true;
+}
+
+__device__ __forceinline__ bool hm_grid_sync(HmSync* S, HmClock* C, unsigned target) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        s_ok = 1;
+        __threadfence();
+        *(volatile unsigned*)&S->arrive[blockIdx.x * HM_ARRIVE_STRIDE] = target;
+    }
+    if (blockIdx.x == 0) {
+        int ok = 1;
+        for (int k = threadIdx.x; k < (int)gridDim.x; k += blockDim.x)
+            ok &= hm_spin_until(&S->arrive[k * HM_ARRIVE_STRIDE], target, C);
+        ok = __syncthreads_and(ok);
+        if (threadIdx.x == 0) {
+            __threadfence();
+            *(volatile unsigned*)&S->gen = target;
+            if (!ok) s_ok = 0;
+        }
+    } else if (threadIdx.x == 0) {
+        if (!hm_spin_until(&S->gen, target, C)) s_ok = 0;
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (*(volatile int*)&C->err) s_ok = 0;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+__device__ __forceinline__ unsigned long long hm_globaltimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Phase A for one segment: its minimum of t + dt (bits) and count at the minimum, into the
+// parity-p slots; the minimum also into the global minimum *gmin.
+__device__ __forceinline__ void hm_segment_min(const HmRun& R, int seg, int reset, int p, unsigned long long* gmin,
+                                               unsigned long long* sm) {
+    const HmState& P = R.P;
+    const int i = seg * HM_SEG + (int)threadIdx.x;
+    unsigned long long b = ~0ull;
+    if (i < P.n) {
+        double t = P.t[i];
+        if (reset) {
+            t = 0.0;
+            P.t[i] = 0.0;
+        }
+        b = (unsigned long long)__double_as_longlong(hm_add(t, P.dt[i]));
+    }
+    const unsigned long long m = block_min_u64<HM_NT>(b, sm);
+    const int c = __syncthreads_count(i < P.n && b == m);
+    if (threadIdx.x == 0) {
+        R.W.bmin[p * R.nseg + seg] = m;
+        R.W.bcnt[p * R.nseg + seg] = c;
+        atomicMin(gmin, m);
+    }
+}
+
+// Phase B for one segment: j-prediction of its particles; its active ones (in index order from
+// offset base) into the active list with their predicted i-records.
+__device__ __forceinline__ void hm_segment_build(const HmRun& R, int seg, double tg, int base, bool ff, int* sw) {
+    const HmState& P = R.P;
+    const HmWork& W = R.W;
+    const int i = seg * HM_SEG + (int)threadIdx.x;
+    bool act = false;
+    if (i < P.n) {
+        // j predictor of the library (gravity.c:149-193) on (pos, vel, acc/2, jerk/6, t)
+        const double d = tg - P.t[i], d2 = d * d, d3 = d2 * d;
+        double x[3];
+        float v[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const double a2 = P.acc[3 * i + c] * 0.5, j6 = P.jrk[3 * i + c] * (1.0 / 6.0);
+            x[c] = P.pos[3 * i + c] + P.vel[3 * i + c] * d + a2 * d2 + j6 * d3;
+            v[c] = (float)(P.vel[3 * i + c] + 2.0 * a2 * d + 3.0 * j6 * d2);
+        }
+        G6PredJ o;
+        store_pos(o.p, x[0], x[1], x[2], ff);
+        o.m = (float)P.mass[i];
+        o.id = i;
+        o.vx = v[0];
+        o.vy = v[1];
+        o.vz = v[2];
+        o.pad = 0.f;
+        W.jpred[i] = o;
+        act = hm_add(P.t[i], P.dt[i]) == tg;
+    }
+    int tot;
+    const int inc = block_scan<HM_NT>(act ? 1 : 0, sw, &tot);
+    if (act) {
+        const int k = base + inc - 1;
+        W.active[k] = i;
+        double xp[3], vp[3];
+        hm_predict_i(P, i, tg, xp, vp);
+        G6I rec;
+        store_pos(rec.p, xp[0], xp[1], xp[2], ff);
+        rec.vx = (float)vp[0];
+        rec.vy = (float)vp[1];
+        rec.vz = (float)vp[2];
+        rec.id = i;
+        rec.h2 = 0.f;
+        rec.pad = 0.f;
+        W.irec[k] = rec;
+    }
+}
+
+// The force decomposition of a step with ni active particles (identical in every CTA): the pair
+// kernel's shape by ni (i-tile of 16, 32, 64, 128 or 512: j-lanes 16, 8, 4, 2 or two i per
+// thread), j-chunks for about one task per CTA, at least minj j per chunk, partial rows and
+// task flags within their buffers.
+struct HmShape {
+    int variant, itile, itiles, nch, ntasks;
+};
+__device__ __forceinline__ HmShape hm_shape(const HmRun& R, int ni) {
+    HmShape h;
+    h.variant = ni <= 16 ? 0 : ni <= 32 ? 1 : ni <= 64 ? 2 : ni <= 2048 ? 3 : 4;
+    h.itile = h.variant == 4 ? 512 : (16 << h.variant);
+    h.itiles = (ni + h.itile - 1) / h.itile;
+    const int nj = R.P.n;
+    int nch = ((int)gridDim.x + h.itiles - 1) / h.itiles;
+    const int by_j = nj / R.minj > 1 ? nj / R.minj : 1;
+    nch = nch < by_j ? nch : by_j;
+    const long long cap = R.W.part_cap / ((long long)h.itiles * h.itile);
+    if (nch > cap) nch = cap > 1 ? (int)cap : 1;
+    const int tcap = R.W.task_cap / h.itiles;
+    if (nch > tcap) nch = tcap > 1 ? tcap : 1;
+    h.nch = nch < 1 ? 1 : nch;
+    h.ntasks = h.itiles * h.nch;
+    return h;
+}
+
+// Wait (all threads of the CTA) until every flag[k] for which need(k) holds equals tag; then the
+// data published before those flags is visible to the CTA.  False if a wait gave up.
+template <class Need>
+__device__ __forceinline__ bool hm_wait_flags(unsigned* flag, int nflag, unsigned tag, HmClock* C, Need need) {
+    int ok = 1;
+    for (int k = threadIdx.x; k < nflag; k += HM_NT)
+        if (need(k)) ok &= hm_spin_until(flag + k, tag, C);
+    __threadfence();
+    return __syncthreads_and(ok) != 0;
+}
+
+// Publish (thread 0, after the CTA's writes): flag = tag.
+__device__ __forceinline__ void hm_publish(unsigned* flag, unsigned tag) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        *(volatile unsigned*)flag = tag;
+    }
+}
+
+template <bool FF>
+__global__ void __launch_bounds__(HM_NT, 2) hm_run_kernel(const HmRun R) {
+    __shared__ __align__(16) unsigned char smem[HM_NT * sizeof(G6Out)];
+    __shared__ int s_boff[HM_MAXSEG + 1];   // offsets of every segment's active particles (+ ni)
+    __shared__ unsigned long long sm[HM_NT / 32];
+    __shared__ int sw[HM_NT / 32];
+    const HmWork& W = R.W;
+    HmClock* C = W.clk;
+    const int G = (int)gridDim.x, nseg = R.nseg;
+    unsigned epoch = *(volatile unsigned*)&W.sync->gen;   // both stable between launches
+    unsigned E = *(volatile unsigned*)&W.sync->step;
+    // A (once per launch): segment minima of the current state and their global minimum
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        W.gmin[E % 3] = ~0ull;
+        W.gmin[(E + 1) % 3] = ~0ull;
+    }
+    if (!hm_grid_sync(W.sync, C, ++epoch)) return;
+    for (int seg = blockIdx.x; seg < nseg; seg += G) {
+        hm_segment_min(R, seg, 0, E & 1, W.gmin + E % 3, sm);
+        __syncthreads();
+    }
+    if (!hm_grid_sync(W.sync, C, ++epoch)) return;
+    for (int step = 0;; step++) {
+        // the loop condition of banana01.c:146 on the clock written before the last barrier
+        if (R.startup ? step >= 1 : (!(*(volatile double*)&C->time < R.tend) || step >= R.max_steps)) break;
+        const int p = E & 1;
+        // B: the block time, every segment's active offset, own segments' predictions and
+        // i-records (published per segment)
+        const unsigned long long g = *(volatile unsigned long long*)(W.gmin + E % 3);
+        int run = 0;
+        for (int b0 = 0; b0 < nseg; b0 += HM_NT) {
+            const int k = b0 + (int)threadIdx.x;
+            const int v = (k < nseg && W.bmin[p * nseg + k] == g) ? W.bcnt[p * nseg + k] : 0;
+            int sum;
+            const int inc = block_scan<HM_NT>(v, sw, &sum);
+            if (k < nseg) s_boff[k] = run + inc - v;
+            run += sum;
+        }
+        const int ni = run;
+        if (threadIdx.x == 0) s_boff[nseg] = ni;
+        const double tg = __longlong_as_double((long long)g);
+        for (int seg = blockIdx.x; seg < nseg; seg += G) {
+            __syncthreads();
+            hm_segment_build(R, seg, tg, s_boff[seg], FF, sw);
+            hm_publish(W.seg_flag + seg, E);
+        }
+        __syncthreads();
+        const HmShape sh = hm_shape(R, ni);
+        // banana01.c:161-179: after a step that ends on a multiple of dtmax the times restart
+        // (reset_time, applied with the corrector below) and t_mod counts the interval
+        int rs = 0;
+        if (!R.startup) {
+            const double q = (double)__double2int_rz(hm_mul(tg, 1.0 / R.dtmax));
+            rs = hm_sub(tg, hm_mul(q, R.dtmax)) == 0.0;
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            W.gmin[(E + 2) % 3] = ~0ull;   // read last in step E-1, next atomicMin in step E+1
+            C->t_gl = tg;
+            C->ni = ni;
+            C->nch = sh.nch;
+            C->itile = sh.itile;
+            C->psteps += ni;
+            C->bsteps += 1;
+            C->force_pairs += (long long)ni * R.P.n;
+            C->variant_steps[sh.variant] += 1;
+            if (!R.startup) {
+                const int tm = C->t_mod + rs;
+                C->t_mod = tm;
+                C->time = rs ? hm_add(hm_mul((double)tm, R.dtmax), 0.0) : hm_add(hm_mul((double)tm, R.dtmax), tg);
+            }
+        }
+        // C: force tasks, each after the segments it reads are built
+        {
+            G6Args a;
+            a.ipart = W.irec;
+            a.jpred = W.jpred;
+            a.eps2 = R.eps2;
+            a.tasks = nullptr;
+            a.ntasks = sh.ntasks;
+            a.task_counter = nullptr;
+            a.groups = nullptr;
+            a.group_counters = nullptr;
+            a.partial = W.partial;
+            a.out = W.out;
+            a.itile = sh.itile;
+            a.nb_count = nullptr;
+            a.nb_list = nullptr;
+            a.nb_maxlen = 0;
+            a.reg_ni = ni;
+            a.reg_nj = R.P.n;
+            a.reg_nch = sh.nch;
+            a.partial_only = true;
+            for (int t = blockIdx.x; t < sh.ntasks; t += G) {
+                const Task T = regular_task(a, t);
+                const int js0 = T.j0 / HM_SEG, js1 = (T.j0 + T.nj - 1) / HM_SEG;
+                const int k0 = T.i0, k1 = T.i0 + T.ni;
+                const bool ok = hm_wait_flags(W.seg_flag, nseg, E, C, [&](int s) {
+                    return (s >= js0 && s <= js1) || (s_boff[s] < k1 && s_boff[s + 1] > k0);
+                });
+                if (!ok) return;
+                switch (sh.variant) {
+                    case 0: g6_task<HM_NT, 1, 16, FF, false, false>(a, T, smem); break;
+                    case 1: g6_task<HM_NT, 1, 8, FF, false, false>(a, T, smem); break;
+                    case 2: g6_task<HM_NT, 1, 4, FF, false, false>(a, T, smem); break;
+                    case 3: g6_task<HM_NT, 1, 2, FF, false, false>(a, T, smem); break;
+                    default: g6_task<HM_NT, 2, 1, FF, false, false>(a, T, smem); break;
+                }
+                hm_publish(W.task_flag + t, E);
+            }
+        }
+        // D + next A, segment by segment (the CTA that built it): after the force tasks of its
+        // active particles' i-tiles, the corrector (or start-up step) of each, one warp each;
+        // the time reset; the segment's new minimum
+        const int wpc = HM_NT / 32;
+        for (int seg = blockIdx.x; seg < nseg; seg += G) {
+            const int k0 = s_boff[seg], k1 = s_boff[seg + 1];
+            if (k1 > k0) {
+                const int it0 = k0 / sh.itile, it1 = (k1 - 1) / sh.itile;
+                const bool ok = hm_wait_flags(W.task_flag, sh.ntasks, E, C,
+                                              [&](int t) { return t / sh.nch >= it0 && t / sh.nch <= it1; });
+                if (!ok) return;
+            }
+            for (int k = k0 + (int)(threadIdx.x >> 5); k < k1; k += wpc) {
+                const G6Out F = hm_force_of(W, k, sh.nch, sh.itile);
+                if ((threadIdx.x & 31) == 0) {
+                    const int i = W.active[k];
+                    if (R.startup) hm_startup(R.P, W, i, F, R.eta_s, R.dtmax);
+                    else hm_correct(R.P, i, tg, F, R.eta, R.dtmax);
+                }
+            }
+            __syncthreads();   // the segment's updated t, dt
+            hm_segment_min(R, seg, rs, p ^ 1, W.gmin + (E + 1) % 3, sm);
+            __syncthreads();
+        }
+        if (!hm_grid_sync(W.sync, C, ++epoch)) return;
+        E++;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) W.sync->step = E;
+}
+
+// reset_time (timestep.c:127-135) on its own, for reads of the state between steps: applies
+// the pending reset and clears it.
+__global__ void hm_reset_kernel(HmState P, HmClock* clk) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < P.n) P.t[i] = 0.0;
+    if (i == 0) clk->reset = 0;
 }
 
 // Kinetic and potential energy (calc_energy.c:9-33): ek = sum m v^2 / 2, ew = sum m pot / 2.

@@ -270,6 +270,8 @@ class G6(_ErrMixin):
         _sig(L, "pgb6_hermite_last_step", [vp, ip, dp, dp, dp], C.c_int)
         _sig(L, "pgb6_hermite_energy", [vp, dp, dp], C.c_int)
         _sig(L, "pgb6_hermite_counts", [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)])
+        _sig(L, "pgb6_hermite_stream", [vp], vp)
+        _sig(L, "pgb6_hermite_stats", [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)])
         _sig(L, "pgb6_hermite_destroy", [vp])
         sz = [C.c_int() for _ in range(4)]
         L.pgb6_record_sizes(*[C.byref(s) for s in sz])
@@ -581,6 +583,16 @@ class Hermite:
         p, b = C.c_longlong(), C.c_longlong()
         self.L.pgb6_hermite_counts(self.h, C.byref(p), C.byref(b))
         return p.value, b.value
+
+    @property
+    def stream(self):
+        return self.L.pgb6_hermite_stream(self.h)
+
+    def stats(self):
+        """(pair interactions so far, steps by force i-tile 16 / 32 / 64 / 128 / 512)."""
+        pairs, by = C.c_longlong(), (C.c_longlong * 5)()
+        self.L.pgb6_hermite_stats(self.h, C.byref(pairs), by)
+        return pairs.value, list(by)
 
     def close(self):
         if self.h:

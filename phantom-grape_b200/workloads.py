@@ -132,6 +132,15 @@ def plummer_hermite(n: int, seed: int, rmax: float = 22.8):
     return x, v, np.full(n, 1.0 / n), rng
 
 
+def plummer_henon(n: int, seed: int):
+    """Plummer sphere in Henon units (G = M = 1, E = -1/4: scale radius 3 pi / 16), equal
+    masses 1/n, centre of mass at rest -- the units of the reference sample integrator's
+    initial conditions (PG6/banana/init/pl*.init).  Returns (x, v, m)."""
+    x, v, m, _ = plummer_hermite(n, seed)
+    a = 3.0 * np.pi / 16.0
+    return x * a, v / np.sqrt(a), m
+
+
 def hermite_state(n: int = 65536, seed: int = SEED0 + 1, eps: float = 1e-4,
                   force_fn=None, t_now: float = 1.0) -> HermiteState:
     """Block time-step state.  ``force_fn(x, v, m, eps2) -> (acc, jrk)`` supplies the
