@@ -438,7 +438,6 @@ bool run_small(int nj, int ni, float eps2, bool nn, bool nbl, G6Out* out_dev) {
     a.nb_count = nullptr;
     a.nb_list = nullptr;
     a.nb_maxlen = nbmax();
-    a.irec = nullptr;
     if (nbl) {
         PGB_CUDA_OR(g_err, LIB, S.nbc_d.reserve(ni), return false);
         PGB_CUDA_OR(g_err, LIB, S.nbl_d.reserve((size_t)ni * nbmax()), return false);

@@ -14,7 +14,7 @@
 //      the rows (reduce_rows: fixed row order) and writes the final scaled result -- CL CTAs
 //      share the final stage and no cluster waits for another.
 // The i-records come in the parameter block (no upload; staged to shared memory with
-// broadcast reads), or from device memory when the caller built them there, and the j-chunks are a pure function of (blockIdx, nj, gridDim), so a call
+// broadcast reads) and the j-chunks are a pure function of (blockIdx, nj, gridDim), so a call
 // is one launch.  The result is deterministic for a given
 // grid and cluster size.  Per pair the arithmetic is g6_pair(), identical to g6_kernel.
 #pragma once
@@ -40,9 +40,6 @@ struct G6SmallArgs {
     // polling instead of synchronising the stream
     volatile unsigned* done;
     unsigned seq;
-    // i-records in device memory (nullptr: in the parameter block), for callers whose i-records
-    // are built on the device
-    const G6I* irec;
 };
 
 // Publish a final slice: every thread's result writes are made visible to the host before
@@ -84,18 +81,14 @@ __global__ void __launch_bounds__(ISL * JL, 2)
     int nt = min(NT, j1 - jt);
     G6PredJ jr;
     if (threadIdx.x < nt) jr = A.jpred[jt + threadIdx.x];
-    if (A.irec) {
-        if (threadIdx.x < A.ni) s_i[threadIdx.x] = A.irec[threadIdx.x];
-    } else {
-        for (int r = threadIdx.x / 32; r < A.ni; r += NT / 32) {
-            const uint4* src = reinterpret_cast<const uint4*>(&ib.rec[r]);
-            const uint4 w0 = src[0], w1 = src[1], w2 = src[2];
-            if ((threadIdx.x & 31) == 0) {
-                uint4* d = reinterpret_cast<uint4*>(&s_i[r]);
-                d[0] = w0;
-                d[1] = w1;
-                d[2] = w2;
-            }
+    for (int r = threadIdx.x / 32; r < A.ni; r += NT / 32) {
+        const uint4* src = reinterpret_cast<const uint4*>(&ib.rec[r]);
+        const uint4 w0 = src[0], w1 = src[1], w2 = src[2];
+        if ((threadIdx.x & 31) == 0) {
+            uint4* d = reinterpret_cast<uint4*>(&s_i[r]);
+            d[0] = w0;
+            d[1] = w1;
+            d[2] = w2;
         }
     }
     if (threadIdx.x < nt) sj[threadIdx.x] = jr;
