@@ -398,55 +398,124 @@ class BHSet:
         return np.stack([self.gfirst, self.gcount, off[:-1], np.diff(off)], 1).astype(np.int32)
 
 
+def _bh_read(L, pre, h, x, m, eps, theta, nleaf, ncrit):
+    """Read a built tree through the accessors <pre>n, <pre>groups, ... of library L."""
+    import ctypes as C
+    vp, dp, ip, lp = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int), C.POINTER(C.c_longlong)
+    for f, r in (("ngroups", C.c_int), ("nnodes", C.c_int), ("np", C.c_longlong), ("nc", C.c_longlong)):
+        getattr(L, pre + f).argtypes = [vp]
+        getattr(L, pre + f).restype = r
+    getattr(L, pre + "perm").argtypes = [vp, ip]
+    getattr(L, pre + "groups").argtypes = [vp, ip, ip, dp, dp]
+    getattr(L, pre + "cells").argtypes = [vp, dp, dp, dp]
+    getattr(L, pre + "lists").argtypes = [vp, lp, ip, lp, ip]
+    getattr(L, pre + "nodes").argtypes = [vp, ip, ip, dp, dp, ip]
+    n = len(m)
+    fn = lambda name: getattr(L, pre + name)  # noqa: E731
+    ng, nn, npl, ncl = fn("ngroups")(h), fn("nnodes")(h), fn("np")(h), fn("nc")(h)
+    perm = np.empty(n, np.int32)
+    fn("perm")(h, perm.ctypes.data_as(ip))
+    gfirst, gcount = np.empty(ng, np.int32), np.empty(ng, np.int32)
+    gcentre, ghalf = np.empty((ng, 3)), np.empty(ng)
+    fn("groups")(h, gfirst.ctypes.data_as(ip), gcount.ctypes.data_as(ip), gcentre.ctypes.data_as(dp),
+                 ghalf.ctypes.data_as(dp))
+    ccom, cmass, cquad = np.empty((nn, 3)), np.empty(nn), np.empty((nn, 6))
+    fn("cells")(h, ccom.ctypes.data_as(dp), cmass.ctypes.data_as(dp), cquad.ctypes.data_as(dp))
+    poff, coff = np.empty(ng + 1, np.int64), np.empty(ng + 1, np.int64)
+    pidx, cidx = np.empty(max(npl, 1), np.int32), np.empty(max(ncl, 1), np.int32)
+    fn("lists")(h, poff.ctypes.data_as(lp), pidx.ctypes.data_as(ip), coff.ctypes.data_as(lp), cidx.ctypes.data_as(ip))
+    nfirst, ncount, nhalf = np.empty(nn, np.int32), np.empty(nn, np.int32), np.empty(nn)
+    ncentre, nchild = np.empty((nn, 3)), np.empty((nn, 8), np.int32)
+    fn("nodes")(h, nfirst.ctypes.data_as(ip), ncount.ctypes.data_as(ip), nhalf.ctypes.data_as(dp),
+                ncentre.ctypes.data_as(dp), nchild.ctypes.data_as(ip))
+    return BHSet(x=x[perm], m=m[perm], perm=perm, gfirst=gfirst, gcount=gcount, gcentre=gcentre, ghalf=ghalf,
+                 poff=poff, pidx=pidx[:npl], coff=coff, cidx=cidx[:ncl], ccom=ccom, cmass=cmass, cquad=cquad,
+                 nfirst=nfirst, ncount=ncount, nhalf=nhalf, ncentre=ncentre, nchild=nchild, eps=eps, theta=theta,
+                 nleaf=nleaf, ncrit=ncrit)
+
+
 def bh_tree(x: np.ndarray, m: np.ndarray, theta: float = 0.5, nleaf: int = 16, ncrit: int = 256,
             eps: float = 1e-3) -> BHSet:
     """Octree, moments and interaction lists of particles x (n x 3), m (n) with the reference's
-    rules (drivers/pgb_bhtree.c)."""
+    rules, built on the host (drivers/pgb_bhtree.c)."""
     import ctypes as C
     from . import ffi
     L = C.CDLL(ffi.lib_path("libpgbdrv.so"), mode=C.RTLD_LOCAL)
-    vp, dp, ip, lp = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int), C.POINTER(C.c_longlong)
+    dp = C.POINTER(C.c_double)
     L.bh_build.argtypes = [C.c_int, dp, dp, C.c_double, C.c_int, C.c_int]
-    L.bh_build.restype = vp
-    for f, r in (("bh_n", C.c_int), ("bh_ngroups", C.c_int), ("bh_nnodes", C.c_int), ("bh_np", C.c_longlong),
-                 ("bh_nc", C.c_longlong)):
-        getattr(L, f).argtypes = [vp]
-        getattr(L, f).restype = r
-    L.bh_perm.argtypes = [vp, ip]
-    L.bh_groups.argtypes = [vp, ip, ip, dp, dp]
-    L.bh_cells.argtypes = [vp, dp, dp, dp]
-    L.bh_lists.argtypes = [vp, lp, ip, lp, ip]
-    L.bh_nodes.argtypes = [vp, ip, ip, dp, dp, ip]
-    L.bh_free.argtypes = [vp]
+    L.bh_build.restype = C.c_void_p
+    L.bh_free.argtypes = [C.c_void_p]
     x = np.ascontiguousarray(x, np.float64)
     m = np.ascontiguousarray(m, np.float64)
-    n = len(m)
-    h = L.bh_build(n, x.ctypes.data_as(dp), m.ctypes.data_as(dp), theta, nleaf, ncrit)
+    h = L.bh_build(len(m), x.ctypes.data_as(dp), m.ctypes.data_as(dp), theta, nleaf, ncrit)
     if not h:
         raise MemoryError("bh_build failed")
     try:
-        ng, nn, npl, ncl = L.bh_ngroups(h), L.bh_nnodes(h), L.bh_np(h), L.bh_nc(h)
-        perm = np.empty(n, np.int32)
-        L.bh_perm(h, perm.ctypes.data_as(ip))
-        gfirst, gcount = np.empty(ng, np.int32), np.empty(ng, np.int32)
-        gcentre, ghalf = np.empty((ng, 3)), np.empty(ng)
-        L.bh_groups(h, gfirst.ctypes.data_as(ip), gcount.ctypes.data_as(ip), gcentre.ctypes.data_as(dp),
-                    ghalf.ctypes.data_as(dp))
-        ccom, cmass, cquad = np.empty((nn, 3)), np.empty(nn), np.empty((nn, 6))
-        L.bh_cells(h, ccom.ctypes.data_as(dp), cmass.ctypes.data_as(dp), cquad.ctypes.data_as(dp))
-        poff, coff = np.empty(ng + 1, np.int64), np.empty(ng + 1, np.int64)
-        pidx, cidx = np.empty(max(npl, 1), np.int32), np.empty(max(ncl, 1), np.int32)
-        L.bh_lists(h, poff.ctypes.data_as(lp), pidx.ctypes.data_as(ip), coff.ctypes.data_as(lp),
-                   cidx.ctypes.data_as(ip))
-        nfirst, ncount, nhalf = np.empty(nn, np.int32), np.empty(nn, np.int32), np.empty(nn)
-        ncentre, nchild = np.empty((nn, 3)), np.empty((nn, 8), np.int32)
-        L.bh_nodes(h, nfirst.ctypes.data_as(ip), ncount.ctypes.data_as(ip), nhalf.ctypes.data_as(dp),
-                   ncentre.ctypes.data_as(dp), nchild.ctypes.data_as(ip))
+        return _bh_read(L, "bh_", h, x, m, eps, theta, nleaf, ncrit)
     finally:
         L.bh_free(h)
-    return BHSet(x=x[perm], m=m[perm], perm=perm, gfirst=gfirst, gcount=gcount, gcentre=gcentre, ghalf=ghalf,
-                 poff=poff, pidx=pidx[:npl], coff=coff, cidx=cidx[:ncl], ccom=ccom, cmass=cmass, cquad=cquad,
-                 nfirst=nfirst, ncount=ncount, nhalf=nhalf, ncentre=ncentre, nchild=nchild, eps=eps, theta=theta, nleaf=nleaf, ncrit=ncrit)
+
+
+class GpuTree:
+    """The same tree built on the GPU (lib/libpgbtree.so, pgbt_*): .set() reads it back as a
+    BHSet, .device() gives the device pointers of the batched force launch, .build_ms the
+    device time of the build."""
+
+    def __init__(self, x: np.ndarray, m: np.ndarray, theta: float = 0.5, nleaf: int = 16, ncrit: int = 256,
+                 eps: float = 1e-3):
+        import ctypes as C
+        from . import ffi
+        self.L = L = C.CDLL(ffi.lib_path("libpgbtree.so"), mode=C.RTLD_LOCAL)
+        dp, vp = C.POINTER(C.c_double), C.c_void_p
+        L.pgbt_build.argtypes = [C.c_int, dp, dp, C.c_double, C.c_int, C.c_int]
+        L.pgbt_build.restype = vp
+        L.pgbt_free.argtypes = [vp]
+        L.pgbt_build_ms.argtypes = [vp]
+        L.pgbt_build_ms.restype = C.c_float
+        L.pgbt_device.argtypes = [vp] + [C.POINTER(vp)] * 7
+        L.pgbt_last_error.argtypes = [C.c_char_p, C.c_int]
+        L.pgbt_nnodes.argtypes = [vp]
+        L.pgbt_nnodes.restype = C.c_int
+        self.x = np.ascontiguousarray(x, np.float64)
+        self.m = np.ascontiguousarray(m, np.float64)
+        self.args = (eps, theta, nleaf, ncrit)
+        self.h = L.pgbt_build(len(self.m), self.x.ctypes.data_as(dp), self.m.ctypes.data_as(dp), theta, nleaf, ncrit)
+        if not self.h:
+            buf = C.create_string_buffer(512)
+            L.pgbt_last_error(buf, 512)
+            raise RuntimeError(f"pgbt_build failed: {buf.value.decode()}")
+        self.build_ms = L.pgbt_build_ms(self.h)
+
+    def set(self) -> BHSet:
+        return _bh_read(self.L, "pgbt_", self.h, self.x, self.m, *self.args)
+
+    def records(self):
+        """Host copies of the force-launch records: particles (n, 4), cells (nn, 4), quadrupoles (nn, 8)."""
+        import ctypes as C
+        nn = self.L.pgbt_nnodes(self.h)
+        part = np.empty((len(self.m), 4), np.float32)
+        cell, cquad = np.empty((nn, 4), np.float32), np.empty((nn, 8), np.float32)
+        fp = C.POINTER(C.c_float)
+        self.L.pgbt_records.argtypes = [C.c_void_p, fp, fp, fp]
+        self.L.pgbt_records(self.h, part.ctypes.data_as(fp), cell.ctypes.data_as(fp), cquad.ctypes.data_as(fp))
+        return part, cell, cquad
+
+    def device(self):
+        import ctypes as C
+        ptrs = [C.c_void_p() for _ in range(7)]
+        self.L.pgbt_device(self.h, *[C.byref(p) for p in ptrs])
+        return dict(zip(("part", "cell", "cquad", "poff", "pidx", "coff", "cidx"), (p.value for p in ptrs)))
+
+    def close(self):
+        if self.h:
+            self.L.pgbt_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def bh_hernquist(n: int = 1 << 22, seed: int = SEED0 + 3, theta: float = 0.5, nleaf: int = 16, ncrit: int = 256,

@@ -15,6 +15,7 @@ HEADERS = {
     "pgb_g5.h": ["libpg5.so", "libpg5sym.so"],
     "pgb_g5table.h": ["libpg5table.so"],
     "pgb_g6.h": ["libpg6.so"],
+    "pgb_bhtree.h": ["libpgbtree.so"],
 }
 
 
@@ -37,7 +38,7 @@ def declared_functions(header, symmetric=False):
         if all(keep):
             out.append(line)
     text = "\n".join(out)
-    names = re.findall(r"^\s*(?:extern\s+)?(?:void|int|long long|double|float)\s+\**\s*(\w+)\s*\(", text, re.M)
+    names = re.findall(r"^\s*(?:extern\s+)?(?:void|int|long long|double|float|pgbt_tree)\s+\**\s*(\w+)\s*\(", text, re.M)
     return sorted(set(names))
 
 
@@ -88,7 +89,7 @@ def test_reference_symbol_sets_are_covered():
         pytest.skip("reference not built")
 
 
-@pytest.mark.parametrize("lib", ["libpg5.so", "libpg5sym.so", "libpg5table.so", "libpg6.so"])
+@pytest.mark.parametrize("lib", ["libpg5.so", "libpg5sym.so", "libpg5table.so", "libpg6.so", "libpgbtree.so"])
 def test_product_does_not_use_the_oracle(lib):
     out = subprocess.run(["nm", "-D", pgb.ffi.lib_path(lib)], capture_output=True, text=True).stdout
     assert "orc_" not in out
