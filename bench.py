@@ -908,9 +908,7 @@ def run_bh(args, pgb, ws, rank, local):
     W = pgb.workloads
     g5 = pgb.ffi.G5()
     g5.L.g5_open()
-    t0 = time.time()
     bh = W.bh_hernquist(args.bh_n, seed=W.SEED0 + 3 + rank)
-    t_tree = time.time() - t0
     ip, pp, cp, cq = bh.records()
     d_i, d_p = torch.from_numpy(ip).to(dev), torch.from_numpy(pp).to(dev)
     d_c, d_q = torch.from_numpy(cp).to(dev), torch.from_numpy(cq).to(dev)
@@ -997,6 +995,44 @@ def run_bh(args, pgb, ws, rank, local):
     h2d = sum(t.numel() * t.element_size() for t in h_in)
     d2h = sum(t.numel() * t.element_size() for t in h_out)
 
+    # a whole tree-code step through this repository's API, from particles in host memory to
+    # forces in host memory: the tree, moments, groups and lists built on the GPU
+    # (lib/libpgbtree.so), both plans created from its group table, both launches, both results
+    # read back -- every step; host clock
+    x_in, m_in = np.empty_like(bh.x), np.empty_like(bh.m)
+    x_in[bh.perm], m_in[bh.perm] = bh.x, bh.m
+    t0 = time.perf_counter()
+    W.bh_tree(x_in, m_in, bh.theta, bh.nleaf, bh.ncrit, bh.eps)
+    host_build_s = time.perf_counter() - t0
+    d_i2 = torch.empty_like(d_i)
+    step_s, build_ms, same = [], [], True
+    for k in range(args.warmup + args.e2e_steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        tr = W.GpuTree(x_in, m_in, bh.theta, bh.nleaf, bh.ncrit, bh.eps)
+        dv = tr.device()
+        it_p, it_c = tr.items()
+        tr.irecords(bh.eps * bh.eps, d_i2.data_ptr())
+        q_p, q_c = g5.plan_create(g5.NEWTON, it_p), g5.plan_create(g5.QUAD, it_c)
+        g5.L.pgb5_plan_set_config(q_p, cfg_p)
+        g5.L.pgb5_plan_set_config(q_c, cfg_c)
+        g5.plan_launch_indexed(q_p, d_i2.data_ptr(), dv["part"], None, dv["pidx"], o_p.data_ptr(), s.cuda_stream)
+        g5.plan_launch_indexed(q_c, d_i2.data_ptr(), dv["cell"], dv["cquad"], dv["cidx"], o_c.data_ptr(),
+                               s.cuda_stream)
+        with torch.cuda.stream(s):
+            h_out[0].copy_(o_p, non_blocking=True)
+            h_out[1].copy_(o_c, non_blocking=True)
+        s.synchronize()
+        dt = time.perf_counter() - t0
+        if k >= args.warmup:
+            step_s.append(dt)
+            build_ms.append(tr.build_ms)
+        g5.plan_destroy(q_p)
+        g5.plan_destroy(q_c)
+        tr.close()
+    same = bool(np.array_equal((h_out[0][:, :3] + h_out[1][:, :3]).numpy(), acc_b))
+    tree_val = reduce_sum(float(pairs) * len(step_s), ws, dev) / reduce_max(sum(step_s), ws, dev) / 1e9
+
     # the per-group drop-in calls with host buffers (source.cpp:813-866 call sequence)
     drv = Driver(pgb)
     p = Driver.p
@@ -1058,10 +1094,16 @@ def run_bh(args, pgb, ws, rank, local):
                  pairs, "38 (point mass) / 60 (quadrupole cell)", f"Barnes-Hut N={args.bh_n} Hernquist (a=1, r<=100) eps=1e-3, theta=0.5, ncrit=256, "
                  f"nleaf=16: {bh.ngroups} groups, {bh.p_pairs:.3e} point-mass + {bh.c_pairs:.3e} cell pairs",
                  "f32 (f64 cross-tile sums)", achieved, clk,
-                 {"value": round(e2e_val, 2), "unit": "Gint/s", "h2d_bytes_per_step": int(h2d),
-                  "d2h_bytes_per_step": int(d2h), "steps": len(e2e_ms),
-                  "api": "pgb5_plan_launch_indexed x 2 (point-mass and cell lists) with the records and index "
-                         "lists copied from pinned host memory and both results read back every step"},
+                 {"value": round(tree_val, 2), "unit": "Gint/s", "h2d_bytes_per_step": int(x_in.nbytes + m_in.nbytes),
+                  "d2h_bytes_per_step": int(d2h), "steps": len(step_s),
+                  "api": "whole step from host particles to host forces: pgbt_build (octree, moments, groups, "
+                         "lists on the GPU) + pgbt_group_table + pgbt_irecords + pgb5_plan_create x 2 + "
+                         "pgb5_plan_launch_indexed x 2, both results read back; host clock",
+                  "forces_equal_batched": same,
+                  "lists_copied": {"value": round(e2e_val, 2), "unit": "Gint/s", "h2d_bytes_per_step": int(h2d),
+                                   "d2h_bytes_per_step": int(d2h), "steps": len(e2e_ms),
+                                   "api": "pgb5_plan_launch_indexed x 2 with the host-built records and index lists "
+                                          "copied from pinned host memory and both results read back every step"}},
                  cpu, 2 * len(tms),
                  extra={"dropin": {"value": round(dropin_val, 2), "unit": "Gint/s", "threads": nthr,
                                    "api": "per group g5_set_xmjMC + g5_set_nMC + g5_calculate_force_on_xMC and "
@@ -1069,7 +1111,12 @@ def run_bh(args, pgb, ws, rank, local):
                                           "host thread, host buffers; list gathers inside the timed loop"},
                         "launch_ms": {"point_masses": round(ms_p, 3), "cells": round(ms_c, 3)},
                         "autotune": {"point_masses": G5_CFG_NAMES[cfg_p], "cells": G5_CFG_NAMES[cfg_c]},
-                        "tree_build_s": round(t_tree, 2), "errors": errors},
+                        "tree_build": {"gpu_ms": round(float(np.median(build_ms)), 2),
+                                       "host_s": round(host_build_s, 2),
+                                       "gpu": "lib/libpgbtree.so pgbt_build (device time, CUDA events)",
+                                       "host": "drivers/pgb_bhtree.c bh_build (OpenMP lists)",
+                                       "identical": "tests/test_bhtree_gpu.py"},
+                        "errors": errors},
                  kernel=f"pgb::g5_kernel<NEWTON,{G5_CFG_NAMES[cfg_p]}> + <QUAD,{G5_CFG_NAMES[cfg_c]}> (index lists)")
 
 

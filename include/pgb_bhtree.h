@@ -44,6 +44,11 @@ int  pgbt_device(pgbt_tree *tree, void **part, void **cell, void **cquad, void *
                  void **cidx);
 /* host copies of those records: part [n][4], cell [nnodes][4], cquad [nnodes][8] (any may be NULL) */
 int  pgbt_records(pgbt_tree *tree, float *part, float *cell, float *cquad);
+/* i-records float4 (x, y, z, eps2) in tree order into the caller's device buffer out[n] */
+int  pgbt_irecords(pgbt_tree *tree, double eps2, void *out);
+/* the groups' particle ranges (ngroup) and list offsets (ngroup + 1): the work items of the
+ * batched launches (any pointer may be NULL) */
+int  pgbt_group_table(pgbt_tree *tree, int *first, int *count, long long *poff, long long *coff);
 
 int  pgbt_last_error(char *buf, int len);
 void pgbt_clear_error(void);

@@ -954,6 +954,46 @@ PGB_EXPORT int pgbt_lists(pgbt_tree* T, long long* poff, int* pidx, long long* c
     return rc;
 }
 
+namespace {
+__global__ void k_irecords(int n, const double* xt, float eps2, float4* out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n)
+        out[k] = make_float4((float)xt[3 * (size_t)k], (float)xt[3 * (size_t)k + 1], (float)xt[3 * (size_t)k + 2], eps2);
+}
+}  // namespace
+
+// i-records of the batched force launch into the caller's device buffer out[n]: float4
+// (x, y, z, eps2) in tree order, on the tree's stream (complete when the call returns).
+PGB_EXPORT int pgbt_irecords(pgbt_tree* T, double eps2, void* out) {
+    if (!T || !out) return PGB_ERR_ARG;
+    if (!ensure_device()) return PGB_ERR_NOGPU;
+    k_irecords<<<nblk(T->n, 256), 256, 0, T->s>>>(T->n, T->xt.p, (float)eps2, (float4*)out);
+    PGB_CUDA_OR(g_err, LIB, cudaGetLastError(), return PGB_ERR_CUDA);
+    PGB_CUDA_OR(g_err, LIB, cudaStreamSynchronize(T->s), return PGB_ERR_CUDA);
+    return PGB_OK;
+}
+
+// Host copies of the groups' particle ranges and list offsets only (first, count: ngroup;
+// poff, coff: ngroup + 1; any pointer may be NULL): what a batched launch's work items need.
+PGB_EXPORT int pgbt_group_table(pgbt_tree* T, int* first, int* count, long long* poff, long long* coff) {
+    if (!T) return PGB_ERR_ARG;
+    if (!ensure_device()) return PGB_ERR_NOGPU;
+    const int ng = T->ng;
+    DevBuf<int> f, c;
+    DevBuf<double> ce, h;
+    PGB_CUDA_OR(g_err, LIB, f.reserve((size_t)ng + 1), return PGB_ERR_CUDA);
+    PGB_CUDA_OR(g_err, LIB, c.reserve((size_t)ng + 1), return PGB_ERR_CUDA);
+    PGB_CUDA_OR(g_err, LIB, ce.reserve(3 * (size_t)ng + 3), return PGB_ERR_CUDA);
+    PGB_CUDA_OR(g_err, LIB, h.reserve((size_t)ng + 1), return PGB_ERR_CUDA);
+    Tree P{T->first.p, T->count.p, T->child.p, T->c.p, T->half.p, T->com.p, T->mass.p, T->quad.p};
+    k_group_fields<<<nblk(ng, 256), 256, 0, T->s>>>(P, T->gnode.p, ng, f.p, c.p, ce.p, h.p);
+    int rc = copy_out(T, first, f.p, (size_t)ng);
+    if (!rc) rc = copy_out(T, count, c.p, (size_t)ng);
+    if (!rc) rc = copy_out(T, poff, T->poff.p, (size_t)ng + 1);
+    if (!rc) rc = copy_out(T, coff, T->coff.p, (size_t)ng + 1);
+    return rc;
+}
+
 // Host copies of the force-launch records (layouts as pgbt_device; any pointer may be NULL):
 // part [n][4], cell [nnodes][4], cquad [nnodes][8] floats.
 PGB_EXPORT int pgbt_records(pgbt_tree* T, float* part, float* cell, float* cquad) {

@@ -476,6 +476,8 @@ class GpuTree:
         L.pgbt_last_error.argtypes = [C.c_char_p, C.c_int]
         L.pgbt_nnodes.argtypes = [vp]
         L.pgbt_nnodes.restype = C.c_int
+        L.pgbt_ngroups.argtypes = [vp]
+        L.pgbt_ngroups.restype = C.c_int
         self.x = np.ascontiguousarray(x, np.float64)
         self.m = np.ascontiguousarray(m, np.float64)
         self.args = (eps, theta, nleaf, ncrit)
@@ -499,6 +501,26 @@ class GpuTree:
         self.L.pgbt_records.argtypes = [C.c_void_p, fp, fp, fp]
         self.L.pgbt_records(self.h, part.ctypes.data_as(fp), cell.ctypes.data_as(fp), cquad.ctypes.data_as(fp))
         return part, cell, cquad
+
+    def irecords(self, eps2: float, out_ptr: int):
+        """Write the i-records float4 (x, y, z, eps2) in tree order to device memory out_ptr."""
+        import ctypes as C
+        self.L.pgbt_irecords.argtypes = [C.c_void_p, C.c_double, C.c_void_p]
+        if self.L.pgbt_irecords(self.h, eps2, out_ptr):
+            raise RuntimeError("pgbt_irecords failed")
+
+    def items(self):
+        """Work items (i_offset, i_count, j_offset, j_count) of the point-mass and the cell lists."""
+        import ctypes as C
+        ng = self.L.pgbt_ngroups(self.h)
+        first, count = np.empty(ng, np.int32), np.empty(ng, np.int32)
+        poff, coff = np.empty(ng + 1, np.int64), np.empty(ng + 1, np.int64)
+        ip, lp = C.POINTER(C.c_int), C.POINTER(C.c_longlong)
+        self.L.pgbt_group_table.argtypes = [C.c_void_p, ip, ip, lp, lp]
+        self.L.pgbt_group_table(self.h, first.ctypes.data_as(ip), count.ctypes.data_as(ip), poff.ctypes.data_as(lp),
+                                coff.ctypes.data_as(lp))
+        mk = lambda off: np.stack([first, count, off[:-1], np.diff(off)], 1).astype(np.int32)  # noqa: E731
+        return mk(poff), mk(coff)
 
     def device(self):
         import ctypes as C

@@ -88,6 +88,15 @@ def test_device_records_follow_the_tree():
         d = t.device()
         assert all(v for v in d.values())
         assert t.build_ms > 0
+        items_p, items_c = t.items()
+        np.testing.assert_array_equal(items_p, s.items("p"))
+        np.testing.assert_array_equal(items_c, s.items("c"))
+        import torch
+        irec = torch.empty((len(m), 4), dtype=torch.float32, device="cuda")
+        t.irecords(1e-6, irec.data_ptr())
+        ir = irec.cpu().numpy()
+        np.testing.assert_array_equal(ir[:, :3], s.x.astype(np.float32))
+        np.testing.assert_array_equal(ir[:, 3], np.float32(1e-6))
     finally:
         t.close()
     np.testing.assert_array_equal(p[:, :3], s.x.astype(np.float32))
