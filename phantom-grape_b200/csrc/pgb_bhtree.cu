@@ -31,8 +31,8 @@
 // prefix sum, and a scatter kernel places each particle at child start + tile offset + its rank
 // among the tile's particles of the same octant (warp ballots) -- a stable partition, as the
 // host's counting sort.  Pre-order numbers follow from subtree sizes; moments are computed
-// bottom-up one level at a time; lists by one thread per group (an explicit stack), a counting
-// pass, a prefix sum and a filling pass.
+// bottom-up one level at a time; lists by 64 threads per group (one per grandchild of the root,
+// each with an explicit stack), a counting pass, a prefix sum and a filling pass.
 #include "pgb_common.cuh"
 
 using namespace pgb;
@@ -173,10 +173,11 @@ __global__ void k_tile_nodes(int b, int e, const int* tile_off, int* tile_node) 
 
 // Octant of every particle of a tile and the tile's octant counts.
 __global__ void __launch_bounds__(HT_NT) k_octants(Nodes N, const int* tile_node, const int* tile_off, int b,
-                                                   const double* x, const int* perm, unsigned char* oct,
-                                                   int* tcount) {
+                                                   const int* ntiles, const double* x, const int* perm,
+                                                   unsigned char* oct, int* tcount) {
     __shared__ int cnt[8];
     const int t = blockIdx.x;
+    if (t >= *ntiles) return;
     const int v = tile_node[t];
     const int lt = t - tile_off[v - b];
     const int k0 = N.first[v] + lt * HT_TILE;
@@ -242,12 +243,13 @@ __global__ void k_children(Nodes N, int b, int e, int level, int nleaf, const in
 // Stable scatter of a tile's particles to their children: child start + the tile's offset in
 // the octant + the particle's rank among the tile's earlier particles of the same octant.
 __global__ void __launch_bounds__(HT_NT) k_scatter(Nodes N, const int* tile_node, const int* tile_off, int b,
-                                                   const unsigned char* oct, const int* tbase, const int* perm,
-                                                   int* perm2) {
+                                                   const int* ntiles, const unsigned char* oct, const int* tbase,
+                                                   const int* perm, int* perm2) {
     __shared__ int wcnt[HT_NT / 32][8];
     __shared__ int run[8];
     __shared__ int cstart[8];
     const int t = blockIdx.x;
+    if (t >= *ntiles) return;
     const int v = tile_node[t];
     const int lt = t - tile_off[v - b];
     const int k0 = N.first[v] + lt * HT_TILE;
@@ -429,6 +431,30 @@ __global__ void k_compact(const int* flag, const int* off, int nn, int* out) {
     if (flag[v]) out[off[v]] = v;
 }
 
+// What the list walk reads of a node, packed: centre of mass, side^2 (side = 2 x half side),
+// particle range and kind (WK_ONE: a single particle; WK_PARTS: at most nleaf particles or
+// no children -- the walk takes its particles; WK_SPLIT: walked further if not accepted).
+enum { WK_ONE = 0, WK_PARTS = 1, WK_SPLIT = 2 };
+struct __align__(16) WalkNode {
+    double com[3];
+    double side2;
+    int first, count, kind, pad;
+};
+
+__global__ void k_walk_nodes(Tree T, int nn, int nleaf, WalkNode* wn) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= nn) return;
+    WalkNode w;
+    for (int a = 0; a < 3; a++) w.com[a] = T.com[3 * v + a];
+    const double side = 2.0 * T.half[v];
+    w.side2 = dm(side, side);
+    w.first = T.first[v];
+    w.count = T.count[v];
+    w.kind = w.count == 1 ? WK_ONE : ((w.count <= nleaf || is_leaf(T, v)) ? WK_PARTS : WK_SPLIT);
+    w.pad = 0;
+    wn[v] = w;
+}
+
 // distance^2 from point p to the cube (centre g, half side h), calc_dist's order
 __device__ __forceinline__ double box_d2(const double* p, const double g[3], double h) {
     double d2 = 0.0;
@@ -439,79 +465,140 @@ __device__ __forceinline__ double box_d2(const double* p, const double g[3], dou
     return d2;
 }
 
-// The interaction list of group gi: counts only (pl == nullptr) or fills pl / cl.
-__device__ void group_walk(const Tree& T, int gv, int nleaf, double th2, int* pl, long long* np, int* cl,
-                           long long* nc) {
-    const double g[3] = {T.c[3 * gv], T.c[3 * gv + 1], T.c[3 * gv + 2]};
-    const double h = T.half[gv];
-    long long a = 0, b = 0;
-    const double rside = 2.0 * T.half[0];
-    if (!(dm(box_d2(T.com, g, h), th2) < dm(rside, rside))) {
-        if (cl) cl[0] = 0;
-        *np = 0;
-        *nc = 1;
-        return;
+// The interaction lists are made by HT_UNITS work units per group, so that the walks spread
+// over many threads: unit u = 8 o + o2 of a group produces the part of the group's list that
+// the host builder's depth-first walk (make_interaction_list) produces for the root's child o
+// when that child is taken whole (its particle, itself as a cell, or its particles: unit
+// o2 = 0 emits it) or, when the walk descends into it, for that child's child o2.  The units'
+// lists, concatenated in unit order, are the group's list.
+constexpr int HT_UNITS = 64;
+
+struct ListOut {
+    int* pl;        // point-mass entries (nullptr: count only)
+    int* cl;        // cell entries
+    long long a, b; // entries so far
+    __device__ __forceinline__ void part(int k) {
+        if (pl) pl[a] = k;
+        a++;
     }
+    __device__ __forceinline__ void cell(int w) {
+        if (cl) cl[b] = w;
+        b++;
+    }
+};
+
+// A node the walk reaches: its particle (one particle), itself as a cell (theta^2 d^2 >
+// side^2), its particles (at most nleaf or no children) -- or false: the walk descends.
+__device__ __forceinline__ bool take_node(const WalkNode& C, int w, const double g[3], double h, double th2,
+                                          ListOut& L) {
+    if (C.kind == WK_ONE) {
+        L.part(C.first);
+        return true;
+    }
+    if (dm(box_d2(C.com, g, h), th2) > C.side2) {
+        L.cell(w);
+        return true;
+    }
+    if (C.kind == WK_PARTS) {
+        for (int k = C.first; k < C.first + C.count; k++) L.part(k);
+        return true;
+    }
+    return false;
+}
+
+// Depth-first walk below node v (descended into), children in octant order.
+__device__ void walk_below(const Tree& T, const WalkNode* __restrict__ wn, int v, const double g[3], double h,
+                           double th2, ListOut& L) {
     int sv[HT_MAXDEPTH + 2], so[HT_MAXDEPTH + 2];
-    int sp = 0;
-    // the root: a small node or a depth-capped leaf gives its particles
-    if (T.count[0] <= nleaf || is_leaf(T, 0)) {
-        for (int k = T.first[0]; k < T.first[0] + T.count[0]; k++) {
-            if (pl) pl[a] = k;
-            a++;
-        }
-    } else {
-        sv[0] = 0;
-        so[0] = 0;
-        sp = 1;
-    }
+    int sp = 1;
+    sv[0] = v;
+    so[0] = 0;
     while (sp > 0) {
-        const int v = sv[sp - 1];
+        const int u = sv[sp - 1];
         int o = so[sp - 1];
-        while (o < 8 && T.child[8 * v + o] < 0) o++;
+        int w = -1;
+        for (; o < 8; o++) {
+            w = T.child[8 * u + o];
+            if (w >= 0) break;
+        }
         if (o == 8) {
             sp--;
             continue;
         }
         so[sp - 1] = o + 1;
-        const int w = T.child[8 * v + o];
-        const int cw = T.count[w];
-        if (cw == 1) {
-            if (pl) pl[a] = T.first[w];
-            a++;
-            continue;
-        }
-        const double side = 2.0 * T.half[w];
-        if (dm(box_d2(T.com + 3 * w, g, h), th2) > dm(side, side)) {
-            if (cl) cl[b] = w;
-            b++;
-        } else if (cw <= nleaf || is_leaf(T, w)) {
-            for (int k = T.first[w]; k < T.first[w] + cw; k++) {
-                if (pl) pl[a] = k;
-                a++;
-            }
-        } else {
+        if (!take_node(wn[w], w, g, h, th2, L)) {
             sv[sp] = w;
             so[sp] = 0;
             sp++;
         }
     }
-    *np = a;
-    *nc = b;
 }
 
-__global__ void k_list_count(Tree T, const int* gnode, int ng, int nleaf, double th2, long long* np, long long* nc) {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= ng) return;
-    group_walk(T, gnode[g], nleaf, th2, nullptr, np + g, nullptr, nc + g);
+// Work unit u of the group with node gv.  The root: the group's list is the root as one cell
+// when the root passes the opening test (group_list of the host builder), the root's particles
+// when it has at most nleaf particles or no children; unit 0 emits either.
+__device__ void unit_walk(const Tree& T, const WalkNode* __restrict__ wn, int gv, int u, double th2, ListOut& L) {
+    const double g[3] = {T.c[3 * gv], T.c[3 * gv + 1], T.c[3 * gv + 2]};
+    const double h = T.half[gv];
+    const WalkNode R = wn[0];
+    if (!(dm(box_d2(R.com, g, h), th2) < R.side2)) {
+        if (u == 0) L.cell(0);
+        return;
+    }
+    if (R.kind != WK_SPLIT) {
+        if (u == 0)
+            for (int k = R.first; k < R.first + R.count; k++) L.part(k);
+        return;
+    }
+    const int o = u >> 3, o2 = u & 7;
+    const int c1 = T.child[o];
+    if (c1 < 0) return;
+    const WalkNode C1 = wn[c1];
+    if (C1.kind != WK_SPLIT || dm(box_d2(C1.com, g, h), th2) > C1.side2) {
+        if (o2 == 0) take_node(C1, c1, g, h, th2, L);
+        return;
+    }
+    const int c2 = T.child[8 * c1 + o2];
+    if (c2 < 0) return;
+    if (!take_node(wn[c2], c2, g, h, th2, L)) walk_below(T, wn, c2, g, h, th2, L);
 }
 
-__global__ void k_list_fill(Tree T, const int* gnode, int ng, int nleaf, double th2, const long long* poff,
-                            const long long* coff, int* pidx, int* cidx) {
+// Thread q takes unit q / ng of group q % ng: the lanes of a warp take the same unit of
+// neighbouring groups, whose walks are alike (a group's longest unit is the one around it).
+// Counts and offsets are stored group-major (g * HT_UNITS + u), the order of the lists.
+__global__ void k_list_count(Tree T, const WalkNode* wn, const int* gnode, int ng, double th2, long long* np,
+                             long long* nc) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= (long long)ng * HT_UNITS) return;
+    const int u = (int)(q / ng), g = (int)(q % ng);
+    ListOut L{nullptr, nullptr, 0, 0};
+    unit_walk(T, wn, gnode[g], u, th2, L);
+    np[(long long)g * HT_UNITS + u] = L.a;
+    nc[(long long)g * HT_UNITS + u] = L.b;
+}
+
+__global__ void k_list_fill(Tree T, const WalkNode* wn, const int* gnode, int ng, double th2, const long long* uoffp,
+                            const long long* uoffc, int* pidx, int* cidx) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= (long long)ng * HT_UNITS) return;
+    const int u = (int)(q / ng), g = (int)(q % ng);
+    const long long r = (long long)g * HT_UNITS + u;
+    ListOut L{pidx + uoffp[r], cidx + uoffc[r], 0, 0};
+    unit_walk(T, wn, gnode[g], u, th2, L);
+}
+
+// per-group offsets from the per-unit offsets (entry ng: the totals)
+__global__ void k_group_offsets(int ng, const long long* uoffp, const long long* uoffc, long long* poff,
+                                long long* coff) {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= ng) return;
-    long long a, b;
-    group_walk(T, gnode[g], nleaf, th2, pidx + poff[g], &a, cidx + coff[g], &b);
+    if (g > ng) return;
+    poff[g] = uoffp[(long long)g * HT_UNITS];
+    coff[g] = uoffc[(long long)g * HT_UNITS];
+}
+
+__global__ void k_iota(int n, int* p) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) p[k] = k;
 }
 
 __global__ void k_maxabs(const double* x, long long n3, unsigned long long* out) {
@@ -642,13 +729,7 @@ bool build(pgbt_tree* T, const double* xh, const double* mh) {
     // level-by-level partition
     PGB_CUDA_OR(g_err, LIB, T->perm.reserve((size_t)n), return false);
     PGB_CUDA_OR(g_err, LIB, T->perm2.reserve((size_t)n), return false);
-    {
-        std::vector<int> id((size_t)n);
-        for (int k = 0; k < n; k++) id[k] = k;
-        PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(T->perm.p, id.data(), (size_t)n * sizeof(int), cudaMemcpyHostToDevice, s),
-                    return false);
-        PGB_CUDA_OR(g_err, LIB, cudaStreamSynchronize(s), return false);
-    }
+    k_iota<<<nblk(n, 256), 256, 0, s>>>(n, T->perm.p);
     if (!grow_nodes(T, std::max<size_t>(1024, (size_t)n / 4), 0)) return false;
     {
         const int zero = 0, neg = -1;
@@ -660,32 +741,33 @@ bool build(pgbt_tree* T, const double* xh, const double* mh) {
         PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(T->bhalf.p, &R, sizeof(double), cudaMemcpyHostToDevice, s), return false);
         PGB_CUDA_OR(g_err, LIB, cudaStreamSynchronize(s), return false);
     }
+    // per-level scratch, sized once: a level has at most n nodes, at most n / (nleaf + 1) of
+    // them split, and their tiles number at most n / HT_TILE plus one per splitting node
     DevBuf<int> ntile, tile_off, tile_node, tcount, tbase, ccount, nkids, kid_off;
     DevBuf<unsigned char> oct;
+    const size_t tcap = (size_t)n / HT_TILE + (size_t)n / ((size_t)T->nleaf + 1) + 2;
     PGB_CUDA_OR(g_err, LIB, oct.reserve((size_t)n), return false);
+    PGB_CUDA_OR(g_err, LIB, ntile.reserve((size_t)n + 1), return false);
+    PGB_CUDA_OR(g_err, LIB, tile_off.reserve((size_t)n + 1), return false);
+    PGB_CUDA_OR(g_err, LIB, ccount.reserve(8 * (size_t)n), return false);
+    PGB_CUDA_OR(g_err, LIB, nkids.reserve((size_t)n + 1), return false);
+    PGB_CUDA_OR(g_err, LIB, kid_off.reserve((size_t)n + 1), return false);
+    PGB_CUDA_OR(g_err, LIB, tile_node.reserve(tcap), return false);
+    PGB_CUDA_OR(g_err, LIB, tcount.reserve(8 * tcap), return false);
+    PGB_CUDA_OR(g_err, LIB, tbase.reserve(8 * tcap), return false);
     std::vector<int> lvl = {0, 1};   // level ranges [lvl[L], lvl[L+1])
     for (int L = 0;; L++) {
         const int b = lvl[L], e = lvl[L + 1], cnt = e - b;
         if (cnt <= 0) break;
         Nodes N = bfs(T);
-        PGB_CUDA_OR(g_err, LIB, ntile.reserve((size_t)cnt + 1), return false);
-        PGB_CUDA_OR(g_err, LIB, tile_off.reserve((size_t)cnt + 1), return false);
         k_ntiles<<<nblk(cnt, 256), 256, 0, s>>>(N, b, e, L, T->nleaf, ntile.p);
         if (!excl_scan<int>(ntile.p, cnt, tile_off.p, s, stmp)) return false;
-        int ntiles = 0;
-        if (!to_host(&ntiles, tile_off.p + cnt, 1, s)) return false;
-        PGB_CUDA_OR(g_err, LIB, cudaStreamSynchronize(s), return false);
-        // children are created (child[] = -1 for the rest) even when nothing splits
-        PGB_CUDA_OR(g_err, LIB, ccount.reserve(8 * (size_t)cnt), return false);
-        PGB_CUDA_OR(g_err, LIB, nkids.reserve((size_t)cnt + 1), return false);
-        PGB_CUDA_OR(g_err, LIB, kid_off.reserve((size_t)cnt + 1), return false);
-        if (ntiles > 0) {
-            PGB_CUDA_OR(g_err, LIB, tile_node.reserve((size_t)ntiles), return false);
-            PGB_CUDA_OR(g_err, LIB, tcount.reserve(8 * (size_t)ntiles), return false);
-            PGB_CUDA_OR(g_err, LIB, tbase.reserve(8 * (size_t)ntiles), return false);
-            k_tile_nodes<<<nblk(cnt, 256), 256, 0, s>>>(b, e, tile_off.p, tile_node.p);
-            k_octants<<<ntiles, HT_NT, 0, s>>>(N, tile_node.p, tile_off.p, b, T->x.p, T->perm.p, oct.p, tcount.p);
-        }
+        // the tile kernels run on a grid that covers every possible tile; the count itself
+        // stays on the device (tile_off[cnt])
+        const unsigned tgrid = (unsigned)std::min<size_t>(tcap, (size_t)n / HT_TILE + (size_t)cnt + 2);
+        k_tile_nodes<<<nblk(cnt, 256), 256, 0, s>>>(b, e, tile_off.p, tile_node.p);
+        k_octants<<<tgrid, HT_NT, 0, s>>>(N, tile_node.p, tile_off.p, b, tile_off.p + cnt, T->x.p, T->perm.p, oct.p,
+                                         tcount.p);
         k_node_scan<<<nblk(cnt, 128), 128, 0, s>>>(N, b, e, L, T->nleaf, tile_off.p, tcount.p, tbase.p, ccount.p,
                                                   nkids.p);
         if (!excl_scan<int>(nkids.p, cnt, kid_off.p, s, stmp)) return false;
@@ -694,11 +776,13 @@ bool build(pgbt_tree* T, const double* xh, const double* mh) {
         PGB_CUDA_OR(g_err, LIB, cudaStreamSynchronize(s), return false);
         if (!grow_nodes(T, (size_t)e + nnew, (size_t)e)) return false;
         N = bfs(T);
+        // children are created (child[] = -1 for the rest) even when nothing splits
         k_children<<<nblk(cnt, 128), 128, 0, s>>>(N, b, e, L, T->nleaf, ccount.p, kid_off.p);
-        if (ntiles > 0) {
+        if (nnew > 0) {
             PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(T->perm2.p, T->perm.p, (size_t)n * sizeof(int),
                                                     cudaMemcpyDeviceToDevice, s), return false);
-            k_scatter<<<ntiles, HT_NT, 0, s>>>(N, tile_node.p, tile_off.p, b, oct.p, tbase.p, T->perm.p, T->perm2.p);
+            k_scatter<<<tgrid, HT_NT, 0, s>>>(N, tile_node.p, tile_off.p, b, tile_off.p + cnt, oct.p, tbase.p,
+                                             T->perm.p, T->perm2.p);
             std::swap(T->perm.p, T->perm2.p);
             std::swap(T->perm.n, T->perm2.n);
         }
@@ -762,15 +846,22 @@ bool build(pgbt_tree* T, const double* xh, const double* mh) {
     k_compact<<<nblk(nn, 256), 256, 0, s>>>(gflag.p, goff.p, nn, T->gnode.p);
 
     // interaction lists: count, prefix sums, fill
-    DevBuf<long long> gnp, gnc;
-    PGB_CUDA_OR(g_err, LIB, gnp.reserve((size_t)ng + 1), return false);
-    PGB_CUDA_OR(g_err, LIB, gnc.reserve((size_t)ng + 1), return false);
+    DevBuf<long long> unp, unc, uoffp, uoffc;
+    const long long nu = (long long)ng * HT_UNITS;
+    PGB_CUDA_OR(g_err, LIB, unp.reserve((size_t)nu + 1), return false);
+    PGB_CUDA_OR(g_err, LIB, unc.reserve((size_t)nu + 1), return false);
+    PGB_CUDA_OR(g_err, LIB, uoffp.reserve((size_t)nu + 1), return false);
+    PGB_CUDA_OR(g_err, LIB, uoffc.reserve((size_t)nu + 1), return false);
     PGB_CUDA_OR(g_err, LIB, T->poff.reserve((size_t)ng + 1), return false);
     PGB_CUDA_OR(g_err, LIB, T->coff.reserve((size_t)ng + 1), return false);
     const double th2 = T->theta * T->theta;
-    k_list_count<<<nblk(ng, 128), 128, 0, s>>>(P, T->gnode.p, ng, T->nleaf, th2, gnp.p, gnc.p);
-    if (!excl_scan<long long>(gnp.p, ng, T->poff.p, s, ltmp)) return false;
-    if (!excl_scan<long long>(gnc.p, ng, T->coff.p, s, ltmp)) return false;
+    DevBuf<WalkNode> wn;
+    PGB_CUDA_OR(g_err, LIB, wn.reserve((size_t)nn), return false);
+    k_walk_nodes<<<nblk(nn, 256), 256, 0, s>>>(P, nn, T->nleaf, wn.p);
+    k_list_count<<<nblk(nu, 256), 256, 0, s>>>(P, wn.p, T->gnode.p, ng, th2, unp.p, unc.p);
+    if (!excl_scan<long long>(unp.p, nu, uoffp.p, s, ltmp)) return false;
+    if (!excl_scan<long long>(unc.p, nu, uoffc.p, s, ltmp)) return false;
+    k_group_offsets<<<nblk((long long)ng + 1, 256), 256, 0, s>>>(ng, uoffp.p, uoffc.p, T->poff.p, T->coff.p);
     long long tot[2] = {0, 0};
     if (!to_host(&tot[0], T->poff.p + ng, 1, s) || !to_host(&tot[1], T->coff.p + ng, 1, s)) return false;
     PGB_CUDA_OR(g_err, LIB, cudaStreamSynchronize(s), return false);
@@ -778,8 +869,7 @@ bool build(pgbt_tree* T, const double* xh, const double* mh) {
     T->nc = tot[1];
     PGB_CUDA_OR(g_err, LIB, T->pidx.reserve((size_t)std::max(1LL, T->np)), return false);
     PGB_CUDA_OR(g_err, LIB, T->cidx.reserve((size_t)std::max(1LL, T->nc)), return false);
-    k_list_fill<<<nblk(ng, 128), 128, 0, s>>>(P, T->gnode.p, ng, T->nleaf, th2, T->poff.p, T->coff.p, T->pidx.p,
-                                              T->cidx.p);
+    k_list_fill<<<nblk(nu, 256), 256, 0, s>>>(P, wn.p, T->gnode.p, ng, th2, uoffp.p, uoffc.p, T->pidx.p, T->cidx.p);
     // force-launch records
     PGB_CUDA_OR(g_err, LIB, T->part.reserve((size_t)n), return false);
     PGB_CUDA_OR(g_err, LIB, T->cell.reserve((size_t)nn), return false);
