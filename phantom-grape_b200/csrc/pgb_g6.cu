@@ -52,8 +52,10 @@ int jmemsize() {
     static int v = env_int("PGB_G6_JMEMSIZE", 1 << 22, 1024, 1 << 26);
     return v;
 }
+// neighbour-list capacity per i-particle (the lists are sorted on the device in shared memory:
+// at most 8192 entries)
 int nbmax() {
-    static int v = env_int("PGB_G6_NBMAX", 1024, 1, 1 << 16);
+    static int v = env_int("PGB_G6_NBMAX", 1024, 1, 1 << 13);
     return v;
 }
 
@@ -550,6 +552,13 @@ void nblist_collect(int ni) {
     S.nb_error = 0;
     S.nbcounts.assign(ni, 0);
     S.nblists.assign(ni, {});
+    // every list in j-address order, addresses replaced by ids, on the device
+    int P = 1;
+    while (P < nbmax()) P <<= 1;
+    if (ni > 0) {
+        g6_nb_sort_kernel<<<ni, 256, (size_t)P * sizeof(int), S.stream>>>(S.nbc_d.p, S.nbl_d.p, nbmax(), P, S.jd.p);
+        PGB_CUDA_OR(g_err, LIB, cudaGetLastError(), return);
+    }
     if (S.nbc_h.reserve(ni) != cudaSuccess || S.nbl_h.reserve((size_t)ni * nbmax()) != cudaSuccess) {
         raise(g_err, LIB, PGB_ERR_CUDA, "pinned neighbour-list buffer allocation failed");
         return;
@@ -566,10 +575,8 @@ void nblist_collect(int ni) {
             S.nb_error = 1;
             continue;
         }
-        std::vector<int> v(S.nbl_h.p + (size_t)i * nbmax(), S.nbl_h.p + (size_t)i * nbmax() + c);
-        std::sort(v.begin(), v.end());
-        for (auto& x : v) x = S.jh.p[x].idx;
-        S.nblists[i] = std::move(v);
+        // sorted by j address and mapped to ids on the device (g6_nb_sort_kernel)
+        S.nblists[i].assign(S.nbl_h.p + (size_t)i * nbmax(), S.nbl_h.p + (size_t)i * nbmax() + c);
     }
 }
 

@@ -152,6 +152,38 @@ __global__ void g6_scatter_kernel(const G6Ptcl* __restrict__ rec, const int* __r
     if (a >= 0 && a < cap) jd[a] = rec[k];
 }
 
+// Neighbour lists after the force launch: each i's entries were appended by atomics in
+// arrival order; this kernel (one CTA per i) sorts a list of count <= nbmax entries by j address
+// in shared memory (bitonic network over P >= count slots, P a power of two) and replaces every
+// address by the id stored in the j-memory, so that the list is the reference's (j-address
+// order, gravity.c:888-900, ids).  A list longer than nbmax kept only its count and is left
+// alone (the host reports the overflow).
+__global__ void g6_nb_sort_kernel(const int* __restrict__ nb_count, int* __restrict__ nb_list, int nbmax, int P,
+                                  const G6Ptcl* __restrict__ jmem) {
+    extern __shared__ int sh_nb[];
+    const int c = nb_count[blockIdx.x];
+    if (c > nbmax || c <= 0) return;
+    int* row = nb_list + (size_t)blockIdx.x * nbmax;
+    for (int k = threadIdx.x; k < P; k += blockDim.x) sh_nb[k] = k < c ? row[k] : 0x7fffffff;
+    __syncthreads();
+    for (int size = 2; size <= P; size <<= 1)
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int k = threadIdx.x; k < P; k += blockDim.x) {
+                const int q = k ^ stride;
+                if (q > k) {
+                    const bool up = (k & size) == 0;
+                    const int a = sh_nb[k], b = sh_nb[q];
+                    if ((a > b) == up) {
+                        sh_nb[k] = b;
+                        sh_nb[q] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    for (int k = threadIdx.x; k < c; k += blockDim.x) row[k] = jmem[sh_nb[k]].idx;
+}
+
 struct G6Acc {
     float ax, ay, az, jx, jy, jz, pot;
 };
