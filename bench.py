@@ -908,6 +908,14 @@ def run_bh(args, pgb, ws, rank, local):
     W = pgb.workloads
     g5 = pgb.ffi.G5()
     g5.L.g5_open()
+    if args.profile_tree:
+        # profiling target: the GPU tree of the workload's particles built twice; no timing
+        rng = W.Rng(W.SEED0 + 3 + rank)
+        x = W._isotropic(rng, W.hernquist_radii(rng, args.bh_n, 100.0)).astype(np.float32).astype(np.float64)
+        m = np.full(args.bh_n, np.float32(1.0 / args.bh_n), np.float64)
+        for _ in range(2):
+            W.GpuTree(x, m, 0.5, 16, 256).close()
+        return {"profile": "GPU tree build", "n": args.bh_n, "builds": 2}
     bh = W.bh_hernquist(args.bh_n, seed=W.SEED0 + 3 + rank)
     ip, pp, cp, cq = bh.records()
     d_i, d_p = torch.from_numpy(ip).to(dev), torch.from_numpy(pp).to(dev)
@@ -1402,6 +1410,8 @@ def main():
     ap.add_argument("--profile-largest", action="store_true",
                     help="profiling target: set up, warm, then run the largest call's force launch 3 times "
                          "(direct, treepm: the batch's launch 4 times; bh: both launches twice)")
+    ap.add_argument("--profile-tree", action="store_true",
+                    help="profiling target (--workload bh): build the GPU tree of the workload twice and exit")
     ap.add_argument("--profile-api", action="store_true",
                     help="profiling target: four full-size drop-in API calls (48 i x N j) and exit")
     args = ap.parse_args()
