@@ -42,6 +42,22 @@ namespace {
 const char* LIB = "libpgbtree";
 ErrorSlot g_err;
 
+// Device buffers local to one call: released (cudaFree) when the call returns.
+template <class T>
+struct Scoped : DevBuf<T> {
+    Scoped() = default;
+    Scoped(const Scoped&) = delete;
+    Scoped& operator=(const Scoped&) = delete;
+    ~Scoped() { this->release(); }
+};
+template <class T>
+struct ScopedVec {
+    std::vector<DevBuf<T>> v;
+    ~ScopedVec() {
+        for (auto& b : v) b.release();
+    }
+};
+
 constexpr int HT_MAXDEPTH = 40;   // the host builder's depth cap
 constexpr int HT_TILE = 2048;     // particles per tile of the partition kernels
 constexpr int HT_NT = 256;        // threads per CTA of the tile kernels
@@ -697,8 +713,10 @@ bool to_host(V* dst, const V* src, size_t cnt, cudaStream_t s) {
 bool build(pgbt_tree* T, const double* xh, const double* mh) {
     const int n = T->n;
     cudaStream_t s = T->s;
-    std::vector<DevBuf<int>> stmp;
-    std::vector<DevBuf<long long>> ltmp;
+    ScopedVec<int> stmp_;
+    ScopedVec<long long> ltmp_;
+    std::vector<DevBuf<int>>& stmp = stmp_.v;
+    std::vector<DevBuf<long long>>& ltmp = ltmp_.v;
     PGB_CUDA_OR(g_err, LIB, T->x.reserve(3 * (size_t)n), return false);
     PGB_CUDA_OR(g_err, LIB, T->m.reserve((size_t)n), return false);
     PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(T->x.p, xh, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, s),
@@ -711,7 +729,7 @@ bool build(pgbt_tree* T, const double* xh, const double* mh) {
     PGB_CUDA_OR(g_err, LIB, cudaEventRecord(e0, s), return false);
 
     // root cube: the smallest power of two above every |coordinate|
-    DevBuf<unsigned long long> mx;
+    Scoped<unsigned long long> mx;
     PGB_CUDA_OR(g_err, LIB, mx.reserve(1), return false);
     PGB_CUDA_OR(g_err, LIB, mx.zero_fill(s), return false);
     k_maxabs<<<592, 256, 0, s>>>(T->x.p, 3LL * n, mx.p);
@@ -743,8 +761,8 @@ bool build(pgbt_tree* T, const double* xh, const double* mh) {
     }
     // per-level scratch, sized once: a level has at most n nodes, at most n / (nleaf + 1) of
     // them split, and their tiles number at most n / HT_TILE plus one per splitting node
-    DevBuf<int> ntile, tile_off, tile_node, tcount, tbase, ccount, nkids, kid_off;
-    DevBuf<unsigned char> oct;
+    Scoped<int> ntile, tile_off, tile_node, tcount, tbase, ccount, nkids, kid_off;
+    Scoped<unsigned char> oct;
     const size_t tcap = (size_t)n / HT_TILE + (size_t)n / ((size_t)T->nleaf + 1) + 2;
     PGB_CUDA_OR(g_err, LIB, oct.reserve((size_t)n), return false);
     PGB_CUDA_OR(g_err, LIB, ntile.reserve((size_t)n + 1), return false);
@@ -796,7 +814,7 @@ bool build(pgbt_tree* T, const double* xh, const double* mh) {
     Nodes N = bfs(T);
 
     // pre-order numbering: subtree sizes bottom-up, numbers top-down
-    DevBuf<int> size, pre;
+    Scoped<int> size, pre;
     PGB_CUDA_OR(g_err, LIB, size.reserve((size_t)nn), return false);
     PGB_CUDA_OR(g_err, LIB, pre.reserve((size_t)nn), return false);
     for (int L = nlev - 1; L >= 0; L--)
@@ -822,7 +840,7 @@ bool build(pgbt_tree* T, const double* xh, const double* mh) {
     k_gather<<<nblk(n, 256), 256, 0, s>>>(n, T->perm.p, T->x.p, T->m.p, T->xt.p, T->mt.p);
 
     // moments, deepest level first: the pre-order indices of each level
-    DevBuf<int> lvl_pre;
+    Scoped<int> lvl_pre;
     PGB_CUDA_OR(g_err, LIB, lvl_pre.reserve((size_t)nn), return false);
     PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(lvl_pre.p, pre.p, (size_t)nn * sizeof(int), cudaMemcpyDeviceToDevice, s),
                 return false);
@@ -833,7 +851,7 @@ bool build(pgbt_tree* T, const double* xh, const double* mh) {
 
     // groups in pre-order
     k_parent_pre<<<nblk(nn, 256), 256, 0, s>>>(P, nn, T->ppar.p);
-    DevBuf<int> gflag, goff;
+    Scoped<int> gflag, goff;
     PGB_CUDA_OR(g_err, LIB, gflag.reserve((size_t)nn), return false);
     PGB_CUDA_OR(g_err, LIB, goff.reserve((size_t)nn + 1), return false);
     k_group_flags<<<nblk(nn, 256), 256, 0, s>>>(P, T->ppar.p, nn, T->ncrit, gflag.p);
@@ -846,7 +864,7 @@ bool build(pgbt_tree* T, const double* xh, const double* mh) {
     k_compact<<<nblk(nn, 256), 256, 0, s>>>(gflag.p, goff.p, nn, T->gnode.p);
 
     // interaction lists: count, prefix sums, fill
-    DevBuf<long long> unp, unc, uoffp, uoffc;
+    Scoped<long long> unp, unc, uoffp, uoffc;
     const long long nu = (long long)ng * HT_UNITS;
     PGB_CUDA_OR(g_err, LIB, unp.reserve((size_t)nu + 1), return false);
     PGB_CUDA_OR(g_err, LIB, unc.reserve((size_t)nu + 1), return false);
@@ -855,7 +873,7 @@ bool build(pgbt_tree* T, const double* xh, const double* mh) {
     PGB_CUDA_OR(g_err, LIB, T->poff.reserve((size_t)ng + 1), return false);
     PGB_CUDA_OR(g_err, LIB, T->coff.reserve((size_t)ng + 1), return false);
     const double th2 = T->theta * T->theta;
-    DevBuf<WalkNode> wn;
+    Scoped<WalkNode> wn;
     PGB_CUDA_OR(g_err, LIB, wn.reserve((size_t)nn), return false);
     k_walk_nodes<<<nblk(nn, 256), 256, 0, s>>>(P, nn, T->nleaf, wn.p);
     k_list_count<<<nblk(nu, 256), 256, 0, s>>>(P, wn.p, T->gnode.p, ng, th2, unp.p, unc.p);
@@ -999,8 +1017,8 @@ PGB_EXPORT int pgbt_groups(pgbt_tree* T, int* first, int* count, double* centre,
     if (!T) return PGB_ERR_ARG;
     if (!ensure_device()) return PGB_ERR_NOGPU;
     const int ng = T->ng;
-    DevBuf<int> f, c;
-    DevBuf<double> ce, h;
+    Scoped<int> f, c;
+    Scoped<double> ce, h;
     PGB_CUDA_OR(g_err, LIB, f.reserve((size_t)ng + 1), return PGB_ERR_CUDA);
     PGB_CUDA_OR(g_err, LIB, c.reserve((size_t)ng + 1), return PGB_ERR_CUDA);
     PGB_CUDA_OR(g_err, LIB, ce.reserve(3 * (size_t)ng + 3), return PGB_ERR_CUDA);
@@ -1069,8 +1087,8 @@ PGB_EXPORT int pgbt_group_table(pgbt_tree* T, int* first, int* count, long long*
     if (!T) return PGB_ERR_ARG;
     if (!ensure_device()) return PGB_ERR_NOGPU;
     const int ng = T->ng;
-    DevBuf<int> f, c;
-    DevBuf<double> ce, h;
+    Scoped<int> f, c;
+    Scoped<double> ce, h;
     PGB_CUDA_OR(g_err, LIB, f.reserve((size_t)ng + 1), return PGB_ERR_CUDA);
     PGB_CUDA_OR(g_err, LIB, c.reserve((size_t)ng + 1), return PGB_ERR_CUDA);
     PGB_CUDA_OR(g_err, LIB, ce.reserve(3 * (size_t)ng + 3), return PGB_ERR_CUDA);

@@ -105,3 +105,16 @@ def test_device_records_follow_the_tree():
     np.testing.assert_array_equal(c[:, 3], s.cmass.astype(np.float32))
     np.testing.assert_array_equal(q[:, :6], s.cquad.astype(np.float32))
     np.testing.assert_array_equal(q[:, 6:], 0.0)
+
+
+def test_repeated_builds_release_their_scratch():
+    import torch
+    x, m = hernquist(1 << 18, W.SEED0 + 6)
+    W.GpuTree(x, m, 0.5, 16, 256).close()
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(5):
+        W.GpuTree(x, m, 0.5, 16, 256).close()
+    torch.cuda.synchronize()
+    free1 = torch.cuda.mem_get_info()[0]
+    assert free0 - free1 < (64 << 20), (free0, free1)
