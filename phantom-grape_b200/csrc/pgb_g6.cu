@@ -319,10 +319,13 @@ struct State {
     int predict_flag = 0;
     HostBuf<G6I> ibuf;
     HostBuf<G6Out> outh;    // mapped: the kernel writes the final results into it
+    G6Out* outh_dev = nullptr;            // its device address (looked up once per allocation)
+    const G6Out* outh_seen = nullptr;     // the allocation outh_dev belongs to
     DevBuf<int> pcnt;       // self-resetting counters of the parameter-block launches
     G6IBlock iblk;  // their i-records
     DevBuf<G6Out> spart;    // cluster rows of the small-call kernel
     HostBuf<unsigned> flags;  // mapped completion flags of the small-call kernel
+    unsigned* flags_dev = nullptr;
     unsigned seq = 0;         // sequence number of the last flagged call
     int wait_flags = 0;       // flags the next wait_results() polls (0: synchronise the stream)
     Stager<G6I, G6Out> st;
@@ -455,10 +458,9 @@ bool run_small(int nj, int ni, float eps2, bool nn, bool nbl, G6Out* out_dev) {
             PGB_CUDA_OR(g_err, LIB, S.flags.reserve(SMALL_CL, false, cudaHostAllocPortable | cudaHostAllocMapped),
                         return false);
             std::memset((void*)S.flags.p, 0, SMALL_CL * sizeof(unsigned));
+            PGB_CUDA_OR(g_err, LIB, cudaHostGetDevicePointer((void**)&S.flags_dev, S.flags.p, 0), return false);
         }
-        unsigned* dflags = nullptr;
-        PGB_CUDA_OR(g_err, LIB, cudaHostGetDevicePointer((void**)&dflags, S.flags.p, 0), return false);
-        a.done = dflags;
+        a.done = S.flags_dev;
         a.seq = ++S.seq;
         if (a.seq == 0) a.seq = ++S.seq;   // 0 is the flags' initial value
         S.wait_flags = cl;
@@ -496,8 +498,11 @@ bool wait_results() {
 // resets itself.
 bool run_force(int nj, int ni, float eps2, bool nn, bool nbl) {
     PGB_CUDA_OR(g_err, LIB, S.outh.reserve(ni, false, cudaHostAllocPortable | cudaHostAllocMapped), return false);
-    G6Out* out_dev = nullptr;
-    PGB_CUDA_OR(g_err, LIB, cudaHostGetDevicePointer((void**)&out_dev, S.outh.p, 0), return false);
+    if (S.outh_seen != S.outh.p) {
+        PGB_CUDA_OR(g_err, LIB, cudaHostGetDevicePointer((void**)&S.outh_dev, S.outh.p, 0), return false);
+        S.outh_seen = S.outh.p;
+    }
+    G6Out* out_dev = S.outh_dev;
     if (ni <= G6_SMALL_MAXI && nj > 0) return run_small(nj, ni, eps2, nn, nbl, out_dev);
     const int cfg = pick_cfg(ni);
     const bool ff = dx_ff();
@@ -1424,14 +1429,6 @@ bool hm_launch(pgb6_hermite* H, bool startup, double tend, int max_steps) {
     return true;
 }
 
-bool hm_apply_reset(pgb6_hermite* H) {
-    if (!H->clk.reset) return true;
-    hm_reset_kernel<<<(H->n + 255) / 256, 256, 0, H->s>>>(H->P, H->W.clk);
-    PGB_CUDA_OR(g_err, LIB, cudaGetLastError(), return false);
-    H->clk.reset = 0;
-    return true;
-}
-
 void hm_free(pgb6_hermite* H) {
     if (H->s) cudaStreamSynchronize(H->s);
     H->state.release();
@@ -1539,7 +1536,6 @@ PGB_EXPORT int pgb6_hermite_get(pgb6_hermite* H, double* t, double* dt, double (
     }
     if (!ensure_device()) return PGB_ERR_NOGPU;
     std::lock_guard<std::mutex> g(H->mu);
-    if (!hm_apply_reset(H)) return PGB_ERR_CUDA;
     const size_t n = (size_t)H->n;
     struct {
         void* dst;

@@ -59,8 +59,8 @@ struct HmState {
 
 // The integrator's clock and counters in device memory (banana01.c:119-179 bookkeeping): the
 // last step's block time and active count, the global time after it (t_mod * dtmax + t_gl, or
-// t_mod * dtmax after a reset), the completed dtmax intervals, the pending reset_time, the
-// particle / block steps and the device time of the force phases.
+// t_mod * dtmax after a reset), the completed dtmax intervals, the particle / block steps, the
+// pair interactions and the steps by force decomposition.
 struct HmClock {
     double t_gl;
     double time;
@@ -68,7 +68,6 @@ struct HmClock {
     long long force_pairs;
     long long variant_steps[5];   // steps by force decomposition (i-tile 16, 32, 64, 128, 512)
     int t_mod;
-    int reset;
     int ni;       // the last step's active count
     int nch;      // its force decomposition: j-chunks and i-tile
     int itile;
@@ -619,14 +618,6 @@ __global__ void __launch_bounds__(HM_NT, 2) hm_run_kernel(const HmRun R) {
         E++;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) W.sync->step = E;
-}
-
-// reset_time (timestep.c:127-135) on its own, for reads of the state between steps: applies
-// the pending reset and clears it.
-__global__ void hm_reset_kernel(HmState P, HmClock* clk) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < P.n) P.t[i] = 0.0;
-    if (i == 0) clk->reset = 0;
 }
 
 // Kinetic and potential energy (calc_energy.c:9-33): ek = sum m v^2 / 2, ew = sum m pot / 2.
