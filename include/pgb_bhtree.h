@@ -22,6 +22,9 @@ typedef struct pgbt_tree pgbt_tree;
 /* n particles (x: n x 3, m: n, host arrays), opening angle theta, leaf size nleaf, group size
  * ncrit; NULL on bad arguments or failure (message in pgbt_last_error) */
 pgbt_tree *pgbt_build(int n, const double *x, const double *m, double theta, int nleaf, int ncrit);
+/* rebuild for n new particles with the same parameters, reusing the tree's device buffers (a
+ * code that builds every step saves the allocations); PGB_OK or an error code */
+int  pgbt_rebuild(pgbt_tree *tree, int n, const double *x, const double *m);
 void pgbt_free(pgbt_tree *tree);
 int  pgbt_n(const pgbt_tree *tree);
 int  pgbt_ngroups(const pgbt_tree *tree);

@@ -42,20 +42,13 @@ namespace {
 const char* LIB = "libpgbtree";
 ErrorSlot g_err;
 
-// Device buffers local to one call: released (cudaFree) when the call returns.
+// Device buffers local to one accessor call: released (cudaFree) when the call returns.
 template <class T>
 struct Scoped : DevBuf<T> {
     Scoped() = default;
     Scoped(const Scoped&) = delete;
     Scoped& operator=(const Scoped&) = delete;
     ~Scoped() { this->release(); }
-};
-template <class T>
-struct ScopedVec {
-    std::vector<DevBuf<T>> v;
-    ~ScopedVec() {
-        for (auto& b : v) b.release();
-    }
 };
 
 constexpr int HT_MAXDEPTH = 40;   // the host builder's depth cap
@@ -684,6 +677,15 @@ struct pgbt_tree {
     DevBuf<int> pidx, cidx;
     // force-launch records
     DevBuf<float4> part, cell, cquad;
+    // build scratch, kept for the next pgbt_rebuild (released by pgbt_free)
+    std::vector<DevBuf<int>> stmp;
+    std::vector<DevBuf<long long>> ltmp;
+    DevBuf<unsigned long long> mx;
+    DevBuf<int> ntile, tile_off, tile_node, tcount, tbase, ccount, nkids, kid_off;
+    DevBuf<unsigned char> oct;
+    DevBuf<int> size, pre, lvl_pre, gflag, goff;
+    DevBuf<long long> unp, unc, uoffp, uoffc;
+    DevBuf<unsigned char> wn;   // WalkNode records
 };
 
 namespace {
@@ -713,10 +715,8 @@ bool to_host(V* dst, const V* src, size_t cnt, cudaStream_t s) {
 bool build(pgbt_tree* T, const double* xh, const double* mh) {
     const int n = T->n;
     cudaStream_t s = T->s;
-    ScopedVec<int> stmp_;
-    ScopedVec<long long> ltmp_;
-    std::vector<DevBuf<int>>& stmp = stmp_.v;
-    std::vector<DevBuf<long long>>& ltmp = ltmp_.v;
+    std::vector<DevBuf<int>>& stmp = T->stmp;
+    std::vector<DevBuf<long long>>& ltmp = T->ltmp;
     PGB_CUDA_OR(g_err, LIB, T->x.reserve(3 * (size_t)n), return false);
     PGB_CUDA_OR(g_err, LIB, T->m.reserve((size_t)n), return false);
     PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(T->x.p, xh, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, s),
@@ -729,7 +729,7 @@ bool build(pgbt_tree* T, const double* xh, const double* mh) {
     PGB_CUDA_OR(g_err, LIB, cudaEventRecord(e0, s), return false);
 
     // root cube: the smallest power of two above every |coordinate|
-    Scoped<unsigned long long> mx;
+    DevBuf<unsigned long long>& mx = T->mx;
     PGB_CUDA_OR(g_err, LIB, mx.reserve(1), return false);
     PGB_CUDA_OR(g_err, LIB, mx.zero_fill(s), return false);
     k_maxabs<<<592, 256, 0, s>>>(T->x.p, 3LL * n, mx.p);
@@ -761,8 +761,9 @@ bool build(pgbt_tree* T, const double* xh, const double* mh) {
     }
     // per-level scratch, sized once: a level has at most n nodes, at most n / (nleaf + 1) of
     // them split, and their tiles number at most n / HT_TILE plus one per splitting node
-    Scoped<int> ntile, tile_off, tile_node, tcount, tbase, ccount, nkids, kid_off;
-    Scoped<unsigned char> oct;
+    DevBuf<int>&ntile = T->ntile, &tile_off = T->tile_off, &tile_node = T->tile_node, &tcount = T->tcount,
+                &tbase = T->tbase, &ccount = T->ccount, &nkids = T->nkids, &kid_off = T->kid_off;
+    DevBuf<unsigned char>& oct = T->oct;
     const size_t tcap = (size_t)n / HT_TILE + (size_t)n / ((size_t)T->nleaf + 1) + 2;
     PGB_CUDA_OR(g_err, LIB, oct.reserve((size_t)n), return false);
     PGB_CUDA_OR(g_err, LIB, ntile.reserve((size_t)n + 1), return false);
@@ -814,7 +815,7 @@ bool build(pgbt_tree* T, const double* xh, const double* mh) {
     Nodes N = bfs(T);
 
     // pre-order numbering: subtree sizes bottom-up, numbers top-down
-    Scoped<int> size, pre;
+    DevBuf<int>&size = T->size, &pre = T->pre;
     PGB_CUDA_OR(g_err, LIB, size.reserve((size_t)nn), return false);
     PGB_CUDA_OR(g_err, LIB, pre.reserve((size_t)nn), return false);
     for (int L = nlev - 1; L >= 0; L--)
@@ -840,7 +841,7 @@ bool build(pgbt_tree* T, const double* xh, const double* mh) {
     k_gather<<<nblk(n, 256), 256, 0, s>>>(n, T->perm.p, T->x.p, T->m.p, T->xt.p, T->mt.p);
 
     // moments, deepest level first: the pre-order indices of each level
-    Scoped<int> lvl_pre;
+    DevBuf<int>& lvl_pre = T->lvl_pre;
     PGB_CUDA_OR(g_err, LIB, lvl_pre.reserve((size_t)nn), return false);
     PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(lvl_pre.p, pre.p, (size_t)nn * sizeof(int), cudaMemcpyDeviceToDevice, s),
                 return false);
@@ -851,7 +852,7 @@ bool build(pgbt_tree* T, const double* xh, const double* mh) {
 
     // groups in pre-order
     k_parent_pre<<<nblk(nn, 256), 256, 0, s>>>(P, nn, T->ppar.p);
-    Scoped<int> gflag, goff;
+    DevBuf<int>&gflag = T->gflag, &goff = T->goff;
     PGB_CUDA_OR(g_err, LIB, gflag.reserve((size_t)nn), return false);
     PGB_CUDA_OR(g_err, LIB, goff.reserve((size_t)nn + 1), return false);
     k_group_flags<<<nblk(nn, 256), 256, 0, s>>>(P, T->ppar.p, nn, T->ncrit, gflag.p);
@@ -864,7 +865,7 @@ bool build(pgbt_tree* T, const double* xh, const double* mh) {
     k_compact<<<nblk(nn, 256), 256, 0, s>>>(gflag.p, goff.p, nn, T->gnode.p);
 
     // interaction lists: count, prefix sums, fill
-    Scoped<long long> unp, unc, uoffp, uoffc;
+    DevBuf<long long>&unp = T->unp, &unc = T->unc, &uoffp = T->uoffp, &uoffc = T->uoffc;
     const long long nu = (long long)ng * HT_UNITS;
     PGB_CUDA_OR(g_err, LIB, unp.reserve((size_t)nu + 1), return false);
     PGB_CUDA_OR(g_err, LIB, unc.reserve((size_t)nu + 1), return false);
@@ -873,10 +874,10 @@ bool build(pgbt_tree* T, const double* xh, const double* mh) {
     PGB_CUDA_OR(g_err, LIB, T->poff.reserve((size_t)ng + 1), return false);
     PGB_CUDA_OR(g_err, LIB, T->coff.reserve((size_t)ng + 1), return false);
     const double th2 = T->theta * T->theta;
-    Scoped<WalkNode> wn;
-    PGB_CUDA_OR(g_err, LIB, wn.reserve((size_t)nn), return false);
-    k_walk_nodes<<<nblk(nn, 256), 256, 0, s>>>(P, nn, T->nleaf, wn.p);
-    k_list_count<<<nblk(nu, 256), 256, 0, s>>>(P, wn.p, T->gnode.p, ng, th2, unp.p, unc.p);
+    PGB_CUDA_OR(g_err, LIB, T->wn.reserve((size_t)nn * sizeof(WalkNode)), return false);
+    WalkNode* wn = reinterpret_cast<WalkNode*>(T->wn.p);
+    k_walk_nodes<<<nblk(nn, 256), 256, 0, s>>>(P, nn, T->nleaf, wn);
+    k_list_count<<<nblk(nu, 256), 256, 0, s>>>(P, wn, T->gnode.p, ng, th2, unp.p, unc.p);
     if (!excl_scan<long long>(unp.p, nu, uoffp.p, s, ltmp)) return false;
     if (!excl_scan<long long>(unc.p, nu, uoffc.p, s, ltmp)) return false;
     k_group_offsets<<<nblk((long long)ng + 1, 256), 256, 0, s>>>(ng, uoffp.p, uoffc.p, T->poff.p, T->coff.p);
@@ -887,7 +888,7 @@ bool build(pgbt_tree* T, const double* xh, const double* mh) {
     T->nc = tot[1];
     PGB_CUDA_OR(g_err, LIB, T->pidx.reserve((size_t)std::max(1LL, T->np)), return false);
     PGB_CUDA_OR(g_err, LIB, T->cidx.reserve((size_t)std::max(1LL, T->nc)), return false);
-    k_list_fill<<<nblk(nu, 256), 256, 0, s>>>(P, wn.p, T->gnode.p, ng, th2, uoffp.p, uoffc.p, T->pidx.p, T->cidx.p);
+    k_list_fill<<<nblk(nu, 256), 256, 0, s>>>(P, wn, T->gnode.p, ng, th2, uoffp.p, uoffc.p, T->pidx.p, T->cidx.p);
     // force-launch records
     PGB_CUDA_OR(g_err, LIB, T->part.reserve((size_t)n), return false);
     PGB_CUDA_OR(g_err, LIB, T->cell.reserve((size_t)nn), return false);
@@ -899,14 +900,6 @@ bool build(pgbt_tree* T, const double* xh, const double* mh) {
     cudaEventElapsedTime(&T->build_ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    // the breadth-first arrays are no longer needed
-    T->bfirst.release();
-    T->bcount.release();
-    T->bparent.release();
-    T->bchild.release();
-    T->bc.release();
-    T->bhalf.release();
-    T->perm2.release();
     return true;
 }
 
@@ -923,6 +916,18 @@ void tree_free(pgbt_tree* T) {
     T->part.release();
     T->cell.release();
     T->cquad.release();
+    for (auto& b : T->stmp) b.release();
+    for (auto& b : T->ltmp) b.release();
+    T->mx.release();
+    DevBuf<int>* sc[] = {&T->ntile, &T->tile_off, &T->tile_node, &T->tcount, &T->tbase, &T->ccount, &T->nkids,
+                         &T->kid_off, &T->size, &T->pre, &T->lvl_pre, &T->gflag, &T->goff};
+    for (auto* b : sc) b->release();
+    T->oct.release();
+    T->wn.release();
+    T->unp.release();
+    T->unc.release();
+    T->uoffp.release();
+    T->uoffc.release();
     if (T->s) cudaStreamDestroy(T->s);
     delete T;
 }
@@ -972,6 +977,19 @@ PGB_EXPORT pgbt_tree* pgbt_build(int n, const double* x, const double* m, double
         return nullptr;
     }
     return T;
+}
+
+// Rebuild an existing tree for n new particles (same theta, nleaf, ncrit), reusing its device
+// buffers: a code that builds a tree every step avoids the allocations of a fresh build.
+// Returns PGB_OK, or an error code (the tree is then unusable: pgbt_free it).
+PGB_EXPORT int pgbt_rebuild(pgbt_tree* T, int n, const double* x, const double* m) {
+    if (!T || n <= 0 || !x || !m) {
+        raise(g_err, LIB, PGB_ERR_ARG, "pgbt_rebuild: bad arguments (n %d)", n);
+        return PGB_ERR_ARG;
+    }
+    if (!ensure_device()) return PGB_ERR_NOGPU;
+    T->n = n;
+    return build(T, x, m) ? PGB_OK : PGB_ERR_CUDA;
 }
 
 PGB_EXPORT void pgbt_free(pgbt_tree* T) {

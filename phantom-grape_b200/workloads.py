@@ -488,6 +488,17 @@ class GpuTree:
             raise RuntimeError(f"pgbt_build failed: {buf.value.decode()}")
         self.build_ms = L.pgbt_build_ms(self.h)
 
+    def rebuild(self, x: np.ndarray, m: np.ndarray):
+        """Rebuild the tree for new particles (same parameters), reusing its device buffers."""
+        import ctypes as C
+        dp = C.POINTER(C.c_double)
+        self.L.pgbt_rebuild.argtypes = [C.c_void_p, C.c_int, dp, dp]
+        self.x = np.ascontiguousarray(x, np.float64)
+        self.m = np.ascontiguousarray(m, np.float64)
+        if self.L.pgbt_rebuild(self.h, len(self.m), self.x.ctypes.data_as(dp), self.m.ctypes.data_as(dp)):
+            raise RuntimeError("pgbt_rebuild failed")
+        self.build_ms = self.L.pgbt_build_ms(self.h)
+
     def set(self) -> BHSet:
         return _bh_read(self.L, "pgbt_", self.h, self.x, self.m, *self.args)
 

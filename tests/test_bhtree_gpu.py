@@ -118,3 +118,21 @@ def test_repeated_builds_release_their_scratch():
     torch.cuda.synchronize()
     free1 = torch.cuda.mem_get_info()[0]
     assert free0 - free1 < (64 << 20), (free0, free1)
+
+
+def test_rebuild_reuses_the_tree_object():
+    """pgbt_rebuild on other particles (more, then fewer) gives the host builder's tree."""
+    t = None
+    try:
+        for n, seed in ((1 << 14, 7), (1 << 16, 8), (3000, 9)):
+            x, m = hernquist(n, W.SEED0 + seed)
+            if t is None:
+                t = W.GpuTree(x, m, 0.5, 16, 256)
+            else:
+                t.rebuild(x, m)
+            dev, host = t.set(), W.bh_tree(x, m, 0.5, 16, 256)
+            for f in FIELDS:
+                np.testing.assert_array_equal(getattr(dev, f), getattr(host, f), err_msg=f"{f} (n {n})")
+    finally:
+        if t is not None:
+            t.close()
