@@ -973,10 +973,25 @@ void plan_items(pgb5_plan* P) {
         P->rows += plan_item(P->tasks, P->groups, items[4 * k], ni, items[4 * k + 2], nj, itile, (int)jc, P->rows);
         P->interactions += (long long)ni * nj;
     }
-    // longest tasks first (persistent CTAs then finish together)
-    std::stable_sort(P->tasks.begin(), P->tasks.end(), [](const Task& a, const Task& b) {
-        return (long long)a.ni * a.nj > (long long)b.ni * b.nj;
-    });
+    // longest tasks first (persistent CTAs then finish together): a stable counting sort by the
+    // power of two of the work, largest first -- linear in the task count, which matters for
+    // plans made every step (a tree code's 1e5 tasks)
+    {
+        auto cls = [](const Task& t) {
+            const unsigned long long w = (unsigned long long)t.ni * (unsigned long long)t.nj;
+            return w ? 63 - __builtin_clzll(w) : 0;
+        };
+        size_t cnt[64] = {0};
+        for (const Task& t : P->tasks) cnt[cls(t)]++;
+        size_t pos[64], run = 0;
+        for (int c = 63; c >= 0; c--) {
+            pos[c] = run;
+            run += cnt[c];
+        }
+        std::vector<Task> sorted(P->tasks.size());
+        for (const Task& t : P->tasks) sorted[pos[cls(t)]++] = t;
+        P->tasks.swap(sorted);
+    }
 }
 
 // Autotune results by batch shape (kind, item count, largest item), shared by later plans.
