@@ -1007,7 +1007,9 @@ def run_bh(args, pgb, ws, rank, local):
     # forces in host memory: the tree, moments, groups and lists built on the GPU
     # (lib/libpgbtree.so), both plans created from its group table, both launches, both results
     # read back -- every step; host clock
-    x_in, m_in = np.empty_like(bh.x), np.empty_like(bh.m)
+    # the step's inputs in pinned host memory (input order), as a code would keep its particles
+    x_in = torch.empty(bh.x.shape, dtype=torch.float64).pin_memory().numpy()
+    m_in = torch.empty(bh.m.shape, dtype=torch.float64).pin_memory().numpy()
     x_in[bh.perm], m_in[bh.perm] = bh.x, bh.m
     t0 = time.perf_counter()
     W.bh_tree(x_in, m_in, bh.theta, bh.nleaf, bh.ncrit, bh.eps)
