@@ -53,7 +53,8 @@ SM_COUNT = 148
 # (dram__bytes_read.sum + dram__bytes_write.sum); the bench cannot run ncu itself.
 G5_CFG_NAMES = ["128x4", "256x2", "512x2", "1024x1", "384x2", "128x2", "128x1", "64x1"]   # pgb5 configurations (threads x i/thread)
 PROFILED_TRAFFIC = {
-    "hermite": {"bytes": 25_623_040, "source": "profiles/g6_kernel_hermite_65536x65536.md (256x2 configuration)"},
+    "hermite": {"bytes": 6_464_000 + 18_805_504,
+                "source": "profiles/g6_kernel_hermite_65536x65536.md (256x2 configuration, paired accumulations)"},
     "direct": {"bytes": 542_464, "pairs": 268_435_456, "source": "profiles/g5_kernels_direct_treepm_bh.md (1024x1)"},
     "treepm": {"bytes": 587_407_104, "pairs": 4_463_983_086,
                "source": "profiles/g5_kernels_direct_treepm_bh.md (128x1)"},

@@ -110,6 +110,82 @@ __device__ __forceinline__ void g5_interact(const float4* sj, int j, float xi, f
     }
 }
 
+__device__ __forceinline__ float& lane_of(float2& v, int k) { return k ? v.y : v.x; }
+
+// Two i-particles of a thread (configurations with IPT >= 2) against one j record: the per-i
+// chains exactly as g5_interact / g5_table_pair, the accumulations of the two i issued as paired
+// FP32 instructions (FFMA2 / FADD2, each lane rounded as the scalar instruction: results
+// bit-identical to two g5_interact calls).  a2[c] holds component c of both i.
+template <int KIND, int NT>
+__device__ __forceinline__ void g5_interact2(const float4* sj, int j, const float* xi, const float* yi,
+                                             const float* zi, const float* ei, const float2* tab, int shift,
+                                             float r2cut, float2 (&a2)[4]) {
+    const float4 J = sj[j];
+    float dx[2], dy[2], dz[2], s0[2], s3[2];
+    if constexpr (KIND == G5_QUAD) {
+        const float4 Q0 = sj[NT + 2 * j];
+        const float4 Q1 = sj[NT + 2 * j + 1];
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            dx[k] = J.x - xi[k];
+            dy[k] = J.y - yi[k];
+            dz[k] = J.z - zi[k];
+            float r2 = __fmaf_rn(dz[k], dz[k], __fmaf_rn(dy[k], dy[k], __fmaf_rn(dx[k], dx[k], ei[k])));
+            float q = minus2_over_r(r2);
+            float ri = -0.5f * q;
+            float ri2 = ri * ri;
+            float phi_p = J.w * ri;
+            float qx = __fmaf_rn(Q0.z, dz[k], __fmaf_rn(Q0.y, dy[k], Q0.x * dx[k]));
+            float qy = __fmaf_rn(Q1.x, dz[k], __fmaf_rn(Q0.w, dy[k], Q0.y * dx[k]));
+            float qz = __fmaf_rn(Q1.y, dz[k], __fmaf_rn(Q1.x, dy[k], Q0.z * dx[k]));
+            float drqdr = __fmaf_rn(dz[k], qz, __fmaf_rn(dy[k], qy, dx[k] * qx));
+            float dr5i = ri2 * ri2 * ri;
+            float phi_q = 0.5f * dr5i * drqdr;
+            s3[k] = phi_p + phi_q;
+            s0[k] = __fmaf_rn(5.0f, phi_q, phi_p) * ri2;   // mr3i
+            // the quadrupole terms of the scalar form's inner FMA, per i
+            lane_of(a2[0], k) = __fmaf_rn(-qx, dr5i, lane_of(a2[0], k));
+            lane_of(a2[1], k) = __fmaf_rn(-qy, dr5i, lane_of(a2[1], k));
+            lane_of(a2[2], k) = __fmaf_rn(-qz, dr5i, lane_of(a2[2], k));
+        }
+        const float2 M = make_float2(s0[0], s0[1]);
+        a2[0] = __ffma2_rn(make_float2(dx[0], dx[1]), M, a2[0]);
+        a2[1] = __ffma2_rn(make_float2(dy[0], dy[1]), M, a2[1]);
+        a2[2] = __ffma2_rn(make_float2(dz[0], dz[1]), M, a2[2]);
+        a2[3] = __fadd2_rn(a2[3], make_float2(s3[0], s3[1]));
+    } else {
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            dx[k] = J.x - xi[k];
+            dy[k] = J.y - yi[k];
+            dz[k] = J.z - zi[k];
+            if constexpr (KIND == G5_TABLE) {
+                float s = __fmaf_rn(dz[k], dz[k], __fmaf_rn(dy[k], dy[k], __fmaf_rn(dx[k], dx[k], 2.0f)));
+                s = fminf(s, r2cut);
+                unsigned u = __float_as_uint(s);
+                float node = __uint_as_float((u >> shift) << shift);
+                float2 T = tab[u >> shift];
+                float f = __fmaf_rn(s - node, T.y, T.x);
+                s0[k] = J.w * f;
+            } else {
+                float e = ei[k];
+                if constexpr (KIND == G5_SYMMETRIC) e += sj[NT + j].x;
+                float r2 = __fmaf_rn(dz[k], dz[k], __fmaf_rn(dy[k], dy[k], __fmaf_rn(dx[k], dx[k], e)));
+                float q = minus2_over_r(r2);
+                float mq = J.w * q;
+                float q2 = q * q;
+                s3[k] = mq;
+                s0[k] = mq * q2;
+            }
+        }
+        const float2 M = make_float2(s0[0], s0[1]);
+        a2[0] = __ffma2_rn(M, make_float2(dx[0], dx[1]), a2[0]);
+        a2[1] = __ffma2_rn(M, make_float2(dy[0], dy[1]), a2[1]);
+        a2[2] = __ffma2_rn(M, make_float2(dz[0], dz[1]), a2[2]);
+        if constexpr (KIND != G5_TABLE) a2[3] = __fadd2_rn(a2[3], make_float2(s3[0], s3[1]));
+    }
+}
+
 // Final scaling of the FP64 sums into (acc, pot_raw).
 template <int KIND>
 __device__ __forceinline__ double4 g5_finish(double4 s, double ascale) {
@@ -183,6 +259,24 @@ __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
                 }
             }
             __syncthreads();
+            if constexpr (IPT % 2 == 0) {
+                float2 a2[IPT / 2][4];
+#pragma unroll
+                for (int p = 0; p < IPT / 2; p++) a2[p][0] = a2[p][1] = a2[p][2] = a2[p][3] = make_float2(0.f, 0.f);
+#pragma unroll 4
+                for (int j = 0; j < nt; j++) {
+#pragma unroll
+                    for (int p = 0; p < IPT / 2; p++)
+                        g5_interact2<KIND, NT>(sj, j, xi + 2 * p, yi + 2 * p, zi + 2 * p, ei + 2 * p, tab, shift,
+                                               A.r2cut, a2[p]);
+                }
+#pragma unroll
+                for (int k = 0; k < IPT; k++) {
+#pragma unroll
+                    for (int c = 0; c < 4; c++) S[k][c] += (double)lane_of(a2[k / 2][c], k % 2);
+                }
+                continue;
+            }
             float a[IPT][4];
 #pragma unroll
             for (int k = 0; k < IPT; k++) a[k][0] = a[k][1] = a[k][2] = a[k][3] = 0.f;

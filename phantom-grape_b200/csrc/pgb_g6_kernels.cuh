@@ -242,6 +242,62 @@ __device__ __forceinline__ void g6_pair(const G6PredJ& J, int jadr, const Pos3& 
     a.jz = __fmaf_rn(mq3, __fmaf_rn(c, dz, dvz), a.jz);
 }
 
+// Two i-particles of a thread against one j: the per-i chains exactly as in g6_pair, with the
+// accumulations (acc and both jerk products: nine FMAs for the two i) issued as paired FP32
+// instructions (FFMA2: each lane rounded exactly as the scalar FFMA, so the results are
+// bit-identical to g6_pair).  Paired instructions execute on the heavy half of the FMA pipe
+// only; pairing the accumulations alone lowers the issued instructions without making that half
+// the bottleneck (pairing the r^2 and dx.dv chains as well measured slower).
+struct G6Acc2 {
+    float2 ax, ay, az, jx, jy, jz;
+    float pot[2];
+};
+
+template <bool FF, bool NN, bool NBL>
+__device__ __forceinline__ void g6_pair2(const G6PredJ& J, int jadr, const Pos3* I, const float* vxi,
+                                         const float* vyi, const float* vzi, const int* idi, float eps2,
+                                         const float* hinv, G6Acc2& a, float* kmin, int* kadr, int* const* nbc,
+                                         int* const* nbl, int nbmax) {
+    float dx[2], dy[2], dz[2], dvx[2], dvy[2], dvz[2], mq3[2], c[2];
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        dx[k] = rel1<FF>(J.p, I[k], 0);
+        dy[k] = rel1<FF>(J.p, I[k], 1);
+        dz[k] = rel1<FF>(J.p, I[k], 2);
+        dvx[k] = J.vx - vxi[k];
+        dvy[k] = J.vy - vyi[k];
+        dvz[k] = J.vz - vzi[k];
+        float r2 = __fmaf_rn(dz[k], dz[k], __fmaf_rn(dy[k], dy[k], __fmaf_rn(dx[k], dx[k], eps2)));
+        float q = minus2_over_r(r2);
+        q = (J.id == idi[k]) ? 0.0f : q;
+        if constexpr (NN) {
+            bool lt = q < kmin[k];
+            kmin[k] = lt ? q : kmin[k];
+            kadr[k] = lt ? jadr : kadr[k];
+        }
+        if constexpr (NBL) {
+            if (q <= hinv[k]) {
+                int slot = atomicAdd(nbc[k], 1);
+                if (slot < nbmax) nbl[k][slot] = jadr;
+            }
+        }
+        a.pot[k] = __fmaf_rn(J.m, q, a.pot[k]);
+        float rv = __fmaf_rn(dz[k], dvz[k], __fmaf_rn(dy[k], dvy[k], dx[k] * dvx[k]));
+        float mq = J.m * q;
+        float q2 = q * q;
+        mq3[k] = mq * q2;
+        c[k] = -0.75f * q2 * rv;
+    }
+    const float2 M = make_float2(mq3[0], mq3[1]), C = make_float2(c[0], c[1]);
+    const float2 DX = make_float2(dx[0], dx[1]), DY = make_float2(dy[0], dy[1]), DZ = make_float2(dz[0], dz[1]);
+    a.ax = __ffma2_rn(M, DX, a.ax);
+    a.ay = __ffma2_rn(M, DY, a.ay);
+    a.az = __ffma2_rn(M, DZ, a.az);
+    a.jx = __ffma2_rn(M, __ffma2_rn(C, DX, make_float2(dvx[0], dvx[1])), a.jx);
+    a.jy = __ffma2_rn(M, __ffma2_rn(C, DY, make_float2(dvy[0], dvy[1])), a.jy);
+    a.jz = __ffma2_rn(M, __ffma2_rn(C, DZ, make_float2(dvz[0], dvz[1])), a.jz);
+}
+
 __device__ __forceinline__ G6Out g6_finish(const G6Out& s) {
     G6Out o;
     o.ax = -0.125 * s.ax;
@@ -413,6 +469,44 @@ __device__ __forceinline__ void g6_task(const G6Args& A, const Task& T, unsigned
         __syncthreads();
         if (threadIdx.x < nt) sj[threadIdx.x] = A.jpred[T.j0 + jt + threadIdx.x];
         __syncthreads();
+        if constexpr (IPT % 2 == 0) {
+            constexpr int NP = IPT / 2;
+            G6Acc2 a[NP];
+            const float2 z2 = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int p = 0; p < NP; p++) a[p] = G6Acc2{z2, z2, z2, z2, z2, z2, {0.f, 0.f}};
+            int* nbc[IPT];
+            int* nbl[IPT];
+#pragma unroll
+            for (int k = 0; k < IPT; k++) {
+                int li = slot + k * ISL;
+                int gi = T.i0 + (li < T.ni ? li : 0);
+                nbc[k] = NBL ? A.nb_count + gi : nullptr;
+                nbl[k] = NBL ? A.nb_list + (size_t)gi * A.nb_maxlen : nullptr;
+            }
+#pragma unroll 2
+            for (int j = 0; j < nt; j++) {
+                const G6PredJ J = sj[j];
+                const int jadr = T.j0 + jt + j;
+#pragma unroll
+                for (int p = 0; p < NP; p++)
+                    g6_pair2<FF, NN, NBL>(J, jadr, pi + 2 * p, vxi + 2 * p, vyi + 2 * p, vzi + 2 * p, idi + 2 * p,
+                                          A.eps2, hinv + 2 * p, a[p], kmin + 2 * p, kadr + 2 * p, nbc + 2 * p,
+                                          nbl + 2 * p, A.nb_maxlen);
+            }
+#pragma unroll
+            for (int p = 0; p < NP; p++) {
+                const float2* v = &a[p].ax;
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const int k = 2 * p + h;
+#pragma unroll
+                    for (int c = 0; c < 6; c++) S[k][c] += (double)(h ? v[c].y : v[c].x);
+                    S[k][6] += (double)a[p].pot[h];
+                }
+            }
+            continue;
+        }
         G6Acc a[IPT];
 #pragma unroll
         for (int k = 0; k < IPT; k++) a[k] = G6Acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
