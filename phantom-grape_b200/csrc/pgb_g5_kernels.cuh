@@ -199,6 +199,26 @@ __device__ __forceinline__ double4 add4(double4 a, double4 b) {
     return make_double4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
 }
 
+// One lane's pass over a j tile: records first, first + STRIDE, ... < nt (STRIDE 0: the
+// runtime stride `nl`), accumulated in that order.
+template <int KIND, int NT, int IPT, int STRIDE>
+__device__ __forceinline__ void g5_jloop(const float4* sj, int first, int nt, const float* xi, const float* yi,
+                                         const float* zi, const float* ei, const float2* tab, int shift, float r2cut,
+                                         float (&a)[IPT][4], int nl = 1) {
+    const int step = STRIDE > 0 ? STRIDE : nl;
+#pragma unroll 4
+    for (int j = first; j < nt; j += step) {
+        if constexpr (KIND == G5_TABLE) {
+            const float4 J = sj[j];
+#pragma unroll
+            for (int k = 0; k < IPT; k++) g5_table_pair(J, xi[k], yi[k], zi[k], tab, shift, r2cut, a[k]);
+        } else {
+#pragma unroll
+            for (int k = 0; k < IPT; k++) g5_interact<KIND, NT>(sj, j, xi[k], yi[k], zi[k], ei[k], a[k]);
+        }
+    }
+}
+
 template <int KIND, int NT, int IPT>
 __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
     constexpr int W = JWords<KIND>::n;   // 16-byte words per j record
@@ -280,17 +300,12 @@ __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
             float a[IPT][4];
 #pragma unroll
             for (int k = 0; k < IPT; k++) a[k][0] = a[k][1] = a[k][2] = a[k][3] = 0.f;
-#pragma unroll 4
-            for (int j = lane; j < nt; j += (LANES ? nl : 1)) {
-                if constexpr (KIND == G5_TABLE) {
-                    const float4 J = sj[j];
-#pragma unroll
-                    for (int k = 0; k < IPT; k++) g5_table_pair(J, xi[k], yi[k], zi[k], tab, shift, A.r2cut, a[k]);
-                } else {
-#pragma unroll
-                    for (int k = 0; k < IPT; k++) g5_interact<KIND, NT>(sj, j, xi[k], yi[k], zi[k], ei[k], a[k]);
-                }
-            }
+            // the lane stride as a template constant: the unrolled loop then addresses its j
+            // records with immediate offsets (64-thread CTAs have 1, 2 or 4 lanes)
+            if (!LANES || nl == 1) g5_jloop<KIND, NT, IPT, 1>(sj, lane, nt, xi, yi, zi, ei, tab, shift, A.r2cut, a);
+            else if (nl == 2) g5_jloop<KIND, NT, IPT, 2>(sj, lane, nt, xi, yi, zi, ei, tab, shift, A.r2cut, a);
+            else if (nl == 4) g5_jloop<KIND, NT, IPT, 4>(sj, lane, nt, xi, yi, zi, ei, tab, shift, A.r2cut, a);
+            else g5_jloop<KIND, NT, IPT, 0>(sj, lane, nt, xi, yi, zi, ei, tab, shift, A.r2cut, a, nl);
 #pragma unroll
             for (int k = 0; k < IPT; k++) {
                 S[k][0] += (double)a[k][0];
