@@ -59,7 +59,7 @@ PROFILED_TRAFFIC = {
     "treepm": {"bytes": 587_407_104, "pairs": 4_463_983_086,
                "source": "profiles/g5_kernels_direct_treepm_bh.md (128x1)"},
     # captured at N = 2^20 (both launches of a step); scaled to the run's pairs
-    "bh": {"bytes": 133_551_616 + 27_101_952 + 228_377_600 + 30_923_520, "pairs": 4_462_862_693,
+    "bh": {"bytes": 131_627_264 + 26_349_568 + 227_442_176 + 31_748_864, "pairs": 4_462_862_693,
            "source": "profiles/g5_kernels_direct_treepm_bh.md (64x1, N=2^20 capture scaled by pairs)"},
 }
 
