@@ -70,6 +70,7 @@ int  pgb5_plan_tune(pgb5_plan *plan, const void *ipos, const void *jpos, const v
                     void *stream, float *best_ms);
 int  pgb5_plan_config(const pgb5_plan *plan);
 int  pgb5_plan_set_config(pgb5_plan *plan, int cfg);   /* pin one (PGB5_NCFG configurations) */
+int  pgb5_plan_update(pgb5_plan *plan, int nitem, const int *items);   /* as in pgb_g5.h */
 /* index-list launch and tuning, as in pgb_g5.h */
 int  pgb5_plan_launch_indexed(pgb5_plan *plan, const void *ipos, const void *jpos, const void *jaux,
                               const int *jidx, void *out, void *stream);

@@ -42,15 +42,6 @@ namespace {
 const char* LIB = "libpgbtree";
 ErrorSlot g_err;
 
-// Device buffers local to one accessor call: released (cudaFree) when the call returns.
-template <class T>
-struct Scoped : DevBuf<T> {
-    Scoped() = default;
-    Scoped(const Scoped&) = delete;
-    Scoped& operator=(const Scoped&) = delete;
-    ~Scoped() { this->release(); }
-};
-
 constexpr int HT_MAXDEPTH = 40;   // the host builder's depth cap
 constexpr int HT_TILE = 2048;     // particles per tile of the partition kernels
 constexpr int HT_NT = 256;        // threads per CTA of the tile kernels
@@ -686,6 +677,10 @@ struct pgbt_tree {
     DevBuf<int> size, pre, lvl_pre, gflag, goff;
     DevBuf<long long> unp, unc, uoffp, uoffc;
     DevBuf<unsigned char> wn;   // WalkNode records
+    // device staging of pgbt_groups / pgbt_group_table (kept: no allocation when a step loop
+    // asks every step)
+    DevBuf<int> gt_first, gt_count;
+    DevBuf<double> gt_centre, gt_half;
 };
 
 namespace {
@@ -924,6 +919,10 @@ void tree_free(pgbt_tree* T) {
     for (auto* b : sc) b->release();
     T->oct.release();
     T->wn.release();
+    T->gt_first.release();
+    T->gt_count.release();
+    T->gt_centre.release();
+    T->gt_half.release();
     T->unp.release();
     T->unc.release();
     T->uoffp.release();
@@ -1035,8 +1034,8 @@ PGB_EXPORT int pgbt_groups(pgbt_tree* T, int* first, int* count, double* centre,
     if (!T) return PGB_ERR_ARG;
     if (!ensure_device()) return PGB_ERR_NOGPU;
     const int ng = T->ng;
-    Scoped<int> f, c;
-    Scoped<double> ce, h;
+    auto &f = T->gt_first, &c = T->gt_count;
+    auto &ce = T->gt_centre, &h = T->gt_half;
     PGB_CUDA_OR(g_err, LIB, f.reserve((size_t)ng + 1), return PGB_ERR_CUDA);
     PGB_CUDA_OR(g_err, LIB, c.reserve((size_t)ng + 1), return PGB_ERR_CUDA);
     PGB_CUDA_OR(g_err, LIB, ce.reserve(3 * (size_t)ng + 3), return PGB_ERR_CUDA);
@@ -1105,8 +1104,8 @@ PGB_EXPORT int pgbt_group_table(pgbt_tree* T, int* first, int* count, long long*
     if (!T) return PGB_ERR_ARG;
     if (!ensure_device()) return PGB_ERR_NOGPU;
     const int ng = T->ng;
-    Scoped<int> f, c;
-    Scoped<double> ce, h;
+    auto &f = T->gt_first, &c = T->gt_count;
+    auto &ce = T->gt_centre, &h = T->gt_half;
     PGB_CUDA_OR(g_err, LIB, f.reserve((size_t)ng + 1), return PGB_ERR_CUDA);
     PGB_CUDA_OR(g_err, LIB, c.reserve((size_t)ng + 1), return PGB_ERR_CUDA);
     PGB_CUDA_OR(g_err, LIB, ce.reserve(3 * (size_t)ng + 3), return PGB_ERR_CUDA);

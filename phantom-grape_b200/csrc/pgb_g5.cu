@@ -334,9 +334,21 @@ struct Launcher {
         int slots = sm_count(g_device) * occupancy_of(kind, cfg);
         int grid = st.ntasks < slots ? st.ntasks : slots;
         PGB_CUDA_OR(g_err, LIB, launch_kind(kind, cfg, grid, a, s), return false);
+        if (!launched) PGB_CUDA_OR(g_err, LIB, cudaEventCreateWithFlags(&launched, cudaEventDisableTiming), return false);
+        PGB_CUDA_OR(g_err, LIB, cudaEventRecord(launched, s), return false);
         return true;
     }
-    void release() { st.release(); }
+    // the task list of the latest launch is no longer read once this returns
+    bool wait_launched() {
+        if (launched) PGB_CUDA_OR(g_err, LIB, cudaEventSynchronize(launched), return false);
+        return true;
+    }
+    void release() {
+        st.release();
+        if (launched) cudaEventDestroy(launched);
+        launched = nullptr;
+    }
+    cudaEvent_t launched = nullptr;   // recorded after every launch
 };
 
 struct Dev {
@@ -1069,6 +1081,39 @@ PGB_EXPORT int pgb5_plan_create(pgb5_plan** out, int kind, int nitem, const int*
     return PGB_OK;
 }
 
+// New items for an existing plan (same kind; the plan's configuration, chosen at creation, by
+// the autotuner or pinned, is kept): the tasks are re-planned on the host and staged into the
+// plan's own buffers, which grow only when the new list needs more.  A tree code whose lists
+// change every step keeps one plan per kind instead of creating and destroying one per step
+// (no device allocation, hence no device-wide synchronisation, in the step).  Waits until the
+// plan's previous launches have finished reading its task list.
+PGB_EXPORT int pgb5_plan_update(pgb5_plan* P, int nitem, const int* items) {
+    if (!P || nitem < 0 || (nitem && !items)) {
+        raise(g_err, LIB, PGB_ERR_ARG, "pgb5_plan_update: null plan or bad item count %d", nitem);
+        return PGB_ERR_ARG;
+    }
+    for (int k = 0; k < nitem; k++)
+        if (items[4 * k + 1] < 0 || items[4 * k + 3] < 0 || items[4 * k] < 0 || items[4 * k + 2] < 0) {
+            raise(g_err, LIB, PGB_ERR_ARG, "item %d has a negative offset or count", k);
+            return PGB_ERR_ARG;
+        }
+    if (!ensure_device()) return PGB_ERR_NOGPU;
+    P->items.assign(items, items + 4 * (size_t)nitem);
+    P->shape_key = shape_key(P->kind, nitem, items);
+    plan_items(P);
+    if (!P->L.wait_launched()) return g_err.code ? g_err.code : PGB_ERR_CUDA;
+    cudaStream_t s = nullptr;
+    bool ok = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess;
+    ok = ok && stage_plan(P, s);
+    ok = ok && cudaStreamSynchronize(s) == cudaSuccess;
+    if (s) cudaStreamDestroy(s);
+    if (!ok) {
+        raise(g_err, LIB, PGB_ERR_CUDA, "pgb5_plan_update: staging failed");
+        return PGB_ERR_CUDA;
+    }
+    return PGB_OK;
+}
+
 PGB_EXPORT long long pgb5_plan_interactions(const pgb5_plan* P) { return P ? P->interactions : 0; }
 PGB_EXPORT int pgb5_plan_tasks(const pgb5_plan* P) { return P ? (int)P->tasks.size() : 0; }
 
@@ -1190,6 +1235,7 @@ PGB_EXPORT int pgb5_plan_set_config(pgb5_plan* P, int cfg) {
     if (!ensure_device()) return PGB_ERR_NOGPU;
     P->cfg = cfg;
     plan_items(P);
+    if (!P->L.wait_launched()) return g_err.code ? g_err.code : PGB_ERR_CUDA;
     cudaStream_t s = nullptr;
     bool ok = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess;
     ok = ok && stage_plan(P, s);

@@ -124,6 +124,7 @@ class G5(_ErrMixin):
         _sig(L, "pgb5_plan_tune", [vp, vp, vp, vp, vp, vp, C.POINTER(C.c_float)], C.c_int)
         _sig(L, "pgb5_plan_config", [vp], C.c_int)
         _sig(L, "pgb5_plan_set_config", [vp, C.c_int], C.c_int)
+        _sig(L, "pgb5_plan_update", [vp, C.c_int, ip], C.c_int)
         _sig(L, "pgb5_plan_launch_indexed", [vp, vp, vp, vp, vp, vp, vp], C.c_int)
         _sig(L, "pgb5_plan_tune_indexed", [vp, vp, vp, vp, vp, vp, vp, C.POINTER(C.c_float)], C.c_int)
 
@@ -185,6 +186,13 @@ class G5(_ErrMixin):
         if rc:
             raise RuntimeError(f"pgb5_plan_create failed: {self.last_error()}")
         return h
+
+    def plan_update(self, plan, items):
+        """pgb5_plan_update: new items for an existing plan (configuration and buffers kept)."""
+        items = np.ascontiguousarray(items, dtype=np.int32).reshape(-1, 4)
+        rc = self.L.pgb5_plan_update(plan, len(items), ptr(items, C.c_int))
+        if rc:
+            raise RuntimeError(f"pgb5_plan_update failed: {self.last_error()}")
 
     def plan_launch(self, plan, ipos, jpos, jaux, out, stream=0):
         rc = self.L.pgb5_plan_launch(plan, ipos, jpos, jaux, out, stream)
@@ -466,6 +474,7 @@ class G5Table(_ErrMixin):
         _sig(L, "pgb5_plan_tune", [vp, vp, vp, vp, vp, vp, C.POINTER(C.c_float)], C.c_int)
         _sig(L, "pgb5_plan_config", [vp], C.c_int)
         _sig(L, "pgb5_plan_set_config", [vp, C.c_int], C.c_int)
+        _sig(L, "pgb5_plan_update", [vp, C.c_int, ip], C.c_int)
         _sig(L, "pgb5_plan_launch_indexed", [vp, vp, vp, vp, vp, vp, vp], C.c_int)
         _sig(L, "pgb5_plan_tune_indexed", [vp, vp, vp, vp, vp, vp, vp, C.POINTER(C.c_float)], C.c_int)
         self._cb = None

@@ -147,3 +147,45 @@ def test_multipole_error_vs_direct_sum(g5, bh):
     ad, pd = O.g5_newton(bh.x[sample], eps2, bh.x, bh.m)
     err = rel(acc[sample], ad)
     assert rms(err) <= 2e-3, rms(err)
+
+
+def _launch(g5, bh, pl_p, pl_c):
+    import torch
+    dev = torch.device("cuda")
+    ip, pp, cp, cq = bh.records()
+    d = [torch.from_numpy(a).to(dev) for a in (ip, pp, cp, cq, bh.pidx, bh.cidx)]
+    o_p = torch.zeros((len(ip), 4), dtype=torch.float64, device=dev)
+    o_c = torch.zeros((len(ip), 4), dtype=torch.float64, device=dev)
+    s = torch.cuda.current_stream().cuda_stream
+    g5.plan_launch_indexed(pl_p, d[0].data_ptr(), d[1].data_ptr(), None, d[4].data_ptr(), o_p.data_ptr(), s)
+    g5.plan_launch_indexed(pl_c, d[0].data_ptr(), d[2].data_ptr(), d[3].data_ptr(), d[5].data_ptr(), o_c.data_ptr(), s)
+    torch.cuda.synchronize()
+    op, oc = o_p.cpu().numpy(), o_c.cpu().numpy()
+    return op[:, :3] + oc[:, :3], op[:, 3] - oc[:, 3]
+
+
+@pytest.mark.parametrize("cfg", [7, 1])
+def test_plan_update_matches_fresh_plans(g5, cfg):
+    """pgb5_plan_update on the lists of other trees (more groups, then fewer) gives the results
+    of plans created for them with the same configuration, bit for bit."""
+    sets = [W.bh_hernquist(1 << 14, seed=W.SEED0 + 61), W.bh_hernquist(1 << 16, seed=W.SEED0 + 62),
+            W.bh_hernquist(3000, seed=W.SEED0 + 63)]
+    pl_p = pl_c = None
+    try:
+        for k, bh in enumerate(sets):
+            if pl_p is None:
+                pl_p, pl_c = g5.plan_create(g5.NEWTON, bh.items("p")), g5.plan_create(g5.QUAD, bh.items("c"))
+                assert g5.L.pgb5_plan_set_config(pl_p, cfg) == 0 and g5.L.pgb5_plan_set_config(pl_c, cfg) == 0
+            else:
+                g5.plan_update(pl_p, bh.items("p"))
+                g5.plan_update(pl_c, bh.items("c"))
+            assert g5.L.pgb5_plan_config(pl_p) == cfg and g5.L.pgb5_plan_config(pl_c) == cfg
+            assert g5.L.pgb5_plan_interactions(pl_c) == int(np.sum(np.diff(bh.coff) * bh.gcount))
+            a, p = _launch(g5, bh, pl_p, pl_c)
+            a0, p0 = batched(g5, bh, cfg_p=cfg, cfg_c=cfg)
+            np.testing.assert_array_equal(a, a0, err_msg=f"set {k}")
+            np.testing.assert_array_equal(p, p0, err_msg=f"set {k}")
+    finally:
+        if pl_p is not None:
+            g5.plan_destroy(pl_p)
+            g5.plan_destroy(pl_c)

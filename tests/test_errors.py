@@ -71,3 +71,10 @@ def test_g6_batched_plan_rejects_negative_items(g6):
     items = np.array([[0, 10, 0, -1]], np.int32)
     rc = g6.L.pgb6_plan_create(C.byref(h), 1, pgb.ffi.ptr(items, C.c_int), 0)
     assert rc == ARG and not h.value
+
+
+def test_g5_plan_update_refuses_a_null_plan(g5):
+    items = np.zeros((1, 4), np.int32)
+    assert g5.L.pgb5_plan_update(None, 1, pgb.ffi.ptr(items, C.c_int)) == ARG
+    code, msg = g5.last_error()
+    assert code == ARG and "pgb5_plan_update" in msg
