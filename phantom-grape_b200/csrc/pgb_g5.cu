@@ -287,6 +287,7 @@ bool table_args(G5Args& a) {
     return true;
 }
 
+#ifdef PGB_TABLE
 // i and j coordinates of the table kind are pre-scaled by xscale: j in float arithmetic
 // (phantom_g5.c:112-128: cvtpd2ps then * (float)xscale), i through double
 // (phantom_g5.c:96-104: (float)x * Xscale rounded to float).
@@ -296,6 +297,7 @@ inline float scale_j(double x) {
 inline float scale_i(double x) {
     return (float)((double)(float)x * g_tab.xscale);
 }
+#endif
 
 // Staged work list + launch of one devid / plan.
 struct Launcher {

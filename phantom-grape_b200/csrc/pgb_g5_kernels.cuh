@@ -5,8 +5,8 @@
 // from a global counter.  A CTA of NT threads owns NT*IPT i-particles (IPT per thread, kept
 // in registers), streams its j-chunk through shared memory in tiles of NT records (one
 // coalesced 16-byte load per thread per record word), and every thread reads each j record
-// with a broadcast LDS.128.  Sums are accumulated in FP32 within a j tile and folded into FP64
-// accumulators after every tile (the cross-tile reduction runs in FP64).  Split j-ranges
+// with a broadcast LDS.128.  Sums are accumulated in FP32 over at most 128 terms (G5_FOLD) and
+// then added into FP64 accumulators (the cross-block reduction runs in FP64).  Split j-ranges
 // write FP64 partial rows; the last CTA of a group reduces them in chunk order.
 //
 // Formulae (scaled so that the Newton-refined rsqrt needs no extra multiply):
@@ -45,6 +45,11 @@ struct G5Args {
 // kinds
 enum { G5_NEWTON = 0, G5_SYMMETRIC = 1, G5_QUAD = 2, G5_TABLE = 3 };
 constexpr int G5_TBL_MAX = 4096;   // largest table held in shared memory (32 KB)
+// FP32 partial sums cover at most G5_FOLD terms (per thread and i) before they are added into
+// the FP64 sums: the rounding of a 128-term FP32 sum stays near the level of the FP32 pair
+// arithmetic, a whole 1024-record tile (the direct sum's CTA) adds several times more
+// (acc 1.4e-7 rms against FP64 with 1024-term sums, 4.7e-8 with 64-term sums on N = 16384)
+constexpr int G5_FOLD = 128;
 
 template <int KIND>
 struct JWords { static constexpr int n = (KIND == G5_SYMMETRIC) ? 2 : (KIND == G5_QUAD ? 3 : 1); };
@@ -280,38 +285,51 @@ __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
             }
             __syncthreads();
             if constexpr (IPT % 2 == 0) {
-                float2 a2[IPT / 2][4];
-#pragma unroll
-                for (int p = 0; p < IPT / 2; p++) a2[p][0] = a2[p][1] = a2[p][2] = a2[p][3] = make_float2(0.f, 0.f);
-#pragma unroll 4
-                for (int j = 0; j < nt; j++) {
+                for (int j0 = 0; j0 < nt; j0 += G5_FOLD) {
+                    const int j1 = min(j0 + G5_FOLD, nt);
+                    float2 a2[IPT / 2][4];
 #pragma unroll
                     for (int p = 0; p < IPT / 2; p++)
-                        g5_interact2<KIND, NT>(sj, j, xi + 2 * p, yi + 2 * p, zi + 2 * p, ei + 2 * p, tab, shift,
-                                               A.r2cut, a2[p]);
+                        a2[p][0] = a2[p][1] = a2[p][2] = a2[p][3] = make_float2(0.f, 0.f);
+#pragma unroll 4
+                    for (int j = j0; j < j1; j++) {
+#pragma unroll
+                        for (int p = 0; p < IPT / 2; p++)
+                            g5_interact2<KIND, NT>(sj, j, xi + 2 * p, yi + 2 * p, zi + 2 * p, ei + 2 * p, tab, shift,
+                                                   A.r2cut, a2[p]);
+                    }
+#pragma unroll
+                    for (int k = 0; k < IPT; k++) {
+#pragma unroll
+                        for (int c = 0; c < 4; c++) S[k][c] += (double)lane_of(a2[k / 2][c], k % 2);
+                    }
                 }
+            } else {
+            // blocks of G5_FOLD terms per lane (one block when a tile has no more: NT <= G5_FOLD);
+            // the lane stride as a template constant, so that the unrolled loop addresses its j
+            // records with immediate offsets (64-thread CTAs have 1, 2 or 4 lanes)
+            const int nlanes = LANES ? nl : 1;
+            auto block = [&](int j0, int j1) {
+                float a[IPT][4];
+#pragma unroll
+                for (int k = 0; k < IPT; k++) a[k][0] = a[k][1] = a[k][2] = a[k][3] = 0.f;
+                if (nlanes == 1) g5_jloop<KIND, NT, IPT, 1>(sj, j0 + lane, j1, xi, yi, zi, ei, tab, shift, A.r2cut, a);
+                else if (nlanes == 2) g5_jloop<KIND, NT, IPT, 2>(sj, j0 + lane, j1, xi, yi, zi, ei, tab, shift, A.r2cut, a);
+                else if (nlanes == 4) g5_jloop<KIND, NT, IPT, 4>(sj, j0 + lane, j1, xi, yi, zi, ei, tab, shift, A.r2cut, a);
+                else g5_jloop<KIND, NT, IPT, 0>(sj, j0 + lane, j1, xi, yi, zi, ei, tab, shift, A.r2cut, a, nlanes);
 #pragma unroll
                 for (int k = 0; k < IPT; k++) {
-#pragma unroll
-                    for (int c = 0; c < 4; c++) S[k][c] += (double)lane_of(a2[k / 2][c], k % 2);
+                    S[k][0] += (double)a[k][0];
+                    S[k][1] += (double)a[k][1];
+                    S[k][2] += (double)a[k][2];
+                    S[k][3] += (double)a[k][3];
                 }
-                continue;
+            };
+            if constexpr (NT <= G5_FOLD) {
+                block(0, nt);
+            } else {
+                for (int j0 = 0; j0 < nt; j0 += G5_FOLD * nlanes) block(j0, min(j0 + G5_FOLD * nlanes, nt));
             }
-            float a[IPT][4];
-#pragma unroll
-            for (int k = 0; k < IPT; k++) a[k][0] = a[k][1] = a[k][2] = a[k][3] = 0.f;
-            // the lane stride as a template constant: the unrolled loop then addresses its j
-            // records with immediate offsets (64-thread CTAs have 1, 2 or 4 lanes)
-            if (!LANES || nl == 1) g5_jloop<KIND, NT, IPT, 1>(sj, lane, nt, xi, yi, zi, ei, tab, shift, A.r2cut, a);
-            else if (nl == 2) g5_jloop<KIND, NT, IPT, 2>(sj, lane, nt, xi, yi, zi, ei, tab, shift, A.r2cut, a);
-            else if (nl == 4) g5_jloop<KIND, NT, IPT, 4>(sj, lane, nt, xi, yi, zi, ei, tab, shift, A.r2cut, a);
-            else g5_jloop<KIND, NT, IPT, 0>(sj, lane, nt, xi, yi, zi, ei, tab, shift, A.r2cut, a, nl);
-#pragma unroll
-            for (int k = 0; k < IPT; k++) {
-                S[k][0] += (double)a[k][0];
-                S[k][1] += (double)a[k][1];
-                S[k][2] += (double)a[k][2];
-                S[k][3] += (double)a[k][3];
             }
         }
 

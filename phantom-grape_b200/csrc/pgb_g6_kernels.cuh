@@ -3,8 +3,9 @@
 //
 // Precision layout (the reference's, PG6/libpg6/gravity.c:311-420): the predictor and the
 // relative position x_j - x_i are FP64; the difference is rounded to FP32 and everything after
-// it (r^2, rsqrt, velocity difference, products) is FP32.  Sums are FP32 within one j tile and
-// folded into FP64 after every tile; split j-ranges are reduced in FP64 in chunk order.
+// it (r^2, rsqrt, velocity difference, products) is FP32.  Sums are FP32 over at most 128
+// terms (G6_FOLD) and then added into FP64 sums; split j-ranges are reduced in FP64 in chunk
+// order.
 //
 // Per pair (q = -2/r with one Newton step, pgb::minus2_over_r; self pair masked by index):
 //   pot_sum += m q, acc_sum += (m q^3) dx, jrk_sum += (m q^3) (dv - (3/4) q^2 (dx.dv) dx)
@@ -183,6 +184,14 @@ __global__ void g6_nb_sort_kernel(const int* __restrict__ nb_count, int* __restr
         }
     for (int k = threadIdx.x; k < c; k += blockDim.x) row[k] = jmem[sh_nb[k]].idx;
 }
+
+// FP32 partial sums cover at most G6_FOLD terms (per thread and i) before they are added into
+// the FP64 sums.  Rounding error of the blocked sum alone, acc of a 65536-body Plummer sphere
+// (rms relative, against the exact sum of the same FP32 terms): 2.1e-8 for 128 terms, 3.3e-8
+// for 256, against 1.7e-8 for the FP32 pair arithmetic itself.  Measured on the largest
+// Hermite call (256 x 2 configuration): acc 6.7e-8 -> 5.4e-8 rms against FP64 with no change in
+// speed; 64-term blocks (5.0e-8) cost 7 %.
+constexpr int G6_FOLD = 128;
 
 struct G6Acc {
     float ax, ay, az, jx, jy, jz, pot;
@@ -471,10 +480,6 @@ __device__ __forceinline__ void g6_task(const G6Args& A, const Task& T, unsigned
         __syncthreads();
         if constexpr (IPT % 2 == 0) {
             constexpr int NP = IPT / 2;
-            G6Acc2 a[NP];
-            const float2 z2 = make_float2(0.f, 0.f);
-#pragma unroll
-            for (int p = 0; p < NP; p++) a[p] = G6Acc2{z2, z2, z2, z2, z2, z2, {0.f, 0.f}};
             int* nbc[IPT];
             int* nbl[IPT];
 #pragma unroll
@@ -484,54 +489,65 @@ __device__ __forceinline__ void g6_task(const G6Args& A, const Task& T, unsigned
                 nbc[k] = NBL ? A.nb_count + gi : nullptr;
                 nbl[k] = NBL ? A.nb_list + (size_t)gi * A.nb_maxlen : nullptr;
             }
+            for (int j0 = 0; j0 < nt; j0 += G6_FOLD) {
+                const int j1 = min(j0 + G6_FOLD, nt);
+                G6Acc2 a[NP];
+                const float2 z2 = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int p = 0; p < NP; p++) a[p] = G6Acc2{z2, z2, z2, z2, z2, z2, {0.f, 0.f}};
 #pragma unroll 2
-            for (int j = 0; j < nt; j++) {
+                for (int j = j0; j < j1; j++) {
+                    const G6PredJ J = sj[j];
+                    const int jadr = T.j0 + jt + j;
+#pragma unroll
+                    for (int p = 0; p < NP; p++)
+                        g6_pair2<FF, NN, NBL>(J, jadr, pi + 2 * p, vxi + 2 * p, vyi + 2 * p, vzi + 2 * p,
+                                              idi + 2 * p, A.eps2, hinv + 2 * p, a[p], kmin + 2 * p, kadr + 2 * p,
+                                              nbc + 2 * p, nbl + 2 * p, A.nb_maxlen);
+                }
+#pragma unroll
+                for (int p = 0; p < NP; p++) {
+                    const float2* v = &a[p].ax;
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        const int k = 2 * p + h;
+#pragma unroll
+                        for (int c = 0; c < 6; c++) S[k][c] += (double)(h ? v[c].y : v[c].x);
+                        S[k][6] += (double)a[p].pot[h];
+                    }
+                }
+            }
+        } else {
+        // blocks of G6_FOLD terms per lane
+        for (int j0 = 0; j0 < nt; j0 += G6_FOLD * JL) {
+            const int j1 = min(j0 + G6_FOLD * JL, nt);
+            G6Acc a[IPT];
+#pragma unroll
+            for (int k = 0; k < IPT; k++) a[k] = G6Acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll 2
+            for (int j = j0 + jl; j < j1; j += JL) {
                 const G6PredJ J = sj[j];
                 const int jadr = T.j0 + jt + j;
 #pragma unroll
-                for (int p = 0; p < NP; p++)
-                    g6_pair2<FF, NN, NBL>(J, jadr, pi + 2 * p, vxi + 2 * p, vyi + 2 * p, vzi + 2 * p, idi + 2 * p,
-                                          A.eps2, hinv + 2 * p, a[p], kmin + 2 * p, kadr + 2 * p, nbc + 2 * p,
-                                          nbl + 2 * p, A.nb_maxlen);
-            }
-#pragma unroll
-            for (int p = 0; p < NP; p++) {
-                const float2* v = &a[p].ax;
-#pragma unroll
-                for (int h = 0; h < 2; h++) {
-                    const int k = 2 * p + h;
-#pragma unroll
-                    for (int c = 0; c < 6; c++) S[k][c] += (double)(h ? v[c].y : v[c].x);
-                    S[k][6] += (double)a[p].pot[h];
+                for (int k = 0; k < IPT; k++) {
+                    int li = slot + k * ISL;
+                    int gi = T.i0 + (li < T.ni ? li : 0);
+                    g6_pair<FF, NN, NBL>(J, jadr, pi[k], vxi[k], vyi[k], vzi[k], idi[k], A.eps2, hinv[k],
+                                         a[k], kmin[k], kadr[k], NBL ? A.nb_count + gi : nullptr,
+                                         NBL ? A.nb_list + (size_t)gi * A.nb_maxlen : nullptr, A.nb_maxlen);
                 }
             }
-            continue;
-        }
-        G6Acc a[IPT];
-#pragma unroll
-        for (int k = 0; k < IPT; k++) a[k] = G6Acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-#pragma unroll 2
-        for (int j = jl; j < nt; j += JL) {
-            const G6PredJ J = sj[j];
-            const int jadr = T.j0 + jt + j;
 #pragma unroll
             for (int k = 0; k < IPT; k++) {
-                int li = slot + k * ISL;
-                int gi = T.i0 + (li < T.ni ? li : 0);
-                g6_pair<FF, NN, NBL>(J, jadr, pi[k], vxi[k], vyi[k], vzi[k], idi[k], A.eps2, hinv[k],
-                                 a[k], kmin[k], kadr[k], NBL ? A.nb_count + gi : nullptr,
-                                 NBL ? A.nb_list + (size_t)gi * A.nb_maxlen : nullptr, A.nb_maxlen);
+                S[k][0] += (double)a[k].ax;
+                S[k][1] += (double)a[k].ay;
+                S[k][2] += (double)a[k].az;
+                S[k][3] += (double)a[k].jx;
+                S[k][4] += (double)a[k].jy;
+                S[k][5] += (double)a[k].jz;
+                S[k][6] += (double)a[k].pot;
             }
         }
-#pragma unroll
-        for (int k = 0; k < IPT; k++) {
-            S[k][0] += (double)a[k].ax;
-            S[k][1] += (double)a[k].ay;
-            S[k][2] += (double)a[k].az;
-            S[k][3] += (double)a[k].jx;
-            S[k][4] += (double)a[k].jy;
-            S[k][5] += (double)a[k].jz;
-            S[k][6] += (double)a[k].pot;
         }
     }
 
