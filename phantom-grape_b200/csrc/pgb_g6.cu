@@ -1420,7 +1420,9 @@ bool hm_launch(pgb6_hermite* H, bool startup, double tend, int max_steps) {
     R.startup = startup ? 1 : 0;
     R.max_steps = max_steps;
     R.nseg = H->nseg;
-    static const int minj = env_int("PGB_HM_MINJ", 128, 16, 1 << 20);
+    // j per force chunk at least (fewer, longer tasks mean fewer partial rows for the owners
+    // to sum; N = 16384 block steps: 64 -> 114, 128 -> 120, 256 -> 123, 512 -> 108 Gint/s)
+    static const int minj = env_int("PGB_HM_MINJ", 256, 16, 1 << 20);
     R.minj = minj;
     void* args[] = {&R};
     const void* fn = H->ff ? (const void*)hm_run_kernel<true> : (const void*)hm_run_kernel<false>;
