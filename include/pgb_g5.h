@@ -123,7 +123,8 @@ int  pgb5_plan_config(const pgb5_plan *plan);
 int  pgb5_plan_set_config(pgb5_plan *plan, int cfg);   /* pin one (PGB5_NCFG configurations) */
 /* New items for an existing plan of the same kind, its configuration kept: re-planned on the
  * host, staged into the plan's own buffers (grown only when needed, so no device allocation in
- * a step loop); waits until the plan's previous launches have finished with its task list.
+ * a step loop); waits until the plan's previous stream launches have finished with its task
+ * list (replays of a CUDA graph that captured the plan must be finished by the caller).
  * For codes whose lists change every step (tree codes): one plan per kind for the whole run. */
 int  pgb5_plan_update(pgb5_plan *plan, int nitem, const int *items);
 /* Tree-code interaction lists without copies: the items' j-ranges address the device index

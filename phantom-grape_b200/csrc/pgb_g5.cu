@@ -336,8 +336,15 @@ struct Launcher {
         int slots = sm_count(g_device) * occupancy_of(kind, cfg);
         int grid = st.ntasks < slots ? st.ntasks : slots;
         PGB_CUDA_OR(g_err, LIB, launch_kind(kind, cfg, grid, a, s), return false);
-        if (!launched) PGB_CUDA_OR(g_err, LIB, cudaEventCreateWithFlags(&launched, cudaEventDisableTiming), return false);
-        PGB_CUDA_OR(g_err, LIB, cudaEventRecord(launched, s), return false);
+        // completion marker for pgb5_plan_update; a launch captured into a CUDA graph records
+        // none (its replays are the caller's to finish before the plan is updated)
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        PGB_CUDA_OR(g_err, LIB, cudaStreamIsCapturing(s, &cap), return false);
+        if (cap == cudaStreamCaptureStatusNone) {
+            if (!launched)
+                PGB_CUDA_OR(g_err, LIB, cudaEventCreateWithFlags(&launched, cudaEventDisableTiming), return false);
+            PGB_CUDA_OR(g_err, LIB, cudaEventRecord(launched, s), return false);
+        }
         return true;
     }
     // the task list of the latest launch is no longer read once this returns

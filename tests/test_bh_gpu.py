@@ -189,3 +189,48 @@ def test_plan_update_matches_fresh_plans(g5, cfg):
         if pl_p is not None:
             g5.plan_destroy(pl_p)
             g5.plan_destroy(pl_c)
+
+
+def test_graph_captured_plans_replay_and_update(g5):
+    """Both launches captured in a CUDA graph replay the stream launches' results bit for bit;
+    after the replays have finished the same plans take another tree's lists."""
+    import torch
+    dev = torch.device("cuda")
+    bh, bh2 = W.bh_hernquist(1 << 14, seed=W.SEED0 + 71), W.bh_hernquist(1 << 15, seed=W.SEED0 + 72)
+    ip, pp, cp, cq = bh.records()
+    d = [torch.from_numpy(a).to(dev) for a in (ip, pp, cp, cq, bh.pidx, bh.cidx)]
+    o_p = torch.zeros((len(ip), 4), dtype=torch.float64, device=dev)
+    o_c = torch.zeros((len(ip), 4), dtype=torch.float64, device=dev)
+    pl_p, pl_c = g5.plan_create(g5.NEWTON, bh.items("p")), g5.plan_create(g5.QUAD, bh.items("c"))
+    try:
+        s = torch.cuda.Stream()
+        with torch.cuda.stream(s):
+            g5.plan_launch_indexed(pl_p, d[0].data_ptr(), d[1].data_ptr(), None, d[4].data_ptr(), o_p.data_ptr(),
+                                   s.cuda_stream)
+            g5.plan_launch_indexed(pl_c, d[0].data_ptr(), d[2].data_ptr(), d[3].data_ptr(), d[5].data_ptr(),
+                                   o_c.data_ptr(), s.cuda_stream)
+        s.synchronize()
+        ref_p, ref_c = o_p.clone(), o_c.clone()
+        o_p.zero_()
+        o_c.zero_()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=s):
+            g5.plan_launch_indexed(pl_p, d[0].data_ptr(), d[1].data_ptr(), None, d[4].data_ptr(), o_p.data_ptr(),
+                                   s.cuda_stream)
+            g5.plan_launch_indexed(pl_c, d[0].data_ptr(), d[2].data_ptr(), d[3].data_ptr(), d[5].data_ptr(),
+                                   o_c.data_ptr(), s.cuda_stream)
+        for _ in range(3):
+            graph.replay()
+        torch.cuda.synchronize()
+        assert torch.equal(o_p, ref_p) and torch.equal(o_c, ref_c)
+        del graph
+        g5.plan_update(pl_p, bh2.items("p"))
+        g5.plan_update(pl_c, bh2.items("c"))
+        a, p = _launch(g5, bh2, pl_p, pl_c)
+        cfg_p, cfg_c = g5.L.pgb5_plan_config(pl_p), g5.L.pgb5_plan_config(pl_c)
+        a0, p0 = batched(g5, bh2, cfg_p=cfg_p, cfg_c=cfg_c)
+        np.testing.assert_array_equal(a, a0)
+        np.testing.assert_array_equal(p, p0)
+    finally:
+        g5.plan_destroy(pl_p)
+        g5.plan_destroy(pl_c)
