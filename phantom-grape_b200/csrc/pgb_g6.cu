@@ -912,6 +912,7 @@ struct pgb6_plan {
     int rows = 0;
     long long interactions = 0;
     Stager<G6I, G6Out> st;
+    cudaEvent_t launched = nullptr;   // recorded after every stream (not graph-captured) launch
 };
 
 enum { PGB6_NN = 1, PGB6_POS_F64 = 2 };
@@ -993,6 +994,75 @@ PGB_EXPORT int pgb6_plan_launch(pgb6_plan* P, const void* ipart, const void* jpr
     int slots = sm_count(g_device) * occupancy(P->cfg, P->ff, P->nn, false);
     int grid = a.ntasks < slots ? a.ntasks : slots;
     PGB_CUDA_OR(g_err, LIB, launch_kernel(P->cfg, P->ff, P->nn, false, grid, a, s), return PGB_ERR_CUDA);
+    // completion marker for pgb6_plan_update (none for a launch captured into a CUDA graph)
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    PGB_CUDA_OR(g_err, LIB, cudaStreamIsCapturing(s, &cap), return PGB_ERR_CUDA);
+    if (cap == cudaStreamCaptureStatusNone) {
+        if (!P->launched)
+            PGB_CUDA_OR(g_err, LIB, cudaEventCreateWithFlags(&P->launched, cudaEventDisableTiming),
+                        return PGB_ERR_CUDA);
+        PGB_CUDA_OR(g_err, LIB, cudaEventRecord(P->launched, s), return PGB_ERR_CUDA);
+    }
+    return PGB_OK;
+}
+
+// Pin one kernel configuration (0 .. NCFG-1) and re-plan for it (after the plan's previous
+// stream launches have finished).
+PGB_EXPORT int pgb6_plan_set_config(pgb6_plan* P, int cfg) {
+    if (!P || cfg < 0 || cfg >= NCFG) {
+        raise(g_err, LIB, PGB_ERR_ARG, "pgb6_plan_set_config: configuration %d outside [0, %d)", cfg, (int)NCFG);
+        return PGB_ERR_ARG;
+    }
+    if (!ensure_device()) return PGB_ERR_NOGPU;
+    P->cfg = cfg;
+    const int nitem = (int)(P->items.size() / 4);
+    P->tasks.clear();
+    P->groups.clear();
+    P->interactions = plan_items(P->tasks, P->groups, P->rows, nitem, P->items.data(), cfg, P->ff, P->nn, false);
+    if (P->launched) PGB_CUDA_OR(g_err, LIB, cudaEventSynchronize(P->launched), return PGB_ERR_CUDA);
+    cudaStream_t s = nullptr;
+    bool ok = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess;
+    ok = ok && P->st.stage(s, P->tasks, P->groups, P->rows, ITILE_MAX, (const G6I*)nullptr, 0) == cudaSuccess;
+    ok = ok && cudaStreamSynchronize(s) == cudaSuccess;
+    if (s) cudaStreamDestroy(s);
+    if (!ok) {
+        raise(g_err, LIB, PGB_ERR_CUDA, "pgb6_plan_set_config: staging failed");
+        return PGB_ERR_CUDA;
+    }
+    return PGB_OK;
+}
+
+// New items for an existing plan (same flags; its configuration kept), re-planned on the host
+// and staged into the plan's own buffers, which grow only when needed: a code whose active sets
+// or clusters change every step keeps one plan instead of creating and destroying one per step
+// (no device allocation, hence no device-wide synchronisation, in its step).  Waits until the
+// plan's previous stream launches have finished reading its task list.
+PGB_EXPORT int pgb6_plan_update(pgb6_plan* P, int nitem, const int* items) {
+    if (!P || nitem < 0 || (nitem && !items)) {
+        raise(g_err, LIB, PGB_ERR_ARG, "pgb6_plan_update: null plan or bad item count %d", nitem);
+        return PGB_ERR_ARG;
+    }
+    for (int k = 0; k < nitem; k++)
+        if (items[4 * k] < 0 || items[4 * k + 1] < 0 || items[4 * k + 2] < 0 || items[4 * k + 3] < 0) {
+            raise(g_err, LIB, PGB_ERR_ARG, "pgb6_plan_update: item %d has a negative offset or count", k);
+            return PGB_ERR_ARG;
+        }
+    if (!ensure_device()) return PGB_ERR_NOGPU;
+    P->items.assign(items, items + 4 * (size_t)nitem);
+    P->shape_key = shape_key(nitem, items, P->ff, P->nn);
+    P->tasks.clear();
+    P->groups.clear();
+    P->interactions = plan_items(P->tasks, P->groups, P->rows, nitem, items, P->cfg, P->ff, P->nn, false);
+    if (P->launched) PGB_CUDA_OR(g_err, LIB, cudaEventSynchronize(P->launched), return PGB_ERR_CUDA);
+    cudaStream_t s = nullptr;
+    bool ok = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess;
+    ok = ok && P->st.stage(s, P->tasks, P->groups, P->rows, ITILE_MAX, (const G6I*)nullptr, 0) == cudaSuccess;
+    ok = ok && cudaStreamSynchronize(s) == cudaSuccess;
+    if (s) cudaStreamDestroy(s);
+    if (!ok) {
+        raise(g_err, LIB, PGB_ERR_CUDA, "pgb6_plan_update: staging failed");
+        return PGB_ERR_CUDA;
+    }
     return PGB_OK;
 }
 
@@ -1054,6 +1124,7 @@ PGB_EXPORT void pgb6_plan_destroy(pgb6_plan* P) {
     if (!P) return;
     if (g_device >= 0) cudaSetDevice(g_device);
     P->st.release();
+    if (P->launched) cudaEventDestroy(P->launched);
     delete P;
 }
 

@@ -265,6 +265,8 @@ class G6(_ErrMixin):
         _sig(L, "pgb6_plan_interactions", [vp], C.c_longlong)
         _sig(L, "pgb6_plan_tasks", [vp], C.c_int)
         _sig(L, "pgb6_plan_config", [vp], C.c_int)
+        _sig(L, "pgb6_plan_update", [vp, C.c_int, ip], C.c_int)
+        _sig(L, "pgb6_plan_set_config", [vp, C.c_int], C.c_int)
         _sig(L, "pgb6_plan_tune", [vp, vp, vp, C.c_double, vp, vp, C.POINTER(C.c_float)], C.c_int)
         _sig(L, "pgb6_predict", [vp, C.c_int, C.c_double, vp, C.c_int, vp], C.c_int)
         _sig(L, "pgb6_batch_host", [C.c_int, ip, C.c_int, dp, dp, ip, C.c_int, dp, dp, dp, ip, C.c_double,
@@ -360,6 +362,13 @@ class G6(_ErrMixin):
         if rc:
             raise RuntimeError(f"pgb6_plan_create failed: {self.last_error()}")
         return h
+
+    def plan_update(self, plan, items):
+        """pgb6_plan_update: new items for an existing plan (configuration and buffers kept)."""
+        items = np.ascontiguousarray(items, dtype=np.int32).reshape(-1, 4)
+        rc = self.L.pgb6_plan_update(plan, len(items), ptr(items, C.c_int))
+        if rc:
+            raise RuntimeError(f"pgb6_plan_update failed: {self.last_error()}")
 
     def plan_launch(self, plan, ipart, jpred, eps2, out, stream=0):
         rc = self.L.pgb6_plan_launch(plan, ipart, jpred, eps2, out, stream)

@@ -78,3 +78,11 @@ def test_g5_plan_update_refuses_a_null_plan(g5):
     assert g5.L.pgb5_plan_update(None, 1, pgb.ffi.ptr(items, C.c_int)) == ARG
     code, msg = g5.last_error()
     assert code == ARG and "pgb5_plan_update" in msg
+
+
+def test_g6_plan_update_and_set_config_refuse_a_null_plan(g6):
+    items = np.zeros((1, 4), np.int32)
+    assert g6.L.pgb6_plan_update(None, 1, pgb.ffi.ptr(items, C.c_int)) == ARG
+    assert "pgb6_plan_update" in g6.last_error()[1]
+    g6.clear_error()
+    assert g6.L.pgb6_plan_set_config(None, 0) == ARG

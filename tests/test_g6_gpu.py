@@ -261,3 +261,43 @@ def test_device_plan_graph_capture(g6, ff):
             assert rms(rel(acc, ref["acc"])) <= 1e-6
     finally:
         g6.plan_destroy(plan)
+
+
+def test_plan_update_matches_fresh_plans(g6):
+    """pgb6_plan_update with other cluster sets (more items, then fewer, then one large item)
+    gives the results of plans created for them with the same configuration, bit for bit."""
+    import torch
+    dev = torch.device("cuda")
+    sets = [W.cluster_set(ncl=6, nmin=100, nmax=2000, seed=131), W.cluster_set(ncl=20, nmin=64, nmax=3000, seed=132),
+            W.cluster_set(ncl=3, nmin=50, nmax=500, seed=133), W.cluster_set(ncl=1, nmin=9000, nmax=9000, seed=134)]
+    plan = None
+    try:
+        for k, cs in enumerate(sets):
+            n = len(cs.mass)
+            idx = np.arange(n, dtype=np.int32)
+            d_i = torch.from_numpy(pgb.ffi.g6_irecords(cs.pos, cs.vel, idx).view(np.uint8)).to(dev)
+            d_j = torch.from_numpy(pgb.ffi.g6_jrecords(cs.pos, cs.vel, cs.mass, idx).view(np.uint8)).to(dev)
+            items = np.stack([cs.offsets[:-1], cs.sizes, cs.offsets[:-1], cs.sizes], 1)
+            if plan is None:
+                plan = g6.plan_create(items, nn=True)
+            else:
+                g6.plan_update(plan, items)
+            cfg = g6.L.pgb6_plan_config(plan)
+            assert g6.L.pgb6_plan_interactions(plan) == int(np.sum(cs.sizes.astype(np.int64) ** 2))
+            out = []
+            for p in (plan, None):
+                d_o = torch.zeros(n * pgb.ffi.G6OUT.itemsize, dtype=torch.uint8, device=dev)
+                q = p
+                if q is None:   # a fresh plan pinned to the same configuration
+                    q = g6.plan_create(items, nn=True)
+                    assert g6.L.pgb6_plan_set_config(q, cfg) == 0
+                g6.plan_launch(q, d_i.data_ptr(), d_j.data_ptr(), cs.eps2, d_o.data_ptr(), 0)
+                torch.cuda.synchronize()
+                out.append(d_o.cpu().numpy().view(pgb.ffi.G6OUT).copy())
+                if p is None:
+                    assert g6.L.pgb6_plan_config(q) == cfg
+                    g6.plan_destroy(q)
+            assert out[0].tobytes() == out[1].tobytes(), f"set {k}"
+    finally:
+        if plan is not None:
+            g6.plan_destroy(plan)
