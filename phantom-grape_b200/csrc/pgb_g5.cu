@@ -114,8 +114,10 @@ cudaError_t launch_k(int grid, const G5Args& a, cudaStream_t s, int* occ) {
     if constexpr (!kind_fits<KIND, NT>()) {
         return cudaErrorInvalidConfiguration;
     } else {
-        if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, g5_kernel<KIND, NT, IPT>, NT, 0);
-        g5_kernel<KIND, NT, IPT><<<grid, NT, 0, s>>>(a);
+        // the table kind's table lives in dynamic shared memory (a.tbl_size entries)
+        const size_t dyn = (KIND == G5_TABLE) ? (size_t)a.tbl_size * sizeof(float2) : 0;
+        if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, g5_kernel<KIND, NT, IPT>, NT, dyn);
+        g5_kernel<KIND, NT, IPT><<<grid, NT, dyn, s>>>(a);
         return cudaGetLastError();
     }
 }
@@ -146,17 +148,24 @@ cudaError_t launch_kind(int kind, int cfg, int grid, const G5Args& a, cudaStream
 #endif
 }
 
+int table_entries();   // the table kind's current table size (0 in the other libraries)
+
+// Resident CTAs per SM of a configuration (the table kind's depends on its table size).
 int occupancy_of(int kind, int cfg) {
     static int cache[4][G5_NCFG] = {};
+    static int cache_tbl[4][G5_NCFG] = {};
+    const int tbl = (kind == G5_TABLE) ? table_entries() : 0;
     int& v = cache[kind & 3][cfg];
-    if (!v) {
+    if (!v || cache_tbl[kind & 3][cfg] != tbl) {
         int b = 0;
         G5Args a{};
+        a.tbl_size = tbl;
         if (launch_kind(kind, cfg, 0, a, nullptr, &b) != cudaSuccess || b < 1) {
             cudaGetLastError();
             b = 1;
         }
         v = b;
+        cache_tbl[kind & 3][cfg] = tbl;
     }
     return v;
 }
@@ -201,6 +210,11 @@ inline int tab_frc() {
     return g_tab.frc_bit;
 }
 inline int tab_size() { return 1 << (g_tab.exp_bit + tab_frc()); }
+#ifdef PGB_TABLE
+int table_entries() { return tab_size(); }
+#else
+int table_entries() { return 0; }
+#endif
 
 inline float bits_float(uint32_t u) {
     float f;

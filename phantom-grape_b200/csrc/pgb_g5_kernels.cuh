@@ -231,13 +231,15 @@ __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
     __shared__ float4 sj[NT * (W > 2 ? W : 2)];  // also the reduction buffer (double4 x NT)
     __shared__ int s_task, s_flag;
     // table kind: the whole force table in shared memory for the lifetime of the CTA
-    __shared__ float2 stab[KIND == G5_TABLE ? G5_TBL_MAX : 1];
-    const float2* tab = stab;
+    // table kind: the force table in dynamic shared memory sized to the table (A.tbl_size
+    // entries, 8 KB for 1024) for the lifetime of the CTA; the other kinds launch without any
+    extern __shared__ float2 g5_dyn_tab[];
+    const float2* tab = g5_dyn_tab;
     int shift = 0;
     if constexpr (KIND == G5_TABLE) {
-        for (int k = threadIdx.x; k < A.tbl_size; k += NT) stab[k] = A.table[k];
+        for (int k = threadIdx.x; k < A.tbl_size; k += NT) g5_dyn_tab[k] = A.table[k];
         shift = A.tbl_shift;
-        tab = stab - (0x40000000u >> shift);  // index by (bits of s) >> shift directly
+        tab = g5_dyn_tab - (0x40000000u >> shift);  // index by (bits of s) >> shift directly
         __syncthreads();
     }
 
