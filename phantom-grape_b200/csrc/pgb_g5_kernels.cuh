@@ -230,7 +230,6 @@ __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
     constexpr bool LANES = (IPT == 1 && NT <= 64);
     __shared__ float4 sj[NT * (W > 2 ? W : 2)];  // also the reduction buffer (double4 x NT)
     __shared__ int s_task, s_flag;
-    // table kind: the whole force table in shared memory for the lifetime of the CTA
     // table kind: the force table in dynamic shared memory sized to the table (A.tbl_size
     // entries, 8 KB for 1024) for the lifetime of the CTA; the other kinds launch without any
     extern __shared__ float2 g5_dyn_tab[];
@@ -243,10 +242,131 @@ __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
         __syncthreads();
     }
 
+    // Tasks of more than NT/2 i in the 64-thread one-i-per-thread CTAs: two i per thread
+    // (slot and slot + NT/2) and two j-lanes (even and odd records of each tile), so that every
+    // j record loaded from shared memory serves two i and their sums take paired FP32
+    // instructions; the two lanes' sums are added in lane order.
+    auto lanes_pair_task = [&](const Task& T) {
+        constexpr int H = NT / 2;
+        const int slot = (int)threadIdx.x % H, lane = (int)threadIdx.x / H;
+        float xi[2], yi[2], zi[2], ei[2];
+        double S[2][4];
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const int li = slot + k * H;
+            const float4 p = A.ipos[T.i0 + (li < T.ni ? li : 0)];
+            xi[k] = p.x; yi[k] = p.y; zi[k] = p.z; ei[k] = p.w;
+            S[k][0] = S[k][1] = S[k][2] = S[k][3] = 0.0;
+        }
+        for (int jt = 0; jt < T.nj; jt += NT) {
+            const int nt = min(NT, T.nj - jt);
+            __syncthreads();
+            if (threadIdx.x < nt) {
+                const int jk = T.j0 + jt + threadIdx.x;
+                const int jj = A.jidx ? __ldg(A.jidx + jk) : jk;
+                sj[threadIdx.x] = A.jpos[jj];
+                if constexpr (W == 2) sj[NT + threadIdx.x] = A.jaux[jj];
+                if constexpr (W == 3) {
+                    sj[NT + 2 * threadIdx.x] = A.jaux[2 * jj];
+                    sj[NT + 2 * threadIdx.x + 1] = A.jaux[2 * jj + 1];
+                }
+            }
+            __syncthreads();
+            // one block: a lane sees at most NT/2 <= G5_FOLD records of a tile
+            float2 a2[4];
+            a2[0] = a2[1] = a2[2] = a2[3] = make_float2(0.f, 0.f);
+#pragma unroll 4
+            for (int j = lane; j < nt; j += 2)
+                g5_interact2<KIND, NT>(sj, j, xi, yi, zi, ei, tab, shift, A.r2cut, a2);
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+#pragma unroll
+                for (int c = 0; c < 4; c++) S[k][c] += (double)lane_of(a2[c], k);
+            }
+        }
+        // lane 1's sums into lane 0's, one i per round through the j-tile buffer
+        double4* red = reinterpret_cast<double4*>(sj);
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            __syncthreads();
+            red[threadIdx.x] = make_double4(S[k][0], S[k][1], S[k][2], S[k][3]);
+            __syncthreads();
+            if (lane == 0) {
+                const double4 v = red[slot + H];
+                S[k][0] += v.x;
+                S[k][1] += v.y;
+                S[k][2] += v.z;
+                S[k][3] += v.w;
+            }
+        }
+        if (lane != 0) return;
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const int li = slot + k * H;
+            if (li >= T.ni) continue;
+            const double4 v = make_double4(S[k][0], S[k][1], S[k][2], S[k][3]);
+            if (T.group < 0) A.out[T.i0 + li] = g5_finish<KIND>(v, A.ascale);
+            else A.partial[(size_t)T.slot * A.itile + li] = v;
+        }
+    };
+
+    // The last CTA to finish a task of a split group reduces the group's partial rows.
+    auto group_done = [&](const Task& T) {
+        const Group G = A.groups[T.group];
+        if (group_arrive(A.group_counters, T.group, G.nchunk, &s_flag)) {
+            // Cooperative reduction of the group's partial rows: P threads per i, each summing a
+            // fixed strided subset of the rows, then the P sums in thread order (deterministic
+            // for a given group shape).  `red` reuses the j-tile buffer.
+            double4* red = reinterpret_cast<double4*>(sj);
+            static_assert(sizeof(float4) * NT * (W > 2 ? W : 2) >= sizeof(double4) * NT, "reduction buffer");
+            int P = 1;
+            while (P * 2 * G.ni <= NT) P *= 2;
+            const int per = NT / P;
+            for (int base = 0; base < G.ni; base += per) {
+                const int li = base + threadIdx.x / P, p = threadIdx.x % P;
+                double4 s = make_double4(0, 0, 0, 0);
+                if (li < G.ni) {
+                    // four independent partial sums keep four rows' loads in flight; combined in
+                    // a fixed order (deterministic)
+                    const double4* col = A.partial + (size_t)G.slot0 * A.itile + li;
+                    auto ld = [&](int c) {
+                        const double4* r = col + (size_t)c * A.itile;
+                        return make_double4(__ldcg(&r->x), __ldcg(&r->y), __ldcg(&r->z), __ldcg(&r->w));
+                    };
+                    double4 s1 = s, s2 = s, s3 = s;
+                    int c = p;
+                    for (; c + 3 * P < G.nchunk; c += 4 * P) {
+                        double4 v0 = ld(c), v1 = ld(c + P), v2 = ld(c + 2 * P), v3 = ld(c + 3 * P);
+                        s = add4(s, v0);
+                        s1 = add4(s1, v1);
+                        s2 = add4(s2, v2);
+                        s3 = add4(s3, v3);
+                    }
+                    for (; c < G.nchunk; c += P) s = add4(s, ld(c));
+                    s = add4(add4(s, s1), add4(s2, s3));
+                }
+                __syncthreads();
+                red[threadIdx.x] = s;
+                __syncthreads();
+                if (p == 0 && li < G.ni) {
+                    for (int q = 1; q < P; q++) s = add4(s, red[threadIdx.x + q]);
+                    A.out[G.i0 + li] = g5_finish<KIND>(s, A.ascale);
+                }
+            }
+        }
+    };
+
     for (bool first = true;; first = false) {
         int t = next_task(A.task_counter, &s_task, A.ntasks, first);
         if (t >= A.ntasks) break;
         const Task T = A.tasks[t];
+        if constexpr (LANES) {
+            if (T.ni > NT / 2) {
+                lanes_pair_task(T);
+                if (T.group >= 0) group_done(T);
+                continue;
+            }
+        }
         // j-lanes (the 64-thread one-i-per-thread CTAs): a task of few i takes half-warps of
         // i-slots (isl = ni rounded up to 16; the two half-warps of a warp then read two j records,
         // which a 16-byte shared load serves in the same two wavefronts as a broadcast) and
@@ -370,48 +490,7 @@ __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
             int li = slot + k * NT;
             if (lane0 && li < T.ni) row[li] = make_double4(S[k][0], S[k][1], S[k][2], S[k][3]);
         }
-        const Group G = A.groups[T.group];
-        if (group_arrive(A.group_counters, T.group, G.nchunk, &s_flag)) {
-            // Cooperative reduction of the group's partial rows: P threads per i, each summing a
-            // fixed strided subset of the rows, then the P sums in thread order (deterministic
-            // for a given group shape).  `red` reuses the j-tile buffer.
-            double4* red = reinterpret_cast<double4*>(sj);
-            static_assert(sizeof(float4) * NT * (W > 2 ? W : 2) >= sizeof(double4) * NT, "reduction buffer");
-            int P = 1;
-            while (P * 2 * G.ni <= NT) P *= 2;
-            const int per = NT / P;
-            for (int base = 0; base < G.ni; base += per) {
-                const int li = base + threadIdx.x / P, p = threadIdx.x % P;
-                double4 s = make_double4(0, 0, 0, 0);
-                if (li < G.ni) {
-                    // four independent partial sums keep four rows' loads in flight; combined in
-                    // a fixed order (deterministic)
-                    const double4* col = A.partial + (size_t)G.slot0 * A.itile + li;
-                    auto ld = [&](int c) {
-                        const double4* r = col + (size_t)c * A.itile;
-                        return make_double4(__ldcg(&r->x), __ldcg(&r->y), __ldcg(&r->z), __ldcg(&r->w));
-                    };
-                    double4 s1 = s, s2 = s, s3 = s;
-                    int c = p;
-                    for (; c + 3 * P < G.nchunk; c += 4 * P) {
-                        double4 v0 = ld(c), v1 = ld(c + P), v2 = ld(c + 2 * P), v3 = ld(c + 3 * P);
-                        s = add4(s, v0);
-                        s1 = add4(s1, v1);
-                        s2 = add4(s2, v2);
-                        s3 = add4(s3, v3);
-                    }
-                    for (; c < G.nchunk; c += P) s = add4(s, ld(c));
-                    s = add4(add4(s, s1), add4(s2, s3));
-                }
-                __syncthreads();
-                red[threadIdx.x] = s;
-                __syncthreads();
-                if (p == 0 && li < G.ni) {
-                    for (int q = 1; q < P; q++) s = add4(s, red[threadIdx.x + q]);
-                    A.out[G.i0 + li] = g5_finish<KIND>(s, A.ascale);
-                }
-            }
-        }
+        group_done(T);
     }
 }
 
