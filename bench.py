@@ -56,10 +56,10 @@ PROFILED_TRAFFIC = {
     "hermite": {"bytes": 6_485_760 + 17_935_104,
                 "source": "profiles/g6_kernel_hermite_65536x65536.md (128x2 configuration, paired accumulations)"},
     "direct": {"bytes": 542_720, "pairs": 268_435_456, "source": "profiles/g5_kernels_direct_treepm_bh.md (1024x1)"},
-    "treepm": {"bytes": 555_061_760 + 36_073_728, "pairs": 4_463_983_086,
+    "treepm": {"bytes": 557_901_056 + 35_891_456, "pairs": 4_463_983_086,
                "source": "profiles/g5_kernels_direct_treepm_bh.md (64x1)"},
     # captured at N = 2^20 (both launches of a step); scaled to the run's pairs
-    "bh": {"bytes": 131_627_264 + 26_349_568 + 227_442_176 + 31_748_864, "pairs": 4_462_862_693,
+    "bh": {"bytes": 132_306_688 + 27_293_184 + 228_275_200 + 31_873_536, "pairs": 4_462_862_693,
            "source": "profiles/g5_kernels_direct_treepm_bh.md (64x1, N=2^20 capture scaled by pairs)"},
 }
 
