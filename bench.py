@@ -49,6 +49,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 SM_COUNT = 148
+# the reference source tree (only to build the checker when its build is missing)
+REF_SRC = os.environ.get("PGB_REFERENCE", "/root/reference")
 # DRAM bytes (read + write) of one launch of the roofline kernel, from the committed ncu captures
 # (dram__bytes_read.sum + dram__bytes_write.sum); the bench cannot run ncu itself.
 G5_CFG_NAMES = ["128x4", "256x2", "512x2", "1024x1", "384x2", "128x2", "128x1", "64x1"]   # pgb5 configurations (threads x i/thread)
@@ -95,6 +97,52 @@ def peaks():
         with open(p) as f:
             return json.load(f)
     return {"sm_max_mhz": 1965.0, "hbm_gbs": 6650.0}
+
+
+_PIPE_PEAKS = {}
+
+
+def pipe_peaks(pgb, stream_ptr=0):
+    """Measured FP32 FFMA and MUFU rsqrt throughput of this GPU (lib/libpgbpeak.so: independent
+    FFMA / rsqrt.approx chains on every SM, best of 5 CUDA-event-timed launches), with the SM
+    clock sampled while they run.  Cached per process (measured once, right after the first
+    workload's timed region)."""
+    if _PIPE_PEAKS:
+        return _PIPE_PEAKS
+    L = C.CDLL(pgb.ffi.lib_path("libpgbpeak.so"), mode=os.RTLD_LOCAL | os.RTLD_NOW)
+    dp, ip = C.POINTER(C.c_double), C.POINTER(C.c_int)
+    L.pgb_peak_fp32.argtypes = [C.c_int, C.c_void_p, dp, dp, ip]
+    L.pgb_peak_mufu.argtypes = [C.c_int, C.c_void_p, dp, dp, ip]
+    tf, ms, g = C.c_double(), C.c_double(), C.c_int()
+    mg, mms, mgr = C.c_double(), C.c_double(), C.c_int()
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    clocks.start()
+    rc1 = L.pgb_peak_fp32(20000, C.c_void_p(stream_ptr), C.byref(tf), C.byref(ms), C.byref(g))
+    rc2 = L.pgb_peak_mufu(2500, C.c_void_p(stream_ptr), C.byref(mg), C.byref(mms), C.byref(mgr))
+    clk = clocks.stop()
+    if rc1 == 0:
+        _PIPE_PEAKS.update({"fp32_tflops": round(tf.value, 2), "fp32_ms": round(ms.value, 3), "fp32_ctas": g.value})
+    if rc2 == 0:
+        _PIPE_PEAKS.update({"mufu_grsqrt_s": round(mg.value, 1), "mufu_ms": round(mms.value, 3),
+                            "mufu_per_sm_clk": round(mg.value * 1e9 / SM_COUNT / ((clk.get("sm_mhz") or 1965.0) * 1e6), 2)})
+    _PIPE_PEAKS["sm_mhz"] = clk.get("sm_mhz")
+    _PIPE_PEAKS["how"] = ("lib/libpgbpeak.so: 8 independent FFMA (rsqrt.approx.ftz.f32) chains per thread, 256-thread "
+                          "CTAs at full occupancy on every SM, best of 5 launches (CUDA events)")
+    return _PIPE_PEAKS
+
+
+def fp32_peak(pgb, clk, stream_ptr=0):
+    """The FP32 roofline denominator: the measured FFMA throughput (TFLOP/s) when the
+    microbenchmark ran, else 148 SMs x 128 lanes x 2 x the sampled SM clock; with its source."""
+    pk = peaks()
+    sm_mhz = clk.get("sm_mhz") or pk.get("sm_max_mhz", 1965.0)
+    nominal = SM_COUNT * FP32_LANES * 2 * sm_mhz * 1e6 / 1e12
+    pp = pipe_peaks(pgb, stream_ptr)
+    if pp.get("fp32_tflops"):
+        return pp["fp32_tflops"], nominal, (f"measured: {pp['fp32_tflops']} TFLOP/s FFMA microbenchmark "
+                                            f"(lib/libpgbpeak.so) at {pp.get('sm_mhz')} MHz; nominal 148 SM x 128 "
+                                            f"lanes x 2 x {sm_mhz:.0f} MHz (timed-region clock) = {nominal:.1f}")
+    return nominal, nominal, f"nominal: 148 SM x 128 FP32 lanes x 2 x median SM clock {sm_mhz:.0f} MHz"
 
 
 # ----------------------------------------------------------------------------------------
@@ -248,6 +296,9 @@ class Driver:
         L.g6drv_schedule.argtypes = [vp, C.c_int, C.c_int, ip, ip, dp, dp, dp, C.c_double, C.c_int, C.c_int,
                                      dp, dp, dp, dp, dp, dp, ip, dp, dp, dp, ip, C.POINTER(C.c_float)]
         L.g6drv_schedule.restype = C.c_double
+        L.g6drv_schedule2.argtypes = [vp, C.c_int, C.c_int, ip, ip, dp, dp, dp, C.c_double, C.c_int, C.c_int, ip, ip,
+                                      dp, dp, dp, dp, dp, dp, ip, dp, dp, dp, ip, C.POINTER(C.c_float)]
+        L.g6drv_schedule2.restype = C.c_double
         L.g5drv_open.argtypes = [C.c_char_p]
         L.g5drv_open.restype = vp
         L.g5drv_direct.argtypes = [vp, C.c_int, dp, dp, C.c_double, dp, dp]
@@ -274,8 +325,10 @@ class Driver:
         return self.L.g6drv_set_j(h, len(st.mass), p(st.pos), p(st.vel), p(st.acc2), p(st.jrk6), p(st.mass),
                                   p(st.tj), p(st.idx, C.c_int), None)
 
-    def g6_schedule(self, h, wl, calls=None, resend=True, outputs=False):
-        """Run calls [0, calls) of the schedule; returns (seconds, pairs, outputs or None)."""
+    def g6_schedule(self, h, wl, calls=None, resend=True, outputs=False, resend_sets=None):
+        """Run calls [0, calls) of the schedule; returns (seconds, pairs, outputs or None).
+        resend_sets: {"off", "idx"} of the particles re-sent after each call (default: the
+        call's own active set)."""
         st, p = wl["st"], self.p
         ncalls = len(wl["sets"]) if calls is None else calls
         off = wl["set_off"]
@@ -285,19 +338,21 @@ class Driver:
             out = dict(acc=np.zeros((nact, 3)), jrk=np.zeros((nact, 3)), pot=np.zeros(nact),
                        nnb=np.zeros(nact, np.int32), rnnb=np.zeros(nact, np.float32))
         o = out or {}
-        sec = self.L.g6drv_schedule(h, wl["n"], ncalls, p(off, C.c_int), p(wl["set_idx"], C.c_int), p(wl["t_calls"]),
-                                    p(wl["xi"]), p(wl["vi"]), st.eps2, 1, 1 if resend else 0, p(st.pos), p(st.vel),
-                                    p(st.acc2), p(st.jrk6), p(st.mass), p(st.tj), p(st.idx, C.c_int),
-                                    p(o.get("acc")), p(o.get("jrk")), p(o.get("pot")), p(o.get("nnb"), C.c_int),
-                                    p(o.get("rnnb"), C.c_float))
+        rs = resend_sets or {}
+        sec = self.L.g6drv_schedule2(h, wl["n"], ncalls, p(off, C.c_int), p(wl["set_idx"], C.c_int),
+                                     p(wl["t_calls"]), p(wl["xi"]), p(wl["vi"]), st.eps2, 1, 1 if resend else 0,
+                                     p(rs.get("off"), C.c_int), p(rs.get("idx"), C.c_int), p(st.pos), p(st.vel),
+                                     p(st.acc2), p(st.jrk6), p(st.mass), p(st.tj), p(st.idx, C.c_int),
+                                     p(o.get("acc")), p(o.get("jrk")), p(o.get("pot")), p(o.get("nnb"), C.c_int),
+                                     p(o.get("rnnb"), C.c_float))
         return sec, nact * wl["n"], out
 
 
 def ref_lib(name):
     """The reference's own build (oracle/_ref), compiled here when the reference is present."""
     path = os.path.join(ROOT, "oracle", "_ref", name)
-    if not os.path.exists(path) and os.path.isdir("/root/reference"):
-        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=False)
+    if not os.path.exists(path) and os.path.isdir(REF_SRC):
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={REF_SRC}"], check=False)
     return path if os.path.exists(path) else None
 
 
@@ -323,14 +378,154 @@ def cpu_baseline_hermite(pgb, wl, target_pairs=1.2e10):
                       f"libpg6 AVX2 + OpenMP (PG6/libpg6 built from its sources), npipes 48"}
 
 
+def hermite_shard(pgb, wl, ws, rank):
+    """This rank's part of the schedule: a contiguous slice of every call's active set
+    (phantom-grape_b200/shard.py).  Returns (sub-schedule, its rows in the schedule's order,
+    [(call, local offset, count)], rows of every rank)."""
+    S = pgb.shard
+    sizes = [len(x) for x in wl["sets"]]
+    sl = S.shard_schedule(sizes, ws, rank)
+    off = wl["set_off"]
+    rows, calls, loc = [], [], 0
+    for c, (lo, hi) in enumerate(sl):
+        rows.append(np.arange(off[c] + lo, off[c] + hi))
+        calls.append((c, loc, int(hi - lo)))
+        loc += int(hi - lo)
+    rows = np.concatenate(rows).astype(np.int64)
+    sub = dict(wl)
+    sub["sets"] = [wl["sets"][c][lo:hi] for c, (lo, hi) in enumerate(sl)]
+    sub["set_off"] = np.concatenate([[0], np.cumsum([len(x) for x in sub["sets"]])]).astype(np.int32)
+    sub["set_idx"] = np.ascontiguousarray(wl["set_idx"][rows], np.int32)
+    sub["xi"], sub["vi"] = np.ascontiguousarray(wl["xi"][rows]), np.ascontiguousarray(wl["vi"][rows])
+    sub["pairs"] = len(rows) * wl["n"]
+    _, nrows = S.rank_major_order(sizes, ws)
+    return sub, rows, calls, nrows
+
+
+def hermite_batched(args, pgb, g6, wl, sub, calls, dev, s, ff, tune, steps, warmup, flush, ws, nrows, dist,
+                    clocks=None):
+    """The batched device path of the schedule (this rank's share): j-memory, i-records and
+    results resident in HBM, one plan per call, the calls' (predict + force) launches captured in
+    one CUDA graph; with several ranks the step ends with the all-gather of every rank's results.
+    Times `steps` replays (CUDA events on the launching stream, L2 flushed in between), then each
+    force launch alone.  Returns a dict of the figures and the resident buffers."""
+    import torch
+    ffi = pgb.ffi
+    st, n = wl["st"], wl["n"]
+    ptcl = np.zeros(n, ffi.G6PTCL)
+    ptcl["pos"], ptcl["vel"], ptcl["acc2"], ptcl["jrk6"] = st.pos, st.vel, st.acc2, st.jrk6
+    ptcl["mass"], ptcl["tim"], ptcl["idx"] = st.mass, st.tj, st.idx
+    nrow = len(sub["set_idx"])
+    pflags = 0 if ff else g6.POS_F64
+    irec = ffi.g6_irecords(sub["xi"], sub["vi"], st.idx[sub["set_idx"]], ff=ff)
+    d_ptcl = torch.from_numpy(ptcl.view(np.uint8)).to(dev)
+    d_irec = torch.from_numpy(irec.view(np.uint8)).to(dev)
+    d_pred = torch.zeros(n * ffi.G6PREDJ.itemsize, dtype=torch.uint8, device=dev)
+    d_out = torch.zeros((max(nrow, 1), ffi.G6OUT.itemsize), dtype=torch.uint8, device=dev)
+    live = [(c, loc, cnt) for c, loc, cnt in calls if cnt > 0]
+    plans = {c: g6.plan_create([[loc, cnt, 0, n]], nn=True, f64=not ff) for c, loc, cnt in live}
+
+    def predict(c):
+        rc = g6.L.pgb6_predict(d_ptcl.data_ptr(), n, float(wl["t_calls"][c]), d_pred.data_ptr(), pflags,
+                               s.cuda_stream)
+        assert rc == 0, g6.last_error()
+
+    def step_launches():
+        for c, _, _ in live:
+            predict(c)
+            g6.plan_launch(plans[c], d_irec.data_ptr(), d_pred.data_ptr(), st.eps2, d_out.data_ptr(), s.cuda_stream)
+
+    with torch.cuda.stream(s):
+        step_launches()
+    s.synchronize()
+    tuned = {}
+    if tune:
+        # autotune the kernel configuration once per active-set size, on the real data
+        for c, loc, cnt in live:
+            if cnt in tuned:
+                continue
+            predict(c)
+            cfg, _ = g6.plan_tune(plans[c], d_irec.data_ptr(), d_pred.data_ptr(), st.eps2, d_out.data_ptr(),
+                                  s.cuda_stream)
+            tuned[cnt] = cfg
+        for c, loc, cnt in live:   # re-create the plans so that every plan picks up its tuned shape
+            g6.plan_destroy(plans[c])
+            plans[c] = g6.plan_create([[loc, cnt, 0, n]], nn=True, f64=not ff)
+        with torch.cuda.stream(s):
+            step_launches()
+        s.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=s):
+        step_launches()
+
+    def step():
+        graph.replay()
+        if ws > 1:
+            pgb.shard.gather_rows(d_out[:nrow], nrows, dist)
+
+    with torch.cuda.stream(s):
+        for _ in range(warmup):
+            step()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    if clocks:
+        clocks.start()
+    barrier(ws)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(s):
+        for k in range(steps):
+            ev[k][0].record(s)
+            step()
+            ev[k][1].record(s)
+            flush.fill_(k & 0xFF)   # 256 MiB write between steps: L2 (126 MB) flushed
+    torch.cuda.synchronize()
+    barrier(ws)
+    clk = clocks.stop() if clocks else {}
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    # roofline pass (after the timed region): each force launch timed alone with CUDA events
+    fev = []
+    with torch.cuda.stream(s):
+        for c, _, cnt in live:
+            predict(c)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(s)
+            g6.plan_launch(plans[c], d_irec.data_ptr(), d_pred.data_ptr(), st.eps2, d_out.data_ptr(), s.cuda_stream)
+            b.record(s)
+            fev.append((a, b, cnt * n, c))
+    torch.cuda.synchronize()
+    kern_s = sum(a.elapsed_time(b) for a, b, _, _ in fev) / 1e3
+    kern_pairs = sum(p for _, _, p, _ in fev)
+    big = max(fev, key=lambda e: e[2])
+    return dict(step_ms=step_ms, clk=clk, tuned=tuned, graph=graph, plans=plans, d_ptcl=d_ptcl, d_irec=d_irec,
+                d_out=d_out, ptcl=ptcl, irec=irec, nrow=nrow, kern_s=kern_s, kern_pairs=kern_pairs,
+                big_pairs=big[2], big_ms=big[0].elapsed_time(big[1]), big_call=big[3], step=step,
+                launches_per_step=2 * len(live))
+
+
+def hermite_fp64_check(pgb, wl, sub, calls, out_rows, ff_label=""):
+    """FP64 oracle check of the batched results of the largest call (every 64th active particle)."""
+    st, n = wl["st"], wl["n"]
+    c, loc, cnt = max(calls, key=lambda t: t[2])
+    sel = np.arange(loc, loc + cnt, max(1, cnt // 1024))
+    xp_c, vp_c = predict_np(wl["t_calls"][c], st)
+    ck = fp64_check_g6(out_rows[sel], sub["xi"][sel], sub["vi"][sel], st.idx[sub["set_idx"][sel]], st.eps2,
+                       xp_c, vp_c, st.mass, st.idx)
+    ck["call"] = f"call {c} ({cnt} active x {n} j), every {max(1, cnt // 1024)}th active particle{ff_label}"
+    return ck
+
+
 def run_hermite(args, pgb, ws, rank, local):
     import torch
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
+    dist = None
+    if ws > 1:
+        import torch.distributed as dist
     ffi = pgb.ffi
     g6 = ffi.G6()
     g6.L.g6_open(0)
-    wl = hermite_workload(pgb, g6, seed_offset=rank)
+    # one problem on every rank (strong scaling over the ranks' slices of each call)
+    wl = hermite_workload(pgb, g6)
     st, n, sets = wl["st"], wl["n"], wl["sets"]
     if args.profile_api:
         # profiling target: the drop-in API's full-size call (npipes = 48 i-particles against all
@@ -341,154 +536,144 @@ def run_hermite(args, pgb, ws, rank, local):
         for _ in range(4):
             g6.calc(st.t_now, n, st.pos[:ni], st.vel[:ni], st.idx[:ni], st.eps2, variant="2p")
         return {"profile": "drop-in API call", "ni": ni, "nj": n, "calls": 4}
-
-    # device-resident inputs: j-memory records, the i-records of every call, outputs
-    ptcl = np.zeros(n, ffi.G6PTCL)
-    ptcl["pos"], ptcl["vel"], ptcl["acc2"], ptcl["jrk6"] = st.pos, st.vel, st.acc2, st.jrk6
-    ptcl["mass"], ptcl["tim"], ptcl["idx"] = st.mass, st.tj, st.idx
-    nact = len(wl["set_idx"])
-    ff = not args.f64_positions
-    pflags = 0 if ff else g6.POS_F64
-    irec = ffi.g6_irecords(wl["xi"], wl["vi"], st.idx[wl["set_idx"]], ff=ff)
-    d_ptcl = torch.from_numpy(ptcl.view(np.uint8)).to(dev)
-    d_irec = torch.from_numpy(irec.view(np.uint8)).to(dev)
-    d_pred = torch.zeros(n * ffi.G6PREDJ.itemsize, dtype=torch.uint8, device=dev)
-    d_out = torch.zeros(nact * ffi.G6OUT.itemsize, dtype=torch.uint8, device=dev)
-    off = wl["set_off"]
-    plans = [g6.plan_create([[int(off[c]), len(sets[c]), 0, n]], nn=True, f64=not ff) for c in range(len(sets))]
+    sub, rows, calls, nrows = hermite_shard(pgb, wl, ws, rank)
     s = torch.cuda.Stream(device=dev)
-
-    def step_launches():
-        for c in range(len(sets)):
-            rc = g6.L.pgb6_predict(d_ptcl.data_ptr(), n, float(wl["t_calls"][c]), d_pred.data_ptr(), pflags,
-                                   s.cuda_stream)
-            assert rc == 0
-            g6.plan_launch(plans[c], d_irec.data_ptr(), d_pred.data_ptr(), st.eps2, d_out.data_ptr(), s.cuda_stream)
-
-    with torch.cuda.stream(s):
-        step_launches()
-    s.synchronize()
-    tuned = {}
-    if not args.no_tune and not args.profile_largest:
-        # autotune the kernel configuration once per active-set size, on the real data
-        for c in range(len(sets)):
-            if len(sets[c]) in tuned:
-                continue
-            g6.L.pgb6_predict(d_ptcl.data_ptr(), n, float(wl["t_calls"][c]), d_pred.data_ptr(), pflags,
-                              s.cuda_stream)
-            cfg, ms = g6.plan_tune(plans[c], d_irec.data_ptr(), d_pred.data_ptr(), st.eps2, d_out.data_ptr(),
-                                   s.cuda_stream)
-            tuned[len(sets[c])] = cfg
-        for c in range(len(sets)):   # re-create the plans so that every plan picks up its tuned shape
-            g6.plan_destroy(plans[c])
-            plans[c] = g6.plan_create([[int(off[c]), len(sets[c]), 0, n]], nn=True, f64=not ff)
-        with torch.cuda.stream(s):
-            step_launches()
-        s.synchronize()
+    ff = not args.f64_positions
     if args.profile_largest:
-        # profiling target: after the warm pass above (1 + 64 force launches), the largest call's
-        # force launch three times; nothing else allocated, no timing
-        big = max(range(len(sets)), key=lambda c: len(sets[c]))
+        # profiling target: after the warm pass (1 + 64 force launches), the largest call's force
+        # launch three times; nothing else allocated, no timing
+        live = [(c, loc, cnt) for c, loc, cnt in calls if cnt > 0]
+        ffi_ = pgb.ffi
+        ptcl = np.zeros(n, ffi_.G6PTCL)
+        ptcl["pos"], ptcl["vel"], ptcl["acc2"], ptcl["jrk6"] = st.pos, st.vel, st.acc2, st.jrk6
+        ptcl["mass"], ptcl["tim"], ptcl["idx"] = st.mass, st.tj, st.idx
+        irec = ffi_.g6_irecords(sub["xi"], sub["vi"], st.idx[sub["set_idx"]], ff=ff)
+        d_ptcl = torch.from_numpy(ptcl.view(np.uint8)).to(dev)
+        d_irec = torch.from_numpy(irec.view(np.uint8)).to(dev)
+        d_pred = torch.zeros(n * ffi_.G6PREDJ.itemsize, dtype=torch.uint8, device=dev)
+        d_out = torch.zeros(len(rows) * ffi_.G6OUT.itemsize, dtype=torch.uint8, device=dev)
+        pflags = 0 if ff else g6.POS_F64
+        plans = {c: g6.plan_create([[loc, cnt, 0, n]], nn=True, f64=not ff) for c, loc, cnt in live}
         with torch.cuda.stream(s):
+            for c, _, _ in live:
+                g6.L.pgb6_predict(d_ptcl.data_ptr(), n, float(wl["t_calls"][c]), d_pred.data_ptr(), pflags,
+                                  s.cuda_stream)
+                g6.plan_launch(plans[c], d_irec.data_ptr(), d_pred.data_ptr(), st.eps2, d_out.data_ptr(),
+                               s.cuda_stream)
+            big = max(live, key=lambda t: t[2])[0]
             g6.L.pgb6_predict(d_ptcl.data_ptr(), n, float(wl["t_calls"][big]), d_pred.data_ptr(), pflags,
-                                   s.cuda_stream)
+                              s.cuda_stream)
             for _ in range(3):
                 g6.plan_launch(plans[big], d_irec.data_ptr(), d_pred.data_ptr(), st.eps2, d_out.data_ptr(),
                                s.cuda_stream)
         s.synchronize()
-        for p_ in plans:
+        for p_ in plans.values():
             g6.plan_destroy(p_)
         return {"profile": "largest Hermite call", "call": big, "active": len(sets[big]), "nj": n,
-                "force_launches_before": 1 + len(sets)}
+                "force_launches_before": 1 + len(live)}
+
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    graph = torch.cuda.CUDAGraph()
-    with torch.cuda.graph(graph, stream=s):
-        step_launches()
-
-    for _ in range(args.warmup):
-        graph.replay()
-    torch.cuda.synchronize()
-
     clocks = ClockSampler(local)
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    clocks.start()
-    barrier(ws)
-    torch.cuda.synchronize()
-    for k in range(args.steps):
-        with torch.cuda.stream(s):
-            ev[k][0].record(s)
-            graph.replay()
-            ev[k][1].record(s)
-            flush.fill_(k & 0xFF)   # 256 MiB write between steps: L2 (126 MB) flushed
-    torch.cuda.synchronize()
-    barrier(ws)
-    clk = clocks.stop()
-    step_ms = [a.elapsed_time(b) for a, b in ev]
-    t_local = sum(step_ms) / 1e3
+    B = hermite_batched(args, pgb, g6, wl, sub, calls, dev, s, ff, not args.no_tune, args.steps, args.warmup, flush,
+                        ws, nrows, dist, clocks=clocks)
+    clk = B["clk"]
+    t_local = sum(B["step_ms"]) / 1e3
     t_max = reduce_max(t_local, ws, dev)
-    pairs_total = reduce_sum(float(wl["pairs"]) * args.steps, ws, dev)
-    value = pairs_total / t_max / 1e9
+    value = float(wl["pairs"]) * args.steps / t_max / 1e9      # the whole schedule per step
+    fp32_tf, fp32_nominal, peak_src = fp32_peak(pgb, clk, s.cuda_stream)
+    achieved_tf = B["big_pairs"] * 60 / (B["big_ms"] / 1e3) / 1e12
+    achieved_all_tf = B["kern_pairs"] * 60 / B["kern_s"] / 1e12
 
-    # roofline pass (after the timed region): each force launch timed alone with CUDA events
-    fev = []
-    with torch.cuda.stream(s):
-        for c in range(len(sets)):
-            g6.L.pgb6_predict(d_ptcl.data_ptr(), n, float(wl["t_calls"][c]), d_pred.data_ptr(), pflags,
-                                   s.cuda_stream)
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record(s)
-            g6.plan_launch(plans[c], d_irec.data_ptr(), d_pred.data_ptr(), st.eps2, d_out.data_ptr(), s.cuda_stream)
-            b.record(s)
-            fev.append((a, b, len(sets[c]) * n))
-    torch.cuda.synchronize()
-    kern_s = sum(a.elapsed_time(b) for a, b, _ in fev) / 1e3
-    kern_pairs = sum(p for _, _, p in fev)
-    big = max(fev, key=lambda e: e[2])
-    big_ms = big[0].elapsed_time(big[1])
+    # the batched path end to end with host buffers: every step copies the j-memory and the
+    # i-records of every call from pinned host memory, replays the graph (and gathers), and
+    # reads every result back; CUDA events on the stream around copies and compute
+    h_ptcl = torch.from_numpy(B["ptcl"].view(np.uint8)).pin_memory()
+    h_irec = torch.from_numpy(B["irec"].view(np.uint8)).pin_memory()
+    tot_rows = int(sum(nrows))
+    h_out = torch.empty((tot_rows, ffi.G6OUT.itemsize), dtype=torch.uint8).pin_memory()
+    e2e_b_ms = []
+    for k in range(args.warmup + args.e2e_steps):
+        a_, b_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(s):
+            a_.record(s)
+            B["d_ptcl"].copy_(h_ptcl, non_blocking=True)
+            B["d_irec"].copy_(h_irec, non_blocking=True)
+            B["graph"].replay()
+            res = B["d_out"][:B["nrow"]]
+            if ws > 1:
+                res = pgb.shard.gather_rows(res, nrows, dist)
+            h_out.copy_(res, non_blocking=True)
+            b_.record(s)
+        s.synchronize()
+        if k >= args.warmup:
+            e2e_b_ms.append(a_.elapsed_time(b_))
+    e2e_b = float(wl["pairs"]) * len(e2e_b_ms) / reduce_max(sum(e2e_b_ms) / 1e3, ws, dev) / 1e9
+    h2d_b = h_ptcl.numel() + h_irec.numel()
+    d2h_b = h_out.numel()
 
-    # end to end through the GRAPE-6 API with host buffers (same driver as the reference arm)
+    # end to end through the GRAPE-6 API with host buffers (same driver as the reference arm);
+    # with several ranks each runs the calls' slices it owns, re-sends every active particle (its
+    # j-memory is complete) and the results are gathered
     drv = Driver(pgb)
     h = drv.g6_open(pgb.ffi.lib_path("libpg6.so"))
     drv.g6_set_j(h, st)
-    drv.g6_schedule(h, wl, calls=4)   # warm-up
+    drv.g6_schedule(h, sub, calls=4)   # warm-up
     e2e_steps = max(1, min(args.steps, args.e2e_steps))
+    rs = dict(off=wl["set_off"], idx=wl["set_idx"])
+    outs = None
     torch.cuda.synchronize()
     barrier(ws)
     e2e_t = 0.0
     for _ in range(e2e_steps):
-        sec, _, _ = drv.g6_schedule(h, wl)
+        sec, _, outs = drv.g6_schedule(h, sub, outputs=ws > 1, resend_sets=rs)
+        if ws > 1:
+            t0 = time.perf_counter()
+            loc_rows = np.concatenate([outs["acc"], outs["jrk"], outs["pot"][:, None]], 1)
+            pgb.shard.gather_rows(torch.from_numpy(loc_rows).to(dev), nrows, dist).cpu()
+            sec += time.perf_counter() - t0
         e2e_t += sec
     e2e_max = reduce_max(e2e_t, ws, dev)
-    e2e_val = reduce_sum(float(wl["pairs"]) * e2e_steps, ws, dev) / e2e_max / 1e9
+    e2e_val = float(wl["pairs"]) * e2e_steps / e2e_max / 1e9
+    # the same calls' device time alone (events around each call's device work in the library)
+    g6.L.pgb6_call_device_ms(1)
+    g6.L.pgb6_set_call_timing(1)
+    sec_t, _, _ = drv.g6_schedule(h, sub, resend_sets=rs)
+    g6.L.pgb6_set_call_timing(0)
+    plain_dev_s = g6.L.pgb6_call_device_ms(1) / 1e3
+    plain_dev = float(sub["pairs"]) / plain_dev_s / 1e9 if plain_dev_s > 0 else None
     npipe = g6.L.g6_npipes()
-    nchunks = sum((len(x) + npipe - 1) // npipe for x in sets)
-    h2d = nact * (ffi.G6IREC.itemsize + ffi.G6PTCL.itemsize + 4) + nchunks * 16 + len(sets) * 0
+    nact = len(sub["set_idx"])
+    nchunks = sum((len(x) + npipe - 1) // npipe for x in sub["sets"])
+    h2d = nact * (ffi.G6IREC.itemsize + 4) + len(wl["set_idx"]) * ffi.G6PTCL.itemsize + nchunks * 16
     d2h = nact * ffi.G6OUT.itemsize
 
-    pk = peaks()
-    sm_mhz = clk.get("sm_mhz") or pk.get("sm_max_mhz", 1965.0)
-    fp32_peak_tf = SM_COUNT * FP32_LANES * 2 * sm_mhz * 1e6 / 1e12
-    fp32_peak_max = SM_COUNT * FP32_LANES * 2 * pk.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
-    # roofline of the dominant kernel, on its largest launch (65536 x 65536), timed alone with CUDA
-    # events on its stream; all 64 force launches together are reported beside it
-    achieved_tf = big[2] * 60 / (big_ms / 1e3) / 1e12
-    achieved_all_tf = kern_pairs * 60 / kern_s / 1e12
     cpu = None
+    out_rows = B["d_out"][:B["nrow"]].cpu().numpy().reshape(-1).view(ffi.G6OUT)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_hermite(pgb, wl)
-        # the FP64 check of the batched results of the largest call (the kernel configuration
-        # that dominates the time), on every 64th of its active particles
-        rows = d_out.cpu().numpy().view(ffi.G6OUT)
-        c = int(np.argmax([len(x) for x in sets]))
-        a0, a1 = int(off[c]), int(off[c + 1])
-        sel = np.arange(a0, a1, max(1, (a1 - a0) // 1024))
-        xp_c, vp_c = predict_np(wl["t_calls"][c], st)
-        cpu["fp64_check"] = fp64_check_g6(rows[sel], wl["xi"][sel], wl["vi"][sel],
-                                          st.idx[wl["set_idx"][sel]], st.eps2, xp_c, vp_c, st.mass, st.idx)
-        cpu["fp64_check"]["call"] = f"call {c} ({a1 - a0} active x {n} j), every {max(1, (a1 - a0) // 1024)}th active particle"
-    for p_ in plans:
+        cpu["fp64_check"] = hermite_fp64_check(pgb, wl, sub, calls, out_rows)
+    # the north star's FP64 relative coordinate (DADD + F2F), same schedule, same timing
+    f64line = None
+    if ws == 1 and not args.no_f64_line and ff:
+        s64 = torch.cuda.Stream(device=dev)
+        clk64 = ClockSampler(local)
+        B64 = hermite_batched(args, pgb, g6, wl, sub, calls, dev, s64, False, not args.no_tune,
+                              max(3, min(args.steps, 10)), args.warmup, flush, ws, nrows, dist, clocks=clk64)
+        v64 = float(wl["pairs"]) * len(B64["step_ms"]) / (sum(B64["step_ms"]) / 1e3) / 1e9
+        f64line = {"value": round(v64, 2), "unit": "Gint/s", "steps": len(B64["step_ms"]),
+                   "largest_launch_ms": round(B64["big_ms"], 3),
+                   "roofline_frac": round(B64["big_pairs"] * 60 / (B64["big_ms"] / 1e3) / 1e12 / fp32_tf, 4),
+                   "relative_coordinates": "FP64 subtract + F2F (the reference's own split, gravity.c:316-333)",
+                   "clocks": B64["clk"]}
+        if rank == 0 and not args.no_cpu_baseline:
+            rows64 = B64["d_out"][:B64["nrow"]].cpu().numpy().reshape(-1).view(ffi.G6OUT)
+            f64line["fp64_check"] = hermite_fp64_check(pgb, wl, sub, calls, rows64, " (FP64 x_j - x_i)")
+        for p_ in B64["plans"].values():
+            g6.plan_destroy(p_)
+        del B64
+    for p_ in B["plans"].values():
         g6.plan_destroy(p_)
-    del graph
+    del B["graph"]
     line = {
         "metric": "Gint/s (PG6 Hermite force+jerk+pot+NN, batched)",
         "value": round(value, 2),
@@ -498,35 +683,48 @@ def run_hermite(args, pgb, ws, rank, local):
         "warmup": args.warmup,
         "ms_per_step": round(t_max / args.steps * 1e3, 3),
         "higher_is_better": True,
-        "scaling": "weak",
+        "scaling": "strong" if ws > 1 else "weak",
         "vs_baseline": None,
         "dtype": "f32 (f64 predictor, " + ("double-float" if ff else "f64") + " x_j-x_i, f64 cross-tile sums)",
         "data": "synthetic (seeded Plummer, DF velocities; no dataset)",
-        "config": {"workload": "PG6 Hermite N=65536 Plummer eps=1e-4, 64 block-step calls of 2^k active "
-                               "(k=4..16), force+jerk+pot+nearest neighbour",
-                   "pairs_per_step": wl["pairs"], "flop_per_pair": 60, "l2": "flushed between steps (256 MiB write)",
-                   "parallelism": f"replicas x{ws} (independent schedules, no data-path collective)",
-                   "graph": "64 x (predict + persistent force launch) in one CUDA graph",
-                   "relative_coordinates": "double-float (hi+lo FP32)" if ff else "FP64 subtract + F2F"},
-        "frac_fp32": round(value * 1e9 * 60 / 1e12 / fp32_peak_tf, 4),
-        "roofline": {"bound": "fp32", "achieved": round(achieved_tf, 2), "peak": round(fp32_peak_tf, 2),
-                     "unit": "TFLOP/s", "frac": round(achieved_tf / fp32_peak_tf, 4),
+        "config": hermite_config(wl["pairs"], ws),
+        "setup": {"sharding": (f"i-partition x{ws}: every rank predicts all j and computes a contiguous slice of "
+                               "each call's active set; results all-gathered (NCCL) inside the timed step")
+                  if ws > 1 else "one GPU",
+                  "graph": "64 x (predict + persistent force launch) in one CUDA graph",
+                  "relative_coordinates": "double-float (hi+lo FP32)" if ff else "FP64 subtract + F2F"},
+        "frac_fp32": round(value * 1e9 * 60 / 1e12 / fp32_tf, 4),
+        "roofline": {"bound": "fp32", "achieved": round(achieved_tf, 2), "peak": round(fp32_tf, 2),
+                     "unit": "TFLOP/s", "frac": round(achieved_tf / fp32_tf, 4),
                      "traffic": PROFILED_TRAFFIC["hermite"]["bytes"] if ff else None,
                      "traffic_source": PROFILED_TRAFFIC["hermite"]["source"] if ff else None,
                      "kernel": "pgb::g6_kernel (autotuned configuration), largest call of the step "
-                               f"({big[2]:.3e} pairs, {big_ms:.3f} ms)",
+                               f"({B['big_pairs']:.3e} pairs, {B['big_ms']:.3f} ms)",
                      "achieved_all_launches": round(achieved_all_tf, 2),
-                     "peak_source": f"148 SM x 128 FP32 lanes x 2 x median SM clock {sm_mhz:.0f} MHz sampled "
-                                    f"in the timed region ({fp32_peak_max:.1f} TFLOP/s at sm_max_mhz)"},
+                     "peak_source": peak_src, "peak_nominal": round(fp32_nominal, 2),
+                     "mufu_peak_grsqrt_s": _PIPE_PEAKS.get("mufu_grsqrt_s"),
+                     "mufu_per_sm_clk": _PIPE_PEAKS.get("mufu_per_sm_clk")},
         "e2e": {"value": round(e2e_val, 2), "unit": "Gint/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "api": "GRAPE-6 drop-in (g6_set_ti, g6calc_firsthalf, "
                 "g6calc_lasthalf2p per npipes chunk, g6_set_j_particle of the active set), host buffers",
-                "npipes": npipe, "steps": e2e_steps},
-        "gpu_launches": args.steps * 2 * len(sets),
-        "autotune": {str(k): int(v) for k, v in sorted(tuned.items())},
+                "npipes": npipe, "steps": e2e_steps,
+                "device_only": {"value": round(plain_dev, 2) if plain_dev else None, "unit": "Gint/s",
+                                "how": "the same calls' device time (pgb6_call_device_ms: CUDA events around each "
+                                       "call's j update + prediction and force launch)"},
+                "batched": {"value": round(e2e_b, 2), "unit": "Gint/s", "h2d_bytes_per_step": int(h2d_b),
+                            "d2h_bytes_per_step": int(d2h_b), "steps": len(e2e_b_ms),
+                            "api": "pgb6_predict + pgb6_plan_launch per call (one CUDA graph) with the j-memory and "
+                                   "every call's i-records copied from pinned host memory and every result read "
+                                   "back each step; CUDA events on the stream"}},
+        "batched_vs_plain": {"device": round(value / plain_dev, 2) if plain_dev else None,
+                             "end_to_end": round(e2e_b / e2e_val, 2)},
+        "gpu_launches": args.steps * B["launches_per_step"],
+        "autotune": {str(k): int(v) for k, v in sorted(B["tuned"].items())},
         "clocks": clk,
         "cpu_baseline": cpu,
     }
+    if f64line:
+        line["f64_positions"] = f64line
     return line
 
 
@@ -578,22 +776,20 @@ def _timed_launches(torch, s, launch, steps, warmup, flush):
 
 
 def _line(args, ws, metric, value, t_step, pairs, flop, workload, dtype, achieved_tf, clk, e2e, cpu, launches,
-          extra=None, kernel=""):
+          extra=None, kernel="", parallelism=None):
     traffic, tsrc = profiled_traffic(args.workload, pairs)
-    pk = peaks()
-    sm_mhz = clk.get("sm_mhz") or pk.get("sm_max_mhz", 1965.0)
-    peak_tf = SM_COUNT * FP32_LANES * 2 * sm_mhz * 1e6 / 1e12
+    peak_tf, nominal_tf, peak_src = fp32_peak(load_pkg(), clk)
     line = {
         "metric": metric, "value": round(value, 2), "unit": "Gint/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(t_step * 1e3, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": dtype, "data": "synthetic (seeded; no dataset)",
         "config": {"workload": workload, "pairs_per_step": pairs, "flop_per_pair": flop,
-                   "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{ws}"},
+                   "l2": "flushed between steps (256 MiB write)",
+                   "parallelism": parallelism or (f"replicas x{ws}" if ws > 1 else "one GPU")},
         "frac_fp32": round((value * 1e9 * flop / 1e12 if isinstance(flop, (int, float)) else achieved_tf) / peak_tf, 4),
         "roofline": {"bound": "fp32", "achieved": round(achieved_tf, 2), "peak": round(peak_tf, 2), "unit": "TFLOP/s",
                      "frac": round(achieved_tf / peak_tf, 4), "traffic": traffic, "traffic_source": tsrc,
-                     "kernel": kernel,
-                     "peak_source": f"148 SM x 128 FP32 lanes x 2 x median SM clock {sm_mhz:.0f} MHz"},
+                     "kernel": kernel, "peak_source": peak_src, "peak_nominal": round(nominal_tf, 2)},
         "e2e": e2e, "gpu_launches": launches, "clocks": clk, "cpu_baseline": cpu,
     }
     if extra:
@@ -694,19 +890,33 @@ def run_clusters(args, pgb, ws, rank, local):
     ffi = pgb.ffi
     g6 = ffi.G6()
     g6.L.g6_open(0)
-    cs = W.cluster_set(seed=W.SEED0 + 4 + rank)
+    # one cluster set on every rank; with several ranks each takes a contiguous range of
+    # clusters of about equal cost (N_k^2) and the step ends with the all-gather of the results
+    cs = W.cluster_set(seed=W.SEED0 + 4)
     n = len(cs.mass)
     idx = np.arange(n, dtype=np.int32)
-    irec = ffi.g6_irecords(cs.pos, cs.vel, idx)
-    jrec = ffi.g6_jrecords(cs.pos, cs.vel, cs.mass, idx)
+    bnd = pgb.shard.contiguous_partition(cs.sizes.astype(np.float64) ** 2, ws)
+    c0, c1 = int(bnd[rank]), int(bnd[rank + 1])
+    p0, p1 = int(cs.offsets[c0]), int(cs.offsets[c1])
+    nrows = [int(cs.offsets[bnd[r + 1]] - cs.offsets[bnd[r]]) for r in range(ws)]
+    irec = ffi.g6_irecords(cs.pos[p0:p1], cs.vel[p0:p1], idx[p0:p1])
+    jrec = ffi.g6_jrecords(cs.pos[p0:p1], cs.vel[p0:p1], cs.mass[p0:p1], idx[p0:p1])
     d_i = torch.from_numpy(irec.view(np.uint8)).to(dev)
     d_j = torch.from_numpy(jrec.view(np.uint8)).to(dev)
-    d_o = torch.zeros(n * ffi.G6OUT.itemsize, dtype=torch.uint8, device=dev)
+    d_o = torch.zeros((max(p1 - p0, 1), ffi.G6OUT.itemsize), dtype=torch.uint8, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    items = np.stack([cs.offsets[:-1], cs.sizes, cs.offsets[:-1], cs.sizes], 1)
+    items = np.stack([cs.offsets[c0:c1] - p0, cs.sizes[c0:c1], cs.offsets[c0:c1] - p0, cs.sizes[c0:c1]], 1)
     plan = g6.plan_create(items, nn=True)
     s = torch.cuda.Stream(device=dev)
-    launch = lambda: g6.plan_launch(plan, d_i.data_ptr(), d_j.data_ptr(), cs.eps2, d_o.data_ptr(), s.cuda_stream)  # noqa
+    dist = None
+    if ws > 1:
+        import torch.distributed as dist
+
+    def launch():
+        g6.plan_launch(plan, d_i.data_ptr(), d_j.data_ptr(), cs.eps2, d_o.data_ptr(), s.cuda_stream)
+        if ws > 1:
+            pgb.shard.gather_rows(d_o[:p1 - p0], nrows, dist)
+
     cfg = None
     if not args.no_tune:
         cfg, _ = g6.plan_tune(plan, d_i.data_ptr(), d_j.data_ptr(), cs.eps2, d_o.data_ptr(), s.cuda_stream)
@@ -719,8 +929,9 @@ def run_clusters(args, pgb, ws, rank, local):
     t_local = sum(ts)
     t_max = reduce_max(t_local, ws, dev)
     pairs = int((cs.sizes.astype(np.int64) ** 2).sum())
-    value = reduce_sum(float(pairs) * len(ts), ws, dev) / t_max / 1e9
-    achieved = pairs * len(ts) * 60 / t_local / 1e12
+    my_pairs = int((cs.sizes[c0:c1].astype(np.int64) ** 2).sum())
+    value = float(pairs) * len(ts) / t_max / 1e9
+    achieved = my_pairs * len(ts) * 60 / t_local / 1e12
     # plain: 1024 x (g6_set_j_particle x N_k, g6_set_ti, npipes chunks of firsthalf/lasthalf2p)
     drv = Driver(pgb)
     p = Driver.p
@@ -731,10 +942,11 @@ def run_clusters(args, pgb, ws, rank, local):
     offs = cs.offsets.astype(np.int32)
     pos, vel, mass = (np.ascontiguousarray(a) for a in (cs.pos, cs.vel, cs.mass))
     h = drv.g6_open(pgb.ffi.lib_path("libpg6.so"))
-    drv.L.g6drv_clusters(h, 0, 8, p(offs, C.c_int), p(pos), p(vel), p(mass), cs.eps2, None, None, None, None, None)
-    e2e_t = drv.L.g6drv_clusters(h, 0, len(cs.sizes), p(offs, C.c_int), p(pos), p(vel), p(mass), cs.eps2,
+    drv.L.g6drv_clusters(h, c0, min(c0 + 8, c1), p(offs, C.c_int), p(pos), p(vel), p(mass), cs.eps2, None, None,
+                         None, None, None)
+    e2e_t = drv.L.g6drv_clusters(h, c0, c1, p(offs, C.c_int), p(pos), p(vel), p(mass), cs.eps2,
                                  None, None, None, None, None)
-    e2e_val = reduce_sum(float(pairs), ws, dev) / reduce_max(e2e_t, ws, dev) / 1e9
+    e2e_val = float(pairs) / reduce_max(e2e_t, ws, dev) / 1e9
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         path = ref_lib("libpg6_ref.so")
@@ -751,7 +963,7 @@ def run_clusters(args, pgb, ws, rank, local):
                    "kind": "reference", "sample": f"first {ncl} of 1024 clusters ({cum[ncl - 1]:.3e} pairs), "
                    "PG6/libpg6 AVX2 + OpenMP through the same plain call sequence"}
         # FP64 check of the batched results of every 64th cluster
-        rows = d_o.cpu().numpy().view(ffi.G6OUT)
+        rows = d_o.cpu().numpy().reshape(-1).view(ffi.G6OUT)
         ck = {"acc": [], "jerk": [], "pot": [], "nn": 0, "n": 0}
         nsel = 0
         for k in range(0, len(cs.sizes), 64):
@@ -778,8 +990,11 @@ def run_clusters(args, pgb, ws, rank, local):
                  {"value": round(e2e_val, 3), "unit": "Gint/s", "h2d_bytes_per_step": n * (128 + 48),
                   "d2h_bytes_per_step": n * 64, "api": "plain GRAPE-6 calls per cluster (g6_set_j_particle x N_k, "
                   "g6_set_ti, g6calc_firsthalf/lasthalf2p per npipes), host buffers"},
-                 cpu, len(ts), extra={"autotune": cfg, "batched_vs_plain": round(value / e2e_val, 1)},
-                 kernel="pgb::g6_kernel (autotuned configuration)")
+                 cpu, len(ts), extra={"autotune": cfg, "batched_vs_plain": round(value / e2e_val, 1),
+                                      "scaling": "strong" if ws > 1 else "weak"},
+                 kernel="pgb::g6_kernel (autotuned configuration)",
+                 parallelism=(f"contiguous cost partition of the clusters x{ws}, results all-gathered in the step"
+                              if ws > 1 else "one GPU"))
 
 
 def split_force_np(r, ts_):
@@ -1363,6 +1578,15 @@ def run_reference_integrator(args, pgb, ws, rank):
     }
 
 
+def hermite_config(pairs, ws):
+    """The configuration both arms of the Hermite benchmark report (identical by construction)."""
+    return {"workload": "PG6 Hermite N=65536 Plummer eps=1e-4, 64 block-step calls of 2^k active (k=4..16), "
+                        "force+jerk+pot+nearest neighbour",
+            "pairs_per_step": int(pairs), "flop_per_pair": 60, "calls_per_step": 64,
+            "l2": "flushed between steps (256 MiB write); the CPU arm's working set exceeds its caches",
+            "parallelism": f"i-partition x{ws} (strong)" if ws > 1 else "one device"}
+
+
 def run_reference(args, pgb, ws, rank):
     if rank != 0:
         return None
@@ -1371,12 +1595,22 @@ def run_reference(args, pgb, ws, rank):
     path = ref_lib("libpg6_ref.so")
     if path is None:
         return {"impl": "reference", "unavailable": "reference library (oracle/_ref/libpg6_ref.so) not built"}
+    from oracle import refapi
     W = pgb.workloads
+
+    def ref_force(x, v, m, eps2):
+        # the state's acceleration and jerk from the reference library itself (all particles
+        # active, npipes chunks), so that no part of this arm runs on the GPU engine
+        R = refapi.RefG6()
+        idx = np.arange(len(x), dtype=np.int32)
+        z = np.zeros_like(x)
+        R.set_j(x, v, z, z, m, np.full(len(x), 1.0), idx)
+        r = R.calc(1.0, len(x), x, v, idx, eps2, variant="plain")
+        return r["acc"], r["jrk"]
+
     drv = Driver(pgb)
     h = drv.g6_open(path)
-    # same workload; a = j from an FP64-free source is not needed for timing: use the engine's
-    # own force only if a GPU is present, else zero acc/jerk (prediction cost is the same)
-    st = W.hermite_state(65536, seed=W.SEED0 + 1)
+    st = W.hermite_state(65536, seed=W.SEED0 + 1, force_fn=ref_force)
     sets = W.hermite_schedule(65536, 64, seed=W.SEED0 + 101)
     t_calls = st.t_now + np.arange(64) * 2.0 ** -20
     set_off = np.concatenate([[0], np.cumsum([len(s) for s in sets])]).astype(np.int32)
@@ -1389,25 +1623,25 @@ def run_reference(args, pgb, ws, rank):
         vi[set_off[c]:set_off[c + 1]] = v[s]
     wl = dict(st=st, sets=sets, t_calls=t_calls, set_off=set_off, set_idx=set_idx, xi=xi, vi=vi, n=65536)
     drv.g6_set_j(h, st)
-    calls = cpu_sample_calls(wl, args.ref_pairs)
+    # warm-up steps: one call each (OpenMP thread pool, page faults); timed steps: the whole
+    # 64-call schedule, as the GPU arm's step
     for _ in range(args.warmup):
-        drv.g6_schedule(h, wl, calls=calls)
+        drv.g6_schedule(h, wl, calls=1)
     tot, pairs = 0.0, 0
     for _ in range(args.steps):
-        sec, p_, _ = drv.g6_schedule(h, wl, calls=calls)
+        sec, p_, _ = drv.g6_schedule(h, wl)
         tot += sec
         pairs += p_
     val = pairs / tot / 1e9
-    sample = (f"first {calls} of the 64 block-step calls per step ({pairs // args.steps:.3e} pairs), "
-              f"PG6/libpg6 AVX2 + OpenMP built from its own sources, npipes 48")
+    sample = (f"the whole 64-call schedule per step ({pairs // args.steps:.3e} pairs), PG6/libpg6 AVX2 + OpenMP "
+              f"built from its own sources, npipes 48, the same call sequence as the GPU arm's e2e")
     return {
         "metric": "Gint/s (PG6 Hermite force+jerk+pot+NN, batched)",
         "value": round(val, 3), "unit": "Gint/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": round(tot / args.steps * 1e3, 3), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32 (f64 predictor + x_j-x_i)", "data": "synthetic",
-        "config": {"workload": "PG6 Hermite N=65536 Plummer eps=1e-4, 64 block-step calls of 2^k active "
-                               "(k=4..16), force+jerk+pot+nearest neighbour (sampled prefix)",
-                   "flop_per_pair": 60},
+        "ms_per_step": round(tot / args.steps * 1e3, 3), "higher_is_better": True,
+        "scaling": "strong" if ws > 1 else "weak",
+        "vs_baseline": None, "dtype": "f32 (f64 predictor + x_j-x_i)", "data": "synthetic (seeded Plummer, DF velocities; no dataset)",
+        "config": hermite_config(pairs // args.steps, ws),
         "impl": "reference",
         "cpu_baseline": {"value": round(val, 3), "unit": "Gint/s", "cores": os.cpu_count(), "kind": "reference",
                          "sample": sample},
@@ -1431,6 +1665,10 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--ref-pairs", type=float, default=4e9, help="pairs per reference-arm step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-f64-line", action="store_true",
+                    help="hermite: skip the second batched run with FP64 relative coordinates")
+    ap.add_argument("--no-workloads", action="store_true",
+                    help="hermite on one GPU: skip the other configurations' lines (C1, C3, C4, C5)")
     ap.add_argument("--no-tune", action="store_true", help="skip the kernel-configuration autotuner")
     ap.add_argument("--f64-positions", action="store_true",
                     help="FP64 x_j - x_i (DADD + F2F) instead of the double-float subtraction")
@@ -1455,6 +1693,25 @@ def main():
     runner = {"hermite": run_hermite, "direct": run_direct, "clusters": run_clusters, "treepm": run_treepm,
               "bh": run_bh, "integrator": run_integrator}
     line = runner[args.workload](args, pgb, ws, rank, local)
+    profiling = args.profile_largest or args.profile_tree or args.profile_api
+    if args.workload == "hermite" and ws == 1 and not args.no_workloads and not profiling:
+        # the other configurations of the benchmark, each with its own value, roofline, e2e,
+        # CPU baseline and FP64 check, in the same run
+        import copy
+        import torch
+        wls = {}
+        for key, name in (("C1", "direct"), ("C3", "treepm"), ("C4", "bh"), ("C5", "clusters")):
+            torch.cuda.empty_cache()
+            sub_args = copy.copy(args)
+            sub_args.workload = name
+            t0 = time.perf_counter()
+            try:
+                sub = runner[name](sub_args, pgb, ws, rank, local)
+            except Exception as e:   # reported in the line; the headline stands
+                sub = {"error": f"{type(e).__name__}: {e}"}
+            sub["wall_s"] = round(time.perf_counter() - t0, 1)
+            wls[key] = sub
+        line["workloads"] = wls
     if rank == 0:
         print(json.dumps(line), flush=True)
     if ws > 1:

@@ -84,6 +84,11 @@ void g6_dump_(double *tim, int *n, double *m, double (*x)[3], double (*v)[3]);
 int  pgb6_last_error(char *buf, int len);
 void pgb6_clear_error(void);
 void pgb6_set_abort(int on);
+/* Device time of the drop-in calls (no reference counterpart): with timing on, every
+ * g6calc_firsthalf (j update + prediction) and g6calc_lasthalf* (force) adds the device time
+ * between CUDA events around its work to a total, read (and cleared with reset != 0) in ms. */
+void   pgb6_set_call_timing(int on);
+double pgb6_call_device_ms(int reset);
 
 /* ---- batched path (no reference counterpart) ----------------------------------------------
  * Replaces loops of g6calc_firsthalf/lasthalf over npipes-sized i chunks (PG6/banana/
@@ -159,6 +164,13 @@ int  pgb6_hermite_step(pgb6_hermite *h, double *time, int *ni);
 /* block steps while the global time is below tend; steps taken by this call (optional) */
 int  pgb6_hermite_advance(pgb6_hermite *h, double tend, long long *psteps, long long *bsteps);
 double pgb6_hermite_time(pgb6_hermite *h);
+/* Fault handling of the step kernel: every wait (grid barrier, segment / task flag) gives up
+ * after a limit of SM cycles (default about a second; cycles <= 0 restores it), after which
+ * every CTA returns, the call reports PGB_ERR_DEVICE and the integrator is unusable.
+ * wait_status reads whether a wait gave up, how many CTAs have returned from the kernel (over
+ * all launches) and the CTAs per launch. */
+int  pgb6_hermite_set_wait_limit(pgb6_hermite *h, long long cycles);
+int  pgb6_hermite_wait_status(pgb6_hermite *h, int *gave_up, int *exits, int *grid);
 /* state as struct Particle holds it (any pointer may be NULL; jrk, pot with float values) */
 int  pgb6_hermite_get(pgb6_hermite *h, double *t, double *dt, double (*pos)[3], double (*vel)[3],
                       double (*acc)[3], double (*jrk)[3], double *pot);

@@ -17,7 +17,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
-REF_SRC = "/root/reference"
+REF_SRC = os.environ.get("PGB_REFERENCE", "/root/reference")   # the reference source tree
 
 _lock = threading.Lock()
 _lib = None
@@ -39,7 +39,7 @@ def build(ref: bool | None = None) -> None:
     if ref is None:
         ref = os.path.isdir(REF_SRC)
     if ref:
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REF_SRC}"], check=True)
 
 
 def lib() -> C.CDLL:

@@ -300,11 +300,13 @@ __device__ __forceinline__ float mufu_rsqrt(float x) {
 }
 
 // q = y (r2 y^2 - 3) with y = rsqrt(r2): one Newton step folded into the scale -2/r.
+// Every operation is an explicit round-to-nearest intrinsic, so that the key is the same bit
+// pattern wherever it is computed (the nearest-neighbour search recomputes it, see g6_task).
 __device__ __forceinline__ float minus2_over_r(float r2) {
     float y = mufu_rsqrt(r2);
-    float t = r2 * y;
+    float t = __fmul_rn(r2, y);
     float u = __fmaf_rn(t, y, -3.0f);
-    return u * y;
+    return __fmul_rn(u, y);
 }
 
 // The persistent scheduler.  A CTA's first task is its block index; later ones are drawn from

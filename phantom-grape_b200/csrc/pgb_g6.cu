@@ -85,23 +85,33 @@ bool ensure_device() {
 // ------------------------------------------------------------------------------------------
 // kernel configurations: (threads per CTA, i per thread, j-lanes); i-tile = NT/JL*IPT
 
-enum Cfg { CFG_SMALL = 0, CFG_MED = 1, CFG_LARGE = 2, CFG_128x1 = 3, CFG_128x4 = 4, CFG_256x2 = 5, NCFG = 6 };
-constexpr int CFG_NT[NCFG] = {512, 256, 128, 128, 128, 256};
-constexpr int CFG_IPT[NCFG] = {1, 1, 2, 1, 4, 2};
-constexpr int CFG_JL[NCFG] = {8, 2, 1, 1, 1, 1};
+enum Cfg {
+    CFG_SMALL = 0, CFG_MED = 1, CFG_LARGE = 2, CFG_128x1 = 3, CFG_128x4 = 4, CFG_256x2 = 5,
+    CFG_128x2J = 6, CFG_256x2J = 7, NCFG = 8
+};
+constexpr int CFG_NT[NCFG] = {512, 256, 128, 128, 128, 256, 128, 256};
+constexpr int CFG_IPT[NCFG] = {1, 1, 2, 1, 4, 2, 2, 2};
+constexpr int CFG_JL[NCFG] = {8, 2, 1, 1, 1, 1, 1, 1};
+// j-paired form (g6_jpair): used with double-float positions and without neighbour lists; the
+// other variants of these configurations run the i-paired form
+constexpr bool CFG_JP[NCFG] = {false, false, false, false, false, false, true, true};
 inline int cfg_itile(int c) { return CFG_NT[c] / CFG_JL[c] * CFG_IPT[c]; }
 constexpr int ITILE_MAX = 512;
 
-template <int NT, int IPT, int JL, bool FF>
+template <int NT, int IPT, int JL, bool FF, bool JP = false>
 int occ_of(bool nn, bool nbl) {
     static int v[4] = {0, 0, 0, 0};
     int k = (nn ? 1 : 0) + (nbl ? 2 : 0);
     if (!v[k]) {
         int b = 0;
-        if (k == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, JL, FF, false, false>, NT, 0);
-        if (k == 1) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, JL, FF, true, false>, NT, 0);
-        if (k == 2) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, JL, FF, false, true>, NT, 0);
-        if (k == 3) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, JL, FF, true, true>, NT, 0);
+        if (k == 0)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, JL, FF, false, false, JP>, NT, 0);
+        if (k == 1)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, JL, FF, true, false, JP>, NT, 0);
+        if (k == 2)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, JL, FF, false, true, JP>, NT, 0);
+        if (k == 3)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, g6_kernel<NT, IPT, JL, FF, true, true, JP>, NT, 0);
         v[k] = b > 0 ? b : 1;
     }
     return v[k];
@@ -115,6 +125,8 @@ int occupancy_ff(int cfg, bool nn, bool nbl) {
         case CFG_128x1: return occ_of<128, 1, 1, FF>(nn, nbl);
         case CFG_128x4: return occ_of<128, 4, 1, FF>(nn, nbl);
         case CFG_256x2: return occ_of<256, 2, 1, FF>(nn, nbl);
+        case CFG_128x2J: return occ_of<128, 2, 1, FF, true>(nn, nbl);
+        case CFG_256x2J: return occ_of<256, 2, 1, FF, true>(nn, nbl);
         default: return occ_of<128, 2, 1, FF>(nn, nbl);
     }
 }
@@ -123,12 +135,12 @@ int occupancy(int cfg, bool ff, bool nn, bool nbl) {
     return ff ? occupancy_ff<true>(cfg, nn, nbl) : occupancy_ff<false>(cfg, nn, nbl);
 }
 
-template <int NT, int IPT, int JL, bool FF>
+template <int NT, int IPT, int JL, bool FF, bool JP = false>
 void launch_cfg(bool nn, bool nbl, int grid, const G6Args& a, cudaStream_t s) {
-    if (nn && nbl) g6_kernel<NT, IPT, JL, FF, true, true><<<grid, NT, 0, s>>>(a);
-    else if (nn) g6_kernel<NT, IPT, JL, FF, true, false><<<grid, NT, 0, s>>>(a);
-    else if (nbl) g6_kernel<NT, IPT, JL, FF, false, true><<<grid, NT, 0, s>>>(a);
-    else g6_kernel<NT, IPT, JL, FF, false, false><<<grid, NT, 0, s>>>(a);
+    if (nn && nbl) g6_kernel<NT, IPT, JL, FF, true, true, JP><<<grid, NT, 0, s>>>(a);
+    else if (nn) g6_kernel<NT, IPT, JL, FF, true, false, JP><<<grid, NT, 0, s>>>(a);
+    else if (nbl) g6_kernel<NT, IPT, JL, FF, false, true, JP><<<grid, NT, 0, s>>>(a);
+    else g6_kernel<NT, IPT, JL, FF, false, false, JP><<<grid, NT, 0, s>>>(a);
 }
 
 template <bool FF>
@@ -139,6 +151,8 @@ void launch_ff(int cfg, bool nn, bool nbl, int grid, const G6Args& a, cudaStream
         case CFG_128x1: launch_cfg<128, 1, 1, FF>(nn, nbl, grid, a, s); break;
         case CFG_128x4: launch_cfg<128, 4, 1, FF>(nn, nbl, grid, a, s); break;
         case CFG_256x2: launch_cfg<256, 2, 1, FF>(nn, nbl, grid, a, s); break;
+        case CFG_128x2J: launch_cfg<128, 2, 1, FF, true>(nn, nbl, grid, a, s); break;
+        case CFG_256x2J: launch_cfg<256, 2, 1, FF, true>(nn, nbl, grid, a, s); break;
         default: launch_cfg<128, 2, 1, FF>(nn, nbl, grid, a, s); break;
     }
 }
@@ -334,6 +348,11 @@ struct State {
     HostBuf<int> nbc_h, nbl_h;
     std::vector<std::vector<int>> nblists;
     std::vector<int> nbcounts;
+    // device-time accounting of the drop-in calls (pgb6_set_call_timing): CUDA events around the
+    // j-update + prediction of g6calc_firsthalf and the force launch of g6calc_lasthalf*
+    bool time_calls = false;
+    cudaEvent_t tev[2] = {nullptr, nullptr};
+    double dev_ms = 0.0;
     int nb_ni = 0, nb_error = 0;
 };
 State S;
@@ -409,15 +428,34 @@ bool flush_j() {
     return true;
 }
 
+// Call timing: start / stop marks on the library's stream; stop adds the device time between
+// them once the stop mark has completed.
+bool time_mark(int k) {
+    if (!S.time_calls) return true;
+    if (!S.tev[k]) PGB_CUDA_OR(g_err, LIB, cudaEventCreate(&S.tev[k]), return false);
+    PGB_CUDA_OR(g_err, LIB, cudaEventRecord(S.tev[k], S.stream), return false);
+    return true;
+}
+
+bool time_add() {
+    if (!S.time_calls) return true;
+    float ms = 0.f;
+    PGB_CUDA_OR(g_err, LIB, cudaEventSynchronize(S.tev[1]), return false);
+    PGB_CUDA_OR(g_err, LIB, cudaEventElapsedTime(&ms, S.tev[0], S.tev[1]), return false);
+    S.dev_ms += ms;
+    return true;
+}
+
 bool flush_and_predict(int nj) {
     if (nj <= 0) return true;
-    if (!grow_j(nj) || !flush_j()) return false;
+    if (!grow_j(nj) || !time_mark(0) || !flush_j()) return false;
     PGB_CUDA_OR(g_err, LIB, S.pred.reserve(S.jcap), return false);
     g6_predict_kernel<<<(nj + 255) / 256, 256, 0, S.stream>>>(S.jd.p, nj, S.ti, S.pred.p, dx_ff());
     PGB_CUDA_OR(g_err, LIB, cudaGetLastError(), return false);
+    if (!time_mark(1)) return false;
     // j-memory is read asynchronously from the pinned mirror: later set_j calls wait for it
     PGB_CUDA_OR(g_err, LIB, cudaStreamSynchronize(S.stream), return false);
-    return true;
+    return time_add();
 }
 
 // The small-call path: one launch of the cluster kernel (i-records in its parameter block),
@@ -593,12 +631,17 @@ int lasthalf_impl(int nj, int ni, const int* pidx, const double (*pos)[3], const
         raise(g_err, LIB, PGB_ERR_ARG, "ni = %d outside [0, %d] pipes", ni, npipes());
         return 0;
     }
-    if (nj < 0 || nj > S.jcap) {
-        raise(g_err, LIB, PGB_ERR_ARG, "nj = %d but only %d j-particles were set", nj, S.jcap);
+    if (nj < 0) {
+        raise(g_err, LIB, PGB_ERR_ARG, "nj = %d is negative", nj);
         return 0;
     }
     if (ni == 0) return 0;
     std::lock_guard<std::mutex> g(S.mu);
+    // checked under the lock: a concurrent g6_set_j_particle may grow the j store
+    if (nj > S.jcap) {
+        raise(g_err, LIB, PGB_ERR_ARG, "nj = %d but only %d j-particles were set", nj, S.jcap);
+        return 0;
+    }
     if (!init_state()) return 0;
     if (S.ibuf.reserve(ni) != cudaSuccess) {
         raise(g_err, LIB, PGB_ERR_CUDA, "pinned i-buffer allocation failed");
@@ -617,8 +660,10 @@ int lasthalf_impl(int nj, int ni, const int* pidx, const double (*pos)[3], const
     bool nn = (nnb != nullptr);
     // eps2 is a per-call scalar, used as float (phantom_g6.c:191)
     S.wait_flags = 0;
+    if (!time_mark(0)) return 0;
     if (!run_force(nj, ni, (float)eps2, nn, nbl)) return 0;
-    if (!wait_results()) return 0;
+    if (!time_mark(1)) return 0;
+    if (!wait_results() || !time_add()) return 0;
     for (int i = 0; i < ni; i++) {
         const G6Out& o = S.outh.p[i];
         acc[i][0] = o.ax;
@@ -853,6 +898,23 @@ PGB_EXPORT void pgb6_set_abort(int on) {
 
 // Sizes of the device record types, so callers can lay out device buffers:
 // G6Ptcl (j-memory), G6PredJ (predicted j), G6I (i-particle), G6Out (result).
+// Device-time accounting of the drop-in calls (no counterpart in the reference): with on != 0,
+// every g6calc_firsthalf (j-memory update + prediction) and g6calc_lasthalf* (force launch)
+// adds the device time between CUDA events recorded around its work on the library's stream
+// to a running total; pgb6_call_device_ms returns that total in ms (and clears it when reset
+// != 0).  It separates the device work of the plain API from its host overhead.
+PGB_EXPORT void pgb6_set_call_timing(int on) {
+    std::lock_guard<std::mutex> g(S.mu);
+    S.time_calls = on != 0;
+}
+
+PGB_EXPORT double pgb6_call_device_ms(int reset) {
+    std::lock_guard<std::mutex> g(S.mu);
+    const double v = S.dev_ms;
+    if (reset) S.dev_ms = 0.0;
+    return v;
+}
+
 PGB_EXPORT void pgb6_record_sizes(int* ptcl, int* predj, int* irec, int* out) {
     if (ptcl) *ptcl = (int)sizeof(G6Ptcl);
     if (predj) *predj = (int)sizeof(G6PredJ);
@@ -1305,7 +1367,11 @@ PGB_EXPORT int pgb6_force_noalloc(const void* ipart, int ni, const void* jpred, 
     void* base = nullptr;
     {
         std::lock_guard<std::mutex> g(g_na_mu);
-        if (g_device < 0 || g_device >= 64) return PGB_ERR_NOGPU;
+        if (g_device < 0 || g_device >= 64) {
+            raise(g_err, LIB, PGB_ERR_NOGPU, "pgb6_force_noalloc: device %d outside the supported range [0, 64)",
+                  g_device);
+            return PGB_ERR_NOGPU;
+        }
         if (!g_na_addr[g_device]) {
             cudaError_t e = cudaGetSymbolAddress(&g_na_addr[g_device], g6_noalloc_scratch);
             if (e != cudaSuccess) {
@@ -1573,7 +1639,7 @@ PGB_EXPORT int pgb6_hermite_step(pgb6_hermite* H, double* time, int* ni) {
     }
     if (!ensure_device()) return PGB_ERR_NOGPU;
     std::lock_guard<std::mutex> g(H->mu);
-    if (!hm_launch(H, false, INFINITY, 1) || !hm_sync_clock(H)) return PGB_ERR_CUDA;
+    if (!hm_launch(H, false, INFINITY, 1) || !hm_sync_clock(H)) return H->clk.err ? PGB_ERR_DEVICE : PGB_ERR_CUDA;
     if (time) *time = H->clk.time;
     if (ni) *ni = H->clk.ni;
     return PGB_OK;
@@ -1591,13 +1657,53 @@ PGB_EXPORT int pgb6_hermite_advance(pgb6_hermite* H, double tend, long long* pst
     std::lock_guard<std::mutex> g(H->mu);
     const long long p0 = H->clk.psteps, b0 = H->clk.bsteps;
     while (H->clk.time < tend)
-        if (!hm_launch(H, false, tend, HM_STEPS_PER_LAUNCH) || !hm_sync_clock(H)) return PGB_ERR_CUDA;
+        if (!hm_launch(H, false, tend, HM_STEPS_PER_LAUNCH) || !hm_sync_clock(H))
+            return H->clk.err ? PGB_ERR_DEVICE : PGB_ERR_CUDA;
     if (psteps) *psteps = H->clk.psteps - p0;
     if (bsteps) *bsteps = H->clk.bsteps - b0;
     return PGB_OK;
 }
 
 PGB_EXPORT double pgb6_hermite_time(pgb6_hermite* H) { return H ? H->clk.time : 0.0; }
+
+// The limit, in SM cycles, of every wait of the step kernel (grid barriers, segment and task
+// flags); cycles <= 0 restores the default (about a second).  A wait that runs out sets the
+// integrator's error word: every CTA returns at its next wait, the call reports PGB_ERR_DEVICE
+// and the integrator is unusable afterwards (its barrier state is no longer consistent).  For
+// fault-handling tests; a production run keeps the default.
+PGB_EXPORT int pgb6_hermite_set_wait_limit(pgb6_hermite* H, long long cycles) {
+    if (!H) {
+        raise(g_err, LIB, PGB_ERR_ARG, "pgb6_hermite_set_wait_limit: null integrator");
+        return PGB_ERR_ARG;
+    }
+    if (!ensure_device()) return PGB_ERR_NOGPU;
+    std::lock_guard<std::mutex> g(H->mu);
+    const long long v = cycles > 0 ? cycles : 0;
+    PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(&H->W.clk->spin_limit, &v, sizeof v, cudaMemcpyHostToDevice, H->s),
+                return PGB_ERR_CUDA);
+    PGB_CUDA_OR(g_err, LIB, cudaStreamSynchronize(H->s), return PGB_ERR_CUDA);
+    return PGB_OK;
+}
+
+// The step kernel's failure record, read from the device: *gave_up (a wait ran out, so the
+// integrator is unusable), *exits (CTAs that have returned from the kernel, over every launch
+// so far) and *grid (CTAs per launch).  Any pointer may be NULL.
+PGB_EXPORT int pgb6_hermite_wait_status(pgb6_hermite* H, int* gave_up, int* exits, int* grid) {
+    if (!H) {
+        raise(g_err, LIB, PGB_ERR_ARG, "pgb6_hermite_wait_status: null integrator");
+        return PGB_ERR_ARG;
+    }
+    if (!ensure_device()) return PGB_ERR_NOGPU;
+    std::lock_guard<std::mutex> g(H->mu);
+    HmClock c;
+    PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(&c, H->W.clk, sizeof c, cudaMemcpyDeviceToHost, H->s),
+                return PGB_ERR_CUDA);
+    PGB_CUDA_OR(g_err, LIB, cudaStreamSynchronize(H->s), return PGB_ERR_CUDA);
+    if (gave_up) *gave_up = c.err;
+    if (exits) *exits = c.exits;
+    if (grid) *grid = H->grid;
+    return PGB_OK;
+}
 
 // The particle state (any pointer may be NULL): t, dt, pos, vel, acc, jerk, pot as the
 // reference's struct Particle holds them (jerk and pot with float values).

@@ -215,7 +215,26 @@ __device__ __forceinline__ float rel1(const Pos3& j, const Pos3& i, int c) {
     }
 }
 
-template <bool FF, bool NN, bool NBL>
+// The nearest-neighbour key of one pair: q = -2/r_soft (pgb::minus2_over_r), 0 for the self
+// pair.  Every path of the kernels computes q with exactly these operations, so a key found by
+// one pass can be looked up again by another (g6_rescan).
+template <bool FF>
+__device__ __forceinline__ float g6_key(const G6PredJ& J, const Pos3& I, int idi, float eps2) {
+    const float dx = rel1<FF>(J.p, I, 0), dy = rel1<FF>(J.p, I, 1), dz = rel1<FF>(J.p, I, 2);
+    const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmaf_rn(dx, dx, eps2)));
+    const float q = minus2_over_r(r2);
+    return (J.id == idi) ? 0.0f : q;
+}
+
+// Nearest-neighbour bookkeeping per pair, two forms:
+//  * select (NN, !TILEMIN): kmin/kadr updated per pair with strict '<' in j order;
+//  * tile minimum (TILEMIN): only tmin = min(tmin, q) per pair (one FMNMX); the caller keeps,
+//    per j-tile, whether the tile improved the running minimum and recovers the address of the
+//    best tile's first minimal key afterwards (g6_rescan) -- the same (key, smallest address)
+//    result with one instruction per pair instead of three.
+// SELF: the j-tile may hold the i-particle itself (its id), so the key is masked to 0 for it;
+// tiles that cannot hold it skip the compare and select.
+template <bool FF, bool NN, bool NBL, bool SELF = true, bool TILEMIN = false>
 __device__ __forceinline__ void g6_pair(const G6PredJ& J, int jadr, const Pos3& I, float vxi,
                                         float vyi, float vzi, int idi, float eps2, float hinv, G6Acc& a,
                                         float& kmin, int& kadr, int* nbc, int* nbl, int nbmax) {
@@ -225,8 +244,10 @@ __device__ __forceinline__ void g6_pair(const G6PredJ& J, int jadr, const Pos3& 
     float dvx = J.vx - vxi, dvy = J.vy - vyi, dvz = J.vz - vzi;
     float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmaf_rn(dx, dx, eps2)));
     float q = minus2_over_r(r2);
-    q = (J.id == idi) ? 0.0f : q;
-    if constexpr (NN) {
+    if constexpr (SELF) q = (J.id == idi) ? 0.0f : q;
+    if constexpr (NN && TILEMIN) {
+        kmin = fminf(kmin, q);
+    } else if constexpr (NN) {
         bool lt = q < kmin;
         kmin = lt ? q : kmin;
         kadr = lt ? jadr : kadr;
@@ -262,7 +283,7 @@ struct G6Acc2 {
     float pot[2];
 };
 
-template <bool FF, bool NN, bool NBL>
+template <bool FF, bool NN, bool NBL, bool SELF = true, bool TILEMIN = false>
 __device__ __forceinline__ void g6_pair2(const G6PredJ& J, int jadr, const Pos3* I, const float* vxi,
                                          const float* vyi, const float* vzi, const int* idi, float eps2,
                                          const float* hinv, G6Acc2& a, float* kmin, int* kadr, int* const* nbc,
@@ -278,8 +299,10 @@ __device__ __forceinline__ void g6_pair2(const G6PredJ& J, int jadr, const Pos3*
         dvz[k] = J.vz - vzi[k];
         float r2 = __fmaf_rn(dz[k], dz[k], __fmaf_rn(dy[k], dy[k], __fmaf_rn(dx[k], dx[k], eps2)));
         float q = minus2_over_r(r2);
-        q = (J.id == idi[k]) ? 0.0f : q;
-        if constexpr (NN) {
+        if constexpr (SELF) q = (J.id == idi[k]) ? 0.0f : q;
+        if constexpr (NN && TILEMIN) {
+            kmin[k] = fminf(kmin[k], q);
+        } else if constexpr (NN) {
             bool lt = q < kmin[k];
             kmin[k] = lt ? q : kmin[k];
             kadr[k] = lt ? jadr : kadr[k];
@@ -305,6 +328,98 @@ __device__ __forceinline__ void g6_pair2(const G6PredJ& J, int jadr, const Pos3*
     a.jx = __ffma2_rn(M, __ffma2_rn(C, DX, make_float2(dvx[0], dvx[1])), a.jx);
     a.jy = __ffma2_rn(M, __ffma2_rn(C, DY, make_float2(dvy[0], dvy[1])), a.jy);
     a.jz = __ffma2_rn(M, __ffma2_rn(C, DZ, make_float2(dvz[0], dvz[1])), a.jz);
+}
+
+// ---- j-paired form ------------------------------------------------------------------------
+// One i-particle against two consecutive j (a "j-pair"), with the j-tile in shared memory as
+// one array per field (G6TileSoA), so that a 16-byte shared load returns a field of four
+// consecutive j: every paired FP32 operand is then a natural register pair -- (j, j+1) for the
+// j fields, a loop-invariant (v, v) for the i fields -- and the double-float relative
+// coordinates (nine FADD per j-pair as paired FADD2) join the nine accumulations (FFMA2) on the
+// heavy half of the FMA pipe, while the rest of the chain (dv, r^2, the Newton step, dx.dv and
+// the scalar factors: 18 per pair) stays scalar.  Per pair that is 9 paired + 18 scalar FP32
+// instructions, which loads the two halves of the FMA pipe about equally (a paired instruction
+// occupies the heavy half twice as long as a scalar one), against 4.5 + 27 in g6_pair2.
+// The two lanes of each accumulator sum the even and the odd j of the tile; they are added
+// into the FP64 sums one after the other at every fold.  Per pair the key q is bit-identical
+// to g6_key (FADD2 rounds each lane as FADD does).
+struct G6IPair {
+    float2 nxh, nyh, nzh, nxl, nyl, nzl;   // -x_i (hi, lo) of each coordinate, in both lanes
+    float vx, vy, vz;
+    int id;
+};
+
+template <int NT>
+struct G6TileSoA {
+    float xh[NT], yh[NT], zh[NT], xl[NT], yl[NT], zl[NT];
+    float m[NT], vx[NT], vy[NT], vz[NT];
+    int id[NT];
+};
+
+template <bool NN, bool SELF>
+__device__ __forceinline__ void g6_jpair(float2 xh, float2 yh, float2 zh, float2 xl, float2 yl, float2 zl,
+                                         float2 m, float2 vx, float2 vy, float2 vz, int2 jid,
+                                         const G6IPair& I, float eps2, G6Acc2& a, float& tmin) {
+    const float2 dx = __fadd2_rn(__fadd2_rn(xh, I.nxh), __fadd2_rn(xl, I.nxl));
+    const float2 dy = __fadd2_rn(__fadd2_rn(yh, I.nyh), __fadd2_rn(yl, I.nyl));
+    const float2 dz = __fadd2_rn(__fadd2_rn(zh, I.nzh), __fadd2_rn(zl, I.nzl));
+    float2 dvx, dvy, dvz, mq3, c;
+    const float* dxp = &dx.x;
+    const float* dyp = &dy.x;
+    const float* dzp = &dz.x;
+    const float* vxp = &vx.x;
+    const float* vyp = &vy.x;
+    const float* vzp = &vz.x;
+    const float* mp = &m.x;
+    const int* idp = &jid.x;
+    float* dvxp = &dvx.x;
+    float* dvyp = &dvy.x;
+    float* dvzp = &dvz.x;
+    float* mq3p = &mq3.x;
+    float* cp = &c.x;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        dvxp[h] = vxp[h] - I.vx;
+        dvyp[h] = vyp[h] - I.vy;
+        dvzp[h] = vzp[h] - I.vz;
+        const float r2 = __fmaf_rn(dzp[h], dzp[h], __fmaf_rn(dyp[h], dyp[h], __fmaf_rn(dxp[h], dxp[h], eps2)));
+        float q = minus2_over_r(r2);
+        if constexpr (SELF) q = (idp[h] == I.id) ? 0.0f : q;
+        if constexpr (NN) tmin = fminf(tmin, q);
+        a.pot[h] = __fmaf_rn(mp[h], q, a.pot[h]);
+        const float rv = __fmaf_rn(dzp[h], dvzp[h], __fmaf_rn(dyp[h], dvyp[h], dxp[h] * dvxp[h]));
+        const float mq = mp[h] * q;
+        const float q2 = q * q;
+        mq3p[h] = mq * q2;
+        cp[h] = -0.75f * q2 * rv;
+    }
+    a.ax = __ffma2_rn(mq3, dx, a.ax);
+    a.ay = __ffma2_rn(mq3, dy, a.ay);
+    a.az = __ffma2_rn(mq3, dz, a.az);
+    a.jx = __ffma2_rn(mq3, __ffma2_rn(c, dx, dvx), a.jx);
+    a.jy = __ffma2_rn(mq3, __ffma2_rn(c, dy, dvy), a.jy);
+    a.jz = __ffma2_rn(mq3, __ffma2_rn(c, dz, dvz), a.jz);
+}
+
+// The address of the first j of tile [jb, jb + ne) (every JL-th from lane jl) whose key equals
+// kmin -- the nearest neighbour found by a tile-minimum pass (see g6_pair).  The records are read
+// again from the predicted j-set (L2-resident).  Returns -1 if none matches, which cannot
+// happen for a key that the same arithmetic produced.
+template <bool FF>
+__device__ __forceinline__ int g6_rescan(const G6PredJ* __restrict__ jpred, int jb, int ne, const Pos3& I, int idi,
+                                         float eps2, float kmin) {
+    int j = 0;
+    for (; j + 3 < ne; j += 4) {
+        G6PredJ J[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) J[u] = jpred[jb + j + u];
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+            if (g6_key<FF>(J[u], I, idi, eps2) == kmin) return jb + j + u;
+    }
+    for (; j < ne; j++)
+        if (g6_key<FF>(jpred[jb + j], I, idi, eps2) == kmin) return jb + j;
+    return -1;
 }
 
 __device__ __forceinline__ G6Out g6_finish(const G6Out& s) {
@@ -434,6 +549,19 @@ __device__ __forceinline__ void reduce_rows(const G6Out* base, size_t stride, in
     }
 }
 
+template <bool B>
+struct BoolC {
+    static constexpr bool value = B;
+};
+
+// Shared memory of a g6_kernel CTA: the j-tile (as records, or as field arrays in the j-paired
+// form, which also keeps its threads' FP64 sums there: 7 per i, two i per thread) and, after
+// the tile loop, NT G6Out for the lane and group reductions.
+template <int NT, bool JP>
+constexpr int g6_smem_bytes() {
+    return JP ? (int)((sizeof(G6TileSoA<NT>) + 15) / 16 * 16 + 14 * NT * sizeof(double)) : NT * (int)sizeof(G6Out);
+}
+
 // Thread layout of a CTA: NT threads = JL j-lanes x ISL i-slots (ISL = NT/JL, whole warps per
 // lane so that the shared-memory j reads stay warp-broadcasts).  A thread owns IPT i-particles
 // li = slot + k*ISL of the task's i-tile (ITILE = ISL*IPT) and every JL-th j of each j-tile.
@@ -442,12 +570,27 @@ __device__ __forceinline__ void reduce_rows(const G6Out* base, size_t stride, in
 // g6_task: one task (an i-tile against a j-range) by the whole CTA; smem holds NT G6Out.  A task
 // of a split j-range (T.group >= 0) writes its partial sums to partial row T.slot; otherwise the
 // final result to A.out.  Returns with the CTA's shared memory free for reuse after a barrier.
-template <int NT, int IPT, int JL, bool FF, bool NN, bool NBL>
+//
+// Per j-tile the CTA first tests whether the tile can hold one of the task's i-particles
+// (a j id inside the i-tile's id range, one __syncthreads_or at the staging barrier); only such
+// tiles run the self-pair mask.  With two i per thread (IPT even) the nearest neighbour is
+// found as a tile minimum (see g6_pair) and its address recovered once per i and task by
+// g6_rescan.  JP selects the j-paired form (g6_jpair; double-float positions, no neighbour
+// lists, two i per thread, one j-lane); otherwise the j-tile is an array of G6PredJ records.
+template <int NT, int IPT, int JL, bool FF, bool NN, bool NBL, bool JP = false>
 __device__ __forceinline__ void g6_task(const G6Args& A, const Task& T, unsigned char* smem) {
     static_assert(JL == 1 || IPT == 1, "j-lanes are used with one i per thread");
     constexpr int ISL = NT / JL;
+    constexpr bool PAIRED = (IPT % 2 == 0);
+    constexpr bool USE_JP = JP && FF && !NBL && IPT == 2 && JL == 1;
+    constexpr bool TILEMIN = NN && !NBL && PAIRED;
     G6PredJ* sj = reinterpret_cast<G6PredJ*>(smem);
+    G6TileSoA<NT>* sa = reinterpret_cast<G6TileSoA<NT>*>(smem);
+    // j-paired form: the FP64 sums of thread t, i k, component c at Ssh[(k * 7 + c) * NT + t]
+    // (updated once per G6_FOLD j; kept out of the registers so that four CTAs fit an SM)
+    double* Ssh = reinterpret_cast<double*>(smem + (sizeof(G6TileSoA<NT>) + 15) / 16 * 16);
     G6Out* red = reinterpret_cast<G6Out*>(smem);
+    __shared__ int s_idr[2];
     const int slot = threadIdx.x % ISL;
     const int jl = threadIdx.x / ISL;
 
@@ -455,8 +598,8 @@ __device__ __forceinline__ void g6_task(const G6Args& A, const Task& T, unsigned
     float vxi[IPT], vyi[IPT], vzi[IPT], hinv[IPT];
     int idi[IPT];
     double S[IPT][7];
-    float kmin[IPT];
-    int kadr[IPT];
+    float kmin[IPT], tmin[IPT];
+    int kadr[IPT], ktile[IPT];
 #pragma unroll
     for (int k = 0; k < IPT; k++) {
         int li = slot + k * ISL;
@@ -471,84 +614,250 @@ __device__ __forceinline__ void g6_task(const G6Args& A, const Task& T, unsigned
         for (int c = 0; c < 7; c++) S[k][c] = 0.0;
         kmin[k] = 10.0f;   // gravity_kernel2 starts its key at 10 and index at -1 (:495-496)
         kadr[k] = -1;
+        tmin[k] = 10.0f;
+        ktile[k] = -1;
+    }
+    // the i-tile's id range (padding slots repeat the tile's first i): published to the CTA by
+    // the first barrier of the tile loop
+    {
+        int lo = idi[0], hi = idi[0];
+#pragma unroll
+        for (int k = 1; k < IPT; k++) {
+            lo = min(lo, idi[k]);
+            hi = max(hi, idi[k]);
+        }
+        lo = __reduce_min_sync(0xffffffffu, lo);
+        hi = __reduce_max_sync(0xffffffffu, hi);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            s_idr[0] = 0x7fffffff;
+            s_idr[1] = (int)0x80000000;
+        }
+        __syncthreads();
+        if ((threadIdx.x & 31) == 0) {
+            atomicMin(&s_idr[0], lo);
+            atomicMax(&s_idr[1], hi);
+        }
+    }
+    G6IPair IP[USE_JP ? IPT : 1];
+    if constexpr (USE_JP) {
+#pragma unroll
+        for (int c = 0; c < 7 * IPT; c++) Ssh[c * NT + threadIdx.x] = 0.0;
+#pragma unroll
+        for (int k = 0; k < IPT; k++) {
+            IP[k].nxh = make_float2(-pi[k].f.xh, -pi[k].f.xh);
+            IP[k].nyh = make_float2(-pi[k].f.yh, -pi[k].f.yh);
+            IP[k].nzh = make_float2(-pi[k].f.zh, -pi[k].f.zh);
+            IP[k].nxl = make_float2(-pi[k].f.xl, -pi[k].f.xl);
+            IP[k].nyl = make_float2(-pi[k].f.yl, -pi[k].f.yl);
+            IP[k].nzl = make_float2(-pi[k].f.zl, -pi[k].f.zl);
+            IP[k].vx = vxi[k];
+            IP[k].vy = vyi[k];
+            IP[k].vz = vzi[k];
+            IP[k].id = idi[k];
+        }
     }
 
     for (int jt = 0; jt < T.nj; jt += NT) {
         const int nt = min(NT, T.nj - jt);
         __syncthreads();
-        if (threadIdx.x < nt) sj[threadIdx.x] = A.jpred[T.j0 + jt + threadIdx.x];
-        __syncthreads();
-        if constexpr (IPT % 2 == 0) {
-            constexpr int NP = IPT / 2;
-            int* nbc[IPT];
-            int* nbl[IPT];
-#pragma unroll
-            for (int k = 0; k < IPT; k++) {
-                int li = slot + k * ISL;
-                int gi = T.i0 + (li < T.ni ? li : 0);
-                nbc[k] = NBL ? A.nb_count + gi : nullptr;
-                nbl[k] = NBL ? A.nb_list + (size_t)gi * A.nb_maxlen : nullptr;
-            }
-            for (int j0 = 0; j0 < nt; j0 += G6_FOLD) {
-                const int j1 = min(j0 + G6_FOLD, nt);
-                G6Acc2 a[NP];
-                const float2 z2 = make_float2(0.f, 0.f);
-#pragma unroll
-                for (int p = 0; p < NP; p++) a[p] = G6Acc2{z2, z2, z2, z2, z2, z2, {0.f, 0.f}};
-#pragma unroll 2
-                for (int j = j0; j < j1; j++) {
-                    const G6PredJ J = sj[j];
-                    const int jadr = T.j0 + jt + j;
-#pragma unroll
-                    for (int p = 0; p < NP; p++)
-                        g6_pair2<FF, NN, NBL>(J, jadr, pi + 2 * p, vxi + 2 * p, vyi + 2 * p, vzi + 2 * p,
-                                              idi + 2 * p, A.eps2, hinv + 2 * p, a[p], kmin + 2 * p, kadr + 2 * p,
-                                              nbc + 2 * p, nbl + 2 * p, A.nb_maxlen);
-                }
-#pragma unroll
-                for (int p = 0; p < NP; p++) {
-                    const float2* v = &a[p].ax;
-#pragma unroll
-                    for (int h = 0; h < 2; h++) {
-                        const int k = 2 * p + h;
-#pragma unroll
-                        for (int c = 0; c < 6; c++) S[k][c] += (double)(h ? v[c].y : v[c].x);
-                        S[k][6] += (double)a[p].pot[h];
-                    }
-                }
+        const int idlo = s_idr[0], idhi = s_idr[1];
+        bool mine = false;
+        int nt4 = nt;
+        if constexpr (USE_JP) {
+            // fields of the tile's records, padded to a multiple of 4 with massless copies of
+            // the tile's first record (they add exact zeros, and their key repeats that record's)
+            nt4 = (nt + 3) & ~3;
+            if (threadIdx.x < nt4) {
+                const bool real = threadIdx.x < nt;
+                const G6PredJ r = A.jpred[T.j0 + jt + (real ? threadIdx.x : 0)];
+                sa->xh[threadIdx.x] = r.p.f.xh;
+                sa->yh[threadIdx.x] = r.p.f.yh;
+                sa->zh[threadIdx.x] = r.p.f.zh;
+                sa->xl[threadIdx.x] = r.p.f.xl;
+                sa->yl[threadIdx.x] = r.p.f.yl;
+                sa->zl[threadIdx.x] = r.p.f.zl;
+                sa->m[threadIdx.x] = real ? r.m : 0.0f;
+                sa->vx[threadIdx.x] = r.vx;
+                sa->vy[threadIdx.x] = r.vy;
+                sa->vz[threadIdx.x] = r.vz;
+                sa->id[threadIdx.x] = r.id;
+                mine = real && r.id >= idlo && r.id <= idhi;
             }
         } else {
-        // blocks of G6_FOLD terms per lane
-        for (int j0 = 0; j0 < nt; j0 += G6_FOLD * JL) {
-            const int j1 = min(j0 + G6_FOLD * JL, nt);
-            G6Acc a[IPT];
+            if (threadIdx.x < nt) {
+                const G6PredJ r = A.jpred[T.j0 + jt + threadIdx.x];
+                sj[threadIdx.x] = r;
+                mine = r.id >= idlo && r.id <= idhi;
+            }
+        }
+        const bool self_tile = __syncthreads_or(mine) != 0;
+        if constexpr (TILEMIN) {
 #pragma unroll
-            for (int k = 0; k < IPT; k++) a[k] = G6Acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-#pragma unroll 2
-            for (int j = j0 + jl; j < j1; j += JL) {
-                const G6PredJ J = sj[j];
-                const int jadr = T.j0 + jt + j;
+            for (int k = 0; k < IPT; k++) tmin[k] = kmin[k];
+        }
+
+        auto run_tile = [&](auto self_c) {
+            constexpr bool SELF = decltype(self_c)::value;
+            if constexpr (USE_JP) {
+                for (int j0 = 0; j0 < nt4; j0 += G6_FOLD) {
+                    const int j1 = min(j0 + G6_FOLD, nt4);
+                    G6Acc2 a[IPT];
+                    const float2 z2 = make_float2(0.f, 0.f);
+#pragma unroll
+                    for (int k = 0; k < IPT; k++) a[k] = G6Acc2{z2, z2, z2, z2, z2, z2, {0.f, 0.f}};
+#pragma unroll 1
+                    for (int j = j0; j < j1; j += 4) {
+                        const float4 XH = *reinterpret_cast<const float4*>(&sa->xh[j]);
+                        const float4 YH = *reinterpret_cast<const float4*>(&sa->yh[j]);
+                        const float4 ZH = *reinterpret_cast<const float4*>(&sa->zh[j]);
+                        const float4 XL = *reinterpret_cast<const float4*>(&sa->xl[j]);
+                        const float4 YL = *reinterpret_cast<const float4*>(&sa->yl[j]);
+                        const float4 ZL = *reinterpret_cast<const float4*>(&sa->zl[j]);
+                        const float4 M = *reinterpret_cast<const float4*>(&sa->m[j]);
+                        const float4 VX = *reinterpret_cast<const float4*>(&sa->vx[j]);
+                        const float4 VY = *reinterpret_cast<const float4*>(&sa->vy[j]);
+                        const float4 VZ = *reinterpret_cast<const float4*>(&sa->vz[j]);
+                        int4 ID = make_int4(0, 0, 0, 0);
+                        if constexpr (SELF) ID = *reinterpret_cast<const int4*>(&sa->id[j]);
+#pragma unroll
+                        for (int k = 0; k < IPT; k++) {
+                            g6_jpair<NN, SELF>(make_float2(XH.x, XH.y), make_float2(YH.x, YH.y),
+                                               make_float2(ZH.x, ZH.y), make_float2(XL.x, XL.y),
+                                               make_float2(YL.x, YL.y), make_float2(ZL.x, ZL.y),
+                                               make_float2(M.x, M.y), make_float2(VX.x, VX.y),
+                                               make_float2(VY.x, VY.y), make_float2(VZ.x, VZ.y),
+                                               make_int2(ID.x, ID.y), IP[k], A.eps2, a[k], tmin[k]);
+                            g6_jpair<NN, SELF>(make_float2(XH.z, XH.w), make_float2(YH.z, YH.w),
+                                               make_float2(ZH.z, ZH.w), make_float2(XL.z, XL.w),
+                                               make_float2(YL.z, YL.w), make_float2(ZL.z, ZL.w),
+                                               make_float2(M.z, M.w), make_float2(VX.z, VX.w),
+                                               make_float2(VY.z, VY.w), make_float2(VZ.z, VZ.w),
+                                               make_int2(ID.z, ID.w), IP[k], A.eps2, a[k], tmin[k]);
+                        }
+                    }
+#pragma unroll
+                    for (int k = 0; k < IPT; k++) {
+                        const float2* v = &a[k].ax;
+#pragma unroll
+                        for (int c = 0; c < 6; c++) {
+                            double& d = Ssh[(k * 7 + c) * NT + threadIdx.x];
+                            d = d + (double)v[c].x + (double)v[c].y;
+                        }
+                        double& d = Ssh[(k * 7 + 6) * NT + threadIdx.x];
+                        d = d + (double)a[k].pot[0] + (double)a[k].pot[1];
+                    }
+                }
+            } else if constexpr (PAIRED) {
+                constexpr int NP = IPT / 2;
+                int* nbc[IPT];
+                int* nbl[IPT];
 #pragma unroll
                 for (int k = 0; k < IPT; k++) {
                     int li = slot + k * ISL;
                     int gi = T.i0 + (li < T.ni ? li : 0);
-                    g6_pair<FF, NN, NBL>(J, jadr, pi[k], vxi[k], vyi[k], vzi[k], idi[k], A.eps2, hinv[k],
-                                         a[k], kmin[k], kadr[k], NBL ? A.nb_count + gi : nullptr,
-                                         NBL ? A.nb_list + (size_t)gi * A.nb_maxlen : nullptr, A.nb_maxlen);
+                    nbc[k] = NBL ? A.nb_count + gi : nullptr;
+                    nbl[k] = NBL ? A.nb_list + (size_t)gi * A.nb_maxlen : nullptr;
+                }
+                for (int j0 = 0; j0 < nt; j0 += G6_FOLD) {
+                    const int j1 = min(j0 + G6_FOLD, nt);
+                    G6Acc2 a[NP];
+                    const float2 z2 = make_float2(0.f, 0.f);
+#pragma unroll
+                    for (int p = 0; p < NP; p++) a[p] = G6Acc2{z2, z2, z2, z2, z2, z2, {0.f, 0.f}};
+#pragma unroll 2
+                    for (int j = j0; j < j1; j++) {
+                        const G6PredJ J = sj[j];
+                        const int jadr = T.j0 + jt + j;
+#pragma unroll
+                        for (int p = 0; p < NP; p++)
+                            g6_pair2<FF, NN, NBL, SELF, TILEMIN>(J, jadr, pi + 2 * p, vxi + 2 * p, vyi + 2 * p,
+                                                                 vzi + 2 * p, idi + 2 * p, A.eps2, hinv + 2 * p, a[p],
+                                                                 (TILEMIN ? tmin : kmin) + 2 * p, kadr + 2 * p,
+                                                                 nbc + 2 * p, nbl + 2 * p, A.nb_maxlen);
+                    }
+#pragma unroll
+                    for (int p = 0; p < NP; p++) {
+                        const float2* v = &a[p].ax;
+#pragma unroll
+                        for (int h = 0; h < 2; h++) {
+                            const int k = 2 * p + h;
+#pragma unroll
+                            for (int c = 0; c < 6; c++) S[k][c] += (double)(h ? v[c].y : v[c].x);
+                            S[k][6] += (double)a[p].pot[h];
+                        }
+                    }
+                }
+            } else {
+                // blocks of G6_FOLD terms per lane
+                for (int j0 = 0; j0 < nt; j0 += G6_FOLD * JL) {
+                    const int j1 = min(j0 + G6_FOLD * JL, nt);
+                    G6Acc a[IPT];
+#pragma unroll
+                    for (int k = 0; k < IPT; k++) a[k] = G6Acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll 2
+                    for (int j = j0 + jl; j < j1; j += JL) {
+                        const G6PredJ J = sj[j];
+                        const int jadr = T.j0 + jt + j;
+#pragma unroll
+                        for (int k = 0; k < IPT; k++) {
+                            int li = slot + k * ISL;
+                            int gi = T.i0 + (li < T.ni ? li : 0);
+                            g6_pair<FF, NN, NBL, SELF>(J, jadr, pi[k], vxi[k], vyi[k], vzi[k], idi[k], A.eps2,
+                                                       hinv[k], a[k], kmin[k], kadr[k],
+                                                       NBL ? A.nb_count + gi : nullptr,
+                                                       NBL ? A.nb_list + (size_t)gi * A.nb_maxlen : nullptr,
+                                                       A.nb_maxlen);
+                        }
+                    }
+#pragma unroll
+                    for (int k = 0; k < IPT; k++) {
+                        S[k][0] += (double)a[k].ax;
+                        S[k][1] += (double)a[k].ay;
+                        S[k][2] += (double)a[k].az;
+                        S[k][3] += (double)a[k].jx;
+                        S[k][4] += (double)a[k].jy;
+                        S[k][5] += (double)a[k].jz;
+                        S[k][6] += (double)a[k].pot;
+                    }
                 }
             }
+        };
+        if (self_tile) run_tile(BoolC<true>{});
+        else run_tile(BoolC<false>{});
+
+        if constexpr (TILEMIN) {
 #pragma unroll
-            for (int k = 0; k < IPT; k++) {
-                S[k][0] += (double)a[k].ax;
-                S[k][1] += (double)a[k].ay;
-                S[k][2] += (double)a[k].az;
-                S[k][3] += (double)a[k].jx;
-                S[k][4] += (double)a[k].jy;
-                S[k][5] += (double)a[k].jz;
-                S[k][6] += (double)a[k].pot;
+            for (int k = 0; k < IPT; k++)
+                if (tmin[k] < kmin[k]) {
+                    kmin[k] = tmin[k];
+                    ktile[k] = jt;
+                }
+        }
+    }
+    if constexpr (TILEMIN) {
+        // the address of each i's nearest neighbour: the first j of its best tile with that key
+        // (the j-paired form reads its i-record again rather than keep it in registers)
+#pragma unroll
+        for (int k = 0; k < IPT; k++) {
+            const int li = slot + k * ISL;
+            if (li < T.ni && ktile[k] >= 0) {
+                if constexpr (USE_JP) {
+                    const G6I P = A.ipart[T.i0 + li];
+                    kadr[k] = g6_rescan<FF>(A.jpred, T.j0 + ktile[k], min(NT, T.nj - ktile[k]), P.p, P.id, A.eps2,
+                                            kmin[k]);
+                } else {
+                    kadr[k] = g6_rescan<FF>(A.jpred, T.j0 + ktile[k], min(NT, T.nj - ktile[k]), pi[k], idi[k],
+                                            A.eps2, kmin[k]);
+                }
             }
         }
-        }
+    }
+    if constexpr (USE_JP) {
+#pragma unroll
+        for (int k = 0; k < IPT; k++)
+#pragma unroll
+            for (int c = 0; c < 7; c++) S[k][c] = Ssh[(k * 7 + c) * NT + threadIdx.x];
     }
 
     G6Out* dst_row = (T.group < 0) ? nullptr : A.partial + (size_t)T.slot * A.itile;
@@ -575,17 +884,18 @@ __device__ __forceinline__ void g6_task(const G6Args& A, const Task& T, unsigned
     }
 }
 
-template <int NT, int IPT, int JL, bool FF, bool NN, bool NBL>
-__global__ void __launch_bounds__(NT) g6_kernel(const G6Args A) {
-    // j tile during the loop, per-thread results (G6Out) after it
-    __shared__ __align__(16) unsigned char smem[NT * sizeof(G6Out)];
+template <int NT, int IPT, int JL, bool FF, bool NN, bool NBL, bool JP = false>
+__global__ void __launch_bounds__(NT, (JP && FF && !NBL) ? 512 / NT : 1) g6_kernel(const G6Args A) {
+    // j tile during the loop, per-thread results (G6Out) after it; the j-paired form is held to
+    // 128 registers a thread (512 threads an SM at least)
+    __shared__ __align__(16) unsigned char smem[g6_smem_bytes<NT, JP && FF && !NBL && IPT == 2 && JL == 1>()];
     __shared__ int s_task, s_flag;
 
     for (bool first = true;; first = false) {
         int t = next_task(A.task_counter, &s_task, A.ntasks, first);
         if (t >= A.ntasks) break;
         const Task T = A.tasks ? A.tasks[t] : regular_task(A, t);
-        g6_task<NT, IPT, JL, FF, NN, NBL>(A, T, smem);
+        g6_task<NT, IPT, JL, FF, NN, NBL, JP>(A, T, smem);
         if (T.group < 0 || A.partial_only) continue;
         const Group G = A.groups ? A.groups[T.group] : regular_group(A, T.group);
         double2* W = reinterpret_cast<double2*>(smem);

@@ -38,7 +38,8 @@
 // rewritten only after the closing barrier.
 // Every CTA derives the step's decisions (block time, ni, decomposition, end of the run) from
 // the same data, so they agree without further communication.  The barriers are bounded: a
-// barrier that waits longer than about a second sets an error word and the kernel returns.
+// barrier that waits longer than about a second (a limit the host may lower) sets an error word
+// and the kernel returns.
 // The i-predictor and the corrector use the reference's formulas and constants in the order
 // its C source evaluates them, with every FP64 multiply and add rounded separately (no fused
 // multiply-add): given the same forces the new state equals a plain C evaluation bit for bit.
@@ -67,14 +68,19 @@ struct HmClock {
     long long psteps, bsteps;
     long long force_pairs;
     long long variant_steps[5];   // steps by force decomposition (i-tile 16, 32, 64, 128, 512)
+    long long spin_limit;         // SM cycles a wait may last (0: HM_SPIN_LIMIT)
     int t_mod;
     int ni;       // the last step's active count
     int nch;      // its force decomposition: j-chunks and i-tile
     int itile;
     int bad;      // start-up steps below dtmin
     int err;      // a wait gave up
+    int exits;    // CTAs that have returned from the step kernel (all launches)
     int pad;
 };
+
+// Default limit of every wait of the step kernel: about a second of SM clock.
+constexpr long long HM_SPIN_LIMIT = 2000000000LL;
 
 // Grid barrier state: the generation CTA 0 last released, the step number (the tag of the
 // flags below) at the end of the last launch, and per CTA the generation it last arrived at
@@ -316,11 +322,13 @@ __device__ __forceinline__ void hm_startup(const HmState& P, const HmWork& W, in
 // in its own arrival word; CTA 0's threads watch the arrival words, and once every CTA is in
 // they release the generation, for which the other CTAs wait.  No atomics, no shared counter.
 // Release/acquire through the fences around the flag stores and loads.  A wait gives up after
-// about a second of SM clock (error word set); returns false on error (the caller returns).
+// about a second of SM clock (C->spin_limit cycles when set; error word set); returns false on
+// error (the caller returns).
 __device__ __forceinline__ bool hm_spin_until(volatile unsigned* w, unsigned target, HmClock* C) {
     const long long t0 = clock64();
+    const long long lim = C->spin_limit > 0 ? C->spin_limit : HM_SPIN_LIMIT;
     while (*w != target) {
-        if (clock64() - t0 > 2000000000LL) {
+        if (clock64() - t0 > lim) {
             atomicExch(&C->err, 1);
             return false;
         }
@@ -481,7 +489,7 @@ __device__ __forceinline__ void hm_publish(unsigned* flag, unsigned tag) {
 }
 
 template <bool FF>
-__global__ void __launch_bounds__(HM_NT, 2) hm_run_kernel(const HmRun R) {
+__device__ __forceinline__ void hm_run_body(const HmRun& R) {
     __shared__ __align__(16) unsigned char smem[HM_NT * sizeof(G6Out)];
     __shared__ int s_boff[HM_MAXSEG + 1];   // offsets of every segment's active particles (+ ni)
     __shared__ unsigned long long sm[HM_NT / 32];
@@ -618,6 +626,15 @@ __global__ void __launch_bounds__(HM_NT, 2) hm_run_kernel(const HmRun R) {
         E++;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) W.sync->step = E;
+}
+
+// The step kernel: the body above, then every CTA counts its return (on every path, the early
+// returns of a wait that gave up included), so the host can tell that the whole grid has left.
+template <bool FF>
+__global__ void __launch_bounds__(HM_NT, 2) hm_run_kernel(const HmRun R) {
+    hm_run_body<FF>(R);
+    __syncthreads();
+    if (threadIdx.x == 0) atomicAdd(&R.W.clk->exits, 1);
 }
 
 // Kinetic and potential energy (calc_energy.c:9-33): ek = sum m v^2 / 2, ew = sum m pot / 2.

@@ -1,0 +1,130 @@
+// pgb_peak.cu -- measured throughput ceilings of the two pipes the force kernels run on, for the
+// benchmark's roofline (lib/libpgbpeak.so).  Not part of the GRAPE drop-in.
+//
+//  * FP32 FMA pipe: every thread runs PEAK_CHAINS independent FFMA dependency chains
+//    (x = x * a + b), long enough that the launch overhead is negligible; the grid is a whole
+//    number of waves of resident CTAs on every SM.  2 flop per FFMA.
+//  * MUFU (XU pipe) reciprocal square root: every thread runs PEAK_CHAINS independent chains of
+//    rsqrt.approx.ftz.f32 (x = rsqrt(x), which stays in [1, 4) for a start in [1, 4)), the
+//    instruction the force kernels use.
+// Both kernels write one value per thread (so that nothing is optimised away) into a caller
+// buffer or a small internal one.  Times are CUDA-event times on the caller's stream.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+
+#define PGB_EXPORT extern "C" __attribute__((visibility("default")))
+
+namespace {
+
+constexpr int PEAK_THREADS = 256;
+constexpr int PEAK_CHAINS = 8;
+
+__global__ void __launch_bounds__(PEAK_THREADS) ffma_kernel(float* out, int iters, float a, float b) {
+    float x[PEAK_CHAINS];
+#pragma unroll
+    for (int c = 0; c < PEAK_CHAINS; c++) x[c] = (float)(threadIdx.x + c) * 1e-3f;
+    for (int k = 0; k < iters; k++) {
+#pragma unroll
+        for (int u = 0; u < 16; u++)
+#pragma unroll
+            for (int c = 0; c < PEAK_CHAINS; c++) x[c] = __fmaf_rn(x[c], a, b);
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int c = 0; c < PEAK_CHAINS; c++) s += x[c];
+    out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+__device__ __forceinline__ float rsqrt_approx(float x) {
+    float y;
+    asm volatile("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+__global__ void __launch_bounds__(PEAK_THREADS) mufu_kernel(float* out, int iters) {
+    float x[PEAK_CHAINS];
+#pragma unroll
+    for (int c = 0; c < PEAK_CHAINS; c++) x[c] = 1.0f + (float)((threadIdx.x + c) & 255) * (1.0f / 128.0f);
+    for (int k = 0; k < iters; k++) {
+#pragma unroll
+        for (int u = 0; u < 16; u++)
+#pragma unroll
+            for (int c = 0; c < PEAK_CHAINS; c++) x[c] = rsqrt_approx(x[c]);
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int c = 0; c < PEAK_CHAINS; c++) s += x[c];
+    out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+// Runs kern `reps` times after one warm-up launch and returns the best launch time (ms), or a
+// negative value on a CUDA error.
+template <typename L>
+float best_ms(L launch, int reps, cudaStream_t s) {
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return -1.f;
+    launch();
+    float best = 1e30f;
+    for (int r = 0; r < reps; r++) {
+        cudaEventRecord(e0, s);
+        launch();
+        cudaEventRecord(e1, s);
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+            best = -1.f;
+            break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best) best = ms;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (cudaGetLastError() != cudaSuccess) return -1.f;
+    return best;
+}
+
+int grid_blocks(const void* kern) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, PEAK_THREADS, 0);
+    if (per_sm < 1) per_sm = 1;
+    return sms * per_sm;
+}
+
+}  // namespace
+
+// FP32 FFMA throughput of the current device: *tflops = flops / best launch time (2 flop per
+// FFMA), *ms = that time, *blocks = the grid (resident CTAs x SMs).  iters x 16 x 8 FFMA per
+// thread.  Returns 0, or -1 on a CUDA error.
+PGB_EXPORT int pgb_peak_fp32(int iters, void* stream, double* tflops, double* ms, int* blocks) {
+    cudaStream_t s = (cudaStream_t)stream;
+    const int grid = grid_blocks((const void*)ffma_kernel);
+    float* out = nullptr;
+    if (cudaMalloc(&out, (size_t)grid * PEAK_THREADS * sizeof(float)) != cudaSuccess) return -1;
+    float t = best_ms([&] { ffma_kernel<<<grid, PEAK_THREADS, 0, s>>>(out, iters, 0.999f, 1e-3f); }, 5, s);
+    cudaFree(out);
+    if (t <= 0.f) return -1;
+    const double flops = 2.0 * grid * PEAK_THREADS * (double)iters * 16 * PEAK_CHAINS;
+    if (tflops) *tflops = flops / (t * 1e-3) / 1e12;
+    if (ms) *ms = t;
+    if (blocks) *blocks = grid;
+    return 0;
+}
+
+// MUFU rsqrt.approx.ftz.f32 throughput of the current device: *gops = rsqrt per second / 1e9.
+PGB_EXPORT int pgb_peak_mufu(int iters, void* stream, double* gops, double* ms, int* blocks) {
+    cudaStream_t s = (cudaStream_t)stream;
+    const int grid = grid_blocks((const void*)mufu_kernel);
+    float* out = nullptr;
+    if (cudaMalloc(&out, (size_t)grid * PEAK_THREADS * sizeof(float)) != cudaSuccess) return -1;
+    float t = best_ms([&] { mufu_kernel<<<grid, PEAK_THREADS, 0, s>>>(out, iters); }, 5, s);
+    cudaFree(out);
+    if (t <= 0.f) return -1;
+    const double ops = (double)grid * PEAK_THREADS * (double)iters * 16 * PEAK_CHAINS;
+    if (gops) *gops = ops / (t * 1e-3) / 1e9;
+    if (ms) *ms = t;
+    if (blocks) *blocks = grid;
+    return 0;
+}

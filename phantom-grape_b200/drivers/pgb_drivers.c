@@ -97,11 +97,33 @@ double g6drv_set_j(void *handle, int n, const double *pos, const double *vel, co
  * xi/vi[set_off[c] ..].  With `resend`, the active particles' j-records (from pos..tj) are
  * re-sent after each call, as the corrector does (hermite.c:255-275).  Outputs (optional) are
  * written per active particle in the same concatenated order.  Returns the elapsed seconds. */
+double g6drv_schedule2(void *handle, int nj, int ncalls, const int *set_off, const int *set_idx,
+                       const double *t_calls, const double *xi, const double *vi, double eps2, int with_nnb,
+                       int resend, const int *rs_off, const int *rs_idx, const double *pos, const double *vel,
+                       const double *acc2, const double *jrk6, const double *mass, const double *tj, const int *idx,
+                       double *acc_out, double *jrk_out, double *pot_out, int *nnb_out, float *rnnb_out);
+
 double g6drv_schedule(void *handle, int nj, int ncalls, const int *set_off, const int *set_idx,
                       const double *t_calls, const double *xi, const double *vi, double eps2, int with_nnb,
                       int resend, const double *pos, const double *vel, const double *acc2, const double *jrk6,
                       const double *mass, const double *tj, const int *idx, double *acc_out, double *jrk_out,
                       double *pot_out, int *nnb_out, float *rnnb_out) {
+    return g6drv_schedule2(handle, nj, ncalls, set_off, set_idx, t_calls, xi, vi, eps2, with_nnb, resend, NULL, NULL,
+                           pos, vel, acc2, jrk6, mass, tj, idx, acc_out, jrk_out, pot_out, nnb_out, rnnb_out);
+}
+
+/* As g6drv_schedule, with the particles re-sent after call c given separately (rs_off / rs_idx,
+ * NULL: the call's own set): a rank of a sharded schedule computes the forces of a slice of each
+ * active set but updates its j-memory with the whole set. */
+double g6drv_schedule2(void *handle, int nj, int ncalls, const int *set_off, const int *set_idx,
+                       const double *t_calls, const double *xi, const double *vi, double eps2, int with_nnb,
+                       int resend, const int *rs_off, const int *rs_idx, const double *pos, const double *vel,
+                       const double *acc2, const double *jrk6, const double *mass, const double *tj, const int *idx,
+                       double *acc_out, double *jrk_out, double *pot_out, int *nnb_out, float *rnnb_out) {
+    if (!rs_off || !rs_idx) {
+        rs_off = set_off;
+        rs_idx = set_idx;
+    }
     g6api *a = (g6api *)handle;
     int npipe = a->npipes();
     int *pidx = (int *)malloc(sizeof(int) * npipe);
@@ -134,8 +156,8 @@ double g6drv_schedule(void *handle, int nj, int ncalls, const int *set_off, cons
             if (rnnb_out && with_nnb) memcpy(rnnb_out + o, rnnb, sizeof(float) * nii);
         }
         if (resend) {
-            for (int k = 0; k < ni; k++) {
-                int j = set_idx[off + k];
+            for (int k = rs_off[c]; k < rs_off[c + 1]; k++) {
+                int j = rs_idx[k];
                 a->set_j(0, j, idx[j], tj[j], 0.0, mass[j], snp, (double *)jrk6 + 3 * j, (double *)acc2 + 3 * j,
                          (double *)vel + 3 * j, (double *)pos + 3 * j);
             }

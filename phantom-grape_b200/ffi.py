@@ -258,6 +258,8 @@ class G6(_ErrMixin):
         _sig(L, "pgb6_last_error", [C.c_char_p, C.c_int], C.c_int)
         _sig(L, "pgb6_clear_error", [])
         _sig(L, "pgb6_set_abort", [C.c_int])
+        _sig(L, "pgb6_set_call_timing", [C.c_int])
+        _sig(L, "pgb6_call_device_ms", [C.c_int], C.c_double)
         _sig(L, "pgb6_record_sizes", [ip, ip, ip, ip])
         _sig(L, "pgb6_plan_create", [C.POINTER(vp), C.c_int, ip, C.c_int], C.c_int)
         _sig(L, "pgb6_plan_launch", [vp, vp, vp, C.c_double, vp, vp], C.c_int)
@@ -276,6 +278,8 @@ class G6(_ErrMixin):
         _sig(L, "pgb6_hermite_step", [vp, dp, ip], C.c_int)
         _sig(L, "pgb6_hermite_advance", [vp, C.c_double, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)], C.c_int)
         _sig(L, "pgb6_hermite_time", [vp], C.c_double)
+        _sig(L, "pgb6_hermite_set_wait_limit", [vp, C.c_longlong], C.c_int)
+        _sig(L, "pgb6_hermite_wait_status", [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int)
         _sig(L, "pgb6_hermite_get", [vp, dp, dp, dp, dp, dp, dp, dp], C.c_int)
         _sig(L, "pgb6_hermite_last_step", [vp, ip, dp, dp, dp], C.c_int)
         _sig(L, "pgb6_hermite_energy", [vp, dp, dp], C.c_int)
@@ -574,6 +578,16 @@ class Hermite:
     @property
     def time(self):
         return self.L.pgb6_hermite_time(self.h)
+
+    def set_wait_limit(self, cycles):
+        """pgb6_hermite_set_wait_limit: the SM cycles after which a wait of the step kernel gives up."""
+        self._check(self.L.pgb6_hermite_set_wait_limit(self.h, int(cycles)), "set_wait_limit")
+
+    def wait_status(self):
+        """(a wait gave up, CTAs returned from the step kernel so far, CTAs per launch)."""
+        g, e, n = C.c_int(), C.c_int(), C.c_int()
+        self._check(self.L.pgb6_hermite_wait_status(self.h, C.byref(g), C.byref(e), C.byref(n)), "wait_status")
+        return g.value, e.value, n.value
 
     def get(self):
         n = self.n

@@ -22,7 +22,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = "/root/reference"
+REF = os.environ.get("PGB_REFERENCE", "/root/reference")
 BANANA = os.path.join(ROOT, "oracle", "_ref", "banana01")
 INIT = os.path.join(REF, "PG6", "banana", "init", "pl001k.init")
 

@@ -301,3 +301,66 @@ def test_plan_update_matches_fresh_plans(g6):
     finally:
         if plan is not None:
             g6.plan_destroy(plan)
+
+
+def test_every_configuration_vs_fp64(g6, state):
+    """Every kernel configuration of the batched Hermite path (pinned with pgb6_plan_set_config;
+    both position layouts, with and without the nearest neighbour) on items that exercise the
+    per-tile self test (i-particles inside their own j-range and outside it), ragged j-tiles
+    (j counts that are not multiples of 4 or of the tile) and single-j items, against the FP64
+    oracle: rms relative acc / jerk / pot <= 1e-6 per item, nearest neighbour identical wherever
+    the FP64 first and second neighbours are separated."""
+    import torch
+    st = state
+    n = len(st.mass)
+    xp, vp = O.g6_predict(st.t_now, st.pos, st.vel, st.acc2, st.jrk6, st.tj)
+    vpf = vp.astype(np.float32).astype(np.float64)
+    mf = st.mass.astype(np.float32).astype(np.float64)
+    rng = W.Rng(77)
+    act = np.sort(rng.permutation(n)[:3000]).astype(np.int32)
+    # (i indices, j range): all j; a ragged j-range; a single j (the i-set excludes it); i
+    # outside their j-range; a j-range that holds every i
+    cases = [(act, 0, n), (act[:37], 0, 4099), (np.arange(10, 60, dtype=np.int32), 5, 1),
+             (np.arange(5000, 5300, dtype=np.int32), 0, 130), (np.arange(200, 457, dtype=np.int32), 190, 1003)]
+    ii = np.concatenate([c[0] for c in cases])
+    ioff = np.concatenate([[0], np.cumsum([len(c[0]) for c in cases])]).astype(np.int64)
+    items = np.array([[ioff[k], len(c[0]), c[1], c[2]] for k, c in enumerate(cases)], np.int32)
+    refs = [O.g6_force(xp[c[0]], vpf[c[0]], st.idx[c[0]], np.float32(st.eps2), xp[c[1]:c[1] + c[2]],
+                       vpf[c[1]:c[1] + c[2]], mf[c[1]:c[1] + c[2]], st.idx[c[1]:c[1] + c[2]]) for c in cases]
+    dev = torch.device("cuda")
+    ncfg = 0
+    for ff in (True, False):
+        d_i = torch.from_numpy(pgb.ffi.g6_irecords(xp[ii], vp[ii], st.idx[ii], ff=ff).view(np.uint8)).to(dev)
+        d_j = torch.from_numpy(pgb.ffi.g6_jrecords(xp, vp, st.mass, st.idx, ff=ff).view(np.uint8)).to(dev)
+        d_o = torch.zeros(len(ii) * pgb.ffi.G6OUT.itemsize, dtype=torch.uint8, device=dev)
+        for nn in (True, False):
+            plan = g6.plan_create(items, nn=nn, f64=not ff)
+            try:
+                g6.set_abort(False)
+                cfg = 0
+                while g6.L.pgb6_plan_set_config(plan, cfg) == 0:
+                    d_o.fill_(0xFF)
+                    g6.plan_launch(plan, d_i.data_ptr(), d_j.data_ptr(), st.eps2, d_o.data_ptr(), 0)
+                    torch.cuda.synchronize()
+                    out = d_o.cpu().numpy().view(pgb.ffi.G6OUT)
+                    for k, (c, ref) in enumerate(zip(cases, refs)):
+                        o = out[ioff[k]:ioff[k + 1]]
+                        tag = (ff, nn, cfg, k)
+                        acc = np.stack([o["ax"], o["ay"], o["az"]], 1)
+                        jrk = np.stack([o["jx"], o["jy"], o["jz"]], 1)
+                        assert rms(rel(acc, ref["acc"])) <= 1e-6, tag
+                        assert rms(rel(jrk, ref["jrk"])) <= 1e-6, tag
+                        assert rms((o["pot"] - ref["pot"]) / np.abs(ref["pot"])) <= 1e-6, tag
+                        if nn:
+                            clear = ref["r2nn2"] / ref["r2nn"] - 1.0 > 1e-5 if c[2] > 1 else np.ones(len(o), bool)
+                            jadr = o["jadr"]
+                            assert np.all((jadr >= c[1]) & (jadr < c[1] + c[2])), tag
+                            assert np.array_equal(st.idx[jadr][clear], ref["nnb"][clear]), tag
+                            np.testing.assert_allclose(-2.0 / o["key"], ref["rnnb"], rtol=1e-6, err_msg=str(tag))
+                    cfg += 1
+                ncfg = max(ncfg, cfg)
+            finally:
+                g6.clear_error()
+                g6.set_abort(True)
+                g6.plan_destroy(plan)
+    assert ncfg >= 8

@@ -16,6 +16,7 @@ output time and the step counts stay within the spread that force rounding cause
 reference and the FP64 oracle (tolerances in the tests).  Sizes: 1024 bodies (one selection
 segment, small-call force kernel) and 16384 (eight segments, regular-mode force kernel).
 """
+import ctypes as C
 import os
 
 import numpy as np
@@ -176,3 +177,36 @@ def test_bad_arguments_are_refused(g6):
     finally:
         g6.clear_error()
         g6.set_abort(True)
+
+
+def test_bounded_wait_gives_up_and_every_cta_returns(g6):
+    """The step kernel's waits are bounded.  With the limit lowered to 100 SM cycles, a wait of
+    an ordinary advance (the first grid barrier: 296 CTAs do not all arrive within 100 cycles)
+    runs out: the error word is set, every CTA of the launch returns (the exit count grows by
+    the grid), the call reports PGB_ERR_DEVICE, and the context stays usable (a fresh integrator
+    with the default limit runs afterwards).  Nothing hangs: every wait ends after its limit."""
+    x, v, m = W.plummer_henon(2048, W.SEED0 + 31)
+    H = pgb.ffi.Hermite(g6, m, x, v, 1.0 / 64 ** 2, 0.2, 0.01, 0.125)
+    try:
+        gave_up, exits0, grid = H.wait_status()
+        assert gave_up == 0 and exits0 == grid > 0          # the start-up launch
+        H.set_wait_limit(100)
+        g6.set_abort(False)
+        g6.clear_error()
+        p, b = C.c_longlong(), C.c_longlong()
+        rc = g6.L.pgb6_hermite_advance(H.h, 0.125, C.byref(p), C.byref(b))
+        code, msg = g6.last_error()
+        assert rc == 4 and code == 4 and "timed out" in msg   # PGB_ERR_DEVICE
+        gave_up, exits1, _ = H.wait_status()
+        assert gave_up == 1 and exits1 == exits0 + grid
+    finally:
+        g6.clear_error()
+        g6.set_abort(True)
+        H.close()
+    H2 = pgb.ffi.Hermite(g6, m, x, v, 1.0 / 64 ** 2, 0.2, 0.01, 0.125)
+    try:
+        H2.advance(0.125)
+        assert H2.time == 0.125
+        assert H2.wait_status()[0] == 0
+    finally:
+        H2.close()
