@@ -53,7 +53,8 @@ SM_COUNT = 148
 REF_SRC = os.environ.get("PGB_REFERENCE", "/root/reference")
 # DRAM bytes (read + write) of one launch of the roofline kernel, from the committed ncu captures
 # (dram__bytes_read.sum + dram__bytes_write.sum); the bench cannot run ncu itself.
-G5_CFG_NAMES = ["128x4", "256x2", "512x2", "1024x1", "384x2", "128x2", "128x1", "64x1"]   # pgb5 configurations (threads x i/thread)
+G5_CFG_NAMES = ["128x4", "256x2", "512x2", "1024x1", "384x2", "128x2", "128x1", "64x1", "64x1 j-paired",
+                "1024x1 j-paired", "256x1 j-paired"]   # pgb5 configurations (threads x i/thread)
 PROFILED_TRAFFIC = {
     "hermite": {"bytes": 6_485_760 + 17_935_104,
                 "source": "profiles/g6_kernel_hermite_65536x65536.md (128x2 configuration, paired accumulations)"},
@@ -1336,6 +1337,12 @@ def run_bh(args, pgb, ws, rank, local):
             cpu = {"value": sp / tr / 1e9, "unit": "Gint/s", "cores": cores, "kind": "reference",
                    "sample": f"first {ng} of {bh.ngroups} groups ({sp:.3e} pairs), PG5/newton_quad libraries "
                    "(libpg5 + quad, AVX2) built from their sources, OpenMP over groups with g5_*MC / g5c_*MC"}
+    if "same_lists_fp64" in errors:
+        cpu = cpu if cpu is not None else {}
+        cpu["fp64_check"] = {"acc": errors["same_lists_fp64"], "direct_sum_acc": errors["direct_sum_fp64"],
+                             "oracle": "FP64 on the same interaction lists and float32 inputs (every 97th group); "
+                                       "the full FP64 direct sum on 4096 sampled particles measures the multipole "
+                                       "truncation at theta = 0.5"}
     g5.plan_destroy(pl_p)
     g5.plan_destroy(pl_c)
     return _line(args, ws, "Gint/s (Barnes-Hut point masses + quadrupole cells, batched)", value, t_max / len(tms),

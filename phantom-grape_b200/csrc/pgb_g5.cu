@@ -51,12 +51,15 @@ constexpr int MAXDEV = 64;
 // most of its threads); the table
 // kind keeps its force table in static shared memory (CTAs of <= 256 threads) and the quad
 // kind stages three words per cell (<= 512 threads).  Plans pick one with pgb5_plan_tune.
+// G5C_*J: the j-paired form (newton point masses and quadrupole cells only;
+// pgb_g5_kernels.cuh g5_newton_jpair / g5_quad_jpair).
 enum G5Cfg {
     G5C_128x4 = 0, G5C_256x2 = 1, G5C_512x2 = 2, G5C_1024x1 = 3, G5C_384x2 = 4, G5C_128x2 = 5, G5C_128x1 = 6,
-    G5C_64x1 = 7, G5_NCFG = 8
+    G5C_64x1 = 7, G5C_64x1J = 8, G5C_1024x1J = 9, G5C_256x1J = 10, G5_NCFG = 11
 };
-constexpr int G5C_NT[G5_NCFG] = {128, 256, 512, 1024, 384, 128, 128, 64};
-constexpr int G5C_IPT[G5_NCFG] = {4, 2, 2, 1, 2, 2, 1, 1};
+constexpr int G5C_NT[G5_NCFG] = {128, 256, 512, 1024, 384, 128, 128, 64, 64, 1024, 256};
+constexpr int G5C_IPT[G5_NCFG] = {4, 2, 2, 1, 2, 2, 1, 1, 1, 1, 1};
+inline bool cfg_jp(int c) { return c >= G5C_64x1J; }
 constexpr int ITILE_MAX = 1024;
 inline int cfg_itile(int c) { return G5C_NT[c] * G5C_IPT[c]; }
 template <int KIND, int NT>
@@ -64,6 +67,7 @@ constexpr bool kind_fits() {
     return KIND == G5_TABLE ? NT <= 256 : (KIND == G5_QUAD ? NT <= 512 : true);
 }
 inline bool cfg_valid(int kind, int c) {
+    if (cfg_jp(c)) return (kind == G5_NEWTON || kind == G5_QUAD) && (kind != G5_QUAD || G5C_NT[c] <= 512);
     return kind == G5_TABLE ? G5C_NT[c] <= 256 : (kind == G5_QUAD ? G5C_NT[c] <= 512 : true);
 }
 constexpr int MAXPIPE = 4096;
@@ -109,15 +113,15 @@ bool ensure_device() {
 }
 
 // Launch (occ == nullptr) or query the resident CTAs per SM (into *occ) of one kernel.
-template <int KIND, int NT, int IPT>
+template <int KIND, int NT, int IPT, bool JP = false>
 cudaError_t launch_k(int grid, const G5Args& a, cudaStream_t s, int* occ) {
-    if constexpr (!kind_fits<KIND, NT>()) {
+    if constexpr (!kind_fits<KIND, NT>() || (JP && KIND != G5_NEWTON && KIND != G5_QUAD)) {
         return cudaErrorInvalidConfiguration;
     } else {
         // the table kind's table lives in dynamic shared memory (a.tbl_size entries)
         const size_t dyn = (KIND == G5_TABLE) ? (size_t)a.tbl_size * sizeof(float2) : 0;
-        if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, g5_kernel<KIND, NT, IPT>, NT, dyn);
-        g5_kernel<KIND, NT, IPT><<<grid, NT, dyn, s>>>(a);
+        if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, g5_kernel<KIND, NT, IPT, JP>, NT, dyn);
+        g5_kernel<KIND, NT, IPT, JP><<<grid, NT, dyn, s>>>(a);
         return cudaGetLastError();
     }
 }
@@ -132,6 +136,9 @@ cudaError_t launch_cfg(int cfg, int grid, const G5Args& a, cudaStream_t s, int* 
         case G5C_128x2: return launch_k<KIND, 128, 2>(grid, a, s, occ);
         case G5C_128x1: return launch_k<KIND, 128, 1>(grid, a, s, occ);
         case G5C_64x1: return launch_k<KIND, 64, 1>(grid, a, s, occ);
+        case G5C_64x1J: return launch_k<KIND, 64, 1, true>(grid, a, s, occ);
+        case G5C_1024x1J: return launch_k<KIND, 1024, 1, true>(grid, a, s, occ);
+        case G5C_256x1J: return launch_k<KIND, 256, 1, true>(grid, a, s, occ);
         default: return launch_k<KIND, 128, 4>(grid, a, s, occ);
     }
 }

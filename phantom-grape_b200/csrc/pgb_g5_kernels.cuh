@@ -196,6 +196,84 @@ __device__ __forceinline__ void g5_interact2(const float4* sj, int j, const floa
     }
 }
 
+// ---- j-paired form (the 64-thread tree-code CTAs) ------------------------------------------
+// One i-particle against two consecutive j records (a "j-pair"), the j-tile held in shared memory
+// as one array per field (G5TileSoA), so that a 16-byte shared load returns a field of four
+// consecutive j and every paired FP32 operand is a natural register pair: (j, j+1) for the j
+// fields, a loop-invariant (v, v) for the i position.  The relative coordinates and the
+// accumulations -- and for cells the Q.dr products -- issue as paired FP32 instructions on the
+// heavy half of the FMA pipe, the rest of the chain stays scalar, loading the two halves about
+// equally.  Per pair the arithmetic is g5_interact's, operation for operation (FADD2 / FFMA2
+// round each lane as FADD / FFMA): the two lanes of an accumulator sum the even and the odd j.
+// The cells' quadrupole moments are stored negated (-Q), which turns the subtraction of the
+// -Q.dr / r^5 term into a plain FFMA2 with the same rounding.
+template <int NT>
+struct G5TileSoA {
+    float x[NT], y[NT], z[NT], m[NT];
+    float q[6][NT];   // cells: -q00 -q01 -q02 -q11 -q12 -q22
+};
+
+__device__ __forceinline__ void g5_newton_jpair(float2 X, float2 Y, float2 Z, float2 M, float2 nx, float2 ny,
+                                                float2 nz, float e, float2 (&a)[4]) {
+    const float2 dx = __fadd2_rn(X, nx), dy = __fadd2_rn(Y, ny), dz = __fadd2_rn(Z, nz);
+    float2 mq, q;
+    const float* dxp = &dx.x;
+    const float* dyp = &dy.x;
+    const float* dzp = &dz.x;
+    const float* mp = &M.x;
+    float* mqp = &mq.x;
+    float* qp = &q.x;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const float r2 = __fmaf_rn(dzp[h], dzp[h], __fmaf_rn(dyp[h], dyp[h], __fmaf_rn(dxp[h], dxp[h], e)));
+        qp[h] = minus2_over_r(r2);
+        mqp[h] = mp[h] * qp[h];
+    }
+    const float2 mq3 = __fmul2_rn(mq, __fmul2_rn(q, q));
+    a[3] = __fadd2_rn(a[3], mq);
+    a[0] = __ffma2_rn(mq3, dx, a[0]);
+    a[1] = __ffma2_rn(mq3, dy, a[1]);
+    a[2] = __ffma2_rn(mq3, dz, a[2]);
+}
+
+// Q = (-q00 -q01 -q02 -q11 -q12 -q22) of the two cells, as pairs.
+__device__ __forceinline__ void g5_quad_jpair(float2 X, float2 Y, float2 Z, float2 M, const float2 (&Q)[6], float2 nx,
+                                              float2 ny, float2 nz, float e, float2 (&a)[4]) {
+    const float2 dx = __fadd2_rn(X, nx), dy = __fadd2_rn(Y, ny), dz = __fadd2_rn(Z, nz);
+    // -(Q dr), component by component (c_GravityKernel, quad_avx2.c:35-149)
+    const float2 qx = __ffma2_rn(Q[2], dz, __ffma2_rn(Q[1], dy, __fmul2_rn(Q[0], dx)));
+    const float2 qy = __ffma2_rn(Q[4], dz, __ffma2_rn(Q[3], dy, __fmul2_rn(Q[1], dx)));
+    const float2 qz = __ffma2_rn(Q[5], dz, __ffma2_rn(Q[4], dy, __fmul2_rn(Q[2], dx)));
+    float2 dr5i, mr3i, s3;
+    const float* dxp = &dx.x;
+    const float* dyp = &dy.x;
+    const float* dzp = &dz.x;
+    const float* qxp = &qx.x;
+    const float* qyp = &qy.x;
+    const float* qzp = &qz.x;
+    const float* mp = &M.x;
+    float* d5p = &dr5i.x;
+    float* m3p = &mr3i.x;
+    float* s3p = &s3.x;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const float r2 = __fmaf_rn(dzp[h], dzp[h], __fmaf_rn(dyp[h], dyp[h], __fmaf_rn(dxp[h], dxp[h], e)));
+        const float q = minus2_over_r(r2);
+        const float ri = -0.5f * q;
+        const float ri2 = ri * ri;
+        const float phi_p = mp[h] * ri;
+        const float ndrqdr = __fmaf_rn(dzp[h], qzp[h], __fmaf_rn(dyp[h], qyp[h], dxp[h] * qxp[h]));   // -dr.Q.dr
+        d5p[h] = ri2 * ri2 * ri;
+        const float nphi_q = 0.5f * d5p[h] * ndrqdr;   // -phi_q
+        s3p[h] = phi_p - nphi_q;
+        m3p[h] = __fmaf_rn(-5.0f, nphi_q, phi_p) * ri2;
+    }
+    a[3] = __fadd2_rn(a[3], s3);
+    a[0] = __ffma2_rn(dx, mr3i, __ffma2_rn(qx, dr5i, a[0]));
+    a[1] = __ffma2_rn(dy, mr3i, __ffma2_rn(qy, dr5i, a[1]));
+    a[2] = __ffma2_rn(dz, mr3i, __ffma2_rn(qz, dr5i, a[2]));
+}
+
 // Final scaling of the FP64 sums into (acc, pot_raw).
 template <int KIND>
 __device__ __forceinline__ double4 g5_finish(double4 s, double ascale) {
@@ -229,11 +307,17 @@ __device__ __forceinline__ void g5_jloop(const float4* sj, int first, int nt, co
     }
 }
 
-template <int KIND, int NT, int IPT>
+template <int KIND, int NT, int IPT, bool JP = false>
 __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
     constexpr int W = JWords<KIND>::n;   // 16-byte words per j record
     constexpr bool LANES = (IPT == 1 && NT <= 64);
-    __shared__ float4 sj[NT * (W > 2 ? W : 2)];  // also the reduction buffer (double4 x NT)
+    // the j-paired form: newton point masses and quadrupole cells, one i per thread (the
+    // 64-thread CTAs run two for tasks of more than 32 i)
+    constexpr bool USE_JP = JP && IPT == 1 && (KIND == G5_NEWTON || KIND == G5_QUAD);
+    constexpr int KM = LANES ? 2 : 1;   // i per thread at most in the j-paired form
+    constexpr int SJ_RECS = NT * (W > 2 ? W : 2);
+    constexpr int SJ_SOA = USE_JP ? (int)((sizeof(G5TileSoA<NT>) + 15) / 16) : 0;
+    __shared__ float4 sj[SJ_RECS > SJ_SOA ? SJ_RECS : SJ_SOA];  // also the reduction buffer (double4 x NT)
     __shared__ int s_task, s_flag;
     // table kind: the force table in dynamic shared memory sized to the table (A.tbl_size
     // entries, 8 KB for 1024) for the lifetime of the CTA; the other kinds launch without any
@@ -315,6 +399,142 @@ __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
         }
     };
 
+    // The j-paired task (USE_JP).  In the 64-thread CTAs a task of more than NT/2 i runs two i
+    // per thread (slot and slot + NT/2) over two j-lanes, a smaller one one i per thread over
+    // nl = NT / isl lanes (isl = ni rounded up to 16, as the other form); lane l takes the tile's
+    // j-quads l, l + nl, ...  Larger CTAs: one i per thread, one lane.  The tile is staged as
+    // field arrays padded to a multiple of 4 with massless copies of its first record (and zero
+    // moments for cells), which add exact zeros.  FP32 sums are folded into FP64 every G5_FOLD
+    // j of a lane; the lanes' sums are added in lane order.
+    auto jp_task = [&](const Task& T) {
+        G5TileSoA<NT>* sa = reinterpret_cast<G5TileSoA<NT>*>(sj);
+        const bool two = LANES && T.ni > NT / 2;
+        int nl = 1, isl = NT;
+        if (two) {
+            nl = 2;
+            isl = NT / 2;
+        } else if (LANES) {
+            const int need = (T.ni + 15) & ~15;
+            nl = NT / (need > 0 ? need : 32);
+            isl = NT / nl;
+        }
+        const int slot = (int)threadIdx.x % isl, lane = (int)threadIdx.x / isl;
+        const int nik = two ? 2 : 1;
+        float2 nx[KM], ny[KM], nz[KM];
+        float ei[KM];
+        double S[KM][4];
+#pragma unroll
+        for (int k = 0; k < KM; k++) {
+            const int li = slot + k * isl;
+            const float4 p = A.ipos[T.i0 + (li < T.ni ? li : 0)];
+            nx[k] = make_float2(-p.x, -p.x);
+            ny[k] = make_float2(-p.y, -p.y);
+            nz[k] = make_float2(-p.z, -p.z);
+            ei[k] = p.w;
+            S[k][0] = S[k][1] = S[k][2] = S[k][3] = 0.0;
+        }
+        for (int jt = 0; jt < T.nj; jt += NT) {
+            const int nt = min(NT, T.nj - jt);
+            const int nt4 = (nt + 3) & ~3;
+            __syncthreads();
+            if ((int)threadIdx.x < nt4) {
+                const bool real = (int)threadIdx.x < nt;
+                const int jk = T.j0 + jt + (real ? (int)threadIdx.x : 0);
+                const int jj = A.jidx ? __ldg(A.jidx + jk) : jk;
+                const float4 J = A.jpos[jj];
+                sa->x[threadIdx.x] = J.x;
+                sa->y[threadIdx.x] = J.y;
+                sa->z[threadIdx.x] = J.z;
+                sa->m[threadIdx.x] = real ? J.w : 0.0f;
+                if constexpr (KIND == G5_QUAD) {
+                    const float4 Q0 = A.jaux[2 * jj], Q1 = A.jaux[2 * jj + 1];
+                    const float f = real ? -1.0f : 0.0f;
+                    sa->q[0][threadIdx.x] = f * Q0.x;
+                    sa->q[1][threadIdx.x] = f * Q0.y;
+                    sa->q[2][threadIdx.x] = f * Q0.z;
+                    sa->q[3][threadIdx.x] = f * Q0.w;
+                    sa->q[4][threadIdx.x] = f * Q1.x;
+                    sa->q[5][threadIdx.x] = f * Q1.y;
+                }
+            }
+            __syncthreads();
+            for (int jb = 0; jb < nt4; jb += G5_FOLD * nl) {
+            const int je = min(jb + G5_FOLD * nl, nt4);
+            float2 a2[KM][4];
+#pragma unroll
+            for (int k = 0; k < KM; k++) a2[k][0] = a2[k][1] = a2[k][2] = a2[k][3] = make_float2(0.f, 0.f);
+            for (int j = jb + 4 * lane; j < je; j += 4 * nl) {
+                const float4 X = *reinterpret_cast<const float4*>(&sa->x[j]);
+                const float4 Y = *reinterpret_cast<const float4*>(&sa->y[j]);
+                const float4 Z = *reinterpret_cast<const float4*>(&sa->z[j]);
+                const float4 M = *reinterpret_cast<const float4*>(&sa->m[j]);
+                if constexpr (KIND == G5_QUAD) {
+                    float4 Qv[6];
+#pragma unroll
+                    for (int c = 0; c < 6; c++) Qv[c] = *reinterpret_cast<const float4*>(&sa->q[c][j]);
+                    float2 Qa[6], Qb[6];
+#pragma unroll
+                    for (int c = 0; c < 6; c++) {
+                        Qa[c] = make_float2(Qv[c].x, Qv[c].y);
+                        Qb[c] = make_float2(Qv[c].z, Qv[c].w);
+                    }
+#pragma unroll
+                    for (int k = 0; k < KM; k++) {
+                        if (k < nik) {
+                            g5_quad_jpair(make_float2(X.x, X.y), make_float2(Y.x, Y.y), make_float2(Z.x, Z.y),
+                                          make_float2(M.x, M.y), Qa, nx[k], ny[k], nz[k], ei[k], a2[k]);
+                            g5_quad_jpair(make_float2(X.z, X.w), make_float2(Y.z, Y.w), make_float2(Z.z, Z.w),
+                                          make_float2(M.z, M.w), Qb, nx[k], ny[k], nz[k], ei[k], a2[k]);
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int k = 0; k < KM; k++) {
+                        if (k < nik) {
+                            g5_newton_jpair(make_float2(X.x, X.y), make_float2(Y.x, Y.y), make_float2(Z.x, Z.y),
+                                            make_float2(M.x, M.y), nx[k], ny[k], nz[k], ei[k], a2[k]);
+                            g5_newton_jpair(make_float2(X.z, X.w), make_float2(Y.z, Y.w), make_float2(Z.z, Z.w),
+                                            make_float2(M.z, M.w), nx[k], ny[k], nz[k], ei[k], a2[k]);
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < KM; k++)
+#pragma unroll
+                for (int c = 0; c < 4; c++) S[k][c] = S[k][c] + (double)a2[k][c].x + (double)a2[k][c].y;
+            }
+        }
+        // lane sums in lane order, one i per round through the j-tile buffer
+        double4* red = reinterpret_cast<double4*>(sj);
+#pragma unroll
+        for (int k = 0; k < KM; k++) {
+            if (k < nik && nl > 1) {
+                __syncthreads();
+                red[threadIdx.x] = make_double4(S[k][0], S[k][1], S[k][2], S[k][3]);
+                __syncthreads();
+                if (lane == 0) {
+                    for (int l = 1; l < nl; l++) {
+                        const double4 v = red[slot + l * isl];
+                        S[k][0] += v.x;
+                        S[k][1] += v.y;
+                        S[k][2] += v.z;
+                        S[k][3] += v.w;
+                    }
+                }
+            }
+        }
+        if (lane != 0) return;
+#pragma unroll
+        for (int k = 0; k < KM; k++) {
+            const int li = slot + k * isl;
+            if (k >= nik || li >= T.ni) continue;
+            const double4 v = make_double4(S[k][0], S[k][1], S[k][2], S[k][3]);
+            if (T.group < 0) A.out[T.i0 + li] = g5_finish<KIND>(v, A.ascale);
+            else A.partial[(size_t)T.slot * A.itile + li] = v;
+        }
+    };
+
     // The last CTA to finish a task of a split group reduces the group's partial rows.
     auto group_done = [&](const Task& T) {
         const Group G = A.groups[T.group];
@@ -365,6 +585,11 @@ __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
         int t = next_task(A.task_counter, &s_task, A.ntasks, first);
         if (t >= A.ntasks) break;
         const Task T = A.tasks[t];
+        if constexpr (USE_JP) {
+            jp_task(T);
+            if (T.group >= 0) group_done(T);
+            continue;
+        }
         if constexpr (LANES) {
             if (T.ni > NT / 2) {
                 lanes_pair_task(T);

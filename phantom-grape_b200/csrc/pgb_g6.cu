@@ -87,14 +87,14 @@ bool ensure_device() {
 
 enum Cfg {
     CFG_SMALL = 0, CFG_MED = 1, CFG_LARGE = 2, CFG_128x1 = 3, CFG_128x4 = 4, CFG_256x2 = 5,
-    CFG_128x2J = 6, CFG_256x2J = 7, NCFG = 8
+    CFG_128x2J = 6, CFG_256x2J = 7, CFG_128x4J = 8, NCFG = 9
 };
-constexpr int CFG_NT[NCFG] = {512, 256, 128, 128, 128, 256, 128, 256};
-constexpr int CFG_IPT[NCFG] = {1, 1, 2, 1, 4, 2, 2, 2};
-constexpr int CFG_JL[NCFG] = {8, 2, 1, 1, 1, 1, 1, 1};
+constexpr int CFG_NT[NCFG] = {512, 256, 128, 128, 128, 256, 128, 256, 128};
+constexpr int CFG_IPT[NCFG] = {1, 1, 2, 1, 4, 2, 2, 2, 4};
+constexpr int CFG_JL[NCFG] = {8, 2, 1, 1, 1, 1, 1, 1, 1};
 // j-paired form (g6_jpair): used with double-float positions and without neighbour lists; the
 // other variants of these configurations run the i-paired form
-constexpr bool CFG_JP[NCFG] = {false, false, false, false, false, false, true, true};
+constexpr bool CFG_JP[NCFG] = {false, false, false, false, false, false, true, true, true};
 inline int cfg_itile(int c) { return CFG_NT[c] / CFG_JL[c] * CFG_IPT[c]; }
 constexpr int ITILE_MAX = 512;
 
@@ -127,6 +127,7 @@ int occupancy_ff(int cfg, bool nn, bool nbl) {
         case CFG_256x2: return occ_of<256, 2, 1, FF>(nn, nbl);
         case CFG_128x2J: return occ_of<128, 2, 1, FF, true>(nn, nbl);
         case CFG_256x2J: return occ_of<256, 2, 1, FF, true>(nn, nbl);
+        case CFG_128x4J: return occ_of<128, 4, 1, FF, true>(nn, nbl);
         default: return occ_of<128, 2, 1, FF>(nn, nbl);
     }
 }
@@ -153,6 +154,7 @@ void launch_ff(int cfg, bool nn, bool nbl, int grid, const G6Args& a, cudaStream
         case CFG_256x2: launch_cfg<256, 2, 1, FF>(nn, nbl, grid, a, s); break;
         case CFG_128x2J: launch_cfg<128, 2, 1, FF, true>(nn, nbl, grid, a, s); break;
         case CFG_256x2J: launch_cfg<256, 2, 1, FF, true>(nn, nbl, grid, a, s); break;
+        case CFG_128x4J: launch_cfg<128, 4, 1, FF, true>(nn, nbl, grid, a, s); break;
         default: launch_cfg<128, 2, 1, FF>(nn, nbl, grid, a, s); break;
     }
 }

@@ -555,11 +555,12 @@ struct BoolC {
 };
 
 // Shared memory of a g6_kernel CTA: the j-tile (as records, or as field arrays in the j-paired
-// form, which also keeps its threads' FP64 sums there: 7 per i, two i per thread) and, after
-// the tile loop, NT G6Out for the lane and group reductions.
-template <int NT, bool JP>
+// form, which also keeps its threads' FP64 sums there: 7 per i) and, after the tile loop, NT
+// G6Out for the lane and group reductions.
+template <int NT, int IPT, bool JP>
 constexpr int g6_smem_bytes() {
-    return JP ? (int)((sizeof(G6TileSoA<NT>) + 15) / 16 * 16 + 14 * NT * sizeof(double)) : NT * (int)sizeof(G6Out);
+    return JP ? (int)((sizeof(G6TileSoA<NT>) + 15) / 16 * 16 + 7 * IPT * NT * sizeof(double))
+              : NT * (int)sizeof(G6Out);
 }
 
 // Thread layout of a CTA: NT threads = JL j-lanes x ISL i-slots (ISL = NT/JL, whole warps per
@@ -582,12 +583,12 @@ __device__ __forceinline__ void g6_task(const G6Args& A, const Task& T, unsigned
     static_assert(JL == 1 || IPT == 1, "j-lanes are used with one i per thread");
     constexpr int ISL = NT / JL;
     constexpr bool PAIRED = (IPT % 2 == 0);
-    constexpr bool USE_JP = JP && FF && !NBL && IPT == 2 && JL == 1;
+    constexpr bool USE_JP = JP && FF && !NBL && (IPT == 2 || IPT == 4) && JL == 1;
     constexpr bool TILEMIN = NN && !NBL && PAIRED;
     G6PredJ* sj = reinterpret_cast<G6PredJ*>(smem);
     G6TileSoA<NT>* sa = reinterpret_cast<G6TileSoA<NT>*>(smem);
     // j-paired form: the FP64 sums of thread t, i k, component c at Ssh[(k * 7 + c) * NT + t]
-    // (updated once per G6_FOLD j; kept out of the registers so that four CTAs fit an SM)
+    // (updated once per G6_FOLD j; kept out of the registers)
     double* Ssh = reinterpret_cast<double*>(smem + (sizeof(G6TileSoA<NT>) + 15) / 16 * 16);
     G6Out* red = reinterpret_cast<G6Out*>(smem);
     __shared__ int s_idr[2];
@@ -884,11 +885,22 @@ __device__ __forceinline__ void g6_task(const G6Args& A, const Task& T, unsigned
     }
 }
 
+// Resident CTAs an SM that the register budget must allow (the minBlocks of the launch bounds).
+// Measured on the largest Hermite call (128-thread CTAs): the i-paired form at <= 128 registers
+// (4 CTAs) takes 5.83 ms against 6.15 ms with ptxas's own choice of 104; the j-paired form at
+// <= 170 registers (3 CTAs, it uses 164) 5.78 ms against 6.03 ms capped at 128 (spills).
+template <int NT, int IPT, bool JPE>
+constexpr int g6_min_ctas() {
+    const int v = (IPT >= 4) ? 256 / NT : (JPE ? 384 / NT : 512 / NT);
+    return v > 0 ? v : 1;
+}
+
 template <int NT, int IPT, int JL, bool FF, bool NN, bool NBL, bool JP = false>
-__global__ void __launch_bounds__(NT, (JP && FF && !NBL) ? 512 / NT : 1) g6_kernel(const G6Args A) {
-    // j tile during the loop, per-thread results (G6Out) after it; the j-paired form is held to
-    // 128 registers a thread (512 threads an SM at least)
-    __shared__ __align__(16) unsigned char smem[g6_smem_bytes<NT, JP && FF && !NBL && IPT == 2 && JL == 1>()];
+__global__ void __launch_bounds__(NT, g6_min_ctas<NT, IPT, JP && FF && !NBL && (IPT == 2 || IPT == 4) && JL == 1>())
+    g6_kernel(const G6Args A) {
+    // j tile during the loop, per-thread results (G6Out) after it
+    __shared__ __align__(16) unsigned char
+        smem[g6_smem_bytes<NT, IPT, JP && FF && !NBL && (IPT == 2 || IPT == 4) && JL == 1>()];
     __shared__ int s_task, s_flag;
 
     for (bool first = true;; first = false) {

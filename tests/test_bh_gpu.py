@@ -104,7 +104,7 @@ def test_batched_index_lists_vs_fp64_same_lists(g5, bh):
 
 def test_every_configuration_gives_the_same_forces(g5, bh):
     ref_a, ref_p = batched(g5, bh)
-    for cp_, cc_ in ((0, 0), (1, 1), (2, 2), (3, 4), (4, 5), (5, 6), (6, 7), (7, 1)):
+    for cp_, cc_ in ((0, 0), (1, 1), (2, 2), (3, 4), (4, 5), (5, 6), (6, 7), (7, 1), (8, 8), (7, 8), (8, 7), (10, 10), (9, 8)):
         a, p = batched(g5, bh, cfg_p=cp_, cfg_c=cc_)
         assert rms(rel(a, ref_a)) <= 1e-6 and rms((p - ref_p) / ref_p) <= 1e-6, (cp_, cc_)
     a, p = batched(g5, bh, tune=True)
@@ -234,3 +234,12 @@ def test_graph_captured_plans_replay_and_update(g5):
     finally:
         g5.plan_destroy(pl_p)
         g5.plan_destroy(pl_c)
+
+
+def test_jpaired_configuration_vs_fp64_same_lists(g5, bh):
+    """The j-paired form (configuration 8) of both kinds on the tree's lists against FP64 on the
+    same lists (every group: ragged tiles, 1..4 j-lanes and two-i tiles all occur)."""
+    acc, phi = batched(g5, bh, cfg_p=8, cfg_c=8)
+    ra, rp, idx = fp64_lists(bh, range(bh.ngroups))
+    assert rms(rel(acc[idx], ra)) <= 1e-6, rms(rel(acc[idx], ra))
+    assert rms((phi[idx] - rp) / rp) <= 1e-6

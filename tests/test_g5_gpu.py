@@ -216,8 +216,9 @@ def test_batched_plan_matches_per_group_oracle(g5):
     d_o = torch.zeros((len(xi), 4), dtype=torch.float64, device=dev)
     plan = g5.plan_create(g5.NEWTON, items)
     try:
-        # every kernel configuration, each launched twice (the same plan gives the same answer)
-        for cfg in list(range(8)) * 2:
+        # every kernel configuration (8-10: the j-paired form), each launched twice (the same plan gives
+        # the same answer)
+        for cfg in list(range(11)) * 2:
             assert g5.L.pgb5_plan_set_config(plan, cfg) == 0 and g5.L.pgb5_plan_config(plan) == cfg
             d_o.zero_()
             g5.plan_launch(plan, d_i.data_ptr(), d_j.data_ptr(), None, d_o.data_ptr(),
@@ -236,6 +237,6 @@ def test_batched_plan_matches_per_group_oracle(g5):
                 np.testing.assert_allclose(-out[si, 3], po, rtol=2e-6)
         cfg, ms = g5.plan_tune(plan, d_i.data_ptr(), d_j.data_ptr(), None, d_o.data_ptr(),
                                torch.cuda.current_stream().cuda_stream)
-        assert 0 <= cfg < 8 and ms > 0 and g5.L.pgb5_plan_config(plan) == cfg
+        assert 0 <= cfg < 11 and ms > 0 and g5.L.pgb5_plan_config(plan) == cfg
     finally:
         g5.plan_destroy(plan)
