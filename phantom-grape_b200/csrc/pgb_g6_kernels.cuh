@@ -885,14 +885,14 @@ __device__ __forceinline__ void g6_task(const G6Args& A, const Task& T, unsigned
     }
 }
 
-// Resident CTAs an SM that the register budget must allow (the minBlocks of the launch bounds).
-// Measured on the largest Hermite call (128-thread CTAs): the i-paired form at <= 128 registers
-// (4 CTAs) takes 5.83 ms against 6.15 ms with ptxas's own choice of 104; the j-paired form at
-// <= 170 registers (3 CTAs, it uses 164) 5.78 ms against 6.03 ms capped at 128 (spills).
+// The minBlocks of the launch bounds (0: unstated, ptxas's own register choice).  Measured on
+// the largest Hermite call (128-thread CTAs), with run-to-run spread of about 1 %: the i-paired
+// form takes 5.83 ms with minBlocks 1 (ptxas then uses 128 registers), 6.15 ms unstated (104)
+// and 6.09 ms with 4 (123); the j-paired form 5.78 ms unstated (164 registers), 5.91 ms with 3
+// (166) and 6.03 ms capped at 128 (spills).  Four i per thread is slower in both forms (6.55 ms).
 template <int NT, int IPT, bool JPE>
 constexpr int g6_min_ctas() {
-    const int v = (IPT >= 4) ? 256 / NT : (JPE ? 384 / NT : 512 / NT);
-    return v > 0 ? v : 1;
+    return (!JPE && IPT == 2) ? (NT <= 128 ? 1 : 512 / NT) : 0;   // 256 threads: <= 128 registers, 2 CTAs
 }
 
 template <int NT, int IPT, int JL, bool FF, bool NN, bool NBL, bool JP = false>
