@@ -123,6 +123,14 @@ def pipe_peaks(pgb, stream_ptr=0):
     clk = clocks.stop()
     if rc1 == 0:
         _PIPE_PEAKS.update({"fp32_tflops": round(tf.value, 2), "fp32_ms": round(ms.value, 3), "fp32_ctas": g.value})
+    L.pgb_peak_fp32_mix.argtypes = [C.c_int, C.c_int, C.c_void_p, dp, dp]
+    mix = {}
+    for kind, name in ((0, "ffma2_only"), (1, "ffma2_ffma_1to2"), (2, "ffma2_ffma_1to6")):
+        t2, m2 = C.c_double(), C.c_double()
+        if L.pgb_peak_fp32_mix(kind, 20000, C.c_void_p(stream_ptr), C.byref(t2), C.byref(m2)) == 0:
+            mix[name] = round(t2.value, 2)
+    if mix:
+        _PIPE_PEAKS["fp32_mix_tflops"] = mix
     if rc2 == 0:
         _PIPE_PEAKS.update({"mufu_grsqrt_s": round(mg.value, 1), "mufu_ms": round(mms.value, 3),
                             "mufu_per_sm_clk": round(mg.value * 1e9 / SM_COUNT / ((clk.get("sm_mhz") or 1965.0) * 1e6), 2)})
@@ -473,6 +481,9 @@ def hermite_batched(args, pgb, g6, wl, sub, calls, dev, s, ff, tune, steps, warm
         clocks.start()
     barrier(ws)
     torch.cuda.synchronize()
+    # the timed steps inside an NVTX range, so that a profiler's launch list can select them
+    # (ncu --nvtx --nvtx-include "pgb_timed_steps/")
+    torch.cuda.nvtx.range_push("pgb_timed_steps")
     with torch.cuda.stream(s):
         for k in range(steps):
             ev[k][0].record(s)
@@ -480,6 +491,7 @@ def hermite_batched(args, pgb, g6, wl, sub, calls, dev, s, ff, tune, steps, warm
             ev[k][1].record(s)
             flush.fill_(k & 0xFF)   # 256 MiB write between steps: L2 (126 MB) flushed
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
     barrier(ws)
     clk = clocks.stop() if clocks else {}
     step_ms = [a.elapsed_time(b) for a, b in ev]
@@ -704,7 +716,8 @@ def run_hermite(args, pgb, ws, rank, local):
                      "achieved_all_launches": round(achieved_all_tf, 2),
                      "peak_source": peak_src, "peak_nominal": round(fp32_nominal, 2),
                      "mufu_peak_grsqrt_s": _PIPE_PEAKS.get("mufu_grsqrt_s"),
-                     "mufu_per_sm_clk": _PIPE_PEAKS.get("mufu_per_sm_clk")},
+                     "mufu_per_sm_clk": _PIPE_PEAKS.get("mufu_per_sm_clk"),
+                     "fp32_mix_tflops": _PIPE_PEAKS.get("fp32_mix_tflops")},
         "e2e": {"value": round(e2e_val, 2), "unit": "Gint/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "api": "GRAPE-6 drop-in (g6_set_ti, g6calc_firsthalf, "
                 "g6calc_lasthalf2p per npipes chunk, g6_set_j_particle of the active set), host buffers",

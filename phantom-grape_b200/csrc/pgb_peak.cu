@@ -36,6 +36,35 @@ __global__ void __launch_bounds__(PEAK_THREADS) ffma_kernel(float* out, int iter
     out[blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
+// FP32 work issued as paired (FFMA2) and scalar (FFMA) instructions in the ratio P : S per
+// step, on independent chains: the FMA pipe's throughput for the instruction mixes of the force
+// kernels (j-paired Hermite 9 : 18, i-paired 4.5 : 27); 4 flop per FFMA2, 2 per FFMA.
+template <int P, int S>
+__global__ void __launch_bounds__(PEAK_THREADS) mix_kernel(float* out, int iters, float a, float b) {
+    float2 x2[P > 0 ? P : 1];
+    float x[S > 0 ? S : 1];
+#pragma unroll
+    for (int c = 0; c < P; c++) x2[c] = make_float2((float)(threadIdx.x + c) * 1e-3f, (float)c * 1e-3f);
+#pragma unroll
+    for (int c = 0; c < S; c++) x[c] = (float)(threadIdx.x + 2 * c) * 1e-3f;
+    const float2 a2 = make_float2(a, a), b2 = make_float2(b, b);
+    for (int k = 0; k < iters; k++) {
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+#pragma unroll
+            for (int c = 0; c < P; c++) x2[c] = __ffma2_rn(x2[c], a2, b2);
+#pragma unroll
+            for (int c = 0; c < S; c++) x[c] = __fmaf_rn(x[c], a, b);
+        }
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int c = 0; c < P; c++) s += x2[c].x + x2[c].y;
+#pragma unroll
+    for (int c = 0; c < S; c++) s += x[c];
+    out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
 __device__ __forceinline__ float rsqrt_approx(float x) {
     float y;
     asm volatile("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
@@ -126,5 +155,31 @@ PGB_EXPORT int pgb_peak_mufu(int iters, void* stream, double* gops, double* ms, 
     if (gops) *gops = ops / (t * 1e-3) / 1e9;
     if (ms) *ms = t;
     if (blocks) *blocks = grid;
+    return 0;
+}
+
+// FP32 throughput (TFLOP/s) of a paired : scalar instruction mix, kind 0: paired only (8 FFMA2
+// chains), 1: 4 FFMA2 : 8 FFMA (the j-paired Hermite form's 1 : 2), 2: 2 FFMA2 : 12 FFMA (the
+// i-paired form's 1 : 6).
+PGB_EXPORT int pgb_peak_fp32_mix(int kind, int iters, void* stream, double* tflops, double* ms) {
+    cudaStream_t s = (cudaStream_t)stream;
+    const void* fn = kind == 0 ? (const void*)mix_kernel<8, 0> : kind == 1 ? (const void*)mix_kernel<4, 8>
+                                                                            : (const void*)mix_kernel<2, 12>;
+    const int grid = grid_blocks(fn);
+    float* out = nullptr;
+    if (cudaMalloc(&out, (size_t)grid * PEAK_THREADS * sizeof(float)) != cudaSuccess) return -1;
+    float t = best_ms(
+        [&] {
+            if (kind == 0) mix_kernel<8, 0><<<grid, PEAK_THREADS, 0, s>>>(out, iters, 0.999f, 1e-3f);
+            else if (kind == 1) mix_kernel<4, 8><<<grid, PEAK_THREADS, 0, s>>>(out, iters, 0.999f, 1e-3f);
+            else mix_kernel<2, 12><<<grid, PEAK_THREADS, 0, s>>>(out, iters, 0.999f, 1e-3f);
+        },
+        5, s);
+    cudaFree(out);
+    if (t <= 0.f) return -1;
+    const int P = kind == 0 ? 8 : kind == 1 ? 4 : 2, S = kind == 0 ? 0 : kind == 1 ? 8 : 12;
+    const double flops = (double)grid * PEAK_THREADS * (double)iters * 8 * (4.0 * P + 2.0 * S);
+    if (tflops) *tflops = flops / (t * 1e-3) / 1e12;
+    if (ms) *ms = t;
     return 0;
 }
