@@ -53,11 +53,16 @@ SM_COUNT = 148
 REF_SRC = os.environ.get("PGB_REFERENCE", "/root/reference")
 # DRAM bytes (read + write) of one launch of the roofline kernel, from the committed ncu captures
 # (dram__bytes_read.sum + dram__bytes_write.sum); the bench cannot run ncu itself.
+G6_CFG_NAMES = ["512x1 (8 j-lanes)", "256x1 (2 j-lanes)", "128x2 i-paired", "128x1", "128x4 i-paired",
+                "256x2 i-paired", "128x2 j-paired", "256x2 j-paired", "128x4 j-paired"]   # pgb6 configurations
 G5_CFG_NAMES = ["128x4", "256x2", "512x2", "1024x1", "384x2", "128x2", "128x1", "64x1", "64x1 j-paired",
                 "1024x1 j-paired", "256x1 j-paired"]   # pgb5 configurations (threads x i/thread)
 PROFILED_TRAFFIC = {
-    "hermite": {"bytes": 6_485_760 + 17_935_104,
-                "source": "profiles/g6_kernel_hermite_65536x65536.md (128x2 configuration, paired accumulations)"},
+    # the largest Hermite call by the configuration that runs it (6: 128x2 j-paired, 2: 128x2 i-paired)
+    "hermite": {"bytes": 6_471_168 + 3_581_696,
+                "source": "profiles/g6_kernel_hermite_65536x65536.md (128x2 j-paired)"},
+    "hermite_cfg2": {"bytes": 6_578_944 + 17_873_152,
+                     "source": "profiles/g6_kernel_hermite_65536x65536.md (128x2 i-paired)"},
     "direct": {"bytes": 542_720, "pairs": 268_435_456, "source": "profiles/g5_kernels_direct_treepm_bh.md (1024x1)"},
     "treepm": {"bytes": 557_901_056 + 35_891_456, "pairs": 4_463_983_086,
                "source": "profiles/g5_kernels_direct_treepm_bh.md (64x1)"},
@@ -595,6 +600,9 @@ def run_hermite(args, pgb, ws, rank, local):
     value = float(wl["pairs"]) * args.steps / t_max / 1e9      # the whole schedule per step
     fp32_tf, fp32_nominal, peak_src = fp32_peak(pgb, clk, s.cuda_stream)
     achieved_tf = B["big_pairs"] * 60 / (B["big_ms"] / 1e3) / 1e12
+    # DRAM traffic of the largest launch from the committed capture of the configuration it runs
+    big_cfg = g6.L.pgb6_plan_config(B["plans"][B["big_call"]])
+    tkey = ("hermite" if big_cfg == 6 else "hermite_cfg2" if big_cfg == 2 else None) if ff and ws == 1 else None
     achieved_all_tf = B["kern_pairs"] * 60 / B["kern_s"] / 1e12
 
     # the batched path end to end with host buffers: every step copies the j-memory and the
@@ -709,10 +717,11 @@ def run_hermite(args, pgb, ws, rank, local):
         "frac_fp32": round(value * 1e9 * 60 / 1e12 / fp32_tf, 4),
         "roofline": {"bound": "fp32", "achieved": round(achieved_tf, 2), "peak": round(fp32_tf, 2),
                      "unit": "TFLOP/s", "frac": round(achieved_tf / fp32_tf, 4),
-                     "traffic": PROFILED_TRAFFIC["hermite"]["bytes"] if ff else None,
-                     "traffic_source": PROFILED_TRAFFIC["hermite"]["source"] if ff else None,
-                     "kernel": "pgb::g6_kernel (autotuned configuration), largest call of the step "
-                               f"({B['big_pairs']:.3e} pairs, {B['big_ms']:.3f} ms)",
+                     "traffic": PROFILED_TRAFFIC[tkey]["bytes"] if tkey else None,
+                     "traffic_source": PROFILED_TRAFFIC[tkey]["source"] if tkey else None,
+                     "kernel": f"pgb::g6_kernel (autotuned configuration {big_cfg}: "
+                               f"{G6_CFG_NAMES[big_cfg] if 0 <= big_cfg < len(G6_CFG_NAMES) else '?'}), largest "
+                               f"call of the step ({B['big_pairs']:.3e} pairs, {B['big_ms']:.3f} ms)",
                      "achieved_all_launches": round(achieved_all_tf, 2),
                      "peak_source": peak_src, "peak_nominal": round(fp32_nominal, 2),
                      "mufu_peak_grsqrt_s": _PIPE_PEAKS.get("mufu_grsqrt_s"),
