@@ -399,6 +399,74 @@ __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
         }
     };
 
+    // Tasks of 33..48 i in the 64-thread CTAs: three i per thread (slot, slot + 16, slot + 32)
+    // over four j-lanes, so that such a task occupies 48 i-slots instead of the pair layout's 64
+    // (tree-code groups of 33..63 i leave a third of those idle); each lane's records are read
+    // once for its three i.  The lanes' sums are added in lane order.
+    auto lanes_triple_task = [&](const Task& T) {
+        constexpr int H = NT / 4;
+        const int slot = (int)threadIdx.x % H, lane = (int)threadIdx.x / H;
+        float xi[3], yi[3], zi[3], ei[3];
+        double S[3][4];
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const int li = slot + k * H;
+            const float4 p = A.ipos[T.i0 + (li < T.ni ? li : 0)];
+            xi[k] = p.x; yi[k] = p.y; zi[k] = p.z; ei[k] = p.w;
+            S[k][0] = S[k][1] = S[k][2] = S[k][3] = 0.0;
+        }
+        for (int jt = 0; jt < T.nj; jt += NT) {
+            const int nt = min(NT, T.nj - jt);
+            __syncthreads();
+            if (threadIdx.x < nt) {
+                const int jk = T.j0 + jt + threadIdx.x;
+                const int jj = A.jidx ? __ldg(A.jidx + jk) : jk;
+                sj[threadIdx.x] = A.jpos[jj];
+                if constexpr (W == 2) sj[NT + threadIdx.x] = A.jaux[jj];
+                if constexpr (W == 3) {
+                    sj[NT + 2 * threadIdx.x] = A.jaux[2 * jj];
+                    sj[NT + 2 * threadIdx.x + 1] = A.jaux[2 * jj + 1];
+                }
+            }
+            __syncthreads();
+            // one block: a lane sees at most NT/4 <= G5_FOLD records of a tile
+            float a[3][4];
+#pragma unroll
+            for (int k = 0; k < 3; k++) a[k][0] = a[k][1] = a[k][2] = a[k][3] = 0.f;
+            g5_jloop<KIND, NT, 3, 4>(sj, lane, nt, xi, yi, zi, ei, tab, shift, A.r2cut, a);
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+#pragma unroll
+                for (int c = 0; c < 4; c++) S[k][c] += (double)a[k][c];
+            }
+        }
+        double4* red = reinterpret_cast<double4*>(sj);
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            __syncthreads();
+            red[threadIdx.x] = make_double4(S[k][0], S[k][1], S[k][2], S[k][3]);
+            __syncthreads();
+            if (lane == 0) {
+                for (int l = 1; l < 4; l++) {
+                    const double4 v = red[slot + l * H];
+                    S[k][0] += v.x;
+                    S[k][1] += v.y;
+                    S[k][2] += v.z;
+                    S[k][3] += v.w;
+                }
+            }
+        }
+        if (lane != 0) return;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const int li = slot + k * H;
+            if (li >= T.ni) continue;
+            const double4 v = make_double4(S[k][0], S[k][1], S[k][2], S[k][3]);
+            if (T.group < 0) A.out[T.i0 + li] = g5_finish<KIND>(v, A.ascale);
+            else A.partial[(size_t)T.slot * A.itile + li] = v;
+        }
+    };
+
     // The j-paired task (USE_JP).  In the 64-thread CTAs a task of more than NT/2 i runs two i
     // per thread (slot and slot + NT/2) over two j-lanes, a smaller one one i per thread over
     // nl = NT / isl lanes (isl = ni rounded up to 16, as the other form); lane l takes the tile's
@@ -591,6 +659,11 @@ __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
             continue;
         }
         if constexpr (LANES) {
+            if (NT == 64 && T.ni > NT / 2 && T.ni <= 3 * NT / 4) {
+                lanes_triple_task(T);
+                if (T.group >= 0) group_done(T);
+                continue;
+            }
             if (T.ni > NT / 2) {
                 lanes_pair_task(T);
                 if (T.group >= 0) group_done(T);

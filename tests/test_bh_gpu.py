@@ -236,10 +236,15 @@ def test_graph_captured_plans_replay_and_update(g5):
         g5.plan_destroy(pl_c)
 
 
-def test_jpaired_configuration_vs_fp64_same_lists(g5, bh):
-    """The j-paired form (configuration 8) of both kinds on the tree's lists against FP64 on the
-    same lists (every group: ragged tiles, 1..4 j-lanes and two-i tiles all occur)."""
-    acc, phi = batched(g5, bh, cfg_p=8, cfg_c=8)
+@pytest.mark.parametrize("cfg", [7, 8])
+def test_64_thread_configurations_vs_fp64_same_lists(g5, bh, cfg):
+    """The 64-thread CTAs of both kinds -- 7: one, two or three i per thread by the task's size
+    (j-lanes for tasks of <= 32 i, 3 i x 4 lanes for 33..48, 2 i x 2 lanes above), 8: the
+    j-paired form -- on the tree's lists against FP64 on the same lists, every group (ragged
+    tiles and every task layout occur)."""
+    acc, phi = batched(g5, bh, cfg_p=cfg, cfg_c=cfg)
     ra, rp, idx = fp64_lists(bh, range(bh.ngroups))
     assert rms(rel(acc[idx], ra)) <= 1e-6, rms(rel(acc[idx], ra))
     assert rms((phi[idx] - rp) / rp) <= 1e-6
+    sizes = np.asarray(bh.gcount) % 64
+    assert np.any((sizes > 32) & (sizes <= 48)) and np.any((sizes > 0) & (sizes <= 32)) and np.any(sizes > 48)
