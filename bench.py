@@ -54,7 +54,8 @@ REF_SRC = os.environ.get("PGB_REFERENCE", "/root/reference")
 # DRAM bytes (read + write) of one launch of the roofline kernel, from the committed ncu captures
 # (dram__bytes_read.sum + dram__bytes_write.sum); the bench cannot run ncu itself.
 G6_CFG_NAMES = ["512x1 (8 j-lanes)", "256x1 (2 j-lanes)", "128x2 i-paired", "128x1", "128x4 i-paired",
-                "256x2 i-paired", "128x2 j-paired", "256x2 j-paired", "128x4 j-paired"]   # pgb6 configurations
+                "256x2 i-paired", "128x2 j-paired", "256x2 j-paired", "128x4 j-paired",
+                "128x2 j-paired stage-ordered"]   # pgb6 configurations
 G5_CFG_NAMES = ["128x4", "256x2", "512x2", "1024x1", "384x2", "128x2", "128x1", "64x1", "64x1 j-paired",
                 "1024x1 j-paired", "256x1 j-paired"]   # pgb5 configurations (threads x i/thread)
 PROFILED_TRAFFIC = {
@@ -602,7 +603,8 @@ def run_hermite(args, pgb, ws, rank, local):
     achieved_tf = B["big_pairs"] * 60 / (B["big_ms"] / 1e3) / 1e12
     # DRAM traffic of the largest launch from the committed capture of the configuration it runs
     big_cfg = g6.L.pgb6_plan_config(B["plans"][B["big_call"]])
-    tkey = ("hermite" if big_cfg == 6 else "hermite_cfg2" if big_cfg == 2 else None) if ff and ws == 1 else None
+    tkey = ({6: "hermite", 9: "hermite_cfg9", 2: "hermite_cfg2"}.get(big_cfg)) if ff and ws == 1 else None
+    tkey = tkey if tkey in PROFILED_TRAFFIC else None
     achieved_all_tf = B["kern_pairs"] * 60 / B["kern_s"] / 1e12
 
     # the batched path end to end with host buffers: every step copies the j-memory and the
@@ -660,8 +662,8 @@ def run_hermite(args, pgb, ws, rank, local):
     g6.L.pgb6_set_call_timing(1)
     sec_t, _, _ = drv.g6_schedule(h, sub, resend_sets=rs)
     g6.L.pgb6_set_call_timing(0)
-    plain_dev_s = g6.L.pgb6_call_device_ms(1) / 1e3
-    plain_dev = float(sub["pairs"]) / plain_dev_s / 1e9 if plain_dev_s > 0 else None
+    plain_dev_s = reduce_max(g6.L.pgb6_call_device_ms(1) / 1e3, ws, dev)
+    plain_dev = float(wl["pairs"]) / plain_dev_s / 1e9 if plain_dev_s > 0 else None
     npipe = g6.L.g6_npipes()
     nact = len(sub["set_idx"])
     nchunks = sum((len(x) + npipe - 1) // npipe for x in sub["sets"])

@@ -87,18 +87,18 @@ bool ensure_device() {
 
 enum Cfg {
     CFG_SMALL = 0, CFG_MED = 1, CFG_LARGE = 2, CFG_128x1 = 3, CFG_128x4 = 4, CFG_256x2 = 5,
-    CFG_128x2J = 6, CFG_256x2J = 7, CFG_128x4J = 8, NCFG = 9
+    CFG_128x2J = 6, CFG_256x2J = 7, CFG_128x4J = 8, CFG_128x2JS = 9, NCFG = 10
 };
-constexpr int CFG_NT[NCFG] = {512, 256, 128, 128, 128, 256, 128, 256, 128};
-constexpr int CFG_IPT[NCFG] = {1, 1, 2, 1, 4, 2, 2, 2, 4};
-constexpr int CFG_JL[NCFG] = {8, 2, 1, 1, 1, 1, 1, 1, 1};
-// j-paired form (g6_jpair): used with double-float positions and without neighbour lists; the
-// other variants of these configurations run the i-paired form
-constexpr bool CFG_JP[NCFG] = {false, false, false, false, false, false, true, true, true};
+constexpr int CFG_NT[NCFG] = {512, 256, 128, 128, 128, 256, 128, 256, 128, 128};
+constexpr int CFG_IPT[NCFG] = {1, 1, 2, 1, 4, 2, 2, 2, 4, 2};
+constexpr int CFG_JL[NCFG] = {8, 2, 1, 1, 1, 1, 1, 1, 1, 1};
+// j-paired form (1: g6_jpair, 2: stage-ordered g6_jquad2): used with double-float positions and
+// without neighbour lists; the other variants of these configurations run the i-paired form
+constexpr int CFG_JP[NCFG] = {0, 0, 0, 0, 0, 0, 1, 1, 1, 2};
 inline int cfg_itile(int c) { return CFG_NT[c] / CFG_JL[c] * CFG_IPT[c]; }
 constexpr int ITILE_MAX = 512;
 
-template <int NT, int IPT, int JL, bool FF, bool JP = false>
+template <int NT, int IPT, int JL, bool FF, int JP = 0>
 int occ_of(bool nn, bool nbl) {
     static int v[4] = {0, 0, 0, 0};
     int k = (nn ? 1 : 0) + (nbl ? 2 : 0);
@@ -125,9 +125,10 @@ int occupancy_ff(int cfg, bool nn, bool nbl) {
         case CFG_128x1: return occ_of<128, 1, 1, FF>(nn, nbl);
         case CFG_128x4: return occ_of<128, 4, 1, FF>(nn, nbl);
         case CFG_256x2: return occ_of<256, 2, 1, FF>(nn, nbl);
-        case CFG_128x2J: return occ_of<128, 2, 1, FF, true>(nn, nbl);
-        case CFG_256x2J: return occ_of<256, 2, 1, FF, true>(nn, nbl);
-        case CFG_128x4J: return occ_of<128, 4, 1, FF, true>(nn, nbl);
+        case CFG_128x2J: return occ_of<128, 2, 1, FF, 1>(nn, nbl);
+        case CFG_256x2J: return occ_of<256, 2, 1, FF, 1>(nn, nbl);
+        case CFG_128x4J: return occ_of<128, 4, 1, FF, 1>(nn, nbl);
+        case CFG_128x2JS: return occ_of<128, 2, 1, FF, 2>(nn, nbl);
         default: return occ_of<128, 2, 1, FF>(nn, nbl);
     }
 }
@@ -136,7 +137,7 @@ int occupancy(int cfg, bool ff, bool nn, bool nbl) {
     return ff ? occupancy_ff<true>(cfg, nn, nbl) : occupancy_ff<false>(cfg, nn, nbl);
 }
 
-template <int NT, int IPT, int JL, bool FF, bool JP = false>
+template <int NT, int IPT, int JL, bool FF, int JP = 0>
 void launch_cfg(bool nn, bool nbl, int grid, const G6Args& a, cudaStream_t s) {
     if (nn && nbl) g6_kernel<NT, IPT, JL, FF, true, true, JP><<<grid, NT, 0, s>>>(a);
     else if (nn) g6_kernel<NT, IPT, JL, FF, true, false, JP><<<grid, NT, 0, s>>>(a);
@@ -152,9 +153,10 @@ void launch_ff(int cfg, bool nn, bool nbl, int grid, const G6Args& a, cudaStream
         case CFG_128x1: launch_cfg<128, 1, 1, FF>(nn, nbl, grid, a, s); break;
         case CFG_128x4: launch_cfg<128, 4, 1, FF>(nn, nbl, grid, a, s); break;
         case CFG_256x2: launch_cfg<256, 2, 1, FF>(nn, nbl, grid, a, s); break;
-        case CFG_128x2J: launch_cfg<128, 2, 1, FF, true>(nn, nbl, grid, a, s); break;
-        case CFG_256x2J: launch_cfg<256, 2, 1, FF, true>(nn, nbl, grid, a, s); break;
-        case CFG_128x4J: launch_cfg<128, 4, 1, FF, true>(nn, nbl, grid, a, s); break;
+        case CFG_128x2J: launch_cfg<128, 2, 1, FF, 1>(nn, nbl, grid, a, s); break;
+        case CFG_256x2J: launch_cfg<256, 2, 1, FF, 1>(nn, nbl, grid, a, s); break;
+        case CFG_128x4J: launch_cfg<128, 4, 1, FF, 1>(nn, nbl, grid, a, s); break;
+        case CFG_128x2JS: launch_cfg<128, 2, 1, FF, 2>(nn, nbl, grid, a, s); break;
         default: launch_cfg<128, 2, 1, FF>(nn, nbl, grid, a, s); break;
     }
 }

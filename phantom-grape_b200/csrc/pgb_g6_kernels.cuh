@@ -401,6 +401,82 @@ __device__ __forceinline__ void g6_jpair(float2 xh, float2 yh, float2 zh, float2
     a.jz = __ffma2_rn(mq3, __ffma2_rn(c, dz, dvz), a.jz);
 }
 
+// The j-paired form for two i, stage-ordered: the four j-pair chains of a j-quad (two i x two
+// j-pairs) advanced together stage by stage -- relative coordinates, dv and r^2, the eight
+// rsqrt, the Newton steps and scalar factors, the accumulations -- which hands the scheduler
+// independent work in every stage (largest Hermite call 5.65 against 5.77 ms for the chain-by-
+// chain order of g6_jpair; the autotuner chooses between them per call size).  The same
+// operations as g6_jpair on the same values: bit-identical results.
+template <bool NN, bool SELF>
+__device__ __forceinline__ void g6_jquad2(const float4& XH, const float4& YH, const float4& ZH, const float4& XL,
+                                          const float4& YL, const float4& ZL, const float4& M, const float4& VX,
+                                          const float4& VY, const float4& VZ, const int4& ID, const G6IPair* IP,
+                                          float eps2, G6Acc2* a, float* tmin) {
+    float2 dx[4], dy[4], dz[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        const G6IPair& I = IP[c >> 1];
+        const bool hi = c & 1;
+        const float2 xh = hi ? make_float2(XH.z, XH.w) : make_float2(XH.x, XH.y);
+        const float2 yh = hi ? make_float2(YH.z, YH.w) : make_float2(YH.x, YH.y);
+        const float2 zh = hi ? make_float2(ZH.z, ZH.w) : make_float2(ZH.x, ZH.y);
+        const float2 xl = hi ? make_float2(XL.z, XL.w) : make_float2(XL.x, XL.y);
+        const float2 yl = hi ? make_float2(YL.z, YL.w) : make_float2(YL.x, YL.y);
+        const float2 zl = hi ? make_float2(ZL.z, ZL.w) : make_float2(ZL.x, ZL.y);
+        dx[c] = __fadd2_rn(__fadd2_rn(xh, I.nxh), __fadd2_rn(xl, I.nxl));
+        dy[c] = __fadd2_rn(__fadd2_rn(yh, I.nyh), __fadd2_rn(yl, I.nyl));
+        dz[c] = __fadd2_rn(__fadd2_rn(zh, I.nzh), __fadd2_rn(zl, I.nzl));
+    }
+    const float vxs[4] = {VX.x, VX.y, VX.z, VX.w}, vys[4] = {VY.x, VY.y, VY.z, VY.w}, vzs[4] = {VZ.x, VZ.y, VZ.z, VZ.w};
+    const float ms[4] = {M.x, M.y, M.z, M.w};
+    const int ids[4] = {ID.x, ID.y, ID.z, ID.w};
+    float r2[8], dvx[8], dvy[8], dvz[8];
+#pragma unroll
+    for (int l = 0; l < 8; l++) {
+        const int c = l >> 1, h = l & 1;
+        const G6IPair& I = IP[c >> 1];
+        const int jj = ((c & 1) << 1) + h;
+        const float ddx = h ? dx[c].y : dx[c].x, ddy = h ? dy[c].y : dy[c].x, ddz = h ? dz[c].y : dz[c].x;
+        dvx[l] = vxs[jj] - I.vx;
+        dvy[l] = vys[jj] - I.vy;
+        dvz[l] = vzs[jj] - I.vz;
+        r2[l] = __fmaf_rn(ddz, ddz, __fmaf_rn(ddy, ddy, __fmaf_rn(ddx, ddx, eps2)));
+    }
+    float y[8];
+#pragma unroll
+    for (int l = 0; l < 8; l++) y[l] = mufu_rsqrt(r2[l]);
+    float mq3[8], cc[8];
+#pragma unroll
+    for (int l = 0; l < 8; l++) {
+        const int c = l >> 1, h = l & 1;
+        const G6IPair& I = IP[c >> 1];
+        const int jj = ((c & 1) << 1) + h;
+        const float t = __fmul_rn(r2[l], y[l]);
+        const float u = __fmaf_rn(t, y[l], -3.0f);
+        float q = __fmul_rn(u, y[l]);
+        if constexpr (SELF) q = (ids[jj] == I.id) ? 0.0f : q;
+        if constexpr (NN) tmin[c >> 1] = fminf(tmin[c >> 1], q);
+        a[c >> 1].pot[h] = __fmaf_rn(ms[jj], q, a[c >> 1].pot[h]);
+        const float ddx = h ? dx[c].y : dx[c].x, ddy = h ? dy[c].y : dy[c].x, ddz = h ? dz[c].y : dz[c].x;
+        const float rv = __fmaf_rn(ddz, dvz[l], __fmaf_rn(ddy, dvy[l], ddx * dvx[l]));
+        const float mq = ms[jj] * q;
+        const float q2 = q * q;
+        mq3[l] = mq * q2;
+        cc[l] = -0.75f * q2 * rv;
+    }
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        G6Acc2& A = a[c >> 1];
+        const float2 M3 = make_float2(mq3[2 * c], mq3[2 * c + 1]), C2 = make_float2(cc[2 * c], cc[2 * c + 1]);
+        A.ax = __ffma2_rn(M3, dx[c], A.ax);
+        A.ay = __ffma2_rn(M3, dy[c], A.ay);
+        A.az = __ffma2_rn(M3, dz[c], A.az);
+        A.jx = __ffma2_rn(M3, __ffma2_rn(C2, dx[c], make_float2(dvx[2 * c], dvx[2 * c + 1])), A.jx);
+        A.jy = __ffma2_rn(M3, __ffma2_rn(C2, dy[c], make_float2(dvy[2 * c], dvy[2 * c + 1])), A.jy);
+        A.jz = __ffma2_rn(M3, __ffma2_rn(C2, dz[c], make_float2(dvz[2 * c], dvz[2 * c + 1])), A.jz);
+    }
+}
+
 // The address of the first j of tile [jb, jb + ne) (every JL-th from lane jl) whose key equals
 // kmin -- the nearest neighbour found by a tile-minimum pass (see g6_pair).  The records are read
 // again from the predicted j-set (L2-resident).  Returns -1 if none matches, which cannot
@@ -576,9 +652,10 @@ constexpr int g6_smem_bytes() {
 // (a j id inside the i-tile's id range, one __syncthreads_or at the staging barrier); only such
 // tiles run the self-pair mask.  With two i per thread (IPT even) the nearest neighbour is
 // found as a tile minimum (see g6_pair) and its address recovered once per i and task by
-// g6_rescan.  JP selects the j-paired form (g6_jpair; double-float positions, no neighbour
-// lists, two i per thread, one j-lane); otherwise the j-tile is an array of G6PredJ records.
-template <int NT, int IPT, int JL, bool FF, bool NN, bool NBL, bool JP = false>
+// g6_rescan.  JP selects the j-paired form (1: g6_jpair, 2: g6_jquad2 for two i per thread;
+// double-float positions, no neighbour lists, one j-lane); otherwise the j-tile is an array of
+// G6PredJ records.
+template <int NT, int IPT, int JL, bool FF, bool NN, bool NBL, int JP = 0>
 __device__ __forceinline__ void g6_task(const G6Args& A, const Task& T, unsigned char* smem) {
     static_assert(JL == 1 || IPT == 1, "j-lanes are used with one i per thread");
     constexpr int ISL = NT / JL;
@@ -721,6 +798,9 @@ __device__ __forceinline__ void g6_task(const G6Args& A, const Task& T, unsigned
                         const float4 VZ = *reinterpret_cast<const float4*>(&sa->vz[j]);
                         int4 ID = make_int4(0, 0, 0, 0);
                         if constexpr (SELF) ID = *reinterpret_cast<const int4*>(&sa->id[j]);
+                        if constexpr (JP == 2 && IPT == 2) {
+                            g6_jquad2<NN, SELF>(XH, YH, ZH, XL, YL, ZL, M, VX, VY, VZ, ID, IP, A.eps2, a, tmin);
+                        } else {
 #pragma unroll
                         for (int k = 0; k < IPT; k++) {
                             g6_jpair<NN, SELF>(make_float2(XH.x, XH.y), make_float2(YH.x, YH.y),
@@ -735,6 +815,7 @@ __device__ __forceinline__ void g6_task(const G6Args& A, const Task& T, unsigned
                                                make_float2(M.z, M.w), make_float2(VX.z, VX.w),
                                                make_float2(VY.z, VY.w), make_float2(VZ.z, VZ.w),
                                                make_int2(ID.z, ID.w), IP[k], A.eps2, a[k], tmin[k]);
+                        }
                         }
                     }
 #pragma unroll
@@ -895,7 +976,7 @@ constexpr int g6_min_ctas() {
     return (!JPE && IPT == 2) ? (NT <= 128 ? 1 : 512 / NT) : 0;   // 256 threads: <= 128 registers, 2 CTAs
 }
 
-template <int NT, int IPT, int JL, bool FF, bool NN, bool NBL, bool JP = false>
+template <int NT, int IPT, int JL, bool FF, bool NN, bool NBL, int JP = 0>
 __global__ void __launch_bounds__(NT, g6_min_ctas<NT, IPT, JP && FF && !NBL && (IPT == 2 || IPT == 4) && JL == 1>())
     g6_kernel(const G6Args A) {
     // j tile during the loop, per-thread results (G6Out) after it

@@ -363,4 +363,4 @@ def test_every_configuration_vs_fp64(g6, state):
                 g6.clear_error()
                 g6.set_abort(True)
                 g6.plan_destroy(plan)
-    assert ncfg >= 9
+    assert ncfg >= 10
