@@ -62,6 +62,8 @@ PROFILED_TRAFFIC = {
     # the largest Hermite call by the configuration that runs it (6: 128x2 j-paired, 2: 128x2 i-paired)
     "hermite": {"bytes": 6_471_168 + 3_581_696,
                 "source": "profiles/g6_kernel_hermite_65536x65536.md (128x2 j-paired)"},
+    "hermite_cfg9": {"bytes": 6_554_880 + 4_392_192,
+                     "source": "profiles/g6_kernel_hermite_65536x65536.md (128x2 j-paired, stage-ordered)"},
     "hermite_cfg2": {"bytes": 6_578_944 + 17_873_152,
                      "source": "profiles/g6_kernel_hermite_65536x65536.md (128x2 i-paired)"},
     "direct": {"bytes": 542_720, "pairs": 268_435_456, "source": "profiles/g5_kernels_direct_treepm_bh.md (1024x1)"},
