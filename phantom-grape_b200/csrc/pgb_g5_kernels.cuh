@@ -54,6 +54,65 @@ constexpr int G5_FOLD = 128;
 template <int KIND>
 struct JWords { static constexpr int n = (KIND == G5_SYMMETRIC) ? 2 : (KIND == G5_QUAD ? 3 : 1); };
 
+// FP32 block sums per i: (acc, pot) for the point-mass and table kinds; the quadrupole kind
+// keeps [0..2] sum (w dr + K q^5 v), [3] sum m q, [4] sum K q^5 D (g5_quad_pair), which g5_fold
+// scales and combines into (acc, phi_p + phi_q).
+template <int KIND>
+struct NAcc { static constexpr int n = KIND == G5_QUAD ? 5 : 4; };
+
+// The cells' moments as staged in shared memory: Q' = (5/32) Q, which makes the coefficient of
+// the monopole and of the D q^7 term of the acceleration the same; K = -8/5 puts the (Q dr) r^-5
+// term into the same sums (g5_quad_pair).
+constexpr float G5_QSCALE = 0.15625f;
+constexpr float G5_QK = -1.6f;
+
+__device__ __forceinline__ float4 scale4(float4 v, float f) {
+    return make_float4(f * v.x, f * v.y, f * v.z, f * v.w);
+}
+
+// One FP32 block sum (a[NAcc]) into the FP64 sums S = (ax, ay, az, pot) -- pot as each kind's
+// raw sum (the quadrupole kind's +sum(phi_p + phi_q), which needs no finishing).
+template <int KIND>
+__device__ __forceinline__ void g5_fold(double (&S)[4], const float* a) {
+    if constexpr (KIND == G5_QUAD) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) S[c] += -0.125 * (double)a[c];
+        S[3] += -0.5 * (double)a[3] - (0.1 / (double)G5_QK) * (double)a[4];
+    } else {
+#pragma unroll
+        for (int c = 0; c < 4; c++) S[c] += (double)a[c];
+    }
+}
+
+// The same for paired sums: lane k of each a2[c] (k < 0: both lanes, x then y).
+template <int KIND>
+__device__ __forceinline__ void g5_fold2(double (&S)[4], const float2* a2, int k) {
+    float a[2][NAcc<KIND>::n];
+#pragma unroll
+    for (int c = 0; c < NAcc<KIND>::n; c++) {
+        a[0][c] = k == 1 ? a2[c].y : a2[c].x;
+        a[1][c] = a2[c].y;
+    }
+    if (k < 0) {
+        if constexpr (KIND == G5_QUAD) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) S[c] += -0.125 * ((double)a[0][c] + (double)a[1][c]);
+            S[3] += -0.5 * ((double)a[0][3] + (double)a[1][3]) - (0.1 / (double)G5_QK) * ((double)a[0][4] + (double)a[1][4]);
+        } else {
+#pragma unroll
+            for (int c = 0; c < 4; c++) S[c] = S[c] + (double)a[0][c] + (double)a[1][c];
+        }
+    } else {
+        g5_fold<KIND>(S, a[0]);
+    }
+}
+
+// A cell's two moment words into shared memory (word 1 at sq[0], word 2 at sq[1]), scaled.
+__device__ __forceinline__ void g5_stage_quad(float4* sq, const float4* jaux, int jj) {
+    sq[0] = scale4(jaux[2 * jj], G5_QSCALE);
+    sq[1] = scale4(jaux[2 * jj + 1], G5_QSCALE);
+}
+
 // Table lookup of the cutoff force (PG5/table/libpg5/gravity_kernel_avx2.c:70-124):
 // s = min(2 + |dx'|^2, r2cut); the table bin is the float bit pattern of s shifted right by
 // 23-FRC_BIT (the exponent and FRC_BIT leading mantissa bits); the bin's node is s with its
@@ -75,31 +134,39 @@ __device__ __forceinline__ void g5_table_pair(float4 J, float xi, float yi, floa
     a[2] = __fmaf_rn(mf, dz, a[2]);
 }
 
+// The quadrupole cell (c_GravityKernel, PG5/newton_quad/quad/quad_avx2.c:35-149; FP64 form
+// source.cpp:1160-1184): with r^-1 = -q/2 and the moments staged as Q' = (5/32) Q,
+//   v = Q' dr,  D = dr . v,  w = q^3 (m + D q^4),  p = K q^5 (K = -8/5)
+//   acc = dr (m r^-3 + (5/2) (dr.Q.dr) r^-7) - (Q dr) r^-5 = -(w dr + p v) / 8
+//   phi_p + phi_q = m r^-1 + (1/2) (dr.Q.dr) r^-5 = -(m q) / 2 - (p D) / (10 K)
+// 36 FP32 operations per pair (the r^-1, r^-2, r^-5 form takes 38); the block sums of
+// w dr + p v, m q and p D are scaled and combined in FP64 by g5_fold.  K rounded to FP32 weighs
+// the (Q dr) term 1.5e-8 (relative) heavier.
+__device__ __forceinline__ void g5_quad_pair(float dx, float dy, float dz, float m, float4 Q0, float4 Q1,
+                                             float e, float (&a)[5]) {
+    // Q0 = q00 q01 q02 q11, Q1 = q12 q22 - -
+    const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmaf_rn(dx, dx, e)));
+    const float q = minus2_over_r(r2);
+    const float vx = __fmaf_rn(Q0.z, dz, __fmaf_rn(Q0.y, dy, Q0.x * dx));
+    const float vy = __fmaf_rn(Q1.x, dz, __fmaf_rn(Q0.w, dy, Q0.y * dx));
+    const float vz = __fmaf_rn(Q1.y, dz, __fmaf_rn(Q1.x, dy, Q0.z * dx));
+    const float D = __fmaf_rn(dz, vz, __fmaf_rn(dy, vy, dx * vx));
+    const float q2 = q * q, q3 = q2 * q, q4 = q2 * q2, p = q4 * (G5_QK * q);
+    const float w = q3 * __fmaf_rn(D, q4, m);
+    a[0] = __fmaf_rn(w, dx, __fmaf_rn(p, vx, a[0]));
+    a[1] = __fmaf_rn(w, dy, __fmaf_rn(p, vy, a[1]));
+    a[2] = __fmaf_rn(w, dz, __fmaf_rn(p, vz, a[2]));
+    a[3] = __fmaf_rn(m, q, a[3]);
+    a[4] = __fmaf_rn(p, D, a[4]);
+}
+
 template <int KIND, int NT>
 __device__ __forceinline__ void g5_interact(const float4* sj, int j, float xi, float yi, float zi,
-                                            float ei, float (&a)[4]) {
+                                            float ei, float (&a)[NAcc<KIND>::n]) {
     float4 J = sj[j];
     float dx = J.x - xi, dy = J.y - yi, dz = J.z - zi;
     if constexpr (KIND == G5_QUAD) {
-        // c_GravityKernel, PG5/newton_quad/quad/quad_avx2.c:35-149 (FP64 form source.cpp:1160-1184)
-        float4 Q0 = sj[NT + 2 * j];      // q00 q01 q02 q11
-        float4 Q1 = sj[NT + 2 * j + 1];  // q12 q22  -   -
-        float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmaf_rn(dx, dx, ei)));
-        float q = minus2_over_r(r2);
-        float ri = -0.5f * q;
-        float ri2 = ri * ri;
-        float phi_p = J.w * ri;
-        float qx = __fmaf_rn(Q0.z, dz, __fmaf_rn(Q0.y, dy, Q0.x * dx));
-        float qy = __fmaf_rn(Q1.x, dz, __fmaf_rn(Q0.w, dy, Q0.y * dx));
-        float qz = __fmaf_rn(Q1.y, dz, __fmaf_rn(Q1.x, dy, Q0.z * dx));
-        float drqdr = __fmaf_rn(dz, qz, __fmaf_rn(dy, qy, dx * qx));
-        float dr5i = ri2 * ri2 * ri;
-        float phi_q = 0.5f * dr5i * drqdr;
-        a[3] += phi_p + phi_q;
-        float mr3i = __fmaf_rn(5.0f, phi_q, phi_p) * ri2;
-        a[0] = __fmaf_rn(dx, mr3i, __fmaf_rn(-qx, dr5i, a[0]));
-        a[1] = __fmaf_rn(dy, mr3i, __fmaf_rn(-qy, dr5i, a[1]));
-        a[2] = __fmaf_rn(dz, mr3i, __fmaf_rn(-qz, dr5i, a[2]));
+        g5_quad_pair(dx, dy, dz, J.w, sj[NT + 2 * j], sj[NT + 2 * j + 1], ei, a);
     } else {
         float e = ei;
         if constexpr (KIND == G5_SYMMETRIC) e += sj[NT + j].x;  // GravityKernel0
@@ -121,49 +188,28 @@ __device__ __forceinline__ float& lane_of(float2& v, int k) { return k ? v.y : v
 // tiles) against one j record: the per-i chains exactly as g5_interact / g5_table_pair, the
 // accumulations of the two i issued as paired FP32 instructions (FFMA2 / FADD2, each lane rounded
 // as the scalar instruction: results bit-identical to two g5_interact calls), except the
-// quadrupole kind's.  a2[c] holds component c of both i.
+// quadrupole kind's, whose sums stay scalar (g5_quad_pair per i: its many other FMAs already
+// load the FMA pipe's heavy half, which alone executes paired instructions; paired sums measured
+// 2 % slower).  a2[c] holds component c of both i.
 template <int KIND, int NT>
 __device__ __forceinline__ void g5_interact2(const float4* sj, int j, const float* xi, const float* yi,
                                              const float* zi, const float* ei, const float2* tab, int shift,
-                                             float r2cut, float2 (&a2)[4]) {
+                                             float r2cut, float2 (&a2)[NAcc<KIND>::n]) {
     const float4 J = sj[j];
-    float dx[2], dy[2], dz[2], s0[2], s3[2];
     if constexpr (KIND == G5_QUAD) {
         const float4 Q0 = sj[NT + 2 * j];
         const float4 Q1 = sj[NT + 2 * j + 1];
 #pragma unroll
         for (int k = 0; k < 2; k++) {
-            dx[k] = J.x - xi[k];
-            dy[k] = J.y - yi[k];
-            dz[k] = J.z - zi[k];
-            float r2 = __fmaf_rn(dz[k], dz[k], __fmaf_rn(dy[k], dy[k], __fmaf_rn(dx[k], dx[k], ei[k])));
-            float q = minus2_over_r(r2);
-            float ri = -0.5f * q;
-            float ri2 = ri * ri;
-            float phi_p = J.w * ri;
-            float qx = __fmaf_rn(Q0.z, dz[k], __fmaf_rn(Q0.y, dy[k], Q0.x * dx[k]));
-            float qy = __fmaf_rn(Q1.x, dz[k], __fmaf_rn(Q0.w, dy[k], Q0.y * dx[k]));
-            float qz = __fmaf_rn(Q1.y, dz[k], __fmaf_rn(Q1.x, dy[k], Q0.z * dx[k]));
-            float drqdr = __fmaf_rn(dz[k], qz, __fmaf_rn(dy[k], qy, dx[k] * qx));
-            float dr5i = ri2 * ri2 * ri;
-            float phi_q = 0.5f * dr5i * drqdr;
-            s3[k] = phi_p + phi_q;
-            s0[k] = __fmaf_rn(5.0f, phi_q, phi_p) * ri2;   // mr3i
-            // the quadrupole terms of the scalar form's inner FMA, per i
-            lane_of(a2[0], k) = __fmaf_rn(-qx, dr5i, lane_of(a2[0], k));
-            lane_of(a2[1], k) = __fmaf_rn(-qy, dr5i, lane_of(a2[1], k));
-            lane_of(a2[2], k) = __fmaf_rn(-qz, dr5i, lane_of(a2[2], k));
-        }
-        // the cell's sums stay scalar: its many other FMAs already load the FMA pipe's heavy
-        // half, which alone executes paired instructions (paired sums measured 2 % slower)
+            float a[5];
 #pragma unroll
-        for (int k = 0; k < 2; k++) {
-            lane_of(a2[0], k) = __fmaf_rn(dx[k], s0[k], lane_of(a2[0], k));
-            lane_of(a2[1], k) = __fmaf_rn(dy[k], s0[k], lane_of(a2[1], k));
-            lane_of(a2[2], k) = __fmaf_rn(dz[k], s0[k], lane_of(a2[2], k));
-            lane_of(a2[3], k) = __fadd_rn(lane_of(a2[3], k), s3[k]);
+            for (int c = 0; c < 5; c++) a[c] = lane_of(a2[c], k);
+            g5_quad_pair(J.x - xi[k], J.y - yi[k], J.z - zi[k], J.w, Q0, Q1, ei[k], a);
+#pragma unroll
+            for (int c = 0; c < 5; c++) lane_of(a2[c], k) = a[c];
         }
     } else {
+        float dx[2], dy[2], dz[2], s0[2], s3[2];
 #pragma unroll
         for (int k = 0; k < 2; k++) {
             dx[k] = J.x - xi[k];
@@ -201,16 +247,15 @@ __device__ __forceinline__ void g5_interact2(const float4* sj, int j, const floa
 // as one array per field (G5TileSoA), so that a 16-byte shared load returns a field of four
 // consecutive j and every paired FP32 operand is a natural register pair: (j, j+1) for the j
 // fields, a loop-invariant (v, v) for the i position.  The relative coordinates and the
-// accumulations -- and for cells the Q.dr products -- issue as paired FP32 instructions on the
-// heavy half of the FMA pipe, the rest of the chain stays scalar, loading the two halves about
-// equally.  Per pair the arithmetic is g5_interact's, operation for operation (FADD2 / FFMA2
-// round each lane as FADD / FFMA): the two lanes of an accumulator sum the even and the odd j.
-// The cells' quadrupole moments are stored negated (-Q), which turns the subtraction of the
-// -Q.dr / r^5 term into a plain FFMA2 with the same rounding.
+// accumulations -- and for cells the Q.dr products and D -- issue as paired FP32 instructions on
+// the heavy half of the FMA pipe, the rest of the chain stays scalar, loading the two halves
+// about equally.  Per pair the arithmetic is g5_interact's, operation for operation (FADD2 /
+// FFMA2 round each lane as FADD / FFMA): the two lanes of an accumulator sum the even and the
+// odd j.
 template <int NT>
 struct G5TileSoA {
     float x[NT], y[NT], z[NT], m[NT];
-    float q[6][NT];   // cells: -q00 -q01 -q02 -q11 -q12 -q22
+    float q[6][NT];   // cells: (5/32) (q00 q01 q02 q11 q12 q22)
 };
 
 __device__ __forceinline__ void g5_newton_jpair(float2 X, float2 Y, float2 Z, float2 M, float2 nx, float2 ny,
@@ -236,42 +281,37 @@ __device__ __forceinline__ void g5_newton_jpair(float2 X, float2 Y, float2 Z, fl
     a[2] = __ffma2_rn(mq3, dz, a[2]);
 }
 
-// Q = (-q00 -q01 -q02 -q11 -q12 -q22) of the two cells, as pairs.
+// Q = (q00 q01 q02 q11 q12 q22) of the two cells, as pairs, staged as Q' = (5/32) Q: the
+// arithmetic of g5_quad_pair, the moment products, D and the sums paired.
 __device__ __forceinline__ void g5_quad_jpair(float2 X, float2 Y, float2 Z, float2 M, const float2 (&Q)[6], float2 nx,
-                                              float2 ny, float2 nz, float e, float2 (&a)[4]) {
+                                              float2 ny, float2 nz, float e, float2 (&a)[5]) {
     const float2 dx = __fadd2_rn(X, nx), dy = __fadd2_rn(Y, ny), dz = __fadd2_rn(Z, nz);
-    // -(Q dr), component by component (c_GravityKernel, quad_avx2.c:35-149)
-    const float2 qx = __ffma2_rn(Q[2], dz, __ffma2_rn(Q[1], dy, __fmul2_rn(Q[0], dx)));
-    const float2 qy = __ffma2_rn(Q[4], dz, __ffma2_rn(Q[3], dy, __fmul2_rn(Q[1], dx)));
-    const float2 qz = __ffma2_rn(Q[5], dz, __ffma2_rn(Q[4], dy, __fmul2_rn(Q[2], dx)));
-    float2 dr5i, mr3i, s3;
+    const float2 vx = __ffma2_rn(Q[2], dz, __ffma2_rn(Q[1], dy, __fmul2_rn(Q[0], dx)));
+    const float2 vy = __ffma2_rn(Q[4], dz, __ffma2_rn(Q[3], dy, __fmul2_rn(Q[1], dx)));
+    const float2 vz = __ffma2_rn(Q[5], dz, __ffma2_rn(Q[4], dy, __fmul2_rn(Q[2], dx)));
+    const float2 D = __ffma2_rn(dz, vz, __ffma2_rn(dy, vy, __fmul2_rn(dx, vx)));
+    float2 q, p, w;
     const float* dxp = &dx.x;
     const float* dyp = &dy.x;
     const float* dzp = &dz.x;
-    const float* qxp = &qx.x;
-    const float* qyp = &qy.x;
-    const float* qzp = &qz.x;
+    const float* Dp = &D.x;
     const float* mp = &M.x;
-    float* d5p = &dr5i.x;
-    float* m3p = &mr3i.x;
-    float* s3p = &s3.x;
+    float* qp = &q.x;
+    float* pp = &p.x;
+    float* wp = &w.x;
 #pragma unroll
     for (int h = 0; h < 2; h++) {
         const float r2 = __fmaf_rn(dzp[h], dzp[h], __fmaf_rn(dyp[h], dyp[h], __fmaf_rn(dxp[h], dxp[h], e)));
-        const float q = minus2_over_r(r2);
-        const float ri = -0.5f * q;
-        const float ri2 = ri * ri;
-        const float phi_p = mp[h] * ri;
-        const float ndrqdr = __fmaf_rn(dzp[h], qzp[h], __fmaf_rn(dyp[h], qyp[h], dxp[h] * qxp[h]));   // -dr.Q.dr
-        d5p[h] = ri2 * ri2 * ri;
-        const float nphi_q = 0.5f * d5p[h] * ndrqdr;   // -phi_q
-        s3p[h] = phi_p - nphi_q;
-        m3p[h] = __fmaf_rn(-5.0f, nphi_q, phi_p) * ri2;
+        qp[h] = minus2_over_r(r2);
+        const float q2 = qp[h] * qp[h], q3 = q2 * qp[h], q4 = q2 * q2;
+        pp[h] = q4 * (G5_QK * qp[h]);
+        wp[h] = q3 * __fmaf_rn(Dp[h], q4, mp[h]);
     }
-    a[3] = __fadd2_rn(a[3], s3);
-    a[0] = __ffma2_rn(dx, mr3i, __ffma2_rn(qx, dr5i, a[0]));
-    a[1] = __ffma2_rn(dy, mr3i, __ffma2_rn(qy, dr5i, a[1]));
-    a[2] = __ffma2_rn(dz, mr3i, __ffma2_rn(qz, dr5i, a[2]));
+    a[0] = __ffma2_rn(w, dx, __ffma2_rn(p, vx, a[0]));
+    a[1] = __ffma2_rn(w, dy, __ffma2_rn(p, vy, a[1]));
+    a[2] = __ffma2_rn(w, dz, __ffma2_rn(p, vz, a[2]));
+    a[3] = __ffma2_rn(M, q, a[3]);
+    a[4] = __ffma2_rn(p, D, a[4]);
 }
 
 // Final scaling of the FP64 sums into (acc, pot_raw).
@@ -292,7 +332,7 @@ __device__ __forceinline__ double4 add4(double4 a, double4 b) {
 template <int KIND, int NT, int IPT, int STRIDE>
 __device__ __forceinline__ void g5_jloop(const float4* sj, int first, int nt, const float* xi, const float* yi,
                                          const float* zi, const float* ei, const float2* tab, int shift, float r2cut,
-                                         float (&a)[IPT][4], int nl = 1) {
+                                         float (&a)[IPT][NAcc<KIND>::n], int nl = 1) {
     const int step = STRIDE > 0 ? STRIDE : nl;
 #pragma unroll 4
     for (int j = first; j < nt; j += step) {
@@ -355,23 +395,18 @@ __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
                 const int jj = A.jidx ? __ldg(A.jidx + jk) : jk;
                 sj[threadIdx.x] = A.jpos[jj];
                 if constexpr (W == 2) sj[NT + threadIdx.x] = A.jaux[jj];
-                if constexpr (W == 3) {
-                    sj[NT + 2 * threadIdx.x] = A.jaux[2 * jj];
-                    sj[NT + 2 * threadIdx.x + 1] = A.jaux[2 * jj + 1];
-                }
+                if constexpr (W == 3) g5_stage_quad(sj + NT + 2 * threadIdx.x, A.jaux, jj);
             }
             __syncthreads();
             // one block: a lane sees at most NT/2 <= G5_FOLD records of a tile
-            float2 a2[4];
-            a2[0] = a2[1] = a2[2] = a2[3] = make_float2(0.f, 0.f);
+            float2 a2[NAcc<KIND>::n];
+#pragma unroll
+            for (int c = 0; c < NAcc<KIND>::n; c++) a2[c] = make_float2(0.f, 0.f);
 #pragma unroll 4
             for (int j = lane; j < nt; j += 2)
                 g5_interact2<KIND, NT>(sj, j, xi, yi, zi, ei, tab, shift, A.r2cut, a2);
 #pragma unroll
-            for (int k = 0; k < 2; k++) {
-#pragma unroll
-                for (int c = 0; c < 4; c++) S[k][c] += (double)lane_of(a2[c], k);
-            }
+            for (int k = 0; k < 2; k++) g5_fold2<KIND>(S[k], a2, k);
         }
         // lane 1's sums into lane 0's, one i per round through the j-tile buffer
         double4* red = reinterpret_cast<double4*>(sj);
@@ -423,22 +458,18 @@ __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
                 const int jj = A.jidx ? __ldg(A.jidx + jk) : jk;
                 sj[threadIdx.x] = A.jpos[jj];
                 if constexpr (W == 2) sj[NT + threadIdx.x] = A.jaux[jj];
-                if constexpr (W == 3) {
-                    sj[NT + 2 * threadIdx.x] = A.jaux[2 * jj];
-                    sj[NT + 2 * threadIdx.x + 1] = A.jaux[2 * jj + 1];
-                }
+                if constexpr (W == 3) g5_stage_quad(sj + NT + 2 * threadIdx.x, A.jaux, jj);
             }
             __syncthreads();
             // one block: a lane sees at most NT/4 <= G5_FOLD records of a tile
-            float a[3][4];
+            float a[3][NAcc<KIND>::n];
 #pragma unroll
-            for (int k = 0; k < 3; k++) a[k][0] = a[k][1] = a[k][2] = a[k][3] = 0.f;
+            for (int k = 0; k < 3; k++)
+#pragma unroll
+                for (int c = 0; c < NAcc<KIND>::n; c++) a[k][c] = 0.f;
             g5_jloop<KIND, NT, 3, 4>(sj, lane, nt, xi, yi, zi, ei, tab, shift, A.r2cut, a);
 #pragma unroll
-            for (int k = 0; k < 3; k++) {
-#pragma unroll
-                for (int c = 0; c < 4; c++) S[k][c] += (double)a[k][c];
-            }
+            for (int k = 0; k < 3; k++) g5_fold<KIND>(S[k], a[k]);
         }
         double4* red = reinterpret_cast<double4*>(sj);
 #pragma unroll
@@ -516,7 +547,7 @@ __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
                 sa->m[threadIdx.x] = real ? J.w : 0.0f;
                 if constexpr (KIND == G5_QUAD) {
                     const float4 Q0 = A.jaux[2 * jj], Q1 = A.jaux[2 * jj + 1];
-                    const float f = real ? -1.0f : 0.0f;
+                    const float f = real ? G5_QSCALE : 0.0f;
                     sa->q[0][threadIdx.x] = f * Q0.x;
                     sa->q[1][threadIdx.x] = f * Q0.y;
                     sa->q[2][threadIdx.x] = f * Q0.z;
@@ -528,9 +559,11 @@ __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
             __syncthreads();
             for (int jb = 0; jb < nt4; jb += G5_FOLD * nl) {
             const int je = min(jb + G5_FOLD * nl, nt4);
-            float2 a2[KM][4];
+            float2 a2[KM][NAcc<KIND>::n];
 #pragma unroll
-            for (int k = 0; k < KM; k++) a2[k][0] = a2[k][1] = a2[k][2] = a2[k][3] = make_float2(0.f, 0.f);
+            for (int k = 0; k < KM; k++)
+#pragma unroll
+                for (int c = 0; c < NAcc<KIND>::n; c++) a2[k][c] = make_float2(0.f, 0.f);
             for (int j = jb + 4 * lane; j < je; j += 4 * nl) {
                 const float4 X = *reinterpret_cast<const float4*>(&sa->x[j]);
                 const float4 Y = *reinterpret_cast<const float4*>(&sa->y[j]);
@@ -568,9 +601,7 @@ __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
                 }
             }
 #pragma unroll
-            for (int k = 0; k < KM; k++)
-#pragma unroll
-                for (int c = 0; c < 4; c++) S[k][c] = S[k][c] + (double)a2[k][c].x + (double)a2[k][c].y;
+            for (int k = 0; k < KM; k++) g5_fold2<KIND>(S[k], a2[k], -1);
             }
         }
         // lane sums in lane order, one i per round through the j-tile buffer
@@ -703,19 +734,17 @@ __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
                 const int jj = A.jidx ? __ldg(A.jidx + jk) : jk;
                 sj[threadIdx.x] = A.jpos[jj];
                 if constexpr (W == 2) sj[NT + threadIdx.x] = A.jaux[jj];
-                if constexpr (W == 3) {
-                    sj[NT + 2 * threadIdx.x] = A.jaux[2 * jj];
-                    sj[NT + 2 * threadIdx.x + 1] = A.jaux[2 * jj + 1];
-                }
+                if constexpr (W == 3) g5_stage_quad(sj + NT + 2 * threadIdx.x, A.jaux, jj);
             }
             __syncthreads();
             if constexpr (IPT % 2 == 0) {
                 for (int j0 = 0; j0 < nt; j0 += G5_FOLD) {
                     const int j1 = min(j0 + G5_FOLD, nt);
-                    float2 a2[IPT / 2][4];
+                    float2 a2[IPT / 2][NAcc<KIND>::n];
 #pragma unroll
                     for (int p = 0; p < IPT / 2; p++)
-                        a2[p][0] = a2[p][1] = a2[p][2] = a2[p][3] = make_float2(0.f, 0.f);
+#pragma unroll
+                        for (int c = 0; c < NAcc<KIND>::n; c++) a2[p][c] = make_float2(0.f, 0.f);
 #pragma unroll 4
                     for (int j = j0; j < j1; j++) {
 #pragma unroll
@@ -724,10 +753,7 @@ __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
                                                    A.r2cut, a2[p]);
                     }
 #pragma unroll
-                    for (int k = 0; k < IPT; k++) {
-#pragma unroll
-                        for (int c = 0; c < 4; c++) S[k][c] += (double)lane_of(a2[k / 2][c], k % 2);
-                    }
+                    for (int k = 0; k < IPT; k++) g5_fold2<KIND>(S[k], a2[k / 2], k % 2);
                 }
             } else {
             // blocks of G5_FOLD terms per lane (one block when a tile has no more: NT <= G5_FOLD);
@@ -735,20 +761,17 @@ __global__ void __launch_bounds__(NT) g5_kernel(G5Args A) {
             // records with immediate offsets (64-thread CTAs have 1, 2 or 4 lanes)
             const int nlanes = LANES ? nl : 1;
             auto block = [&](int j0, int j1) {
-                float a[IPT][4];
+                float a[IPT][NAcc<KIND>::n];
 #pragma unroll
-                for (int k = 0; k < IPT; k++) a[k][0] = a[k][1] = a[k][2] = a[k][3] = 0.f;
+                for (int k = 0; k < IPT; k++)
+#pragma unroll
+                    for (int c = 0; c < NAcc<KIND>::n; c++) a[k][c] = 0.f;
                 if (nlanes == 1) g5_jloop<KIND, NT, IPT, 1>(sj, j0 + lane, j1, xi, yi, zi, ei, tab, shift, A.r2cut, a);
                 else if (nlanes == 2) g5_jloop<KIND, NT, IPT, 2>(sj, j0 + lane, j1, xi, yi, zi, ei, tab, shift, A.r2cut, a);
                 else if (nlanes == 4) g5_jloop<KIND, NT, IPT, 4>(sj, j0 + lane, j1, xi, yi, zi, ei, tab, shift, A.r2cut, a);
                 else g5_jloop<KIND, NT, IPT, 0>(sj, j0 + lane, j1, xi, yi, zi, ei, tab, shift, A.r2cut, a, nlanes);
 #pragma unroll
-                for (int k = 0; k < IPT; k++) {
-                    S[k][0] += (double)a[k][0];
-                    S[k][1] += (double)a[k][1];
-                    S[k][2] += (double)a[k][2];
-                    S[k][3] += (double)a[k][3];
-                }
+                for (int k = 0; k < IPT; k++) g5_fold<KIND>(S[k], a[k]);
             };
             if constexpr (NT <= G5_FOLD) {
                 block(0, nt);

@@ -778,8 +778,11 @@ __device__ __forceinline__ void g6_task(const G6Args& A, const Task& T, unsigned
         auto run_tile = [&](auto self_c) {
             constexpr bool SELF = decltype(self_c)::value;
             if constexpr (USE_JP) {
-                for (int j0 = 0; j0 < nt4; j0 += G6_FOLD) {
-                    const int j1 = min(j0 + G6_FOLD, nt4);
+                // a full tile that cannot hold one of the task's i runs every fold block with a
+                // constant trip count (FULL); self and partial tiles with the run-time count
+                constexpr bool FULL = !SELF && NT % G6_FOLD == 0;
+                for (int j0 = 0; j0 < (FULL ? NT : nt4); j0 += G6_FOLD) {
+                    const int j1 = FULL ? j0 + G6_FOLD : min(j0 + G6_FOLD, nt4);
                     G6Acc2 a[IPT];
                     const float2 z2 = make_float2(0.f, 0.f);
 #pragma unroll
@@ -905,7 +908,7 @@ __device__ __forceinline__ void g6_task(const G6Args& A, const Task& T, unsigned
                 }
             }
         };
-        if (self_tile) run_tile(BoolC<true>{});
+        if (USE_JP ? (self_tile || nt4 != NT) : self_tile) run_tile(BoolC<true>{});
         else run_tile(BoolC<false>{});
 
         if constexpr (TILEMIN) {
