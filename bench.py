@@ -60,7 +60,7 @@ G5_CFG_NAMES = ["128x4", "256x2", "512x2", "1024x1", "384x2", "128x2", "128x1", 
                 "1024x1 j-paired", "256x1 j-paired"]   # pgb5 configurations (threads x i/thread)
 PROFILED_TRAFFIC = {
     # the largest Hermite call by the configuration that runs it (6: 128x2 j-paired, 2: 128x2 i-paired)
-    "hermite": {"bytes": 6_471_168 + 3_581_696,
+    "hermite": {"bytes": 6_475_008 + 4_498_688,
                 "source": "profiles/g6_kernel_hermite_65536x65536.md (128x2 j-paired)"},
     "hermite_cfg9": {"bytes": 6_554_880 + 4_392_192,
                      "source": "profiles/g6_kernel_hermite_65536x65536.md (128x2 j-paired, stage-ordered)"},
@@ -139,6 +139,16 @@ def pipe_peaks(pgb, stream_ptr=0):
             mix[name] = round(t2.value, 2)
     if mix:
         _PIPE_PEAKS["fp32_mix_tflops"] = mix
+    # the Hermite kernel's j-paired pair loop alone on a resident shared-memory tile (no j
+    # staging, scheduling or partial rows): the rate its arithmetic sustains
+    L.pgb_peak_g6_loop.argtypes = [C.c_int, C.c_int, C.c_void_p, dp, dp, ip]
+    loop = {}
+    for form, name in ((1, "jpair"), (2, "jquad2")):
+        gp, lm, rg = C.c_double(), C.c_double(), C.c_int()
+        if L.pgb_peak_g6_loop(form, 400, C.c_void_p(stream_ptr), C.byref(gp), C.byref(lm), C.byref(rg)) == 0:
+            loop[name] = {"gpairs": round(gp.value, 1), "registers": rg.value}
+    if loop:
+        _PIPE_PEAKS["g6_pair_loop"] = loop
     if rc2 == 0:
         _PIPE_PEAKS.update({"mufu_grsqrt_s": round(mg.value, 1), "mufu_ms": round(mms.value, 3),
                             "mufu_per_sm_clk": round(mg.value * 1e9 / SM_COUNT / ((clk.get("sm_mhz") or 1965.0) * 1e6), 2)})
@@ -146,6 +156,21 @@ def pipe_peaks(pgb, stream_ptr=0):
     _PIPE_PEAKS["how"] = ("lib/libpgbpeak.so: 8 independent FFMA (rsqrt.approx.ftz.f32) chains per thread, 256-thread "
                           "CTAs at full occupancy on every SM, best of 5 launches (CUDA events)")
     return _PIPE_PEAKS
+
+
+def pair_loop_ceiling(fp32_tf, kernel_gpairs):
+    """The Hermite pair loop's own rate on a resident tile (pipe_peaks) beside the force kernel's:
+    the part of the gap to the FFMA peak that the arithmetic itself leaves, and the part the
+    kernel's staging, scheduling and reductions add."""
+    loop = _PIPE_PEAKS.get("g6_pair_loop")
+    if not loop:
+        return None
+    best = max(v["gpairs"] for v in loop.values())
+    return {"forms": loop, "best_gpairs": best, "frac_of_peak": round(best * 1e9 * 60 / 1e12 / fp32_tf, 4),
+            "kernel_vs_loop": round(kernel_gpairs / best, 4),
+            "how": "lib/libpgbpeak.so pgb_peak_g6_loop: the j-paired inner loop (two i per thread, NN tile "
+                   "minimum, FP64 folds every 128 j) over one 128-record tile staged once, a wave of resident "
+                   "CTAs, best of 5 launches"}
 
 
 def fp32_peak(pgb, clk, stream_ptr=0):
@@ -736,7 +761,8 @@ def run_hermite(args, pgb, ws, rank, local):
                      "peak_source": peak_src, "peak_nominal": round(fp32_nominal, 2),
                      "mufu_peak_grsqrt_s": _PIPE_PEAKS.get("mufu_grsqrt_s"),
                      "mufu_per_sm_clk": _PIPE_PEAKS.get("mufu_per_sm_clk"),
-                     "fp32_mix_tflops": _PIPE_PEAKS.get("fp32_mix_tflops")},
+                     "fp32_mix_tflops": _PIPE_PEAKS.get("fp32_mix_tflops"),
+                     "pair_loop_ceiling": pair_loop_ceiling(fp32_tf, B["big_pairs"] / (B["big_ms"] / 1e3) / 1e9)},
         "e2e": {"value": round(e2e_val, 2), "unit": "Gint/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "api": "GRAPE-6 drop-in (g6_set_ti, g6calc_firsthalf, "
                 "g6calc_lasthalf2p per npipes chunk, g6_set_j_particle of the active set), host buffers",

@@ -7,11 +7,18 @@
 //  * MUFU (XU pipe) reciprocal square root: every thread runs PEAK_CHAINS independent chains of
 //    rsqrt.approx.ftz.f32 (x = rsqrt(x), which stays in [1, 4) for a start in [1, 4)), the
 //    instruction the force kernels use.
+//  * The Hermite pair loop's own ceiling: the j-paired inner loop of the force kernel
+//    (pgb_g6_kernels.cuh g6_jpair / g6_jquad2, two i per thread, nearest-neighbour tile minimum,
+//    FP32 sums folded into FP64 in shared memory every 128 j) over one shared-memory tile staged
+//    once, with no j staging, task scheduling or partial rows: what the kernel's arithmetic
+//    sustains when nothing else runs.
 // Both kernels write one value per thread (so that nothing is optimised away) into a caller
 // buffer or a small internal one.  Times are CUDA-event times on the caller's stream.
 #include <cuda_runtime.h>
 
 #include <cstdio>
+
+#include "pgb_g6_kernels.cuh"
 
 #define PGB_EXPORT extern "C" __attribute__((visibility("default")))
 
@@ -85,6 +92,89 @@ __global__ void __launch_bounds__(PEAK_THREADS) mufu_kernel(float* out, int iter
 #pragma unroll
     for (int c = 0; c < PEAK_CHAINS; c++) s += x[c];
     out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+constexpr int LOOP_NT = 128;
+
+// Synthetic values in [-1, 1) from a hashed counter (run-time values for every field, so that
+// nothing folds at compile time).
+__device__ __forceinline__ float hash_unit(unsigned& h) {
+    h = h * 1664525u + 1013904223u;
+    return (float)(h >> 8) * (1.0f / 8388608.0f) - 1.0f;
+}
+
+template <int JP>
+__global__ void __launch_bounds__(LOOP_NT) g6_loop_kernel(double* out, int passes, float eps2) {
+    __shared__ pgb::G6TileSoA<LOOP_NT> tile;
+    __shared__ double Ssh[14 * LOOP_NT];
+    const int t = threadIdx.x;
+    unsigned h = (blockIdx.x * 977u + t * 7919u + 1u) * 2654435761u;
+    tile.xh[t] = hash_unit(h); tile.yh[t] = hash_unit(h); tile.zh[t] = hash_unit(h);
+    tile.xl[t] = hash_unit(h) * 1e-8f; tile.yl[t] = hash_unit(h) * 1e-8f; tile.zl[t] = hash_unit(h) * 1e-8f;
+    tile.m[t] = 1.0f / 65536; tile.vx[t] = hash_unit(h); tile.vy[t] = hash_unit(h); tile.vz[t] = hash_unit(h);
+    tile.id[t] = t;
+    pgb::G6IPair IP[2];
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        const float x = hash_unit(h), y = hash_unit(h), z = hash_unit(h);
+        const float lx = hash_unit(h) * 1e-8f, ly = hash_unit(h) * 1e-8f, lz = hash_unit(h) * 1e-8f;
+        IP[k].nxh = make_float2(-x, -x); IP[k].nyh = make_float2(-y, -y); IP[k].nzh = make_float2(-z, -z);
+        IP[k].nxl = make_float2(-lx, -lx); IP[k].nyl = make_float2(-ly, -ly); IP[k].nzl = make_float2(-lz, -lz);
+        IP[k].vx = hash_unit(h); IP[k].vy = hash_unit(h); IP[k].vz = hash_unit(h);
+        IP[k].id = -1;
+    }
+    for (int c = 0; c < 14; c++) Ssh[c * LOOP_NT + t] = 0.0;
+    float tmin[2] = {10.f, 10.f};
+    __syncthreads();
+    for (int p = 0; p < passes; p++) {
+        pgb::G6Acc2 a[2];
+        const float2 z2 = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int k = 0; k < 2; k++) a[k] = pgb::G6Acc2{z2, z2, z2, z2, z2, z2, {0.f, 0.f}};
+#pragma unroll 1
+        for (int j = 0; j < LOOP_NT; j += 4) {
+            const float4 XH = *reinterpret_cast<const float4*>(&tile.xh[j]);
+            const float4 YH = *reinterpret_cast<const float4*>(&tile.yh[j]);
+            const float4 ZH = *reinterpret_cast<const float4*>(&tile.zh[j]);
+            const float4 XL = *reinterpret_cast<const float4*>(&tile.xl[j]);
+            const float4 YL = *reinterpret_cast<const float4*>(&tile.yl[j]);
+            const float4 ZL = *reinterpret_cast<const float4*>(&tile.zl[j]);
+            const float4 M = *reinterpret_cast<const float4*>(&tile.m[j]);
+            const float4 VX = *reinterpret_cast<const float4*>(&tile.vx[j]);
+            const float4 VY = *reinterpret_cast<const float4*>(&tile.vy[j]);
+            const float4 VZ = *reinterpret_cast<const float4*>(&tile.vz[j]);
+            const int4 ID = make_int4(0, 0, 0, 0);
+            if constexpr (JP == 2) {
+                pgb::g6_jquad2<true, false>(XH, YH, ZH, XL, YL, ZL, M, VX, VY, VZ, ID, IP, eps2, a, tmin);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 2; k++) {
+                    pgb::g6_jpair<true, false>(make_float2(XH.x, XH.y), make_float2(YH.x, YH.y), make_float2(ZH.x, ZH.y),
+                                               make_float2(XL.x, XL.y), make_float2(YL.x, YL.y), make_float2(ZL.x, ZL.y),
+                                               make_float2(M.x, M.y), make_float2(VX.x, VX.y), make_float2(VY.x, VY.y),
+                                               make_float2(VZ.x, VZ.y), make_int2(ID.x, ID.y), IP[k], eps2, a[k], tmin[k]);
+                    pgb::g6_jpair<true, false>(make_float2(XH.z, XH.w), make_float2(YH.z, YH.w), make_float2(ZH.z, ZH.w),
+                                               make_float2(XL.z, XL.w), make_float2(YL.z, YL.w), make_float2(ZL.z, ZL.w),
+                                               make_float2(M.z, M.w), make_float2(VX.z, VX.w), make_float2(VY.z, VY.w),
+                                               make_float2(VZ.z, VZ.w), make_int2(ID.z, ID.w), IP[k], eps2, a[k], tmin[k]);
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const float2* v = &a[k].ax;
+#pragma unroll
+            for (int c = 0; c < 6; c++) {
+                double& d = Ssh[(k * 7 + c) * LOOP_NT + t];
+                d = d + (double)v[c].x + (double)v[c].y;
+            }
+            double& d = Ssh[(k * 7 + 6) * LOOP_NT + t];
+            d = d + (double)a[k].pot[0] + (double)a[k].pot[1];
+        }
+    }
+    double s = (double)tmin[0] + (double)tmin[1];
+    for (int c = 0; c < 14; c++) s += Ssh[c * LOOP_NT + t];
+    out[blockIdx.x * LOOP_NT + t] = s;
 }
 
 // Runs kern `reps` times after one warm-up launch and returns the best launch time (ms), or a
@@ -181,5 +271,37 @@ PGB_EXPORT int pgb_peak_fp32_mix(int kind, int iters, void* stream, double* tflo
     const double flops = (double)grid * PEAK_THREADS * (double)iters * 8 * (4.0 * P + 2.0 * S);
     if (tflops) *tflops = flops / (t * 1e-3) / 1e12;
     if (ms) *ms = t;
+    return 0;
+}
+
+// Pair rate of the Hermite force kernel's j-paired inner loop on a resident tile (see the top of
+// the file): form 1 = g6_jpair (the autotuner's 128 x 2 j-paired configuration), 2 = g6_jquad2
+// (stage-ordered).  `passes` sweeps of the 128-record tile per CTA, the grid a whole wave of
+// resident CTAs.  *gpairs = pairs / best launch time / 1e9, *regs = registers per thread.
+PGB_EXPORT int pgb_peak_g6_loop(int form, int passes, void* stream, double* gpairs, double* ms, int* regs) {
+    cudaStream_t s = (cudaStream_t)stream;
+    const void* fn = form == 2 ? (const void*)g6_loop_kernel<2> : (const void*)g6_loop_kernel<1>;
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, LOOP_NT, 0);
+    if (per_sm < 1) per_sm = 1;
+    const int grid = sms * per_sm;
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, fn) != cudaSuccess) return -1;
+    double* out = nullptr;
+    if (cudaMalloc(&out, (size_t)grid * LOOP_NT * sizeof(double)) != cudaSuccess) return -1;
+    float t = best_ms(
+        [&] {
+            if (form == 2) g6_loop_kernel<2><<<grid, LOOP_NT, 0, s>>>(out, passes, 1e-8f);
+            else g6_loop_kernel<1><<<grid, LOOP_NT, 0, s>>>(out, passes, 1e-8f);
+        },
+        5, s);
+    cudaFree(out);
+    if (t <= 0.f) return -1;
+    const double pairs = (double)grid * LOOP_NT * 2 * LOOP_NT * passes;
+    if (gpairs) *gpairs = pairs / (t * 1e-3) / 1e9;
+    if (ms) *ms = t;
+    if (regs) *regs = fa.numRegs;
     return 0;
 }
