@@ -578,6 +578,7 @@ bool run_force(int nj, int ni, float eps2, bool nn, bool nbl) {
     a.reg_ni = ni;
     a.reg_nj = nj;
     a.reg_nch = nch;
+    a.jn = nj;
     if (nbl) {
         PGB_CUDA_OR(g_err, LIB, S.nbc_d.reserve(ni), return false);
         PGB_CUDA_OR(g_err, LIB, S.nbl_d.reserve((size_t)ni * nbmax()), return false);
@@ -967,11 +968,19 @@ void set_tuned(long long key, int cfg) {
 }
 }  // namespace
 
+// The largest j_offset + j_count of an item table ([k][4] = i_off, i_cnt, j_off, j_cnt).
+int items_jend(int nitem, const int* items) {
+    long long e = 0;
+    for (int k = 0; k < nitem; k++) e = std::max<long long>(e, (long long)items[4 * k + 2] + items[4 * k + 3]);
+    return (int)std::min<long long>(e, 0x7fffffff);
+}
+
 struct pgb6_plan {
     int cfg;
     bool nn;
     bool ff;
     std::vector<int> items;    // the work-item table, kept for re-planning (autotuning)
+    int jend = 0;              // the items' largest j_offset + j_count (the j records they read)
     long long shape_key = 0;   // autotune cache key of this work-item table
     std::vector<Task> tasks;
     std::vector<Group> groups;
@@ -1006,6 +1015,7 @@ PGB_EXPORT int pgb6_plan_create(pgb6_plan** out, int nitem, const int* items, in
     long long total_i = 0;
     for (int k = 0; k < nitem; k++) total_i += items[4 * k + 1];
     P->items.assign(items, items + 4 * (size_t)nitem);
+    P->jend = items_jend(nitem, items);
     P->shape_key = shape_key(nitem, items, P->ff, P->nn);
     int tuned = tuned_cfg(P->shape_key);
     P->cfg = tuned >= 0 ? tuned : pick_cfg(nitem > 1 ? std::max<long long>(nimax, total_i / 4) : nimax);
@@ -1057,6 +1067,7 @@ PGB_EXPORT int pgb6_plan_launch(pgb6_plan* P, const void* ipart, const void* jpr
     a.nb_count = nullptr;
     a.nb_list = nullptr;
     a.nb_maxlen = 0;
+    a.jn = P->jend;
     int slots = sm_count(g_device) * occupancy(P->cfg, P->ff, P->nn, false);
     int grid = a.ntasks < slots ? a.ntasks : slots;
     PGB_CUDA_OR(g_err, LIB, launch_kernel(P->cfg, P->ff, P->nn, false, grid, a, s), return PGB_ERR_CUDA);
@@ -1115,6 +1126,7 @@ PGB_EXPORT int pgb6_plan_update(pgb6_plan* P, int nitem, const int* items) {
         }
     if (!ensure_device()) return PGB_ERR_NOGPU;
     P->items.assign(items, items + 4 * (size_t)nitem);
+    P->jend = items_jend(nitem, items);
     P->shape_key = shape_key(nitem, items, P->ff, P->nn);
     P->tasks.clear();
     P->groups.clear();
@@ -1419,6 +1431,7 @@ PGB_EXPORT int pgb6_force_noalloc(const void* ipart, int ni, const void* jpred, 
     a.nb_count = nullptr;
     a.nb_list = nullptr;
     a.nb_maxlen = 0;
+    a.jn = nj;
     int grid = ntasks < slots ? ntasks : slots;
     PGB_CUDA_OR(g_err, LIB, launch_kernel(cfg, ff, nn, false, grid, a, s), return PGB_ERR_CUDA);
     return PGB_OK;

@@ -103,6 +103,8 @@ struct G6Args {
     // leave the partial rows of split j-ranges unreduced (the caller's next kernel sums them in
     // chunk order): no arrival counters, fences or last-CTA reduction in this launch
     bool partial_only = false;
+    // records in jpred (bounds the nearest-neighbour address lookups of split groups)
+    int jn = 0;
 };
 
 // The task and group of regular mode (the same decomposition plan_item() writes out).
@@ -563,10 +565,11 @@ __device__ __forceinline__ double2 word_zero(bool w3) {
 // the R group sums are added in group order through shared memory W (NT words).  The order is
 // fixed for a given (NT, nw, nrows): deterministic.  finish: write the final scaled result (acc,
 // jerk x -1/8, pot x 1/2) instead of the raw sum.  dst (same word indexing) may be row 0 itself:
-// every word is read before it is written.
+// every word is read before it is written.  nnk (optional, with wbeg = 0): the summed (key,
+// address) word of row i also into nnk[i].
 template <int NT>
 __device__ __forceinline__ void reduce_rows(const G6Out* base, size_t stride, int nrows, int wbeg, int nw,
-                                            G6Out* dst, bool finish, double2* W) {
+                                            G6Out* dst, bool finish, double2* W, double* nnk = nullptr) {
     // row groups: as many as the threads allow, but no more than the rows and at most 8 (their
     // sums are combined serially)
     const int R = (2 * nw <= NT) ? min(min(NT / nw, nrows), 8) : 1;
@@ -621,6 +624,7 @@ __device__ __forceinline__ void reduce_rows(const G6Out* base, size_t stride, in
             s0.x *= w3 ? 0.5 : -0.125;
             if (!w3) s0.y *= -0.125;
         }
+        if (nnk && w3) nnk[f >> 2] = s0.y;
         out[f] = s0;
     }
 }
@@ -922,11 +926,18 @@ __device__ __forceinline__ void g6_task(const G6Args& A, const Task& T, unsigned
     }
     if constexpr (TILEMIN) {
         // the address of each i's nearest neighbour: the first j of its best tile with that key
-        // (the j-paired form reads its i-record again rather than keep it in registers)
+        // (the j-paired form reads its i-record again rather than keep it in registers).  A task
+        // of a split j-range leaves the start of its best tile instead: the group's reduction
+        // keeps the best (key, tile start) over the chunks -- the same winner as over addresses,
+        // the chunks being consecutive j-ranges -- and g6_resolve_nn looks up that one tile per i
+        // (one lookup per i instead of one per i and chunk).
+        const bool defer = T.group >= 0 && !A.partial_only;
 #pragma unroll
         for (int k = 0; k < IPT; k++) {
             const int li = slot + k * ISL;
-            if (li < T.ni && ktile[k] >= 0) {
+            if (defer) {
+                if (ktile[k] >= 0) kadr[k] = T.j0 + ktile[k];
+            } else if (li < T.ni && ktile[k] >= 0) {
                 if constexpr (USE_JP) {
                     const G6I P = A.ipart[T.i0 + li];
                     kadr[k] = g6_rescan<FF>(A.jpred, T.j0 + ktile[k], min(NT, T.nj - ktile[k]), P.p, P.id, A.eps2,
@@ -979,6 +990,23 @@ constexpr int g6_min_ctas() {
     return (!JPE && IPT == 2) ? (NT <= 128 ? 1 : 512 / NT) : 0;   // 256 threads: <= 128 registers, 2 CTAs
 }
 
+// The nearest neighbours of a reduced split group whose tasks left tile starts (g6_task):
+// nnk[li] = the group's best (key, tile start) of i li; the first j of that tile with the key,
+// looked up from the predicted j-set, goes into out[i].jadr.  Threads take the group's i in
+// turn, so the lookups run side by side.
+template <int NT, bool FF>
+__device__ __forceinline__ void g6_resolve_nn(const G6Args& A, const Group& G, const double* nnk) {
+    __syncthreads();   // nnk written by the reduction's threads
+    for (int li = threadIdx.x; li < G.ni; li += NT) {
+        const long long w = __double_as_longlong(nnk[li]);
+        const int tile = (int)(w >> 32);
+        if (tile < 0) continue;   // no candidate (address -1)
+        const float key = __int_as_float((int)(w & 0xffffffffLL));
+        const G6I P = A.ipart[G.i0 + li];
+        A.out[G.i0 + li].jadr = g6_rescan<FF>(A.jpred, tile, min(NT, A.jn - tile), P.p, P.id, A.eps2, key);
+    }
+}
+
 template <int NT, int IPT, int JL, bool FF, bool NN, bool NBL, int JP = 0>
 __global__ void __launch_bounds__(NT, g6_min_ctas<NT, IPT, JP && FF && !NBL && (IPT == 2 || IPT == 4) && JL == 1>())
     g6_kernel(const G6Args A) {
@@ -995,6 +1023,12 @@ __global__ void __launch_bounds__(NT, g6_min_ctas<NT, IPT, JP && FF && !NBL && (
         if (T.group < 0 || A.partial_only) continue;
         const Group G = A.groups ? A.groups[T.group] : regular_group(A, T.group);
         double2* W = reinterpret_cast<double2*>(smem);
+        // the tile-minimum nearest-neighbour search leaves tile starts in split groups' rows
+        constexpr bool TILEMIN = NN && !NBL && IPT % 2 == 0;
+        double* nnk = TILEMIN ? reinterpret_cast<double*>(smem + NT * sizeof(double2)) : nullptr;
+        static_assert(!TILEMIN || NT * sizeof(double2) + NT * IPT * sizeof(double) <=
+                                      (size_t)g6_smem_bytes<NT, IPT, JP && FF && !NBL && (IPT == 2 || IPT == 4) && JL == 1>(),
+                      "reduction scratch and nearest-neighbour words fit the j-tile buffer");
         const int B = bundle_size(G.nchunk, A.bundle_counters != nullptr);
         if (B < G.nchunk) {
             // two levels: the last CTA of each bundle of B consecutive chunks sums the bundle's
@@ -1008,12 +1042,13 @@ __global__ void __launch_bounds__(NT, g6_min_ctas<NT, IPT, JP && FF && !NBL && (
             const int nb = (G.nchunk + B - 1) / B;
             if (!group_arrive(A.group_counters, T.group, nb, &s_flag)) continue;
             reduce_rows<NT>(A.partial + (size_t)G.slot0 * A.itile, (size_t)B * A.itile, nb, 0, 4 * G.ni, A.out + G.i0, true,
-                            W);
+                            W, nnk);
         } else {
             if (!group_arrive(A.group_counters, T.group, G.nchunk, &s_flag)) continue;
             reduce_rows<NT>(A.partial + (size_t)G.slot0 * A.itile, (size_t)A.itile, G.nchunk, 0, 4 * G.ni, A.out + G.i0,
-                            true, W);
+                            true, W, nnk);
         }
+        if constexpr (TILEMIN) g6_resolve_nn<NT, FF>(A, G, nnk);
     }
 }
 
