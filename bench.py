@@ -60,7 +60,7 @@ G5_CFG_NAMES = ["128x4", "256x2", "512x2", "1024x1", "384x2", "128x2", "128x1", 
                 "1024x1 j-paired", "256x1 j-paired"]   # pgb5 configurations (threads x i/thread)
 PROFILED_TRAFFIC = {
     # the largest Hermite call by the configuration that runs it (6: 128x2 j-paired, 2: 128x2 i-paired)
-    "hermite": {"bytes": 6_475_008 + 4_498_688,
+    "hermite": {"bytes": 6_463_232 + 5_087_488,
                 "source": "profiles/g6_kernel_hermite_65536x65536.md (128x2 j-paired)"},
     "hermite_cfg9": {"bytes": 6_554_880 + 4_392_192,
                      "source": "profiles/g6_kernel_hermite_65536x65536.md (128x2 j-paired, stage-ordered)"},
