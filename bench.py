@@ -551,7 +551,7 @@ def hermite_batched(args, pgb, g6, wl, sub, calls, dev, s, ff, tune, steps, warm
     return dict(step_ms=step_ms, clk=clk, tuned=tuned, graph=graph, plans=plans, d_ptcl=d_ptcl, d_irec=d_irec,
                 d_out=d_out, ptcl=ptcl, irec=irec, nrow=nrow, kern_s=kern_s, kern_pairs=kern_pairs,
                 big_pairs=big[1], big_ms=big[0], big_call=big[2], step=step,
-                launches_per_step=2 * len(live))
+                launches_per_step=sum(1 + g6.L.pgb6_plan_kernels(plans[c]) for c, _, _ in live))
 
 
 def hermite_fp64_check(pgb, wl, sub, calls, out_rows, ff_label=""):
@@ -1042,6 +1042,7 @@ def run_clusters(args, pgb, ws, rank, local):
         cpu["fp64_check"].update({"nn_mismatch": ck["nn"], "particles": ck["n"],
                                   "clusters": f"every 64th of 1024 ({nsel})",
                                   "oracle": "FP64 direct sum on the same inputs (oracle/pg_oracle.c)"})
+    kernels_per_launch = max(1, g6.L.pgb6_plan_kernels(plan))
     g6.plan_destroy(plan)
     return _line(args, ws, "Gint/s (independent Hermite clusters, batched)", value, t_max / len(ts), pairs, 60,
                  "1024 Plummer clusters, N log-uniform [256,16384], eps=1e-4, one force+jerk+pot+NN each",
@@ -1049,7 +1050,7 @@ def run_clusters(args, pgb, ws, rank, local):
                  {"value": round(e2e_val, 3), "unit": "Gint/s", "h2d_bytes_per_step": n * (128 + 48),
                   "d2h_bytes_per_step": n * 64, "api": "plain GRAPE-6 calls per cluster (g6_set_j_particle x N_k, "
                   "g6_set_ti, g6calc_firsthalf/lasthalf2p per npipes), host buffers"},
-                 cpu, len(ts), extra={"autotune": cfg, "batched_vs_plain": round(value / e2e_val, 1),
+                 cpu, len(ts) * kernels_per_launch, extra={"autotune": cfg, "batched_vs_plain": round(value / e2e_val, 1),
                                       "scaling": "strong" if ws > 1 else "weak"},
                  kernel="pgb::g6_kernel (autotuned configuration)",
                  parallelism=(f"contiguous cost partition of the clusters x{ws}, results all-gathered in the step"

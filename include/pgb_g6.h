@@ -111,11 +111,14 @@ void pgb6_plan_destroy(pgb6_plan *plan);
 long long pgb6_plan_interactions(const pgb6_plan *plan);
 int  pgb6_plan_tasks(const pgb6_plan *plan);
 int  pgb6_plan_config(const pgb6_plan *plan);
+/* kernels one pgb6_plan_launch issues (the force kernel, plus the nearest-neighbour lookup kernel
+ * of split i-tiles when the plan's configuration defers them) */
+int  pgb6_plan_kernels(const pgb6_plan *plan);
 /* new items for an existing plan (its flags and configuration kept), staged into its own buffers
  * (no device allocation in a step loop); waits for the plan's previous stream launches */
 int  pgb6_plan_update(pgb6_plan *plan, int nitem, const int *items);
 int  pgb6_plan_set_config(pgb6_plan *plan, int cfg);   /* pin one of PGB6_NCFG configurations */
-enum { PGB6_NCFG = 6 };
+enum { PGB6_NCFG = 10 };
 /* autotuner: times every kernel configuration on the caller's data, keeps the fastest for this
  * plan and for later plans of the same shape; returns the configuration, *best_ms its time */
 int  pgb6_plan_tune(pgb6_plan *plan, const void *ipart, const void *jpred, double eps2, void *out,

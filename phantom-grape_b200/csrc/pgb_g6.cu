@@ -167,6 +167,23 @@ cudaError_t launch_kernel(int cfg, bool ff, bool nn, bool nbl, int grid, const G
     return cudaGetLastError();
 }
 
+// Whether a force launch of this shape leaves nearest-neighbour lookups to g6_resolve_kernel:
+// the tile-minimum search (two or four i per thread; one j-lane), split i-tiles (ngroups > 0),
+// j addresses below the G6_NN_TILE mark (g6_task's `defer`).
+bool needs_resolve(int cfg, bool nn, bool nbl, int ngroups, int jn) {
+    return nn && !nbl && ngroups > 0 && CFG_IPT[cfg] % 2 == 0 && CFG_JL[cfg] == 1 && jn < G6_NN_TILE;
+}
+
+// The deferred nearest-neighbour lookups of a force launch (after it, on the same stream).
+cudaError_t launch_resolve(int cfg, bool ff, bool nn, bool nbl, int ngroups, const G6Args& a, cudaStream_t s) {
+    if (!needs_resolve(cfg, nn, nbl, ngroups, a.jn)) return cudaSuccess;
+    constexpr int rpb = 128 / G6_RES_LANES;
+    const long long grid = (long long)ngroups * ((a.itile + rpb - 1) / rpb);
+    if (ff) g6_resolve_kernel<true><<<(unsigned)grid, 128, 0, s>>>(a, ngroups, CFG_NT[cfg]);
+    else g6_resolve_kernel<false><<<(unsigned)grid, 128, 0, s>>>(a, ngroups, CFG_NT[cfg]);
+    return cudaGetLastError();
+}
+
 // The small-call cluster kernel (pgb_g6_small.cuh): i-slots x j-lanes by the call's i count.
 struct SmallShape {
     int isl, jl;
@@ -589,6 +606,7 @@ bool run_force(int nj, int ni, float eps2, bool nn, bool nbl) {
     if (a.ntasks == 0) return true;
     const int grid = a.ntasks < slots ? a.ntasks : slots;
     PGB_CUDA_OR(g_err, LIB, launch_kernel(cfg, ff, nn, nbl, grid, a, S.stream), return false);
+    PGB_CUDA_OR(g_err, LIB, launch_resolve(cfg, ff, nn, nbl, nch > 1 ? itiles : 0, a, S.stream), return false);
     return true;
 }
 
@@ -1038,6 +1056,12 @@ PGB_EXPORT int pgb6_plan_create(pgb6_plan** out, int nitem, const int* items, in
 PGB_EXPORT long long pgb6_plan_interactions(const pgb6_plan* P) { return P ? P->interactions : 0; }
 PGB_EXPORT int pgb6_plan_tasks(const pgb6_plan* P) { return P ? (int)P->tasks.size() : 0; }
 PGB_EXPORT int pgb6_plan_config(const pgb6_plan* P) { return P ? P->cfg : -1; }
+// Kernels one pgb6_plan_launch issues: the force kernel, and the nearest-neighbour lookups of
+// split i-tiles when the plan's configuration defers them.
+PGB_EXPORT int pgb6_plan_kernels(const pgb6_plan* P) {
+    if (!P || P->tasks.empty()) return 0;
+    return 1 + (needs_resolve(P->cfg, P->nn, false, (int)P->groups.size(), P->jend) ? 1 : 0);
+}
 
 // Device-resident launch (capturable in a CUDA graph): ipart = G6I[], jpred = G6PredJ[],
 // out = G6Out[] indexed by absolute i (acc, jerk, pot final; key = -2/r_soft of the nearest
@@ -1071,6 +1095,8 @@ PGB_EXPORT int pgb6_plan_launch(pgb6_plan* P, const void* ipart, const void* jpr
     int slots = sm_count(g_device) * occupancy(P->cfg, P->ff, P->nn, false);
     int grid = a.ntasks < slots ? a.ntasks : slots;
     PGB_CUDA_OR(g_err, LIB, launch_kernel(P->cfg, P->ff, P->nn, false, grid, a, s), return PGB_ERR_CUDA);
+    PGB_CUDA_OR(g_err, LIB, launch_resolve(P->cfg, P->ff, P->nn, false, (int)P->groups.size(), a, s),
+                return PGB_ERR_CUDA);
     // completion marker for pgb6_plan_update (none for a launch captured into a CUDA graph)
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     PGB_CUDA_OR(g_err, LIB, cudaStreamIsCapturing(s, &cap), return PGB_ERR_CUDA);
@@ -1434,6 +1460,7 @@ PGB_EXPORT int pgb6_force_noalloc(const void* ipart, int ni, const void* jpred, 
     a.jn = nj;
     int grid = ntasks < slots ? ntasks : slots;
     PGB_CUDA_OR(g_err, LIB, launch_kernel(cfg, ff, nn, false, grid, a, s), return PGB_ERR_CUDA);
+    PGB_CUDA_OR(g_err, LIB, launch_resolve(cfg, ff, nn, false, nch > 1 ? (int)itiles : 0, a, s), return PGB_ERR_CUDA);
     return PGB_OK;
 }
 

@@ -69,6 +69,10 @@ __host__ __device__ inline void store_pos(Pos3& p, double x, double y, double z,
     }
 }
 
+// jadr of a split i-tile's result before g6_resolve_kernel: the start of the j-tile that holds
+// the nearest neighbour, with this bit set (j addresses stay below it; -1: no candidate).
+constexpr int G6_NN_TILE = 1 << 30;
+
 // Per-i result (final or partial).  key/jadr: nearest-neighbour key and j address.
 struct __align__(16) G6Out {
     double ax, ay, az;
@@ -565,11 +569,10 @@ __device__ __forceinline__ double2 word_zero(bool w3) {
 // the R group sums are added in group order through shared memory W (NT words).  The order is
 // fixed for a given (NT, nw, nrows): deterministic.  finish: write the final scaled result (acc,
 // jerk x -1/8, pot x 1/2) instead of the raw sum.  dst (same word indexing) may be row 0 itself:
-// every word is read before it is written.  nnk (optional, with wbeg = 0): the summed (key,
-// address) word of row i also into nnk[i].
+// every word is read before it is written.
 template <int NT>
 __device__ __forceinline__ void reduce_rows(const G6Out* base, size_t stride, int nrows, int wbeg, int nw,
-                                            G6Out* dst, bool finish, double2* W, double* nnk = nullptr) {
+                                            G6Out* dst, bool finish, double2* W) {
     // row groups: as many as the threads allow, but no more than the rows and at most 8 (their
     // sums are combined serially)
     const int R = (2 * nw <= NT) ? min(min(NT / nw, nrows), 8) : 1;
@@ -624,7 +627,6 @@ __device__ __forceinline__ void reduce_rows(const G6Out* base, size_t stride, in
             s0.x *= w3 ? 0.5 : -0.125;
             if (!w3) s0.y *= -0.125;
         }
-        if (nnk && w3) nnk[f >> 2] = s0.y;
         out[f] = s0;
     }
 }
@@ -927,16 +929,17 @@ __device__ __forceinline__ void g6_task(const G6Args& A, const Task& T, unsigned
     if constexpr (TILEMIN) {
         // the address of each i's nearest neighbour: the first j of its best tile with that key
         // (the j-paired form reads its i-record again rather than keep it in registers).  A task
-        // of a split j-range leaves the start of its best tile instead: the group's reduction
-        // keeps the best (key, tile start) over the chunks -- the same winner as over addresses,
-        // the chunks being consecutive j-ranges -- and g6_resolve_nn looks up that one tile per i
-        // (one lookup per i instead of one per i and chunk).
-        const bool defer = T.group >= 0 && !A.partial_only;
+        // of a split j-range leaves the start of its best tile instead, marked G6_NN_TILE: the
+        // group's reduction keeps the best (key, tile start) over the chunks -- the same winner
+        // as over addresses, the chunks being consecutive j-ranges -- and g6_resolve_kernel
+        // looks up that one tile per i after the launch (one lookup per i instead of one per i
+        // and chunk, spread over the whole GPU instead of the CTA that completes the group).
+        const bool defer = T.group >= 0 && !A.partial_only && A.jn < G6_NN_TILE;
 #pragma unroll
         for (int k = 0; k < IPT; k++) {
             const int li = slot + k * ISL;
             if (defer) {
-                if (ktile[k] >= 0) kadr[k] = T.j0 + ktile[k];
+                if (ktile[k] >= 0) kadr[k] = (T.j0 + ktile[k]) | G6_NN_TILE;
             } else if (li < T.ni && ktile[k] >= 0) {
                 if constexpr (USE_JP) {
                     const G6I P = A.ipart[T.i0 + li];
@@ -990,23 +993,6 @@ constexpr int g6_min_ctas() {
     return (!JPE && IPT == 2) ? (NT <= 128 ? 1 : 512 / NT) : 0;   // 256 threads: <= 128 registers, 2 CTAs
 }
 
-// The nearest neighbours of a reduced split group whose tasks left tile starts (g6_task):
-// nnk[li] = the group's best (key, tile start) of i li; the first j of that tile with the key,
-// looked up from the predicted j-set, goes into out[i].jadr.  Threads take the group's i in
-// turn, so the lookups run side by side.
-template <int NT, bool FF>
-__device__ __forceinline__ void g6_resolve_nn(const G6Args& A, const Group& G, const double* nnk) {
-    __syncthreads();   // nnk written by the reduction's threads
-    for (int li = threadIdx.x; li < G.ni; li += NT) {
-        const long long w = __double_as_longlong(nnk[li]);
-        const int tile = (int)(w >> 32);
-        if (tile < 0) continue;   // no candidate (address -1)
-        const float key = __int_as_float((int)(w & 0xffffffffLL));
-        const G6I P = A.ipart[G.i0 + li];
-        A.out[G.i0 + li].jadr = g6_rescan<FF>(A.jpred, tile, min(NT, A.jn - tile), P.p, P.id, A.eps2, key);
-    }
-}
-
 template <int NT, int IPT, int JL, bool FF, bool NN, bool NBL, int JP = 0>
 __global__ void __launch_bounds__(NT, g6_min_ctas<NT, IPT, JP && FF && !NBL && (IPT == 2 || IPT == 4) && JL == 1>())
     g6_kernel(const G6Args A) {
@@ -1023,12 +1009,6 @@ __global__ void __launch_bounds__(NT, g6_min_ctas<NT, IPT, JP && FF && !NBL && (
         if (T.group < 0 || A.partial_only) continue;
         const Group G = A.groups ? A.groups[T.group] : regular_group(A, T.group);
         double2* W = reinterpret_cast<double2*>(smem);
-        // the tile-minimum nearest-neighbour search leaves tile starts in split groups' rows
-        constexpr bool TILEMIN = NN && !NBL && IPT % 2 == 0;
-        double* nnk = TILEMIN ? reinterpret_cast<double*>(smem + NT * sizeof(double2)) : nullptr;
-        static_assert(!TILEMIN || NT * sizeof(double2) + NT * IPT * sizeof(double) <=
-                                      (size_t)g6_smem_bytes<NT, IPT, JP && FF && !NBL && (IPT == 2 || IPT == 4) && JL == 1>(),
-                      "reduction scratch and nearest-neighbour words fit the j-tile buffer");
         const int B = bundle_size(G.nchunk, A.bundle_counters != nullptr);
         if (B < G.nchunk) {
             // two levels: the last CTA of each bundle of B consecutive chunks sums the bundle's
@@ -1042,14 +1022,61 @@ __global__ void __launch_bounds__(NT, g6_min_ctas<NT, IPT, JP && FF && !NBL && (
             const int nb = (G.nchunk + B - 1) / B;
             if (!group_arrive(A.group_counters, T.group, nb, &s_flag)) continue;
             reduce_rows<NT>(A.partial + (size_t)G.slot0 * A.itile, (size_t)B * A.itile, nb, 0, 4 * G.ni, A.out + G.i0, true,
-                            W, nnk);
+                            W);
         } else {
             if (!group_arrive(A.group_counters, T.group, G.nchunk, &s_flag)) continue;
             reduce_rows<NT>(A.partial + (size_t)G.slot0 * A.itile, (size_t)A.itile, G.nchunk, 0, 4 * G.ni, A.out + G.i0,
-                            true, W, nnk);
+                            true, W);
         }
-        if constexpr (TILEMIN) g6_resolve_nn<NT, FF>(A, G, nnk);
     }
+}
+
+// The nearest-neighbour addresses of split i-tiles (the tasks' deferred lookups, see g6_task):
+// for every result row of a split group whose jadr carries G6_NN_TILE, the first j of the
+// marked tile (ntile records, bounded by A.jn) whose key equals the row's key.  G6_RES_LANES
+// threads per row each scan ntile / G6_RES_LANES records with all their loads in flight at once
+// (one L2 round trip for a 128-record tile), and the smallest match wins.  Block b covers the
+// 128 / G6_RES_LANES rows of group b / (itile / rows per block) from row (b % that) x rows.
+constexpr int G6_RES_LANES = 16;
+
+template <bool FF>
+__global__ void __launch_bounds__(128) g6_resolve_kernel(const G6Args A, int ngroups, int ntile) {
+    constexpr int RPB = 128 / G6_RES_LANES;   // rows per block
+    const int per_group = (A.itile + RPB - 1) / RPB;
+    const int g = blockIdx.x / per_group;
+    if (g >= ngroups) return;
+    const Group G = A.groups ? A.groups[g] : regular_group(A, g);
+    const int li = (blockIdx.x % per_group) * RPB + (int)(threadIdx.x / G6_RES_LANES);
+    const int q = threadIdx.x % G6_RES_LANES;
+    int tile = -1;
+    float key = 0.f;
+    if (li < G.ni && G.nchunk > 1) {
+        const G6Out& o = A.out[G.i0 + li];
+        const int a = o.jadr;
+        if (a >= 0 && (a & G6_NN_TILE)) {
+            tile = a & (G6_NN_TILE - 1);
+            key = o.key;
+        }
+    }
+    int found = 0x7fffffff;
+    if (tile >= 0) {
+        const int per = (ntile + G6_RES_LANES - 1) / G6_RES_LANES;
+        const int b = tile + q * per, e = min(min(b + per, tile + ntile), A.jn);
+        const G6I P = A.ipart[G.i0 + li];
+        for (int j0 = b; j0 < e && found == 0x7fffffff; j0 += 8) {
+            G6PredJ J[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++)
+                if (j0 + u < e) J[u] = A.jpred[j0 + u];
+#pragma unroll
+            for (int u = 7; u >= 0; u--)
+                if (j0 + u < e && g6_key<FF>(J[u], P.p, P.id, A.eps2) == key) found = j0 + u;
+        }
+    }
+    // the smallest match of the row's lanes (consecutive lanes of one warp)
+#pragma unroll
+    for (int m = 1; m < G6_RES_LANES; m <<= 1) found = min(found, __shfl_xor_sync(0xffffffffu, found, m));
+    if (tile >= 0 && q == 0) A.out[G.i0 + li].jadr = found == 0x7fffffff ? -1 : found;
 }
 
 }  // namespace pgb
