@@ -292,7 +292,7 @@ int pick_cfg(long long ni_max) {
 // about 4 tasks per resident CTA, chunks of at least 128 j, at most 512 chunks per i-tile
 // (their partial rows are summed by the cooperative reduction of the group's last CTA).
 long long plan_items(std::vector<Task>& tasks, std::vector<Group>& groups, int& rows, int nitem, const int* items,
-                     int cfg, bool ff, bool nn, bool nbl) {
+                     int cfg, bool ff, bool nn, bool nbl, int nch_fixed = 0) {
     int slots = sm_count(g_device) * occupancy(cfg, ff, nn, nbl);
     int itile = cfg_itile(cfg);
     long long work = 0;
@@ -312,9 +312,10 @@ long long plan_items(std::vector<Task>& tasks, std::vector<Group>& groups, int& 
         int ni = items[4 * k + 1], nj = items[4 * k + 3];
         long long jc;
         if (nitem == 1) {
-            // one item of equal tasks: the chunk count that minimises the wave quantisation
+            // one item of equal tasks: the chunk count that minimises the wave quantisation, or
+            // the autotuner's (nch_fixed)
             long long itiles = (ni + itile - 1) / itile;
-            int nch = best_nch(itiles, nj, slots, (int)maxch);
+            int nch = nch_fixed > 0 ? nch_fixed : best_nch(itiles, nj, slots, (int)maxch);
             jc = (nj + nch - 1) / nch;
         } else {
             jc = per_task / itile;
@@ -329,6 +330,27 @@ long long plan_items(std::vector<Task>& tasks, std::vector<Group>& groups, int& 
         return (long long)a.ni * a.nj > (long long)b.ni * b.nj;
     });
     return inter;
+}
+
+// The chunk counts the autotuner tries for a single item besides the wave model's choice m:
+// m x 3/4, 5/4, 3/2, and the counts whose chunks are whole 128-record j-tiles (nj / nch a
+// multiple of 128) between m/2 and 2m.  Measured on the largest Hermite calls, the time moves
+// by up to 5 % from one count to the next (the persistent CTAs' last wave; counts whose chunks
+// are whole tiles were within 1 % of the best and never bimodal), which the model cannot predict.
+std::vector<int> chunk_candidates(int m, int nj, int maxch) {
+    std::vector<int> c;
+    auto add = [&](long long v) {
+        const long long hi = std::max<long long>(1, std::min<long long>(maxch, nj / 128));
+        v = std::max<long long>(1, std::min<long long>(v, hi));
+        if (std::find(c.begin(), c.end(), (int)v) == c.end()) c.push_back((int)v);
+    };
+    add(m);
+    add((3LL * m + 2) / 4);
+    add((5LL * m + 2) / 4);
+    add((3LL * m + 1) / 2);
+    for (long long n = std::max(1, m / 2); n <= 2LL * m; n++)
+        if (nj % n == 0 && (nj / n) % 128 == 0) add(n);
+    return c;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -950,7 +972,10 @@ namespace {
 // pgb6_plan_tune.  The shape key buckets the item count, the largest i and j counts (powers of
 // two) and the variant flags, so plans of the same shape reuse a measured choice.
 std::mutex g_tune_mu;
-std::vector<std::pair<long long, int>> g_tune;
+struct Tuned {
+    int cfg, nch;   // nch 0: the wave model's chunk count
+};
+std::vector<std::pair<long long, Tuned>> g_tune;
 
 int ilog2up(long long v) {
     int k = 0;
@@ -968,21 +993,21 @@ long long shape_key(int nitem, const int* items, bool ff, bool nn) {
            ((long long)ilog2up(njmax + 1) << 8) | (ff ? 2 : 0) | (nn ? 1 : 0);
 }
 
-int tuned_cfg(long long key) {
+Tuned tuned_cfg(long long key) {
     std::lock_guard<std::mutex> g(g_tune_mu);
     for (auto& e : g_tune)
         if (e.first == key) return e.second;
-    return -1;
+    return Tuned{-1, 0};
 }
 
-void set_tuned(long long key, int cfg) {
+void set_tuned(long long key, Tuned t) {
     std::lock_guard<std::mutex> g(g_tune_mu);
     for (auto& e : g_tune)
         if (e.first == key) {
-            e.second = cfg;
+            e.second = t;
             return;
         }
-    g_tune.emplace_back(key, cfg);
+    g_tune.emplace_back(key, t);
 }
 }  // namespace
 
@@ -1000,6 +1025,7 @@ struct pgb6_plan {
     std::vector<int> items;    // the work-item table, kept for re-planning (autotuning)
     int jend = 0;              // the items' largest j_offset + j_count (the j records they read)
     long long shape_key = 0;   // autotune cache key of this work-item table
+    int nch = 0;               // a single item's chunk count (0: the wave model's, see plan_items)
     std::vector<Task> tasks;
     std::vector<Group> groups;
     int rows = 0;
@@ -1035,9 +1061,10 @@ PGB_EXPORT int pgb6_plan_create(pgb6_plan** out, int nitem, const int* items, in
     P->items.assign(items, items + 4 * (size_t)nitem);
     P->jend = items_jend(nitem, items);
     P->shape_key = shape_key(nitem, items, P->ff, P->nn);
-    int tuned = tuned_cfg(P->shape_key);
-    P->cfg = tuned >= 0 ? tuned : pick_cfg(nitem > 1 ? std::max<long long>(nimax, total_i / 4) : nimax);
-    P->interactions = plan_items(P->tasks, P->groups, P->rows, nitem, items, P->cfg, P->ff, P->nn, false);
+    const Tuned tuned = tuned_cfg(P->shape_key);
+    P->cfg = tuned.cfg >= 0 ? tuned.cfg : pick_cfg(nitem > 1 ? std::max<long long>(nimax, total_i / 4) : nimax);
+    P->nch = tuned.cfg >= 0 ? tuned.nch : 0;
+    P->interactions = plan_items(P->tasks, P->groups, P->rows, nitem, items, P->cfg, P->ff, P->nn, false, P->nch);
     cudaStream_t s = nullptr;
     bool ok = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess;
     ok = ok && P->st.stage(s, P->tasks, P->groups, P->rows, ITILE_MAX, (const G6I*)nullptr, 0) == cudaSuccess;
@@ -1118,6 +1145,7 @@ PGB_EXPORT int pgb6_plan_set_config(pgb6_plan* P, int cfg) {
     }
     if (!ensure_device()) return PGB_ERR_NOGPU;
     P->cfg = cfg;
+    P->nch = 0;
     const int nitem = (int)(P->items.size() / 4);
     P->tasks.clear();
     P->groups.clear();
@@ -1154,9 +1182,11 @@ PGB_EXPORT int pgb6_plan_update(pgb6_plan* P, int nitem, const int* items) {
     P->items.assign(items, items + 4 * (size_t)nitem);
     P->jend = items_jend(nitem, items);
     P->shape_key = shape_key(nitem, items, P->ff, P->nn);
+    const Tuned tuned = tuned_cfg(P->shape_key);
+    P->nch = (tuned.cfg == P->cfg) ? tuned.nch : 0;
     P->tasks.clear();
     P->groups.clear();
-    P->interactions = plan_items(P->tasks, P->groups, P->rows, nitem, items, P->cfg, P->ff, P->nn, false);
+    P->interactions = plan_items(P->tasks, P->groups, P->rows, nitem, items, P->cfg, P->ff, P->nn, false, P->nch);
     if (P->launched) PGB_CUDA_OR(g_err, LIB, cudaEventSynchronize(P->launched), return PGB_ERR_CUDA);
     cudaStream_t s = nullptr;
     bool ok = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess;
@@ -1171,10 +1201,12 @@ PGB_EXPORT int pgb6_plan_update(pgb6_plan* P, int nitem, const int* items) {
 }
 
 // Autotuner: launches the plan with every kernel configuration (threads per CTA x i per
-// thread x j-lanes) on the caller's data, keeps the fastest (CUDA-event time, best of 2 after a
-// warm-up launch), re-stages the plan with it and records it for plans of the same shape.
-// Returns the chosen configuration index; *best_ms (optional) receives its launch time.
-// Overwrites `out`.  Not capturable (it synchronises the stream).
+// thread x j-lanes) on the caller's data -- a plan of one item also with the chunk counts of
+// chunk_candidates for its three fastest configurations -- keeps the fastest (CUDA-event time,
+// the median of three launches after a warm-up launch, so that a shape whose time alternates
+// between launches is judged by its usual time), re-stages the plan with it and records it for
+// plans of the same shape.  Returns the chosen configuration index; *best_ms (optional)
+// receives its launch time.  Overwrites `out`.  Not capturable (it synchronises the stream).
 PGB_EXPORT int pgb6_plan_tune(pgb6_plan* P, const void* ipart, const void* jpred, double eps2, void* out,
                               void* stream, float* best_ms) {
     if (!P || !ipart || !jpred || !out) {
@@ -1186,42 +1218,73 @@ PGB_EXPORT int pgb6_plan_tune(pgb6_plan* P, const void* ipart, const void* jpred
     cudaEvent_t e0, e1;
     PGB_CUDA_OR(g_err, LIB, cudaEventCreate(&e0), return -1);
     PGB_CUDA_OR(g_err, LIB, cudaEventCreate(&e1), return -1);
-    int nitem = (int)(P->items.size() / 4);
-    int best = P->cfg;
-    float best_t = 1e30f;
-    for (int cfg = 0; cfg < NCFG; cfg++) {
+    const int nitem = (int)(P->items.size() / 4);
+    // one (configuration, chunk count): the median of three timed launches after a warm-up
+    auto time_plan = [&](int cfg, int nch, float* t) -> bool {
         P->tasks.clear();
         P->groups.clear();
         P->cfg = cfg;
-        plan_items(P->tasks, P->groups, P->rows, nitem, P->items.data(), cfg, P->ff, P->nn, false);
-        if (P->st.stage(s, P->tasks, P->groups, P->rows, ITILE_MAX, (const G6I*)nullptr, 0) != cudaSuccess) break;
-        float t = 1e30f;
+        P->nch = nch;
+        plan_items(P->tasks, P->groups, P->rows, nitem, P->items.data(), cfg, P->ff, P->nn, false, nch);
+        if (P->st.stage(s, P->tasks, P->groups, P->rows, ITILE_MAX, (const G6I*)nullptr, 0) != cudaSuccess) return false;
+        if (pgb6_plan_launch(P, ipart, jpred, eps2, out, stream) != PGB_OK) return false;
+        float ts[3];
         for (int rep = 0; rep < 3; rep++) {
             cudaEventRecord(e0, s);
-            if (pgb6_plan_launch(P, ipart, jpred, eps2, out, stream) != PGB_OK) break;
+            if (pgb6_plan_launch(P, ipart, jpred, eps2, out, stream) != PGB_OK) return false;
             cudaEventRecord(e1, s);
-            cudaEventSynchronize(e1);
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, e0, e1);
-            if (rep > 0 && ms < t) t = ms;
+            if (cudaEventSynchronize(e1) != cudaSuccess) return false;
+            cudaEventElapsedTime(&ts[rep], e0, e1);
         }
-        if (t < best_t) {
-            best_t = t;
-            best = cfg;
+        std::sort(ts, ts + 3);
+        *t = ts[1];
+        return true;
+    };
+    std::vector<std::pair<float, int>> by_cfg;
+    for (int cfg = 0; cfg < NCFG; cfg++) {
+        float t;
+        if (!time_plan(cfg, 0, &t)) break;
+        by_cfg.emplace_back(t, cfg);
+    }
+    std::sort(by_cfg.begin(), by_cfg.end());
+    Tuned best{P->cfg, 0};
+    float best_t = 1e30f;
+    if (!by_cfg.empty()) {
+        best = Tuned{by_cfg[0].second, 0};
+        best_t = by_cfg[0].first;
+    }
+    if (nitem == 1 && P->items[1] > 0 && P->items[3] > 0) {
+        static const int maxch = env_int("PGB_G6_MAXCHUNKS", 512, 1, 4096);
+        const int ni = P->items[1], nj = P->items[3];
+        for (size_t r = 0; r < by_cfg.size() && r < 3; r++) {
+            const int cfg = by_cfg[r].second;
+            const int itile = cfg_itile(cfg);
+            const int slots = sm_count(g_device) * occupancy(cfg, P->ff, P->nn, false);
+            const int m = best_nch((ni + itile - 1) / itile, nj, slots, maxch);
+            for (int nch : chunk_candidates(m, nj, maxch)) {
+                if (nch == m) continue;   // timed above
+                float t;
+                if (!time_plan(cfg, nch, &t)) break;
+                if (t < best_t) {
+                    best_t = t;
+                    best = Tuned{cfg, nch};
+                }
+            }
         }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     P->tasks.clear();
     P->groups.clear();
-    P->cfg = best;
-    plan_items(P->tasks, P->groups, P->rows, nitem, P->items.data(), best, P->ff, P->nn, false);
+    P->cfg = best.cfg;
+    P->nch = best.nch;
+    plan_items(P->tasks, P->groups, P->rows, nitem, P->items.data(), best.cfg, P->ff, P->nn, false, best.nch);
     PGB_CUDA_OR(g_err, LIB, P->st.stage(s, P->tasks, P->groups, P->rows, ITILE_MAX, (const G6I*)nullptr, 0),
                 return -1);
     PGB_CUDA_OR(g_err, LIB, cudaStreamSynchronize(s), return -1);
     set_tuned(P->shape_key, best);
     if (best_ms) *best_ms = best_t;
-    return best;
+    return best.cfg;
 }
 
 PGB_EXPORT void pgb6_plan_destroy(pgb6_plan* P) {
