@@ -60,8 +60,8 @@ G5_CFG_NAMES = ["128x4", "256x2", "512x2", "1024x1", "384x2", "128x2", "128x1", 
                 "1024x1 j-paired", "256x1 j-paired"]   # pgb5 configurations (threads x i/thread)
 PROFILED_TRAFFIC = {
     # the largest Hermite call by the configuration that runs it (6: 128x2 j-paired, 2: 128x2 i-paired)
-    "hermite": {"bytes": 6_463_232 + 5_087_488,
-                "source": "profiles/g6_kernel_hermite_65536x65536.md (128x2 j-paired)"},
+    "hermite": {"bytes": 6_564_864 + 13_965_568,
+                "source": "profiles/g6_kernel_hermite_65536x65536.md (128x2 j-paired, 15 chunks)"},
     "hermite_cfg9": {"bytes": 6_554_880 + 4_392_192,
                      "source": "profiles/g6_kernel_hermite_65536x65536.md (128x2 j-paired, stage-ordered)"},
     "hermite_cfg2": {"bytes": 6_578_944 + 17_873_152,
@@ -496,6 +496,7 @@ def hermite_batched(args, pgb, g6, wl, sub, calls, dev, s, ff, tune, steps, warm
         with torch.cuda.stream(s):
             step_launches()
         s.synchronize()
+    tuned_chunks = {str(cnt): int(g6.L.pgb6_plan_chunks(plans[c])) for c, _, cnt in sorted(live, key=lambda t: t[2])}
     graph = torch.cuda.CUDAGraph()
     with torch.cuda.graph(graph, stream=s):
         step_launches()
@@ -548,7 +549,8 @@ def hermite_batched(args, pgb, g6, wl, sub, calls, dev, s, ff, tune, steps, warm
     kern_s = sum(ms for ms, _, _ in fms) / 1e3
     kern_pairs = sum(p for _, p, _ in fms)
     big = max(fms, key=lambda e: e[1])
-    return dict(step_ms=step_ms, clk=clk, tuned=tuned, graph=graph, plans=plans, d_ptcl=d_ptcl, d_irec=d_irec,
+    return dict(step_ms=step_ms, clk=clk, tuned=tuned, tuned_chunks=tuned_chunks, graph=graph, plans=plans,
+                d_ptcl=d_ptcl, d_irec=d_irec,
                 d_out=d_out, ptcl=ptcl, irec=irec, nrow=nrow, kern_s=kern_s, kern_pairs=kern_pairs,
                 big_pairs=big[1], big_ms=big[0], big_call=big[2], step=step,
                 launches_per_step=sum(1 + g6.L.pgb6_plan_kernels(plans[c]) for c, _, _ in live))
@@ -779,6 +781,7 @@ def run_hermite(args, pgb, ws, rank, local):
                              "end_to_end": round(e2e_b / e2e_val, 2)},
         "gpu_launches": args.steps * B["launches_per_step"],
         "autotune": {str(k): int(v) for k, v in sorted(B["tuned"].items())},
+        "autotune_chunks": B["tuned_chunks"],
         "clocks": clk,
         "cpu_baseline": cpu,
     }

@@ -111,6 +111,8 @@ void pgb6_plan_destroy(pgb6_plan *plan);
 long long pgb6_plan_interactions(const pgb6_plan *plan);
 int  pgb6_plan_tasks(const pgb6_plan *plan);
 int  pgb6_plan_config(const pgb6_plan *plan);
+/* j-chunks per i-tile of a one-item plan (1: unsplit; 0: a plan of several items) */
+int  pgb6_plan_chunks(const pgb6_plan *plan);
 /* kernels one pgb6_plan_launch issues (the force kernel, plus the nearest-neighbour lookup kernel
  * of split i-tiles when the plan's configuration defers them) */
 int  pgb6_plan_kernels(const pgb6_plan *plan);

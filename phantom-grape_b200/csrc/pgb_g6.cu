@@ -315,7 +315,8 @@ long long plan_items(std::vector<Task>& tasks, std::vector<Group>& groups, int& 
             // one item of equal tasks: the chunk count that minimises the wave quantisation, or
             // the autotuner's (nch_fixed)
             long long itiles = (ni + itile - 1) / itile;
-            int nch = nch_fixed > 0 ? nch_fixed : best_nch(itiles, nj, slots, (int)maxch);
+            static const int forced_nch = env_int("PGB_G6_NCH", 0, 0, 4096);   // profiling: a pinned count
+            int nch = forced_nch > 0 ? forced_nch : nch_fixed > 0 ? nch_fixed : best_nch(itiles, nj, slots, (int)maxch);
             jc = (nj + nch - 1) / nch;
         } else {
             jc = per_task / itile;
@@ -1083,6 +1084,11 @@ PGB_EXPORT int pgb6_plan_create(pgb6_plan** out, int nitem, const int* items, in
 PGB_EXPORT long long pgb6_plan_interactions(const pgb6_plan* P) { return P ? P->interactions : 0; }
 PGB_EXPORT int pgb6_plan_tasks(const pgb6_plan* P) { return P ? (int)P->tasks.size() : 0; }
 PGB_EXPORT int pgb6_plan_config(const pgb6_plan* P) { return P ? P->cfg : -1; }
+// j-chunks per i-tile of a one-item plan (1: the j-range unsplit); 0 for plans of several items.
+PGB_EXPORT int pgb6_plan_chunks(const pgb6_plan* P) {
+    if (!P || P->items.size() != 4 || P->tasks.empty()) return 0;
+    return P->groups.empty() ? 1 : (int)(P->tasks.size() / P->groups.size());
+}
 // Kernels one pgb6_plan_launch issues: the force kernel, and the nearest-neighbour lookups of
 // split i-tiles when the plan's configuration defers them.
 PGB_EXPORT int pgb6_plan_kernels(const pgb6_plan* P) {

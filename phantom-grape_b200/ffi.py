@@ -268,6 +268,7 @@ class G6(_ErrMixin):
         _sig(L, "pgb6_plan_tasks", [vp], C.c_int)
         _sig(L, "pgb6_plan_config", [vp], C.c_int)
         _sig(L, "pgb6_plan_kernels", [vp], C.c_int)
+        _sig(L, "pgb6_plan_chunks", [vp], C.c_int)
         _sig(L, "pgb6_plan_update", [vp, C.c_int, ip], C.c_int)
         _sig(L, "pgb6_plan_set_config", [vp, C.c_int], C.c_int)
         _sig(L, "pgb6_plan_tune", [vp, vp, vp, C.c_double, vp, vp, C.POINTER(C.c_float)], C.c_int)
