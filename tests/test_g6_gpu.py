@@ -364,3 +364,56 @@ def test_every_configuration_vs_fp64(g6, state):
                 g6.set_abort(True)
                 g6.plan_destroy(plan)
     assert ncfg >= 10
+
+
+def test_tuned_chunk_count_and_deferred_lookups(g6, state):
+    """A one-item plan (the batched path of one block-step call) after pgb6_plan_tune, which picks
+    the kernel configuration and, for one item, the j-chunk count: results against the FP64
+    oracle (acc / jerk / pot rms relative <= 1e-6; the nearest neighbour's address identical
+    wherever the FP64 first and second neighbours are separated, and never a deferred-lookup tile
+    mark), the reported chunk and kernel counts (split i-tiles of the tile-minimum configurations
+    add the lookup kernel), and a new plan of the same shape taking the tuned configuration and
+    chunk count."""
+    import torch
+    st = state
+    n = len(st.mass)
+    xp, vp = O.g6_predict(st.t_now, st.pos, st.vel, st.acc2, st.jrk6, st.tj)
+    vpf = vp.astype(np.float32).astype(np.float64)
+    mf = st.mass.astype(np.float32).astype(np.float64)
+    act = np.sort(W.Rng(91).permutation(n)[:4096]).astype(np.int32)
+    ref = O.g6_force(xp[act], vpf[act], st.idx[act], np.float32(st.eps2), xp, vpf, mf, st.idx)
+    dev = torch.device("cuda")
+    d_i = torch.from_numpy(pgb.ffi.g6_irecords(xp[act], vp[act], st.idx[act]).view(np.uint8)).to(dev)
+    d_j = torch.from_numpy(pgb.ffi.g6_jrecords(xp, vp, st.mass, st.idx).view(np.uint8)).to(dev)
+    d_o = torch.zeros(len(act) * pgb.ffi.G6OUT.itemsize, dtype=torch.uint8, device=dev)
+    items = np.array([[0, len(act), 0, n]], np.int32)
+    ipt = [1, 1, 2, 1, 4, 2, 2, 2, 4, 2]   # i per thread of each configuration (pgb_g6.cu CFG_IPT)
+    plan = g6.plan_create(items, nn=True)
+    plan2 = None
+    try:
+        cfg, ms = g6.plan_tune(plan, d_i.data_ptr(), d_j.data_ptr(), st.eps2, d_o.data_ptr(), 0)
+        chunks = g6.L.pgb6_plan_chunks(plan)
+        kernels = g6.L.pgb6_plan_kernels(plan)
+        assert g6.L.pgb6_plan_config(plan) == cfg and ms > 0
+        assert 1 <= chunks <= n // 128
+        assert kernels == (2 if chunks > 1 and ipt[cfg] % 2 == 0 else 1), (cfg, chunks, kernels)
+        d_o.fill_(0xFF)
+        g6.plan_launch(plan, d_i.data_ptr(), d_j.data_ptr(), st.eps2, d_o.data_ptr(), 0)
+        torch.cuda.synchronize()
+        o = d_o.cpu().numpy().view(pgb.ffi.G6OUT)
+        acc = np.stack([o["ax"], o["ay"], o["az"]], 1)
+        jrk = np.stack([o["jx"], o["jy"], o["jz"]], 1)
+        assert rms(rel(acc, ref["acc"])) <= 1e-6
+        assert rms(rel(jrk, ref["jrk"])) <= 1e-6
+        assert rms((o["pot"] - ref["pot"]) / np.abs(ref["pot"])) <= 1e-6
+        jadr = o["jadr"]
+        assert np.all((jadr >= 0) & (jadr < n))   # resolved addresses: no (1 << 30) tile mark
+        clear = ref["r2nn2"] / ref["r2nn"] - 1.0 > 1e-5
+        assert np.array_equal(st.idx[jadr][clear], ref["nnb"][clear])
+        plan2 = g6.plan_create(items, nn=True)
+        assert g6.L.pgb6_plan_config(plan2) == cfg
+        assert g6.L.pgb6_plan_chunks(plan2) == chunks
+    finally:
+        g6.plan_destroy(plan)
+        if plan2 is not None:
+            g6.plan_destroy(plan2)
