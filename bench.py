@@ -341,6 +341,8 @@ class Driver:
         L.g6drv_schedule2.argtypes = [vp, C.c_int, C.c_int, ip, ip, dp, dp, dp, C.c_double, C.c_int, C.c_int, ip, ip,
                                       dp, dp, dp, dp, dp, dp, ip, dp, dp, dp, ip, C.POINTER(C.c_float)]
         L.g6drv_schedule2.restype = C.c_double
+        L.g6drv_call_time.argtypes = [vp, C.c_int, C.c_int, C.c_int, dp, dp, ip, C.c_double]
+        L.g6drv_call_time.restype = C.c_double
         L.g5drv_open.argtypes = [C.c_char_p]
         L.g5drv_open.restype = vp
         L.g5drv_direct.argtypes = [vp, C.c_int, dp, dp, C.c_double, dp, dp]
@@ -1720,6 +1722,40 @@ def run_reference(args, pgb, ws, rank):
 
 # ----------------------------------------------------------------------------------------
 
+def run_api_floor(pgb):
+    """The drop-in API's per-call wall time for several (i, j) shapes on the C2 state (C caller:
+    drivers/pgb_drivers.c g6drv_call_time, g6calc_firsthalf + g6calc_lasthalf2p, best of three runs
+    of 2000 calls) and the floor of a launch and its completion (lib/libpgbpeak.so
+    pgb_peak_launch_floor: empty kernels waited for by stream synchronisation or by a polled
+    flag in mapped host memory)."""
+    g6 = pgb.ffi.G6()
+    g6.L.g6_open(0)
+    wl = hermite_workload(pgb, g6)
+    st, n = wl["st"], wl["n"]
+    drv = Driver(pgb)
+    h = drv.g6_open(pgb.ffi.lib_path("libpg6.so"))
+    drv.g6_set_j(h, st)
+    g6.L.g6_set_ti(0, float(wl["t_calls"][0]))
+    sel = np.arange(0, 48 * 97, 97) % n
+    xi, vi = np.ascontiguousarray(st.pos[sel]), np.ascontiguousarray(st.vel[sel])
+    idi = np.ascontiguousarray(st.idx[sel], np.int32)
+    calls = {}
+    for ni, nj in ((48, n), (16, n), (1, n), (48, 16384), (48, 1024), (1, 128)):
+        t = drv.L.g6drv_call_time(h, ni, nj, 2000, Driver.p(xi), Driver.p(vi), Driver.p(idi, C.c_int), st.eps2)
+        calls[f"{ni}x{nj}"] = round(t * 1e6, 2)
+    L = C.CDLL(pgb.ffi.lib_path("libpgbpeak.so"), mode=os.RTLD_LOCAL | os.RTLD_NOW)
+    L.pgb_peak_launch_floor.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_double)]
+    floor = {}
+    for kind, name in ((0, "stream_sync"), (1, "flag_poll")):
+        for grid in (1, 264):
+            us = C.c_double()
+            if L.pgb_peak_launch_floor(kind, grid, 3000, None, C.byref(us)) == 0:
+                floor[f"{name}_grid{grid}"] = round(us.value, 2)
+    return {"api_call_us": calls, "empty_launch_us": floor, "npipes": int(g6.L.g6_npipes()),
+            "how": "µs per drop-in call (firsthalf + lasthalf2p) by i x j shape on the C2 state, host clock; "
+                   "empty-kernel launch + completion for comparison"}
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -1748,6 +1784,9 @@ def main():
                     help="profiling target (--workload bh): build the GPU tree of the workload twice and exit")
     ap.add_argument("--profile-api", action="store_true",
                     help="profiling target: four full-size drop-in API calls (48 i x N j) and exit")
+    ap.add_argument("--api-floor", action="store_true",
+                    help="per-call time of the GRAPE-6 drop-in API by call shape, beside the launch and "
+                         "completion floor of empty kernels; one JSON line")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -1757,6 +1796,9 @@ def main():
         line = run_reference(args, pgb, ws, rank)
         if line is not None:
             print(json.dumps(line), flush=True)
+        return
+    if args.api_floor:
+        print(json.dumps(run_api_floor(pgb)), flush=True)
         return
     dist = dist_init(ws, local)
     runner = {"hermite": run_hermite, "direct": run_direct, "clusters": run_clusters, "treepm": run_treepm,

@@ -16,6 +16,7 @@
 // buffer or a small internal one.  Times are CUDA-event times on the caller's stream.
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <cstdio>
 
 #include "pgb_g6_kernels.cuh"
@@ -303,5 +304,52 @@ PGB_EXPORT int pgb_peak_g6_loop(int form, int passes, void* stream, double* gpai
     if (gpairs) *gpairs = pairs / (t * 1e-3) / 1e9;
     if (ms) *ms = t;
     if (regs) *regs = fa.numRegs;
+    return 0;
+}
+
+// The floor of a small call: `n` launches of an empty kernel (`grid` CTAs of 128 threads) on the
+// caller's stream, each waited for before the next -- kind 0: cudaStreamSynchronize; kind 1: the
+// kernel sets a flag in mapped host memory (after a system-scope fence) that the host polls, as
+// the drop-in API's small calls do.  *us = microseconds per launch (host clock), after 100
+// untimed launches.
+__global__ void floor_kernel(volatile unsigned* done, unsigned seq) {
+    __syncthreads();
+    if (done && threadIdx.x == 0 && blockIdx.x == 0) {
+        __threadfence_system();
+        done[0] = seq;
+    }
+}
+
+PGB_EXPORT int pgb_peak_launch_floor(int kind, int grid, int n, void* stream, double* us) {
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned* hflag = nullptr;
+    unsigned* dflag = nullptr;
+    if (kind == 1) {
+        if (cudaHostAlloc((void**)&hflag, 64, cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess) return -1;
+        if (cudaHostGetDevicePointer((void**)&dflag, hflag, 0) != cudaSuccess) return -1;
+        hflag[0] = 0;
+    }
+    auto one = [&](unsigned seq) {
+        if (kind == 1) {
+            floor_kernel<<<grid, 128, 0, s>>>(dflag, seq);
+            // bounded: a launch that never signals ends the measurement with an error
+            for (long it = 0; ((volatile unsigned*)hflag)[0] != seq; it++)
+                if (it > (1L << 30)) return false;
+        } else {
+            floor_kernel<<<grid, 128, 0, s>>>(nullptr, seq);
+            if (cudaStreamSynchronize(s) != cudaSuccess) return false;
+        }
+        return true;
+    };
+    unsigned seq = 1;
+    bool ok = true;
+    for (int k = 0; k < 100 && ok; k++) ok = one(seq++);
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int k = 0; k < n && ok; k++) ok = one(seq++);
+    const auto t1 = std::chrono::steady_clock::now();
+    cudaStreamSynchronize(s);
+    if (hflag) cudaFreeHost(hflag);
+    if (!ok || cudaGetLastError() != cudaSuccess) return -1;
+    if (us) *us = std::chrono::duration<double, std::micro>(t1 - t0).count() / n;
     return 0;
 }

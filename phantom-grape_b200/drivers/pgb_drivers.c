@@ -92,6 +92,51 @@ double g6drv_set_j(void *handle, int n, const double *pos, const double *vel, co
     return now() - t0;
 }
 
+/* Seconds per drop-in call of one shape: `calls` x (g6calc_firsthalf + g6calc_lasthalf2p) for the
+ * first ni of the given i-particles against j-records [0, nj) of the j-memory (set before),
+ * after 100 untimed calls; the best of three runs. */
+double g6drv_call_time(void *handle, int ni, int nj, int calls, const double *xi, const double *vi, const int *idx,
+                       double eps2) {
+    g6api *a = (g6api *)handle;
+    if (ni < 1 || ni > a->npipes() || calls < 1) return -1.0;
+    int *pidx = (int *)malloc(sizeof(int) * ni);
+    double(*pos)[3] = malloc(sizeof(double) * 3 * ni);
+    double(*vel)[3] = malloc(sizeof(double) * 3 * ni);
+    double(*acc)[3] = malloc(sizeof(double) * 3 * ni);
+    double(*jrk)[3] = malloc(sizeof(double) * 3 * ni);
+    double *pot = (double *)malloc(sizeof(double) * ni), *h2 = (double *)calloc(ni, sizeof(double));
+    int *nnb = (int *)malloc(sizeof(int) * ni);
+    float *rnnb = (float *)malloc(sizeof(float) * ni);
+    for (int i = 0; i < ni; i++) {
+        pidx[i] = idx[i];
+        for (int c = 0; c < 3; c++) {
+            pos[i][c] = xi[3 * i + c];
+            vel[i][c] = vi[3 * i + c];
+        }
+    }
+    double best = 1e30;
+    for (int run = 0; run < 4; run++) {
+        const int n = run == 0 ? 100 : calls;
+        double t0 = now();
+        for (int k = 0; k < n; k++) {
+            a->firsthalf(0, nj, ni, pidx, pos, vel, acc, jrk, pot, eps2, h2);
+            a->lasthalf2p(0, nj, ni, pidx, pos, vel, eps2, h2, acc, jrk, pot, nnb, rnnb);
+        }
+        double t = (now() - t0) / n;
+        if (run > 0 && t < best) best = t;
+    }
+    free(pidx);
+    free(pos);
+    free(vel);
+    free(acc);
+    free(jrk);
+    free(pot);
+    free(h2);
+    free(nnb);
+    free(rnnb);
+    return best;
+}
+
 /* One pass over `ncalls` block steps.  Call c uses time t_calls[c] and the active particles
  * set_idx[set_off[c] .. set_off[c+1]) whose predicted positions / velocities are
  * xi/vi[set_off[c] ..].  With `resend`, the active particles' j-records (from pos..tj) are
