@@ -215,6 +215,55 @@ __global__ void k_node_scan(Nodes N, int b, int e, int level, int nleaf, const i
     nkids[v - b] = splits(N.count[v], level, nleaf) ? nk : 0;
 }
 
+// The same for a level of few nodes (the top of the tree, where a node has up to thousands of
+// tiles): one CTA per node, HT_NT threads each over a contiguous run of its tiles -- the runs'
+// octant sums, their exclusive scan in thread order through shared memory, then each thread's
+// tiles' offsets.  Integer sums in tile order: the same offsets as k_node_scan.
+__global__ void __launch_bounds__(HT_NT) k_node_scan_cta(Nodes N, int b, int level, int nleaf, const int* tile_off,
+                                                         const int* tcount, int* tbase, int* ccount, int* nkids) {
+    __shared__ int part[HT_NT][8];
+    __shared__ int total[8];
+    const int v = b + blockIdx.x;
+    const int t0 = tile_off[v - b], t1 = tile_off[v - b + 1];
+    const int per = (t1 - t0 + HT_NT - 1) / HT_NT;
+    const int a = min(t0 + (int)threadIdx.x * per, t1), z = min(a + per, t1);
+    int run[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int t = a; t < z; t++)
+#pragma unroll
+        for (int o = 0; o < 8; o++) run[o] += tcount[8 * t + o];
+#pragma unroll
+    for (int o = 0; o < 8; o++) part[threadIdx.x][o] = run[o];
+    __syncthreads();
+    if (threadIdx.x < 8) {
+        // exclusive scan of column o over the threads, in thread order
+        const int o = threadIdx.x;
+        int acc = 0;
+        for (int q = 0; q < HT_NT; q++) {
+            const int c = part[q][o];
+            part[q][o] = acc;
+            acc += c;
+        }
+        total[o] = acc;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int o = 0; o < 8; o++) run[o] = part[threadIdx.x][o];
+    for (int t = a; t < z; t++)
+#pragma unroll
+        for (int o = 0; o < 8; o++) {
+            tbase[8 * t + o] = run[o];
+            run[o] += tcount[8 * t + o];
+        }
+    if (threadIdx.x == 0) {
+        int nk = 0;
+        for (int o = 0; o < 8; o++) {
+            ccount[8 * (v - b) + o] = total[o];
+            nk += total[o] > 0;
+        }
+        nkids[v - b] = splits(N.count[v], level, nleaf) ? nk : 0;
+    }
+}
+
 // Children of the level's splitting nodes, appended from index e + kid_off[v - b].
 __global__ void k_children(Nodes N, int b, int e, int level, int nleaf, const int* ccount, const int* kid_off) {
     const int v = b + blockIdx.x * blockDim.x + threadIdx.x;
@@ -776,8 +825,12 @@ bool build(pgbt_tree* T, const double* xh, const double* mh) {
         k_tile_nodes<<<nblk(cnt, 256), 256, 0, s>>>(b, e, tile_off.p, tile_node.p);
         k_octants<<<tgrid, HT_NT, 0, s>>>(N, tile_node.p, tile_off.p, b, tile_off.p + cnt, T->x.p, T->perm.p, oct.p,
                                          tcount.p);
-        k_node_scan<<<nblk(cnt, 128), 128, 0, s>>>(N, b, e, L, T->nleaf, tile_off.p, tcount.p, tbase.p, ccount.p,
-                                                  nkids.p);
+        // levels of few nodes (whose nodes hold many tiles): one CTA per node; deeper: a thread
+        if (cnt <= 512)
+            k_node_scan_cta<<<cnt, HT_NT, 0, s>>>(N, b, L, T->nleaf, tile_off.p, tcount.p, tbase.p, ccount.p, nkids.p);
+        else
+            k_node_scan<<<nblk(cnt, 128), 128, 0, s>>>(N, b, e, L, T->nleaf, tile_off.p, tcount.p, tbase.p, ccount.p,
+                                                      nkids.p);
         if (!excl_scan<int>(nkids.p, cnt, kid_off.p, s, stmp)) return false;
         int nnew = 0;
         if (!to_host(&nnew, kid_off.p + cnt, 1, s)) return false;
