@@ -528,22 +528,69 @@ constexpr int HT_UNITS = 64;
 // 64, 13.0 with 256 threads)
 constexpr int HT_WALK_NT = 128;
 
-struct ListOut {
-    int* pl;        // point-mass entries (nullptr: count only)
-    int* cl;        // cell entries
-    long long a, b; // entries so far
-    __device__ __forceinline__ void part(int k) {
-        if (pl) pl[a] = k;
-        a++;
+// The count walk's output: the numbers of point-mass and cell entries.
+struct ListCount {
+    long long a = 0, b = 0;
+    __device__ __forceinline__ void part(int) { a++; }
+    __device__ __forceinline__ void cell(int) { b++; }
+    __device__ __forceinline__ void flush() {}
+};
+
+// One list of the fill walk, written in aligned 16-byte chunks: the entries of the chunk that
+// holds the next address wait in v0..v3 (slot = address / 4 mod 4) and go out as one vector
+// store when its last slot is filled.  The first chunk's slots before the list's start, and the
+// last chunk's slots after its end, belong to the neighbouring units' lists: a partial chunk is
+// written entry by entry.  A lane stores one sector per four entries instead of one per entry.
+struct ChunkOut {
+    int* p; // address of the next entry
+    int s0; // first slot of the current chunk that belongs to this list
+    int v0 = 0, v1 = 0, v2 = 0, v3 = 0;
+    __device__ __forceinline__ static int slot(const int* q) {
+        return (int)((reinterpret_cast<unsigned long long>(q) >> 2) & 3);
     }
-    __device__ __forceinline__ void cell(int w) {
-        if (cl) cl[b] = w;
-        b++;
+    __device__ __forceinline__ explicit ChunkOut(int* q) : p(q), s0(slot(q)) {}
+    __device__ __forceinline__ void push(int k) {
+        const int s = slot(p);
+        v0 = s == 0 ? k : v0;
+        v1 = s == 1 ? k : v1;
+        v2 = s == 2 ? k : v2;
+        v3 = s == 3 ? k : v3;
+        if (s == 3) {
+            int* c = p - 3;
+            if (s0 == 0) {
+                *reinterpret_cast<int4*>(c) = make_int4(v0, v1, v2, v3);
+            } else {
+                if (s0 <= 1) c[1] = v1;
+                if (s0 <= 2) c[2] = v2;
+                c[3] = v3;
+            }
+            s0 = 0;
+        }
+        p++;
+    }
+    // the pending entries: slots s0 .. slot(p) - 1 of the current chunk
+    __device__ __forceinline__ void flush() {
+        const int s = slot(p);
+        int* c = p - s;
+        if (s0 <= 0 && 0 < s) c[0] = v0;
+        if (s0 <= 1 && 1 < s) c[1] = v1;
+        if (s0 <= 2 && 2 < s) c[2] = v2;
+    }
+};
+
+struct ListFill {
+    ChunkOut P, C; // point-mass and cell entries
+    __device__ __forceinline__ void part(int k) { P.push(k); }
+    __device__ __forceinline__ void cell(int w) { C.push(w); }
+    __device__ __forceinline__ void flush() {
+        P.flush();
+        C.flush();
     }
 };
 
 // A node the walk reaches: its particle (one particle), itself as a cell (theta^2 d^2 >
 // side^2), its particles (at most nleaf or no children) -- or false: the walk descends.
+template <class ListOut>
 __device__ __forceinline__ bool take_node(const WalkNode& C, int w, const double g[3], double h, double th2,
                                           ListOut& L) {
     if (C.kind == WK_ONE) {
@@ -566,6 +613,7 @@ __device__ __forceinline__ bool take_node(const WalkNode& C, int w, const double
 // subtree (w + nsub), a node descended into by its first child (w + 1), and the walk ends at
 // the end of v's subtree -- the same nodes in the same order as a recursive walk over the
 // children, one node record read per step.
+template <class ListOut>
 __device__ void walk_below(const Tree& T, const WalkNode* __restrict__ wn, int v, const double g[3], double h,
                            double th2, ListOut& L) {
     (void)T;
@@ -579,6 +627,7 @@ __device__ void walk_below(const Tree& T, const WalkNode* __restrict__ wn, int v
 // Work unit u of the group with node gv.  The root: the group's list is the root as one cell
 // when the root passes the opening test (group_list of the host builder), the root's particles
 // when it has at most nleaf particles or no children; unit 0 emits either.
+template <class ListOut>
 __device__ void unit_walk(const Tree& T, const WalkNode* __restrict__ wn, int gv, int u, double th2, ListOut& L) {
     const double g[3] = {T.c[3 * gv], T.c[3 * gv + 1], T.c[3 * gv + 2]};
     const double h = T.half[gv];
@@ -613,7 +662,7 @@ __global__ void k_list_count(Tree T, const WalkNode* wn, const int* gnode, int n
     const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= (long long)ng * HT_UNITS) return;
     const int u = (int)(q / ng), g = (int)(q % ng);
-    ListOut L{nullptr, nullptr, 0, 0};
+    ListCount L;
     unit_walk(T, wn, gnode[g], u, th2, L);
     np[(long long)g * HT_UNITS + u] = L.a;
     nc[(long long)g * HT_UNITS + u] = L.b;
@@ -625,8 +674,9 @@ __global__ void k_list_fill(Tree T, const WalkNode* wn, const int* gnode, int ng
     if (q >= (long long)ng * HT_UNITS) return;
     const int u = (int)(q / ng), g = (int)(q % ng);
     const long long r = (long long)g * HT_UNITS + u;
-    ListOut L{pidx + uoffp[r], cidx + uoffc[r], 0, 0};
+    ListFill L{ChunkOut(pidx + uoffp[r]), ChunkOut(cidx + uoffc[r])};
     unit_walk(T, wn, gnode[g], u, th2, L);
+    L.flush();
 }
 
 // per-group offsets from the per-unit offsets (entry ng: the totals)
