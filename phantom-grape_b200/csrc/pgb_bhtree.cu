@@ -517,12 +517,16 @@ __device__ __forceinline__ double box_d2(const double* p, const double g[3], dou
 }
 
 // The interaction lists are made by HT_UNITS work units per group, so that the walks spread
-// over many threads: unit u = 8 o + o2 of a group produces the part of the group's list that
-// the host builder's depth-first walk (make_interaction_list) produces for the root's child o
-// when that child is taken whole (its particle, itself as a cell, or its particles: unit
-// o2 = 0 emits it) or, when the walk descends into it, for that child's child o2.  The units'
-// lists, concatenated in unit order, are the group's list.
-constexpr int HT_UNITS = 64;
+// over many threads: unit u, whose base-8 digits (o_1 .. o_D, most significant first) name a
+// node D levels below the root, produces the part of the group's list that the host builder's
+// depth-first walk (make_interaction_list) produces inside that node's subtree.  Where the walk
+// takes a node of level l < D whole (its particle, itself as a cell, or its particles), the unit
+// whose digits below l are zero emits it.  The units' lists, concatenated in unit order, are the
+// group's list.  Most of a group's list lies in the few units around the group itself, so the
+// depth sets how many threads share that work: at D = 2 the long walks of an N = 2^20 tree fill
+// ~3 warps per SM.
+constexpr int HT_UNIT_LEVELS = 2;
+constexpr int HT_UNITS = 1 << (3 * HT_UNIT_LEVELS);
 // threads per block of the list walks: a block stays resident until its slowest walk ends, so
 // smaller blocks keep fewer finished warps idle (N = 2^22 build: 12.3 ms with 128, 12.7 with
 // 64, 13.0 with 256 threads)
@@ -532,6 +536,7 @@ constexpr int HT_WALK_NT = 128;
 struct ListCount {
     long long a = 0, b = 0;
     __device__ __forceinline__ void part(int) { a++; }
+    __device__ __forceinline__ void parts(int, int n) { a += n; }
     __device__ __forceinline__ void cell(int) { b++; }
     __device__ __forceinline__ void flush() {}
 };
@@ -568,6 +573,13 @@ struct ChunkOut {
         }
         p++;
     }
+    // the n consecutive entries k, k + 1, ...: pushed one by one up to a chunk boundary (where
+    // the chunk before has just gone out, or the list starts), then whole chunks stored directly
+    __device__ __forceinline__ void push_range(int k, int n) {
+        for (; n > 0 && slot(p) != 0; n--) push(k++);
+        for (; n >= 4; n -= 4, k += 4, p += 4) *reinterpret_cast<int4*>(p) = make_int4(k, k + 1, k + 2, k + 3);
+        for (; n > 0; n--) push(k++);
+    }
     // the pending entries: slots s0 .. slot(p) - 1 of the current chunk
     __device__ __forceinline__ void flush() {
         const int s = slot(p);
@@ -581,6 +593,7 @@ struct ChunkOut {
 struct ListFill {
     ChunkOut P, C; // point-mass and cell entries
     __device__ __forceinline__ void part(int k) { P.push(k); }
+    __device__ __forceinline__ void parts(int k, int n) { P.push_range(k, n); }
     __device__ __forceinline__ void cell(int w) { C.push(w); }
     __device__ __forceinline__ void flush() {
         P.flush();
@@ -602,7 +615,7 @@ __device__ __forceinline__ bool take_node(const WalkNode& C, int w, const double
         return true;
     }
     if (C.kind == WK_PARTS) {
-        for (int k = C.first; k < C.first + C.count; k++) L.part(k);
+        L.parts(C.first, C.count);
         return true;
     }
     return false;
@@ -637,45 +650,74 @@ __device__ void unit_walk(const Tree& T, const WalkNode* __restrict__ wn, int gv
         return;
     }
     if (R.kind != WK_SPLIT) {
-        if (u == 0)
-            for (int k = R.first; k < R.first + R.count; k++) L.part(k);
+        if (u == 0) L.parts(R.first, R.count);
         return;
     }
-    const int o = u >> 3, o2 = u & 7;
-    const int c1 = T.child[o];
-    if (c1 < 0) return;
-    const WalkNode C1 = wn[c1];
-    if (C1.kind != WK_SPLIT || dm(box_d2(C1.com, g, h), th2) > C1.side2) {
-        if (o2 == 0) take_node(C1, c1, g, h, th2, L);
-        return;
+    int v = 0; // a node the walk descends into
+#pragma unroll
+    for (int l = 1; l <= HT_UNIT_LEVELS; l++) {
+        const int below = 3 * (HT_UNIT_LEVELS - l);
+        const int c = T.child[8 * v + ((u >> below) & 7)];
+        if (c < 0) return;
+        const WalkNode C = wn[c];
+        if (l == HT_UNIT_LEVELS) {
+            if (!take_node(C, c, g, h, th2, L)) walk_below(T, wn, c, g, h, th2, L);
+            return;
+        }
+        if (C.kind != WK_SPLIT || dm(box_d2(C.com, g, h), th2) > C.side2) {
+            if ((u & ((1 << below) - 1)) == 0) take_node(C, c, g, h, th2, L);
+            return;
+        }
+        v = c;
     }
-    const int c2 = T.child[8 * c1 + o2];
-    if (c2 < 0) return;
-    if (!take_node(wn[c2], c2, g, h, th2, L)) walk_below(T, wn, c2, g, h, th2, L);
 }
 
-// Thread q takes unit q / ng of group q % ng: the lanes of a warp take the same unit of
-// neighbouring groups, whose walks are alike (a group's longest unit is the one around it).
+// The unit whose node (HT_UNIT_LEVELS levels below the root) holds the group's node gv: its
+// octant digits from the centres, as the partition assigns them (a point above a node's centre
+// on an axis goes to the upper half).  A group above that depth takes the digits down to itself
+// and zeros below.
+__device__ __forceinline__ int home_unit(const Tree& T, int gv) {
+    const double cx = T.c[3 * gv], cy = T.c[3 * gv + 1], cz = T.c[3 * gv + 2];
+    int u = 0, v = 0;
+#pragma unroll
+    for (int l = 0; l < HT_UNIT_LEVELS; l++) {
+        int o = 0;
+        if (v >= 0 && v != gv) {
+            o = ((cx > T.c[3 * v]) << 2) | ((cy > T.c[3 * v + 1]) << 1) | (int)(cz > T.c[3 * v + 2]);
+            v = T.child[8 * v + o];
+        }
+        u = (u << 3) | o;
+    }
+    return u;
+}
+
+// Thread q takes rank q / ng of group q % ng: the lanes of a warp take the same rank of
+// neighbouring groups, whose walks are alike.  Rank r is unit r ^ home: rank 0 is the unit
+// around the group (the longest walk), ranks 1-7 its siblings, then the units under the other
+// children of the root -- so the long walks start first and the grid's last blocks are short.
 // Counts and offsets are stored group-major (g * HT_UNITS + u), the order of the lists.
-__global__ void k_list_count(Tree T, const WalkNode* wn, const int* gnode, int ng, double th2, long long* np,
-                             long long* nc) {
+__global__ void __launch_bounds__(HT_WALK_NT) k_list_count(Tree T, const WalkNode* wn, const int* gnode, int ng,
+                                                          double th2, long long* np, long long* nc) {
     const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= (long long)ng * HT_UNITS) return;
-    const int u = (int)(q / ng), g = (int)(q % ng);
+    const int g = (int)(q % ng), gv = gnode[g];
+    const int u = (int)(q / ng) ^ home_unit(T, gv);
     ListCount L;
-    unit_walk(T, wn, gnode[g], u, th2, L);
+    unit_walk(T, wn, gv, u, th2, L);
     np[(long long)g * HT_UNITS + u] = L.a;
     nc[(long long)g * HT_UNITS + u] = L.b;
 }
 
-__global__ void k_list_fill(Tree T, const WalkNode* wn, const int* gnode, int ng, double th2, const long long* uoffp,
-                            const long long* uoffc, int* pidx, int* cidx) {
+__global__ void __launch_bounds__(HT_WALK_NT) k_list_fill(Tree T, const WalkNode* wn, const int* gnode, int ng,
+                                                         double th2, const long long* uoffp, const long long* uoffc,
+                                                         int* pidx, int* cidx) {
     const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= (long long)ng * HT_UNITS) return;
-    const int u = (int)(q / ng), g = (int)(q % ng);
+    const int g = (int)(q % ng), gv = gnode[g];
+    const int u = (int)(q / ng) ^ home_unit(T, gv);
     const long long r = (long long)g * HT_UNITS + u;
     ListFill L{ChunkOut(pidx + uoffp[r]), ChunkOut(cidx + uoffc[r])};
-    unit_walk(T, wn, gnode[g], u, th2, L);
+    unit_walk(T, wn, gv, u, th2, L);
     L.flush();
 }
 
