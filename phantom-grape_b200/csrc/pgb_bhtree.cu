@@ -26,13 +26,15 @@
 //    the cell's centre of mass to the group's cube).
 //
 // Construction is level by level: at each level the particles of every splitting node are
-// cut into tiles of HT_TILE; one kernel computes octants and per-tile octant counts, one thread
+// cut into tiles (of HT_TILE for a CTA, or of HT_TILE_W for a warp where the level's nodes are
+// many and small); one kernel computes octants and per-tile octant counts, a CTA, warp or thread
 // per node scans its tiles in order (tile offsets, child sizes), children are allocated with a
 // prefix sum, and a scatter kernel places each particle at child start + tile offset + its rank
 // among the tile's particles of the same octant (warp ballots) -- a stable partition, as the
 // host's counting sort.  Pre-order numbers follow from subtree sizes; moments are computed
 // bottom-up one level at a time; lists by 64 threads per group (one per grandchild of the root,
-// each with an explicit stack), a counting pass, a prefix sum and a filling pass.
+// each walking the pre-order node array without a stack), a counting pass, a prefix sum and a
+// filling pass.
 #include "pgb_common.cuh"
 
 using namespace pgb;
@@ -43,8 +45,11 @@ const char* LIB = "libpgbtree";
 ErrorSlot g_err;
 
 constexpr int HT_MAXDEPTH = 40;   // the host builder's depth cap
-constexpr int HT_TILE = 2048;     // particles per tile of the partition kernels
+constexpr int HT_TILE = 2048;     // particles per tile of the partition kernels (a CTA per tile)
+constexpr int HT_TILE_W = 512;    // the same for a warp per tile
 constexpr int HT_NT = 256;        // threads per CTA of the tile kernels
+constexpr int HT_SMALL_LEVEL = 4096;     // levels of at least this many nodes: a warp per tile
+constexpr int HT_WARP_SCAN_LEVEL = 131072; // levels of 513 up to this many nodes: a warp per node
 
 // ---- device helpers ---------------------------------------------------------------------
 
@@ -158,30 +163,38 @@ __device__ __forceinline__ bool splits(int count, int level, int nleaf) {
 }
 
 // Tiles of a level's splitting nodes: ntile[v - b] for nodes [b, e).
-__global__ void k_ntiles(Nodes N, int b, int e, int level, int nleaf, int* ntile) {
+__global__ void k_ntiles(Nodes N, int b, int e, int level, int nleaf, int tile, int* ntile) {
     const int v = b + blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= e) return;
     const int c = N.count[v];
-    ntile[v - b] = splits(c, level, nleaf) ? (c + HT_TILE - 1) / HT_TILE : 0;
+    ntile[v - b] = splits(c, level, nleaf) ? (c + tile - 1) / tile : 0;
 }
 
-__global__ void k_tile_nodes(int b, int e, const int* tile_off, int* tile_node) {
-    const int v = b + blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= e) return;
-    for (int t = tile_off[v - b]; t < tile_off[v - b + 1]; t++) tile_node[t] = v;
+// The node of every tile: the last node i of the level whose first tile tile_off[i] <= t (a
+// node without tiles has the same tile_off as the next node, so the last such is the owner).
+__global__ void k_tile_nodes(int b, int cnt, const int* tile_off, const int* ntiles, int* tile_node) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= *ntiles) return;
+    int lo = 0, hi = cnt - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (tile_off[mid] <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    tile_node[t] = b + lo;
 }
 
 // Octant of every particle of a tile and the tile's octant counts.
 __global__ void __launch_bounds__(HT_NT) k_octants(Nodes N, const int* tile_node, const int* tile_off, int b,
-                                                   const int* ntiles, const double* x, const int* perm,
-                                                   unsigned char* oct, int* tcount) {
+                                                   const int* ntiles, int tile, const double* x,
+                                                   const int* perm, unsigned char* oct, int* tcount) {
     __shared__ int cnt[8];
     const int t = blockIdx.x;
     if (t >= *ntiles) return;
     const int v = tile_node[t];
     const int lt = t - tile_off[v - b];
-    const int k0 = N.first[v] + lt * HT_TILE;
-    const int k1 = min(N.first[v] + N.count[v], k0 + HT_TILE);
+    const int k0 = N.first[v] + lt * tile;
+    const int k1 = min(N.first[v] + N.count[v], k0 + tile);
     if (threadIdx.x < 8) cnt[threadIdx.x] = 0;
     __syncthreads();
     const double cx = N.c[3 * v], cy = N.c[3 * v + 1], cz = N.c[3 * v + 2];
@@ -193,6 +206,37 @@ __global__ void __launch_bounds__(HT_NT) k_octants(Nodes N, const int* tile_node
     }
     __syncthreads();
     if (threadIdx.x < 8) tcount[8 * t + threadIdx.x] = cnt[threadIdx.x];
+}
+
+// The same with one warp per tile, for levels of many small nodes (a tile of a few dozen
+// particles would leave most of a CTA idle): lane o < 8 keeps octant o's count.
+__global__ void __launch_bounds__(HT_NT) k_octants_w(Nodes N, const int* tile_node, const int* tile_off, int b,
+                                                     const int* ntiles, int tile, const double* x,
+                                                     const int* perm, unsigned char* oct, int* tcount) {
+    const int t = (int)((blockIdx.x * (unsigned)HT_NT + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (t >= *ntiles) return; // whole warps
+    const int v = tile_node[t];
+    const int lt = t - tile_off[v - b];
+    const int k0 = N.first[v] + lt * tile;
+    const int k1 = min(N.first[v] + N.count[v], k0 + tile);
+    const double cx = N.c[3 * v], cy = N.c[3 * v + 1], cz = N.c[3 * v + 2];
+    int cnt = 0;
+    for (int r0 = k0; r0 < k1; r0 += 32) {
+        const int k = r0 + lane;
+        int o = 8;
+        if (k < k1) {
+            const double* p = x + 3 * (size_t)perm[k];
+            o = ((p[0] > cx) << 2) | ((p[1] > cy) << 1) | (p[2] > cz);
+            oct[k] = (unsigned char)o;
+        }
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const unsigned m = __ballot_sync(0xffffffffu, o == q);
+            if (lane == q) cnt += __popc(m);
+        }
+    }
+    if (lane < 8) tcount[8 * t + lane] = cnt;
 }
 
 // Per splitting node: its tiles' offsets within each octant (in tile order), the child sizes
@@ -264,6 +308,45 @@ __global__ void __launch_bounds__(HT_NT) k_node_scan_cta(Nodes N, int b, int lev
     }
 }
 
+// The same for levels of a few thousand nodes (a dense centre leaves some of them hundreds of
+// tiles): one warp per node, each lane over a contiguous run of its tiles, the runs' octant
+// sums scanned across the lanes with shuffles.
+__global__ void __launch_bounds__(256) k_node_scan_warp(Nodes N, int b, int e, int level, int nleaf,
+                                                        const int* tile_off, const int* tcount, int* tbase,
+                                                        int* ccount, int* nkids) {
+    const int v = b + (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (v >= e) return; // whole warps
+    const int t0 = tile_off[v - b], t1 = tile_off[v - b + 1];
+    const int per = (t1 - t0 + 31) >> 5;
+    const int a = min(t0 + lane * per, t1), z = min(a + per, t1);
+    int run[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int t = a; t < z; t++)
+#pragma unroll
+        for (int o = 0; o < 8; o++) run[o] += tcount[8 * t + o];
+    int nk = 0;
+#pragma unroll
+    for (int o = 0; o < 8; o++) {
+        int x = run[o];
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, d);
+            if (lane >= d) x += y;
+        }
+        const int total = __shfl_sync(0xffffffffu, x, 31);
+        if (lane == 0) ccount[8 * (v - b) + o] = total;
+        nk += total > 0;
+        run[o] = x - run[o]; // exclusive
+    }
+    for (int t = a; t < z; t++)
+#pragma unroll
+        for (int o = 0; o < 8; o++) {
+            tbase[8 * t + o] = run[o];
+            run[o] += tcount[8 * t + o];
+        }
+    if (lane == 0) nkids[v - b] = splits(N.count[v], level, nleaf) ? nk : 0;
+}
+
 // Children of the level's splitting nodes, appended from index e + kid_off[v - b].
 __global__ void k_children(Nodes N, int b, int e, int level, int nleaf, const int* ccount, const int* kid_off) {
     const int v = b + blockIdx.x * blockDim.x + threadIdx.x;
@@ -292,8 +375,8 @@ __global__ void k_children(Nodes N, int b, int e, int level, int nleaf, const in
 // Stable scatter of a tile's particles to their children: child start + the tile's offset in
 // the octant + the particle's rank among the tile's earlier particles of the same octant.
 __global__ void __launch_bounds__(HT_NT) k_scatter(Nodes N, const int* tile_node, const int* tile_off, int b,
-                                                   const int* ntiles, const unsigned char* oct, const int* tbase,
-                                                   const int* perm, int* perm2) {
+                                                   const int* ntiles, int tile, const unsigned char* oct,
+                                                   const int* tbase, const int* perm, int* perm2) {
     __shared__ int wcnt[HT_NT / 32][8];
     __shared__ int run[8];
     __shared__ int cstart[8];
@@ -301,8 +384,8 @@ __global__ void __launch_bounds__(HT_NT) k_scatter(Nodes N, const int* tile_node
     if (t >= *ntiles) return;
     const int v = tile_node[t];
     const int lt = t - tile_off[v - b];
-    const int k0 = N.first[v] + lt * HT_TILE;
-    const int k1 = min(N.first[v] + N.count[v], k0 + HT_TILE);
+    const int k0 = N.first[v] + lt * tile;
+    const int k1 = min(N.first[v] + N.count[v], k0 + tile);
     const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
     if (threadIdx.x < 8) {
         run[threadIdx.x] = tbase[8 * t + threadIdx.x];
@@ -334,6 +417,43 @@ __global__ void __launch_bounds__(HT_NT) k_scatter(Nodes N, const int* tile_node
             run[threadIdx.x] += s;
         }
         __syncthreads();
+    }
+}
+
+// The same with one warp per tile: lane o < 8 keeps octant o's next destination (the child's
+// start + the tile's offset in the octant + the octant's particles so far), ranks within a
+// chunk of 32 from the octant's ballot.
+__global__ void __launch_bounds__(HT_NT) k_scatter_w(Nodes N, const int* tile_node, const int* tile_off, int b,
+                                                     const int* ntiles, int tile, const unsigned char* oct,
+                                                     const int* tbase, const int* perm, int* perm2) {
+    const int t = (int)((blockIdx.x * (unsigned)HT_NT + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (t >= *ntiles) return; // whole warps
+    const int v = tile_node[t];
+    const int lt = t - tile_off[v - b];
+    const int k0 = N.first[v] + lt * tile;
+    const int k1 = min(N.first[v] + N.count[v], k0 + tile);
+    int dst = 0;
+    if (lane < 8) {
+        const int w = N.child[8 * v + lane];
+        dst = (w >= 0 ? N.first[w] : 0) + tbase[8 * t + lane];
+    }
+    const unsigned below = (1u << lane) - 1u;
+    for (int r0 = k0; r0 < k1; r0 += 32) {
+        const int k = r0 + lane;
+        const bool in = k < k1;
+        const int o = in ? oct[k] : 8;
+        unsigned mine = 0;
+        int add = 0;
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const unsigned m = __ballot_sync(0xffffffffu, o == q);
+            if (o == q) mine = m;
+            if (lane == q) add = __popc(m);
+        }
+        const int base = __shfl_sync(0xffffffffu, dst, o & 7);
+        if (in) perm2[base + __popc(mine & below)] = perm[k];
+        dst += add;
     }
 }
 
@@ -890,11 +1010,11 @@ bool build(pgbt_tree* T, const double* xh, const double* mh) {
         PGB_CUDA_OR(g_err, LIB, cudaStreamSynchronize(s), return false);
     }
     // per-level scratch, sized once: a level has at most n nodes, at most n / (nleaf + 1) of
-    // them split, and their tiles number at most n / HT_TILE plus one per splitting node
+    // them split, and their tiles number at most n / tile plus one per splitting node
     DevBuf<int>&ntile = T->ntile, &tile_off = T->tile_off, &tile_node = T->tile_node, &tcount = T->tcount,
                 &tbase = T->tbase, &ccount = T->ccount, &nkids = T->nkids, &kid_off = T->kid_off;
     DevBuf<unsigned char>& oct = T->oct;
-    const size_t tcap = (size_t)n / HT_TILE + (size_t)n / ((size_t)T->nleaf + 1) + 2;
+    const size_t tcap = (size_t)n / HT_TILE_W + (size_t)n / ((size_t)T->nleaf + 1) + 2;
     PGB_CUDA_OR(g_err, LIB, oct.reserve((size_t)n), return false);
     PGB_CUDA_OR(g_err, LIB, ntile.reserve((size_t)n + 1), return false);
     PGB_CUDA_OR(g_err, LIB, tile_off.reserve((size_t)n + 1), return false);
@@ -909,17 +1029,29 @@ bool build(pgbt_tree* T, const double* xh, const double* mh) {
         const int b = lvl[L], e = lvl[L + 1], cnt = e - b;
         if (cnt <= 0) break;
         Nodes N = bfs(T);
-        k_ntiles<<<nblk(cnt, 256), 256, 0, s>>>(N, b, e, L, T->nleaf, ntile.p);
+        // a level of many nodes has small ones: a warp per tile of HT_TILE_W instead of a CTA
+        // per tile of HT_TILE
+        const bool small = cnt >= HT_SMALL_LEVEL;
+        const int tile = small ? HT_TILE_W : HT_TILE;
+        k_ntiles<<<nblk(cnt, 256), 256, 0, s>>>(N, b, e, L, T->nleaf, tile, ntile.p);
         if (!excl_scan<int>(ntile.p, cnt, tile_off.p, s, stmp)) return false;
         // the tile kernels run on a grid that covers every possible tile; the count itself
         // stays on the device (tile_off[cnt])
-        const unsigned tgrid = (unsigned)std::min<size_t>(tcap, (size_t)n / HT_TILE + (size_t)cnt + 2);
-        k_tile_nodes<<<nblk(cnt, 256), 256, 0, s>>>(b, e, tile_off.p, tile_node.p);
-        k_octants<<<tgrid, HT_NT, 0, s>>>(N, tile_node.p, tile_off.p, b, tile_off.p + cnt, T->x.p, T->perm.p, oct.p,
-                                         tcount.p);
-        // levels of few nodes (whose nodes hold many tiles): one CTA per node; deeper: a thread
+        const unsigned tgrid = (unsigned)std::min<size_t>(tcap, (size_t)n / tile + (size_t)cnt + 2);
+        k_tile_nodes<<<nblk(tgrid, 256), 256, 0, s>>>(b, cnt, tile_off.p, tile_off.p + cnt, tile_node.p);
+        if (small)
+            k_octants_w<<<nblk(tgrid, HT_NT / 32), HT_NT, 0, s>>>(N, tile_node.p, tile_off.p, b, tile_off.p + cnt,
+                                                                 tile, T->x.p, T->perm.p, oct.p, tcount.p);
+        else
+            k_octants<<<tgrid, HT_NT, 0, s>>>(N, tile_node.p, tile_off.p, b, tile_off.p + cnt, tile, T->x.p,
+                                             T->perm.p, oct.p, tcount.p);
+        // the tile scans: a CTA per node where a level has few nodes (the top, whose nodes hold
+        // many tiles), a warp per node below, a thread per node where the nodes are small
         if (cnt <= 512)
             k_node_scan_cta<<<cnt, HT_NT, 0, s>>>(N, b, L, T->nleaf, tile_off.p, tcount.p, tbase.p, ccount.p, nkids.p);
+        else if (cnt <= HT_WARP_SCAN_LEVEL)
+            k_node_scan_warp<<<nblk(cnt, 256 / 32), 256, 0, s>>>(N, b, e, L, T->nleaf, tile_off.p, tcount.p, tbase.p,
+                                                                ccount.p, nkids.p);
         else
             k_node_scan<<<nblk(cnt, 128), 128, 0, s>>>(N, b, e, L, T->nleaf, tile_off.p, tcount.p, tbase.p, ccount.p,
                                                       nkids.p);
@@ -934,8 +1066,12 @@ bool build(pgbt_tree* T, const double* xh, const double* mh) {
         if (nnew > 0) {
             PGB_CUDA_OR(g_err, LIB, cudaMemcpyAsync(T->perm2.p, T->perm.p, (size_t)n * sizeof(int),
                                                     cudaMemcpyDeviceToDevice, s), return false);
-            k_scatter<<<tgrid, HT_NT, 0, s>>>(N, tile_node.p, tile_off.p, b, tile_off.p + cnt, oct.p, tbase.p,
-                                             T->perm.p, T->perm2.p);
+            if (small)
+                k_scatter_w<<<nblk(tgrid, HT_NT / 32), HT_NT, 0, s>>>(N, tile_node.p, tile_off.p, b, tile_off.p + cnt,
+                                                                     tile, oct.p, tbase.p, T->perm.p, T->perm2.p);
+            else
+                k_scatter<<<tgrid, HT_NT, 0, s>>>(N, tile_node.p, tile_off.p, b, tile_off.p + cnt, tile, oct.p,
+                                                 tbase.p, T->perm.p, T->perm2.p);
             std::swap(T->perm.p, T->perm2.p);
             std::swap(T->perm.n, T->perm2.n);
         }
