@@ -661,52 +661,44 @@ struct ListCount {
     __device__ __forceinline__ void flush() {}
 };
 
-// One list of the fill walk, written in aligned 16-byte chunks: the entries of the chunk that
-// holds the next address wait in v0..v3 (slot = address / 4 mod 4) and go out as one vector
-// store when its last slot is filled.  The first chunk's slots before the list's start, and the
-// last chunk's slots after its end, belong to the neighbouring units' lists: a partial chunk is
-// written entry by entry.  A lane stores one sector per four entries instead of one per entry.
+// One list of the fill walk, written in aligned 16-byte chunks: the entries of the current chunk
+// wait in the thread's four staging slots in shared memory (slot j at sm[j * HT_WALK_NT], so that
+// the lanes' slots lie in distinct banks) and go out as one vector store when the last slot is
+// filled.  The first chunk's slots before the list's start, and the last chunk's slots after its
+// end, belong to the neighbouring units' lists: a partial chunk is written entry by entry.  A lane
+// stores one sector per four entries instead of one per entry.
 struct ChunkOut {
-    int* p; // address of the next entry
-    int s0; // first slot of the current chunk that belongs to this list
-    int v0 = 0, v1 = 0, v2 = 0, v3 = 0;
-    __device__ __forceinline__ static int slot(const int* q) {
-        return (int)((reinterpret_cast<unsigned long long>(q) >> 2) & 3);
+    int* c;  // the current chunk (16-byte aligned)
+    int* sm; // the staging slots
+    int s;   // the next entry's slot
+    int s0;  // the current chunk's first slot that belongs to this list
+    __device__ __forceinline__ ChunkOut(int* q, int* stage) : sm(stage) {
+        s = s0 = (int)((reinterpret_cast<unsigned long long>(q) >> 2) & 3);
+        c = q - s;
     }
-    __device__ __forceinline__ explicit ChunkOut(int* q) : p(q), s0(slot(q)) {}
-    __device__ __forceinline__ void push(int k) {
-        const int s = slot(p);
-        v0 = s == 0 ? k : v0;
-        v1 = s == 1 ? k : v1;
-        v2 = s == 2 ? k : v2;
-        v3 = s == 3 ? k : v3;
-        if (s == 3) {
-            int* c = p - 3;
-            if (s0 == 0) {
-                *reinterpret_cast<int4*>(c) = make_int4(v0, v1, v2, v3);
-            } else {
-                if (s0 <= 1) c[1] = v1;
-                if (s0 <= 2) c[2] = v2;
-                c[3] = v3;
-            }
-            s0 = 0;
+    __device__ __forceinline__ void out() {
+        if (s0 == 0) {
+            *reinterpret_cast<int4*>(c) = make_int4(sm[0], sm[HT_WALK_NT], sm[2 * HT_WALK_NT], sm[3 * HT_WALK_NT]);
+        } else {
+            for (int j = s0; j < 4; j++) c[j] = sm[j * HT_WALK_NT];
         }
-        p++;
+        c += 4;
+        s = s0 = 0;
+    }
+    __device__ __forceinline__ void push(int k) {
+        sm[s * HT_WALK_NT] = k;
+        if (++s == 4) out();
     }
     // the n consecutive entries k, k + 1, ...: pushed one by one up to a chunk boundary (where
     // the chunk before has just gone out, or the list starts), then whole chunks stored directly
     __device__ __forceinline__ void push_range(int k, int n) {
-        for (; n > 0 && slot(p) != 0; n--) push(k++);
-        for (; n >= 4; n -= 4, k += 4, p += 4) *reinterpret_cast<int4*>(p) = make_int4(k, k + 1, k + 2, k + 3);
+        for (; n > 0 && s != 0; n--) push(k++);
+        for (; n >= 4; n -= 4, k += 4, c += 4) *reinterpret_cast<int4*>(c) = make_int4(k, k + 1, k + 2, k + 3);
         for (; n > 0; n--) push(k++);
     }
-    // the pending entries: slots s0 .. slot(p) - 1 of the current chunk
+    // the pending entries: slots s0 .. s - 1 of the current chunk
     __device__ __forceinline__ void flush() {
-        const int s = slot(p);
-        int* c = p - s;
-        if (s0 <= 0 && 0 < s) c[0] = v0;
-        if (s0 <= 1 && 1 < s) c[1] = v1;
-        if (s0 <= 2 && 2 < s) c[2] = v2;
+        for (int j = s0; j < s; j++) c[j] = sm[j * HT_WALK_NT];
     }
 };
 
@@ -836,7 +828,8 @@ __global__ void __launch_bounds__(HT_WALK_NT) k_list_fill(Tree T, const WalkNode
     const int g = (int)(q % ng), gv = gnode[g];
     const int u = (int)(q / ng) ^ home_unit(T, gv);
     const long long r = (long long)g * HT_UNITS + u;
-    ListFill L{ChunkOut(pidx + uoffp[r]), ChunkOut(cidx + uoffc[r])};
+    __shared__ int stage[2][4][HT_WALK_NT];
+    ListFill L{ChunkOut(pidx + uoffp[r], &stage[0][0][threadIdx.x]), ChunkOut(cidx + uoffc[r], &stage[1][0][threadIdx.x])};
     unit_walk(T, wn, gv, u, th2, L);
     L.flush();
 }
