@@ -149,6 +149,15 @@ def pipe_peaks(pgb, stream_ptr=0):
             loop[name] = {"gpairs": round(gp.value, 1), "registers": rg.value}
     if loop:
         _PIPE_PEAKS["g6_pair_loop"] = loop
+    # the relative error of the kernels' scale q = -2/r over every float r2 in [1, 4): the MUFU
+    # estimate alone (the default build) and refined by the reference's Newton step
+    L.pgb_peak_rsqrt_error.argtypes = [C.c_void_p, dp, dp]
+    emax, erms = (C.c_double * 2)(), (C.c_double * 2)()
+    if L.pgb_peak_rsqrt_error(C.c_void_p(stream_ptr), emax, erms) == 0:
+        _PIPE_PEAKS["rsqrt_rel_error"] = {
+            "mufu": {"max": float(emax[0]), "rms": float(erms[0])},
+            "newton": {"max": float(emax[1]), "rms": float(erms[1])},
+            "how": "q = -2/r against FP64 for every float r2 in [1, 4) (lib/libpgbpeak.so pgb_peak_rsqrt_error)"}
     if rc2 == 0:
         _PIPE_PEAKS.update({"mufu_grsqrt_s": round(mg.value, 1), "mufu_ms": round(mms.value, 3),
                             "mufu_per_sm_clk": round(mg.value * 1e9 / SM_COUNT / ((clk.get("sm_mhz") or 1965.0) * 1e6), 2)})
@@ -731,6 +740,28 @@ def run_hermite(args, pgb, ws, rank, local):
         for p_ in B64["plans"].values():
             g6.plan_destroy(p_)
         del B64
+    # the reference's rsqrt form (the MUFU estimate refined by one Newton step,
+    # lib/libpg6_newton.so), same schedule, same timing
+    nline = None
+    if ws == 1 and not args.no_newton_line:
+        g6n = ffi.G6("libpg6_newton.so")
+        sn = torch.cuda.Stream(device=dev)
+        clkn = ClockSampler(local)
+        Bn = hermite_batched(args, pgb, g6n, wl, sub, calls, dev, sn, ff, not args.no_tune,
+                             max(3, min(args.steps, 10)), args.warmup, flush, ws, nrows, dist, clocks=clkn)
+        vn = float(wl["pairs"]) * len(Bn["step_ms"]) / (sum(Bn["step_ms"]) / 1e3) / 1e9
+        nline = {"value": round(vn, 2), "unit": "Gint/s", "steps": len(Bn["step_ms"]),
+                 "largest_launch_ms": round(Bn["big_ms"], 3),
+                 "roofline_frac": round(Bn["big_pairs"] * 60 / (Bn["big_ms"] / 1e3) / 1e12 / fp32_tf, 4),
+                 "rsqrt": "rsqrt.approx + one Newton step, q = y (r2 y^2 - 3) (the reference's form, "
+                          "gravity.c:341-346), lib/libpg6_newton.so",
+                 "clocks": Bn["clk"]}
+        if rank == 0 and not args.no_cpu_baseline:
+            rowsn = Bn["d_out"][:Bn["nrow"]].cpu().numpy().reshape(-1).view(ffi.G6OUT)
+            nline["fp64_check"] = hermite_fp64_check(pgb, wl, sub, calls, rowsn, " (Newton-refined rsqrt)")
+        for p_ in Bn["plans"].values():
+            g6n.plan_destroy(p_)
+        del Bn
     for p_ in B["plans"].values():
         g6.plan_destroy(p_)
     del B["graph"]
@@ -752,7 +783,8 @@ def run_hermite(args, pgb, ws, rank, local):
                                "each call's active set; results all-gathered (NCCL) inside the timed step")
                   if ws > 1 else "one GPU",
                   "graph": "64 x (predict + persistent force launch) in one CUDA graph",
-                  "relative_coordinates": "double-float (hi+lo FP32)" if ff else "FP64 subtract + F2F"},
+                  "relative_coordinates": "double-float (hi+lo FP32)" if ff else "FP64 subtract + F2F",
+                  "rsqrt": "rsqrt.approx alone, q = -2 y (lib/libpg6.so)"},
         "frac_fp32": round(value * 1e9 * 60 / 1e12 / fp32_tf, 4),
         "roofline": {"bound": "fp32", "achieved": round(achieved_tf, 2), "peak": round(fp32_tf, 2),
                      "unit": "TFLOP/s", "frac": round(achieved_tf / fp32_tf, 4),
@@ -766,7 +798,8 @@ def run_hermite(args, pgb, ws, rank, local):
                      "mufu_peak_grsqrt_s": _PIPE_PEAKS.get("mufu_grsqrt_s"),
                      "mufu_per_sm_clk": _PIPE_PEAKS.get("mufu_per_sm_clk"),
                      "fp32_mix_tflops": _PIPE_PEAKS.get("fp32_mix_tflops"),
-                     "pair_loop_ceiling": pair_loop_ceiling(fp32_tf, B["big_pairs"] / (B["big_ms"] / 1e3) / 1e9)},
+                     "pair_loop_ceiling": pair_loop_ceiling(fp32_tf, B["big_pairs"] / (B["big_ms"] / 1e3) / 1e9),
+                     "rsqrt_rel_error": _PIPE_PEAKS.get("rsqrt_rel_error")},
         "e2e": {"value": round(e2e_val, 2), "unit": "Gint/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "api": "GRAPE-6 drop-in (g6_set_ti, g6calc_firsthalf, "
                 "g6calc_lasthalf2p per npipes chunk, g6_set_j_particle of the active set), host buffers",
@@ -789,6 +822,8 @@ def run_hermite(args, pgb, ws, rank, local):
     }
     if f64line:
         line["f64_positions"] = f64line
+    if nline:
+        line["newton_rsqrt"] = nline
     return line
 
 
@@ -858,6 +893,9 @@ def _line(args, ws, metric, value, t_step, pairs, flop, workload, dtype, achieve
     }
     if extra:
         line.update(extra)
+    nl = line.get("newton_rsqrt")
+    if nl and "achieved_tflops" in nl:
+        nl["roofline_frac"] = round(nl["achieved_tflops"] / peak_tf, 4)
     return line
 
 
@@ -903,6 +941,23 @@ def run_direct(args, pgb, ws, rank, local):
     pairs = n * n
     value = reduce_sum(float(pairs) * len(ts), ws, dev) / t_max / 1e9
     achieved = pairs * len(ts) * 38 / t_local / 1e12
+    # the reference's rsqrt form (the MUFU estimate refined by one Newton step,
+    # lib/libpg5_newton.so): same inputs, same timing
+    nline, d_on = None, None
+    if ws == 1 and not args.no_newton_line:
+        g5n = pgb.ffi.G5("libpg5_newton.so")
+        g5n.L.g5_open()
+        d_on = torch.zeros_like(d_o)
+        pn = g5n.plan_create(g5n.NEWTON, [[0, n, 0, n]])
+        if not args.no_tune:
+            g5n.plan_tune(pn, d_i.data_ptr(), d_j.data_ptr(), None, d_on.data_ptr(), s.cuda_stream)
+        tn = _timed_launches(torch, s, lambda: g5n.plan_launch(pn, d_i.data_ptr(), d_j.data_ptr(), None,
+                                                               d_on.data_ptr(), s.cuda_stream),
+                             max(args.steps, 2000), args.warmup, flush)
+        nline = {"value": round(pairs * len(tn) / sum(tn) / 1e9, 2), "unit": "Gint/s", "launches": len(tn),
+                 "achieved_tflops": round(pairs * len(tn) * 38 / sum(tn) / 1e12, 2),
+                 "rsqrt": "rsqrt.approx + one Newton step (the reference's form), lib/libpg5_newton.so"}
+        g5n.plan_destroy(pn)
     drv = Driver(pgb)
     h = drv.L.g5drv_open(pgb.ffi.lib_path("libpg5.so").encode())
     acc = np.zeros((n, 3))
@@ -933,6 +988,10 @@ def run_direct(args, pgb, ws, rank, local):
             cpu = {}
         cpu["fp64_check"] = {"acc": _err_stats(og[:, :3], ao), "pot": _err_stats(-og[:, 3], po, vec=False),
                              "particles": 1024, "oracle": "FP64 direct sum on the same float32 inputs"}
+        if nline:
+            on = d_on.cpu().numpy()[smp]
+            nline["fp64_check"] = {"acc": _err_stats(on[:, :3], ao), "pot": _err_stats(-on[:, 3], po, vec=False),
+                                   "particles": 1024}
     g5.plan_destroy(plan)
     return _line(args, ws, "Gint/s (PG5 newton direct sum, batched)", value, t_max / len(ts), pairs, 38,
                  "PG5 newton N=16384 Plummer eps=0.01, all i vs all j (acc + pot)", "f32 (f64 cross-tile sums)",
@@ -940,7 +999,7 @@ def run_direct(args, pgb, ws, rank, local):
                  {"value": round(e2e_val, 2), "unit": "Gint/s", "h2d_bytes_per_step": n * 16 * 2,
                   "d2h_bytes_per_step": n * 32, "api": "g5_set_xmj + g5_set_eps_to_all + g5_set_n + "
                   "g5_calculate_force_on_x (direct.c:133-176), host buffers"},
-                 cpu, len(ts), extra={"steps": len(ts)},
+                 cpu, len(ts), extra={"steps": len(ts), **({"newton_rsqrt": nline} if nline else {})},
                  kernel=f"pgb::g5_kernel<NEWTON,{G5_CFG_NAMES[dcfg]}> (autotuned)")
 
 
@@ -1262,6 +1321,38 @@ def run_bh(args, pgb, ws, rank, local):
     acc_b = (o_p[:, :3] + o_c[:, :3]).cpu().numpy()
     phi_b = (o_p[:, 3] - o_c[:, 3]).cpu().numpy()
     del graph
+    # the reference's rsqrt form (the MUFU estimate refined by one Newton step,
+    # lib/libpg5_newton.so): the same two launches, same timing
+    nline, acc_n = None, None
+    if ws == 1 and not args.no_newton_line:
+        g5n = pgb.ffi.G5("libpg5_newton.so")
+        g5n.L.g5_open()
+        qn_p, qn_c = g5n.plan_create(g5n.NEWTON, bh.items("p")), g5n.plan_create(g5n.QUAD, bh.items("c"))
+        on_p, on_c = torch.zeros_like(o_p), torch.zeros_like(o_c)
+        an_p = (d_i.data_ptr(), d_p.data_ptr(), None, d_pi.data_ptr(), on_p.data_ptr(), s.cuda_stream)
+        an_c = (d_i.data_ptr(), d_c.data_ptr(), d_q.data_ptr(), d_ci.data_ptr(), on_c.data_ptr(), s.cuda_stream)
+        if not args.no_tune:
+            g5n.plan_tune_indexed(qn_p, *an_p)
+            g5n.plan_tune_indexed(qn_c, *an_c)
+
+        def launch_n():
+            g5n.plan_launch_indexed(qn_p, *an_p)
+            g5n.plan_launch_indexed(qn_c, *an_c)
+
+        gn = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(s):
+            launch_n()
+        torch.cuda.synchronize()
+        with torch.cuda.graph(gn, stream=s):
+            launch_n()
+        tn = _timed_launches(torch, s, gn.replay, args.steps, args.warmup, flush)
+        del gn
+        acc_n = (on_p[:, :3] + on_c[:, :3]).cpu().numpy()
+        nline = {"value": round(pairs * len(tn) / sum(tn) / 1e9, 2), "unit": "Gint/s", "steps": len(tn),
+                 "achieved_tflops": round(flops * len(tn) / sum(tn) / 1e12, 2),
+                 "rsqrt": "rsqrt.approx + one Newton step (the reference's form), lib/libpg5_newton.so"}
+        g5n.plan_destroy(qn_p)
+        g5n.plan_destroy(qn_c)
 
     # end to end through the batched API with host buffers: every step copies the records and
     # both index lists from pinned host memory, launches both plans and reads both results back
@@ -1372,7 +1463,7 @@ def run_bh(args, pgb, ws, rank, local):
         from oracle import oracle as O
         # FP64 on the same lists and inputs (every 97th group), and the full FP64 direct sum
         # (multipole truncation) on 4096 sampled particles
-        e1 = []
+        e1, en = [], []
         for g in range(0, bh.ngroups, 97):
             sl = slice(bh.gfirst[g], bh.gfirst[g] + bh.gcount[g])
             pl = bh.pidx[bh.poff[g]:bh.poff[g + 1]]
@@ -1381,7 +1472,13 @@ def run_bh(args, pgb, ws, rank, local):
             a2, _ = O.g5_quad(xi[sl], float(ip[0, 3]), cpos[cl], cm[cl], cqq[cl])
             ref = a1 + a2
             e1.append(np.linalg.norm(acc_b[sl] - ref, axis=1) / np.linalg.norm(ref, axis=1))
+            if acc_n is not None:
+                en.append(np.linalg.norm(acc_n[sl] - ref, axis=1) / np.linalg.norm(ref, axis=1))
         e1 = np.concatenate(e1)
+        if nline:
+            en = np.concatenate(en)
+            nline["fp64_check"] = {"acc": {"rms": float(np.sqrt(np.mean(en ** 2))), "max": float(en.max()),
+                                           "particles": int(len(en))}, "oracle": "FP64 on the same lists"}
         smp = np.sort(W.Rng(4096).permutation(len(mp))[:4096])
         ad, _ = O.g5_newton(xi[smp], float(ip[0, 3]), xp, mp)
         e2 = np.linalg.norm(acc_b[smp] - ad, axis=1) / np.linalg.norm(ad, axis=1)
@@ -1437,7 +1534,7 @@ def run_bh(args, pgb, ws, rank, local):
                                        "gpu": "lib/libpgbtree.so pgbt_rebuild of the step's tree object (device time, CUDA events)",
                                        "host": "drivers/pgb_bhtree.c bh_build (OpenMP lists)",
                                        "identical": "tests/test_bhtree_gpu.py"},
-                        "errors": errors},
+                        "errors": errors, **({"newton_rsqrt": nline} if nline else {})},
                  kernel=f"pgb::g5_kernel<NEWTON,{G5_CFG_NAMES[cfg_p]}> + <QUAD,{G5_CFG_NAMES[cfg_c]}> (index lists)")
 
 
@@ -1772,6 +1869,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-f64-line", action="store_true",
                     help="hermite: skip the second batched run with FP64 relative coordinates")
+    ap.add_argument("--no-newton-line", action="store_true",
+                    help="skip the second run with the reference's Newton-refined rsqrt (lib*_newton.so)")
     ap.add_argument("--no-workloads", action="store_true",
                     help="hermite on one GPU: skip the other configurations' lines (C1, C3, C4, C5)")
     ap.add_argument("--no-tune", action="store_true", help="skip the kernel-configuration autotuner")

@@ -12,6 +12,7 @@ import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIBDIR = os.path.join(HERE, "lib")
-LIBS = ("libpg5.so", "libpg5sym.so", "libpg5table.so", "libpg6.so", "libpgbtree.so", "libpgbpeak.so")
+LIBS = ("libpg5.so", "libpg5sym.so", "libpg5table.so", "libpg6.so", "libpgbtree.so", "libpgbpeak.so",
+        "libpg5_newton.so", "libpg6_newton.so")
 
 from . import ffi, shard, workloads  # noqa: E402,F401

@@ -8,9 +8,9 @@
 // * the work-list types shared by all kernels: a Task is one (i-tile, j-chunk) pair, a Group
 //   collects the tasks whose partial sums are reduced, in chunk order, by the last CTA that
 //   finishes one of them (deterministic; no second launch).
-// * the MUFU reciprocal square root (PTX rsqrt.approx.ftz.f32) plus the one-Newton-step form
-//   q = y (r2 y^2 - 3) = -2/r used by every kernel (the reference's "rsqrt_1st_phantom" form,
-//   PG6/libpg6/gravity.c:341-346).
+// * the MUFU reciprocal square root (PTX rsqrt.approx.ftz.f32) and the scale q = -2/r used by
+//   every kernel: q = -2 y by default, or -- built with PGB_RSQRT_NEWTON -- the reference's
+//   one-Newton-step form q = y (r2 y^2 - 3) ("rsqrt_1st_phantom", PG6/libpg6/gravity.c:341-346).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -299,15 +299,31 @@ __device__ __forceinline__ float mufu_rsqrt(float x) {
     return y;
 }
 
-// q = y (r2 y^2 - 3) with y = rsqrt(r2): one Newton step folded into the scale -2/r.
-// Every operation is an explicit round-to-nearest intrinsic, so that the key is the same bit
-// pattern wherever it is computed (the nearest-neighbour search recomputes it, see g6_task).
-__device__ __forceinline__ float minus2_over_r(float r2) {
-    float y = mufu_rsqrt(r2);
-    float t = __fmul_rn(r2, y);
-    float u = __fmaf_rn(t, y, -3.0f);
+// q = -2/r from y = rsqrt.approx(r2).  By default q = -2 y: sm_100's MUFU estimate is already
+// accurate to about an ulp, so a Newton step only adds rounding (and three FP32 operations per
+// pair).  Built with PGB_RSQRT_NEWTON (the lib*_newton.so libraries), the reference's form: one
+// Newton step folded into the scale, q = y (r2 y^2 - 3), which the AVX code needs to refine its
+// 12-bit estimate.  Every operation is an explicit round-to-nearest intrinsic, so that the key
+// is the same bit pattern wherever it is computed (the nearest-neighbour search recomputes it,
+// see g6_task).
+__device__ __forceinline__ float minus2_mufu(float y) { return __fmul_rn(-2.0f, y); }
+
+__device__ __forceinline__ float minus2_newton(float r2, float y) {
+    const float t = __fmul_rn(r2, y);
+    const float u = __fmaf_rn(t, y, -3.0f);
     return __fmul_rn(u, y);
 }
+
+__device__ __forceinline__ float minus2_from_rsqrt(float r2, float y) {
+#ifdef PGB_RSQRT_NEWTON
+    return minus2_newton(r2, y);
+#else
+    (void)r2;
+    return minus2_mufu(y);
+#endif
+}
+
+__device__ __forceinline__ float minus2_over_r(float r2) { return minus2_from_rsqrt(r2, mufu_rsqrt(r2)); }
 
 // The persistent scheduler.  A CTA's first task is its block index; later ones are drawn from
 // a global counter as gridDim.x + k.  Every CTA draws until it gets a task >= ntasks, so a

@@ -13,7 +13,7 @@
 //  * g5_get_force returns acc = sum m dx/r^3 and pot = +sum m/r (self pair included), the sign
 //    the reference returns after Pot_correct (phantom_g5.c:251-259).  The reference's rsqrt
 //    bias factors (1-3 bias, 1-bias) are NOT applied: they only undo the 12-bit rsqrt's mean
-//    error, and the Newton-refined MUFU rsqrt has none to undo.
+//    error, and the MUFU rsqrt (with or without the Newton step) has none to undo.
 //  * g5c_* (quad_g5c.c:198-303) share the i-pipes of g5_set_xiMC and the output path of
 //    g5_get_forceMC, so the quadrupole potential comes back as -sum(phi_p + phi_q) while the
 //    monopole one comes back positive; callers reconcile this (source.cpp:854, 866).

@@ -9,7 +9,8 @@
 // then added into FP64 accumulators (the cross-block reduction runs in FP64).  Split j-ranges
 // write FP64 partial rows; the last CTA of a group reduces them in chunk order.
 //
-// Formulae (scaled so that the Newton-refined rsqrt needs no extra multiply):
+// Formulae (in the scale of the reference's Newton-refined rsqrt, -2/r, so that its form needs
+// no extra multiply):
 //   q = -2/r (pgb::minus2_over_r),  pot_sum += m q,  acc_sum += (m q^3) dx   (m q^3 = -8 m/r^3)
 //   acc = acc_sum * (-1/8),  pot_raw = pot_sum * (1/2) = -sum m/r
 // i.e. the reference's GravityKernel accumulators (PG5/newton/libpg5/gravity_avx2.c:95-153:

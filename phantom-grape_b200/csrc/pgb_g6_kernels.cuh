@@ -7,7 +7,7 @@
 // terms (G6_FOLD) and then added into FP64 sums; split j-ranges are reduced in FP64 in chunk
 // order.
 //
-// Per pair (q = -2/r with one Newton step, pgb::minus2_over_r; self pair masked by index):
+// Per pair (q = -2/r from the MUFU rsqrt, pgb::minus2_over_r; self pair masked by index):
 //   pot_sum += m q, acc_sum += (m q^3) dx, jrk_sum += (m q^3) (dv - (3/4) q^2 (dx.dv) dx)
 // and finally acc = -acc_sum/8, jerk = -jrk_sum/8, pot = pot_sum/2 (phantom_g6.c:200-208), i.e.
 //   acc = sum m dx/r^3, jerk = sum m (dv/r^3 - 3 (dx.dv) dx/r^5), pot = -sum m/r.
@@ -342,10 +342,11 @@ __device__ __forceinline__ void g6_pair2(const G6PredJ& J, int jadr, const Pos3*
 // consecutive j: every paired FP32 operand is then a natural register pair -- (j, j+1) for the
 // j fields, a loop-invariant (v, v) for the i fields -- and the double-float relative
 // coordinates (nine FADD per j-pair as paired FADD2) join the nine accumulations (FFMA2) on the
-// heavy half of the FMA pipe, while the rest of the chain (dv, r^2, the Newton step, dx.dv and
-// the scalar factors: 18 per pair) stays scalar.  Per pair that is 9 paired + 18 scalar FP32
-// instructions, which loads the two halves of the FMA pipe about equally (a paired instruction
-// occupies the heavy half twice as long as a scalar one), against 4.5 + 27 in g6_pair2.
+// heavy half of the FMA pipe, while the rest of the chain (dv, r^2, the scale q, dx.dv and
+// the scalar factors: 16 per pair, 18 with the Newton step) stays scalar.  Per pair that is 9
+// paired + 16 scalar FP32 instructions, which loads the two halves of the FMA pipe about equally
+// (a paired instruction occupies the heavy half twice as long as a scalar one), against 4.5 + 25
+// in g6_pair2.
 // The two lanes of each accumulator sum the even and the odd j of the tile; they are added
 // into the FP64 sums one after the other at every fold.  Per pair the key q is bit-identical
 // to g6_key (FADD2 rounds each lane as FADD does).
@@ -409,7 +410,7 @@ __device__ __forceinline__ void g6_jpair(float2 xh, float2 yh, float2 zh, float2
 
 // The j-paired form for two i, stage-ordered: the four j-pair chains of a j-quad (two i x two
 // j-pairs) advanced together stage by stage -- relative coordinates, dv and r^2, the eight
-// rsqrt, the Newton steps and scalar factors, the accumulations -- which hands the scheduler
+// rsqrt, the scales q and the scalar factors, the accumulations -- which hands the scheduler
 // independent work in every stage (largest Hermite call 5.65 against 5.77 ms for the chain-by-
 // chain order of g6_jpair; the autotuner chooses between them per call size).  The same
 // operations as g6_jpair on the same values: bit-identical results.
@@ -457,9 +458,7 @@ __device__ __forceinline__ void g6_jquad2(const float4& XH, const float4& YH, co
         const int c = l >> 1, h = l & 1;
         const G6IPair& I = IP[c >> 1];
         const int jj = ((c & 1) << 1) + h;
-        const float t = __fmul_rn(r2[l], y[l]);
-        const float u = __fmaf_rn(t, y[l], -3.0f);
-        float q = __fmul_rn(u, y[l]);
+        float q = minus2_from_rsqrt(r2[l], y[l]);
         if constexpr (SELF) q = (ids[jj] == I.id) ? 0.0f : q;
         if constexpr (NN) tmin[c >> 1] = fminf(tmin[c >> 1], q);
         a[c >> 1].pot[h] = __fmaf_rn(ms[jj], q, a[c >> 1].pot[h]);

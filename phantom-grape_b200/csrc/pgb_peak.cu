@@ -12,12 +12,15 @@
 //    FP32 sums folded into FP64 in shared memory every 128 j) over one shared-memory tile staged
 //    once, with no j staging, task scheduling or partial rows: what the kernel's arithmetic
 //    sustains when nothing else runs.
+//  * The accuracy of the rsqrt forms the kernels can be built with (pgb_peak_rsqrt_error).
 // Both kernels write one value per thread (so that nothing is optimised away) into a caller
 // buffer or a small internal one.  Times are CUDA-event times on the caller's stream.
 #include <cuda_runtime.h>
 
 #include <chrono>
+#include <cmath>
 #include <cstdio>
+#include <cstring>
 
 #include "pgb_g6_kernels.cuh"
 
@@ -312,12 +315,77 @@ PGB_EXPORT int pgb_peak_g6_loop(int form, int passes, void* stream, double* gpai
 // kernel sets a flag in mapped host memory (after a system-scope fence) that the host polls, as
 // the drop-in API's small calls do.  *us = microseconds per launch (host clock), after 100
 // untimed launches.
+// Accuracy of the two forms of the scale q = -2/r from the MUFU estimate y = rsqrt.approx(r2)
+// (pgb_common.cuh): q = -2 y, the default, and the reference's one Newton step
+// q = y (r2 y^2 - 3), each against -2/sqrt(r2) in FP64, for every float r2 in [1, 4) -- two
+// binades, one period of the estimate's relative error.  mx[f]: the largest |relative error| of
+// form f (the bits of a non-negative double, which order as integers), ss[f]: the sum of squares.
+constexpr unsigned RSQ_N = 1u << 24;   // the floats in [1, 4)
+
+__global__ void __launch_bounds__(PEAK_THREADS) rsqrt_err_kernel(unsigned long long* mx, double* ss) {
+    double m0 = 0.0, m1 = 0.0, s0 = 0.0, s1 = 0.0;
+    for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < RSQ_N; k += gridDim.x * blockDim.x) {
+        const float r2 = __uint_as_float(0x3f800000u + k);
+        const float y = pgb::mufu_rsqrt(r2);
+        const double ref = -2.0 / sqrt((double)r2);
+        const double e0 = fabs(((double)pgb::minus2_mufu(y) - ref) / ref);
+        const double e1 = fabs(((double)pgb::minus2_newton(r2, y) - ref) / ref);
+        m0 = fmax(m0, e0);
+        m1 = fmax(m1, e1);
+        s0 += e0 * e0;
+        s1 += e1 * e1;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        m0 = fmax(m0, __shfl_xor_sync(0xffffffffu, m0, o));
+        m1 = fmax(m1, __shfl_xor_sync(0xffffffffu, m1, o));
+        s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(&mx[0], (unsigned long long)__double_as_longlong(m0));
+        atomicMax(&mx[1], (unsigned long long)__double_as_longlong(m1));
+        atomicAdd(&ss[0], s0);
+        atomicAdd(&ss[1], s1);
+    }
+}
+
 __global__ void floor_kernel(volatile unsigned* done, unsigned seq) {
     __syncthreads();
     if (done && threadIdx.x == 0 && blockIdx.x == 0) {
         __threadfence_system();
         done[0] = seq;
     }
+}
+
+// max_rel[f], rms_rel[f]: the relative error of q = -2/r over every float r2 in [1, 4), form
+// f = 0: -2 y (the default build), f = 1: one Newton step (the lib*_newton.so builds).
+PGB_EXPORT int pgb_peak_rsqrt_error(void* stream, double* max_rel, double* rms_rel) {
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned long long* mx = nullptr;
+    double* ss = nullptr;
+    if (cudaMalloc(&mx, 2 * sizeof(unsigned long long)) != cudaSuccess) return -1;
+    if (cudaMalloc(&ss, 2 * sizeof(double)) != cudaSuccess) {
+        cudaFree(mx);
+        return -1;
+    }
+    cudaMemsetAsync(mx, 0, 2 * sizeof(unsigned long long), s);
+    cudaMemsetAsync(ss, 0, 2 * sizeof(double), s);
+    rsqrt_err_kernel<<<4 * 148, PEAK_THREADS, 0, s>>>(mx, ss);
+    unsigned long long hm[2] = {0, 0};
+    double hs[2] = {0, 0};
+    cudaMemcpyAsync(hm, mx, sizeof hm, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(hs, ss, sizeof hs, cudaMemcpyDeviceToHost, s);
+    const cudaError_t e = cudaStreamSynchronize(s);
+    cudaFree(mx);
+    cudaFree(ss);
+    if (e != cudaSuccess || cudaGetLastError() != cudaSuccess) return -1;
+    for (int f = 0; f < 2; f++) {
+        double m;
+        std::memcpy(&m, &hm[f], sizeof m);
+        if (max_rel) max_rel[f] = m;
+        if (rms_rel) rms_rel[f] = std::sqrt(hs[f] / RSQ_N);
+    }
+    return 0;
 }
 
 PGB_EXPORT int pgb_peak_launch_floor(int kind, int grid, int n, void* stream, double* us) {

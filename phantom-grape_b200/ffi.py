@@ -70,15 +70,18 @@ class _ErrMixin:
 
 
 class G5(_ErrMixin):
-    """GRAPE-5 newton + newton_quad API (libpg5.so) or its symmetric build (libpg5sym.so)."""
+    """GRAPE-5 newton + newton_quad API (libpg5.so) or its symmetric build (libpg5sym.so).
+
+    ``lib`` picks another build of the same API, e.g. "libpg5_newton.so" (the reference's
+    Newton-refined rsqrt)."""
 
     LIBNAME = "libpg5.so"
     SYMMETRIC = False
     # kinds of the batched path (include/pgb_g5.h)
     NEWTON, SYMMETRIC_KIND, QUAD = 0, 1, 2
 
-    def __init__(self):
-        L = self.L = _load(self.LIBNAME)
+    def __init__(self, lib: str = None):
+        L = self.L = _load(lib or self.LIBNAME)
         _sig(L, "g5_open", [])
         _sig(L, "g5_close", [])
         _sig(L, "g5_get_number_of_pipelines", [], C.c_int)
@@ -230,14 +233,17 @@ class G5Sym(G5):
 
 
 class G6(_ErrMixin):
-    """GRAPE-6 API (libpg6.so): g6_open ... g6calc_lasthalf2np, plus the batched pgb6_* path."""
+    """GRAPE-6 API (libpg6.so): g6_open ... g6calc_lasthalf2np, plus the batched pgb6_* path.
+
+    ``lib`` picks another build of the same API, e.g. "libpg6_newton.so" (the reference's
+    Newton-refined rsqrt)."""
 
     prefix = "pgb6"
     NN = 1
     POS_F64 = 2
 
-    def __init__(self):
-        L = self.L = _load("libpg6.so")
+    def __init__(self, lib: str = "libpg6.so"):
+        L = self.L = _load(lib)
         for n in ("g6_open", "g6_close", "g6_set_tunit", "g6_set_xunit", "g6_reset", "g6_reset_fofpga"):
             _sig(L, n, [C.c_int])
         _sig(L, "g6_npipes", [], C.c_int)

@@ -12,9 +12,9 @@ from conftest import ROOT, pgb
 
 INC = os.path.join(ROOT, "include")
 HEADERS = {
-    "pgb_g5.h": ["libpg5.so", "libpg5sym.so"],
+    "pgb_g5.h": ["libpg5.so", "libpg5sym.so", "libpg5_newton.so"],
     "pgb_g5table.h": ["libpg5table.so"],
-    "pgb_g6.h": ["libpg6.so"],
+    "pgb_g6.h": ["libpg6.so", "libpg6_newton.so"],
     "pgb_bhtree.h": ["libpgbtree.so"],
 }
 

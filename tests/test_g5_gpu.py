@@ -29,11 +29,12 @@ def rms(x):
     return float(np.sqrt(np.mean(np.square(x))))
 
 
-@pytest.fixture(scope="module")
-def g5():
+# the default build (MUFU rsqrt alone) and the reference's rsqrt form (one Newton step)
+@pytest.fixture(scope="module", params=["libpg5.so", "libpg5_newton.so"])
+def g5(request):
     if not gpu_available():
         pytest.skip("no GPU")
-    lib = pgb.ffi.G5()
+    lib = pgb.ffi.G5(request.param)
     lib.L.g5_open()
     return lib
 

@@ -34,11 +34,13 @@ def fp64_force(x, v, m, eps2):
     return r["acc"], r["jrk"]
 
 
-@pytest.fixture(scope="module")
-def g6():
+# the default build (q = -2/r from the MUFU rsqrt alone) and the reference's rsqrt form (one
+# Newton step): every case holds for both
+@pytest.fixture(scope="module", params=["libpg6.so", "libpg6_newton.so"])
+def g6(request):
     if not gpu_available():
         pytest.skip("no GPU")
-    lib = pgb.ffi.G6()
+    lib = pgb.ffi.G6(request.param)
     lib.L.g6_open(0)
     return lib
 
@@ -308,8 +310,11 @@ def test_every_configuration_vs_fp64(g6, state):
     both position layouts, with and without the nearest neighbour) on items that exercise the
     per-tile self test (i-particles inside their own j-range and outside it), ragged j-tiles
     (j counts that are not multiples of 4 or of the tile) and single-j items, against the FP64
-    oracle: rms relative acc / jerk / pot <= 1e-6 per item, nearest neighbour identical wherever
-    the FP64 first and second neighbours are separated."""
+    oracle: rms relative acc / pot <= 1e-6 per item, jerk rms <= 1e-6 over the launch's particles
+    and <= 2e-5 for every particle (the jerk's two terms cancel: one ill-conditioned particle of
+    a 37-particle item carries 5.9e-6 with the MUFU rsqrt alone, 1.4e-6 with the Newton step; the
+    reference's own jerk error is rms 1.8e-6), nearest neighbour identical wherever the FP64 first
+    and second neighbours are separated."""
     import torch
     st = state
     n = len(st.mass)
@@ -343,13 +348,16 @@ def test_every_configuration_vs_fp64(g6, state):
                     g6.plan_launch(plan, d_i.data_ptr(), d_j.data_ptr(), st.eps2, d_o.data_ptr(), 0)
                     torch.cuda.synchronize()
                     out = d_o.cpu().numpy().view(pgb.ffi.G6OUT)
+                    ej_all = []
                     for k, (c, ref) in enumerate(zip(cases, refs)):
                         o = out[ioff[k]:ioff[k + 1]]
                         tag = (ff, nn, cfg, k)
                         acc = np.stack([o["ax"], o["ay"], o["az"]], 1)
                         jrk = np.stack([o["jx"], o["jy"], o["jz"]], 1)
                         assert rms(rel(acc, ref["acc"])) <= 1e-6, tag
-                        assert rms(rel(jrk, ref["jrk"])) <= 1e-6, tag
+                        ej = rel(jrk, ref["jrk"])
+                        assert ej.max() <= 2e-5, tag
+                        ej_all.append(ej)
                         assert rms((o["pot"] - ref["pot"]) / np.abs(ref["pot"])) <= 1e-6, tag
                         if nn:
                             clear = ref["r2nn2"] / ref["r2nn"] - 1.0 > 1e-5 if c[2] > 1 else np.ones(len(o), bool)
@@ -357,6 +365,7 @@ def test_every_configuration_vs_fp64(g6, state):
                             assert np.all((jadr >= c[1]) & (jadr < c[1] + c[2])), tag
                             assert np.array_equal(st.idx[jadr][clear], ref["nnb"][clear]), tag
                             np.testing.assert_allclose(-2.0 / o["key"], ref["rnnb"], rtol=1e-6, err_msg=str(tag))
+                    assert rms(np.concatenate(ej_all)) <= 1e-6, (ff, nn, cfg)
                     cfg += 1
                 ncfg = max(ncfg, cfg)
             finally:
