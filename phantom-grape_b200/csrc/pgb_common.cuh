@@ -325,6 +325,35 @@ __device__ __forceinline__ float minus2_from_rsqrt(float r2, float y) {
 
 __device__ __forceinline__ float minus2_over_r(float r2) { return minus2_from_rsqrt(r2, mufu_rsqrt(r2)); }
 
+// The pair scale.  Every kernel forms its pair terms from one scale s of 1/r and removes the
+// scale with FP64 constants where the sums are finished.  By default s = y, the MUFU estimate
+// itself (no operation after the rsqrt); built with PGB_RSQRT_NEWTON, s = q = -2/r in the
+// reference's Newton-refined form.  Every term is a product of powers of s, so the default's
+// terms are those of s = -2 y (the MUFU estimate in the reference's scale) times exact powers
+// of two, and the finished results are the same bit for bit.
+//   PG6: pot = S_POT sum m s,  acc = S_ACC sum m s^3 dx,
+//        jerk = S_ACC sum m s^3 (dv + S_JERK s^2 (dx.dv) dx)
+//   PG5: pot_raw = S_POT sum m s (= -sum m/r),  acc = S_ACC sum m s^3 dx
+// Nearest-neighbour key: k = nn_key(s), smaller is nearer; reported as q = -2/r_soft =
+// key_out(k) = KEY_OUT k.
+#ifdef PGB_RSQRT_NEWTON
+constexpr double S_POT = 0.5, S_ACC = -0.125;
+constexpr float S_JERK = -0.75f, KEY_OUT = 1.0f;
+__device__ __forceinline__ float pair_scale_from_rsqrt(float r2, float y) { return minus2_newton(r2, y); }
+__device__ __forceinline__ float nn_key(float s) { return s; }
+#else
+constexpr double S_POT = -1.0, S_ACC = 1.0;
+constexpr float S_JERK = -3.0f, KEY_OUT = 2.0f;
+__device__ __forceinline__ float pair_scale_from_rsqrt(float, float y) { return y; }
+// -y: the negation is an operand modifier of the compare or min that consumes it
+__device__ __forceinline__ float nn_key(float s) { return -s; }
+#endif
+__device__ __forceinline__ float pair_scale(float r2) { return pair_scale_from_rsqrt(r2, mufu_rsqrt(r2)); }
+// KEY_OUT k, with a self-only key's -0 reported as +0 (the key of s = 0)
+__device__ __forceinline__ float key_out(float k) { return __fmaf_rn(KEY_OUT, k, 0.0f); }
+// a key as reported back to the kernels' scale (exact)
+__device__ __forceinline__ float key_in(float q) { return q * (1.0f / KEY_OUT); }
+
 // The persistent scheduler.  A CTA's first task is its block index; later ones are drawn from
 // a global counter as gridDim.x + k.  Every CTA draws until it gets a task >= ntasks, so a
 // launch draws exactly ntasks times (the ntasks - min(grid, ntasks) extra tasks plus one failed

@@ -9,10 +9,10 @@
 // then added into FP64 accumulators (the cross-block reduction runs in FP64).  Split j-ranges
 // write FP64 partial rows; the last CTA of a group reduces them in chunk order.
 //
-// Formulae (in the scale of the reference's Newton-refined rsqrt, -2/r, so that its form needs
-// no extra multiply):
-//   q = -2/r (pgb::minus2_over_r),  pot_sum += m q,  acc_sum += (m q^3) dx   (m q^3 = -8 m/r^3)
-//   acc = acc_sum * (-1/8),  pot_raw = pot_sum * (1/2) = -sum m/r
+// Formulae, with the pair scale s of 1/r (pgb::pair_scale: the MUFU estimate 1/r by default,
+// -2/r in the reference's Newton-refined form with PGB_RSQRT_NEWTON):
+//   pot_sum += m s,  acc_sum += (m s^3) dx,  acc = S_ACC acc_sum,  pot_raw = S_POT pot_sum
+//   = -sum m/r
 // i.e. the reference's GravityKernel accumulators (PG5/newton/libpg5/gravity_avx2.c:95-153:
 // phi -= m/r, acc += m dx / r^3) without its 12-bit rsqrt.
 #pragma once
@@ -56,16 +56,27 @@ template <int KIND>
 struct JWords { static constexpr int n = (KIND == G5_SYMMETRIC) ? 2 : (KIND == G5_QUAD ? 3 : 1); };
 
 // FP32 block sums per i: (acc, pot) for the point-mass and table kinds; the quadrupole kind
-// keeps [0..2] sum (w dr + K q^5 v), [3] sum m q, [4] sum K q^5 D (g5_quad_pair), which g5_fold
+// keeps [0..2] sum (w dr + K s^5 v), [3] sum m s, [4] sum K s^5 D (g5_quad_pair), which g5_fold
 // scales and combines into (acc, phi_p + phi_q).
 template <int KIND>
 struct NAcc { static constexpr int n = KIND == G5_QUAD ? 5 : 4; };
 
-// The cells' moments as staged in shared memory: Q' = (5/32) Q, which makes the coefficient of
-// the monopole and of the D q^7 term of the acceleration the same; K = -8/5 puts the (Q dr) r^-5
-// term into the same sums (g5_quad_pair).
+// The cells' moments as staged in shared memory, Q' = G5_QSCALE Q, and the constant K of the
+// (Q dr) r^-5 term (g5_quad_pair).  For s = -2/r: Q' = (5/32) Q, which makes the coefficient of
+// the monopole and of the D s^7 term of the acceleration the same, and K = -8/5 puts the
+// (Q dr) r^-5 term into the same sums; the sums are scaled by G5_QACC (acc) and G5_QP3, G5_QP4
+// (phi_p + phi_q = G5_QP3 a[3] + G5_QP4 a[4]).  For s = 1/r the moments are staged 16 times
+// larger and K is a quarter: every term is the same term times an exact power of two (K is the
+// FP32 -8/5 divided by 4), and the constants remove them.
+#ifdef PGB_RSQRT_NEWTON
 constexpr float G5_QSCALE = 0.15625f;
 constexpr float G5_QK = -1.6f;
+constexpr double G5_QACC = -0.125, G5_QP3 = -0.5, G5_QP4 = -(0.1 / (double)(-1.6f));
+#else
+constexpr float G5_QSCALE = 2.5f;
+constexpr float G5_QK = -0.4f;
+constexpr double G5_QACC = 1.0, G5_QP3 = 1.0, G5_QP4 = 8.0 * (0.1 / (double)(-1.6f));
+#endif
 
 __device__ __forceinline__ float4 scale4(float4 v, float f) {
     return make_float4(f * v.x, f * v.y, f * v.z, f * v.w);
@@ -77,8 +88,8 @@ template <int KIND>
 __device__ __forceinline__ void g5_fold(double (&S)[4], const float* a) {
     if constexpr (KIND == G5_QUAD) {
 #pragma unroll
-        for (int c = 0; c < 3; c++) S[c] += -0.125 * (double)a[c];
-        S[3] += -0.5 * (double)a[3] - (0.1 / (double)G5_QK) * (double)a[4];
+        for (int c = 0; c < 3; c++) S[c] += G5_QACC * (double)a[c];
+        S[3] += G5_QP3 * (double)a[3] + G5_QP4 * (double)a[4];
     } else {
 #pragma unroll
         for (int c = 0; c < 4; c++) S[c] += (double)a[c];
@@ -97,8 +108,8 @@ __device__ __forceinline__ void g5_fold2(double (&S)[4], const float2* a2, int k
     if (k < 0) {
         if constexpr (KIND == G5_QUAD) {
 #pragma unroll
-            for (int c = 0; c < 3; c++) S[c] += -0.125 * ((double)a[0][c] + (double)a[1][c]);
-            S[3] += -0.5 * ((double)a[0][3] + (double)a[1][3]) - (0.1 / (double)G5_QK) * ((double)a[0][4] + (double)a[1][4]);
+            for (int c = 0; c < 3; c++) S[c] += G5_QACC * ((double)a[0][c] + (double)a[1][c]);
+            S[3] += G5_QP3 * ((double)a[0][3] + (double)a[1][3]) + G5_QP4 * ((double)a[0][4] + (double)a[1][4]);
         } else {
 #pragma unroll
             for (int c = 0; c < 4; c++) S[c] = S[c] + (double)a[0][c] + (double)a[1][c];
@@ -136,18 +147,21 @@ __device__ __forceinline__ void g5_table_pair(float4 J, float xi, float yi, floa
 }
 
 // The quadrupole cell (c_GravityKernel, PG5/newton_quad/quad/quad_avx2.c:35-149; FP64 form
-// source.cpp:1160-1184): with r^-1 = -q/2 and the moments staged as Q' = (5/32) Q,
-//   v = Q' dr,  D = dr . v,  w = q^3 (m + D q^4),  p = K q^5 (K = -8/5)
-//   acc = dr (m r^-3 + (5/2) (dr.Q.dr) r^-7) - (Q dr) r^-5 = -(w dr + p v) / 8
-//   phi_p + phi_q = m r^-1 + (1/2) (dr.Q.dr) r^-5 = -(m q) / 2 - (p D) / (10 K)
-// 36 FP32 operations per pair (the r^-1, r^-2, r^-5 form takes 38); the block sums of
-// w dr + p v, m q and p D are scaled and combined in FP64 by g5_fold.  K rounded to FP32 weighs
-// the (Q dr) term 1.5e-8 (relative) heavier.
+// source.cpp:1160-1184): with the pair scale s (below q; 1/r by default) and the moments staged
+// as Q' = G5_QSCALE Q,
+//   v = Q' dr,  D = dr . v,  w = s^3 (m + D s^4),  p = K s^5
+//   acc = dr (m r^-3 + (5/2) (dr.Q.dr) r^-7) - (Q dr) r^-5 = G5_QACC (w dr + p v)
+//   phi_p + phi_q = m r^-1 + (1/2) (dr.Q.dr) r^-5 = G5_QP3 (m s) + G5_QP4 (p D)
+// (s = 1/r: Q' = (5/2) Q, K = -2/5, G5_QACC = 1, G5_QP3 = 1, G5_QP4 = -1/2; s = -2/r: (5/32) Q,
+// -8/5, -1/8, -1/2, -1/(10 K)).  34 FP32 operations per pair with s = 1/r (36 with the Newton
+// step; the r^-1, r^-2, r^-5 form takes 38); the block sums of w dr + p v, m s and p D are
+// scaled and combined in FP64 by g5_fold.  K rounded to FP32 weighs the (Q dr) term 1.5e-8
+// (relative) heavier.
 __device__ __forceinline__ void g5_quad_pair(float dx, float dy, float dz, float m, float4 Q0, float4 Q1,
                                              float e, float (&a)[5]) {
     // Q0 = q00 q01 q02 q11, Q1 = q12 q22 - -
     const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmaf_rn(dx, dx, e)));
-    const float q = minus2_over_r(r2);
+    const float q = pair_scale(r2);
     const float vx = __fmaf_rn(Q0.z, dz, __fmaf_rn(Q0.y, dy, Q0.x * dx));
     const float vy = __fmaf_rn(Q1.x, dz, __fmaf_rn(Q0.w, dy, Q0.y * dx));
     const float vz = __fmaf_rn(Q1.y, dz, __fmaf_rn(Q1.x, dy, Q0.z * dx));
@@ -172,7 +186,7 @@ __device__ __forceinline__ void g5_interact(const float4* sj, int j, float xi, f
         float e = ei;
         if constexpr (KIND == G5_SYMMETRIC) e += sj[NT + j].x;  // GravityKernel0
         float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmaf_rn(dx, dx, e)));
-        float q = minus2_over_r(r2);
+        float q = pair_scale(r2);
         float mq = J.w * q;
         float q2 = q * q;
         float mq3 = mq * q2;
@@ -228,7 +242,7 @@ __device__ __forceinline__ void g5_interact2(const float4* sj, int j, const floa
                 float e = ei[k];
                 if constexpr (KIND == G5_SYMMETRIC) e += sj[NT + j].x;
                 float r2 = __fmaf_rn(dz[k], dz[k], __fmaf_rn(dy[k], dy[k], __fmaf_rn(dx[k], dx[k], e)));
-                float q = minus2_over_r(r2);
+                float q = pair_scale(r2);
                 float mq = J.w * q;
                 float q2 = q * q;
                 s3[k] = mq;
@@ -256,7 +270,7 @@ __device__ __forceinline__ void g5_interact2(const float4* sj, int j, const floa
 template <int NT>
 struct G5TileSoA {
     float x[NT], y[NT], z[NT], m[NT];
-    float q[6][NT];   // cells: (5/32) (q00 q01 q02 q11 q12 q22)
+    float q[6][NT];   // cells: G5_QSCALE (q00 q01 q02 q11 q12 q22)
 };
 
 __device__ __forceinline__ void g5_newton_jpair(float2 X, float2 Y, float2 Z, float2 M, float2 nx, float2 ny,
@@ -272,7 +286,7 @@ __device__ __forceinline__ void g5_newton_jpair(float2 X, float2 Y, float2 Z, fl
 #pragma unroll
     for (int h = 0; h < 2; h++) {
         const float r2 = __fmaf_rn(dzp[h], dzp[h], __fmaf_rn(dyp[h], dyp[h], __fmaf_rn(dxp[h], dxp[h], e)));
-        qp[h] = minus2_over_r(r2);
+        qp[h] = pair_scale(r2);
         mqp[h] = mp[h] * qp[h];
     }
     const float2 mq3 = __fmul2_rn(mq, __fmul2_rn(q, q));
@@ -282,7 +296,7 @@ __device__ __forceinline__ void g5_newton_jpair(float2 X, float2 Y, float2 Z, fl
     a[2] = __ffma2_rn(mq3, dz, a[2]);
 }
 
-// Q = (q00 q01 q02 q11 q12 q22) of the two cells, as pairs, staged as Q' = (5/32) Q: the
+// Q = (q00 q01 q02 q11 q12 q22) of the two cells, as pairs, staged as Q' = G5_QSCALE Q: the
 // arithmetic of g5_quad_pair, the moment products, D and the sums paired.
 __device__ __forceinline__ void g5_quad_jpair(float2 X, float2 Y, float2 Z, float2 M, const float2 (&Q)[6], float2 nx,
                                               float2 ny, float2 nz, float e, float2 (&a)[5]) {
@@ -303,7 +317,7 @@ __device__ __forceinline__ void g5_quad_jpair(float2 X, float2 Y, float2 Z, floa
 #pragma unroll
     for (int h = 0; h < 2; h++) {
         const float r2 = __fmaf_rn(dzp[h], dzp[h], __fmaf_rn(dyp[h], dyp[h], __fmaf_rn(dxp[h], dxp[h], e)));
-        qp[h] = minus2_over_r(r2);
+        qp[h] = pair_scale(r2);
         const float q2 = qp[h] * qp[h], q3 = q2 * qp[h], q4 = q2 * q2;
         pp[h] = q4 * (G5_QK * qp[h]);
         wp[h] = q3 * __fmaf_rn(Dp[h], q4, mp[h]);
@@ -321,7 +335,7 @@ __device__ __forceinline__ double4 g5_finish(double4 s, double ascale) {
     if constexpr (KIND == G5_QUAD) return s;  // quad sums are already (acc, +sum(phi_p+phi_q))
     if constexpr (KIND == G5_TABLE)           // acc *= 1/xscale (gravity_kernel_avx2.c:127-129)
         return make_double4(ascale * s.x, ascale * s.y, ascale * s.z, 0.0);
-    return make_double4(-0.125 * s.x, -0.125 * s.y, -0.125 * s.z, 0.5 * s.w);
+    return make_double4(S_ACC * s.x, S_ACC * s.y, S_ACC * s.z, S_POT * s.w);
 }
 
 __device__ __forceinline__ double4 add4(double4 a, double4 b) {

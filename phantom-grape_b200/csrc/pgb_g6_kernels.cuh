@@ -7,12 +7,15 @@
 // terms (G6_FOLD) and then added into FP64 sums; split j-ranges are reduced in FP64 in chunk
 // order.
 //
-// Per pair (q = -2/r from the MUFU rsqrt, pgb::minus2_over_r; self pair masked by index):
-//   pot_sum += m q, acc_sum += (m q^3) dx, jrk_sum += (m q^3) (dv - (3/4) q^2 (dx.dv) dx)
-// and finally acc = -acc_sum/8, jerk = -jrk_sum/8, pot = pot_sum/2 (phantom_g6.c:200-208), i.e.
+// Per pair, with the pair scale s of 1/r (pgb::pair_scale: the MUFU estimate 1/r, or -2/r in the
+// reference's Newton-refined form; self pair masked by index):
+//   pot_sum += m s, acc_sum += (m s^3) dx, jrk_sum += (m s^3) (dv + S_JERK s^2 (dx.dv) dx)
+// and finally acc = S_ACC acc_sum, jerk = S_ACC jrk_sum, pot = S_POT pot_sum (for s = -2/r:
+// -1/8, -1/8, 1/2 and S_JERK = -3/4, phantom_g6.c:200-208), i.e.
 //   acc = sum m dx/r^3, jerk = sum m (dv/r^3 - 3 (dx.dv) dx/r^5), pot = -sum m/r.
-// Nearest neighbour: the smallest key q (= -2/r_soft) over j != i; ties -> smallest j address.
-// Neighbour list: j with q <= -2/h_i (softened r <= h_i), appended with an atomic counter.
+// Nearest neighbour: the smallest key k = nn_key(s) over j != i (reported as q = -2/r_soft);
+// ties -> smallest j address.  Neighbour list: j with k <= key of h_i (softened r <= h_i),
+// appended with an atomic counter.
 #pragma once
 
 #include "pgb_common.cuh"
@@ -221,20 +224,29 @@ __device__ __forceinline__ float rel1(const Pos3& j, const Pos3& i, int c) {
     }
 }
 
-// The nearest-neighbour key of one pair: q = -2/r_soft (pgb::minus2_over_r), 0 for the self
-// pair.  Every path of the kernels computes q with exactly these operations, so a key found by
+// The initial nearest-neighbour key (gravity_kernel2's 10 in the reported scale) and the key
+// bound of an i-particle's neighbour radius h (gravity.c:688-695: -2/h, or -1e10 when h2 == 0:
+// no neighbours; none for a padding slot), both in the kernels' key scale.
+constexpr float G6_KEY0 = 10.0f / KEY_OUT;
+__device__ __forceinline__ float g6_hkey(bool real, float h2) {
+    if (!real) return -INFINITY;
+    return h2 == 0.0f ? -1e10f / KEY_OUT : (-2.0f / KEY_OUT) / sqrtf(h2);
+}
+
+// The nearest-neighbour key of one pair: nn_key of the pair scale, that of s = 0 for the self
+// pair.  Every path of the kernels computes it with exactly these operations, so a key found by
 // one pass can be looked up again by another (g6_rescan).
 template <bool FF>
 __device__ __forceinline__ float g6_key(const G6PredJ& J, const Pos3& I, int idi, float eps2) {
     const float dx = rel1<FF>(J.p, I, 0), dy = rel1<FF>(J.p, I, 1), dz = rel1<FF>(J.p, I, 2);
     const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmaf_rn(dx, dx, eps2)));
-    const float q = minus2_over_r(r2);
-    return (J.id == idi) ? 0.0f : q;
+    const float s = pair_scale(r2);
+    return nn_key((J.id == idi) ? 0.0f : s);
 }
 
 // Nearest-neighbour bookkeeping per pair, two forms:
 //  * select (NN, !TILEMIN): kmin/kadr updated per pair with strict '<' in j order;
-//  * tile minimum (TILEMIN): only tmin = min(tmin, q) per pair (one FMNMX); the caller keeps,
+//  * tile minimum (TILEMIN): only tmin = min(tmin, k) per pair (one FMNMX); the caller keeps,
 //    per j-tile, whether the tile improved the running minimum and recovers the address of the
 //    best tile's first minimal key afterwards (g6_rescan) -- the same (key, smallest address)
 //    result with one instruction per pair instead of three.
@@ -249,27 +261,28 @@ __device__ __forceinline__ void g6_pair(const G6PredJ& J, int jadr, const Pos3& 
     float dz = rel1<FF>(J.p, I, 2);
     float dvx = J.vx - vxi, dvy = J.vy - vyi, dvz = J.vz - vzi;
     float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmaf_rn(dx, dx, eps2)));
-    float q = minus2_over_r(r2);
-    if constexpr (SELF) q = (J.id == idi) ? 0.0f : q;
+    float s = pair_scale(r2);
+    if constexpr (SELF) s = (J.id == idi) ? 0.0f : s;
     if constexpr (NN && TILEMIN) {
-        kmin = fminf(kmin, q);
+        kmin = fminf(kmin, nn_key(s));
     } else if constexpr (NN) {
-        bool lt = q < kmin;
-        kmin = lt ? q : kmin;
+        const float k = nn_key(s);
+        bool lt = k < kmin;
+        kmin = lt ? k : kmin;
         kadr = lt ? jadr : kadr;
     }
     if constexpr (NBL) {
-        if (q <= hinv) {
+        if (nn_key(s) <= hinv) {
             int slot = atomicAdd(nbc, 1);
             if (slot < nbmax) nbl[slot] = jadr;
         }
     }
-    a.pot = __fmaf_rn(J.m, q, a.pot);
+    a.pot = __fmaf_rn(J.m, s, a.pot);
     float rv = __fmaf_rn(dz, dvz, __fmaf_rn(dy, dvy, dx * dvx));
-    float mq = J.m * q;
-    float q2 = q * q;
-    float mq3 = mq * q2;
-    float c = -0.75f * q2 * rv;
+    float ms = J.m * s;
+    float s2 = s * s;
+    float mq3 = ms * s2;
+    float c = S_JERK * s2 * rv;
     a.ax = __fmaf_rn(mq3, dx, a.ax);
     a.ay = __fmaf_rn(mq3, dy, a.ay);
     a.az = __fmaf_rn(mq3, dz, a.az);
@@ -304,27 +317,28 @@ __device__ __forceinline__ void g6_pair2(const G6PredJ& J, int jadr, const Pos3*
         dvy[k] = J.vy - vyi[k];
         dvz[k] = J.vz - vzi[k];
         float r2 = __fmaf_rn(dz[k], dz[k], __fmaf_rn(dy[k], dy[k], __fmaf_rn(dx[k], dx[k], eps2)));
-        float q = minus2_over_r(r2);
-        if constexpr (SELF) q = (J.id == idi[k]) ? 0.0f : q;
+        float s = pair_scale(r2);
+        if constexpr (SELF) s = (J.id == idi[k]) ? 0.0f : s;
         if constexpr (NN && TILEMIN) {
-            kmin[k] = fminf(kmin[k], q);
+            kmin[k] = fminf(kmin[k], nn_key(s));
         } else if constexpr (NN) {
-            bool lt = q < kmin[k];
-            kmin[k] = lt ? q : kmin[k];
+            const float kk = nn_key(s);
+            bool lt = kk < kmin[k];
+            kmin[k] = lt ? kk : kmin[k];
             kadr[k] = lt ? jadr : kadr[k];
         }
         if constexpr (NBL) {
-            if (q <= hinv[k]) {
+            if (nn_key(s) <= hinv[k]) {
                 int slot = atomicAdd(nbc[k], 1);
                 if (slot < nbmax) nbl[k][slot] = jadr;
             }
         }
-        a.pot[k] = __fmaf_rn(J.m, q, a.pot[k]);
+        a.pot[k] = __fmaf_rn(J.m, s, a.pot[k]);
         float rv = __fmaf_rn(dz[k], dvz[k], __fmaf_rn(dy[k], dvy[k], dx[k] * dvx[k]));
-        float mq = J.m * q;
-        float q2 = q * q;
-        mq3[k] = mq * q2;
-        c[k] = -0.75f * q2 * rv;
+        float ms = J.m * s;
+        float s2 = s * s;
+        mq3[k] = ms * s2;
+        c[k] = S_JERK * s2 * rv;
     }
     const float2 M = make_float2(mq3[0], mq3[1]), C = make_float2(c[0], c[1]);
     const float2 DX = make_float2(dx[0], dx[1]), DY = make_float2(dy[0], dy[1]), DZ = make_float2(dz[0], dz[1]);
@@ -390,15 +404,15 @@ __device__ __forceinline__ void g6_jpair(float2 xh, float2 yh, float2 zh, float2
         dvyp[h] = vyp[h] - I.vy;
         dvzp[h] = vzp[h] - I.vz;
         const float r2 = __fmaf_rn(dzp[h], dzp[h], __fmaf_rn(dyp[h], dyp[h], __fmaf_rn(dxp[h], dxp[h], eps2)));
-        float q = minus2_over_r(r2);
-        if constexpr (SELF) q = (idp[h] == I.id) ? 0.0f : q;
-        if constexpr (NN) tmin = fminf(tmin, q);
-        a.pot[h] = __fmaf_rn(mp[h], q, a.pot[h]);
+        float s = pair_scale(r2);
+        if constexpr (SELF) s = (idp[h] == I.id) ? 0.0f : s;
+        if constexpr (NN) tmin = fminf(tmin, nn_key(s));
+        a.pot[h] = __fmaf_rn(mp[h], s, a.pot[h]);
         const float rv = __fmaf_rn(dzp[h], dvzp[h], __fmaf_rn(dyp[h], dvyp[h], dxp[h] * dvxp[h]));
-        const float mq = mp[h] * q;
-        const float q2 = q * q;
-        mq3p[h] = mq * q2;
-        cp[h] = -0.75f * q2 * rv;
+        const float ms = mp[h] * s;
+        const float s2 = s * s;
+        mq3p[h] = ms * s2;
+        cp[h] = S_JERK * s2 * rv;
     }
     a.ax = __ffma2_rn(mq3, dx, a.ax);
     a.ay = __ffma2_rn(mq3, dy, a.ay);
@@ -458,16 +472,16 @@ __device__ __forceinline__ void g6_jquad2(const float4& XH, const float4& YH, co
         const int c = l >> 1, h = l & 1;
         const G6IPair& I = IP[c >> 1];
         const int jj = ((c & 1) << 1) + h;
-        float q = minus2_from_rsqrt(r2[l], y[l]);
-        if constexpr (SELF) q = (ids[jj] == I.id) ? 0.0f : q;
-        if constexpr (NN) tmin[c >> 1] = fminf(tmin[c >> 1], q);
-        a[c >> 1].pot[h] = __fmaf_rn(ms[jj], q, a[c >> 1].pot[h]);
+        float s = pair_scale_from_rsqrt(r2[l], y[l]);
+        if constexpr (SELF) s = (ids[jj] == I.id) ? 0.0f : s;
+        if constexpr (NN) tmin[c >> 1] = fminf(tmin[c >> 1], nn_key(s));
+        a[c >> 1].pot[h] = __fmaf_rn(ms[jj], s, a[c >> 1].pot[h]);
         const float ddx = h ? dx[c].y : dx[c].x, ddy = h ? dy[c].y : dy[c].x, ddz = h ? dz[c].y : dz[c].x;
         const float rv = __fmaf_rn(ddz, dvz[l], __fmaf_rn(ddy, dvy[l], ddx * dvx[l]));
-        const float mq = ms[jj] * q;
-        const float q2 = q * q;
-        mq3[l] = mq * q2;
-        cc[l] = -0.75f * q2 * rv;
+        const float msq = ms[jj] * s;
+        const float s2 = s * s;
+        mq3[l] = msq * s2;
+        cc[l] = S_JERK * s2 * rv;
     }
 #pragma unroll
     for (int c = 0; c < 4; c++) {
@@ -505,14 +519,14 @@ __device__ __forceinline__ int g6_rescan(const G6PredJ* __restrict__ jpred, int 
 
 __device__ __forceinline__ G6Out g6_finish(const G6Out& s) {
     G6Out o;
-    o.ax = -0.125 * s.ax;
-    o.ay = -0.125 * s.ay;
-    o.az = -0.125 * s.az;
-    o.jx = -0.125 * s.jx;
-    o.jy = -0.125 * s.jy;
-    o.jz = -0.125 * s.jz;
-    o.pot = 0.5 * s.pot;
-    o.key = s.key;
+    o.ax = S_ACC * s.ax;
+    o.ay = S_ACC * s.ay;
+    o.az = S_ACC * s.az;
+    o.jx = S_ACC * s.jx;
+    o.jy = S_ACC * s.jy;
+    o.jz = S_ACC * s.jz;
+    o.pot = S_POT * s.pot;
+    o.key = key_out(s.key);
     o.jadr = s.jadr;
     return o;
 }
@@ -560,6 +574,15 @@ __device__ __forceinline__ double2 word_add(double2 s, double2 v, bool w3) {
 __device__ __forceinline__ double2 word_zero(bool w3) {
     // word 3: key +inf, address -1 (every real candidate is better)
     return make_double2(0.0, w3 ? __longlong_as_double((long long)0xffffffff7f800000ULL) : 0.0);
+}
+
+// A finished result word: the sums times the scale's constants, the key as reported.
+__device__ __forceinline__ double2 word_finish(double2 v, bool w3) {
+    if (!w3) return make_double2(S_ACC * v.x, S_ACC * v.y);
+    const long long b = __double_as_longlong(v.y);
+    const float k = key_out(__int_as_float((int)(b & 0xffffffffLL)));
+    const long long packed = (b & ~0xffffffffLL) | (long long)(unsigned)__float_as_int(k);
+    return make_double2(S_POT * v.x, __longlong_as_double(packed));
 }
 
 // Sum `nrows` partial rows (row r at base + r*stride G6Out) word by word over the words
@@ -622,10 +645,7 @@ __device__ __forceinline__ void reduce_rows(const G6Out* base, size_t stride, in
         } else if (k >= nw) {
             continue;
         }
-        if (finish) {
-            s0.x *= w3 ? 0.5 : -0.125;
-            if (!w3) s0.y *= -0.125;
-        }
+        if (finish) s0 = word_finish(s0, w3);
         out[f] = s0;
     }
 }
@@ -692,12 +712,12 @@ __device__ __forceinline__ void g6_task(const G6Args& A, const Task& T, unsigned
         vxi[k] = P.vx; vyi[k] = P.vy; vzi[k] = P.vz;
         idi[k] = P.id;
         // gravity.c:688-695: -2/h, or -1e10 when h2 == 0 (no neighbours); padding lanes none
-        hinv[k] = (li >= T.ni) ? -INFINITY : ((P.h2 == 0.0f) ? -1e10f : -2.0f / sqrtf(P.h2));
+        hinv[k] = g6_hkey(li < T.ni, P.h2);
 #pragma unroll
         for (int c = 0; c < 7; c++) S[k][c] = 0.0;
-        kmin[k] = 10.0f;   // gravity_kernel2 starts its key at 10 and index at -1 (:495-496)
+        kmin[k] = G6_KEY0;   // gravity_kernel2 starts its key at 10 and index at -1 (:495-496)
         kadr[k] = -1;
-        tmin[k] = 10.0f;
+        tmin[k] = G6_KEY0;
         ktile[k] = -1;
     }
     // the i-tile's id range (padding slots repeat the tile's first i): published to the CTA by
@@ -1054,7 +1074,7 @@ __global__ void __launch_bounds__(128) g6_resolve_kernel(const G6Args A, int ngr
         const int a = o.jadr;
         if (a >= 0 && (a & G6_NN_TILE)) {
             tile = a & (G6_NN_TILE - 1);
-            key = o.key;
+            key = key_in(o.key);
         }
     }
     int found = 0x7fffffff;

@@ -96,10 +96,9 @@ __global__ void __launch_bounds__(ISL * JL, 2)
 
     const int ii = slot < A.ni ? slot : 0;
     const G6I P = s_i[ii];
-    // gravity.c:688-695: -2/h, or -1e10 when h2 == 0 (no neighbours); padding slots none
-    const float hinv = (slot >= A.ni) ? -INFINITY : ((P.h2 == 0.0f) ? -1e10f : -2.0f / sqrtf(P.h2));
+    const float hinv = g6_hkey(slot < A.ni, P.h2);
     double S[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    float kmin = 10.0f;  // gravity_kernel2's initial key and index (:495-496)
+    float kmin = G6_KEY0;  // gravity_kernel2's initial key and index (:495-496)
     int kadr = -1;
     int* nbc = NBL ? A.nb_count + ii : nullptr;
     int* nbl = NBL ? A.nb_list + (size_t)ii * A.nb_maxlen : nullptr;
@@ -146,9 +145,7 @@ __global__ void __launch_bounds__(ISL * JL, 2)
         for (int l = 1; l < JL; l++) v = word_add(v, rw[4 * (l * ISL + s) + wd], w3);
         if (nch == 1) {
             // the whole call in one CTA: final result directly
-            v.x *= w3 ? 0.5 : -0.125;
-            if (!w3) v.y *= -0.125;
-            reinterpret_cast<double2*>(A.out)[threadIdx.x] = v;
+            reinterpret_cast<double2*>(A.out)[threadIdx.x] = word_finish(v, w3);
         }
         cta_w[threadIdx.x] = v;
     }

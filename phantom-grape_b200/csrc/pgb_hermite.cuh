@@ -218,9 +218,9 @@ __device__ __forceinline__ G6Out hm_force_of(const HmWork& W, int k, int nch, in
 #pragma unroll
     for (int q = 0; q < 7; q++) s[q] = __shfl_sync(full, s[q], 0);
     G6Out F;
-    F.ax = -0.125 * s[0]; F.ay = -0.125 * s[1]; F.az = -0.125 * s[2];
-    F.jx = -0.125 * s[3]; F.jy = -0.125 * s[4]; F.jz = -0.125 * s[5];
-    F.pot = 0.5 * s[6];
+    F.ax = S_ACC * s[0]; F.ay = S_ACC * s[1]; F.az = S_ACC * s[2];
+    F.jx = S_ACC * s[3]; F.jy = S_ACC * s[4]; F.jz = S_ACC * s[5];
+    F.pot = S_POT * s[6];
     F.key = 0.f;
     F.jadr = -1;
     if (lane == 0) W.out[k] = F;

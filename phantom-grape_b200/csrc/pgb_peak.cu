@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(LOOP_NT) g6_loop_kernel(double* out, int passe
         IP[k].id = -1;
     }
     for (int c = 0; c < 14; c++) Ssh[c * LOOP_NT + t] = 0.0;
-    float tmin[2] = {10.f, 10.f};
+    float tmin[2] = {pgb::G6_KEY0, pgb::G6_KEY0};
     __syncthreads();
     for (int p = 0; p < passes; p++) {
         pgb::G6Acc2 a[2];
