@@ -62,16 +62,16 @@ PROFILED_TRAFFIC = {
     # the largest Hermite call by the configuration that runs it (6: 128x2 j-paired, 2: 128x2 i-paired)
     "hermite": {"bytes": 6_564_864 + 13_965_568,
                 "source": "profiles/g6_kernel_hermite_65536x65536.md (128x2 j-paired, 15 chunks)"},
-    "hermite_cfg9": {"bytes": 6_451_200 + 3_118_080,
-                     "source": "profiles/g6_kernel_hermite_65536x65536.md (128x2 j-paired, stage-ordered, 12 chunks)"},
+    "hermite_cfg9": {"bytes": 6_520_064 + 14_211_072,
+                     "source": "profiles/g6_kernel_hermite_65536x65536.md (128x2 j-paired, stage-ordered, 15 chunks)"},
     "hermite_cfg2": {"bytes": 6_578_944 + 17_873_152,
                      "source": "profiles/g6_kernel_hermite_65536x65536.md (128x2 i-paired)"},
-    "direct": {"bytes": 541_184, "pairs": 268_435_456,
+    "direct": {"bytes": 540_928, "pairs": 268_435_456,
                "source": "profiles/g5_kernels_direct_treepm_bh.md (1024x1 j-paired)"},
     "treepm": {"bytes": 557_901_056 + 35_891_456, "pairs": 4_463_983_086,
                "source": "profiles/g5_kernels_direct_treepm_bh.md (64x1)"},
     # captured at N = 2^20 (both launches of a step); scaled to the run's pairs
-    "bh": {"bytes": 131_887_616 + 26_603_264 + 228_129_792 + 31_506_944, "pairs": 4_462_862_693,
+    "bh": {"bytes": 131_828_224 + 26_739_456 + 227_582_208 + 31_331_072, "pairs": 4_462_862_693,
            "source": "profiles/g5_kernels_direct_treepm_bh.md (64x1, N=2^20 capture scaled by pairs)"},
 }
 
