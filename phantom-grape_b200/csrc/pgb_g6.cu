@@ -194,9 +194,9 @@ inline SmallShape small_shape(int ni) {
     if (ni <= 48) return {48, 10};
     return {64, 8};
 }
-// CTAs per cluster: with 4, every SM holds two of the co-resident CTAs (74 clusters on 148 SMs;
-// clusters of 8 fit 33, leaving 32 SMs with one CTA that the others wait for): the 48 x 65536
-// call 27.2 -> 26.6 us, 48 x 16384 23.0 -> 19.7 us
+// CTAs per cluster: 71 co-resident clusters of 4 (284 CTAs) leave 12 of the 148 SMs with one
+// CTA, where the 33 clusters of 8 left 32 (the others, with two, set the call's time): the
+// 48 x 65536 call 27.2 -> 26.6 us, 48 x 16384 23.0 -> 19.7 us
 constexpr int SMALL_CL = 4;
 
 template <int ISL, int JL, bool FF, bool NN, bool NBL>
