@@ -722,7 +722,7 @@ def run_hermite(args, pgb, ws, rank, local):
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_hermite(pgb, wl)
         cpu["fp64_check"] = hermite_fp64_check(pgb, wl, sub, calls, out_rows)
-    # the north star's FP64 relative coordinate (DADD + F2F), same schedule, same timing
+    # the FP64 relative coordinate (DADD + F2F, the reference's own split), same schedule, same timing
     f64line = None
     if ws == 1 and not args.no_f64_line and ff:
         s64 = torch.cuda.Stream(device=dev)

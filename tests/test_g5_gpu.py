@@ -3,7 +3,7 @@
 Every case is checked against the FP64 oracle (oracle/pg_oracle.c) and, where the reference
 library was compiled here (oracle/_ref), against the reference's own AVX2 result on the same
 inputs.  Tolerances:
-  * vs FP64: rms relative |da|/|a| <= 1e-6, rms relative pot error <= 1e-6 (north-star bar)
+  * vs FP64: rms relative |da|/|a| <= 1e-6, rms relative pot error <= 1e-6
   * vs reference AVX2: max relative |da|/|a| <= 2e-3 and pot <= 2e-5 (newton), and
     rms 1e-3 / max 1e-2 / pot 3e-4 (quadrupole cells), the reference's own error against
     FP64 (raw 12-bit rsqrt) being the floor.
