@@ -461,6 +461,9 @@ def hermite_batched(args, pgb, g6, wl, sub, calls, dev, s, ff, tune, steps, warm
     """The batched device path of the schedule (this rank's share): j-memory, i-records and
     results resident in HBM, one plan per call, the calls' (predict + force) launches captured in
     one CUDA graph; with several ranks the step ends with the all-gather of every rank's results.
+    Consecutive calls alternate between two streams and two predicted j-sets, so that a call's
+    predictor and nearest-neighbour lookups can run in the tail of the neighbouring call's force
+    launch (each stream keeps its own calls in order, which makes reusing its j-set safe).
     Times `steps` replays (CUDA events on the launching stream, L2 flushed in between), then each
     force launch alone.  Returns a dict of the figures and the resident buffers."""
     import torch
@@ -475,19 +478,30 @@ def hermite_batched(args, pgb, g6, wl, sub, calls, dev, s, ff, tune, steps, warm
     d_ptcl = torch.from_numpy(ptcl.view(np.uint8)).to(dev)
     d_irec = torch.from_numpy(irec.view(np.uint8)).to(dev)
     d_pred = torch.zeros(n * ffi.G6PREDJ.itemsize, dtype=torch.uint8, device=dev)
+    d_pred2 = torch.zeros_like(d_pred)
+    s2 = torch.cuda.Stream(device=dev)
     d_out = torch.zeros((max(nrow, 1), ffi.G6OUT.itemsize), dtype=torch.uint8, device=dev)
     live = [(c, loc, cnt) for c, loc, cnt in calls if cnt > 0]
     plans = {c: g6.plan_create([[loc, cnt, 0, n]], nn=True, f64=not ff) for c, loc, cnt in live}
 
-    def predict(c):
-        rc = g6.L.pgb6_predict(d_ptcl.data_ptr(), n, float(wl["t_calls"][c]), d_pred.data_ptr(), pflags,
-                               s.cuda_stream)
+    def predict(c, buf=None, stream=None):
+        buf = d_pred if buf is None else buf
+        stream = s if stream is None else stream
+        rc = g6.L.pgb6_predict(d_ptcl.data_ptr(), n, float(wl["t_calls"][c]), buf.data_ptr(), pflags,
+                               stream.cuda_stream)
         assert rc == 0, g6.last_error()
 
     def step_launches():
-        for c, _, _ in live:
-            predict(c)
-            g6.plan_launch(plans[c], d_irec.data_ptr(), d_pred.data_ptr(), st.eps2, d_out.data_ptr(), s.cuda_stream)
+        fork = torch.cuda.Event()
+        fork.record(s)
+        s2.wait_event(fork)
+        for k, (c, _, _) in enumerate(live):
+            stream, buf = (s, d_pred) if k % 2 == 0 else (s2, d_pred2)
+            predict(c, buf, stream)
+            g6.plan_launch(plans[c], d_irec.data_ptr(), buf.data_ptr(), st.eps2, d_out.data_ptr(), stream.cuda_stream)
+        join = torch.cuda.Event()
+        join.record(s2)
+        s.wait_event(join)
 
     with torch.cuda.stream(s):
         step_launches()
@@ -783,7 +797,8 @@ def run_hermite(args, pgb, ws, rank, local):
         "setup": {"sharding": (f"i-partition x{ws}: every rank predicts all j and computes a contiguous slice of "
                                "each call's active set; results all-gathered (NCCL) inside the timed step")
                   if ws > 1 else "one GPU",
-                  "graph": "64 x (predict + persistent force launch) in one CUDA graph",
+                  "graph": "64 x (predict + persistent force launch) in one CUDA graph, consecutive calls on "
+                           "two streams with two predicted j-sets",
                   "relative_coordinates": "double-float (hi+lo FP32)" if ff else "FP64 subtract + F2F",
                   "rsqrt": "rsqrt.approx alone, q = -2 y (lib/libpg6.so)"},
         "frac_fp32": round(value * 1e9 * 60 / 1e12 / fp32_tf, 4),
