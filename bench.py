@@ -86,6 +86,8 @@ def profiled_traffic(workload, pairs):
         return int(e["bytes"] * pairs / e["pairs"]), e["source"]
     return e["bytes"], e["source"]
 FP32_LANES = 128
+HERMITE_STREAMS = 3   # streams of the batched Hermite schedule (see hermite_batched; C2 step:
+                      # 818 Gint/s on one stream, 858 on two, 866 on three)
 
 
 def load_pkg():
@@ -461,7 +463,7 @@ def hermite_batched(args, pgb, g6, wl, sub, calls, dev, s, ff, tune, steps, warm
     """The batched device path of the schedule (this rank's share): j-memory, i-records and
     results resident in HBM, one plan per call, the calls' (predict + force) launches captured in
     one CUDA graph; with several ranks the step ends with the all-gather of every rank's results.
-    Consecutive calls alternate between two streams and two predicted j-sets, so that a call's
+    Consecutive calls alternate between HERMITE_STREAMS streams and predicted j-sets, so that a call's
     predictor and nearest-neighbour lookups can run in the tail of the neighbouring call's force
     launch (each stream keeps its own calls in order, which makes reusing its j-set safe).
     Times `steps` replays (CUDA events on the launching stream, L2 flushed in between), then each
@@ -478,8 +480,10 @@ def hermite_batched(args, pgb, g6, wl, sub, calls, dev, s, ff, tune, steps, warm
     d_ptcl = torch.from_numpy(ptcl.view(np.uint8)).to(dev)
     d_irec = torch.from_numpy(irec.view(np.uint8)).to(dev)
     d_pred = torch.zeros(n * ffi.G6PREDJ.itemsize, dtype=torch.uint8, device=dev)
-    d_pred2 = torch.zeros_like(d_pred)
-    s2 = torch.cuda.Stream(device=dev)
+    # the streams the calls alternate between (the launching stream first), each with its own
+    # predicted j-set
+    lanes = [(s, d_pred)] + [(torch.cuda.Stream(device=dev), torch.zeros_like(d_pred))
+                             for _ in range(HERMITE_STREAMS - 1)]
     d_out = torch.zeros((max(nrow, 1), ffi.G6OUT.itemsize), dtype=torch.uint8, device=dev)
     live = [(c, loc, cnt) for c, loc, cnt in calls if cnt > 0]
     plans = {c: g6.plan_create([[loc, cnt, 0, n]], nn=True, f64=not ff) for c, loc, cnt in live}
@@ -494,14 +498,16 @@ def hermite_batched(args, pgb, g6, wl, sub, calls, dev, s, ff, tune, steps, warm
     def step_launches():
         fork = torch.cuda.Event()
         fork.record(s)
-        s2.wait_event(fork)
+        for st2, _ in lanes[1:]:
+            st2.wait_event(fork)
         for k, (c, _, _) in enumerate(live):
-            stream, buf = (s, d_pred) if k % 2 == 0 else (s2, d_pred2)
+            stream, buf = lanes[k % len(lanes)]
             predict(c, buf, stream)
             g6.plan_launch(plans[c], d_irec.data_ptr(), buf.data_ptr(), st.eps2, d_out.data_ptr(), stream.cuda_stream)
-        join = torch.cuda.Event()
-        join.record(s2)
-        s.wait_event(join)
+        for st2, _ in lanes[1:]:
+            join = torch.cuda.Event()
+            join.record(st2)
+            s.wait_event(join)
 
     with torch.cuda.stream(s):
         step_launches()
@@ -798,7 +804,7 @@ def run_hermite(args, pgb, ws, rank, local):
                                "each call's active set; results all-gathered (NCCL) inside the timed step")
                   if ws > 1 else "one GPU",
                   "graph": "64 x (predict + persistent force launch) in one CUDA graph, consecutive calls on "
-                           "two streams with two predicted j-sets",
+                           f"{HERMITE_STREAMS} streams with a predicted j-set each",
                   "relative_coordinates": "double-float (hi+lo FP32)" if ff else "FP64 subtract + F2F",
                   "rsqrt": "rsqrt.approx alone, q = -2 y (lib/libpg6.so)"},
         "frac_fp32": round(value * 1e9 * 60 / 1e12 / fp32_tf, 4),
