@@ -355,12 +355,13 @@ __device__ __forceinline__ void g6_pair2(const G6PredJ& J, int jadr, const Pos3*
 // one array per field (G6TileSoA), so that a 16-byte shared load returns a field of four
 // consecutive j: every paired FP32 operand is then a natural register pair -- (j, j+1) for the
 // j fields, a loop-invariant (v, v) for the i fields -- and the double-float relative
-// coordinates (nine FADD per j-pair as paired FADD2) join the nine accumulations (FFMA2) on the
-// heavy half of the FMA pipe, while the rest of the chain (dv, r^2, the scale q, dx.dv and
-// the scalar factors: 16 per pair, 18 with the Newton step) stays scalar.  Per pair that is 9
-// paired + 16 scalar FP32 instructions, which loads the two halves of the FMA pipe about equally
-// (a paired instruction occupies the heavy half twice as long as a scalar one), against 4.5 + 25
-// in g6_pair2.
+// coordinates (nine FADD per j-pair as paired FADD2) and the velocity differences (three) join
+// the nine accumulations (FFMA2) on the heavy half of the FMA pipe, while the rest of the chain
+// (r^2, dx.dv and the scalar factors: 12 per pair, 15 with the Newton step) stays scalar.  Per
+// j-pair that is 21 paired + 2 x 12 scalar FP32 instructions; a paired instruction occupies the
+// heavy half twice as long as a scalar one.  With the velocity differences scalar as well the
+// largest Hermite call took 4.99 instead of 4.93 ms, with the relative coordinates scalar too
+// 5.10 ms.
 // The two lanes of each accumulator sum the even and the odd j of the tile; they are added
 // into the FP64 sums one after the other at every fold.  Per pair the key q is bit-identical
 // to g6_key (FADD2 rounds each lane as FADD does).
@@ -384,25 +385,23 @@ __device__ __forceinline__ void g6_jpair(float2 xh, float2 yh, float2 zh, float2
     const float2 dx = __fadd2_rn(__fadd2_rn(xh, I.nxh), __fadd2_rn(xl, I.nxl));
     const float2 dy = __fadd2_rn(__fadd2_rn(yh, I.nyh), __fadd2_rn(yl, I.nyl));
     const float2 dz = __fadd2_rn(__fadd2_rn(zh, I.nzh), __fadd2_rn(zl, I.nzl));
-    float2 dvx, dvy, dvz, mq3, c;
+    // v_j - v_i as v_j + (-v_i): each lane rounded as the scalar subtraction
+    const float2 dvx = __fadd2_rn(vx, make_float2(-I.vx, -I.vx));
+    const float2 dvy = __fadd2_rn(vy, make_float2(-I.vy, -I.vy));
+    const float2 dvz = __fadd2_rn(vz, make_float2(-I.vz, -I.vz));
+    float2 mq3, c;
     const float* dxp = &dx.x;
     const float* dyp = &dy.x;
     const float* dzp = &dz.x;
-    const float* vxp = &vx.x;
-    const float* vyp = &vy.x;
-    const float* vzp = &vz.x;
     const float* mp = &m.x;
     const int* idp = &jid.x;
-    float* dvxp = &dvx.x;
-    float* dvyp = &dvy.x;
-    float* dvzp = &dvz.x;
+    const float* dvxp = &dvx.x;
+    const float* dvyp = &dvy.x;
+    const float* dvzp = &dvz.x;
     float* mq3p = &mq3.x;
     float* cp = &c.x;
 #pragma unroll
     for (int h = 0; h < 2; h++) {
-        dvxp[h] = vxp[h] - I.vx;
-        dvyp[h] = vyp[h] - I.vy;
-        dvzp[h] = vzp[h] - I.vz;
         const float r2 = __fmaf_rn(dzp[h], dzp[h], __fmaf_rn(dyp[h], dyp[h], __fmaf_rn(dxp[h], dxp[h], eps2)));
         float s = pair_scale(r2);
         if constexpr (SELF) s = (idp[h] == I.id) ? 0.0f : s;
@@ -453,14 +452,20 @@ __device__ __forceinline__ void g6_jquad2(const float4& XH, const float4& YH, co
     const int ids[4] = {ID.x, ID.y, ID.z, ID.w};
     float r2[8], dvx[8], dvy[8], dvz[8];
 #pragma unroll
+    for (int c = 0; c < 4; c++) {
+        const G6IPair& I = IP[c >> 1];
+        const int j0 = (c & 1) << 1;
+        const float2 vx = __fadd2_rn(make_float2(vxs[j0], vxs[j0 + 1]), make_float2(-I.vx, -I.vx));
+        const float2 vy = __fadd2_rn(make_float2(vys[j0], vys[j0 + 1]), make_float2(-I.vy, -I.vy));
+        const float2 vz = __fadd2_rn(make_float2(vzs[j0], vzs[j0 + 1]), make_float2(-I.vz, -I.vz));
+        dvx[2 * c] = vx.x; dvx[2 * c + 1] = vx.y;
+        dvy[2 * c] = vy.x; dvy[2 * c + 1] = vy.y;
+        dvz[2 * c] = vz.x; dvz[2 * c + 1] = vz.y;
+    }
+#pragma unroll
     for (int l = 0; l < 8; l++) {
         const int c = l >> 1, h = l & 1;
-        const G6IPair& I = IP[c >> 1];
-        const int jj = ((c & 1) << 1) + h;
         const float ddx = h ? dx[c].y : dx[c].x, ddy = h ? dy[c].y : dy[c].x, ddz = h ? dz[c].y : dz[c].x;
-        dvx[l] = vxs[jj] - I.vx;
-        dvy[l] = vys[jj] - I.vy;
-        dvz[l] = vzs[jj] - I.vz;
         r2[l] = __fmaf_rn(ddz, ddz, __fmaf_rn(ddy, ddy, __fmaf_rn(ddx, ddx, eps2)));
     }
     float y[8];
