@@ -354,14 +354,12 @@ __device__ __forceinline__ void g6_pair2(const G6PredJ& J, int jadr, const Pos3*
 // One i-particle against two consecutive j (a "j-pair"), with the j-tile in shared memory as
 // one array per field (G6TileSoA), so that a 16-byte shared load returns a field of four
 // consecutive j: every paired FP32 operand is then a natural register pair -- (j, j+1) for the
-// j fields, a loop-invariant (v, v) for the i fields -- and the double-float relative
-// coordinates (nine FADD per j-pair as paired FADD2) and the velocity differences (three) join
-// the nine accumulations (FFMA2) on the heavy half of the FMA pipe, while the rest of the chain
-// (r^2, dx.dv and the scalar factors: 12 per pair, 15 with the Newton step) stays scalar.  Per
-// j-pair that is 21 paired + 2 x 12 scalar FP32 instructions; a paired instruction occupies the
-// heavy half twice as long as a scalar one.  With the velocity differences scalar as well the
-// largest Hermite call took 4.99 instead of 4.93 ms, with the relative coordinates scalar too
-// 5.10 ms.
+// j fields, a loop-invariant (v, v) for the i fields.  The double-float relative coordinates
+// (nine FADD2 per j-pair), the velocity differences (three), r^2 and dx.dv (three FFMA2 each)
+// and the nine accumulations issue paired; the scalar factors (6 per pair, 9 with the Newton
+// step) stay scalar: 27 paired + 2 x 6 scalar FP32 instructions per j-pair.  Measured on the
+// largest Hermite call: 4.80 ms, against 4.93 ms with r^2 and dx.dv scalar, 4.99 ms with the
+// velocity differences scalar as well and 5.10 ms with the relative coordinates scalar too.
 // The two lanes of each accumulator sum the even and the odd j of the tile; they are added
 // into the FP64 sums one after the other at every fold.  Per pair the key q is bit-identical
 // to g6_key (FADD2 rounds each lane as FADD does).
@@ -389,25 +387,21 @@ __device__ __forceinline__ void g6_jpair(float2 xh, float2 yh, float2 zh, float2
     const float2 dvx = __fadd2_rn(vx, make_float2(-I.vx, -I.vx));
     const float2 dvy = __fadd2_rn(vy, make_float2(-I.vy, -I.vy));
     const float2 dvz = __fadd2_rn(vz, make_float2(-I.vz, -I.vz));
+    // r^2 and dx.dv of both j, paired
+    const float2 r2v = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __ffma2_rn(dx, dx, make_float2(eps2, eps2))));
+    const float2 rvv = __ffma2_rn(dz, dvz, __ffma2_rn(dy, dvy, __fmul2_rn(dx, dvx)));
     float2 mq3, c;
-    const float* dxp = &dx.x;
-    const float* dyp = &dy.x;
-    const float* dzp = &dz.x;
     const float* mp = &m.x;
     const int* idp = &jid.x;
-    const float* dvxp = &dvx.x;
-    const float* dvyp = &dvy.x;
-    const float* dvzp = &dvz.x;
     float* mq3p = &mq3.x;
     float* cp = &c.x;
 #pragma unroll
     for (int h = 0; h < 2; h++) {
-        const float r2 = __fmaf_rn(dzp[h], dzp[h], __fmaf_rn(dyp[h], dyp[h], __fmaf_rn(dxp[h], dxp[h], eps2)));
-        float s = pair_scale(r2);
+        float s = pair_scale((&r2v.x)[h]);
         if constexpr (SELF) s = (idp[h] == I.id) ? 0.0f : s;
         if constexpr (NN) tmin = fminf(tmin, nn_key(s));
         a.pot[h] = __fmaf_rn(mp[h], s, a.pot[h]);
-        const float rv = __fmaf_rn(dzp[h], dvzp[h], __fmaf_rn(dyp[h], dvyp[h], dxp[h] * dvxp[h]));
+        const float rv = (&rvv.x)[h];
         const float ms = mp[h] * s;
         const float s2 = s * s;
         mq3p[h] = ms * s2;
@@ -462,11 +456,17 @@ __device__ __forceinline__ void g6_jquad2(const float4& XH, const float4& YH, co
         dvy[2 * c] = vy.x; dvy[2 * c + 1] = vy.y;
         dvz[2 * c] = vz.x; dvz[2 * c + 1] = vz.y;
     }
+    float rvv[8];
 #pragma unroll
-    for (int l = 0; l < 8; l++) {
-        const int c = l >> 1, h = l & 1;
-        const float ddx = h ? dx[c].y : dx[c].x, ddy = h ? dy[c].y : dy[c].x, ddz = h ? dz[c].y : dz[c].x;
-        r2[l] = __fmaf_rn(ddz, ddz, __fmaf_rn(ddy, ddy, __fmaf_rn(ddx, ddx, eps2)));
+    for (int c = 0; c < 4; c++) {
+        const float2 r = __ffma2_rn(dz[c], dz[c], __ffma2_rn(dy[c], dy[c], __ffma2_rn(dx[c], dx[c], make_float2(eps2, eps2))));
+        r2[2 * c] = r.x;
+        r2[2 * c + 1] = r.y;
+        const float2 v = __ffma2_rn(dz[c], make_float2(dvz[2 * c], dvz[2 * c + 1]),
+                                    __ffma2_rn(dy[c], make_float2(dvy[2 * c], dvy[2 * c + 1]),
+                                               __fmul2_rn(dx[c], make_float2(dvx[2 * c], dvx[2 * c + 1]))));
+        rvv[2 * c] = v.x;
+        rvv[2 * c + 1] = v.y;
     }
     float y[8];
 #pragma unroll
@@ -481,8 +481,7 @@ __device__ __forceinline__ void g6_jquad2(const float4& XH, const float4& YH, co
         if constexpr (SELF) s = (ids[jj] == I.id) ? 0.0f : s;
         if constexpr (NN) tmin[c >> 1] = fminf(tmin[c >> 1], nn_key(s));
         a[c >> 1].pot[h] = __fmaf_rn(ms[jj], s, a[c >> 1].pot[h]);
-        const float ddx = h ? dx[c].y : dx[c].x, ddy = h ? dy[c].y : dy[c].x, ddz = h ? dz[c].y : dz[c].x;
-        const float rv = __fmaf_rn(ddz, dvz[l], __fmaf_rn(ddy, dvy[l], ddx * dvx[l]));
+        const float rv = rvv[l];
         const float msq = ms[jj] * s;
         const float s2 = s * s;
         mq3[l] = msq * s2;
