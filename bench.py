@@ -62,8 +62,8 @@ PROFILED_TRAFFIC = {
     # the largest Hermite call by the configuration that runs it (6: 128x2 j-paired, 2: 128x2 i-paired)
     "hermite": {"bytes": 6_564_864 + 13_965_568,
                 "source": "profiles/g6_kernel_hermite_65536x65536.md (128x2 j-paired, 15 chunks)"},
-    "hermite_cfg9": {"bytes": 6_653_440 + 14_401_792,
-                     "source": "profiles/g6_kernel_hermite_65536x65536.md (128x2 j-paired, stage-ordered, 15 chunks)"},
+    "hermite_cfg9": {"bytes": 6_416_384 + 72_704,
+                     "source": "profiles/g6_kernel_hermite_65536x65536.md (128x2 j-paired, stage-ordered, 8 chunks)"},
     "hermite_cfg2": {"bytes": 6_578_944 + 17_873_152,
                      "source": "profiles/g6_kernel_hermite_65536x65536.md (128x2 i-paired)"},
     "direct": {"bytes": 540_928, "pairs": 268_435_456,
