@@ -355,11 +355,13 @@ __device__ __forceinline__ void g6_pair2(const G6PredJ& J, int jadr, const Pos3*
 // one array per field (G6TileSoA), so that a 16-byte shared load returns a field of four
 // consecutive j: every paired FP32 operand is then a natural register pair -- (j, j+1) for the
 // j fields, a loop-invariant (v, v) for the i fields.  The double-float relative coordinates
-// (nine FADD2 per j-pair), the velocity differences (three), r^2 and dx.dv (three FFMA2 each)
-// and the nine accumulations issue paired; the scalar factors (6 per pair, 9 with the Newton
-// step) stay scalar: 27 paired + 2 x 6 scalar FP32 instructions per j-pair.  Measured on the
-// largest Hermite call: 4.80 ms, against 4.93 ms with r^2 and dx.dv scalar, 4.99 ms with the
-// velocity differences scalar as well and 5.10 ms with the relative coordinates scalar too.
+// (nine FADD2 per j-pair), the velocity differences (three), r^2 and dx.dv (three FFMA2 each),
+// the potential and the factors m s, s^2, m s^3 and S_JERK s^2 (dx.dv) (six) and the nine
+// accumulations issue paired: 33 paired FP32 instructions per j-pair, only the rsqrt (and the
+// Newton step's 3 operations), the self select and the key minimum stay per lane.  Measured on
+// the largest Hermite call: 4.69 ms, against 4.75 ms with the potential scalar, 4.82 ms with
+// all six factors scalar, 4.93 ms with r^2 and dx.dv scalar as well, 4.99 ms with the velocity
+// differences scalar too and 5.10 ms with the relative coordinates scalar also.
 // The two lanes of each accumulator sum the even and the odd j of the tile; they are added
 // into the FP64 sums one after the other at every fold.  Per pair the key q is bit-identical
 // to g6_key (FADD2 rounds each lane as FADD does).
@@ -390,23 +392,25 @@ __device__ __forceinline__ void g6_jpair(float2 xh, float2 yh, float2 zh, float2
     // r^2 and dx.dv of both j, paired
     const float2 r2v = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __ffma2_rn(dx, dx, make_float2(eps2, eps2))));
     const float2 rvv = __ffma2_rn(dz, dvz, __ffma2_rn(dy, dvy, __fmul2_rn(dx, dvx)));
-    float2 mq3, c;
+    float2 sv;
     const float* mp = &m.x;
     const int* idp = &jid.x;
-    float* mq3p = &mq3.x;
-    float* cp = &c.x;
 #pragma unroll
     for (int h = 0; h < 2; h++) {
         float s = pair_scale((&r2v.x)[h]);
         if constexpr (SELF) s = (idp[h] == I.id) ? 0.0f : s;
         if constexpr (NN) tmin = fminf(tmin, nn_key(s));
-        a.pot[h] = __fmaf_rn(mp[h], s, a.pot[h]);
-        const float rv = (&rvv.x)[h];
-        const float ms = mp[h] * s;
-        const float s2 = s * s;
-        mq3p[h] = ms * s2;
-        cp[h] = S_JERK * s2 * rv;
+        (&sv.x)[h] = s;
     }
+    {
+        float2 P = make_float2(a.pot[0], a.pot[1]);
+        P = __ffma2_rn(m, sv, P);
+        a.pot[0] = P.x;
+        a.pot[1] = P.y;
+    }
+    const float2 s2 = __fmul2_rn(sv, sv);
+    const float2 mq3 = __fmul2_rn(__fmul2_rn(m, sv), s2);
+    const float2 c = __fmul2_rn(__fmul2_rn(make_float2(S_JERK, S_JERK), s2), rvv);
     a.ax = __ffma2_rn(mq3, dx, a.ax);
     a.ay = __ffma2_rn(mq3, dy, a.ay);
     a.az = __ffma2_rn(mq3, dz, a.az);
@@ -417,7 +421,7 @@ __device__ __forceinline__ void g6_jpair(float2 xh, float2 yh, float2 zh, float2
 
 // The j-paired form for two i, stage-ordered: the four j-pair chains of a j-quad (two i x two
 // j-pairs) advanced together stage by stage -- relative coordinates, dv and r^2, the eight
-// rsqrt, the scales q and the scalar factors, the accumulations -- which hands the scheduler
+// rsqrt and the scales s, the paired potential, factors and accumulations -- which hands the scheduler
 // independent work in every stage (largest Hermite call 5.65 against 5.77 ms for the chain-by-
 // chain order of g6_jpair; the autotuner chooses between them per call size).  The same
 // operations as g6_jpair on the same values: bit-identical results.
@@ -471,7 +475,7 @@ __device__ __forceinline__ void g6_jquad2(const float4& XH, const float4& YH, co
     float y[8];
 #pragma unroll
     for (int l = 0; l < 8; l++) y[l] = mufu_rsqrt(r2[l]);
-    float mq3[8], cc[8];
+    float sv[8];
 #pragma unroll
     for (int l = 0; l < 8; l++) {
         const int c = l >> 1, h = l & 1;
@@ -480,17 +484,22 @@ __device__ __forceinline__ void g6_jquad2(const float4& XH, const float4& YH, co
         float s = pair_scale_from_rsqrt(r2[l], y[l]);
         if constexpr (SELF) s = (ids[jj] == I.id) ? 0.0f : s;
         if constexpr (NN) tmin[c >> 1] = fminf(tmin[c >> 1], nn_key(s));
-        a[c >> 1].pot[h] = __fmaf_rn(ms[jj], s, a[c >> 1].pot[h]);
-        const float rv = rvv[l];
-        const float msq = ms[jj] * s;
-        const float s2 = s * s;
-        mq3[l] = msq * s2;
-        cc[l] = S_JERK * s2 * rv;
+        sv[l] = s;
     }
 #pragma unroll
     for (int c = 0; c < 4; c++) {
         G6Acc2& A = a[c >> 1];
-        const float2 M3 = make_float2(mq3[2 * c], mq3[2 * c + 1]), C2 = make_float2(cc[2 * c], cc[2 * c + 1]);
+        const int j0 = (c & 1) << 1;
+        const float2 S = make_float2(sv[2 * c], sv[2 * c + 1]), MJ = make_float2(ms[j0], ms[j0 + 1]);
+        {
+            float2 P = make_float2(A.pot[0], A.pot[1]);
+            P = __ffma2_rn(MJ, S, P);
+            A.pot[0] = P.x;
+            A.pot[1] = P.y;
+        }
+        const float2 S2 = __fmul2_rn(S, S);
+        const float2 M3 = __fmul2_rn(__fmul2_rn(MJ, S), S2);
+        const float2 C2 = __fmul2_rn(__fmul2_rn(make_float2(S_JERK, S_JERK), S2), make_float2(rvv[2 * c], rvv[2 * c + 1]));
         A.ax = __ffma2_rn(M3, dx[c], A.ax);
         A.ay = __ffma2_rn(M3, dy[c], A.ay);
         A.az = __ffma2_rn(M3, dz[c], A.az);
