@@ -297,7 +297,11 @@ __device__ __forceinline__ void g5_newton_jpair(float2 X, float2 Y, float2 Z, fl
 }
 
 // Q = (q00 q01 q02 q11 q12 q22) of the two cells, as pairs, staged as Q' = G5_QSCALE Q: the
-// arithmetic of g5_quad_pair, the moment products, D and the sums paired.
+// arithmetic of g5_quad_pair with every FP32 operation paired (the moment products, D, r^2, the
+// factors q^2 .. w and the sums; only the rsqrt runs per lane), each lane rounded as the scalar
+// operation.  An earlier form computed r^2 and the factors per lane (23 paired + 2 x 10 scalar
+// instructions per j-pair); pairing them as well (33 paired) follows the Hermite j-paired forms,
+// where the same move made the largest call 5 % faster.
 __device__ __forceinline__ void g5_quad_jpair(float2 X, float2 Y, float2 Z, float2 M, const float2 (&Q)[6], float2 nx,
                                               float2 ny, float2 nz, float e, float2 (&a)[5]) {
     const float2 dx = __fadd2_rn(X, nx), dy = __fadd2_rn(Y, ny), dz = __fadd2_rn(Z, nz);
@@ -305,23 +309,11 @@ __device__ __forceinline__ void g5_quad_jpair(float2 X, float2 Y, float2 Z, floa
     const float2 vy = __ffma2_rn(Q[4], dz, __ffma2_rn(Q[3], dy, __fmul2_rn(Q[1], dx)));
     const float2 vz = __ffma2_rn(Q[5], dz, __ffma2_rn(Q[4], dy, __fmul2_rn(Q[2], dx)));
     const float2 D = __ffma2_rn(dz, vz, __ffma2_rn(dy, vy, __fmul2_rn(dx, vx)));
-    float2 q, p, w;
-    const float* dxp = &dx.x;
-    const float* dyp = &dy.x;
-    const float* dzp = &dz.x;
-    const float* Dp = &D.x;
-    const float* mp = &M.x;
-    float* qp = &q.x;
-    float* pp = &p.x;
-    float* wp = &w.x;
-#pragma unroll
-    for (int h = 0; h < 2; h++) {
-        const float r2 = __fmaf_rn(dzp[h], dzp[h], __fmaf_rn(dyp[h], dyp[h], __fmaf_rn(dxp[h], dxp[h], e)));
-        qp[h] = pair_scale(r2);
-        const float q2 = qp[h] * qp[h], q3 = q2 * qp[h], q4 = q2 * q2;
-        pp[h] = q4 * (G5_QK * qp[h]);
-        wp[h] = q3 * __fmaf_rn(Dp[h], q4, mp[h]);
-    }
+    const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __ffma2_rn(dx, dx, make_float2(e, e))));
+    const float2 q = make_float2(pair_scale(r2.x), pair_scale(r2.y));
+    const float2 q2 = __fmul2_rn(q, q), q3 = __fmul2_rn(q2, q), q4 = __fmul2_rn(q2, q2);
+    const float2 p = __fmul2_rn(q4, __fmul2_rn(make_float2(G5_QK, G5_QK), q));
+    const float2 w = __fmul2_rn(q3, __ffma2_rn(D, q4, M));
     a[0] = __ffma2_rn(w, dx, __ffma2_rn(p, vx, a[0]));
     a[1] = __ffma2_rn(w, dy, __ffma2_rn(p, vy, a[1]));
     a[2] = __ffma2_rn(w, dz, __ffma2_rn(p, vz, a[2]));
